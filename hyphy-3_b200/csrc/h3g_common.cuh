@@ -1,0 +1,93 @@
+// h3g_common.cuh — device-side layout shared by the FP64 and mixed-precision paths.
+//
+// HBM layout (one problem = one tree x one compressed alignment):
+//   states / masks     [T][Pp]              leaf observations, taxon-major so a
+//                                           pattern tile of one taxon is contiguous
+//   P, PT, dP          [M][n][64*64]        per rate class and branch, 61 states
+//                                           zero-padded to 64 (PT = transpose)
+//   D, Ms, U           [NI][M][64][Pp]      inside partial, P*D message to the
+//                                           parent, outside partial; state-major so
+//                                           a warp reading one state of 32
+//                                           consecutive patterns is coalesced
+//   Ecum, Eown         [NI][M][Pp]          power-of-two scaling exponents
+//   Vf                 [n][M][64][Pp]       outside vector at the top of each branch
+//                                           times w_p * posterior_m / L_m
+// Leaves never get a partial: their message P_b * leaf_vector is a column of P_b
+// (a row of PT_b), a masked column sum, or the P_b row sums for missing data.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace h3g {
+
+constexpr int SP = 64;       // padded state count (61 sense codons -> 64)
+constexpr int SP2 = SP * SP; // one padded matrix
+constexpr int TP = 64;       // patterns per CTA in the pruning kernels (one thread per pattern)
+constexpr int kRescaleBits = 256;  // rescale a partial when its max falls below 2^-256
+constexpr int kMaxRateClasses = 16;
+
+struct Topo {
+    int n, root, NI, T, P, Pp, S;
+    const int* ch_off;       // [n+1] children CSR, children in increasing id order
+    const int* ch;
+    const int* iidx;         // [n] internal-node slot, -1 for leaves
+    const uint8_t* leaf;     // [n]
+    const int* taxon;        // [n] alignment row of a leaf, -1 = missing
+    const int8_t* states;    // [T][Pp]
+    const uint64_t* masks;   // [T][Pp]
+    const double* w;         // [Pp] pattern weights, 0 on padding
+    uint64_t all_mask;
+};
+
+struct Model {
+    int M, K, has_bg, nmod, time_mode, ndirs, sentinel;
+    const double* pi;        // [64]
+    const double* Q;         // [nmod][64*64]
+    const double* lam;       // [nmod][64]
+    const double* U;         // [nmod][64*64]
+    const double* V;         // [nmod][64*64]
+    const double* mu;        // [nmod]
+    const double* class_w;   // [K]
+    const double* rates;     // [M]
+    const double* rate_w;    // [M]
+    const uint8_t* is_test;  // [n] or null
+    const double* dQ;        // [ndirs][nmod][64*64]
+};
+
+struct Work {
+    const double* bl;        // [n]
+    double* P;               // [M][n][64*64]
+    double* PT;              // [M][n][64*64]
+    double* dP;              // [M][n][64*64]
+    double* rs;              // [M][n][64] row sums of P
+    double* D;               // [NI][M][64][Pp]
+    double* Ms;              // [NI][M][64][Pp]
+    double* U;               // [NI][M][64][Pp]
+    int* Ecum;               // [NI][M][Pp]
+    int* Eown;               // [NI][M][Pp]
+    double* Vf;              // [n][M][64][Pp]
+    double* f;               // [M][Pp]   w_p * post_{m,p} / L_{m,p}
+    double* contrib;         // [Pp]      this pattern's term of lnL
+    double* site;            // [Pp]      per-pattern lnL
+    double* rw;              // [M][Pp]   w_p * post_{m,p} / rho_m
+    int nchunk, chunk;
+    double* Apart;           // [n][M][nchunk][64*64]
+    double* gt;              // [M][n]    <A_{m,b}, dP_{m,b}>
+    double* Hpart;           // [nmod][M][n][64*64]
+    double* gc;              // [K][M][n] <A_{m,b}, P_k(tau)>
+    double* stg;             // [nmod][M][n] c_k * tau * <A_{m,b}, Q_k P_k(tau)>
+    double* H;               // [nmod][64*64]
+    double* dirpart;         // [ndirs][nmod]
+    double* out;             // [2 + n + K + nmod + M] lnl | pad | grad_t | gc | stg | grad_rate_w
+};
+
+__device__ __forceinline__ size_t mat_off(int m, int b, int n) { return (size_t(m) * n + b) * SP2; }
+__device__ __forceinline__ size_t part_off(int ii, int m, int M, int Pp) { return (size_t(ii) * M + m) * SP * size_t(Pp); }
+__device__ __forceinline__ size_t col_off(int ii, int m, int M, int Pp) { return (size_t(ii) * M + m) * size_t(Pp); }
+
+__device__ __forceinline__ double time_conv(const Model& md, int k) {
+    return md.time_mode == 1 ? 3.0 / fmax(md.mu[k], 1e-12) : 1.0;
+}
+
+}  // namespace h3g

@@ -1,0 +1,620 @@
+// h3g_fp64.cu — FP64 kernels of the likelihood + adjoint-gradient pipeline.
+//
+// Per evaluation (one CUDA stream, level-synchronous over the tree):
+//   k_build_P      P_{m,b} = sum_k c_k clamp(U_k diag(e^{lam_k tau}) V_k), dP = d P / d t
+//                  (rate_matrix.hpp:251-257, likelihood.hpp:1118-1127, busted.hpp:1191-1216)
+//   k_inside       one launch per height level: D_u = prod_c P_c D_c with power-of-two
+//                  rescaling, then the message P_u D_u for the parent (likelihood.hpp:500-597)
+//   k_root         L = pi . D_root, log-sum-exp over rate classes, per-pattern scale
+//                  factors f = w * post / L (likelihood.hpp:599-610, busted.hpp:1346-1375)
+//   k_outside      one launch per depth level: V_c = 2^{e_u} U_u o prod_{s != c} P_s D_s,
+//                  U_c = P_c^T V_c (likelihood.hpp:612-761)
+//   k_accumA       A_{m,b} = sum_p f V D^T  (likelihood.hpp:1435 generalised)
+//   k_frechet      dlnL/dt_b = <A, dP>; spectral Frechet pieces U^T A V^T o E
+//                  (likelihood.hpp:1428-1471)
+//   k_hsum, k_dir, k_small   fixed-order reductions -> lnL, gradients
+// All reductions run in a fixed order, so repeated evaluations are bit-identical.
+#include "h3g_common.cuh"
+#include "h3g_kernels.h"
+
+namespace h3g {
+
+__device__ __forceinline__ int renorm64(double (&v)[SP]) {
+    double mx = 0.0;
+#pragma unroll
+    for (int i = 0; i < SP; ++i) mx = fmax(mx, v[i]);
+    if (mx > 0.0 && mx < 0x1p-256) {
+        const int sh = -ilogb(mx) - 1;    // brings the max into [0.5, 1)
+#pragma unroll
+        for (int i = 0; i < SP; ++i) v[i] = ldexp(v[i], sh);
+        return sh;
+    }
+    return 0;
+}
+
+// v *= P_c * leaf_vector(c, p): a column of P_c, a masked column sum or the row sums.
+__device__ __forceinline__ void mul_leaf_msg(double (&v)[SP], const Topo& t, const Work& w, int m, int c, int p) {
+    const int tx = t.taxon[c];
+    const double* PTc = w.PT + mat_off(m, c, t.n);
+    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
+    if (st >= 0) {
+        const double2* r = reinterpret_cast<const double2*>(PTc + st * SP);
+#pragma unroll
+        for (int i = 0; i < SP / 2; ++i) { double2 x = __ldg(r + i); v[2 * i] *= x.x; v[2 * i + 1] *= x.y; }
+        return;
+    }
+    const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * t.Pp + p];
+    if (mk == 0 || (mk & t.all_mask) == t.all_mask) {
+        const double2* r = reinterpret_cast<const double2*>(w.rs + (size_t(m) * t.n + c) * SP);
+#pragma unroll
+        for (int i = 0; i < SP / 2; ++i) { double2 x = __ldg(r + i); v[2 * i] *= x.x; v[2 * i + 1] *= x.y; }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < SP; ++i) {
+        double s = 0.0;
+        for (uint64_t b = mk; b; b &= b - 1) s += __ldg(PTc + (__ffsll((long long)b) - 1) * SP + i);
+        v[i] *= s;
+    }
+}
+
+// out[i] = sum_j S[j*64 + i] * v[j] for a 64x64 matrix staged in shared memory,
+// written with a stride to global memory (one thread = one pattern).
+__device__ __forceinline__ void smem_matvec_store(const double* __restrict__ sM, const double (&v)[SP], double* dst, size_t stride) {
+    for (int i8 = 0; i8 < SP; i8 += 8) {
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
+#pragma unroll
+        for (int j = 0; j < SP; ++j) {
+            const double2* r = reinterpret_cast<const double2*>(sM + j * SP + i8);
+            const double2 a = r[0], b = r[1], c = r[2], d = r[3];
+            const double x = v[j];
+            s0 = fma(a.x, x, s0); s1 = fma(a.y, x, s1); s2 = fma(b.x, x, s2); s3 = fma(b.y, x, s3);
+            s4 = fma(c.x, x, s4); s5 = fma(c.y, x, s5); s6 = fma(d.x, x, s6); s7 = fma(d.y, x, s7);
+        }
+        dst[(i8 + 0) * stride] = s0; dst[(i8 + 1) * stride] = s1; dst[(i8 + 2) * stride] = s2; dst[(i8 + 3) * stride] = s3;
+        dst[(i8 + 4) * stride] = s4; dst[(i8 + 5) * stride] = s5; dst[(i8 + 6) * stride] = s6; dst[(i8 + 7) * stride] = s7;
+    }
+}
+
+__device__ __forceinline__ void stage_matrix(double* __restrict__ s, const double* __restrict__ g, int tid, int nthr) {
+    const double2* g2 = reinterpret_cast<const double2*>(g);
+    double2* s2 = reinterpret_cast<double2*>(s);
+    for (int k = tid; k < SP2 / 2; k += nthr) s2[k] = __ldg(g2 + k);
+}
+
+// ------------------------------------------------------------------ build P
+// grid (n, M), block 256: each thread owns 16 entries (row r, columns c0..c0+15).
+__global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
+    extern __shared__ double sm[];
+    double* sA = sm;            // U_k, later P_k
+    double* sB = sm + SP2;      // V_k, later Q_k
+    __shared__ double se[SP];
+    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
+    if (b == t.root) return;
+    const int r = tid >> 2, c0 = (tid & 3) * 16;
+    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+    const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
+    double accP[16], accD[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) accP[q] = accD[q] = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        const double cw = test ? md.class_w[k] : 1.0;
+        const double cv = time_conv(md, k);
+        const double rate = md.rates[m];
+        const double tau = rate * w.bl[b] * cv;
+        __syncthreads();
+        stage_matrix(sA, md.U + size_t(k) * SP2, tid, 256);
+        stage_matrix(sB, md.V + size_t(k) * SP2, tid, 256);
+        if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
+        __syncthreads();
+        double pk[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) pk[q] = 0.0;
+        for (int l = 0; l < SP; ++l) {
+            const double u = sA[r * SP + l] * se[l];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) pk[q] = fma(u, sB[l * SP + c0 + q], pk[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) pk[q] = fmax(pk[q], 0.0);
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 16; ++q) sA[r * SP + c0 + q] = pk[q];
+        stage_matrix(sB, md.Q + size_t(k) * SP2, tid, 256);
+        __syncthreads();
+        double qp[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) qp[q] = 0.0;
+        for (int l = 0; l < SP; ++l) {
+            const double qq = sB[r * SP + l];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) qp[q] = fma(qq, sA[l * SP + c0 + q], qp[q]);
+        }
+        const double sc = cw * rate * cv;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) { accP[q] = fma(cw, pk[q], accP[q]); accD[q] = fma(sc, qp[q], accD[q]); }
+    }
+    double* P = w.P + mat_off(m, b, t.n);
+    double* PT = w.PT + mat_off(m, b, t.n);
+    double* dP = w.dP + mat_off(m, b, t.n);
+    double rsum = 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        P[r * SP + c0 + q] = accP[q];
+        PT[(c0 + q) * SP + r] = accP[q];
+        dP[r * SP + c0 + q] = accD[q];
+        rsum += accP[q];
+    }
+    rsum += __shfl_xor_sync(0xffffffffu, rsum, 1);
+    rsum += __shfl_xor_sync(0xffffffffu, rsum, 2);
+    if ((tid & 3) == 0) w.rs[(size_t(m) * t.n + b) * SP + r] = rsum;
+}
+
+// Caller-supplied P (compute_tree_log_likelihood_from_P): derive PT and row sums.
+__global__ void k_prep_given_P(Topo t, Work w) {
+    const int b = blockIdx.x, tid = threadIdx.x;
+    if (b == t.root) return;
+    const double* P = w.P + mat_off(0, b, t.n);
+    double* PT = w.PT + mat_off(0, b, t.n);
+    for (int e = tid; e < SP2; e += blockDim.x) PT[(e % SP) * SP + e / SP] = P[e];
+    if (tid < SP) {
+        double s = 0.0;
+        for (int j = 0; j < SP; ++j) s += P[tid * SP + j];
+        w.rs[size_t(b) * SP + tid] = s;
+    }
+}
+
+// ------------------------------------------------------------------- inside
+// grid (Pp/TP, nodes in level, M), block TP.
+__global__ void __launch_bounds__(TP) k_inside(Topo t, Model md, Work w, const int* __restrict__ nodes) {
+    __shared__ __align__(16) double sP[SP2];
+    const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
+    const int p = blockIdx.x * TP + tid;
+    const int iu = t.iidx[u];
+    const int M = md.M;
+    const size_t Pp = size_t(t.Pp);
+    const bool root = (u == t.root);
+    if (!root) stage_matrix(sP, w.PT + mat_off(m, u, t.n), tid, TP);
+    double acc[SP];
+#pragma unroll
+    for (int i = 0; i < SP; ++i) acc[i] = i < t.S ? 1.0 : 0.0;
+    int ecum = 0, eown = 0;
+    for (int q = t.ch_off[u]; q < t.ch_off[u + 1]; ++q) {
+        const int c = t.ch[q];
+        if (t.leaf[c]) {
+            mul_leaf_msg(acc, t, w, m, c, p);
+        } else {
+            const int ic = t.iidx[c];
+            const double* src = w.Ms + part_off(ic, m, M, t.Pp) + p;
+#pragma unroll
+            for (int i = 0; i < SP; ++i) acc[i] *= src[i * Pp];
+            ecum += w.Ecum[col_off(ic, m, M, t.Pp) + p];
+        }
+        eown += renorm64(acc);
+    }
+    double* dst = w.D + part_off(iu, m, M, t.Pp) + p;
+#pragma unroll
+    for (int i = 0; i < SP; ++i) dst[i * Pp] = acc[i];
+    w.Eown[col_off(iu, m, M, t.Pp) + p] = eown;
+    w.Ecum[col_off(iu, m, M, t.Pp) + p] = ecum + eown;
+    if (root) return;
+    __syncthreads();
+    // message to the parent: (P_u D_u)_i = sum_j PT[j][i] D_j
+    smem_matvec_store(sP, acc, w.Ms + part_off(iu, m, M, t.Pp) + p, Pp);
+}
+
+// --------------------------------------------------------------------- root
+__global__ void k_root(Topo t, Model md, Work w) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= t.Pp) return;
+    const int ir = t.iidx[t.root], M = md.M;
+    const double wt = t.w[p];
+    double L[kMaxRateClasses], ll[kMaxRateClasses];
+    for (int m = 0; m < M; ++m) {
+        const double* D = w.D + part_off(ir, m, M, t.Pp) + p;
+        double s = 0.0;
+        for (int i = 0; i < SP; ++i) s = fma(md.pi[i], D[size_t(i) * t.Pp], s);
+        L[m] = s;
+        ll[m] = s > 0.0 ? log(s) - double(w.Ecum[col_off(ir, m, M, t.Pp) + p]) * 0.69314718055994530942 : -1e20;
+    }
+    double site = -1e20, contrib = 0.0;
+    bool ok = false;
+    if (M == 1) {
+        if (L[0] > 0.0) {
+            ok = true; site = ll[0]; contrib = wt * ll[0];
+            w.f[p] = wt / L[0];
+        } else {
+            w.f[p] = 0.0;
+        }
+        w.rw[p] = 0.0;
+    } else {
+        double mx = -INFINITY;
+        for (int m = 0; m < M; ++m)
+            if (md.rate_w[m] > 1e-12 && L[m] > 0.0) mx = fmax(mx, log(md.rate_w[m]) + ll[m]);
+        double post[kMaxRateClasses], se = 0.0;
+        for (int m = 0; m < M; ++m) {
+            post[m] = 0.0;
+            if (mx > -1e19 && md.rate_w[m] > 1e-12 && L[m] > 0.0) { post[m] = exp(log(md.rate_w[m]) + ll[m] - mx); se += post[m]; }
+        }
+        if (mx > -1e19 && se > 0.0) { ok = true; site = mx + log(se); contrib = wt * site; }
+        for (int m = 0; m < M; ++m) {
+            const double pw = ok ? post[m] / se : 0.0;
+            w.f[size_t(m) * t.Pp + p] = (ok && pw > 1e-12) ? wt * pw / L[m] : 0.0;
+            w.rw[size_t(m) * t.Pp + p] = ok ? wt * pw / md.rate_w[m] : 0.0;
+        }
+    }
+    if (!ok && md.sentinel) contrib = wt * -1e20;
+    w.contrib[p] = contrib;
+    w.site[p] = site;
+}
+
+// ------------------------------------------------------------------ outside
+// grid (Pp/TP, nodes in level, M), block TP, dynamic smem = 2 * 64 * 64 doubles.
+__global__ void __launch_bounds__(TP) k_outside(Topo t, Model md, Work w, const int* __restrict__ nodes, int want_v) {
+    extern __shared__ __align__(16) double sm[];
+    double* sU = sm;          // [64][TP] outside partial of u
+    double* sP = sm + SP2;    // P_c row-major
+    const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
+    const int p = blockIdx.x * TP + tid;
+    const int iu = t.iidx[u], M = md.M;
+    const size_t Pp = size_t(t.Pp);
+    if (u == t.root) {
+        for (int i = 0; i < SP; ++i) sU[i * TP + tid] = md.pi[i];
+    } else {
+        const double* src = w.U + part_off(iu, m, M, t.Pp) + p;
+        for (int i = 0; i < SP; ++i) sU[i * TP + tid] = src[i * Pp];
+    }
+    const int eu = w.Eown[col_off(iu, m, M, t.Pp) + p];
+    const double fp = w.f[size_t(m) * Pp + p];
+    const int q0 = t.ch_off[u], q1 = t.ch_off[u + 1];
+    for (int q = q0; q < q1; ++q) {
+        const int c = t.ch[q];
+        double v[SP];
+#pragma unroll
+        for (int i = 0; i < SP; ++i) v[i] = sU[i * TP + tid];
+        int ev = eu;
+        for (int q2 = q0; q2 < q1; ++q2) {
+            if (q2 == q) continue;
+            const int s = t.ch[q2];
+            if (t.leaf[s]) {
+                mul_leaf_msg(v, t, w, m, s, p);
+            } else {
+                const double* src = w.Ms + part_off(t.iidx[s], m, M, t.Pp) + p;
+#pragma unroll
+                for (int i = 0; i < SP; ++i) v[i] *= src[i * Pp];
+            }
+            ev -= renorm64(v);
+        }
+        if (ev != 0) {
+#pragma unroll
+            for (int i = 0; i < SP; ++i) v[i] = ldexp(v[i], ev);
+        }
+        if (want_v) {
+            double* dst = w.Vf + part_off(c, m, M, t.Pp) + p;
+#pragma unroll
+            for (int i = 0; i < SP; ++i) dst[i * Pp] = fp * v[i];
+        }
+        if (!t.leaf[c]) {
+            __syncthreads();
+            stage_matrix(sP, w.P + mat_off(m, c, t.n), tid, TP);
+            __syncthreads();
+            // U_c = P_c^T V_c : (U_c)_i = sum_j P[j][i] v_j
+            smem_matvec_store(sP, v, w.U + part_off(t.iidx[c], m, M, t.Pp) + p, Pp);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ accum A
+// A_{m,b,chunk} = sum_{p in chunk} Vf_b[:, p] D_b[:, p]^T.  grid (n, M, nchunk), block 256.
+__global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w) {
+    __shared__ __align__(16) double sV[32][SP + 2];
+    __shared__ __align__(16) double sD[32][SP + 2];
+    const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
+    if (b == t.root) return;
+    const int M = md.M;
+    const size_t Pp = size_t(t.Pp);
+    const int ti = tid & 15, tj = tid >> 4;
+    const int p_begin = ck * w.chunk, p_end = min(t.Pp, p_begin + w.chunk);
+    const bool lf = t.leaf[b];
+    const int tx = lf ? t.taxon[b] : -1;
+    const double* Vb = w.Vf + part_off(b, m, M, t.Pp);
+    const double* Db = lf ? nullptr : w.D + part_off(t.iidx[b], m, M, t.Pp);
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+    for (int p0 = p_begin; p0 < p_end; p0 += 32) {
+        for (int e = tid; e < 32 * SP; e += 256) {
+            const int pp = e & 31, i = e >> 5, p = p0 + pp;
+            const bool in = p < p_end;
+            sV[pp][i] = in ? Vb[i * Pp + p] : 0.0;
+            double d = 0.0;
+            if (in) {
+                if (!lf) {
+                    d = Db[i * Pp + p];
+                } else if (i < t.S) {
+                    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
+                    if (st >= 0) d = (st == i) ? 1.0 : 0.0;
+                    else {
+                        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * Pp + p];
+                        d = (mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> i) & 1)) ? 1.0 : 0.0;
+                    }
+                }
+            }
+            sD[pp][i] = d;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int pp = 0; pp < 32; ++pp) {
+            const double2 a01 = *reinterpret_cast<const double2*>(&sV[pp][4 * ti]);
+            const double2 a23 = *reinterpret_cast<const double2*>(&sV[pp][4 * ti + 2]);
+            const double2 b01 = *reinterpret_cast<const double2*>(&sD[pp][4 * tj]);
+            const double2 b23 = *reinterpret_cast<const double2*>(&sD[pp][4 * tj + 2]);
+            const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+        }
+        __syncthreads();
+    }
+    double* dst = w.Apart + ((size_t(b) * M + m) * w.nchunk + ck) * SP2;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dst[(4 * ti + a) * SP + 4 * tj + c] = acc[a][c];
+}
+
+__device__ __forceinline__ double block_sum_256(double x, double* red) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = x;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) for (int i = 0; i < 8; ++i) s += red[i];
+    return s;   // valid on thread 0
+}
+
+// ------------------------------------------------------------------ frechet
+// grid (n, M), block 256, dynamic smem 3 * 64 * 64 doubles.
+__global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int want_global) {
+    extern __shared__ __align__(16) double sm[];
+    double* sA = sm;
+    double* sB = sm + SP2;
+    double* sT = sm + 2 * SP2;
+    __shared__ double red[8];
+    __shared__ double se[SP];
+    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x, n = t.n, M = md.M;
+    if (b == t.root) return;
+    const double* Ap = w.Apart + (size_t(b) * M + m) * w.nchunk * SP2;
+    for (int e = tid; e < SP2; e += 256) {
+        double s = 0.0;
+        for (int ck = 0; ck < w.nchunk; ++ck) s += Ap[size_t(ck) * SP2 + e];
+        sA[e] = s;
+    }
+    __syncthreads();
+    const double* dP = w.dP + mat_off(m, b, n);
+    double g = 0.0;
+    for (int e = tid; e < SP2; e += 256) g = fma(sA[e], dP[e], g);
+    g = block_sum_256(g, red);
+    if (tid == 0) w.gt[size_t(m) * n + b] = g;
+    if (!want_global) return;
+    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+    const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
+    const int r = tid >> 2, c0 = (tid & 3) * 16;
+    for (int k = k0; k < k1; ++k) {
+        const double cw = test ? md.class_w[k] : 1.0;
+        const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
+        __syncthreads();
+        stage_matrix(sB, md.U + size_t(k) * SP2, tid, 256);
+        if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
+        __syncthreads();
+        // T = U^T A
+        double acc[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+        for (int l = 0; l < SP; ++l) {
+            const double u = sB[l * SP + r];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc[q] = fma(u, sA[l * SP + c0 + q], acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) sT[r * SP + c0 + q] = acc[q];
+        __syncthreads();
+        stage_matrix(sB, md.V + size_t(k) * SP2, tid, 256);
+        __syncthreads();
+        // At = T V^T
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+        for (int l = 0; l < SP; ++l) {
+            const double x = sT[r * SP + l];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc[q] = fma(x, sB[(c0 + q) * SP + l], acc[q]);
+        }
+        const double* lam = md.lam + size_t(k) * SP;
+        const double li = lam[r], ei = se[r];
+        double* Hp = w.Hpart + ((size_t(k) * M + m) * n + b) * SP2;
+        double dg = 0.0, dq = 0.0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int j = c0 + q;
+            const double lj = lam[j], ej = se[j], d = li - lj;
+            const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
+            Hp[r * SP + j] = cw * acc[q] * E;
+            if (j == r) { dg = ei * acc[q]; dq = li * ei * acc[q]; }
+        }
+        dg = block_sum_256(dg, red);
+        dq = block_sum_256(dq, red);
+        if (tid == 0) {
+            if (test) w.gc[(size_t(k) * M + m) * n + b] = dg;
+            w.stg[(size_t(k) * M + m) * n + b] = cw * tau * dq;
+        }
+    }
+}
+
+// H_k[e] = sum over (m, b) using model k, fixed order.  grid (nmod, 16), block 256.
+__global__ void k_hsum(Topo t, Model md, Work w) {
+    const int k = blockIdx.x, e = blockIdx.y * 256 + threadIdx.x, n = t.n, M = md.M;
+    double s = 0.0;
+    for (int m = 0; m < M; ++m)
+        for (int b = 0; b < n; ++b) {
+            if (b == t.root) continue;
+            const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+            if ((k < md.K) != test) continue;
+            s += w.Hpart[((size_t(k) * M + m) * n + b) * SP2 + e];
+        }
+    w.H[size_t(k) * SP2 + e] = s;
+}
+
+// per (direction x, model k): sum_ij (V_k dQ U_k)_ij H_k,ij - [normalized] dmu/mu * stg_k
+// grid (ndirs, nmod), block 256, dynamic smem 3 * 64 * 64 doubles.
+__global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
+    extern __shared__ __align__(16) double sm[];
+    double* sX = sm;
+    double* sY = sm + SP2;
+    double* sZ = sm + 2 * SP2;
+    __shared__ double red[8];
+    const int x = blockIdx.x, k = blockIdx.y, tid = threadIdx.x;
+    const double* dQ = md.dQ + (size_t(x) * md.nmod + k) * SP2;
+    stage_matrix(sX, md.V + size_t(k) * SP2, tid, 256);
+    stage_matrix(sY, dQ, tid, 256);
+    __syncthreads();
+    const int r = tid >> 2, c0 = (tid & 3) * 16;
+    double acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int l = 0; l < SP; ++l) {
+        const double a = sX[r * SP + l];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = fma(a, sY[l * SP + c0 + q], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) sZ[r * SP + c0 + q] = acc[q];
+    __syncthreads();
+    stage_matrix(sX, md.U + size_t(k) * SP2, tid, 256);
+    __syncthreads();
+    double g = 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int l = 0; l < SP; ++l) {
+        const double a = sZ[r * SP + l];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[q] = fma(a, sX[l * SP + c0 + q], acc[q]);
+    }
+    const double* H = w.H + size_t(k) * SP2;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) g = fma(acc[q], H[r * SP + c0 + q], g);
+    double dmu = 0.0;
+    if (tid < SP) dmu = -md.pi[tid] * dQ[tid * SP + tid];
+    g = block_sum_256(g, red);
+    dmu = block_sum_256(dmu, red);
+    if (tid == 0) {
+        double v = g;
+        if (md.time_mode == 1) {
+            // stg_k total sits in out[] after k_small: out[2 + n + K + k]
+            v -= dmu / fmax(md.mu[k], 1e-12) * w.out[2 + t.n + md.K + k];
+        }
+        w.dirpart[size_t(x) * md.nmod + k] = v;
+    }
+}
+
+// Fixed-order reductions of the small per-branch / per-pattern partials.
+// One block of 256 threads.
+__global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int grads) {
+    __shared__ double red[8];
+    const int tid = threadIdx.x, n = t.n, M = md.M;
+    // lnL: per-thread Neumaier over a strided slice, then a fixed tree
+    double s = 0.0, c = 0.0;
+    for (int p = tid; p < t.Pp; p += 256) {
+        const double x = w.contrib[p], y = s + x;
+        c += fabs(s) >= fabs(x) ? (s - y) + x : (x - y) + s;
+        s = y;
+    }
+    double tot = block_sum_256(s + c, red);
+    if (tid == 0) { w.out[0] = tot; w.out[1] = 0.0; }
+    if (!grads) return;
+    for (int b = tid; b < n; b += 256) {
+        double g = 0.0;
+        if (b != t.root) for (int m = 0; m < M; ++m) g += w.gt[size_t(m) * n + b];
+        w.out[2 + b] = g;
+    }
+    for (int k = 0; k < md.nmod; ++k) {
+        double a = 0.0, z = 0.0;
+        for (int idx = tid; idx < M * n; idx += 256) {
+            const int b = idx % n;
+            if (b == t.root) continue;
+            const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+            if ((k < md.K) != test) continue;
+            if (k < md.K) a += w.gc[size_t(k) * M * n + idx];
+            z += w.stg[size_t(k) * M * n + idx];
+        }
+        a = block_sum_256(a, red);
+        z = block_sum_256(z, red);
+        if (tid == 0) {
+            if (k < md.K) w.out[2 + n + k] = a;
+            w.out[2 + n + md.K + k] = z;
+        }
+    }
+    for (int m = 0; m < M; ++m) {
+        double a = 0.0;
+        for (int p = tid; p < t.Pp; p += 256) a += w.rw[size_t(m) * t.Pp + p];
+        a = block_sum_256(a, red);
+        if (tid == 0) w.out[2 + n + md.K + md.nmod + m] = a;
+    }
+}
+
+// ------------------------------------------------------------------ launch
+static size_t smem_bytes(int mats) { return size_t(mats) * SP2 * sizeof(double); }
+
+void fp64_configure() {
+    cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(2)));
+    cudaFuncSetAttribute(k_outside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(2)));
+    cudaFuncSetAttribute(k_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(3)));
+    cudaFuncSetAttribute(k_dir, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(3)));
+}
+
+int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
+    k_build_P<<<dim3(t.n, md.M), 256, smem_bytes(2), s>>>(t, md, w);
+    return 1;
+}
+int launch_prep_given_P(const Topo& t, const Work& w, cudaStream_t s) {
+    k_prep_given_P<<<t.n, 256, 0, s>>>(t, w);
+    return 1;
+}
+int launch_inside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, cudaStream_t s) {
+    k_inside<<<dim3(t.Pp / TP, count, md.M), TP, 0, s>>>(t, md, w, d_nodes);
+    return 1;
+}
+int launch_root(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
+    k_root<<<(t.Pp + 127) / 128, 128, 0, s>>>(t, md, w);
+    return 1;
+}
+int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, int want_v, cudaStream_t s) {
+    k_outside<<<dim3(t.Pp / TP, count, md.M), TP, smem_bytes(2), s>>>(t, md, w, d_nodes, want_v);
+    return 1;
+}
+int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
+    k_accumA<<<dim3(t.n, md.M, w.nchunk), 256, 0, s>>>(t, md, w);
+    return 1;
+}
+int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {
+    k_frechet<<<dim3(t.n, md.M), 256, smem_bytes(3), s>>>(t, md, w, want_global);
+    return 1;
+}
+int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
+    k_hsum<<<dim3(md.nmod, SP2 / 256), 256, 0, s>>>(t, md, w);
+    return 1;
+}
+int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
+    if (md.ndirs <= 0) return 0;
+    k_dir<<<dim3(md.ndirs, md.nmod), 256, smem_bytes(3), s>>>(t, md, w);
+    return 1;
+}
+int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s) {
+    k_small<<<1, 256, 0, s>>>(t, md, w, grads);
+    return 1;
+}
+
+}  // namespace h3g

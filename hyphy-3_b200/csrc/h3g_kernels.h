@@ -1,0 +1,20 @@
+// h3g_kernels.h — host-callable launchers of the device pipeline (one per stage).
+// Each returns the number of kernels it enqueued on the stream.
+#pragma once
+#include "h3g_common.cuh"
+
+namespace h3g {
+
+void fp64_configure();
+int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
+int launch_prep_given_P(const Topo& t, const Work& w, cudaStream_t s);
+int launch_inside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, cudaStream_t s);
+int launch_root(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
+int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, int want_v, cudaStream_t s);
+int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
+int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s);
+int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
+int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
+int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s);
+
+}  // namespace h3g

@@ -1,0 +1,229 @@
+// _hyphy3 — Python module with the reference binding's names for the likelihood
+// core (src/python/bindings.cpp:50-119 core types, :725-732 the gradient call),
+// backed by the B200 LikelihoodEngine (include/hyphy/core/likelihood_gpu.hpp).
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include "hyphy/core/likelihood_gpu.hpp"
+
+namespace py = pybind11;
+using namespace hyphy::core;
+using namespace pybind11::literals;
+
+static py::dict mixture_dict(const MixtureGradients& g) {
+    py::dict d;
+    d["log_likelihood"] = g.log_likelihood;
+    d["grad_branches"] = g.grad_branches;
+    d["grad_omegas"] = g.grad_omegas;
+    d["grad_omega_bg"] = g.grad_omega_bg;
+    d["grad_weights"] = g.grad_weights;
+    d["grad_theta"] = std::vector<double>(g.grad_theta, g.grad_theta + 5);
+    d["grad_syn_weights"] = g.grad_syn_weights;
+    d["site_log_likelihoods"] = g.site_log_likelihoods;
+    return d;
+}
+
+static const std::vector<bool>* opt_mask(const py::object& o, std::vector<bool>& store) {
+    if (o.is_none()) return nullptr;
+    store = o.cast<std::vector<bool>>();
+    return &store;
+}
+
+PYBIND11_MODULE(_hyphy3, m) {
+    m.doc() = "HyPhy 3 likelihood core on NVIDIA B200 (libh3g)";
+
+    py::class_<GeneticCode, std::shared_ptr<GeneticCode>>(m, "GeneticCode")
+        .def_static("universal", []() { return std::const_pointer_cast<GeneticCode>(GeneticCode::universal()); })
+        .def_static("from_name", [](const std::string& nm) { return std::const_pointer_cast<GeneticCode>(GeneticCode::from_name(nm)); })
+        .def_readonly("name", &GeneticCode::name)
+        .def_readonly("num_sense_codons", &GeneticCode::num_sense_codons)
+        .def_readonly("sense_codons", &GeneticCode::sense_codons);
+
+    py::class_<TreeNode>(m, "TreeNode")
+        .def_readonly("id", &TreeNode::id)
+        .def_readonly("name", &TreeNode::name)
+        .def_readonly("parent_id", &TreeNode::parent_id)
+        .def_readonly("children", &TreeNode::children)
+        .def_readwrite("branch_length", &TreeNode::branch_length)
+        .def_readonly("is_leaf", &TreeNode::is_leaf);
+
+    py::class_<Tree>(m, "Tree")
+        .def(py::init<>())
+        .def_static("from_newick", [](const std::string& s, bool keep_rooted) { return Tree::from_newick(s, keep_rooted); },
+                    "newick"_a, "keep_rooted"_a = true)
+        .def_static("from_newick_file", &Tree::from_newick_file, "filepath"_a, "keep_rooted"_a = true)
+        .def("num_nodes", &Tree::num_nodes)
+        .def("num_leaves", &Tree::num_leaves)
+        .def_readonly("root_id", &Tree::root_id)
+        .def_readonly("post_order", &Tree::post_order)
+        .def_readonly("nodes", &Tree::nodes)
+        .def_readonly("leaf_name_to_id", &Tree::leaf_name_to_id)
+        .def("get_branch_lengths", [](const Tree& t) {
+            std::vector<Scalar> bl(t.num_nodes(), 0.0);
+            for (size_t i = 0; i < t.nodes.size(); ++i) bl[i] = t.nodes[i].branch_length;
+            return bl;
+        })
+        .def("set_branch_lengths", [](Tree& t, const std::vector<Scalar>& bl) {
+            for (size_t i = 0; i < t.nodes.size() && i < bl.size(); ++i) t.nodes[i].branch_length = bl[i];
+        })
+        .def("get_branch_length", [](const Tree& t, int32_t id) { return t.nodes.at(size_t(id)).branch_length; }, "id"_a)
+        .def("set_branch_length", [](Tree& t, int32_t id, Scalar v) { t.nodes.at(size_t(id)).branch_length = v; }, "id"_a, "length"_a)
+        .def_property_readonly("parents", [](const Tree& t) {
+            std::vector<int32_t> p(t.num_nodes());
+            for (auto& nd : t.nodes) p[size_t(nd.id)] = nd.parent_id;
+            return p;
+        });
+
+    py::class_<Alignment>(m, "Alignment")
+        .def(py::init<>())
+        .def_static("load", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
+        .def_static("from_fasta", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
+        .def_static("from_nexus", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
+        .def_static("from_text", [](const std::string& s) { return Alignment::from_text(s); }, "text"_a)
+        .def_static("from_sequences", [](const std::vector<std::string>& names, const std::vector<std::string>& seqs, const std::string& code) {
+            if (names.size() != seqs.size()) throw std::runtime_error("names and seqs differ in length");
+            Alignment a;
+            for (size_t i = 0; i < names.size(); ++i) a.add_sequence(names[i], seqs[i]);
+            a.finalize(GeneticCode::from_name(code));
+            return a;
+        }, "names"_a, "seqs"_a, "code"_a = "Universal")
+        .def_readonly("num_taxa", &Alignment::num_taxa)
+        .def_property_readonly("num_sequences", [](const Alignment& a) { return a.num_taxa; })
+        .def_readonly("num_codons", &Alignment::num_codons)
+        .def_readonly("num_nucleotides", &Alignment::num_nucleotides)
+        .def_property_readonly("num_sites", [](const Alignment& a) { return a.num_codons; })
+        .def_property_readonly("num_patterns", [](const Alignment& a) { return a.patterns.size(); })
+        .def_readonly("embedded_tree_newick", &Alignment::embedded_tree_newick)
+        .def_readonly("taxon_names", &Alignment::taxon_names)
+        .def_readonly("codon_frequencies", &Alignment::codon_frequencies_f3x4)
+        .def_property_readonly("nuc_frequencies", [](const Alignment& a) { return std::vector<double>(a.nuc_frequencies, a.nuc_frequencies + 4); })
+        .def_property_readonly("pos_nuc_frequencies", [](const Alignment& a) {
+            py::array_t<double> r({3, 4});
+            std::copy(&a.pos_nuc_frequencies[0][0], &a.pos_nuc_frequencies[0][0] + 12, r.mutable_data());
+            return r;
+        })
+        .def("pattern_arrays", [](const Alignment& a) {
+            const size_t P = a.patterns.size(), T = a.num_taxa;
+            py::array_t<int8_t> st({P, T});
+            py::array_t<uint64_t> mk({P, T});
+            py::array_t<double> w(P);
+            for (size_t p = 0; p < P; ++p) {
+                w.mutable_data()[p] = double(a.patterns[p].weight);
+                for (size_t t = 0; t < T; ++t) {
+                    st.mutable_data()[p * T + t] = a.patterns[p].states[t];
+                    mk.mutable_data()[p * T + t] = a.patterns[p].ambiguous_masks[t];
+                }
+            }
+            return py::make_tuple(st, mk, w);
+        }, "(states[P,T] int8, masks[P,T] uint64, weights[P]) of the compressed patterns");
+
+    py::class_<MG94Parameters>(m, "MG94Parameters")
+        .def(py::init<>())
+        .def_readwrite("alpha", &MG94Parameters::alpha)
+        .def_readwrite("beta", &MG94Parameters::beta)
+        .def_readwrite("theta_AC", &MG94Parameters::theta_AC)
+        .def_readwrite("theta_AT", &MG94Parameters::theta_AT)
+        .def_readwrite("theta_CG", &MG94Parameters::theta_CG)
+        .def_readwrite("theta_CT", &MG94Parameters::theta_CT)
+        .def_readwrite("theta_GT", &MG94Parameters::theta_GT)
+        .def_readwrite("delta", &MG94Parameters::delta)
+        .def_readwrite("psi", &MG94Parameters::psi);
+
+    m.def("mg94_eigensystem", [](const Alignment& a, const MG94Parameters& p) {
+        MG94Matrix mm;
+        mm.update(p, a.pos_nuc_frequencies, a.codon_frequencies_f3x4, a.code ? *a.code : *GeneticCode::universal());
+        auto arr = [&](const Matrix& x) {
+            py::array_t<double> r({x.rows(), x.cols()});
+            std::copy(x.v.begin(), x.v.end(), r.mutable_data());
+            return r;
+        };
+        py::dict d;
+        d["Q"] = arr(mm.Q); d["U"] = arr(mm.U_pi); d["V"] = arr(mm.V_pi);
+        d["lam"] = mm.eigenvalues; d["mu"] = mm.scale_factor; d["pi"] = mm.pi;
+        return d;
+    }, "aln"_a, "params"_a);
+
+    m.def("compute_branch_length_gradients", [](const Tree& t, const Alignment& a, const MG94Parameters& p, const std::vector<Scalar>& bl) {
+        py::gil_scoped_release rel;
+        return LikelihoodEngine::compute_branch_length_gradients(t, a, p, bl);
+    }, "tree"_a, "aln"_a, "params"_a, "branch_lengths"_a = std::vector<Scalar>{},
+       "Compute log-likelihood and exact analytical branch gradients d ln L / d t_b via Inside-Outside");
+
+    m.def("compute_joint_frechet_gradients", [](const Tree& t, const Alignment& a, const MG94Parameters& p, const std::vector<Scalar>& bl,
+                                                py::object is_test, Scalar omega_bg) {
+        std::vector<bool> store;
+        const std::vector<bool>* mask = opt_mask(is_test, store);
+        JointMG94Gradients g;
+        {
+            py::gil_scoped_release rel;
+            g = LikelihoodEngine::compute_joint_frechet_gradients(t, a, p, bl, nullptr, mask, omega_bg);
+        }
+        py::dict d;
+        d["log_likelihood"] = g.log_likelihood;
+        d["grad_branches"] = g.grad_branches;
+        d["grad_omega"] = g.grad_omega;
+        d["grad_omega_bg"] = g.grad_omega_bg;
+        d["grad_theta"] = std::vector<double>{g.grad_theta_AC, g.grad_theta_AT, g.grad_theta_CG, g.grad_theta_CT, g.grad_theta_GT};
+        return d;
+    }, "tree"_a, "aln"_a, "params"_a, "branch_lengths"_a = std::vector<Scalar>{}, "is_test_branch"_a = py::none(), "omega_bg"_a = -1.0);
+
+    m.def("compute_mixture_gradients", [](const Tree& t, const Alignment& a, const MG94Parameters& base, const std::vector<Scalar>& bl,
+                                          const std::vector<Scalar>& omegas, const std::vector<Scalar>& weights,
+                                          const std::vector<Scalar>& syn_rates, const std::vector<Scalar>& syn_weights,
+                                          py::object is_test, Scalar omega_bg, bool want_gradients, bool sentinel) {
+        std::vector<bool> store;
+        const std::vector<bool>* mask = opt_mask(is_test, store);
+        MixtureGradients g;
+        {
+            py::gil_scoped_release rel;
+            g = LikelihoodEngine::compute_mixture_gradients(t, a, base, bl, omegas, weights, syn_rates, syn_weights, mask, omega_bg,
+                                                            want_gradients, sentinel);
+        }
+        return mixture_dict(g);
+    }, "tree"_a, "aln"_a, "base_params"_a, "branch_lengths"_a, "omegas"_a, "weights"_a,
+       "syn_rates"_a = std::vector<Scalar>{1.0}, "syn_weights"_a = std::vector<Scalar>{1.0}, "is_test_branch"_a = py::none(),
+       "omega_bg"_a = -1.0, "want_gradients"_a = true, "zero_likelihood_sentinel"_a = false);
+
+    m.def("compute_tree_log_likelihood_from_P", [](const Tree& t, const Alignment& a,
+                                                   const std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>>& Ps,
+                                                   const std::vector<double>& pi) {
+        const int S = int(pi.size());
+        std::vector<Matrix> Pb;
+        for (auto& x : Ps) {
+            if (x.ndim() != 2 || x.shape(0) != S || x.shape(1) != S) throw std::runtime_error("each P must be S x S");
+            Matrix mm(S, S);
+            std::copy(x.data(), x.data() + size_t(S) * S, mm.v.begin());
+            Pb.push_back(std::move(mm));
+        }
+        std::vector<Scalar> site;
+        Scalar l;
+        {
+            py::gil_scoped_release rel;
+            l = LikelihoodEngine::compute_tree_log_likelihood_from_P(t, a, Pb, pi, S, nullptr, &site);
+        }
+        return py::make_tuple(l, site);
+    }, "tree"_a, "aln"_a, "P_branches"_a, "pi"_a);
+
+    m.def("compute_mg94_log_likelihood", [](const Tree& t, const Alignment& a, const MG94Parameters& p, Scalar branch_scale) {
+        MG94Matrix mm;
+        mm.update(p, a.pos_nuc_frequencies, a.codon_frequencies_f3x4, a.code ? *a.code : *GeneticCode::universal());
+        py::gil_scoped_release rel;
+        return LikelihoodEngine::compute_mg94_log_likelihood(t, a, mm, nullptr, branch_scale);
+    }, "tree"_a, "aln"_a, "params"_a, "branch_scale"_a = 1.0);
+
+    m.def("build_leaf_to_taxon_map", [](const Tree& t, const Alignment& a) {
+        auto v = LikelihoodEngine::build_leaf_to_taxon_map(t, a);
+        std::vector<long long> out(v.size());
+        for (size_t i = 0; i < v.size(); ++i) out[i] = v[i] == size_t(-1) ? -1 : (long long)v[i];
+        return out;
+    });
+
+    m.def("set_precision", [](const std::string& p) {
+        if (p == "fp64") LikelihoodEngine::set_precision(H3G_PREC_FP64);
+        else if (p == "mixed") LikelihoodEngine::set_precision(H3G_PREC_MIXED);
+        else throw std::runtime_error("precision must be 'fp64' or 'mixed'");
+    }, "precision"_a);
+    m.def("get_precision", []() { return LikelihoodEngine::get_precision() == H3G_PREC_MIXED ? "mixed" : "fp64"; });
+    m.def("library_version", []() { return std::string(h3g_version()); });
+}

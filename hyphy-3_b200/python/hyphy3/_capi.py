@@ -1,0 +1,199 @@
+"""ctypes binding of the C ABI in include/h3g.h (libh3g.so).
+
+This is the thin layer a Python caller (or a test) uses to reach the device
+library without the pybind11 module: plain pointers, sizes and status codes.
+Loading fails loudly when the shared library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+_PKG = pathlib.Path(__file__).resolve().parent.parent.parent  # hyphy-3_b200/
+LIB_PATH = pathlib.Path(os.environ.get("H3G_LIBRARY", _PKG / "lib" / "libh3g.so"))
+
+H3G_OK, H3G_ERR_ARG, H3G_ERR_OOM, H3G_ERR_CUDA, H3G_ERR_NUMERIC, H3G_ERR_TIMEOUT, H3G_ERR_STATE = range(7)
+PREC_FP64, PREC_MIXED = 0, 1
+TIME_RAW, TIME_NORMALIZED = 0, 1
+WANT_LNL, WANT_SITE_LNL, WANT_GRAD_T, WANT_GRAD_GLOBAL = 1, 2, 4, 8
+
+EXPORTED = [
+    "h3g_ctx_create", "h3g_ctx_destroy", "h3g_last_error", "h3g_version", "h3g_problem_create",
+    "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
+    "h3g_last_eval_stats",
+]
+
+_dp = C.POINTER(C.c_double)
+
+
+class ModelDesc(C.Structure):
+    _fields_ = [
+        ("S", C.c_int), ("pi", _dp), ("n_models", C.c_int), ("Q", _dp), ("lam", _dp), ("U", _dp), ("V", _dp),
+        ("mu", _dp), ("K", C.c_int), ("class_w", _dp), ("has_bg", C.c_int), ("is_test", C.POINTER(C.c_uint8)),
+        ("M", C.c_int), ("rates", _dp), ("rate_w", _dp), ("time_mode", C.c_int), ("n_dirs", C.c_int),
+        ("dQ", _dp), ("precision", C.c_int), ("zero_l_sentinel", C.c_int),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [("lnl", C.c_double), ("site_lnl", _dp), ("grad_t", _dp), ("grad_dir", _dp),
+                ("grad_class_w", _dp), ("grad_rate_w", _dp)]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libh3g.so once; raises if it is missing (there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"libh3g.so not built at {LIB_PATH}; run __graft_entry__.build()")
+        lib = C.CDLL(str(LIB_PATH))
+        vp = C.c_void_p
+        lib.h3g_version.restype = C.c_char_p
+        lib.h3g_last_error.restype = C.c_char_p
+        lib.h3g_last_error.argtypes = [vp]
+        lib.h3g_ctx_create.argtypes = [C.c_int, vp, C.POINTER(vp)]
+        lib.h3g_ctx_destroy.argtypes = [vp]
+        lib.h3g_problem_create.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_int32),
+                                           C.c_int, C.c_int, C.POINTER(C.c_int8), C.POINTER(C.c_uint64), _dp, C.POINTER(vp)]
+        lib.h3g_problem_destroy.argtypes = [vp]
+        lib.h3g_model_set.argtypes = [vp, C.POINTER(ModelDesc)]
+        lib.h3g_eval.argtypes = [vp, _dp, C.c_uint, C.POINTER(Result)]
+        lib.h3g_eval_from_P.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp]
+        lib.h3g_branch_length_gradients.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp]
+        lib.h3g_last_eval_stats.argtypes = [vp, _dp, C.POINTER(C.c_int)]
+        for name in EXPORTED:
+            getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
+        lib.h3g_version.restype = C.c_char_p
+        lib.h3g_last_error.restype = C.c_char_p
+        _lib = lib
+    return _lib
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a: np.ndarray | None, ct=C.c_double):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ct))
+
+
+class H3GError(RuntimeError):
+    pass
+
+
+class Context:
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.lib = load()
+        self.h = C.c_void_p()
+        st = self.lib.h3g_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(self.h))
+        if st != H3G_OK:
+            raise H3GError(f"h3g_ctx_create failed with status {st}")
+
+    def check(self, st: int) -> None:
+        if st != H3G_OK:
+            raise H3GError(f"status {st}: {self.lib.h3g_last_error(self.h).decode()}")
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.h3g_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Problem:
+    """One tree + compressed alignment resident on the device."""
+
+    def __init__(self, ctx: Context, parent, is_leaf, leaf_taxon, states, masks, weights):
+        self.ctx = ctx
+        self.parent = np.ascontiguousarray(parent, dtype=np.int32)
+        self.is_leaf = np.ascontiguousarray(is_leaf, dtype=np.uint8)
+        self.leaf_taxon = np.ascontiguousarray(leaf_taxon, dtype=np.int32)
+        self.states = np.ascontiguousarray(states, dtype=np.int8)
+        self.masks = np.ascontiguousarray(masks, dtype=np.uint64)
+        self.weights = _f64(weights)
+        self.n = int(self.parent.size)
+        self.P, self.T = (int(self.states.shape[0]), int(self.states.shape[1])) if self.states.ndim == 2 else (0, 0)
+        self.root = int(np.flatnonzero(self.parent < 0)[0])
+        self.h = C.c_void_p()
+        ctx.check(ctx.lib.h3g_problem_create(
+            ctx.h, self.n, _ptr(self.parent, C.c_int32), _ptr(self.is_leaf, C.c_uint8), _ptr(self.leaf_taxon, C.c_int32),
+            self.T, self.P, _ptr(self.states, C.c_int8), _ptr(self.masks, C.c_uint64), _ptr(self.weights), C.byref(self.h)))
+        self._keep = []
+        self.K = self.M = self.ndirs = 0
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.h3g_problem_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_model(self, *, pi, Q, lam, U, V, mu=None, class_w=(1.0,), has_bg=False, is_test=None, rates=(1.0,),
+                  rate_w=(1.0,), time_mode=TIME_RAW, dQ=None, precision=PREC_FP64, zero_l_sentinel=False) -> None:
+        """Q, U, V: [n_models, S, S]; lam: [n_models, S]; dQ: [n_dirs, n_models, S, S]."""
+        Q = _f64(Q); U = _f64(U); V = _f64(V); lam = _f64(lam)
+        if Q.ndim == 2:
+            Q, U, V, lam = Q[None], U[None], V[None], lam[None]
+        nm, S = Q.shape[0], Q.shape[1]
+        pi = _f64(pi)
+        mu_a = _f64(mu if mu is not None else np.ones(nm))
+        cw = _f64(class_w); rt = _f64(rates); rw = _f64(rate_w)
+        it = None if is_test is None else np.ascontiguousarray(is_test, dtype=np.uint8)
+        dq = None if dQ is None else _f64(dQ)
+        nd = 0 if dq is None else int(dq.shape[0])
+        d = ModelDesc(S=S, pi=_ptr(pi), n_models=nm, Q=_ptr(Q), lam=_ptr(lam), U=_ptr(U), V=_ptr(V), mu=_ptr(mu_a),
+                      K=len(cw), class_w=_ptr(cw), has_bg=int(bool(has_bg)), is_test=_ptr(it, C.c_uint8), M=len(rt),
+                      rates=_ptr(rt), rate_w=_ptr(rw), time_mode=time_mode, n_dirs=nd, dQ=_ptr(dq),
+                      precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)))
+        self.ctx.check(self.ctx.lib.h3g_model_set(self.h, C.byref(d)))
+        self.K, self.M, self.ndirs, self.nmod = len(cw), len(rt), nd, nm
+
+    def eval(self, bl, want=WANT_LNL | WANT_GRAD_T, out=None) -> dict:
+        bl = _f64(bl)
+        if bl.size != self.n:
+            raise ValueError("branch lengths must have one entry per node")
+        if out is None:
+            out = {"site_lnl": np.zeros(self.P), "grad_t": np.zeros(self.n), "grad_dir": np.zeros(max(self.ndirs, 1)),
+                   "grad_class_w": np.zeros(self.K), "grad_rate_w": np.zeros(self.M)}
+        r = Result(site_lnl=_ptr(out["site_lnl"]), grad_t=_ptr(out["grad_t"]), grad_dir=_ptr(out["grad_dir"]),
+                   grad_class_w=_ptr(out["grad_class_w"]), grad_rate_w=_ptr(out["grad_rate_w"]))
+        self.ctx.check(self.ctx.lib.h3g_eval(self.h, _ptr(bl), want, C.byref(r)))
+        out["lnl"] = r.lnl
+        return out
+
+    def eval_from_P(self, P, pi) -> tuple[float, np.ndarray]:
+        P = _f64(P); pi = _f64(pi)
+        S = int(pi.size)
+        lnl = C.c_double()
+        site = np.zeros(self.P)
+        self.ctx.check(self.ctx.lib.h3g_eval_from_P(self.h, S, _ptr(P), _ptr(pi), C.byref(lnl), _ptr(site)))
+        return lnl.value, site
+
+    def branch_length_gradients(self, *, pi, Q, lam, U, V, bl, precision=PREC_FP64) -> tuple[float, np.ndarray]:
+        pi, Q, lam, U, V, bl = (_f64(x) for x in (pi, Q, lam, U, V, bl))
+        lnl = C.c_double()
+        g = np.zeros(self.n)
+        self.ctx.check(self.ctx.lib.h3g_branch_length_gradients(
+            self.h, int(pi.size), _ptr(pi), _ptr(Q), _ptr(lam), _ptr(U), _ptr(V), _ptr(bl), precision, C.byref(lnl), _ptr(g)))
+        return lnl.value, g
+
+    def last_stats(self) -> tuple[float, int]:
+        ms = C.c_double()
+        nl = C.c_int()
+        self.ctx.check(self.ctx.lib.h3g_last_eval_stats(self.h, C.byref(ms), C.byref(nl)))
+        return ms.value, nl.value

@@ -1,0 +1,151 @@
+/* h3g.h — C ABI of the B200 codon-likelihood core (libh3g.so).
+ *
+ * The reference (veg/hyphy-3) exposes its likelihood core only as header-only
+ * C++ static functions of hyphy::core::LikelihoodEngine plus a nanobind module;
+ * it has no C ABI.  These entry points are what those call sites bind to:
+ *
+ *   h3g_branch_length_gradients   <- LikelihoodEngine::compute_branch_length_gradients
+ *                                    (include/hyphy/core/likelihood.hpp:1102-1211) and
+ *                                    _hyphy3.compute_branch_length_gradients
+ *                                    (src/python/bindings.cpp:725-732)
+ *   h3g_eval                      <- the general engine behind
+ *                                    LikelihoodEngine::compute_joint_frechet_gradients
+ *                                    (likelihood.hpp:1228-1594) and BUSTED's
+ *                                    compute_busted_branch_gradients / evaluate_log_l
+ *                                    (include/hyphy/analyses/busted.hpp:509-660, :1138-1429)
+ *   h3g_eval_from_P               <- LikelihoodEngine::compute_tree_log_likelihood_from_P
+ *                                    (likelihood.hpp:766-806)
+ *
+ * Conventions.  Plain pointers and sizes; every host array is read or written
+ * during the call only.  Matrices are row-major doubles.  Node ids are the
+ * reference's Newick creation order (tree.hpp:273-585); per-node vectors have
+ * n_nodes entries and the root entry of a gradient is 0.  Every function
+ * returns an h3g_status; h3g_last_error() describes the last failure on a
+ * context.  No C++ exception crosses this boundary.  A context is bound to one
+ * device and one CUDA stream and is not thread-safe: use one per thread.
+ */
+#ifndef H3G_H
+#define H3G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    H3G_OK = 0,
+    H3G_ERR_ARG = 1,      /* invalid argument (sizes, topology, missing arrays) */
+    H3G_ERR_OOM = 2,      /* device allocation failed */
+    H3G_ERR_CUDA = 3,     /* CUDA runtime error or no usable device / kernel image */
+    H3G_ERR_NUMERIC = 4,  /* non-finite input parameters or results */
+    H3G_ERR_TIMEOUT = 5,  /* a bounded device wait expired */
+    H3G_ERR_STATE = 6     /* call order violated (e.g. eval before model_set) */
+} h3g_status;
+
+typedef enum {
+    H3G_PREC_FP64 = 0,    /* every contraction in FP64 (parity path, 1e-10 of the CPU engine) */
+    H3G_PREC_MIXED = 1    /* split-precision tensor-core contractions, FP32 partials, FP64 model/root */
+} h3g_precision;
+
+typedef enum {
+    H3G_TIME_RAW = 0,        /* P = exp(Q * r_m * t)             (likelihood.hpp:1118-1127) */
+    H3G_TIME_NORMALIZED = 1  /* P = exp(Q * r_m * t * 3 / mu)    (likelihood.hpp:1246-1271) */
+} h3g_time_mode;
+
+/* what h3g_eval computes */
+enum {
+    H3G_WANT_LNL = 1u,        /* total log-likelihood (always computed) */
+    H3G_WANT_SITE_LNL = 2u,   /* per-pattern log-likelihood */
+    H3G_WANT_GRAD_T = 4u,     /* d lnL / d t for every branch */
+    H3G_WANT_GRAD_GLOBAL = 8u /* directional, mixture-weight and rate-weight gradients */
+};
+
+typedef struct h3g_ctx h3g_ctx;
+typedef struct h3g_problem h3g_problem;
+
+/* Reversible substitution models as eigensystems, P(tau) = U diag(exp(lam*tau)) V,
+ * clamped at 0 (rate_matrix.hpp:251-257).  Models [0, K) are mixed at the P
+ * level with weights class_w on test branches; when has_bg != 0 model K is
+ * used alone on branches whose is_test entry is 0. */
+typedef struct {
+    int S;                    /* states (<= 64; 61 for the universal code) */
+    const double* pi;         /* S equilibrium frequencies (root prior) */
+    int n_models;             /* K + (has_bg ? 1 : 0) */
+    const double* Q;          /* n_models * S * S generators */
+    const double* lam;        /* n_models * S eigenvalues (clamped <= 0) */
+    const double* U;          /* n_models * S * S, U_pi */
+    const double* V;          /* n_models * S * S, V_pi = U_pi^-1 */
+    const double* mu;         /* n_models mean rates (used by H3G_TIME_NORMALIZED) */
+    int K;                    /* test-branch classes */
+    const double* class_w;    /* K mixing weights */
+    int has_bg;
+    const uint8_t* is_test;   /* n_nodes flags, NULL = every branch is a test branch */
+    int M;                    /* synonymous-rate classes (separate pruning passes) */
+    const double* rates;      /* M rate multipliers r_m */
+    const double* rate_w;     /* M class weights rho_m */
+    int time_mode;            /* h3g_time_mode */
+    int n_dirs;               /* global gradient directions x */
+    const double* dQ;         /* n_dirs * n_models * S * S : dQ_model / dx */
+    int precision;            /* h3g_precision */
+    int zero_l_sentinel;      /* 1: a pattern with L <= 0 adds weight * -1e20 to lnL (evaluate_log_l);
+                                 0: it adds 0 (the gradient entry points) */
+} h3g_model_desc;
+
+typedef struct {
+    double lnl;
+    double* site_lnl;         /* n_patterns, or NULL */
+    double* grad_t;           /* n_nodes, or NULL */
+    double* grad_dir;         /* n_dirs, or NULL */
+    double* grad_class_w;     /* K partials d lnL / d class_w[k], or NULL */
+    double* grad_rate_w;      /* M partials d lnL / d rate_w[m], or NULL */
+} h3g_result;
+
+/* Context: one device, one stream (NULL = a private non-blocking stream). */
+h3g_status h3g_ctx_create(int device, void* cuda_stream, h3g_ctx** out);
+h3g_status h3g_ctx_destroy(h3g_ctx* ctx);
+const char* h3g_last_error(const h3g_ctx* ctx);
+const char* h3g_version(void);
+
+/* Upload one tree and its compressed site patterns.
+ *   parent[n_nodes]       parent id, -1 for the root (exactly one)
+ *   leaf_taxon[n_nodes]   alignment row of each leaf, -1 for a leaf without a
+ *                         sequence (all-ones partial); ignored for internal nodes
+ *   is_leaf[n_nodes]      1 for leaves
+ *   states[P * T]         sense index per (pattern, taxon), -1 if unresolved
+ *   masks[P * T]          compatible-state bitmask per (pattern, taxon)
+ *   weights[P]            pattern multiplicities
+ * Children are visited in increasing node id, the reference's child order. */
+h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_t* parent, const uint8_t* is_leaf,
+                              const int32_t* leaf_taxon, int n_taxa, int n_patterns, const int8_t* states,
+                              const uint64_t* masks, const double* weights, h3g_problem** out);
+h3g_status h3g_problem_destroy(h3g_problem* prob);
+
+/* Install a model (copies all arrays; allocates the device workspace). */
+h3g_status h3g_model_set(h3g_problem* prob, const h3g_model_desc* desc);
+
+/* One likelihood (+ gradient) evaluation at branch lengths bl[n_nodes]
+ * (root entry ignored).  Blocks until results are on the host. */
+h3g_status h3g_eval(h3g_problem* prob, const double* bl, unsigned want, h3g_result* out);
+
+/* Log-likelihood from caller-supplied transition matrices P[n_nodes * S * S]
+ * (root entry ignored) and root frequencies pi[S]; zero-likelihood patterns
+ * contribute weight * -1e20.  site_lnl may be NULL. */
+h3g_status h3g_eval_from_P(h3g_problem* prob, int S, const double* P, const double* pi, double* lnl, double* site_lnl);
+
+/* compute_branch_length_gradients in one call: MG94 eigensystem (S, pi, Q, lam,
+ * U, V) with raw time, FP64 or mixed precision; grad[n_nodes]. */
+h3g_status h3g_branch_length_gradients(h3g_problem* prob, int S, const double* pi, const double* Q, const double* lam,
+                                       const double* U, const double* V, const double* bl, int precision,
+                                       double* lnl, double* grad);
+
+/* Device time of the last h3g_eval's kernels in milliseconds (CUDA events on
+ * the context stream), and the number of kernel launches it made. */
+h3g_status h3g_last_eval_stats(const h3g_problem* prob, double* device_ms, int* n_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* H3G_H */

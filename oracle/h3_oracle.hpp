@@ -1,0 +1,1012 @@
+// h3_oracle.hpp — CPU oracle for the MG94xREV codon likelihood core.
+//
+// TEST INFRASTRUCTURE ONLY.  This is a plain FP64 restatement of the
+// reference engine (veg/hyphy-3, header-only C++ with Eigen) written without
+// Eigen, used by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+// leg as the checker.  The product library never links or calls it.
+//
+// Every function cites the reference file:line it restates.  Parity is pinned
+// against the reference's own known answers (tests/golden/): the MG94 point
+// log-likelihood on cd2_reduced (benchmarks/ground_truth/
+// cd2_reduced_point_truth.json, asserted in tests/test_core.cpp:95-124), the
+// alignment statistics asserted in tests/test_core.cpp:12-37, and the finite
+// difference gradient tests (tests/test_core.cpp:149-223,
+// tests/test_cpp_autograd.cpp:47-104).
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cctype>
+#include <cmath>
+#include <cstdint>
+#include <fstream>
+#include <limits>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace h3o {
+
+// ---------------------------------------------------------------- matrices
+struct Mat {
+    int r = 0, c = 0;
+    std::vector<double> a;
+    Mat() = default;
+    Mat(int r_, int c_, double v = 0.0) : r(r_), c(c_), a(size_t(r_) * c_, v) {}
+    double& operator()(int i, int j) { return a[size_t(i) * c + j]; }
+    double operator()(int i, int j) const { return a[size_t(i) * c + j]; }
+    static Mat eye(int n) { Mat m(n, n); for (int i = 0; i < n; ++i) m(i, i) = 1.0; return m; }
+};
+
+inline Mat matmul(const Mat& A, const Mat& B) {
+    Mat C(A.r, B.c);
+    for (int i = 0; i < A.r; ++i)
+        for (int k = 0; k < A.c; ++k) {
+            double a = A(i, k);
+            if (a == 0.0) continue;
+            const double* b = &B.a[size_t(k) * B.c];
+            double* c = &C.a[size_t(i) * C.c];
+            for (int j = 0; j < B.c; ++j) c[j] += a * b[j];
+        }
+    return C;
+}
+inline Mat transpose(const Mat& A) {
+    Mat T(A.c, A.r);
+    for (int i = 0; i < A.r; ++i) for (int j = 0; j < A.c; ++j) T(j, i) = A(i, j);
+    return T;
+}
+// y = A x
+inline void matvec(const Mat& A, const double* x, double* y) {
+    for (int i = 0; i < A.r; ++i) {
+        const double* row = &A.a[size_t(i) * A.c];
+        double s = 0.0;
+        for (int j = 0; j < A.c; ++j) s += row[j] * x[j];
+        y[i] = s;
+    }
+}
+// y = A^T x
+inline void matvec_t(const Mat& A, const double* x, double* y) {
+    for (int j = 0; j < A.c; ++j) y[j] = 0.0;
+    for (int i = 0; i < A.r; ++i) {
+        const double* row = &A.a[size_t(i) * A.c];
+        double xi = x[i];
+        for (int j = 0; j < A.c; ++j) y[j] += row[j] * xi;
+    }
+}
+
+// Neumaier compensated summation (likelihood.hpp:33-51).
+struct Neumaier {
+    double s = 0.0, c = 0.0;
+    void add(double x) {
+        double t = s + x;
+        if (std::fabs(s) >= std::fabs(x)) c += (s - t) + x; else c += (x - t) + s;
+        s = t;
+    }
+    double value() const { return s + c; }
+};
+
+// ------------------------------------------------------------ genetic code
+// Nucleotide coding A=0 C=1 G=2 T=3 (types.hpp:34-43).
+inline int nuc_index(char ch) {
+    switch (ch) {
+        case 'A': case 'a': return 0;
+        case 'C': case 'c': return 1;
+        case 'G': case 'g': return 2;
+        case 'T': case 't': case 'U': case 'u': return 3;
+        default: return -1;
+    }
+}
+// IUPAC bitmask A=1 C=2 G=4 T=8 (types.hpp:47-67).
+inline unsigned iupac_bits(char ch) {
+    switch (std::toupper(static_cast<unsigned char>(ch))) {
+        case 'A': return 1; case 'C': return 2; case 'G': return 4; case 'T': case 'U': return 8;
+        case 'R': return 5; case 'Y': return 10; case 'S': return 6; case 'W': return 9;
+        case 'K': return 12; case 'M': return 3; case 'B': return 14; case 'D': return 13;
+        case 'H': return 11; case 'V': return 7;
+        default: return 15;
+    }
+}
+
+// Sense-codon table and codon-pair difference records (genetic_code.hpp:127-200).
+struct Code {
+    std::string name;
+    int S = 0;
+    char aa[64];        // amino acid of codon index 16*n1+4*n2+n3, '*' for stop
+    int sense[64];      // codon index -> sense index or -1
+    int codon[64];      // sense index -> codon index
+    struct Diff { int nd = 0; bool syn = false; int pos[3] = {-1, -1, -1}, from[3] = {-1, -1, -1}, to[3] = {-1, -1, -1}; };
+    std::vector<Diff> diff; // S*S, row-major [from][to]
+
+    // Standard code (NCBI table 1) as amino-acid letters in TCAG-major codon order,
+    // the order in which the table is conventionally printed.
+    static Code make(const std::string& which) {
+        static const char* tcag = "FFLLSSSSYY**CC*WLLLLPPPPHHQQRRRRIIIMTTTTNNKKSSRRVVVVAAAADDEEGGGG";
+        static const int to_tcag[4] = {2, 1, 3, 0}; // A C G T -> position in T C A G
+        Code c;
+        c.name = which;
+        for (int n1 = 0; n1 < 4; ++n1) for (int n2 = 0; n2 < 4; ++n2) for (int n3 = 0; n3 < 4; ++n3)
+            c.aa[16 * n1 + 4 * n2 + n3] = tcag[16 * to_tcag[n1] + 4 * to_tcag[n2] + to_tcag[n3]];
+        auto set = [&](const char* trip, char a) {
+            c.aa[16 * nuc_index(trip[0]) + 4 * nuc_index(trip[1]) + nuc_index(trip[2])] = a;
+        };
+        std::string w = which;
+        std::transform(w.begin(), w.end(), w.begin(), ::tolower);
+        if (w == "universal" || w == "standard" || w == "1") {
+        } else if (w == "vertebrate-mtdna" || w == "vertebrate_mtdna" || w == "2") {
+            set("AGA", '*'); set("AGG", '*'); set("ATA", 'M'); set("TGA", 'W');
+        } else {
+            throw std::runtime_error("oracle: unsupported genetic code " + which);
+        }
+        int s = 0;
+        for (int i = 0; i < 64; ++i) {
+            c.codon[i] = -1;
+            if (c.aa[i] == '*') { c.sense[i] = -1; continue; }
+            c.sense[i] = s; c.codon[s] = i; ++s;
+        }
+        c.S = s;
+        c.diff.assign(size_t(s) * s, Diff{});
+        for (int u = 0; u < s; ++u) for (int v = 0; v < s; ++v) {
+            if (u == v) continue;
+            Diff& d = c.diff[size_t(u) * s + v];
+            int cu = c.codon[u], cv = c.codon[v];
+            for (int p = 0; p < 3; ++p) {
+                int sh = 2 * (2 - p);
+                int a = (cu >> sh) & 3, b = (cv >> sh) & 3;
+                if (a != b) { d.pos[d.nd] = p; d.from[d.nd] = a; d.to[d.nd] = b; ++d.nd; }
+            }
+            d.syn = (c.aa[cu] == c.aa[cv]);
+        }
+        return c;
+    }
+    const Diff& df(int u, int v) const { return diff[size_t(u) * S + v]; }
+    uint64_t all_sense() const { return S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1); }
+    int triplet_sense(char a, char b, char c3) const {
+        int x = nuc_index(a), y = nuc_index(b), z = nuc_index(c3);
+        if (x < 0 || y < 0 || z < 0) return -1;
+        return sense[16 * x + 4 * y + z];
+    }
+    // genetic_code.hpp:82-109
+    uint64_t triplet_mask(char a, char b, char c3) const {
+        if (a == '!' || b == '!' || c3 == '!') return all_sense();
+        unsigned m1 = iupac_bits(a), m2 = iupac_bits(b), m3 = iupac_bits(c3);
+        if (m1 == 15 && m2 == 15 && m3 == 15) return all_sense();
+        uint64_t m = 0;
+        for (int i = 0; i < 4; ++i) if (m1 >> i & 1)
+            for (int j = 0; j < 4; ++j) if (m2 >> j & 1)
+                for (int k = 0; k < 4; ++k) if (m3 >> k & 1) {
+                    int s = sense[16 * i + 4 * j + k];
+                    if (s >= 0) m |= uint64_t(1) << s;
+                }
+        return m ? m : all_sense();
+    }
+    int codon_nuc(int s, int pos) const { return (codon[s] >> (2 * (2 - pos))) & 3; }
+};
+
+// --------------------------------------------------------------- alignment
+struct Alignment {
+    std::vector<std::string> names;
+    std::vector<std::string> seqs;
+    std::string embedded_tree;
+    Code code;
+    int n_codons = 0;
+    // pattern store: states[p * T + t], masks[p * T + t]
+    int T = 0, P = 0;
+    std::vector<int8_t> states;
+    std::vector<uint64_t> masks;
+    std::vector<double> weights;
+    double nuc_freq[4] = {0, 0, 0, 0};
+    double pos_freq[3][4] = {};   // CF3x4-corrected (alignment.hpp:1017)
+    std::vector<double> pi;       // codon_frequencies_f3x4
+
+    // alignment.hpp:665-723 (finalize) + :893-1019 (frequencies) + :1021-1078 (patterns)
+    void finalize(const std::string& code_name = "Universal") {
+        code = Code::make(code_name);
+        if (seqs.empty()) throw std::runtime_error("Empty alignment");
+        T = int(seqs.size());
+        size_t L = seqs[0].size();
+        for (auto& s : seqs) if (s.size() != L) throw std::runtime_error("Sequences have unequal lengths in alignment");
+        if (L % 3) throw std::runtime_error("Nucleotide alignment length is not a multiple of 3");
+        n_codons = int(L / 3);
+        std::vector<int8_t> cs(size_t(T) * n_codons);
+        std::vector<uint64_t> cm(size_t(T) * n_codons);
+        for (int t = 0; t < T; ++t) for (int c = 0; c < n_codons; ++c) {
+            const char* x = &seqs[t][3 * c];
+            int s = code.triplet_sense(x[0], x[1], x[2]);
+            cs[size_t(t) * n_codons + c] = int8_t(s);
+            cm[size_t(t) * n_codons + c] = s >= 0 ? (uint64_t(1) << s) : code.triplet_mask(x[0], x[1], x[2]);
+        }
+        frequencies();
+        // first-occurrence pattern order
+        std::map<std::pair<std::vector<int8_t>, std::vector<uint64_t>>, int> seen;
+        states.clear(); masks.clear(); weights.clear(); P = 0;
+        std::vector<int8_t> ks(T); std::vector<uint64_t> km(T);
+        for (int c = 0; c < n_codons; ++c) {
+            for (int t = 0; t < T; ++t) { ks[t] = cs[size_t(t) * n_codons + c]; km[t] = cm[size_t(t) * n_codons + c]; }
+            auto key = std::make_pair(ks, km);
+            auto it = seen.find(key);
+            if (it == seen.end()) {
+                seen.emplace(key, P++);
+                states.insert(states.end(), ks.begin(), ks.end());
+                masks.insert(masks.end(), km.begin(), km.end());
+                weights.push_back(1.0);
+            } else {
+                weights[it->second] += 1.0;
+            }
+        }
+    }
+
+    void frequencies() {
+        double nc[4] = {0, 0, 0, 0}, pc[3][4] = {};
+        for (auto& s : seqs)
+            for (int c = 0; c < n_codons; ++c)
+                for (int p = 0; p < 3; ++p) {
+                    int n = nuc_index(s[3 * c + p]);
+                    if (n >= 0) { nc[n] += 1; pc[p][n] += 1; }
+                }
+        double tot = nc[0] + nc[1] + nc[2] + nc[3];
+        if (tot > 0) for (int b = 0; b < 4; ++b) nuc_freq[b] = nc[b] / tot;
+        bool pad = false;
+        for (int b = 0; b < 4; ++b) if (nuc_freq[b] < 1e-8) { nuc_freq[b] = 1e-8; pad = true; }
+        if (pad) { double z = nuc_freq[0] + nuc_freq[1] + nuc_freq[2] + nuc_freq[3]; for (int b = 0; b < 4; ++b) nuc_freq[b] /= z; }
+        double emp[3][4] = {};
+        for (int p = 0; p < 3; ++p) {
+            double z = pc[p][0] + pc[p][1] + pc[p][2] + pc[p][3];
+            if (z > 0) for (int b = 0; b < 4; ++b) emp[p][b] = pc[p][b] / z;
+            bool pd = false;
+            for (int b = 0; b < 4; ++b) if (emp[p][b] < 1e-8) { emp[p][b] = 1e-8; pd = true; }
+            if (pd) { double s = emp[p][0] + emp[p][1] + emp[p][2] + emp[p][3]; for (int b = 0; b < 4; ++b) emp[p][b] /= s; }
+        }
+        // CF3x4 fixed point (alignment.hpp:962-1018)
+        const int S = code.S;
+        pi.assign(S, 0.0);
+        double cur[3][4];
+        std::copy(&emp[0][0], &emp[0][0] + 12, &cur[0][0]);
+        auto product_freqs = [&]() {
+            double z = 0;
+            for (int s = 0; s < S; ++s) {
+                pi[s] = cur[0][code.codon_nuc(s, 0)] * cur[1][code.codon_nuc(s, 1)] * cur[2][code.codon_nuc(s, 2)];
+                z += pi[s];
+            }
+            if (z > 0) for (int s = 0; s < S; ++s) pi[s] /= z;
+        };
+        for (int it = 0; it < 200; ++it) {
+            double prev[3][4];
+            std::copy(&cur[0][0], &cur[0][0] + 12, &prev[0][0]);
+            product_freqs();
+            double q[3][4] = {};
+            for (int s = 0; s < S; ++s) for (int p = 0; p < 3; ++p) q[p][code.codon_nuc(s, p)] += pi[s];
+            for (int p = 0; p < 3; ++p) {
+                for (int b = 0; b < 4; ++b) cur[p][b] *= emp[p][b] / std::max(q[p][b], 1e-12);
+                double z = cur[p][0] + cur[p][1] + cur[p][2] + cur[p][3];
+                if (z > 0) for (int b = 0; b < 4; ++b) cur[p][b] /= z;
+            }
+            double d = 0;
+            for (int p = 0; p < 3; ++p) for (int b = 0; b < 4; ++b) d = std::max(d, std::fabs(cur[p][b] - prev[p][b]));
+            if (d < 1e-14) break;
+        }
+        product_freqs();
+        std::copy(&cur[0][0], &cur[0][0] + 12, &pos_freq[0][0]);
+    }
+};
+
+inline std::string read_text(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw std::runtime_error("Could not open alignment file: " + path);
+    std::stringstream ss; ss << f.rdbuf();
+    return ss.str();
+}
+
+// FASTA: '>' header lines, sequence lines concatenated with whitespace removed.
+inline Alignment parse_fasta(const std::string& text) {
+    Alignment a;
+    std::string line; std::istringstream in(text);
+    int cur = -1;
+    while (std::getline(in, line)) {
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.empty()) continue;
+        if (line[0] == '>') {
+            std::string nm = line.substr(1);
+            while (!nm.empty() && std::isspace(static_cast<unsigned char>(nm.back()))) nm.pop_back();
+            size_t b = 0; while (b < nm.size() && std::isspace(static_cast<unsigned char>(nm[b]))) ++b;
+            a.names.push_back(nm.substr(b)); a.seqs.emplace_back(); cur = int(a.seqs.size()) - 1;
+        } else if (cur >= 0) {
+            for (char ch : line) if (!std::isspace(static_cast<unsigned char>(ch))) a.seqs[cur] += ch;
+        }
+    }
+    return a;
+}
+
+// Minimal NEXUS reader: TAXLABELS, MATRIX (sequential or interleaved) and the first TREE.
+inline Alignment parse_nexus(const std::string& raw) {
+    // strip [...] comments
+    std::string t; t.reserve(raw.size());
+    int depth = 0; char q = 0;
+    for (char ch : raw) {
+        if (q) { t += ch; if (ch == q) q = 0; continue; }
+        if (depth == 0 && (ch == '\'' || ch == '"')) { q = ch; t += ch; continue; }
+        if (ch == '[') { ++depth; continue; }
+        if (ch == ']' && depth > 0) { --depth; continue; }
+        if (depth == 0) t += (ch == '\r') ? '\n' : ch;
+    }
+    auto upper = [](std::string s) { for (auto& ch : s) ch = char(std::toupper(static_cast<unsigned char>(ch))); return s; };
+    std::string T = upper(t);
+    Alignment a;
+    auto unq = [](std::string s) {
+        if (s.size() >= 2 && (s[0] == '\'' || s[0] == '"') && s.back() == s[0]) s = s.substr(1, s.size() - 2);
+        return s;
+    };
+    auto tokens = [&](const std::string& body) {
+        std::vector<std::pair<std::string, bool>> out; // token, starts_line
+        size_t i = 0; bool nl = true;
+        while (i < body.size()) {
+            char ch = body[i];
+            if (ch == '\n') { nl = true; ++i; continue; }
+            if (std::isspace(static_cast<unsigned char>(ch))) { ++i; continue; }
+            std::string tok;
+            if (ch == '\'' || ch == '"') {
+                char qq = ch; tok += ch; ++i;
+                while (i < body.size() && body[i] != qq) tok += body[i++];
+                if (i < body.size()) tok += body[i++];
+            } else {
+                while (i < body.size() && !std::isspace(static_cast<unsigned char>(body[i]))) tok += body[i++];
+            }
+            out.push_back({tok, nl}); nl = false;
+        }
+        return out;
+    };
+    std::vector<std::string> labels;
+    size_t tl = T.find("TAXLABELS");
+    if (tl != std::string::npos) {
+        size_t e = T.find(';', tl);
+        for (auto& tk : tokens(t.substr(tl + 9, e - tl - 9))) labels.push_back(unq(tk.first));
+    }
+    size_t mx = T.find("MATRIX");
+    if (mx == std::string::npos) throw std::runtime_error("NEXUS: no MATRIX");
+    size_t me = t.find(';', mx);
+    auto toks = tokens(t.substr(mx + 6, me - mx - 6));
+    std::unordered_map<std::string, int> idx;
+    for (auto& l : labels) { idx[l] = int(a.names.size()); a.names.push_back(l); a.seqs.emplace_back(); }
+    int cur = -1;
+    for (auto& [tok, starts] : toks) {
+        std::string u = unq(tok);
+        auto it = idx.find(u);
+        bool is_name = labels.empty() ? starts : (it != idx.end());
+        if (is_name) {
+            if (it == idx.end()) { idx[u] = int(a.names.size()); a.names.push_back(u); a.seqs.emplace_back(); it = idx.find(u); }
+            cur = it->second;
+        } else if (cur >= 0) {
+            a.seqs[cur] += tok;
+        }
+    }
+    size_t tr = T.find("BEGIN TREES");
+    if (tr != std::string::npos) {
+        size_t k = T.find("TREE ", tr + 11);
+        if (k != std::string::npos) {
+            size_t eq = t.find('=', k);
+            size_t sc = t.find(';', eq);
+            std::string nw = t.substr(eq + 1, sc - eq - 1);
+            size_t b = 0; while (b < nw.size() && std::isspace(static_cast<unsigned char>(nw[b]))) ++b;
+            a.embedded_tree = nw.substr(b) + ";";
+        }
+    }
+    return a;
+}
+
+inline Alignment load_alignment(const std::string& path, const std::string& code_name = "Universal") {
+    std::string txt = read_text(path);
+    size_t b = 0; while (b < txt.size() && std::isspace(static_cast<unsigned char>(txt[b]))) ++b;
+    Alignment a = (txt.compare(b, 6, "#NEXUS") == 0 || txt.compare(b, 6, "#nexus") == 0) ? parse_nexus(txt) : parse_fasta(txt);
+    a.finalize(code_name);
+    return a;
+}
+
+// -------------------------------------------------------------------- tree
+// Node ids follow the reference parser's creation order: '(' opens an
+// internal node, a label before ',' or ')' creates a leaf (tree.hpp:273-585).
+struct Tree {
+    std::vector<int> parent;
+    std::vector<std::vector<int>> children;
+    std::vector<std::string> name;
+    std::vector<double> bl;
+    std::vector<char> leaf;
+    std::vector<int> post;
+    int root = -1;
+    int n() const { return int(parent.size()); }
+
+    int add() { parent.push_back(-1); children.emplace_back(); name.emplace_back(); bl.push_back(0.0); leaf.push_back(0); return n() - 1; }
+    void label(int id, std::string tok) {
+        size_t lb = tok.find('{'), rb = tok.find('}');
+        if (lb != std::string::npos && rb != std::string::npos && rb > lb) tok.erase(lb, rb - lb + 1);
+        size_t col = std::string::npos; char q = 0;
+        for (size_t k = 0; k < tok.size(); ++k) {
+            char ch = tok[k];
+            if (q) { if (ch == q) q = 0; continue; }
+            if (ch == '\'' || ch == '"') { q = ch; continue; }
+            if (ch == ':') { col = k; break; }
+        }
+        std::string nm = col == std::string::npos ? tok : tok.substr(0, col);
+        if (col != std::string::npos) { try { bl[id] = std::stod(tok.substr(col + 1)); } catch (...) { bl[id] = 0.0; } }
+        if (nm.size() >= 2 && (nm[0] == '\'' || nm[0] == '"') && nm.back() == nm[0]) nm = nm.substr(1, nm.size() - 2);
+        name[id] = nm;
+    }
+    static Tree parse(std::string s, bool keep_rooted = true) {
+        Tree tr;
+        while (!s.empty() && (s.back() == ';' || std::isspace(static_cast<unsigned char>(s.back())))) s.pop_back();
+        std::string c; bool cm = false; char q = 0;
+        for (char ch : s) {
+            if (q) { c += ch; if (ch == q) q = 0; continue; }
+            if (cm) { if (ch == ']') cm = false; continue; }
+            if (ch == '[') { cm = true; continue; }
+            if (ch == '\'' || ch == '"') { q = ch; c += ch; continue; }
+            if (!std::isspace(static_cast<unsigned char>(ch))) c += ch;
+        }
+        std::vector<int> st; std::string tok; q = 0;
+        for (size_t i = 0; i < c.size(); ++i) {
+            char ch = c[i];
+            if (q) { tok += ch; if (ch == q) q = 0; continue; }
+            if (ch == '\'' || ch == '"') { q = ch; tok += ch; continue; }
+            if (ch == ';') break;
+            if (ch == '(') {
+                int id = tr.add();
+                if (!st.empty()) { tr.children[st.back()].push_back(id); tr.parent[id] = st.back(); }
+                st.push_back(id);
+            } else if (ch == ',' || ch == ')') {
+                if (!tok.empty()) {
+                    int id = tr.add(); tr.leaf[id] = 1; tr.label(id, tok); tok.clear();
+                    if (!st.empty()) { tr.children[st.back()].push_back(id); tr.parent[id] = st.back(); }
+                }
+                if (ch == ')') {
+                    if (st.empty()) throw std::runtime_error("Invalid Newick tree: unbalanced parentheses");
+                    int cur = st.back(); st.pop_back();
+                    size_t j = i + 1; std::string it; char iq = 0;
+                    while (j < c.size()) {
+                        char cj = c[j];
+                        if (iq) { it += cj; if (cj == iq) iq = 0; ++j; continue; }
+                        if (cj == '\'' || cj == '"') { iq = cj; it += cj; ++j; continue; }
+                        if (cj == ',' || cj == ')' || cj == '(' || cj == ';') break;
+                        it += cj; ++j;
+                    }
+                    if (!it.empty()) { tr.label(cur, it); i = j - 1; }
+                }
+            } else tok += ch;
+        }
+        if (!st.empty()) throw std::runtime_error("Invalid Newick tree: unbalanced parentheses");
+        if (tr.n() == 0) throw std::runtime_error("Failed to parse Newick tree: empty tree");
+        for (int i = 0; i < tr.n(); ++i) if (tr.parent[i] < 0) tr.root = i;
+        if (!keep_rooted) tr.unroot();
+        tr.order();
+        return tr;
+    }
+    void order() {
+        post.clear();
+        std::vector<std::pair<int, size_t>> stk{{root, 0}};
+        while (!stk.empty()) {
+            auto& [u, k] = stk.back();
+            if (k < children[u].size()) { int c = children[u][k++]; stk.push_back({c, 0}); }
+            else { post.push_back(u); stk.pop_back(); }
+        }
+    }
+    // tree.hpp:591-690 (model tags are not tracked by the oracle)
+    void unroot() {
+        if (root < 0 || n() <= 3 || children[root].size() != 2) return;
+        int c0 = children[root][0], c1 = children[root][1], ab, ot;
+        if (!leaf[c0]) { ab = c0; ot = c1; } else if (!leaf[c1]) { ab = c1; ot = c0; } else return;
+        bl[ot] += bl[ab];
+        std::vector<int> nc;
+        if (ab == c0) { nc = children[ab]; nc.push_back(ot); } else { nc.push_back(ot); for (int g : children[ab]) nc.push_back(g); }
+        children[root] = nc;
+        std::vector<int> remap(n(), -1); int k = 0;
+        for (int i = 0; i < n(); ++i) if (i != ab) remap[i] = k++;
+        Tree t2;
+        for (int i = 0; i < n(); ++i) if (i != ab) {
+            int id = t2.add(); t2.name[id] = name[i]; t2.bl[id] = bl[i]; t2.leaf[id] = leaf[i];
+        }
+        t2.root = remap[root];
+        for (int i = 0; i < n(); ++i) if (i != ab) for (int cc : children[i]) {
+            t2.children[remap[i]].push_back(remap[cc]); t2.parent[remap[cc]] = remap[i];
+        }
+        t2.parent[t2.root] = -1; t2.bl[t2.root] = 0.0;
+        *this = t2;
+    }
+};
+
+// leaf -> alignment row: exact, case-insensitive, then unique prefix (likelihood.hpp:106-161)
+inline std::vector<int> leaf_map(const Tree& tr, const Alignment& a) {
+    auto low = [](std::string s) { for (auto& c : s) c = char(std::tolower(static_cast<unsigned char>(c))); return s; };
+    std::vector<int> m(tr.n(), -1); int leaves = 0, hit = 0;
+    for (int i = 0; i < tr.n(); ++i) {
+        if (!tr.leaf[i]) continue;
+        ++leaves;
+        std::string nm = tr.name[i];
+        int f = -1;
+        for (size_t t = 0; t < a.names.size(); ++t) if (a.names[t] == nm) { f = int(t); break; }
+        if (f < 0) for (size_t t = 0; t < a.names.size(); ++t) if (low(a.names[t]) == low(nm)) { f = int(t); break; }
+        if (f < 0 && nm.size() >= 3) {
+            int cnt = 0, last = -1; std::string ln = low(nm);
+            for (size_t t = 0; t < a.names.size(); ++t) {
+                std::string ls = low(a.names[t]);
+                if ((ls.size() > ln.size() && ls.compare(0, ln.size(), ln) == 0) ||
+                    (ls.size() >= 3 && ln.size() > ls.size() && ln.compare(0, ls.size(), ls) == 0)) { ++cnt; last = int(t); }
+            }
+            if (cnt == 1) f = last;
+        }
+        m[i] = f; if (f >= 0) ++hit;
+    }
+    if (leaves > 0 && hit == 0) throw std::runtime_error("Phylogenetic tree leaves do not match any sequences in alignment!");
+    return m;
+}
+
+// ----------------------------------------------------------------- MG94xREV
+struct Params {
+    double alpha = 1.0, beta = 1.0;
+    double theta[5] = {1, 1, 1, 1, 1}; // AC AT CG CT GT (AG == 1)
+    double delta = 0.0, psi = 0.0;
+};
+
+inline void nuc_rates(const Params& p, double r[4][4]) {
+    const double AC = p.theta[0], AT = p.theta[1], CG = p.theta[2], CT = p.theta[3], GT = p.theta[4];
+    double t[4][4] = {{0, AC, 1, AT}, {AC, 0, CG, CT}, {1, CG, 0, GT}, {AT, CT, GT, 0}};
+    std::copy(&t[0][0], &t[0][0] + 16, &r[0][0]);
+}
+
+// Cyclic Jacobi eigensolver for a symmetric matrix (Golub & Van Loan,
+// "Matrix Computations", 4th ed., Alg. 8.5.3 with the threshold strategy).
+// On return A's diagonal holds eigenvalues and the columns of V eigenvectors.
+inline void jacobi_eigen(Mat A, std::vector<double>& w, Mat& V) {
+    const int n = A.r;
+    V = Mat::eye(n);
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0, tot = 0;
+        for (int i = 0; i < n; ++i) for (int j = 0; j < n; ++j) { double x = A(i, j) * A(i, j); tot += x; if (i != j) off += x; }
+        if (off <= 1e-30 * tot || off == 0.0) break;
+        for (int p = 0; p < n - 1; ++p) for (int q = p + 1; q < n; ++q) {
+            double apq = A(p, q);
+            if (std::fabs(apq) < 1e-300) continue;
+            double tau = (A(q, q) - A(p, p)) / (2.0 * apq);
+            double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+            double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c;
+            for (int k = 0; k < n; ++k) {
+                double akp = A(k, p), akq = A(k, q);
+                A(k, p) = c * akp - s * akq; A(k, q) = s * akp + c * akq;
+            }
+            for (int k = 0; k < n; ++k) {
+                double apk = A(p, k), aqk = A(q, k);
+                A(p, k) = c * apk - s * aqk; A(q, k) = s * apk + c * aqk;
+            }
+            for (int k = 0; k < n; ++k) {
+                double vkp = V(k, p), vkq = V(k, q);
+                V(k, p) = c * vkp - s * vkq; V(k, q) = s * vkp + c * vkq;
+            }
+        }
+    }
+    w.resize(n);
+    for (int i = 0; i < n; ++i) w[i] = A(i, i);
+}
+
+struct MG94 {
+    int S = 0;
+    Mat Q, U, Vp;           // Q, U_pi = D^-1/2 E, V_pi = E^T D^1/2
+    std::vector<double> lam, pi;
+    double mu = 0.0;        // scale_factor = -sum pi_i Q_ii (stored, not applied)
+
+    // rate_matrix.hpp:165-249
+    void update(const Params& p, const double pos[3][4], const std::vector<double>& pi_in, const Code& code) {
+        S = code.S; pi = pi_in;
+        double r[4][4]; nuc_rates(p, r);
+        Q = Mat(S, S);
+        for (int i = 0; i < S; ++i) for (int j = 0; j < S; ++j) {
+            if (i == j) continue;
+            const auto& d = code.df(i, j);
+            double rm = d.syn ? p.alpha : p.beta;
+            if (d.nd == 1) Q(i, j) = rm * r[d.from[0]][d.to[0]] * pos[d.pos[0]][d.to[0]];
+            else if (d.nd == 2 && p.delta > 0)
+                Q(i, j) = rm * p.delta * r[d.from[0]][d.to[0]] * r[d.from[1]][d.to[1]] * pos[d.pos[0]][d.to[0]] * pos[d.pos[1]][d.to[1]];
+            else if (d.nd == 3 && p.psi > 0)
+                Q(i, j) = rm * p.psi * r[d.from[0]][d.to[0]] * r[d.from[1]][d.to[1]] * r[d.from[2]][d.to[2]] *
+                          pos[d.pos[0]][d.to[0]] * pos[d.pos[1]][d.to[1]] * pos[d.pos[2]][d.to[2]];
+        }
+        for (int i = 0; i < S; ++i) { double s = 0; for (int j = 0; j < S; ++j) if (j != i) s += Q(i, j); Q(i, i) = -s; }
+        mu = 0; for (int i = 0; i < S; ++i) mu -= pi[i] * Q(i, i);
+        std::vector<double> sq(S), isq(S);
+        for (int i = 0; i < S; ++i) { sq[i] = std::sqrt(std::max(pi[i], 1e-12)); isq[i] = 1.0 / sq[i]; }
+        Mat A(S, S);
+        for (int i = 0; i < S; ++i) for (int j = 0; j < S; ++j) A(i, j) = sq[i] * Q(i, j) * isq[j];
+        for (int i = 0; i < S; ++i) for (int j = i + 1; j < S; ++j) { double m = 0.5 * (A(i, j) + A(j, i)); A(i, j) = A(j, i) = m; }
+        Mat E; jacobi_eigen(A, lam, E);
+        for (auto& l : lam) l = std::min(l, 0.0);
+        U = Mat(S, S); Vp = Mat(S, S);
+        for (int i = 0; i < S; ++i) for (int j = 0; j < S; ++j) { U(i, j) = isq[i] * E(i, j); Vp(j, i) = E(i, j) * sq[i]; }
+    }
+    // rate_matrix.hpp:251-257
+    Mat P(double t) const {
+        Mat W(S, S);
+        for (int i = 0; i < S; ++i) for (int k = 0; k < S; ++k) W(i, k) = U(i, k) * std::exp(lam[k] * t);
+        Mat R = matmul(W, Vp);
+        for (auto& x : R.a) x = std::max(x, 0.0);
+        return R;
+    }
+};
+
+// d Q / d x as used by the Frechet gradients (likelihood.hpp:1537-1576)
+inline Mat dQ_beta(const Params& p, const double pos[3][4], const Code& code) {
+    double r[4][4]; nuc_rates(p, r);
+    Mat d(code.S, code.S);
+    for (int i = 0; i < code.S; ++i) {
+        double s = 0;
+        for (int j = 0; j < code.S; ++j) {
+            if (i == j) continue;
+            const auto& df = code.df(i, j);
+            if (df.nd == 1 && !df.syn) { d(i, j) = r[df.from[0]][df.to[0]] * pos[df.pos[0]][df.to[0]]; s += d(i, j); }
+        }
+        d(i, i) = -s;
+    }
+    return d;
+}
+inline Mat dQ_theta(int u, int v, double alpha, double beta, const double pos[3][4], const Code& code) {
+    Mat d(code.S, code.S);
+    for (int i = 0; i < code.S; ++i) {
+        double s = 0;
+        for (int j = 0; j < code.S; ++j) {
+            if (i == j) continue;
+            const auto& df = code.df(i, j);
+            if (df.nd != 1) continue;
+            int f = df.from[0], t = df.to[0];
+            if ((f == u && t == v) || (f == v && t == u)) { d(i, j) = (df.syn ? alpha : beta) * pos[df.pos[0]][t]; s += d(i, j); }
+        }
+        d(i, i) = -s;
+    }
+    return d;
+}
+static const int kThetaPairs[5][2] = {{0, 1}, {0, 3}, {1, 2}, {1, 3}, {2, 3}}; // AC AT CG CT GT
+
+// ------------------------------------------------- single-pattern inside-outside
+// Per-pattern restatement of the batched two-pass traversal
+// (likelihood.hpp:479-762) with the same 1e-150 / 1e150 scaling scheme.
+struct Pass {
+    std::vector<std::vector<double>> D, V, PD, U;
+    std::vector<int> boost;
+    std::vector<double> lscale;
+    double L = 0, logL = 0;
+};
+
+// likelihood.hpp:54-87
+inline void leaf_vector(const Alignment& a, int p, int taxon, int S, double* out) {
+    if (taxon < 0) { std::fill(out, out + S, 1.0); return; }
+    int st = a.states[size_t(p) * a.T + taxon];
+    if (st >= 0 && st < S) { std::fill(out, out + S, 0.0); out[st] = 1.0; return; }
+    uint64_t m = a.masks[size_t(p) * a.T + taxon];
+    uint64_t all = a.code.all_sense();
+    if (m == 0 || (m & all) == all) { std::fill(out, out + S, 1.0); return; }
+    for (int s = 0; s < S; ++s) out[s] = (m >> s & 1) ? 1.0 : 0.0;
+}
+
+constexpr double kThresh = 1e-150, kUp = 1e150, kDown = 1e-150, kLogScaler = 345.38776394910684;
+
+inline void rescale(double* x, int S, int& count) {
+    double mx = *std::max_element(x, x + S);
+    while (mx < kThresh && mx > 0.0) { for (int i = 0; i < S; ++i) x[i] *= kUp; mx *= kUp; ++count; }
+}
+
+inline void inside_outside(const Tree& tr, const Alignment& a, int p, const std::vector<int>& l2t,
+                           const std::vector<Mat>& Pb, const std::vector<double>& pi, int S, Pass& w, bool outside) {
+    const int n = tr.n();
+    w.D.assign(n, std::vector<double>(S)); w.PD.assign(n, std::vector<double>(S));
+    w.boost.assign(n, 0); w.lscale.assign(n, 0.0);
+    for (int u : tr.post) {
+        if (tr.leaf[u]) { leaf_vector(a, p, l2t[u], S, w.D[u].data()); continue; }
+        auto& D = w.D[u];
+        std::fill(D.begin(), D.end(), 1.0);
+        for (int c : tr.children[u]) {
+            matvec(Pb[c], w.D[c].data(), w.PD[c].data());
+            for (int i = 0; i < S; ++i) D[i] *= w.PD[c][i];
+            w.lscale[u] += w.lscale[c];
+            rescale(D.data(), S, w.boost[u]);
+        }
+        rescale(D.data(), S, w.boost[u]);
+        w.lscale[u] -= w.boost[u] * kLogScaler;
+    }
+    double L = 0; for (int i = 0; i < S; ++i) L += w.D[tr.root][i] * pi[i];
+    w.L = L;
+    w.logL = L > 0 ? std::log(L) + w.lscale[tr.root] : -1e20;
+    if (!outside) return;
+    w.U.assign(n, std::vector<double>(S)); w.V.assign(n, std::vector<double>(S));
+    w.U[tr.root] = pi;
+    for (auto it = tr.post.rbegin(); it != tr.post.rend(); ++it) {
+        int u = *it;
+        if (tr.leaf[u]) continue;
+        const auto& ch = tr.children[u];
+        const size_t k = ch.size();
+        if (!k) continue;
+        std::vector<std::vector<double>> pref(k, std::vector<double>(S, 1.0)), suff(k, std::vector<double>(S, 1.0));
+        std::vector<int> pb(k, 0), sb(k, 0);
+        for (size_t i = 1; i < k; ++i) {
+            for (int s = 0; s < S; ++s) pref[i][s] = pref[i - 1][s] * w.PD[ch[i - 1]][s];
+            pb[i] = pb[i - 1]; rescale(pref[i].data(), S, pb[i]);
+        }
+        for (size_t i = k - 1; i > 0; --i) {
+            for (int s = 0; s < S; ++s) suff[i - 1][s] = suff[i][s] * w.PD[ch[i]][s];
+            sb[i - 1] = sb[i]; rescale(suff[i - 1].data(), S, sb[i - 1]);
+        }
+        for (size_t i = 0; i < k; ++i) {
+            int c = ch[i];
+            auto& Vc = w.V[c];
+            for (int s = 0; s < S; ++s) Vc[s] = w.U[u][s] * pref[i][s] * suff[i][s];
+            int net = w.boost[u] - pb[i] - sb[i];
+            for (; net > 0; --net) for (int s = 0; s < S; ++s) Vc[s] *= kUp;
+            for (; net < 0; ++net) for (int s = 0; s < S; ++s) Vc[s] *= kDown;
+            matvec_t(Pb[c], Vc.data(), w.U[c].data());
+        }
+    }
+}
+
+inline int n_threads_for(int items) {
+#ifdef _OPENMP
+    return std::max(1, std::min(omp_get_max_threads(), items));
+#else
+    (void)items; return 1;
+#endif
+}
+
+// likelihood.hpp:766-806 : lnL from given transition matrices (zero-likelihood
+// patterns contribute weight * -1e20).
+inline double loglik_from_P(const Tree& tr, const Alignment& a, const std::vector<Mat>& Pb,
+                            const std::vector<double>& pi, std::vector<double>* site = nullptr) {
+    const int S = a.code.S, P = a.P;
+    auto l2t = leaf_map(tr, a);
+    std::vector<double> pl(P);
+    #pragma omp parallel num_threads(n_threads_for(P))
+    {
+        Pass w;
+        #pragma omp for schedule(static)
+        for (int p = 0; p < P; ++p) { inside_outside(tr, a, p, l2t, Pb, pi, S, w, false); pl[p] = w.logL; }
+    }
+    Neumaier acc;
+    for (int p = 0; p < P; ++p) acc.add(a.weights[p] * pl[p]);
+    if (site) *site = pl;
+    return acc.value();
+}
+
+// likelihood.hpp:257-292
+inline double mg94_loglik(const Tree& tr, const Alignment& a, const MG94& m, double branch_scale = 1.0,
+                          const std::vector<double>* bl = nullptr) {
+    std::vector<Mat> Pb(tr.n(), Mat::eye(a.code.S));
+    for (int i = 0; i < tr.n(); ++i) if (i != tr.root) Pb[i] = m.P((bl ? (*bl)[i] : tr.bl[i]) * branch_scale);
+    return loglik_from_P(tr, a, Pb, m.pi);
+}
+
+// ------------------------------------------------ general mixture evaluation
+// One engine for the three reference gradient entry points:
+//   * compute_branch_length_gradients   (likelihood.hpp:1102-1211): K=1, M=1, raw time
+//   * compute_joint_frechet_gradients   (likelihood.hpp:1228-1594): K=1, M=1, tau = t*3/mu,
+//     optional test/background partition, global gradients with the d mu term
+//   * BUSTED compute_busted_branch_gradients (busted.hpp:1138-1429): K omega classes mixed
+//     at the P level on test branches, background model elsewhere, M synonymous-rate
+//     classes as separate passes with a root log-sum-exp, raw time.
+// Global gradients for omega classes / mixture weights / thetas extend the same
+// spectral Frechet formula (likelihood.hpp:1428-1520) to the mixture.
+struct MixSpec {
+    std::vector<Params> classes;       // K test-branch models
+    std::vector<double> class_w;       // K mixing weights at the P level
+    bool has_bg = false; Params bg;    // background model for non-test branches
+    std::vector<char> is_test;         // per node (empty = all test)
+    std::vector<double> rates{1.0}, rate_w{1.0};
+    bool normalized_time = false;      // tau = t * 3 / mu (per model)
+    bool want_global = false;
+    bool zero_l_sentinel = false;      // true: L<=0 contributes w * -1e20 to lnL
+};
+struct MixResult {
+    double lnl = 0;
+    std::vector<double> grad_t;        // per node (root 0)
+    std::vector<double> grad_beta;     // per test class k (d/d beta_k)
+    double grad_beta_bg = 0;
+    std::vector<double> grad_class_w;  // d/d c_k (raw partials)
+    double grad_theta[5] = {0, 0, 0, 0, 0};
+    std::vector<double> grad_rate_w;   // d/d rho_m (raw partials)
+    std::vector<double> site_lnl;
+};
+
+inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec& sp, const std::vector<double>& bl) {
+    const int S = a.code.S, n = tr.n(), P = a.P;
+    const int K = int(sp.classes.size()), M = int(sp.rates.size());
+    auto l2t = leaf_map(tr, a);
+    auto test = [&](int b) { return sp.is_test.empty() ? true : bool(sp.is_test[b]); };
+    std::vector<MG94> mk(K); for (int k = 0; k < K; ++k) mk[k].update(sp.classes[k], a.pos_freq, a.pi, a.code);
+    MG94 mbg; if (sp.has_bg) mbg.update(sp.bg, a.pos_freq, a.pi, a.code);
+    auto conv = [&](const MG94& m) { return sp.normalized_time ? 3.0 / std::max(m.mu, 1e-12) : 1.0; };
+    // per (m, b): P, dP/dt, and the per-class (class, tau) used
+    std::vector<std::vector<Mat>> Pm(M, std::vector<Mat>(n, Mat::eye(S))), dPm(M, std::vector<Mat>(n, Mat(S, S)));
+    std::vector<std::vector<std::vector<Mat>>> Pk(M, std::vector<std::vector<Mat>>(n));
+    for (int m = 0; m < M; ++m) for (int b = 0; b < n; ++b) {
+        if (b == tr.root) continue;
+        double r = sp.rates[m];
+        if (test(b)) {
+            Pm[m][b] = Mat(S, S);
+            Pk[m][b].resize(K);
+            for (int k = 0; k < K; ++k) {
+                double cv = conv(mk[k]);
+                Mat Pkb = mk[k].P(r * bl[b] * cv);
+                Mat QP = matmul(mk[k].Q, Pkb);
+                for (size_t e = 0; e < Pkb.a.size(); ++e) {
+                    Pm[m][b].a[e] += sp.class_w[k] * Pkb.a[e];
+                    dPm[m][b].a[e] += sp.class_w[k] * r * cv * QP.a[e];
+                }
+                Pk[m][b][k] = std::move(Pkb);
+            }
+        } else {
+            double cv = conv(mbg);
+            Mat Pb = mbg.P(r * bl[b] * cv);
+            Mat QP = matmul(mbg.Q, Pb);
+            for (size_t e = 0; e < QP.a.size(); ++e) dPm[m][b].a[e] = r * cv * QP.a[e];
+            Pm[m][b] = std::move(Pb);
+        }
+    }
+    MixResult res;
+    res.grad_t.assign(n, 0.0);
+    res.site_lnl.assign(P, 0.0);
+    std::vector<double> pat_ll(P, 0.0);
+    std::vector<std::vector<double>> pat_g(n, std::vector<double>(P, 0.0));
+    std::vector<std::vector<double>> pat_rw(M, std::vector<double>(P, 0.0));
+    // A_{m,b} = sum_p f_{m,p} V D^T, accumulated per thread then reduced in thread order
+    const bool G = sp.want_global;
+    int nt = n_threads_for(P);
+    std::vector<std::vector<Mat>> Athr(G ? nt : 0);
+    #pragma omp parallel num_threads(nt)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        if (G) Athr[tid].assign(size_t(M) * n, Mat(S, S));
+        std::vector<Pass> w(M);
+        std::vector<double> tmp(S);
+        #pragma omp for schedule(static)
+        for (int p = 0; p < P; ++p) {
+            double wt = a.weights[p];
+            std::vector<double> post(M, 0.0);
+            for (int m = 0; m < M; ++m)
+                if (M == 1 || sp.rate_w[m] > 1e-12) inside_outside(tr, a, p, l2t, Pm[m], a.pi, S, w[m], true);
+            bool ok = false;
+            if (M == 1) {
+                if (w[0].L > 0) { pat_ll[p] = wt * w[0].logL; post[0] = 1.0; ok = true; }
+                else if (sp.zero_l_sentinel) pat_ll[p] = wt * -1e20;
+                res.site_lnl[p] = w[0].L > 0 ? w[0].logL : -1e20;
+            } else {
+                double mx = -std::numeric_limits<double>::infinity();
+                for (int m = 0; m < M; ++m)
+                    if (sp.rate_w[m] > 1e-12 && w[m].L > 0) mx = std::max(mx, std::log(sp.rate_w[m]) + w[m].logL);
+                res.site_lnl[p] = -1e20;
+                if (mx > -1e19) {
+                    double se = 0;
+                    for (int m = 0; m < M; ++m)
+                        if (sp.rate_w[m] > 1e-12 && w[m].L > 0) { post[m] = std::exp(std::log(sp.rate_w[m]) + w[m].logL - mx); se += post[m]; }
+                    if (se > 0) {
+                        pat_ll[p] = wt * (mx + std::log(se));
+                        res.site_lnl[p] = mx + std::log(se);
+                        for (int m = 0; m < M; ++m) post[m] /= se;
+                        ok = true;
+                    }
+                }
+                if (!ok && sp.zero_l_sentinel) pat_ll[p] = wt * -1e20;
+            }
+            if (!ok) continue;
+            for (int m = 0; m < M; ++m) {
+                if (post[m] <= 1e-12 && M > 1) continue;
+                if (M > 1) pat_rw[m][p] = wt * post[m] / sp.rate_w[m];
+                double f = wt * post[m] / w[m].L;
+                for (int b = 0; b < n; ++b) {
+                    if (b == tr.root) continue;
+                    matvec(dPm[m][b], w[m].D[b].data(), tmp.data());
+                    double g = 0; for (int s = 0; s < S; ++s) g += w[m].V[b][s] * tmp[s];
+                    pat_g[b][p] += f * g;
+                    if (G) {
+                        Mat& A = Athr[tid][size_t(m) * n + b];
+                        const auto& Vb = w[m].V[b]; const auto& Db = w[m].D[b];
+                        for (int i = 0; i < S; ++i) { double vi = f * Vb[i]; if (vi == 0) continue; double* row = &A.a[size_t(i) * S]; for (int j = 0; j < S; ++j) row[j] += vi * Db[j]; }
+                    }
+                }
+            }
+        }
+    }
+    Neumaier acc; for (int p = 0; p < P; ++p) acc.add(pat_ll[p]);
+    res.lnl = acc.value();
+    std::vector<double> dL_dtau(n, 0.0);
+    for (int b = 0; b < n; ++b) {
+        if (b == tr.root) continue;
+        Neumaier g; for (int p = 0; p < P; ++p) g.add(pat_g[b][p]);
+        res.grad_t[b] = g.value();
+    }
+    res.grad_rate_w.assign(M, 0.0);
+    if (M > 1) for (int m = 0; m < M; ++m) { Neumaier g; for (int p = 0; p < P; ++p) g.add(pat_rw[m][p]); res.grad_rate_w[m] = g.value(); }
+    if (!G) return res;
+    std::vector<Mat> A(size_t(M) * n, Mat(S, S));
+    for (auto& th : Athr) for (size_t i = 0; i < A.size(); ++i) for (size_t e = 0; e < A[i].a.size(); ++e) A[i].a[e] += th[i].a[e];
+    // spectral Frechet accumulation H = sum_b (U^T A_b V^T) o E(lambda, tau_b) (likelihood.hpp:1428-1471)
+    auto frechetE = [&](const MG94& mm, double tau, Mat& E) {
+        E = Mat(S, S);
+        for (int i = 0; i < S; ++i) for (int j = 0; j < S; ++j) {
+            double d = mm.lam[i] - mm.lam[j];
+            E(i, j) = std::fabs(d) < 1e-9 ? tau * std::exp(mm.lam[i] * tau) : (std::exp(mm.lam[i] * tau) - std::exp(mm.lam[j] * tau)) / d;
+        }
+    };
+    std::vector<Mat> Hk(K, Mat(S, S)); Mat Hbg(S, S);
+    std::vector<double> sum_tau_g(K, 0.0); double sum_tau_g_bg = 0.0;
+    res.grad_class_w.assign(K, 0.0);
+    for (int m = 0; m < M; ++m) for (int b = 0; b < n; ++b) {
+        if (b == tr.root) continue;
+        const Mat& Ab = A[size_t(m) * n + b];
+        double r = sp.rates[m];
+        if (test(b)) {
+            for (int k = 0; k < K; ++k) {
+                double tau = r * bl[b] * conv(mk[k]);
+                // d/dc_k : <A, P_k>
+                double s = 0; for (size_t e = 0; e < Ab.a.size(); ++e) s += Ab.a[e] * Pk[m][b][k].a[e];
+                res.grad_class_w[k] += s;
+                Mat At = matmul(matmul(transpose(mk[k].U), Ab), transpose(mk[k].Vp));
+                Mat E; frechetE(mk[k], tau, E);
+                for (size_t e = 0; e < At.a.size(); ++e) Hk[k].a[e] += sp.class_w[k] * At.a[e] * E.a[e];
+                // tau * dlnL/dtau through this class, for the d mu term
+                Mat QP = matmul(mk[k].Q, Pk[m][b][k]);
+                double g = 0; for (size_t e = 0; e < Ab.a.size(); ++e) g += Ab.a[e] * QP.a[e];
+                sum_tau_g[k] += sp.class_w[k] * tau * g;
+            }
+        } else {
+            double tau = r * bl[b] * conv(mbg);
+            Mat At = matmul(matmul(transpose(mbg.U), Ab), transpose(mbg.Vp));
+            Mat E; frechetE(mbg, tau, E);
+            for (size_t e = 0; e < At.a.size(); ++e) Hbg.a[e] += At.a[e] * E.a[e];
+            Mat QP = matmul(mbg.Q, Pm[m][b]);
+            double g = 0; for (size_t e = 0; e < Ab.a.size(); ++e) g += Ab.a[e] * QP.a[e];
+            sum_tau_g_bg += tau * g;
+        }
+    }
+    auto part = [&](const MG94& mm, const Mat& H, double sum_tg, const Mat& dQ) {
+        Mat Mx = matmul(matmul(mm.Vp, dQ), mm.U);
+        double p1 = 0; for (size_t e = 0; e < Mx.a.size(); ++e) p1 += Mx.a[e] * H.a[e];
+        double p2 = 0;
+        if (sp.normalized_time) {
+            double dmu = 0; for (int i = 0; i < S; ++i) dmu -= mm.pi[i] * dQ(i, i);
+            p2 = -(dmu / std::max(mm.mu, 1e-12)) * sum_tg;
+        }
+        return p1 + p2;
+    };
+    res.grad_beta.assign(K, 0.0);
+    for (int k = 0; k < K; ++k) res.grad_beta[k] = part(mk[k], Hk[k], sum_tau_g[k], dQ_beta(sp.classes[k], a.pos_freq, a.code));
+    if (sp.has_bg) res.grad_beta_bg = part(mbg, Hbg, sum_tau_g_bg, dQ_beta(sp.bg, a.pos_freq, a.code));
+    for (int x = 0; x < 5; ++x) {
+        double g = 0;
+        for (int k = 0; k < K; ++k)
+            g += part(mk[k], Hk[k], sum_tau_g[k], dQ_theta(kThetaPairs[x][0], kThetaPairs[x][1], sp.classes[k].alpha, sp.classes[k].beta, a.pos_freq, a.code));
+        if (sp.has_bg)
+            g += part(mbg, Hbg, sum_tau_g_bg, dQ_theta(kThetaPairs[x][0], kThetaPairs[x][1], sp.bg.alpha, sp.bg.beta, a.pos_freq, a.code));
+        res.grad_theta[x] = g;
+    }
+    return res;
+}
+
+// likelihood.hpp:1102-1211
+inline std::pair<double, std::vector<double>> branch_length_gradients(const Tree& tr, const Alignment& a, const Params& p,
+                                                                      std::vector<double> bl) {
+    if (bl.empty()) bl = tr.bl;
+    MixSpec sp; sp.classes = {p}; sp.class_w = {1.0};
+    auto r = mixture_eval(tr, a, sp, bl);
+    return {r.lnl, r.grad_t};
+}
+
+// likelihood.hpp:1228-1594 (grad_branches = conv * dL/dtau; globals include the d mu term)
+inline MixResult joint_frechet_gradients(const Tree& tr, const Alignment& a, const Params& p, std::vector<double> bl,
+                                         const std::vector<char>* is_test = nullptr, double omega_bg = -1.0) {
+    if (bl.empty()) bl = tr.bl;
+    MixSpec sp; sp.classes = {p}; sp.class_w = {1.0}; sp.normalized_time = true; sp.want_global = true;
+    if (is_test && int(is_test->size()) == tr.n() && omega_bg >= 0.0) {
+        sp.has_bg = true; sp.bg = p; sp.bg.beta = omega_bg; sp.is_test = *is_test;
+    }
+    return mixture_eval(tr, a, sp, bl);
+}
+
+} // namespace h3o

@@ -1,0 +1,166 @@
+// Python bindings of the CPU oracle (test infrastructure only; see h3_oracle.hpp).
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include "h3_oracle.hpp"
+
+namespace py = pybind11;
+using namespace h3o;
+
+static Params params_from(const py::dict& d) {
+    Params p;
+    if (d.contains("alpha")) p.alpha = d["alpha"].cast<double>();
+    if (d.contains("beta")) p.beta = d["beta"].cast<double>();
+    if (d.contains("theta")) {
+        auto t = d["theta"].cast<std::vector<double>>();
+        if (t.size() != 5) throw std::runtime_error("theta must have 5 entries (AC AT CG CT GT)");
+        std::copy(t.begin(), t.end(), p.theta);
+    }
+    if (d.contains("delta")) p.delta = d["delta"].cast<double>();
+    if (d.contains("psi")) p.psi = d["psi"].cast<double>();
+    return p;
+}
+
+static py::array_t<double> mat_np(const Mat& m) {
+    py::array_t<double> a({m.r, m.c});
+    std::copy(m.a.begin(), m.a.end(), a.mutable_data());
+    return a;
+}
+static Mat np_mat(const py::array_t<double, py::array::c_style | py::array::forcecast>& a) {
+    if (a.ndim() != 2) throw std::runtime_error("expected a 2-D array");
+    Mat m(int(a.shape(0)), int(a.shape(1)));
+    std::copy(a.data(), a.data() + m.a.size(), m.a.begin());
+    return m;
+}
+
+static py::dict mix_dict(const MixResult& r) {
+    py::dict d;
+    d["lnl"] = r.lnl;
+    d["grad_t"] = r.grad_t;
+    d["grad_beta"] = r.grad_beta;
+    d["grad_beta_bg"] = r.grad_beta_bg;
+    d["grad_class_w"] = r.grad_class_w;
+    d["grad_theta"] = std::vector<double>(r.grad_theta, r.grad_theta + 5);
+    d["grad_rate_w"] = r.grad_rate_w;
+    d["site_lnl"] = r.site_lnl;
+    return d;
+}
+
+PYBIND11_MODULE(h3oracle, m) {
+    m.doc() = "FP64 CPU oracle of the MG94xREV likelihood core (test infrastructure only)";
+
+    py::class_<Alignment>(m, "Alignment")
+        .def_static("load", &load_alignment, py::arg("path"), py::arg("code") = "Universal")
+        .def_static("from_sequences", [](const std::vector<std::string>& names, const std::vector<std::string>& seqs, const std::string& code) {
+            Alignment a; a.names = names; a.seqs = seqs; a.finalize(code); return a;
+        }, py::arg("names"), py::arg("seqs"), py::arg("code") = "Universal")
+        .def_readonly("names", &Alignment::names)
+        .def_readonly("embedded_tree", &Alignment::embedded_tree)
+        .def_readonly("num_taxa", &Alignment::T)
+        .def_readonly("num_patterns", &Alignment::P)
+        .def_readonly("num_codons", &Alignment::n_codons)
+        .def_readonly("weights", &Alignment::weights)
+        .def_readonly("pi", &Alignment::pi)
+        .def_property_readonly("nuc_freq", [](const Alignment& a) { return std::vector<double>(a.nuc_freq, a.nuc_freq + 4); })
+        .def_property_readonly("pos_freq", [](const Alignment& a) {
+            py::array_t<double> r({3, 4}); std::copy(&a.pos_freq[0][0], &a.pos_freq[0][0] + 12, r.mutable_data()); return r; })
+        .def_property_readonly("states", [](const Alignment& a) {
+            py::array_t<int8_t> r({a.P, a.T}); std::copy(a.states.begin(), a.states.end(), r.mutable_data()); return r; })
+        .def_property_readonly("masks", [](const Alignment& a) {
+            py::array_t<uint64_t> r({a.P, a.T}); std::copy(a.masks.begin(), a.masks.end(), r.mutable_data()); return r; });
+
+    py::class_<Tree>(m, "Tree")
+        .def_static("parse", &Tree::parse, py::arg("newick"), py::arg("keep_rooted") = true)
+        .def_readonly("parent", &Tree::parent)
+        .def_readonly("children", &Tree::children)
+        .def_readonly("names", &Tree::name)
+        .def_readonly("branch_lengths", &Tree::bl)
+        .def_readonly("post_order", &Tree::post)
+        .def_readonly("root", &Tree::root)
+        .def_property_readonly("is_leaf", [](const Tree& t) { return std::vector<bool>(t.leaf.begin(), t.leaf.end()); })
+        .def("num_nodes", &Tree::n);
+
+    m.def("leaf_map", &leaf_map);
+    m.def("genetic_code", [](const std::string& name) {
+        Code c = Code::make(name);
+        py::dict d; d["S"] = c.S;
+        std::vector<std::string> sc; std::string aa;
+        const char* N = "ACGT";
+        for (int s = 0; s < c.S; ++s) {
+            int k = c.codon[s];
+            sc.push_back(std::string{N[k >> 4], N[(k >> 2) & 3], N[k & 3]});
+            aa += c.aa[k];
+        }
+        d["sense_codons"] = sc; d["aa"] = aa;
+        return d;
+    });
+    m.def("mg94", [](const Alignment& a, const py::dict& p) {
+        MG94 mm; mm.update(params_from(p), a.pos_freq, a.pi, a.code);
+        py::dict d; d["Q"] = mat_np(mm.Q); d["U"] = mat_np(mm.U); d["V"] = mat_np(mm.Vp);
+        d["lam"] = mm.lam; d["mu"] = mm.mu; d["pi"] = mm.pi;
+        return d;
+    });
+    m.def("transition_matrix", [](const Alignment& a, const py::dict& p, double t) {
+        MG94 mm; mm.update(params_from(p), a.pos_freq, a.pi, a.code); return mat_np(mm.P(t));
+    });
+    m.def("mg94_loglik", [](const Tree& t, const Alignment& a, const py::dict& p, double branch_scale, std::vector<double> bl) {
+        MG94 mm; mm.update(params_from(p), a.pos_freq, a.pi, a.code);
+        py::gil_scoped_release rel;
+        return mg94_loglik(t, a, mm, branch_scale, bl.empty() ? nullptr : &bl);
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_scale") = 1.0, py::arg("branch_lengths") = std::vector<double>{});
+    m.def("loglik_from_P", [](const Tree& t, const Alignment& a, const std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>>& Ps,
+                              const std::vector<double>& pi) {
+        std::vector<Mat> Pb; for (auto& x : Ps) Pb.push_back(np_mat(x));
+        std::vector<double> site;
+        double l;
+        { py::gil_scoped_release rel; l = loglik_from_P(t, a, Pb, pi, &site); }
+        return py::make_tuple(l, site);
+    });
+    m.def("branch_length_gradients", [](const Tree& t, const Alignment& a, const py::dict& p, std::vector<double> bl) {
+        Params pp = params_from(p);
+        py::gil_scoped_release rel;
+        return branch_length_gradients(t, a, pp, bl);
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths") = std::vector<double>{});
+    m.def("joint_frechet_gradients", [](const Tree& t, const Alignment& a, const py::dict& p, std::vector<double> bl,
+                                        std::vector<bool> is_test, double omega_bg) {
+        Params pp = params_from(p);
+        std::vector<char> it(is_test.begin(), is_test.end());
+        MixResult r;
+        { py::gil_scoped_release rel; r = joint_frechet_gradients(t, a, pp, bl, is_test.empty() ? nullptr : &it, omega_bg); }
+        return mix_dict(r);
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths") = std::vector<double>{},
+       py::arg("is_test") = std::vector<bool>{}, py::arg("omega_bg") = -1.0);
+    m.def("mixture_eval", [](const Tree& t, const Alignment& a, const std::vector<py::dict>& classes, const std::vector<double>& class_w,
+                             py::object bg, std::vector<bool> is_test, std::vector<double> rates, std::vector<double> rate_w,
+                             std::vector<double> bl, bool normalized_time, bool want_global, bool zero_l_sentinel) {
+        MixSpec sp;
+        for (auto& c : classes) sp.classes.push_back(params_from(c));
+        sp.class_w = class_w;
+        if (!bg.is_none()) { sp.has_bg = true; sp.bg = params_from(bg.cast<py::dict>()); }
+        sp.is_test.assign(is_test.begin(), is_test.end());
+        if (!rates.empty()) { sp.rates = rates; sp.rate_w = rate_w; }
+        sp.normalized_time = normalized_time; sp.want_global = want_global; sp.zero_l_sentinel = zero_l_sentinel;
+        if (bl.empty()) bl = t.bl;
+        MixResult r;
+        { py::gil_scoped_release rel; r = mixture_eval(t, a, sp, bl); }
+        return mix_dict(r);
+    }, py::arg("tree"), py::arg("aln"), py::arg("classes"), py::arg("class_w"), py::arg("bg") = py::none(),
+       py::arg("is_test") = std::vector<bool>{}, py::arg("rates") = std::vector<double>{}, py::arg("rate_w") = std::vector<double>{},
+       py::arg("branch_lengths") = std::vector<double>{}, py::arg("normalized_time") = false, py::arg("want_global") = false,
+       py::arg("zero_l_sentinel") = false);
+    m.def("set_threads", [](int n) {
+#ifdef _OPENMP
+        omp_set_num_threads(n);
+#else
+        (void)n;
+#endif
+    });
+    m.def("max_threads", []() {
+#ifdef _OPENMP
+        return omp_get_max_threads();
+#else
+        return 1;
+#endif
+    });
+}

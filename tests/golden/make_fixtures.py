@@ -1,0 +1,64 @@
+"""Copy the reference's own parity fixtures for the likelihood path into tests/golden/.
+
+The reference pins its likelihood core with a handful of bundled datasets and a
+HyPhy 2.5 ground-truth JSON; the GPU box has no copy of the reference, so the
+files its tests read are copied here verbatim (data, not code) and the known
+answers its tests assert are recorded in known_answers.json with their source.
+
+Run from the repository root with the reference checked out read-only:
+    python tests/golden/make_fixtures.py /path/to/reference
+"""
+import json
+import pathlib
+import shutil
+import sys
+
+FILES = {
+    # benchmarks/data/cd2_reduced.fna: read by tests/test_core.cpp:12-37, :95-124, :149-223
+    "cd2_reduced.fna": "benchmarks/data/cd2_reduced.fna",
+    "cd2_reduced.nwk": "benchmarks/data/cd2_reduced.nwk",
+    # adh.nex: tests/test_cpp_autograd.cpp:47-104, python/tests/test_python_autograd.py:114-153
+    "adh.nex": "benchmarks/data/adh.nex",
+    # CD2 full alignment with embedded tree (tests/test_fel_cd2_parity.cpp)
+    "CD2.nex": "benchmarks/data/CD2.nex",
+    "cd2_reduced_point_truth.json": "benchmarks/ground_truth/cd2_reduced_point_truth.json",
+}
+
+
+def main(ref: str) -> None:
+    ref_root = pathlib.Path(ref)
+    out = pathlib.Path(__file__).resolve().parent
+    for dst, src in FILES.items():
+        shutil.copyfile(ref_root / src, out / dst)
+    truth = json.loads((ref_root / FILES["cd2_reduced_point_truth.json"]).read_text())
+    known = {
+        "cd2_reduced": {
+            "source": "benchmarks/ground_truth/cd2_reduced_point_truth.json; asserted in tests/test_core.cpp:95-124",
+            "newick": "((((Pig:0.147969,Cow:0.213430):0.085099,Horse:0.165787,Cat:0.264806):0.058611,"
+                      "((RhMonkey:0.002015,Baboon:0.003108):0.022733,(Human:0.004349,Chimp:0.000799):0.011873)"
+                      ":0.101856):0.340802,Rat:0.050958,Mouse:0.097950);",
+            "params": {"alpha": 1.0, "beta": 0.5, "theta": [1.0, 1.0, 1.0, 2.0, 1.0]},
+            "point_mg94_logl": truth["point_mg94_logl"],
+            "sense_codons": truth["sense_codons"][0],
+            "taxa": truth["taxa"],
+            "sites_codon": truth["sites_codon"],
+            # tests/test_core.cpp:21-24 (empirical nucleotide frequencies, epsilon 1e-4)
+            "nuc_freqs_test_core": [0.456140, 0.114035, 0.254386, 0.175439],
+        },
+        "cd2_reduced_frechet": {
+            "source": "tests/test_core.cpp:149-223 (analytic vs central FD, h=1e-6, |d|/(|g|+1) < 1e-4)",
+            "params": {"alpha": 1.0, "beta": 0.45, "theta": [0.8, 1.2, 0.6, 1.8, 0.9]},
+            "min_branch_length": 1e-4,
+        },
+        "adh_autograd": {
+            "source": "tests/test_cpp_autograd.cpp:47-104; python/tests/test_python_autograd.py:114-153",
+            "params": {"alpha": 1.0, "beta": 0.4, "theta": [1, 1, 1, 1, 1]},
+            "branch_length": 0.05, "fd_eps": 1e-6, "rel_err": 1e-5,
+            "num_taxa": 23, "num_codons": 254, "num_nodes": 44,
+        },
+    }
+    (out / "known_answers.json").write_text(json.dumps(known, indent=1) + "\n")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
