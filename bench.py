@@ -1,0 +1,448 @@
+"""Benchmark: codon site-branch lnL+gradient evaluations per second on one B200.
+
+Workload (one step = one lnL + full-gradient evaluation):
+  BUSTED-style MG94xREV omega mixture on a 64-taxon random unrooted binary tree
+  (125 branches), 1000 simulated codons with 3 % gaps and 1 % ambiguous codons,
+  omega classes {0.1, 1, 5} with weights {0.6, 0.3, 0.1} mixed at the P level;
+  lnL plus the gradient w.r.t. all 125 branch lengths, the 3 omegas, the 3
+  mixture weights and the 5 nucleotide exchangeabilities.  Unit: alignment
+  sites x branches per completed evaluation (1000 x 125 per step).
+
+value  device-resident throughput: branch lengths already on the device, each
+       step timed with CUDA events on the library's stream, L2 flushed (256 MiB
+       write) before every timed step.
+e2e    the same evaluation through the public API (_hyphy3.compute_mixture_gradients)
+       with host inputs and host results, host wall clock around the
+       synchronous calls.
+--impl reference  times the CPU restatement of the reference engine (the
+       reference itself needs Eigen, which this image lacks) on the host cores.
+Multi-GPU (torchrun): one process per GPU, each evaluating its own replica
+gene (independent workloads, no collective); value = all ranks' units / max
+time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+for _p in (ROOT / "hyphy-3_b200" / "python", ROOT / "oracle" / "_build"):
+    sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "codon site*branch lnL+grad evals/s: mixed vs FP64 on 1 B200 at |dlnL|/|lnL|<=1e-7"
+UNIT = "site*branch/s"
+WORKLOAD = ("BUSTED-style 3-omega MG94xREV: 64-taxon random unrooted tree (125 branches), 1000 codons "
+            "(3% gaps, 1% ambiguous), omegas {0.1,1,5} w {0.6,0.3,0.1}; lnL + grads wrt 125 t, 3 omega, 3 w, 5 theta")
+
+
+def build_inputs(seed_offset: int = 0):
+    import _hyphy3 as h
+    from hyphy3.simulate import make_workload
+    wl = make_workload(1)
+    if seed_offset:
+        # independent replica gene for another rank: same shapes, different draw
+        import hyphy3.simulate as sim
+        rng = np.random.default_rng(sim.SEED_BASE + 1 + 1000 * seed_offset)
+        names, seqs = sim.simulate_alignment(wl.tree, wl.n_sites, rng, theta=wl.theta,
+                                             pos_freq=rng.dirichlet(np.ones(4), size=3), omegas=wl.omegas,
+                                             omega_w=wl.omega_w, gap_frac=0.03, ambig_frac=0.01)
+        wl.names, wl.seqs = names, seqs
+    aln = h.Alignment.from_sequences(wl.names, wl.seqs)
+    tree = h.Tree.from_newick(wl.newick)
+    return h, wl, aln, tree
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_dgemm_peak() -> float:
+    """Measured FP64 matmul throughput (cuBLAS DGEMM, 8192^3) in TFLOP/s, best of 5."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def stage_work(aln_P: int, tree, M: int) -> dict:
+    """Algorithmic bytes and FP64 flops per stage for one evaluation (61 states, not padded).
+
+    Partials are counted as one HBM round trip each way: the inside stage
+    reads the messages of internal children, writes D and (non-root) the
+    message P*D; the outside stage reads U of the parent and the sibling
+    messages, writes the scaled outside vector of every child and U of
+    internal children; accum_A reads V and D of every branch.
+    """
+    S = 61
+    nodes = tree.nodes
+    root = tree.root_id
+    internal = [nd for nd in nodes if not nd.is_leaf]
+    cols = aln_P * M
+    vec = 8 * S
+    ins_b = ins_f = out_b = out_f = acc_b = acc_f = 0
+    for nd in internal:
+        int_kids = [c for c in nd.children if not nodes[c].is_leaf]
+        ins_b += vec * (len(int_kids) + 1 + (nd.id != root))
+        ins_f += 2 * S * S * (nd.id != root)
+        k = len(nd.children)
+        out_b += vec * (1 + k)
+        for c in nd.children:
+            out_b += vec * sum(1 for s in nd.children if s != c and not nodes[s].is_leaf)
+            if not nodes[c].is_leaf:
+                out_b += vec
+                out_f += 2 * S * S
+    for nd in nodes:
+        if nd.id == root:
+            continue
+        acc_b += vec * (2 if not nd.is_leaf else 1)
+        acc_f += 2 * S * S
+    return {"inside": (ins_b * cols, ins_f * cols), "outside": (out_b * cols, out_f * cols),
+            "accum_A": (acc_b * cols, acc_f * cols)}
+
+
+def cpu_baseline(wl, reps: int = 3) -> dict:
+    import h3oracle as o
+    a = o.Alignment.from_sequences(wl.names, wl.seqs)
+    t = o.Tree.parse(wl.newick)
+    cls = [{"alpha": 1.0, "beta": om, "theta": wl.theta} for om in wl.omegas]
+    threads = o.max_threads()
+    o.set_threads(threads)
+    bl = list(t.branch_lengths)
+    o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
+        times.append(time.perf_counter() - t0)
+    units = wl.n_sites * (t.num_nodes() - 1)
+    med = statistics.median(times)
+    return {"value": units / med, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{reps} full evaluations (lnL + all gradients, {wl.n_sites} sites x {t.num_nodes() - 1} branches) "
+                      f"after 1 warm-up, median {med:.3f} s"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, wl, _, _ = build_inputs()
+    import h3oracle as o
+    a = o.Alignment.from_sequences(wl.names, wl.seqs)
+    t = o.Tree.parse(wl.newick)
+    cls = [{"alpha": 1.0, "beta": om, "theta": wl.theta} for om in wl.omegas]
+    threads = o.max_threads()
+    o.set_threads(threads)
+    bl = list(t.branch_lengths)
+    for _ in range(max(1, min(args.warmup, 2))):
+        o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
+    steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
+    dt = (time.perf_counter() - t0) / steps
+    units = wl.n_sites * (t.num_nodes() - 1)
+    v = units / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sites": wl.n_sites, "branches": t.num_nodes() - 1},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} full evaluations after warm-up (reference engine restated in C++/OpenMP: "
+                                       "the reference itself needs Eigen 3.4, absent from this image)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    h, wl, aln, tree = build_inputs(seed_offset=rank)
+    from hyphy3 import _capi
+    precision = args.precision
+    if precision == "auto":
+        precision = "mixed" if _mixed_available() else "fp64"
+    prec_code = _capi.PREC_MIXED if precision == "mixed" else _capi.PREC_FP64
+    stream = torch.cuda.Stream()
+    ctx = _capi.Context(local, stream=stream.cuda_stream)
+    states, masks, weights = aln.pattern_arrays()
+    l2t = h.build_leaf_to_taxon_map(tree, aln)
+    n = tree.num_nodes()
+    is_leaf = np.array([nd.is_leaf for nd in tree.nodes], dtype=np.uint8)
+    pr = _capi.Problem(ctx, np.array(tree.parents, dtype=np.int32), is_leaf,
+                       np.array([l2t[i] if is_leaf[i] else -1 for i in range(n)], dtype=np.int32),
+                       states, masks, weights)
+    base = h.MG94Parameters()
+    base.theta_AC, base.theta_AT, base.theta_CG, base.theta_CT, base.theta_GT = wl.theta
+
+    def model_arrays():
+        es = []
+        for om in wl.omegas:
+            p = h.MG94Parameters()
+            p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = wl.theta
+            p.beta = om
+            es.append(h.mg94_eigensystem(aln, p))
+        return es
+
+    es = model_arrays()
+    # directions: 3 omegas (dQ/dbeta of one class) + 5 thetas, built like the public API does
+    dirs = _directions(aln, wl, es)
+    want = _capi.WANT_LNL | _capi.WANT_GRAD_T | _capi.WANT_GRAD_GLOBAL
+    bl = np.array(tree.get_branch_lengths())
+    units = wl.n_sites * (n - 1)
+
+    def install(prec):
+        pr.set_model(pi=aln.codon_frequencies, Q=np.stack([e["Q"] for e in es]), lam=np.stack([e["lam"] for e in es]),
+                     U=np.stack([e["U"] for e in es]), V=np.stack([e["V"] for e in es]),
+                     mu=np.array([e["mu"] for e in es]), class_w=wl.omega_w, dQ=dirs, precision=prec)
+        pr.stage_branch_lengths(bl)
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def device_timed(steps, warmup):
+        for _ in range(warmup):
+            pr.eval_resident(want)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for e0, e1 in evs:
+                flush.zero_()
+                e0.record(stream)
+                pr.eval_resident(want)
+                e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return sum(e0.elapsed_time(e1) for e0, e1 in evs) / 1e3
+
+    results = {}
+    for prec_name, code in ([("fp64", _capi.PREC_FP64)] + ([("mixed", _capi.PREC_MIXED)] if precision == "mixed" else [])):
+        install(code)
+        sampler = ClockSampler(local) if prec_name == precision else None
+        if sampler:
+            sampler.start()
+        secs = device_timed(args.steps, max(args.warmup, 3))
+        clocks = sampler.stop() if sampler else None
+        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        res = pr.read_result(want)
+        stages = pr.profile_stages(want, reps=3)
+        results[prec_name] = {"secs": float(t.item()), "lnl": res["lnl"], "grad_t": res["grad_t"].copy(),
+                              "grad_dir": res["grad_dir"].copy(), "clocks": clocks, "stages": stages}
+    head = results[precision]
+    ms_per_step = head["secs"] / args.steps * 1e3
+    value = units * world * args.steps / head["secs"]
+    _, launches = pr.last_stats()
+    launches_per_eval = sum(v[1] for v in head["stages"].values())
+
+    # end to end through the public API, host buffers in and out
+    h.set_precision(precision)
+    bl_list = list(bl)
+    for _ in range(max(args.warmup, 3)):
+        r_api = h.compute_mixture_gradients(tree, aln, base, bl_list, wl.omegas, wl.omega_w)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r_api = h.compute_mixture_gradients(tree, aln, base, bl_list, wl.omegas, wl.omega_w)
+    e2e_secs = time.perf_counter() - t0
+    et = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = units * world * args.steps / float(et.item())
+    h2d = int(n * 8)
+    d2h = int((2 + n + len(wl.omegas) + len(wl.omegas) + 1) * 8 + dirs.shape[0] * len(es) * 8 + aln.num_patterns * 8)
+
+    # accuracy of the headline path against the FP64 path on the same inputs
+    acc = None
+    if precision == "mixed":
+        f, m = results["fp64"], results["mixed"]
+        acc = {"rel_dlnl": abs(m["lnl"] - f["lnl"]) / abs(f["lnl"]),
+               "grad_rel_err": float(np.linalg.norm(np.r_[m["grad_t"], m["grad_dir"]] - np.r_[f["grad_t"], f["grad_dir"]]) /
+                                     np.linalg.norm(np.r_[f["grad_t"], f["grad_dir"]]))}
+
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    work = stage_work(aln.num_patterns, tree, 1)
+    stg = head["stages"]
+    dom = max(("inside", "outside", "accum_A"), key=lambda k: stg.get(k, (0.0, 0))[0])
+    dom_ms, dom_launches = stg[dom]
+    dom_bytes, dom_flops = work[dom]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_bytes / (dom_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                "unit": "GB/s", "frac": dom_bytes / (dom_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None,
+                "peak_source": "measured" if peaks else "fallback",
+                "algorithmic_bytes_per_eval": dom_bytes, "stage_ms": dom_ms, "launches_per_eval": dom_launches}
+    fp64_peak = fp64_dgemm_peak() if rank == 0 else None
+    f_st = results["fp64"]["stages"]
+    fp64_pipe = {}
+    for k in ("inside", "outside", "accum_A"):
+        if k in f_st and f_st[k][0] > 0:
+            fl = work[k][1] / (f_st[k][0] * 1e-3) / 1e12
+            fp64_pipe[k] = {"tflops": fl, "frac_of_dgemm": fl / fp64_peak if fp64_peak else None, "ms": f_st[k][0]}
+
+    cpu = cpu_baseline(wl) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if precision == "fp64" else "tf32x3/f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sites": wl.n_sites, "branches": n - 1, "patterns": aln.num_patterns,
+                       "precision": precision, "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "api": "_hyphy3.compute_mixture_gradients", "timing": "host wall clock around synchronous calls"},
+            "gpu_launches": launches_per_eval * args.steps,
+            "roofline": roofline,
+            "fp64_pipe": {"dgemm_peak_tflops": fp64_peak, "stages": fp64_pipe},
+            "stage_ms": {k: v[0] for k, v in stg.items()},
+            "clocks": head["clocks"],
+            "cpu_baseline": cpu,
+            "fp64_value": units * world * args.steps / results["fp64"]["secs"],
+            "accuracy_vs_fp64": acc,
+            "lnl": head["lnl"], "api_lnl": r_api["log_likelihood"],
+        }
+        print(json.dumps(line), flush=True)
+    pr.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def _mixed_available() -> bool:
+    return os.environ.get("H3G_BENCH_PRECISION", "") == "mixed"
+
+
+def _directions(aln, wl, es):
+    """dQ/d omega_k (one class each) and dQ/d theta_x (all classes), shape [8, K, S, S]."""
+    from hyphy3.simulate import universal_code
+    codons, aas = universal_code()
+    pos = np.asarray(aln.pos_nuc_frequencies)
+    S = len(codons)
+    AC, AT, CG, CT, GT = wl.theta
+    r = np.array([[0, AC, 1, AT], [AC, 0, CG, CT], [1, CG, 0, GT], [AT, CT, GT, 0]], dtype=float)
+    single = np.zeros((S, S), dtype=bool)
+    frm = np.zeros((S, S), dtype=int)
+    to = np.zeros((S, S), dtype=int)
+    ps = np.zeros((S, S), dtype=int)
+    syn = np.zeros((S, S), dtype=bool)
+    for i, ci in enumerate(codons):
+        for j, cj in enumerate(codons):
+            d = [q for q in range(3) if ci[q] != cj[q]]
+            if len(d) == 1:
+                single[i, j] = True
+                ps[i, j], frm[i, j], to[i, j] = d[0], ci[d[0]], cj[d[0]]
+                syn[i, j] = aas[i] == aas[j]
+    K = len(es)
+    out = []
+    for k in range(K):
+        dq = np.zeros((K, S, S))
+        m = single & ~syn
+        dq[k][m] = r[frm[m], to[m]] * pos[ps[m], to[m]]
+        dq[k][np.diag_indices(S)] = -dq[k].sum(1)
+        out.append(dq)
+    pairs = [(0, 1), (0, 3), (1, 2), (1, 3), (2, 3)]
+    for (u, v) in pairs:
+        dq = np.zeros((K, S, S))
+        m = single & (((frm == u) & (to == v)) | ((frm == v) & (to == u)))
+        for k, om in enumerate(wl.omegas):
+            rate = np.where(syn, 1.0, om)
+            dq[k][m] = rate[m] * pos[ps[m], to[m]]
+            dq[k][np.diag_indices(S)] = -dq[k].sum(1)
+        out.append(dq)
+    return np.stack(out)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["auto", "fp64", "mixed"], default="auto")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -43,7 +43,7 @@ struct DevArena {
 
 struct h3g_problem {
     h3g_ctx* ctx = nullptr;
-    int n = 0, root = -1, T = 0, P = 0, Pp = 0, NI = 0;
+    int n = 0, root = -1, T = 0, P = 0, Pp = 0, NI = 0, max_state = -1;
     std::vector<int> ch_off, ch, iidx, taxon, in_off, out_off, in_nodes, out_nodes;
     std::vector<uint8_t> leaf;
     DevArena topo_mem, model_mem, work_mem;
@@ -67,7 +67,23 @@ struct h3g_problem {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
     int last_launches = 0;
+    size_t last_h2d = 0, last_d2h = 0;
+    size_t off_out = 0, off_dir = 0, off_site = 0;    // offsets into h_pin
+    // installed model: device buffers reused while the sizes stay the same
+    size_t model_key[5] = {0, 0, 0, 0, 0};
+    uint64_t model_hash = 0;
+    double *m_pi = nullptr, *m_Q = nullptr, *m_lam = nullptr, *m_U = nullptr, *m_V = nullptr, *m_mu = nullptr;
+    double *m_cw = nullptr, *m_rt = nullptr, *m_rw = nullptr, *m_dQ = nullptr;
+    uint8_t* m_it = nullptr;
+    // captured evaluation graphs, keyed by (want, with host copies)
+    struct GraphEntry { unsigned key; cudaGraphExec_t exec; int launches; };
+    std::vector<GraphEntry> graphs;
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
     ~h3g_problem() {
+        drop_graphs();
         if (h_pin) cudaFreeHost(h_pin);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -212,6 +228,9 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
             if (!(weights[p] >= 0.0) || !std::isfinite(weights[p])) return fail(ctx, H3G_ERR_ARG, "pattern weights must be finite and >= 0");
             wt[p] = weights[p];
             for (int t = 0; t < T; ++t) {
+                const int8_t sv = states[size_t(p) * T + t];
+                if (sv >= SP) return fail(ctx, H3G_ERR_ARG, "state index >= 64");
+                pr->max_state = std::max<int>(pr->max_state, sv);
                 st[size_t(t) * Pp + p] = states[size_t(p) * T + t];
                 mk[size_t(t) * Pp + p] = masks[size_t(p) * T + t];
             }
@@ -265,18 +284,22 @@ static void pad_matrix(const double* src, int S, double* dst) {
     for (int i = 0; i < S; ++i) std::copy(src + size_t(i) * S, src + size_t(i) * S + S, dst + size_t(i) * SP);
 }
 
+static size_t n_out_of(const h3g_problem* pr) { return 2 + size_t(pr->n) + pr->K + pr->nmod + pr->M; }
+
 // Allocate the evaluation workspace for (M, K, nmod, ndirs); reuses it when unchanged.
 static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int ndirs) {
     h3g_ctx* ctx = pr->ctx;
     const size_t key[4] = {size_t(M), size_t(K), size_t(nmod), size_t(ndirs)};
     if (pr->w.P && std::equal(key, key + 4, pr->work_key)) return H3G_OK;
     cudaStreamSynchronize(ctx->stream);
+    pr->drop_graphs();
     pr->work_mem.release();
     if (pr->h_pin) { cudaFreeHost(pr->h_pin); pr->h_pin = nullptr; }
     std::copy(key, key + 4, pr->work_key);
     const size_t n = pr->n, NI = pr->NI, Pp = pr->Pp;
     Work& w = pr->w;
     w = Work{};
+    pr->mw = MixedWork{};
     auto& A = pr->work_mem;
     const size_t mats = size_t(M) * n * SP2;
     // enough A chunks for ~600 CTAs, never below 256 patterns per chunk
@@ -318,9 +341,25 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     cudaMemsetAsync(w.gc, 0, size_t(std::max(K, 1)) * M * n * sizeof(double), ctx->stream);
     cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * n * sizeof(double), ctx->stream);
     cudaMemsetAsync(w.Hpart, 0, size_t(nmod) * M * n * SP2 * sizeof(double), ctx->stream);
-    pr->h_pin_count = n + n_out;
+    pr->off_out = n;
+    pr->off_dir = pr->off_out + n_out;
+    pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod;
+    pr->h_pin_count = pr->off_site + size_t(std::max(pr->P, 1));
     H3G_TRY_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&pr->h_pin), pr->h_pin_count * sizeof(double)));
     return H3G_OK;
+}
+
+static uint64_t hash_bytes(uint64_t h, const void* p, size_t n) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, c + i, 8);
+        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+    }
+    for (; i < n; ++i) { h ^= c[i]; h *= 1099511628211ull; }
+    return h;
 }
 
 extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
@@ -336,18 +375,35 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     if (d->precision != H3G_PREC_FP64 && d->precision != H3G_PREC_MIXED) return fail(ctx, H3G_ERR_ARG, "unknown precision");
     if (d->precision == H3G_PREC_MIXED && !mixed_available()) return fail(ctx, H3G_ERR_CUDA, "mixed-precision path not built");
     const int S = d->S, nm = d->n_models;
+    if (pr->max_state >= S) return fail(ctx, H3G_ERR_ARG, "a pattern state index is >= S");
     auto finite = [](const double* a, size_t k) { for (size_t i = 0; i < k; ++i) if (!std::isfinite(a[i])) return false; return true; };
     if (!finite(d->pi, S) || !finite(d->Q, size_t(nm) * S * S) || !finite(d->lam, size_t(nm) * S) || !finite(d->U, size_t(nm) * S * S) ||
         !finite(d->V, size_t(nm) * S * S) || !finite(d->class_w, d->K) || !finite(d->rates, d->M) || !finite(d->rate_w, d->M))
         return fail(ctx, H3G_ERR_NUMERIC, "non-finite model parameters");
     try {
         cudaSetDevice(ctx->device);
+        // identical model already installed: nothing to upload
+        uint64_t h = 1469598103934665603ull;
+        const int scal[9] = {S, nm, d->K, d->has_bg, d->M, d->time_mode, d->n_dirs, d->precision, d->zero_l_sentinel};
+        h = hash_bytes(h, scal, sizeof(scal));
+        h = hash_bytes(h, d->pi, S * sizeof(double));
+        h = hash_bytes(h, d->Q, size_t(nm) * S * S * sizeof(double));
+        h = hash_bytes(h, d->lam, size_t(nm) * S * sizeof(double));
+        h = hash_bytes(h, d->U, size_t(nm) * S * S * sizeof(double));
+        h = hash_bytes(h, d->V, size_t(nm) * S * S * sizeof(double));
+        if (d->mu) h = hash_bytes(h, d->mu, nm * sizeof(double));
+        h = hash_bytes(h, d->class_w, d->K * sizeof(double));
+        h = hash_bytes(h, d->rates, d->M * sizeof(double));
+        h = hash_bytes(h, d->rate_w, d->M * sizeof(double));
+        if (d->is_test) h = hash_bytes(h, d->is_test, size_t(pr->n));
+        if (d->n_dirs > 0) h = hash_bytes(h, d->dQ, size_t(d->n_dirs) * nm * S * S * sizeof(double));
+        if (pr->has_model && h == pr->model_hash) return H3G_OK;
         cudaStreamSynchronize(ctx->stream);
+        pr->has_model = false;
         pr->S = S; pr->M = d->M; pr->K = d->K; pr->nmod = nm; pr->ndirs = d->n_dirs; pr->has_bg = d->has_bg;
         pr->time_mode = d->time_mode; pr->sentinel = d->zero_l_sentinel;
-        const bool prec_change = pr->precision != d->precision;
+        if (pr->precision != d->precision) { pr->drop_graphs(); pr->work_mem.release(); pr->w = Work{}; }
         pr->precision = d->precision;
-        if (prec_change) { pr->work_mem.release(); pr->w = Work{}; }
         std::vector<double> pi(SP, 0.0), Q(size_t(nm) * SP2), U(size_t(nm) * SP2), V(size_t(nm) * SP2), lam(size_t(nm) * SP, 0.0);
         std::copy(d->pi, d->pi + S, pi.begin());
         for (int k = 0; k < nm; ++k) {
@@ -364,42 +420,48 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             for (int k = 0; k < nm; ++k) pad_matrix(d->dQ + (size_t(x) * nm + k) * S * S, S, &dQ[(size_t(x) * nm + k) * SP2]);
         std::vector<uint8_t> it(pr->n, 1);
         if (d->is_test) std::copy(d->is_test, d->is_test + pr->n, it.begin());
-        auto& A = pr->model_mem;
-        A.release();
-        Model md{};
-        double *dpi, *dQd, *dlam, *dU, *dV, *dmu, *dcw, *drt, *drw, *ddQ;
-        uint8_t* dit;
-        H3G_TRY_CUDA(ctx, A.alloc(&dpi, SP));
-        H3G_TRY_CUDA(ctx, A.alloc(&dQd, Q.size()));
-        H3G_TRY_CUDA(ctx, A.alloc(&dlam, lam.size()));
-        H3G_TRY_CUDA(ctx, A.alloc(&dU, U.size()));
-        H3G_TRY_CUDA(ctx, A.alloc(&dV, V.size()));
-        H3G_TRY_CUDA(ctx, A.alloc(&dmu, mu.size()));
-        H3G_TRY_CUDA(ctx, A.alloc(&dcw, d->K));
-        H3G_TRY_CUDA(ctx, A.alloc(&drt, d->M));
-        H3G_TRY_CUDA(ctx, A.alloc(&drw, d->M));
-        H3G_TRY_CUDA(ctx, A.alloc(&ddQ, dQ.size()));
-        H3G_TRY_CUDA(ctx, A.alloc(&dit, it.size()));
+        const size_t mkey[5] = {size_t(nm), size_t(d->K), size_t(d->M), size_t(std::max(d->n_dirs, 1)), size_t(pr->n)};
+        if (!pr->m_pi || !std::equal(mkey, mkey + 5, pr->model_key)) {
+            pr->drop_graphs();
+            auto& A = pr->model_mem;
+            A.release();
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_pi, SP));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_Q, Q.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_lam, lam.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_U, U.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_V, V.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_mu, mu.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_cw, d->K));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rt, d->M));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rw, d->M));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_dQ, dQ.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_it, it.size()));
+            std::copy(mkey, mkey + 5, pr->model_key);
+        }
         cudaStream_t s = ctx->stream;
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dpi, pi.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dQd, Q.data(), Q.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dlam, lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dU, U.data(), U.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dV, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dmu, mu.data(), mu.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dcw, d->class_w, d->K * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(drt, d->rates, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(drw, d->rate_w, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(ddQ, dQ.data(), dQ.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dit, it.data(), it.size(), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_pi, pi.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_Q, Q.data(), Q.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_lam, lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_U, U.data(), U.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_V, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_mu, mu.data(), mu.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_cw, d->class_w, d->K * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_rt, d->rates, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_rw, d->rate_w, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_dQ, dQ.data(), dQ.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_it, it.data(), it.size(), cudaMemcpyHostToDevice, s));
+        Model md{};
         md.M = d->M; md.K = d->K; md.has_bg = d->has_bg; md.nmod = nm; md.time_mode = d->time_mode; md.ndirs = d->n_dirs;
         md.sentinel = d->zero_l_sentinel;
-        md.pi = dpi; md.Q = dQd; md.lam = dlam; md.U = dU; md.V = dV; md.mu = dmu; md.class_w = dcw; md.rates = drt;
-        md.rate_w = drw; md.is_test = d->is_test ? dit : nullptr; md.dQ = ddQ;
+        md.pi = pr->m_pi; md.Q = pr->m_Q; md.lam = pr->m_lam; md.U = pr->m_U; md.V = pr->m_V; md.mu = pr->m_mu;
+        md.class_w = pr->m_cw; md.rates = pr->m_rt; md.rate_w = pr->m_rw; md.is_test = d->is_test ? pr->m_it : nullptr;
+        md.dQ = pr->m_dQ;
+        if (std::memcmp(&md, &pr->md, sizeof(Model)) != 0) pr->drop_graphs();
         pr->md = md;
         h3g_status st = ensure_workspace(pr, d->M, d->K, nm, d->n_dirs);
-        if (st != H3G_OK) { pr->has_model = false; return st; }
+        if (st != H3G_OK) return st;
         H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+        pr->model_hash = h;
         pr->has_model = true;
         return H3G_OK;
     } catch (const std::bad_alloc&) {
@@ -409,8 +471,16 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     }
 }
 
+// Stage boundaries for h3g_profile_stages (same order as H3G_STAGE_NAMES in h3g.h).
+enum Stage { ST_BUILD_P, ST_PREP_MIXED, ST_INSIDE, ST_ROOT, ST_OUTSIDE, ST_ACCUM_A, ST_FRECHET, ST_HSUM, ST_SMALL, ST_DIR, ST_COUNT };
+struct StageMarks {
+    cudaEvent_t ev[ST_COUNT + 1];
+    bool seen[ST_COUNT];
+    int launches[ST_COUNT];
+};
+
 // Enqueue the pruning pipeline (inside, root and optionally outside + gradients).
-static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P) {
+static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, StageMarks* mk = nullptr) {
     const Topo t = pr->topo();
     const Model& md = pr->md;
     const Work& w = pr->w;
@@ -419,77 +489,214 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P) {
     const bool grads = (want & (H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL)) != 0;
     const bool global = (want & H3G_WANT_GRAD_GLOBAL) != 0;
     int L = 0;
-    L += from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s);
-    if (mixed) L += mixed_prepare(t, md, w, pr->mw, s);
+    auto mark = [&](Stage st, int launched) {
+        L += launched;
+        if (mk && launched) { cudaEventRecord(mk->ev[st + 1], s); mk->seen[st] = true; mk->launches[st] += launched; }
+    };
+    if (mk) cudaEventRecord(mk->ev[0], s);
+    mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
+    if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, pr->mw, s));
+    int l = 0;
     for (size_t lv = 0; lv + 1 < pr->in_off.size(); ++lv) {
         const int cnt = pr->in_off[lv + 1] - pr->in_off[lv];
         if (!cnt) continue;
         const int* nodes = pr->d_in_nodes + pr->in_off[lv];
-        L += mixed ? launch_inside_mixed(t, md, w, pr->mw, nodes, cnt, s) : launch_inside_fp64(t, md, w, nodes, cnt, s);
+        l += mixed ? launch_inside_mixed(t, md, w, pr->mw, nodes, cnt, s) : launch_inside_fp64(t, md, w, nodes, cnt, s);
     }
-    L += mixed ? launch_root_mixed(t, md, w, pr->mw, s) : launch_root(t, md, w, s);
+    mark(ST_INSIDE, l);
+    mark(ST_ROOT, mixed ? launch_root_mixed(t, md, w, pr->mw, s) : launch_root(t, md, w, s));
     if (grads) {
+        l = 0;
         for (size_t lv = 0; lv + 1 < pr->out_off.size(); ++lv) {
             const int cnt = pr->out_off[lv + 1] - pr->out_off[lv];
             if (!cnt) continue;
             const int* nodes = pr->d_out_nodes + pr->out_off[lv];
-            L += mixed ? launch_outside_mixed(t, md, w, pr->mw, nodes, cnt, s) : launch_outside_fp64(t, md, w, nodes, cnt, 1, s);
+            l += mixed ? launch_outside_mixed(t, md, w, pr->mw, nodes, cnt, s) : launch_outside_fp64(t, md, w, nodes, cnt, 1, s);
         }
-        L += mixed ? launch_accumA_mixed(t, md, w, pr->mw, s) : launch_accumA_fp64(t, md, w, s);
-        L += launch_frechet(t, md, w, global ? 1 : 0, s);
-        if (global) L += launch_global(t, md, w, s);
+        mark(ST_OUTSIDE, l);
+        mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, pr->mw, s) : launch_accumA_fp64(t, md, w, s));
+        mark(ST_FRECHET, launch_frechet(t, md, w, global ? 1 : 0, s));
+        if (global) mark(ST_HSUM, launch_global(t, md, w, s));
     }
-    L += launch_small(t, md, w, grads ? 1 : 0, s);
-    if (global) L += launch_dir(t, md, w, s);
+    mark(ST_SMALL, launch_small(t, md, w, grads ? 1 : 0, s));
+    if (global) mark(ST_DIR, launch_dir(t, md, w, s));
     return L;
 }
 
-extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want, h3g_result* out) {
-    if (!pr || !bl || !out) return H3G_ERR_ARG;
-    h3g_ctx* ctx = pr->ctx;
-    if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "h3g_eval before h3g_model_set");
-    const int n = pr->n;
-    for (int i = 0; i < n; ++i)
-        if (i != pr->root && !std::isfinite(bl[i])) return fail(ctx, H3G_ERR_NUMERIC, "non-finite branch length");
-    cudaSetDevice(ctx->device);
-    cudaStream_t s = ctx->stream;
-    double* hbl = pr->h_pin;
-    double* hout = pr->h_pin + n;
-    std::copy(bl, bl + n, hbl);
-    hbl[pr->root] = 0.0;
-    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_bl, hbl, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    H3G_TRY_CUDA(ctx, cudaEventRecord(pr->ev0, s));
-    pr->last_launches = enqueue_eval(pr, want, false);
-    H3G_TRY_CUDA(ctx, cudaGetLastError());
-    H3G_TRY_CUDA(ctx, cudaEventRecord(pr->ev1, s));
-    const size_t n_out = 2 + n + pr->K + pr->nmod + pr->M;
-    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(hout, pr->w.out, n_out * sizeof(double), cudaMemcpyDeviceToHost, s));
-    std::vector<double> dirpart;
-    const bool global = (want & H3G_WANT_GRAD_GLOBAL) != 0;
-    if (global && pr->ndirs > 0) {
-        dirpart.resize(size_t(pr->ndirs) * pr->nmod);
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(dirpart.data(), pr->w.dirpart, dirpart.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+static unsigned norm_want(unsigned want) {
+    unsigned w = want & (H3G_WANT_SITE_LNL | H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL);
+    return w | H3G_WANT_LNL;
+}
+
+// Results the host reads back after an evaluation: the small output vector,
+// the directional partials and (optionally) the per-pattern lnL.
+static size_t enqueue_readback(h3g_problem* pr, unsigned want) {
+    cudaStream_t s = pr->ctx->stream;
+    size_t bytes = n_out_of(pr) * sizeof(double);
+    cudaMemcpyAsync(pr->h_pin + pr->off_out, pr->w.out, bytes, cudaMemcpyDeviceToHost, s);
+    if ((want & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) {
+        const size_t b = size_t(pr->ndirs) * pr->nmod * sizeof(double);
+        cudaMemcpyAsync(pr->h_pin + pr->off_dir, pr->w.dirpart, b, cudaMemcpyDeviceToHost, s);
+        bytes += b;
     }
-    if ((want & H3G_WANT_SITE_LNL) && out->site_lnl && pr->P > 0)
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(out->site_lnl, pr->w.site, pr->P * sizeof(double), cudaMemcpyDeviceToHost, s));
-    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
-    cudaEventElapsedTime(&pr->last_ms, pr->ev0, pr->ev1);
-    out->lnl = hout[0];
+    if ((want & H3G_WANT_SITE_LNL) && pr->P > 0) {
+        const size_t b = size_t(pr->P) * sizeof(double);
+        cudaMemcpyAsync(pr->h_pin + pr->off_site, pr->w.site, b, cudaMemcpyDeviceToHost, s);
+        bytes += b;
+    }
+    return bytes;
+}
+
+static bool graphs_enabled() {
+    static const bool on = [] { const char* e = std::getenv("H3G_NO_GRAPH"); return !(e && e[0] == '1'); }();
+    return on;
+}
+
+// Run one evaluation: as a captured CUDA graph (host copies included when
+// `copies`), instantiated once per (want, copies) and replayed afterwards.
+static h3g_status run_eval(h3g_problem* pr, unsigned want, bool copies) {
+    h3g_ctx* ctx = pr->ctx;
+    cudaStream_t s = ctx->stream;
+    const unsigned key = norm_want(want) | (copies ? 0x100u : 0u);
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : pr->graphs) if (g.key == key) { exec = g.exec; pr->last_launches = g.launches; }
+    if (!exec && graphs_enabled()) {
+        cudaGraph_t graph = nullptr;
+        H3G_TRY_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        if (copies) cudaMemcpyAsync(pr->d_bl, pr->h_pin, pr->n * sizeof(double), cudaMemcpyHostToDevice, s);
+        pr->last_launches = enqueue_eval(pr, key, false);
+        if (copies) enqueue_readback(pr, key);
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess) { ctx->err = std::string("graph capture: ") + cudaGetErrorString(e); return H3G_ERR_CUDA; }
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(e); return H3G_ERR_CUDA; }
+        pr->graphs.push_back({key, exec, pr->last_launches});
+    }
+    H3G_TRY_CUDA(ctx, cudaEventRecord(pr->ev0, s));
+    if (exec) {
+        H3G_TRY_CUDA(ctx, cudaGraphLaunch(exec, s));
+    } else {
+        if (copies) H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_bl, pr->h_pin, pr->n * sizeof(double), cudaMemcpyHostToDevice, s));
+        pr->last_launches = enqueue_eval(pr, key, false);
+        H3G_TRY_CUDA(ctx, cudaGetLastError());
+        if (copies) enqueue_readback(pr, key);
+    }
+    H3G_TRY_CUDA(ctx, cudaEventRecord(pr->ev1, s));
+    pr->last_h2d = copies ? pr->n * sizeof(double) : 0;
+    pr->last_d2h = 0;
+    if (copies) {
+        pr->last_d2h = n_out_of(pr) * sizeof(double);
+        if ((key & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) pr->last_d2h += size_t(pr->ndirs) * pr->nmod * sizeof(double);
+        if ((key & H3G_WANT_SITE_LNL) && pr->P > 0) pr->last_d2h += size_t(pr->P) * sizeof(double);
+    }
+    return H3G_OK;
+}
+
+static void unpack_result(h3g_problem* pr, unsigned want, h3g_result* out) {
+    const int n = pr->n;
+    const double* hout = pr->h_pin + pr->off_out;
     const bool grads = (want & (H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL)) != 0;
+    const bool global = (want & H3G_WANT_GRAD_GLOBAL) != 0;
+    out->lnl = hout[0];
     if (out->grad_t) {
         for (int b = 0; b < n; ++b) out->grad_t[b] = grads ? hout[2 + b] : 0.0;
         out->grad_t[pr->root] = 0.0;
     }
     if (out->grad_class_w) for (int k = 0; k < pr->K; ++k) out->grad_class_w[k] = global ? hout[2 + n + k] : 0.0;
     if (out->grad_rate_w) for (int m = 0; m < pr->M; ++m) out->grad_rate_w[m] = grads ? hout[2 + n + pr->K + pr->nmod + m] : 0.0;
-    if (out->grad_dir)
+    if (out->grad_dir) {
+        const double* dir = pr->h_pin + pr->off_dir;
         for (int x = 0; x < pr->ndirs; ++x) {
             double g = 0.0;
-            if (global) for (int k = 0; k < pr->nmod; ++k) g += dirpart[size_t(x) * pr->nmod + k];
+            if (global) for (int k = 0; k < pr->nmod; ++k) g += dir[size_t(x) * pr->nmod + k];
             out->grad_dir[x] = g;
         }
+    }
+    if ((want & H3G_WANT_SITE_LNL) && out->site_lnl && pr->P > 0)
+        std::copy(pr->h_pin + pr->off_site, pr->h_pin + pr->off_site + pr->P, out->site_lnl);
+}
+
+static h3g_status check_bl(h3g_problem* pr, const double* bl) {
+    for (int i = 0; i < pr->n; ++i)
+        if (i != pr->root && !std::isfinite(bl[i])) return fail(pr->ctx, H3G_ERR_NUMERIC, "non-finite branch length");
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want, h3g_result* out) {
+    if (!pr || !bl || !out) return H3G_ERR_ARG;
+    h3g_ctx* ctx = pr->ctx;
+    if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "h3g_eval before h3g_model_set");
+    if (h3g_status st = check_bl(pr, bl); st != H3G_OK) return st;
+    cudaSetDevice(ctx->device);
+    std::copy(bl, bl + pr->n, pr->h_pin);
+    pr->h_pin[pr->root] = 0.0;
+    if (h3g_status st = run_eval(pr, want, true); st != H3G_OK) return st;
+    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaEventElapsedTime(&pr->last_ms, pr->ev0, pr->ev1);
+    unpack_result(pr, norm_want(want), out);
     if (!std::isfinite(out->lnl)) return fail(ctx, H3G_ERR_NUMERIC, "non-finite log-likelihood");
     return H3G_OK;
+}
+
+extern "C" h3g_status h3g_stage_branch_lengths(h3g_problem* pr, const double* bl) {
+    if (!pr || !bl) return H3G_ERR_ARG;
+    h3g_ctx* ctx = pr->ctx;
+    if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "stage before h3g_model_set");
+    if (h3g_status st = check_bl(pr, bl); st != H3G_OK) return st;
+    cudaSetDevice(ctx->device);
+    std::copy(bl, bl + pr->n, pr->h_pin);
+    pr->h_pin[pr->root] = 0.0;
+    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_bl, pr->h_pin, pr->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_eval_resident(h3g_problem* pr, unsigned want) {
+    if (!pr) return H3G_ERR_ARG;
+    if (!pr->has_model) return fail(pr->ctx, H3G_ERR_STATE, "h3g_eval_resident before h3g_model_set");
+    cudaSetDevice(pr->ctx->device);
+    return run_eval(pr, want, false);
+}
+
+extern "C" h3g_status h3g_read_result(h3g_problem* pr, unsigned want, h3g_result* out) {
+    if (!pr || !out) return H3G_ERR_ARG;
+    h3g_ctx* ctx = pr->ctx;
+    if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "h3g_read_result before h3g_model_set");
+    cudaSetDevice(ctx->device);
+    enqueue_readback(pr, norm_want(want));
+    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unpack_result(pr, norm_want(want), out);
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_profile_stages(h3g_problem* pr, unsigned want, int reps, double* stage_ms, int* stage_launches) {
+    if (!pr || !stage_ms || reps < 1) return H3G_ERR_ARG;
+    h3g_ctx* ctx = pr->ctx;
+    if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "profile before h3g_model_set");
+    cudaSetDevice(ctx->device);
+    StageMarks mk{};
+    for (auto& e : mk.ev) H3G_TRY_CUDA(ctx, cudaEventCreate(&e));
+    std::fill(stage_ms, stage_ms + ST_COUNT, 0.0);
+    if (stage_launches) std::fill(stage_launches, stage_launches + ST_COUNT, 0);
+    h3g_status st = H3G_OK;
+    for (int r = 0; r < reps && st == H3G_OK; ++r) {
+        std::fill(mk.seen, mk.seen + ST_COUNT, false);
+        std::fill(mk.launches, mk.launches + ST_COUNT, 0);
+        enqueue_eval(pr, norm_want(want), false, &mk);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { st = fail(ctx, H3G_ERR_CUDA, "profile run failed"); break; }
+        cudaEvent_t prev = mk.ev[0];
+        for (int k = 0; k < ST_COUNT; ++k) {
+            if (!mk.seen[k]) continue;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, prev, mk.ev[k + 1]);
+            stage_ms[k] += ms / reps;
+            if (stage_launches && r == 0) stage_launches[k] = mk.launches[k];
+            prev = mk.ev[k + 1];
+        }
+    }
+    for (auto& e : mk.ev) cudaEventDestroy(e);
+    return st;
 }
 
 extern "C" h3g_status h3g_eval_from_P(h3g_problem* pr, int S, const double* P, const double* pi, double* lnl, double* site_lnl) {
@@ -513,13 +720,14 @@ extern "C" h3g_status h3g_eval_from_P(h3g_problem* pr, int S, const double* P, c
     pr->last_launches = enqueue_eval(pr, H3G_WANT_LNL, true);
     H3G_TRY_CUDA(ctx, cudaGetLastError());
     H3G_TRY_CUDA(ctx, cudaEventRecord(pr->ev1, s));
-    double* hout = pr->h_pin + n;
+    double* hout = pr->h_pin + pr->off_out;
     H3G_TRY_CUDA(ctx, cudaMemcpyAsync(hout, pr->w.out, sizeof(double), cudaMemcpyDeviceToHost, s));
     if (site_lnl && pr->P > 0)
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(site_lnl, pr->w.site, pr->P * sizeof(double), cudaMemcpyDeviceToHost, s));
     H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
     cudaEventElapsedTime(&pr->last_ms, pr->ev0, pr->ev1);
     pr->has_model = false;   // the installed model described caller P matrices only
+    pr->model_hash = 0;
     *lnl = hout[0];
     return H3G_OK;
 }
@@ -546,5 +754,12 @@ extern "C" h3g_status h3g_last_eval_stats(const h3g_problem* pr, double* device_
     if (!pr) return H3G_ERR_ARG;
     if (device_ms) *device_ms = pr->last_ms;
     if (n_launches) *n_launches = pr->last_launches;
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_last_eval_transfer(const h3g_problem* pr, size_t* h2d_bytes, size_t* d2h_bytes) {
+    if (!pr) return H3G_ERR_ARG;
+    if (h2d_bytes) *h2d_bytes = pr->last_h2d;
+    if (d2h_bytes) *d2h_bytes = pr->last_d2h;
     return H3G_OK;
 }

@@ -23,8 +23,10 @@ WANT_LNL, WANT_SITE_LNL, WANT_GRAD_T, WANT_GRAD_GLOBAL = 1, 2, 4, 8
 EXPORTED = [
     "h3g_ctx_create", "h3g_ctx_destroy", "h3g_last_error", "h3g_version", "h3g_problem_create",
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
-    "h3g_last_eval_stats",
+    "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
+    "h3g_read_result", "h3g_profile_stages",
 ]
+STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
 _dp = C.POINTER(C.c_double)
 
@@ -67,6 +69,11 @@ def load() -> C.CDLL:
         lib.h3g_eval_from_P.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp]
         lib.h3g_branch_length_gradients.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp]
         lib.h3g_last_eval_stats.argtypes = [vp, _dp, C.POINTER(C.c_int)]
+        lib.h3g_last_eval_transfer.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+        lib.h3g_stage_branch_lengths.argtypes = [vp, _dp]
+        lib.h3g_eval_resident.argtypes = [vp, C.c_uint]
+        lib.h3g_read_result.argtypes = [vp, C.c_uint, C.POINTER(Result)]
+        lib.h3g_profile_stages.argtypes = [vp, C.c_uint, C.c_int, _dp, C.POINTER(C.c_int)]
         for name in EXPORTED:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         lib.h3g_version.restype = C.c_char_p
@@ -191,6 +198,40 @@ class Problem:
         self.ctx.check(self.ctx.lib.h3g_branch_length_gradients(
             self.h, int(pi.size), _ptr(pi), _ptr(Q), _ptr(lam), _ptr(U), _ptr(V), _ptr(bl), precision, C.byref(lnl), _ptr(g)))
         return lnl.value, g
+
+    def _result_struct(self, out):
+        return Result(site_lnl=_ptr(out["site_lnl"]), grad_t=_ptr(out["grad_t"]), grad_dir=_ptr(out["grad_dir"]),
+                      grad_class_w=_ptr(out["grad_class_w"]), grad_rate_w=_ptr(out["grad_rate_w"]))
+
+    def empty_result(self) -> dict:
+        return {"site_lnl": np.zeros(self.P), "grad_t": np.zeros(self.n), "grad_dir": np.zeros(max(self.ndirs, 1)),
+                "grad_class_w": np.zeros(self.K), "grad_rate_w": np.zeros(self.M)}
+
+    def stage_branch_lengths(self, bl) -> None:
+        bl = _f64(bl)
+        self.ctx.check(self.ctx.lib.h3g_stage_branch_lengths(self.h, _ptr(bl)))
+
+    def eval_resident(self, want=WANT_LNL | WANT_GRAD_T) -> None:
+        """Enqueue one evaluation on the context stream (inputs already on the device); returns at once."""
+        self.ctx.check(self.ctx.lib.h3g_eval_resident(self.h, want))
+
+    def read_result(self, want=WANT_LNL | WANT_GRAD_T, out=None) -> dict:
+        out = out or self.empty_result()
+        r = self._result_struct(out)
+        self.ctx.check(self.ctx.lib.h3g_read_result(self.h, want, C.byref(r)))
+        out["lnl"] = r.lnl
+        return out
+
+    def profile_stages(self, want=WANT_LNL | WANT_GRAD_T, reps=5) -> dict:
+        ms = np.zeros(len(STAGE_NAMES))
+        nl = (C.c_int * len(STAGE_NAMES))()
+        self.ctx.check(self.ctx.lib.h3g_profile_stages(self.h, want, reps, _ptr(ms), nl))
+        return {name: (float(ms[i]), int(nl[i])) for i, name in enumerate(STAGE_NAMES) if nl[i] > 0}
+
+    def last_transfer(self) -> tuple[int, int]:
+        a, b = C.c_size_t(), C.c_size_t()
+        self.ctx.check(self.ctx.lib.h3g_last_eval_transfer(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def last_stats(self) -> tuple[float, int]:
         ms = C.c_double()

@@ -140,9 +140,28 @@ h3g_status h3g_branch_length_gradients(h3g_problem* prob, int S, const double* p
                                        const double* U, const double* V, const double* bl, int precision,
                                        double* lnl, double* grad);
 
-/* Device time of the last h3g_eval's kernels in milliseconds (CUDA events on
- * the context stream), and the number of kernel launches it made. */
+/* Device time of the last evaluation in milliseconds (CUDA events on the
+ * context stream around the launch sequence, host copies included for
+ * h3g_eval), and the number of kernel launches it made. */
 h3g_status h3g_last_eval_stats(const h3g_problem* prob, double* device_ms, int* n_launches);
+
+/* Bytes the last evaluation copied host->device and device->host. */
+h3g_status h3g_last_eval_transfer(const h3g_problem* prob, size_t* h2d_bytes, size_t* d2h_bytes);
+
+/* Device-resident evaluation, for callers that keep inputs and results on the
+ * GPU: h3g_stage_branch_lengths copies bl[n_nodes] to the device (blocking);
+ * h3g_eval_resident enqueues one evaluation on the context stream and returns
+ * without waiting; h3g_read_result waits for it and copies the results out. */
+h3g_status h3g_stage_branch_lengths(h3g_problem* prob, const double* bl);
+h3g_status h3g_eval_resident(h3g_problem* prob, unsigned want);
+h3g_status h3g_read_result(h3g_problem* prob, unsigned want, h3g_result* out);
+
+/* Per-stage device time of one evaluation (mean over reps runs, events between
+ * stages, no graph): stage_ms[H3G_N_STAGES], stage_launches[H3G_N_STAGES] (may
+ * be NULL).  Stage order: H3G_STAGE_NAMES. */
+#define H3G_N_STAGES 10
+#define H3G_STAGE_NAMES "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir"
+h3g_status h3g_profile_stages(h3g_problem* prob, unsigned want, int reps, double* stage_ms, int* stage_launches);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,7 @@
 #pragma once
 
 #include <cstdlib>
+#include <cstring>
 #include <list>
 #include <memory>
 #include <stdexcept>
@@ -47,9 +48,17 @@ struct MixtureGradients {
 
 namespace gpu_detail {
 
+// Content fingerprint, 8 bytes per step (multiply / xor-shift mixing).
 inline uint64_t fnv(uint64_t h, const void* p, size_t n) {
     const unsigned char* c = static_cast<const unsigned char*>(p);
-    for (size_t i = 0; i < n; ++i) { h ^= c[i]; h *= 1099511628211ull; }
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, c + i, 8);
+        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+    }
+    for (; i < n; ++i) { h ^= c[i]; h *= 1099511628211ull; }
     return h;
 }
 
@@ -152,7 +161,7 @@ public:
             }
         h3g_problem* pr = nullptr;
         check(h3g_problem_create(ctx(), n, parent.data(), leaf.data(), taxon.data(), T, P, st.data(), mk.data(), w.data(), &pr));
-        problems_.push_front({h, n, P, pr});
+        problems_.push_front({h, n, P, pr, 0});
         if (problems_.size() > 4) { h3g_problem_destroy(problems_.back().prob); problems_.pop_back(); }
         return pr;
     }
@@ -172,8 +181,17 @@ public:
         return models_.front().second;
     }
 
+    // key of the mixture model last installed on a problem by compute_mixture_gradients
+    uint64_t installed(h3g_problem* pr) const {
+        for (auto& e : problems_) if (e.prob == pr) return e.model_key;
+        return 0;
+    }
+    void set_installed(h3g_problem* pr, uint64_t k) {
+        for (auto& e : problems_) if (e.prob == pr) e.model_key = k;
+    }
+
 private:
-    struct Entry { uint64_t key; int n, P; h3g_problem* prob; };
+    struct Entry { uint64_t key; int n, P; h3g_problem* prob; uint64_t model_key = 0; };
     h3g_ctx* ctx_ = nullptr;
     std::list<Entry> problems_;
     std::list<std::pair<uint64_t, MG94Matrix>> models_;
@@ -230,6 +248,7 @@ public:
         auto bl = gpu_detail::node_lengths(tree, branch_lengths);
         std::vector<Scalar> grad(tree.num_nodes(), 0.0);
         double lnl = 0.0;
+        eng.set_installed(pr, 0);
         eng.check(h3g_branch_length_gradients(pr, mg.S, aln.codon_frequencies_f3x4.data(), mg.Q.data(), mg.eigenvalues.data(),
                                               mg.U_pi.data(), mg.V_pi.data(), bl.data(), int(get_precision()), &lnl, grad.data()));
         return {lnl, grad};
@@ -275,6 +294,7 @@ public:
         d.K = 1; d.class_w = &one; d.has_bg = part ? 1 : 0; d.is_test = part ? it.data() : nullptr;
         d.M = 1; d.rates = &one; d.rate_w = &one; d.time_mode = H3G_TIME_NORMALIZED;
         d.n_dirs = int(dirs.size()); d.dQ = mp.dQ.data(); d.precision = int(get_precision()); d.zero_l_sentinel = 0;
+        eng.set_installed(pr, 0);
         eng.check(h3g_model_set(pr, &d));
         auto bl = gpu_detail::node_lengths(tree, branch_lengths);
         JointMG94Gradients res;
@@ -323,10 +343,21 @@ public:
         std::vector<MG94Parameters> ps;
         for (int k = 0; k < K; ++k) { MG94Parameters p = base; p.alpha = 1.0; p.beta = omegas[size_t(k)]; ps.push_back(p); }
         if (has_bg) { MG94Parameters p = base; p.alpha = 1.0; p.beta = omega_bg; ps.push_back(p); }
-        for (auto& p : ps) mp.add(eng.model(p, aln));
         const int nm = int(ps.size());
         const size_t SS = size_t(S) * S;
         int ndirs = 0;
+        uint64_t key = 0x51ED270B27A4F1C3ull;
+        key = gpu_detail::fnv(key, &base, sizeof(base));
+        key = gpu_detail::fnv(key, omegas.data(), omegas.size() * 8);
+        key = gpu_detail::fnv(key, weights.data(), weights.size() * 8);
+        key = gpu_detail::fnv(key, syn_rates.data(), syn_rates.size() * 8);
+        key = gpu_detail::fnv(key, syn_weights.data(), syn_weights.size() * 8);
+        key = gpu_detail::fnv(key, it.data(), it.size());
+        const double flags[4] = {omega_bg, double(want_gradients), double(zero_likelihood_sentinel), double(get_precision())};
+        key = gpu_detail::fnv(key, flags, sizeof(flags));
+        const int n_dirs_expected = want_gradients ? K + (has_bg ? 1 : 0) + 5 : 0;
+        if (eng.installed(pr) != key) {
+        for (auto& p : ps) mp.add(eng.model(p, aln));
         auto add_dir = [&](int only_model, const std::vector<std::vector<double>>& per_model) {
             for (int k = 0; k < nm; ++k) {
                 if (only_model >= 0 && k != only_model) mp.dQ.insert(mp.dQ.end(), SS, 0.0);
@@ -354,6 +385,9 @@ public:
         d.n_dirs = ndirs; d.dQ = ndirs ? mp.dQ.data() : nullptr; d.precision = int(get_precision());
         d.zero_l_sentinel = zero_likelihood_sentinel ? 1 : 0;
         eng.check(h3g_model_set(pr, &d));
+        eng.set_installed(pr, key);
+        }
+        ndirs = n_dirs_expected;
         auto bl = gpu_detail::node_lengths(tree, branch_lengths);
         MixtureGradients res;
         res.grad_branches.assign(n, 0.0);
@@ -397,6 +431,7 @@ public:
         }
         double lnl = 0.0;
         if (site_log_likelihoods) site_log_likelihoods->assign(aln.patterns.size(), 0.0);
+        eng.set_installed(pr, 0);
         eng.check(h3g_eval_from_P(pr, S, P.data(), pi.data(), &lnl, site_log_likelihoods ? site_log_likelihoods->data() : nullptr));
         return lnl;
     }
