@@ -24,7 +24,7 @@ EXPORTED = [
     "h3g_ctx_create", "h3g_ctx_destroy", "h3g_last_error", "h3g_version", "h3g_problem_create",
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
-    "h3g_read_result", "h3g_profile_stages",
+    "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -74,6 +74,9 @@ def load() -> C.CDLL:
         lib.h3g_eval_resident.argtypes = [vp, C.c_uint]
         lib.h3g_read_result.argtypes = [vp, C.c_uint, C.POINTER(Result)]
         lib.h3g_profile_stages.argtypes = [vp, C.c_uint, C.c_int, _dp, C.POINTER(C.c_int)]
+        lib.h3g_eval_from_P_noalloc.argtypes = [C.c_int, vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_uint8),
+                                                C.POINTER(C.c_int32), C.c_int, C.c_int, C.POINTER(C.c_int8),
+                                                C.POINTER(C.c_uint64), _dp, C.c_int, _dp, _dp, _dp, _dp]
         for name in EXPORTED:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         lib.h3g_version.restype = C.c_char_p
@@ -238,3 +241,32 @@ class Problem:
         nl = C.c_int()
         self.ctx.check(self.ctx.lib.h3g_last_eval_stats(self.h, C.byref(ms), C.byref(nl)))
         return ms.value, nl.value
+
+
+def eval_from_P_noalloc(parent, is_leaf, leaf_taxon, states, masks, weights, P, pi, device: int = 0,
+                        stream: int | None = None) -> tuple[float, np.ndarray]:
+    """h3g_eval_from_P_noalloc: lnL from given transition matrices with no device allocation.
+
+    For callers that may not allocate device memory while running; the library
+    uses its fixed 32 MiB per-device scratch array instead.  Raises H3GError
+    with the status code (H3G_ERR_ARG when the problem is larger than that).
+    """
+    lib = load()
+    parent = np.ascontiguousarray(parent, dtype=np.int32)
+    is_leaf = np.ascontiguousarray(is_leaf, dtype=np.uint8)
+    leaf_taxon = np.ascontiguousarray(leaf_taxon, dtype=np.int32)
+    states = np.ascontiguousarray(states, dtype=np.int8)
+    masks = np.ascontiguousarray(masks, dtype=np.uint64)
+    weights = _f64(weights)
+    P = _f64(P)
+    pi = _f64(pi)
+    nP, T = states.shape
+    lnl = C.c_double()
+    site = np.zeros(nP)
+    st = lib.h3g_eval_from_P_noalloc(device, C.c_void_p(stream) if stream else None, int(parent.size),
+                                     _ptr(parent, C.c_int32), _ptr(is_leaf, C.c_uint8), _ptr(leaf_taxon, C.c_int32),
+                                     T, nP, _ptr(states, C.c_int8), _ptr(masks, C.c_uint64), _ptr(weights),
+                                     int(pi.size), _ptr(P), _ptr(pi), C.byref(lnl), _ptr(site))
+    if st != H3G_OK:
+        raise H3GError(f"h3g_eval_from_P_noalloc failed with status {st}")
+    return lnl.value, site

@@ -163,6 +163,25 @@ h3g_status h3g_read_result(h3g_problem* prob, unsigned want, h3g_result* out);
 #define H3G_STAGE_NAMES "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir"
 h3g_status h3g_profile_stages(h3g_problem* prob, unsigned want, int reps, double* stage_ms, int* stage_launches);
 
+/* Log-likelihood from caller-supplied transition matrices without allocating
+ * any device memory.  No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc while they run, such as code embedded in a
+ * process whose framework already owns the whole device memory pool, or code
+ * that must not add allocation-driven synchronisation to a latency path.
+ * Same inputs, outputs and results as h3g_eval_from_P, but no context or
+ * problem handle: the topology, patterns, matrices P[n_nodes * S * S] and pi[S]
+ * are host arrays, lnl and site_lnl (NULL allowed) host outputs, the work runs
+ * on cuda_stream (NULL = the legacy default stream) of `device`.
+ * All intermediates live in one 32 MiB __device__ array that every GPU loading
+ * the library holds until exit; problems needing more (or n_nodes > 1024) are
+ * rejected with H3G_ERR_ARG before any work is launched.  The first call on a
+ * device resolves the array's address and should come before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race. */
+h3g_status h3g_eval_from_P_noalloc(int device, void* cuda_stream, int n_nodes, const int32_t* parent,
+                                   const uint8_t* is_leaf, const int32_t* leaf_taxon, int n_taxa, int n_patterns,
+                                   const int8_t* states, const uint64_t* masks, const double* weights, int S,
+                                   const double* P, const double* pi, double* lnl, double* site_lnl);
+
 #ifdef __cplusplus
 }
 #endif
