@@ -386,7 +386,7 @@ def run_ours(args) -> None:
 
 
 def _mixed_available() -> bool:
-    return os.environ.get("H3G_BENCH_PRECISION", "") == "mixed"
+    return os.environ.get("H3G_BENCH_PRECISION", "mixed") == "mixed"
 
 
 def _directions(aln, wl, es):

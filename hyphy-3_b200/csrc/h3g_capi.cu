@@ -20,6 +20,7 @@ struct h3g_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    int live_problems = 0;
     std::string err;
 };
 
@@ -44,10 +45,11 @@ struct DevArena {
 struct h3g_problem {
     h3g_ctx* ctx = nullptr;
     int n = 0, root = -1, T = 0, P = 0, Pp = 0, NI = 0, max_state = -1;
-    std::vector<int> ch_off, ch, iidx, taxon, in_off, out_off, in_nodes, out_nodes;
+    std::vector<int> ch_off, ch, iidx, taxon, in_off, out_off, in_nodes, out_nodes, parent_h;
     std::vector<uint8_t> leaf;
     DevArena topo_mem, model_mem, work_mem;
     int *d_ch_off = nullptr, *d_ch = nullptr, *d_iidx = nullptr, *d_taxon = nullptr, *d_in_nodes = nullptr, *d_out_nodes = nullptr;
+    int* d_parent = nullptr;
     uint8_t* d_leaf = nullptr;
     int8_t* d_states = nullptr;
     uint64_t* d_masks = nullptr;
@@ -91,7 +93,7 @@ struct h3g_problem {
     Topo topo() const {
         Topo t;
         t.n = n; t.root = root; t.NI = NI; t.T = T; t.P = P; t.Pp = Pp; t.S = S;
-        t.ch_off = d_ch_off; t.ch = d_ch; t.iidx = d_iidx; t.leaf = d_leaf; t.taxon = d_taxon;
+        t.ch_off = d_ch_off; t.ch = d_ch; t.parent = d_parent; t.iidx = d_iidx; t.leaf = d_leaf; t.taxon = d_taxon;
         t.states = d_states; t.masks = d_masks; t.w = d_w;
         t.all_mask = S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1);
         return t;
@@ -140,6 +142,7 @@ extern "C" h3g_status h3g_ctx_create(int device, void* cuda_stream, h3g_ctx** ou
 
 extern "C" h3g_status h3g_ctx_destroy(h3g_ctx* ctx) {
     if (!ctx) return H3G_ERR_ARG;
+    if (ctx->live_problems > 0) return fail(ctx, H3G_ERR_STATE, "destroy every problem before its context");
     cudaSetDevice(ctx->device);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -214,11 +217,14 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
             for (int i = 0; i < n; ++i) if (!is_leaf[i] && height[i] == h) pr->in_nodes.push_back(i);
             pr->in_off.push_back(int(pr->in_nodes.size()));
         }
+        // outside levels: the children of the internal nodes at each depth
         pr->out_off.assign(1, 0);
         for (int d = 0; d <= Dp; ++d) {
-            for (int i = 0; i < n; ++i) if (!is_leaf[i] && depth[i] == d) pr->out_nodes.push_back(i);
+            for (int i = 0; i < n; ++i)
+                if (!is_leaf[i] && depth[i] == d) for (int c : kids[i]) pr->out_nodes.push_back(c);
             pr->out_off.push_back(int(pr->out_nodes.size()));
         }
+        pr->parent_h.assign(parent, parent + n);
         // patterns, taxon-major with padding (missing data, weight 0)
         const int Pp = pr->Pp, T = n_taxa;
         std::vector<int8_t> st(size_t(std::max(T, 1)) * Pp, int8_t(-1));
@@ -240,6 +246,7 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ch_off, n + 1));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ch, std::max<size_t>(pr->ch.size(), 1)));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_iidx, n));
+        H3G_TRY_CUDA(ctx, A.alloc(&pr->d_parent, n));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_taxon, n));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_leaf, n));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_in_nodes, std::max<size_t>(pr->in_nodes.size(), 1)));
@@ -250,6 +257,7 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ch_off, pr->ch_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
         if (!pr->ch.empty()) H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ch, pr->ch.data(), pr->ch.size() * sizeof(int), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_iidx, pr->iidx.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_parent, pr->parent_h.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_taxon, pr->taxon.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_leaf, pr->leaf.data(), n, cudaMemcpyHostToDevice, s));
         if (!pr->in_nodes.empty())
@@ -263,6 +271,7 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
         H3G_TRY_CUDA(ctx, cudaEventCreate(&pr->ev0));
         H3G_TRY_CUDA(ctx, cudaEventCreate(&pr->ev1));
         *out = guard.release();
+        ctx->live_problems++;
         return H3G_OK;
     } catch (const std::bad_alloc&) {
         return fail(ctx, H3G_ERR_OOM, "host allocation failed");
@@ -275,6 +284,7 @@ extern "C" h3g_status h3g_problem_destroy(h3g_problem* prob) {
     if (!prob) return H3G_ERR_ARG;
     cudaSetDevice(prob->ctx->device);
     cudaStreamSynchronize(prob->ctx->stream);
+    prob->ctx->live_problems--;
     delete prob;
     return H3G_OK;
 }
@@ -326,9 +336,11 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * n));
     H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * n));
     H3G_TRY_CUDA(ctx, A.alloc(&w.H, size_t(nmod) * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 4));
     const size_t n_out = 2 + n + K + nmod + M;
     H3G_TRY_CUDA(ctx, A.alloc(&w.out, n_out));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.err, 1));
+    cudaMemsetAsync(w.err, 0, sizeof(int), ctx->stream);
     if (pr->precision == H3G_PREC_FP64) {
         H3G_TRY_CUDA(ctx, A.alloc(&w.D, NI * M * SP * Pp));
         H3G_TRY_CUDA(ctx, A.alloc(&w.Ms, NI * M * SP * Pp));
@@ -343,7 +355,7 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     cudaMemsetAsync(w.Hpart, 0, size_t(nmod) * M * n * SP2 * sizeof(double), ctx->stream);
     pr->off_out = n;
     pr->off_dir = pr->off_out + n_out;
-    pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod;
+    pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod * 4;
     pr->h_pin_count = pr->off_site + size_t(std::max(pr->P, 1));
     H3G_TRY_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&pr->h_pin), pr->h_pin_count * sizeof(double)));
     return H3G_OK;
@@ -535,7 +547,7 @@ static size_t enqueue_readback(h3g_problem* pr, unsigned want) {
     size_t bytes = n_out_of(pr) * sizeof(double);
     cudaMemcpyAsync(pr->h_pin + pr->off_out, pr->w.out, bytes, cudaMemcpyDeviceToHost, s);
     if ((want & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) {
-        const size_t b = size_t(pr->ndirs) * pr->nmod * sizeof(double);
+        const size_t b = size_t(pr->ndirs) * pr->nmod * 4 * sizeof(double);
         cudaMemcpyAsync(pr->h_pin + pr->off_dir, pr->w.dirpart, b, cudaMemcpyDeviceToHost, s);
         bytes += b;
     }
@@ -587,7 +599,7 @@ static h3g_status run_eval(h3g_problem* pr, unsigned want, bool copies) {
     pr->last_d2h = 0;
     if (copies) {
         pr->last_d2h = n_out_of(pr) * sizeof(double);
-        if ((key & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) pr->last_d2h += size_t(pr->ndirs) * pr->nmod * sizeof(double);
+        if ((key & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) pr->last_d2h += size_t(pr->ndirs) * pr->nmod * 4 * sizeof(double);
         if ((key & H3G_WANT_SITE_LNL) && pr->P > 0) pr->last_d2h += size_t(pr->P) * sizeof(double);
     }
     return H3G_OK;
@@ -609,7 +621,9 @@ static void unpack_result(h3g_problem* pr, unsigned want, h3g_result* out) {
         const double* dir = pr->h_pin + pr->off_dir;
         for (int x = 0; x < pr->ndirs; ++x) {
             double g = 0.0;
-            if (global) for (int k = 0; k < pr->nmod; ++k) g += dir[size_t(x) * pr->nmod + k];
+            if (global)
+                for (int k = 0; k < pr->nmod; ++k)
+                    for (int rb = 0; rb < 4; ++rb) g += dir[(size_t(x) * pr->nmod + k) * 4 + rb];
             out->grad_dir[x] = g;
         }
     }
@@ -635,6 +649,7 @@ extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want,
     H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     cudaEventElapsedTime(&pr->last_ms, pr->ev0, pr->ev1);
     unpack_result(pr, norm_want(want), out);
+    if (pr->h_pin[pr->off_out + 1] != 0.0) return fail(ctx, H3G_ERR_TIMEOUT, "a bounded tensor-core wait expired on the device");
     if (!std::isfinite(out->lnl)) return fail(ctx, H3G_ERR_NUMERIC, "non-finite log-likelihood");
     return H3G_OK;
 }

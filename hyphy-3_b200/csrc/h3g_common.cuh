@@ -23,14 +23,14 @@ namespace h3g {
 
 constexpr int SP = 64;       // padded state count (61 sense codons -> 64)
 constexpr int SP2 = SP * SP; // one padded matrix
-constexpr int TP = 64;       // patterns per CTA in the pruning kernels (one thread per pattern)
-constexpr int kRescaleBits = 256;  // rescale a partial when its max falls below 2^-256
+constexpr int TP = 128;      // pattern padding granule (the mixed path's CTA tile)
 constexpr int kMaxRateClasses = 16;
 
 struct Topo {
     int n, root, NI, T, P, Pp, S;
     const int* ch_off;       // [n+1] children CSR, children in increasing id order
     const int* ch;
+    const int* parent;       // [n] parent id, -1 at the root
     const int* iidx;         // [n] internal-node slot, -1 for leaves
     const uint8_t* leaf;     // [n]
     const int* taxon;        // [n] alignment row of a leaf, -1 = missing
@@ -78,8 +78,9 @@ struct Work {
     double* gc;              // [K][M][n] <A_{m,b}, P_k(tau)>
     double* stg;             // [nmod][M][n] c_k * tau * <A_{m,b}, Q_k P_k(tau)>
     double* H;               // [nmod][64*64]
-    double* dirpart;         // [ndirs][nmod]
-    double* out;             // [2 + n + K + nmod + M] lnl | pad | grad_t | gc | stg | grad_rate_w
+    double* dirpart;         // [ndirs][nmod][4] row-block partials
+    double* out;             // [2 + n + K + nmod + M] lnl | error flag | grad_t | gc | stg | grad_rate_w
+    int* err;                // sticky device error flags (bounded waits that expired)
 };
 
 __device__ __forceinline__ size_t mat_off(int m, int b, int n) { return (size_t(m) * n + b) * SP2; }

@@ -83,71 +83,74 @@ __device__ __forceinline__ void stage_matrix(double* __restrict__ s, const doubl
 }
 
 // ------------------------------------------------------------------ build P
-// grid (n, M), block 256: each thread owns 16 entries (row r, columns c0..c0+15).
+// grid (n, M, 4): CTA z owns columns [16z, 16z+16) of P_{m,b} and dP_{m,b}.
+// Each of the 256 threads owns 4 entries (row r, columns c0..c0+3).
 __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
-    extern __shared__ double sm[];
-    double* sA = sm;            // U_k, later P_k
-    double* sB = sm + SP2;      // V_k, later Q_k
+    extern __shared__ __align__(16) double sm[];
+    double* sU = sm;                 // U_k (64 x 64), later Q_k
+    double* sV = sm + SP2;           // V_k columns of this block (64 x 16)
+    double* sPk = sV + SP * 16;      // clamp(P_k) columns of this block (64 x 16)
     __shared__ double se[SP];
-    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
+    const int b = blockIdx.x, m = blockIdx.y, cb = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
-    const int r = tid >> 2, c0 = (tid & 3) * 16;
+    const int r = tid >> 2, c0 = (tid & 3) * 4;       // local columns c0..c0+3 of the block
+    const int col0 = cb * 16;
     const bool test = md.is_test == nullptr || md.is_test[b] != 0;
     const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
-    double accP[16], accD[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) accP[q] = accD[q] = 0.0;
+    double accP[4] = {0, 0, 0, 0}, accD[4] = {0, 0, 0, 0};
     for (int k = k0; k < k1; ++k) {
         const double cw = test ? md.class_w[k] : 1.0;
         const double cv = time_conv(md, k);
         const double rate = md.rates[m];
         const double tau = rate * w.bl[b] * cv;
         __syncthreads();
-        stage_matrix(sA, md.U + size_t(k) * SP2, tid, 256);
-        stage_matrix(sB, md.V + size_t(k) * SP2, tid, 256);
+        stage_matrix(sU, md.U + size_t(k) * SP2, tid, 256);
+        for (int e = tid; e < SP * 16; e += 256) sV[e] = md.V[size_t(k) * SP2 + (e >> 4) * SP + col0 + (e & 15)];
         if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
         __syncthreads();
-        double pk[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) pk[q] = 0.0;
+        double pk[4] = {0, 0, 0, 0};
         for (int l = 0; l < SP; ++l) {
-            const double u = sA[r * SP + l] * se[l];
+            const double u = sU[r * SP + l] * se[l];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) pk[q] = fma(u, sB[l * SP + c0 + q], pk[q]);
+            for (int q = 0; q < 4; ++q) pk[q] = fma(u, sV[l * 16 + c0 + q], pk[q]);
         }
 #pragma unroll
-        for (int q = 0; q < 16; ++q) pk[q] = fmax(pk[q], 0.0);
+        for (int q = 0; q < 4; ++q) pk[q] = fmax(pk[q], 0.0);
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < 16; ++q) sA[r * SP + c0 + q] = pk[q];
-        stage_matrix(sB, md.Q + size_t(k) * SP2, tid, 256);
+        for (int q = 0; q < 4; ++q) sPk[r * 16 + c0 + q] = pk[q];
+        stage_matrix(sU, md.Q + size_t(k) * SP2, tid, 256);
         __syncthreads();
-        double qp[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) qp[q] = 0.0;
+        double qp[4] = {0, 0, 0, 0};
         for (int l = 0; l < SP; ++l) {
-            const double qq = sB[r * SP + l];
+            const double qq = sU[r * SP + l];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) qp[q] = fma(qq, sA[l * SP + c0 + q], qp[q]);
+            for (int q = 0; q < 4; ++q) qp[q] = fma(qq, sPk[l * 16 + c0 + q], qp[q]);
         }
         const double sc = cw * rate * cv;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) { accP[q] = fma(cw, pk[q], accP[q]); accD[q] = fma(sc, qp[q], accD[q]); }
+        for (int q = 0; q < 4; ++q) { accP[q] = fma(cw, pk[q], accP[q]); accD[q] = fma(sc, qp[q], accD[q]); }
     }
     double* P = w.P + mat_off(m, b, t.n);
     double* PT = w.PT + mat_off(m, b, t.n);
     double* dP = w.dP + mat_off(m, b, t.n);
-    double rsum = 0.0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        P[r * SP + c0 + q] = accP[q];
-        PT[(c0 + q) * SP + r] = accP[q];
-        dP[r * SP + c0 + q] = accD[q];
-        rsum += accP[q];
+    for (int q = 0; q < 4; ++q) {
+        const int c = col0 + c0 + q;
+        P[r * SP + c] = accP[q];
+        PT[c * SP + r] = accP[q];
+        dP[r * SP + c] = accD[q];
     }
-    rsum += __shfl_xor_sync(0xffffffffu, rsum, 1);
-    rsum += __shfl_xor_sync(0xffffffffu, rsum, 2);
-    if ((tid & 3) == 0) w.rs[(size_t(m) * t.n + b) * SP + r] = rsum;
+}
+
+// Row sums of P_{m,b} (the message of a leaf with missing data).  grid (n, M), block 64.
+__global__ void k_rowsum(Topo t, Model md, Work w) {
+    const int b = blockIdx.x, m = blockIdx.y, r = threadIdx.x;
+    if (b == t.root) return;
+    const double* P = w.P + mat_off(m, b, t.n) + r * SP;
+    double s = 0.0;
+    for (int j = 0; j < SP; ++j) s += P[j];
+    w.rs[(size_t(m) * t.n + b) * SP + r] = s;
 }
 
 // Caller-supplied P (compute_tree_log_likelihood_from_P): derive PT and row sums.
@@ -165,42 +168,120 @@ __global__ void k_prep_given_P(Topo t, Work w) {
 }
 
 // ------------------------------------------------------------------- inside
-// grid (Pp/TP, nodes in level, M), block TP.
-__global__ void __launch_bounds__(TP) k_inside(Topo t, Model md, Work w, const int* __restrict__ nodes) {
-    __shared__ __align__(16) double sP[SP2];
+// CTA = 8 warps x 32 patterns; warp g owns states [8g, 8g+8) of its 32 patterns
+// (lane = pattern), so every global access of a partial is a coalesced 256-byte row.
+constexpr int kTileP = 32;      // patterns per CTA in the FP64 pruning kernels
+constexpr int kGroups = 8;      // state groups (warps) per CTA
+
+// v[q] *= message of leaf child c for states [8g, 8g+8) of pattern p.
+__device__ __forceinline__ void mul_leaf8(double (&v)[8], const Topo& t, const Work& w, int m, int c, int p, int g) {
+    const int tx = t.taxon[c];
+    const double* PTc = w.PT + mat_off(m, c, t.n);
+    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
+    const double* src;
+    if (st >= 0) {
+        src = PTc + st * SP + 8 * g;
+    } else {
+        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * t.Pp + p];
+        if (mk == 0 || (mk & t.all_mask) == t.all_mask) {
+            src = w.rs + (size_t(m) * t.n + c) * SP + 8 * g;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                double s = 0.0;
+                for (uint64_t b = mk; b; b &= b - 1) s += __ldg(PTc + (__ffsll((long long)b) - 1) * SP + 8 * g + q);
+                v[q] *= s;
+            }
+            return;
+        }
+    }
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { const double2 x = __ldg(s2 + q); v[2 * q] *= x.x; v[2 * q + 1] *= x.y; }
+}
+
+// Power-of-two renormalisation of a 64-state column spread over the 8 warps:
+// returns the shift applied (same on every warp of a lane).
+__device__ __forceinline__ int renorm_cols(double (&v)[8], double* smax, int g, int lane) {
+    double mx = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) mx = fmax(mx, v[q]);
+    smax[g * kTileP + lane] = mx;
+    __syncthreads();
+    double all = 0.0;
+#pragma unroll
+    for (int k = 0; k < kGroups; ++k) all = fmax(all, smax[k * kTileP + lane]);
+    __syncthreads();
+    if (all > 0.0 && all < 0x1p-256) {
+        const int sh = -ilogb(all) - 1;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = ldexp(v[q], sh);
+        return sh;
+    }
+    return 0;
+}
+
+// out[q] = sum_j sM[j*64 + 8g + q] * sX[j*32 + lane]   (sM a 64x64 matrix, sX a 64x32 tile)
+__device__ __forceinline__ void tile_matvec8(const double* __restrict__ sM, const double* __restrict__ sX, int g, int lane, double (&o)[8]) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) o[q] = 0.0;
+#pragma unroll 16
+    for (int j = 0; j < SP; ++j) {
+        const double2* r = reinterpret_cast<const double2*>(sM + j * SP + 8 * g);
+        const double2 a = r[0], b = r[1], c = r[2], d = r[3];
+        const double x = sX[j * kTileP + lane];
+        o[0] = fma(a.x, x, o[0]); o[1] = fma(a.y, x, o[1]); o[2] = fma(b.x, x, o[2]); o[3] = fma(b.y, x, o[3]);
+        o[4] = fma(c.x, x, o[4]); o[5] = fma(c.y, x, o[5]); o[6] = fma(d.x, x, o[6]); o[7] = fma(d.y, x, o[7]);
+    }
+}
+
+// grid (Pp/32, nodes in level, M), block 256, dynamic smem (64*64 + 64*32 + 8*32) doubles.
+__global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const int* __restrict__ nodes) {
+    extern __shared__ __align__(16) double sm[];
+    double* sPT = sm;                    // PT_u
+    double* sD = sm + SP2;               // D_u tile [64][32]
+    double* smax = sD + SP * kTileP;     // [8][32]
     const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
-    const int p = blockIdx.x * TP + tid;
-    const int iu = t.iidx[u];
-    const int M = md.M;
+    const int g = tid >> 5, lane = tid & 31;
+    const int p = blockIdx.x * kTileP + lane;
+    const int iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
     const bool root = (u == t.root);
-    if (!root) stage_matrix(sP, w.PT + mat_off(m, u, t.n), tid, TP);
-    double acc[SP];
+    if (!root) stage_matrix(sPT, w.PT + mat_off(m, u, t.n), tid, 256);
+    double v[8];
 #pragma unroll
-    for (int i = 0; i < SP; ++i) acc[i] = i < t.S ? 1.0 : 0.0;
+    for (int q = 0; q < 8; ++q) v[q] = (8 * g + q) < t.S ? 1.0 : 0.0;
     int ecum = 0, eown = 0;
-    for (int q = t.ch_off[u]; q < t.ch_off[u + 1]; ++q) {
-        const int c = t.ch[q];
+    for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
+        const int c = t.ch[k];
         if (t.leaf[c]) {
-            mul_leaf_msg(acc, t, w, m, c, p);
+            mul_leaf8(v, t, w, m, c, p, g);
         } else {
             const int ic = t.iidx[c];
-            const double* src = w.Ms + part_off(ic, m, M, t.Pp) + p;
+            const double* src = w.Ms + part_off(ic, m, M, t.Pp) + size_t(8 * g) * Pp + p;
 #pragma unroll
-            for (int i = 0; i < SP; ++i) acc[i] *= src[i * Pp];
+            for (int q = 0; q < 8; ++q) v[q] *= src[q * Pp];
             ecum += w.Ecum[col_off(ic, m, M, t.Pp) + p];
         }
-        eown += renorm64(acc);
+        eown += renorm_cols(v, smax, g, lane);
     }
-    double* dst = w.D + part_off(iu, m, M, t.Pp) + p;
+    double* dst = w.D + part_off(iu, m, M, t.Pp) + size_t(8 * g) * Pp + p;
 #pragma unroll
-    for (int i = 0; i < SP; ++i) dst[i * Pp] = acc[i];
-    w.Eown[col_off(iu, m, M, t.Pp) + p] = eown;
-    w.Ecum[col_off(iu, m, M, t.Pp) + p] = ecum + eown;
+    for (int q = 0; q < 8; ++q) dst[q * Pp] = v[q];
+    if (g == 0) {
+        w.Eown[col_off(iu, m, M, t.Pp) + p] = eown;
+        w.Ecum[col_off(iu, m, M, t.Pp) + p] = ecum + eown;
+    }
     if (root) return;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sD[(8 * g + q) * kTileP + lane] = v[q];
     __syncthreads();
     // message to the parent: (P_u D_u)_i = sum_j PT[j][i] D_j
-    smem_matvec_store(sP, acc, w.Ms + part_off(iu, m, M, t.Pp) + p, Pp);
+    double o[8];
+    tile_matvec8(sPT, sD, g, lane, o);
+    double* md_ = w.Ms + part_off(iu, m, M, t.Pp) + size_t(8 * g) * Pp + p;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) md_[q * Pp] = o[q];
 }
 
 // --------------------------------------------------------------------- root
@@ -249,59 +330,63 @@ __global__ void k_root(Topo t, Model md, Work w) {
 }
 
 // ------------------------------------------------------------------ outside
-// grid (Pp/TP, nodes in level, M), block TP, dynamic smem = 2 * 64 * 64 doubles.
-__global__ void __launch_bounds__(TP) k_outside(Topo t, Model md, Work w, const int* __restrict__ nodes, int want_v) {
+// One CTA per (child c of a node at this depth, 32-pattern tile, rate class):
+// V_c = 2^{e_u} U_u o prod_{s != c} (P_s D_s), then U_c = P_c^T V_c for internal c.
+// grid (Pp/32, children in level, M), block 256, dynamic smem (64*64 + 64*32 + 8*32) doubles.
+__global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const int* __restrict__ kids, int want_v) {
     extern __shared__ __align__(16) double sm[];
-    double* sU = sm;          // [64][TP] outside partial of u
-    double* sP = sm + SP2;    // P_c row-major
-    const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
-    const int p = blockIdx.x * TP + tid;
-    const int iu = t.iidx[u], M = md.M;
+    double* sP = sm;                     // P_c row-major
+    double* sV = sm + SP2;               // V_c tile [64][32]
+    double* smax = sV + SP * kTileP;
+    const int c = kids[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
+    const int g = tid >> 5, lane = tid & 31;
+    const int p = blockIdx.x * kTileP + lane;
+    const int u = t.parent[c], iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
+    const bool internal = !t.leaf[c];
+    if (internal) stage_matrix(sP, w.P + mat_off(m, c, t.n), tid, 256);
+    double v[8];
     if (u == t.root) {
-        for (int i = 0; i < SP; ++i) sU[i * TP + tid] = md.pi[i];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = md.pi[8 * g + q];
     } else {
-        const double* src = w.U + part_off(iu, m, M, t.Pp) + p;
-        for (int i = 0; i < SP; ++i) sU[i * TP + tid] = src[i * Pp];
+        const double* src = w.U + part_off(iu, m, M, t.Pp) + size_t(8 * g) * Pp + p;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = src[q * Pp];
     }
-    const int eu = w.Eown[col_off(iu, m, M, t.Pp) + p];
-    const double fp = w.f[size_t(m) * Pp + p];
-    const int q0 = t.ch_off[u], q1 = t.ch_off[u + 1];
-    for (int q = q0; q < q1; ++q) {
-        const int c = t.ch[q];
-        double v[SP];
+    int ev = w.Eown[col_off(iu, m, M, t.Pp) + p];
+    for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
+        const int s = t.ch[k];
+        if (s == c) continue;
+        if (t.leaf[s]) {
+            mul_leaf8(v, t, w, m, s, p, g);
+        } else {
+            const double* src = w.Ms + part_off(t.iidx[s], m, M, t.Pp) + size_t(8 * g) * Pp + p;
 #pragma unroll
-        for (int i = 0; i < SP; ++i) v[i] = sU[i * TP + tid];
-        int ev = eu;
-        for (int q2 = q0; q2 < q1; ++q2) {
-            if (q2 == q) continue;
-            const int s = t.ch[q2];
-            if (t.leaf[s]) {
-                mul_leaf_msg(v, t, w, m, s, p);
-            } else {
-                const double* src = w.Ms + part_off(t.iidx[s], m, M, t.Pp) + p;
-#pragma unroll
-                for (int i = 0; i < SP; ++i) v[i] *= src[i * Pp];
-            }
-            ev -= renorm64(v);
+            for (int q = 0; q < 8; ++q) v[q] *= src[q * Pp];
         }
-        if (ev != 0) {
-#pragma unroll
-            for (int i = 0; i < SP; ++i) v[i] = ldexp(v[i], ev);
-        }
-        if (want_v) {
-            double* dst = w.Vf + part_off(c, m, M, t.Pp) + p;
-#pragma unroll
-            for (int i = 0; i < SP; ++i) dst[i * Pp] = fp * v[i];
-        }
-        if (!t.leaf[c]) {
-            __syncthreads();
-            stage_matrix(sP, w.P + mat_off(m, c, t.n), tid, TP);
-            __syncthreads();
-            // U_c = P_c^T V_c : (U_c)_i = sum_j P[j][i] v_j
-            smem_matvec_store(sP, v, w.U + part_off(t.iidx[c], m, M, t.Pp) + p, Pp);
-        }
+        ev -= renorm_cols(v, smax, g, lane);
     }
+    if (ev != 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = ldexp(v[q], ev);
+    }
+    if (want_v) {
+        const double fp = w.f[size_t(m) * Pp + p];
+        double* dst = w.Vf + part_off(c, m, M, t.Pp) + size_t(8 * g) * Pp + p;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) dst[q * Pp] = fp * v[q];
+    }
+    if (!internal) return;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sV[(8 * g + q) * kTileP + lane] = v[q];
+    __syncthreads();
+    // U_c = P_c^T V_c : (U_c)_i = sum_j P[j][i] V_j
+    double o[8];
+    tile_matvec8(sP, sV, g, lane, o);
+    double* dst = w.U + part_off(t.iidx[c], m, M, t.Pp) + size_t(8 * g) * Pp + p;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) dst[q * Pp] = o[q];
 }
 
 // ------------------------------------------------------------------ accum A
@@ -378,7 +463,8 @@ __device__ __forceinline__ double block_sum_256(double x, double* red) {
 }
 
 // ------------------------------------------------------------------ frechet
-// grid (n, M), block 256, dynamic smem 3 * 64 * 64 doubles.
+// grid (n, M, max(K,1)): CTA z handles model k = z on a test branch (k = K, z = 0,
+// on a background branch); z = 0 also writes <A, dP>.  block 256, dynamic smem 3 * 64 * 64 doubles.
 __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int want_global) {
     extern __shared__ __align__(16) double sm[];
     double* sA = sm;
@@ -386,8 +472,11 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int w
     double* sT = sm + 2 * SP2;
     __shared__ double red[8];
     __shared__ double se[SP];
-    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x, n = t.n, M = md.M;
+    const int b = blockIdx.x, m = blockIdx.y, z = blockIdx.z, tid = threadIdx.x, n = t.n, M = md.M;
     if (b == t.root) return;
+    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+    const bool has_model = test ? z < md.K : z == 0;
+    if (!(z == 0 || (want_global && has_model))) return;
     const double* Ap = w.Apart + (size_t(b) * M + m) * w.nchunk * SP2;
     for (int e = tid; e < SP2; e += 256) {
         double s = 0.0;
@@ -395,62 +484,61 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int w
         sA[e] = s;
     }
     __syncthreads();
-    const double* dP = w.dP + mat_off(m, b, n);
-    double g = 0.0;
-    for (int e = tid; e < SP2; e += 256) g = fma(sA[e], dP[e], g);
-    g = block_sum_256(g, red);
-    if (tid == 0) w.gt[size_t(m) * n + b] = g;
-    if (!want_global) return;
-    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-    const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
+    if (z == 0) {
+        const double* dP = w.dP + mat_off(m, b, n);
+        double g = 0.0;
+        for (int e = tid; e < SP2; e += 256) g = fma(sA[e], dP[e], g);
+        g = block_sum_256(g, red);
+        if (tid == 0) w.gt[size_t(m) * n + b] = g;
+    }
+    if (!want_global || !has_model) return;
+    const int k = test ? z : md.K;
     const int r = tid >> 2, c0 = (tid & 3) * 16;
-    for (int k = k0; k < k1; ++k) {
-        const double cw = test ? md.class_w[k] : 1.0;
-        const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
-        __syncthreads();
-        stage_matrix(sB, md.U + size_t(k) * SP2, tid, 256);
-        if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
-        __syncthreads();
-        // T = U^T A
-        double acc[16];
+    const double cw = test ? md.class_w[k] : 1.0;
+    const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
+    __syncthreads();
+    stage_matrix(sB, md.U + size_t(k) * SP2, tid, 256);
+    if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
+    __syncthreads();
+    // T = U^T A
+    double acc[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-        for (int l = 0; l < SP; ++l) {
-            const double u = sB[l * SP + r];
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int l = 0; l < SP; ++l) {
+        const double u = sB[l * SP + r];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc[q] = fma(u, sA[l * SP + c0 + q], acc[q]);
-        }
+        for (int q = 0; q < 16; ++q) acc[q] = fma(u, sA[l * SP + c0 + q], acc[q]);
+    }
 #pragma unroll
-        for (int q = 0; q < 16; ++q) sT[r * SP + c0 + q] = acc[q];
-        __syncthreads();
-        stage_matrix(sB, md.V + size_t(k) * SP2, tid, 256);
-        __syncthreads();
-        // At = T V^T
+    for (int q = 0; q < 16; ++q) sT[r * SP + c0 + q] = acc[q];
+    __syncthreads();
+    stage_matrix(sB, md.V + size_t(k) * SP2, tid, 256);
+    __syncthreads();
+    // At = T V^T
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-        for (int l = 0; l < SP; ++l) {
-            const double x = sT[r * SP + l];
+    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int l = 0; l < SP; ++l) {
+        const double x = sT[r * SP + l];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc[q] = fma(x, sB[(c0 + q) * SP + l], acc[q]);
-        }
-        const double* lam = md.lam + size_t(k) * SP;
-        const double li = lam[r], ei = se[r];
-        double* Hp = w.Hpart + ((size_t(k) * M + m) * n + b) * SP2;
-        double dg = 0.0, dq = 0.0;
+        for (int q = 0; q < 16; ++q) acc[q] = fma(x, sB[(c0 + q) * SP + l], acc[q]);
+    }
+    const double* lam = md.lam + size_t(k) * SP;
+    const double li = lam[r], ei = se[r];
+    double* Hp = w.Hpart + ((size_t(k) * M + m) * n + b) * SP2;
+    double dg = 0.0, dq = 0.0;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int j = c0 + q;
-            const double lj = lam[j], ej = se[j], d = li - lj;
-            const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
-            Hp[r * SP + j] = cw * acc[q] * E;
-            if (j == r) { dg = ei * acc[q]; dq = li * ei * acc[q]; }
-        }
-        dg = block_sum_256(dg, red);
-        dq = block_sum_256(dq, red);
-        if (tid == 0) {
-            if (test) w.gc[(size_t(k) * M + m) * n + b] = dg;
-            w.stg[(size_t(k) * M + m) * n + b] = cw * tau * dq;
-        }
+    for (int q = 0; q < 16; ++q) {
+        const int j = c0 + q;
+        const double lj = lam[j], ej = se[j], d = li - lj;
+        const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
+        Hp[r * SP + j] = cw * acc[q] * E;
+        if (j == r) { dg = ei * acc[q]; dq = li * ei * acc[q]; }
+    }
+    dg = block_sum_256(dg, red);
+    dq = block_sum_256(dq, red);
+    if (tid == 0) {
+        if (test) w.gc[(size_t(k) * M + m) * n + b] = dg;
+        w.stg[(size_t(k) * M + m) * n + b] = cw * tau * dq;
     }
 }
 
@@ -468,55 +556,52 @@ __global__ void k_hsum(Topo t, Model md, Work w) {
     w.H[size_t(k) * SP2 + e] = s;
 }
 
-// per (direction x, model k): sum_ij (V_k dQ U_k)_ij H_k,ij - [normalized] dmu/mu * stg_k
-// grid (ndirs, nmod), block 256, dynamic smem 3 * 64 * 64 doubles.
+// per (direction x, model k, row block rb): sum over rows [16rb, 16rb+16) of
+// (V_k dQ U_k) o H_k, minus (block 0, normalized time) dmu/mu * stg_k.
+// grid (ndirs, nmod, 4), block 256, dynamic smem (64*64 + 16*64 + 64*64) doubles.
 __global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
     extern __shared__ __align__(16) double sm[];
-    double* sX = sm;
-    double* sY = sm + SP2;
-    double* sZ = sm + 2 * SP2;
+    double* sX = sm;                 // dQ, later U_k
+    double* sY = sm + SP2;           // (V dQ)[rows, :]
+    double* sVr = sY + 16 * SP;      // V_k rows of the block
     __shared__ double red[8];
-    const int x = blockIdx.x, k = blockIdx.y, tid = threadIdx.x;
+    const int x = blockIdx.x, k = blockIdx.y, rb = blockIdx.z, tid = threadIdx.x;
     const double* dQ = md.dQ + (size_t(x) * md.nmod + k) * SP2;
-    stage_matrix(sX, md.V + size_t(k) * SP2, tid, 256);
-    stage_matrix(sY, dQ, tid, 256);
+    stage_matrix(sX, dQ, tid, 256);
+    for (int e = tid; e < 16 * SP; e += 256) sVr[e] = md.V[size_t(k) * SP2 + size_t(16 * rb) * SP + e];
     __syncthreads();
-    const int r = tid >> 2, c0 = (tid & 3) * 16;
-    double acc[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    const int r = tid >> 4, c0 = (tid & 15) * 4;   // 16 rows x 64 columns, 4 per thread
+    double acc[4] = {0, 0, 0, 0};
     for (int l = 0; l < SP; ++l) {
-        const double a = sX[r * SP + l];
+        const double a = sVr[r * SP + l];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma(a, sY[l * SP + c0 + q], acc[q]);
+        for (int q = 0; q < 4; ++q) acc[q] = fma(a, sX[l * SP + c0 + q], acc[q]);
     }
 #pragma unroll
-    for (int q = 0; q < 16; ++q) sZ[r * SP + c0 + q] = acc[q];
+    for (int q = 0; q < 4; ++q) sY[r * SP + c0 + q] = acc[q];
+    double dmu = 0.0;
+    if (rb == 0 && tid < SP) dmu = -md.pi[tid] * dQ[tid * SP + tid];
     __syncthreads();
     stage_matrix(sX, md.U + size_t(k) * SP2, tid, 256);
     __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = 0.0;
+    for (int l = 0; l < SP; ++l) {
+        const double a = sY[r * SP + l];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = fma(a, sX[l * SP + c0 + q], acc[q]);
+    }
+    const double* H = w.H + size_t(k) * SP2 + size_t(16 * rb) * SP;
     double g = 0.0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-    for (int l = 0; l < SP; ++l) {
-        const double a = sZ[r * SP + l];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma(a, sX[l * SP + c0 + q], acc[q]);
-    }
-    const double* H = w.H + size_t(k) * SP2;
-#pragma unroll
-    for (int q = 0; q < 16; ++q) g = fma(acc[q], H[r * SP + c0 + q], g);
-    double dmu = 0.0;
-    if (tid < SP) dmu = -md.pi[tid] * dQ[tid * SP + tid];
+    for (int q = 0; q < 4; ++q) g = fma(acc[q], H[r * SP + c0 + q], g);
     g = block_sum_256(g, red);
     dmu = block_sum_256(dmu, red);
     if (tid == 0) {
         double v = g;
-        if (md.time_mode == 1) {
-            // stg_k total sits in out[] after k_small: out[2 + n + K + k]
-            v -= dmu / fmax(md.mu[k], 1e-12) * w.out[2 + t.n + md.K + k];
-        }
-        w.dirpart[size_t(x) * md.nmod + k] = v;
+        // stg_k total sits in out[] after k_small: out[2 + n + K + k]
+        if (rb == 0 && md.time_mode == 1) v -= dmu / fmax(md.mu[k], 1e-12) * w.out[2 + t.n + md.K + k];
+        w.dirpart[(size_t(x) * md.nmod + k) * 4 + rb] = v;
     }
 }
 
@@ -533,7 +618,7 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
         s = y;
     }
     double tot = block_sum_256(s + c, red);
-    if (tid == 0) { w.out[0] = tot; w.out[1] = 0.0; }
+    if (tid == 0) { w.out[0] = tot; w.out[1] = w.err ? double(*w.err) : 0.0; }
     if (!grads) return;
     for (int b = tid; b < n; b += 256) {
         double g = 0.0;
@@ -567,32 +652,37 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
 
 // ------------------------------------------------------------------ launch
 static size_t smem_bytes(int mats) { return size_t(mats) * SP2 * sizeof(double); }
+static const size_t kPruneSmem = (SP2 + SP * kTileP + kGroups * kTileP) * sizeof(double);
+static const size_t kBuildSmem = (SP2 + 2 * SP * 16) * sizeof(double);
+static const size_t kDirSmem = (2 * SP2 + 16 * SP) * sizeof(double);
 
 void fp64_configure() {
-    cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(2)));
-    cudaFuncSetAttribute(k_outside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(2)));
+    cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
+    cudaFuncSetAttribute(k_inside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
+    cudaFuncSetAttribute(k_outside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
     cudaFuncSetAttribute(k_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(3)));
-    cudaFuncSetAttribute(k_dir, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(3)));
+    cudaFuncSetAttribute(k_dir, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kDirSmem));
 }
 
 int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    k_build_P<<<dim3(t.n, md.M), 256, smem_bytes(2), s>>>(t, md, w);
-    return 1;
+    k_build_P<<<dim3(t.n, md.M, 4), 256, kBuildSmem, s>>>(t, md, w);
+    k_rowsum<<<dim3(t.n, md.M), SP, 0, s>>>(t, md, w);
+    return 2;
 }
 int launch_prep_given_P(const Topo& t, const Work& w, cudaStream_t s) {
     k_prep_given_P<<<t.n, 256, 0, s>>>(t, w);
     return 1;
 }
 int launch_inside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, cudaStream_t s) {
-    k_inside<<<dim3(t.Pp / TP, count, md.M), TP, 0, s>>>(t, md, w, d_nodes);
+    k_inside<<<dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s>>>(t, md, w, d_nodes);
     return 1;
 }
 int launch_root(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
     k_root<<<(t.Pp + 127) / 128, 128, 0, s>>>(t, md, w);
     return 1;
 }
-int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, int want_v, cudaStream_t s) {
-    k_outside<<<dim3(t.Pp / TP, count, md.M), TP, smem_bytes(2), s>>>(t, md, w, d_nodes, want_v);
+int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_kids, int count, int want_v, cudaStream_t s) {
+    k_outside<<<dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s>>>(t, md, w, d_kids, want_v);
     return 1;
 }
 int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
@@ -600,7 +690,7 @@ int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream
     return 1;
 }
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {
-    k_frechet<<<dim3(t.n, md.M), 256, smem_bytes(3), s>>>(t, md, w, want_global);
+    k_frechet<<<dim3(t.n, md.M, want_global ? (md.K > 1 ? md.K : 1) : 1), 256, smem_bytes(3), s>>>(t, md, w, want_global);
     return 1;
 }
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
@@ -609,7 +699,7 @@ int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s)
 }
 int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
     if (md.ndirs <= 0) return 0;
-    k_dir<<<dim3(md.ndirs, md.nmod), 256, smem_bytes(3), s>>>(t, md, w);
+    k_dir<<<dim3(md.ndirs, md.nmod, 4), 256, kDirSmem, s>>>(t, md, w);
     return 1;
 }
 int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s) {

@@ -1,15 +1,466 @@
-// h3g_mixed.cu — split-precision pruning path (not built yet: mixed_available() is false).
+// h3g_mixed.cu — split-precision pruning on the sm_100a tensor cores.
+//
+// One CTA = 128 patterns x one node (inside) or one child (outside); thread t
+// owns pattern row t, which is also TMEM lane t of the accumulator, so the
+// per-pattern rescaling, the elementwise products with sibling messages and the
+// epilogue all stay in registers of one thread.  The 61x61 contraction is a
+// tcgen05.mma (M=128 patterns, N=64 states, K=64 states) issued by one thread:
+// A = the CTA's partial tile, written by the threads into shared memory as a
+// K-major BF16 hi/mid/lo triple; B = the branch's P (or P^T) tile, prepared
+// once per evaluation in the same layout and brought in by the bulk-copy (TMA)
+// engine.  The six leading products of the split accumulate in FP32 in TMEM,
+// which reproduces an FP32 contraction to about 2^-24.
+#include <algorithm>
+#include <type_traits>
+
 #include "h3g_mixed.h"
+#include "h3g_tc.cuh"
 
 namespace h3g {
 
-bool mixed_available() { return false; }
-void mixed_configure() {}
-h3g_status mixed_alloc(MixedWork&, std::vector<void*>&, int, int, int, int) { return H3G_ERR_CUDA; }
-int mixed_prepare(const Topo&, const Model&, const Work&, const MixedWork&, cudaStream_t) { return 0; }
-int launch_inside_mixed(const Topo&, const Model&, const Work&, const MixedWork&, const int*, int, cudaStream_t) { return 0; }
-int launch_root_mixed(const Topo&, const Model&, const Work&, const MixedWork&, cudaStream_t) { return 0; }
-int launch_outside_mixed(const Topo&, const Model&, const Work&, const MixedWork&, const int*, int, cudaStream_t) { return 0; }
-int launch_accumA_mixed(const Topo&, const Model&, const Work&, const MixedWork&, cudaStream_t) { return 0; }
+namespace {
+
+constexpr int MT = 128;                       // patterns per CTA = MMA M
+constexpr uint32_t kIdesc = tc::idesc_bf16(MT, SP);
+constexpr size_t kTileBytes = size_t(MT) * SP * 2;       // 16 KB per BF16 term
+constexpr size_t kBBytes = size_t(SP) * SP * 2;          // 8 KB per BF16 term
+constexpr size_t kMxSmem = 3 * kTileBytes + 3 * kBBytes + 64;   // A terms, B terms, barriers
+constexpr int kKSteps = SP / 16;                                 // K = 16 per kind::f16 MMA
+constexpr uint32_t kTmemCols = kKSteps * SP;                     // one 64-column accumulator per K step
+
+__device__ __forceinline__ size_t mat_off_f(int m, int b, int n) { return (size_t(m) * n + b) * SP2; }
+
+// Exact power-of-two scale factor 2^k for |k| <= 126.
+__device__ __forceinline__ float pow2f(int k) { return __int_as_float((127 + k) << 23); }
+
+// Normalise v to a maximum in [0.5, 1); returns the shift s (v_new = v * 2^s).
+__device__ __forceinline__ int renorm_row(float (&v)[SP]) {
+    float mx = 0.f;
+#pragma unroll
+    for (int i = 0; i < SP; ++i) mx = fmaxf(mx, v[i]);
+    if (!(mx > 0.f) || !(mx < INFINITY)) return 0;
+    const int sh = -ilogbf(mx) - 1;
+    for (int rem = sh; rem != 0;) {
+        const int step = rem > 126 ? 126 : (rem < -126 ? -126 : rem);
+        const float f = pow2f(step);
+#pragma unroll
+        for (int i = 0; i < SP; ++i) v[i] *= f;
+        rem -= step;
+    }
+    return sh;
+}
+
+// v *= P_c * leaf_vector(c, p) in FP32.
+__device__ __forceinline__ void mul_leaf_row(float (&v)[SP], const Topo& t, const MixedWork& mw, int m, int c, int p) {
+    const int tx = t.taxon[c];
+    const float* PTc = mw.PT32 + mat_off_f(m, c, t.n);
+    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
+    const float* src;
+    if (st >= 0) {
+        src = PTc + st * SP;
+    } else {
+        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * t.Pp + p];
+        if (mk == 0 || (mk & t.all_mask) == t.all_mask) {
+            src = mw.rs32 + (size_t(m) * t.n + c) * SP;
+        } else {
+#pragma unroll
+            for (int i = 0; i < SP; ++i) {
+                float s = 0.f;
+                for (uint64_t b = mk; b; b &= b - 1) s += __ldg(PTc + (__ffsll((long long)b) - 1) * SP + i);
+                v[i] *= s;
+            }
+            return;
+        }
+    }
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int q = 0; q < SP / 4; ++q) {
+        const float4 x = __ldg(s4 + q);
+        v[4 * q] *= x.x; v[4 * q + 1] *= x.y; v[4 * q + 2] *= x.z; v[4 * q + 3] *= x.w;
+    }
+}
+
+__device__ __forceinline__ void load_col(float (&v)[SP], const float* src, size_t stride) {
+#pragma unroll
+    for (int i = 0; i < SP; ++i) v[i] = src[i * stride];
+}
+__device__ __forceinline__ void mul_col(float (&v)[SP], const float* src, size_t stride) {
+#pragma unroll
+    for (int i = 0; i < SP; ++i) v[i] *= src[i * stride];
+}
+__device__ __forceinline__ void store_col(const float (&v)[SP], float* dst, size_t stride) {
+#pragma unroll
+    for (int i = 0; i < SP; ++i) dst[i * stride] = v[i];
+}
+
+// Shared-memory block of one tensor-core contraction.
+struct TcTile {
+    unsigned char* A[3];   // BF16 hi / mid / lo of the CTA's 128 x 64 partial tile
+    unsigned char* B[3];   // BF16 hi / mid / lo of the 64 x 64 transition tile
+    uint64_t* bars;        // [0] B tile arrival, [1] MMA completion
+    uint32_t* slot;        // TMEM base address written by tcgen05.alloc
+};
+
+__device__ __forceinline__ TcTile carve(unsigned char* sm) {
+    TcTile s;
+    for (int q = 0; q < 3; ++q) s.A[q] = sm + q * kTileBytes;
+    for (int q = 0; q < 3; ++q) s.B[q] = sm + 3 * kTileBytes + q * kBBytes;
+    s.bars = reinterpret_cast<uint64_t*>(sm + 3 * kTileBytes + 3 * kBBytes);
+    s.slot = reinterpret_cast<uint32_t*>(s.bars + 2);
+    return s;
+}
+
+// Barriers, TMEM and the B tile terms for one contraction.  All threads call.
+__device__ __forceinline__ void tc_begin(const TcTile& s, uint16_t* const (&b)[3], size_t off) {
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        tc::mbar_init(&s.bars[0], 1);
+        tc::mbar_init(&s.bars[1], 1);
+        tc::mbar_fence_init();
+    }
+    if ((tid >> 5) == 0) tc::tmem_alloc(s.slot, kTmemCols);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    if (tid == 0) {
+        tc::mbar_expect_tx(&s.bars[0], uint32_t(3 * kBBytes));
+        for (int q = 0; q < 3; ++q) tc::bulk_g2s(s.B[q], b[q] + off, uint32_t(kBBytes), &s.bars[0]);
+    }
+}
+
+// Write this thread's row (64 FP32 values) into the K-major A tiles as a BF16 split.
+__device__ __forceinline__ void tc_write_row(const TcTile& s, const float (&v)[SP]) {
+    const int r = threadIdx.x;
+#pragma unroll
+    for (int kc = 0; kc < SP / 8; ++kc) {
+        uint32_t w[3][4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const tc::Bf16x3 x0 = tc::split3(v[8 * kc + 2 * e]);
+            const tc::Bf16x3 x1 = tc::split3(v[8 * kc + 2 * e + 1]);
+            w[0][e] = uint32_t(x0.hi) | (uint32_t(x1.hi) << 16);
+            w[1][e] = uint32_t(x0.mid) | (uint32_t(x1.mid) << 16);
+            w[2][e] = uint32_t(x0.lo) | (uint32_t(x1.lo) << 16);
+        }
+        const uint32_t off = tc::kmajor_off16(MT, r, 8 * kc);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            *reinterpret_cast<uint4*>(s.A[q] + off) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+    }
+}
+
+// out = A * B^T for this thread's row: issue (one thread), wait (all), read TMEM.
+__device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[SP], int* err) {
+    const int tid = threadIdx.x, warp = tid >> 5;
+    tc::fence_async_smem();
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *s.slot;
+    if (tid == 0) {
+        const bool got_b = tc::mbar_wait(&s.bars[0], 0);
+        if (got_b) {
+            const uint32_t lboA = (MT / 8) * 128, lboB = (SP / 8) * 128;
+            // Each K step accumulates into its own TMEM columns: the five small split
+            // products first (their rounding is ~2^-8 below the result), hi*hi last,
+            // so every accumulator takes at most one add at full magnitude; the
+            // four accumulators are summed in FP64 in the epilogue.
+            const int pa[6] = {1, 2, 0, 1, 0, 0}, pb[6] = {1, 0, 2, 0, 1, 0};   // mm lh hl mh hm hh
+#pragma unroll
+            for (int ks = 0; ks < kKSteps; ++ks) {
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    const uint64_t da = tc::smem_desc(tc::smem_u32(s.A[pa[q]]) + 2 * ks * lboA, lboA, 128);
+                    const uint64_t db = tc::smem_desc(tc::smem_u32(s.B[pb[q]]) + 2 * ks * lboB, lboB, 128);
+                    tc::mma_bf16(tmem + uint32_t(ks * SP), da, db, kIdesc, q == 0 ? 0u : 1u);
+                }
+            }
+        } else {
+            atomicOr(err, 1);
+        }
+        tc::mma_commit(&s.bars[1]);
+    }
+    if (!tc::mbar_wait(&s.bars[1], 0) && (tid & 31) == 0) atomicOr(err, 2);
+    tc::tc_fence_after();
+    const uint32_t row = tmem + (uint32_t(warp * 32) << 16);
+#pragma unroll
+    for (int c4 = 0; c4 < SP / 16; ++c4) {
+        double acc[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < kKSteps; ++ks) {
+            float t16[16];
+            tc::tmem_ld16(row + uint32_t(ks * SP + c4 * 16), t16);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] += double(t16[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) o[c4 * 16 + i] = float(acc[i]);
+    }
+    tc::tmem_wait_ld();
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+}
+
+// ------------------------------------------------------------ P preparation
+// grid (n, M), block 256: BF16 hi/mid/lo tiles of P and P^T, FP32 P^T and row sums.
+__global__ void __launch_bounds__(256) k_prep_mx(Topo t, Model md, Work w, MixedWork mw) {
+    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
+    if (b == t.root) return;
+    const double* P = w.P + mat_off(m, b, t.n);
+    const size_t o = mat_off_f(m, b, t.n);
+    for (int e = tid; e < SP2; e += 256) {
+        const int i = e >> 6, j = e & 63;
+        const float x = float(P[e]);             // P[i][j]
+        const tc::Bf16x3 sp = tc::split3(x);
+        const uint16_t terms[3] = {sp.hi, sp.mid, sp.lo};
+        // inside contraction: row i (output state), K = j;  outside (P^T): row j, K = i
+        const uint32_t oi = tc::kmajor_off16(SP, i, j) / 2, ot = tc::kmajor_off16(SP, j, i) / 2;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            mw.Bp[q][o + oi] = terms[q];
+            mw.Bpt[q][o + ot] = terms[q];
+        }
+        mw.PT32[o + size_t(j) * SP + i] = x;
+    }
+    if (tid < SP) mw.rs32[(size_t(m) * t.n + b) * SP + tid] = float(w.rs[(size_t(m) * t.n + b) * SP + tid]);
+}
+
+// ------------------------------------------------------------------ inside
+// grid (Pp/128, nodes in level, M), block 128.
+__global__ void __launch_bounds__(MT) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ nodes) {
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    const TcTile s = carve(smraw);
+    const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
+    const int p = blockIdx.x * MT + tid;
+    const int iu = t.iidx[u], M = md.M;
+    const size_t Pp = size_t(t.Pp);
+    const bool root = u == t.root;
+    if (!root) tc_begin(s, mw.Bp, mat_off_f(m, u, t.n));
+    float v[SP];
+#pragma unroll
+    for (int i = 0; i < SP; ++i) v[i] = i < t.S ? 1.f : 0.f;
+    int E = 0;
+    for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
+        const int c = t.ch[k];
+        if (t.leaf[c]) {
+            mul_leaf_row(v, t, mw, m, c, p);
+        } else {
+            const int ic = t.iidx[c];
+            mul_col(v, mw.Ms + part_off(ic, m, M, t.Pp) + p, Pp);
+            E += mw.EM[col_off(ic, m, M, t.Pp) + p];
+        }
+        E += renorm_row(v);
+    }
+    store_col(v, mw.D + part_off(iu, m, M, t.Pp) + p, Pp);
+    mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
+    if (root) return;
+    tc_write_row(s, v);
+    float o[SP];
+    tc_run(s, o, w.err);
+    const int sh = renorm_row(o);
+    store_col(o, mw.Ms + part_off(iu, m, M, t.Pp) + p, Pp);
+    mw.EM[col_off(iu, m, M, t.Pp) + p] = E + sh;
+}
+
+// --------------------------------------------------------------------- root
+__global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= t.Pp) return;
+    const int ir = t.iidx[t.root], M = md.M;
+    const double wt = t.w[p];
+    double L[kMaxRateClasses], ll[kMaxRateClasses];
+    for (int m = 0; m < M; ++m) {
+        const float* D = mw.D + part_off(ir, m, M, t.Pp) + p;
+        double s = 0.0;
+        for (int i = 0; i < SP; ++i) s = fma(md.pi[i], double(D[size_t(i) * t.Pp]), s);
+        L[m] = s;
+        ll[m] = s > 0.0 ? log(s) - double(mw.ED[col_off(ir, m, M, t.Pp) + p]) * 0.69314718055994530942 : -1e20;
+    }
+    double site = -1e20, contrib = 0.0;
+    bool ok = false;
+    if (M == 1) {
+        if (L[0] > 0.0) { ok = true; site = ll[0]; contrib = wt * ll[0]; w.f[p] = wt / L[0]; }
+        else w.f[p] = 0.0;
+        w.rw[p] = 0.0;
+    } else {
+        double mx = -INFINITY;
+        for (int m = 0; m < M; ++m)
+            if (md.rate_w[m] > 1e-12 && L[m] > 0.0) mx = fmax(mx, log(md.rate_w[m]) + ll[m]);
+        double post[kMaxRateClasses], se = 0.0;
+        for (int m = 0; m < M; ++m) {
+            post[m] = 0.0;
+            if (mx > -1e19 && md.rate_w[m] > 1e-12 && L[m] > 0.0) { post[m] = exp(log(md.rate_w[m]) + ll[m] - mx); se += post[m]; }
+        }
+        if (mx > -1e19 && se > 0.0) { ok = true; site = mx + log(se); contrib = wt * site; }
+        for (int m = 0; m < M; ++m) {
+            const double pw = ok ? post[m] / se : 0.0;
+            w.f[size_t(m) * t.Pp + p] = (ok && pw > 1e-12) ? wt * pw / L[m] : 0.0;
+            w.rw[size_t(m) * t.Pp + p] = ok ? wt * pw / md.rate_w[m] : 0.0;
+        }
+    }
+    if (!ok && md.sentinel) contrib = wt * -1e20;
+    w.contrib[p] = contrib;
+    w.site[p] = site;
+}
+
+// ------------------------------------------------------------------ outside
+// grid (Pp/128, children in level, M), block 128.
+__global__ void __launch_bounds__(MT) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ kids) {
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    const TcTile s = carve(smraw);
+    const int c = kids[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
+    const int p = blockIdx.x * MT + tid;
+    const int u = t.parent[c], iu = t.iidx[u], M = md.M;
+    const size_t Pp = size_t(t.Pp);
+    const bool internal = !t.leaf[c];
+    if (internal) tc_begin(s, mw.Bpt, mat_off_f(m, c, t.n));
+    float v[SP];
+    int EV = 0;
+    if (u == t.root) {
+#pragma unroll
+        for (int i = 0; i < SP; ++i) v[i] = float(md.pi[i]);
+        EV = renorm_row(v);
+    } else {
+        load_col(v, mw.U + part_off(iu, m, M, t.Pp) + p, Pp);
+        EV = mw.EU[col_off(iu, m, M, t.Pp) + p];
+    }
+    for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
+        const int sb = t.ch[k];
+        if (sb == c) continue;
+        if (t.leaf[sb]) {
+            mul_leaf_row(v, t, mw, m, sb, p);
+        } else {
+            mul_col(v, mw.Ms + part_off(t.iidx[sb], m, M, t.Pp) + p, Pp);
+            EV += mw.EM[col_off(t.iidx[sb], m, M, t.Pp) + p];
+        }
+        EV += renorm_row(v);
+    }
+    // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
+    const int ir = t.iidx[t.root];
+    const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
+    const int EDc = internal ? mw.ED[col_off(t.iidx[c], m, M, t.Pp) + p] : 0;
+    const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
+    float* vf = mw.Vf + part_off(c, m, M, t.Pp) + p;
+#pragma unroll
+    for (int i = 0; i < SP; ++i) vf[i * Pp] = float(double(v[i]) * scale);
+    if (!internal) return;
+    tc_write_row(s, v);
+    float o[SP];
+    tc_run(s, o, w.err);
+    const int sh = renorm_row(o);
+    store_col(o, mw.U + part_off(t.iidx[c], m, M, t.Pp) + p, Pp);
+    mw.EU[col_off(t.iidx[c], m, M, t.Pp) + p] = EV + sh;
+}
+
+// ------------------------------------------------------------------ accum A
+// A_{m,b,chunk} = sum_p Vf D^T with FP32 products and FP32 accumulation inside
+// the chunk; chunks are summed in FP64 afterwards.  grid (n, M, nchunk), block 256.
+__global__ void __launch_bounds__(256) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
+    __shared__ __align__(16) float sV[32][SP + 4];
+    __shared__ __align__(16) float sD[32][SP + 4];
+    const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
+    if (b == t.root) return;
+    const int M = md.M;
+    const size_t Pp = size_t(t.Pp);
+    const int ti = tid & 15, tj = tid >> 4;
+    const int p_begin = ck * w.chunk, p_end = min(t.Pp, p_begin + w.chunk);
+    const bool lf = t.leaf[b];
+    const int tx = lf ? t.taxon[b] : -1;
+    const float* Vb = mw.Vf + part_off(b, m, M, t.Pp);
+    const float* Db = lf ? nullptr : mw.D + part_off(t.iidx[b], m, M, t.Pp);
+    float acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.f;
+    for (int p0 = p_begin; p0 < p_end; p0 += 32) {
+        for (int e = tid; e < 32 * SP; e += 256) {
+            const int pp = e & 31, i = e >> 5, p = p0 + pp;
+            const bool in = p < p_end;
+            sV[pp][i] = in ? Vb[i * Pp + p] : 0.f;
+            float d = 0.f;
+            if (in) {
+                if (!lf) {
+                    d = Db[i * Pp + p];
+                } else if (i < t.S) {
+                    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
+                    if (st >= 0) d = (st == i) ? 1.f : 0.f;
+                    else {
+                        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * Pp + p];
+                        d = (mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> i) & 1)) ? 1.f : 0.f;
+                    }
+                }
+            }
+            sD[pp][i] = d;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int pp = 0; pp < 32; ++pp) {
+            const float4 av = *reinterpret_cast<const float4*>(&sV[pp][4 * ti]);
+            const float4 bv = *reinterpret_cast<const float4*>(&sD[pp][4 * tj]);
+            const float a4[4] = {av.x, av.y, av.z, av.w}, b4[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] = fmaf(a4[a], b4[c], acc[a][c]);
+        }
+        __syncthreads();
+    }
+    double* dst = w.Apart + ((size_t(b) * M + m) * w.nchunk + ck) * SP2;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) dst[(4 * ti + a) * SP + 4 * tj + c] = double(acc[a][c]);
+}
+
+}  // namespace
+
+bool mixed_available() { return true; }
+
+void mixed_configure() {
+    cudaFuncSetAttribute(k_inside_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMxSmem));
+    cudaFuncSetAttribute(k_outside_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMxSmem));
+}
+
+h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, int M, int Pp) {
+    auto take = [&](auto** ptr, size_t count) -> bool {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(**ptr)) != cudaSuccess) return false;
+        owned.push_back(p);
+        *ptr = static_cast<std::remove_reference_t<decltype(*ptr)>>(p);
+        return true;
+    };
+    const size_t part = size_t(NI) * M * SP * Pp, cols = size_t(NI) * M * Pp, mats = size_t(M) * n * SP2;
+    bool ok = take(&mw.D, part) && take(&mw.Ms, part) && take(&mw.U, part) && take(&mw.Vf, size_t(n) * M * SP * Pp) &&
+              take(&mw.ED, cols) && take(&mw.EM, cols) && take(&mw.EU, cols) && take(&mw.PT32, mats) &&
+              take(&mw.rs32, size_t(M) * n * SP);
+    for (int q = 0; q < 3 && ok; ++q) ok = take(&mw.Bp[q], mats) && take(&mw.Bpt[q], mats);
+    return ok ? H3G_OK : H3G_ERR_OOM;
+}
+
+int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
+    k_prep_mx<<<dim3(t.n, md.M), 256, 0, s>>>(t, md, w, mw);
+    return 1;
+}
+int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s) {
+    k_inside_mx<<<dim3(t.Pp / MT, count, md.M), MT, kMxSmem, s>>>(t, md, w, mw, d_nodes);
+    return 1;
+}
+int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
+    k_root_mx<<<(t.Pp + 127) / 128, 128, 0, s>>>(t, md, w, mw);
+    return 1;
+}
+int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s) {
+    k_outside_mx<<<dim3(t.Pp / MT, count, md.M), MT, kMxSmem, s>>>(t, md, w, mw, d_kids);
+    return 1;
+}
+int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
+    k_accumA_mx<<<dim3(t.n, md.M, w.nchunk), 256, 0, s>>>(t, md, w, mw);
+    return 1;
+}
 
 }  // namespace h3g

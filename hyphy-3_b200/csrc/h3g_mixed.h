@@ -1,6 +1,13 @@
-// h3g_mixed.h — split-precision (tensor-core) pruning path: FP32 partials with
-// per-pattern power-of-two exponents, contractions on tcgen05, FP64 for the
-// model, the root log-sum and every reduction.
+// h3g_mixed.h — split-precision (tensor-core) pruning path.
+//
+// Partials are FP32 in block-floating-point form: every stored vector (one
+// node, one pattern, one rate class) is normalised to a maximum in [0.5, 1)
+// and carries an int32 exponent E with  true value = stored * 2^-E.  The
+// 61x61 contractions run on tcgen05 (kind::f16, BF16 operands) as the six
+// leading products of a three-term BF16 split of both operands
+// (hh + hm + mh + hl + lh + mm), accumulated in FP32 in TMEM.
+// The model (eigensystems, P assembly), rate-class mixing, the root log-sum
+// and every reduction stay in FP64.
 #pragma once
 #include <vector>
 #include "../../include/h3g.h"
@@ -9,18 +16,18 @@
 namespace h3g {
 
 struct MixedWork {
-    float* D = nullptr;      // [NI][M][Pp][64]  pattern-major FP32 partials
-    float* Ms = nullptr;     // [NI][M][Pp][64]
-    float* U = nullptr;      // [NI][M][Pp][64]
-    float* Vf = nullptr;     // [n][M][Pp][64]
-    int* Ecum = nullptr;     // [NI][M][Pp]
-    int* Eown = nullptr;     // [NI][M][Pp]
-    int* Eu = nullptr;       // [NI][M][Pp] exponent of the stored outside partial
-    int* Ev = nullptr;       // [n][M][Pp]  exponent of the stored Vf
-    float* Phi = nullptr;    // [M][n][64*64] tf32-rounded high part of P (row-major)
-    float* Plo = nullptr;    // [M][n][64*64] remainder
-    float* PThi = nullptr;   // transposes
-    float* PTlo = nullptr;
+    float* D = nullptr;      // [NI][M][64][Pp]  inside partial (normalised)
+    float* Ms = nullptr;     // [NI][M][64][Pp]  message P*D to the parent (normalised)
+    float* U = nullptr;      // [NI][M][64][Pp]  outside partial below the parent branch (normalised)
+    float* Vf = nullptr;     // [n][M][64][Pp]   f * V * 2^(EL - EV - ED) (gradient operand, O(1) scale)
+    int* ED = nullptr;       // [NI][M][Pp]      exponent of D
+    int* EM = nullptr;       // [NI][M][Pp]      exponent of Ms
+    int* EU = nullptr;       // [NI][M][Pp]      exponent of U
+    uint16_t* Bp[3] = {nullptr, nullptr, nullptr};   // [M][n][64*64] BF16 hi/mid/lo of P (rows = out state,
+                                                     //   K = in state) as a tcgen05 K-major tile
+    uint16_t* Bpt[3] = {nullptr, nullptr, nullptr};  // same for P^T
+    float* PT32 = nullptr;   // [M][n][64*64]    FP32 P^T row-major (leaf messages)
+    float* rs32 = nullptr;   // [M][n][64]       FP32 row sums of P
 };
 
 bool mixed_available();
@@ -29,7 +36,7 @@ h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, 
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s);
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
-int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s);
+int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s);
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 
 }  // namespace h3g

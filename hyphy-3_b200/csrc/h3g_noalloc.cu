@@ -135,6 +135,7 @@ extern "C" h3g_status h3g_eval_from_P_noalloc(int device, void* cuda_stream, int
                 return H3G_ERR_CUDA;
             }
             g_scratch_addr[device] = addr;
+            h3g::fp64_configure();   // shared-memory limits of the pruning kernels on this device
         }
         scratch = static_cast<unsigned char*>(g_scratch_addr[device]);
     }

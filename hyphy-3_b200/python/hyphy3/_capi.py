@@ -9,6 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import pathlib
+import weakref
 
 import numpy as np
 
@@ -101,6 +102,7 @@ class Context:
     def __init__(self, device: int = 0, stream: int | None = None):
         self.lib = load()
         self.h = C.c_void_p()
+        self._problems = weakref.WeakSet()
         st = self.lib.h3g_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(self.h))
         if st != H3G_OK:
             raise H3GError(f"h3g_ctx_create failed with status {st}")
@@ -110,6 +112,9 @@ class Context:
             raise H3GError(f"status {st}: {self.lib.h3g_last_error(self.h).decode()}")
 
     def close(self) -> None:
+        """Destroy the context after every problem still alive on it."""
+        for p in list(self._problems):
+            p.close()
         if self.h:
             self.lib.h3g_ctx_destroy(self.h)
             self.h = C.c_void_p()
@@ -139,13 +144,13 @@ class Problem:
         ctx.check(ctx.lib.h3g_problem_create(
             ctx.h, self.n, _ptr(self.parent, C.c_int32), _ptr(self.is_leaf, C.c_uint8), _ptr(self.leaf_taxon, C.c_int32),
             self.T, self.P, _ptr(self.states, C.c_int8), _ptr(self.masks, C.c_uint64), _ptr(self.weights), C.byref(self.h)))
-        self._keep = []
+        ctx._problems.add(self)
         self.K = self.M = self.ndirs = 0
 
     def close(self) -> None:
-        if self.h:
+        if self.h and self.ctx.h:
             self.ctx.lib.h3g_problem_destroy(self.h)
-            self.h = C.c_void_p()
+        self.h = C.c_void_p()
 
     def __del__(self):
         try:

@@ -102,7 +102,8 @@ typedef struct {
     double* grad_rate_w;      /* M partials d lnL / d rate_w[m], or NULL */
 } h3g_result;
 
-/* Context: one device, one stream (NULL = a private non-blocking stream). */
+/* Context: one device, one stream (NULL = a private non-blocking stream).
+ * h3g_ctx_destroy fails with H3G_ERR_STATE while problems created on it live. */
 h3g_status h3g_ctx_create(int device, void* cuda_stream, h3g_ctx** out);
 h3g_status h3g_ctx_destroy(h3g_ctx* ctx);
 const char* h3g_last_error(const h3g_ctx* ctx);
