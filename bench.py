@@ -44,17 +44,27 @@ WORKLOAD = ("BUSTED-style 3-omega MG94xREV: 64-taxon random unrooted tree (125 b
             "(3% gaps, 1% ambiguous), omegas {0.1,1,5} w {0.6,0.3,0.1}; lnL + grads wrt 125 t, 3 omega, 3 w, 5 theta")
 
 
-def build_inputs(seed_offset: int = 0):
+WORKLOADS = {
+    1: WORKLOAD,
+    3: ("large mixed MG94xREV: 1024-taxon Yule tree (2045 branches), 5000 codons, omegas {0.2,2} w {0.8,0.2} "
+        "mixed at the P level x 4 discrete-gamma synonymous-rate passes (root log-sum-exp); lnL + grads wrt 2045 t, "
+        "2 omega, 2 w, 5 theta, 4 rate weights"),
+}
+
+
+def build_inputs(seed_offset: int = 0, config: int = 1):
     import _hyphy3 as h
     from hyphy3.simulate import make_workload
-    wl = make_workload(1)
+    wl = make_workload(config)
     if seed_offset:
         # independent replica gene for another rank: same shapes, different draw
         import hyphy3.simulate as sim
         rng = np.random.default_rng(sim.SEED_BASE + 1 + 1000 * seed_offset)
+        noisy = config == 1
         names, seqs = sim.simulate_alignment(wl.tree, wl.n_sites, rng, theta=wl.theta,
                                              pos_freq=rng.dirichlet(np.ones(4), size=3), omegas=wl.omegas,
-                                             omega_w=wl.omega_w, gap_frac=0.03, ambig_frac=0.01)
+                                             omega_w=wl.omega_w, rates=wl.rates, rate_w=wl.rate_w,
+                                             gap_frac=0.03 if noisy else 0.0, ambig_frac=0.01 if noisy else 0.0)
         wl.names, wl.seqs = names, seqs
     aln = h.Alignment.from_sequences(wl.names, wl.seqs)
     tree = h.Tree.from_newick(wl.newick)
@@ -129,9 +139,12 @@ def fp64_dgemm_peak() -> float:
     return best
 
 
-def stage_work(aln_P: int, tree, M: int) -> dict:
-    """Algorithmic bytes and FP64 flops per stage for one evaluation (61 states, not padded).
+def stage_work(aln_P: int, tree, M: int, elem_bytes: int = 8) -> dict:
+    """Algorithmic bytes and flops per stage for one evaluation (61 states, not padded).
 
+    elem_bytes is the storage width of a partial entry: 8 on the FP64 path, 4 on
+    the mixed path (FP32 partials; the per-pattern int32 exponent is counted as
+    4 more bytes per stored vector).
     Partials are counted as one HBM round trip each way: the inside stage
     reads the messages of internal children, writes D and (non-root) the
     message P*D; the outside stage reads U of the parent and the sibling
@@ -143,7 +156,7 @@ def stage_work(aln_P: int, tree, M: int) -> dict:
     root = tree.root_id
     internal = [nd for nd in nodes if not nd.is_leaf]
     cols = aln_P * M
-    vec = 8 * S
+    vec = elem_bytes * S + (4 if elem_bytes == 4 else 0)
     ins_b = ins_f = out_b = out_f = acc_b = acc_f = 0
     for nd in internal:
         int_kids = [c for c in nd.children if not nodes[c].is_leaf]
@@ -165,25 +178,30 @@ def stage_work(aln_P: int, tree, M: int) -> dict:
             "accum_A": (acc_b * cols, acc_f * cols)}
 
 
-def cpu_baseline(wl, reps: int = 3) -> dict:
+def cpu_baseline(wl, reps: int = 3, max_sites: int | None = None) -> dict:
+    """The CPU restatement of the reference engine on the host cores (all threads)."""
     import h3oracle as o
-    a = o.Alignment.from_sequences(wl.names, wl.seqs)
+    nsite = wl.n_sites if max_sites is None else min(max_sites, wl.n_sites)
+    seqs = [sq[:3 * nsite] for sq in wl.seqs]
+    a = o.Alignment.from_sequences(wl.names, seqs)
     t = o.Tree.parse(wl.newick)
     cls = [{"alpha": 1.0, "beta": om, "theta": wl.theta} for om in wl.omegas]
+    rates, rw = (list(wl.rates), list(wl.rate_w)) if len(wl.rates) > 1 else ([], [])
     threads = o.max_threads()
     o.set_threads(threads)
     bl = list(t.branch_lengths)
-    o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
+    o.mixture_eval(t, a, cls, wl.omega_w, None, [], rates, rw, bl, False, True, False)
     times = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
+        o.mixture_eval(t, a, cls, wl.omega_w, None, [], rates, rw, bl, False, True, False)
         times.append(time.perf_counter() - t0)
-    units = wl.n_sites * (t.num_nodes() - 1)
+    units = nsite * (t.num_nodes() - 1)
     med = statistics.median(times)
+    what = "full evaluations" if nsite == wl.n_sites else f"evaluations of the first {nsite} of {wl.n_sites} sites"
     return {"value": units / med, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{reps} full evaluations (lnL + all gradients, {wl.n_sites} sites x {t.num_nodes() - 1} branches) "
-                      f"after 1 warm-up, median {med:.3f} s"}
+            "sample": f"{reps} {what} (lnL + all gradients, x {t.num_nodes() - 1} branches) after 1 warm-up, "
+                      f"median {med:.3f} s"}
 
 
 def run_reference(args) -> None:
@@ -229,7 +247,7 @@ def run_ours(args) -> None:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    h, wl, aln, tree = build_inputs(seed_offset=rank)
+    h, wl, aln, tree = build_inputs(seed_offset=rank, config=args.config)
     from hyphy3 import _capi
     precision = args.precision
     if precision == "auto":
@@ -266,7 +284,8 @@ def run_ours(args) -> None:
     def install(prec):
         pr.set_model(pi=aln.codon_frequencies, Q=np.stack([e["Q"] for e in es]), lam=np.stack([e["lam"] for e in es]),
                      U=np.stack([e["U"] for e in es]), V=np.stack([e["V"] for e in es]),
-                     mu=np.array([e["mu"] for e in es]), class_w=wl.omega_w, dQ=dirs, precision=prec)
+                     mu=np.array([e["mu"] for e in es]), class_w=wl.omega_w, rates=list(wl.rates),
+                     rate_w=list(wl.rate_w), dQ=dirs, precision=prec)
         pr.stage_branch_lengths(bl)
 
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -314,14 +333,15 @@ def run_ours(args) -> None:
     # end to end through the public API, host buffers in and out
     h.set_precision(precision)
     bl_list = list(bl)
+    api_args = (tree, aln, base, bl_list, wl.omegas, wl.omega_w, list(wl.rates), list(wl.rate_w))
     for _ in range(max(args.warmup, 3)):
-        r_api = h.compute_mixture_gradients(tree, aln, base, bl_list, wl.omegas, wl.omega_w)
+        r_api = h.compute_mixture_gradients(*api_args)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r_api = h.compute_mixture_gradients(tree, aln, base, bl_list, wl.omegas, wl.omega_w)
+        r_api = h.compute_mixture_gradients(*api_args)
     e2e_secs = time.perf_counter() - t0
     et = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
     if dist:
@@ -340,7 +360,8 @@ def run_ours(args) -> None:
 
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    work = stage_work(aln.num_patterns, tree, 1)
+    work = stage_work(aln.num_patterns, tree, len(wl.rates), 4 if precision == "mixed" else 8)
+    work64 = stage_work(aln.num_patterns, tree, len(wl.rates), 8)
     stg = head["stages"]
     dom = max(("inside", "outside", "accum_A"), key=lambda k: stg.get(k, (0.0, 0))[0])
     dom_ms, dom_launches = stg[dom]
@@ -354,16 +375,17 @@ def run_ours(args) -> None:
     fp64_pipe = {}
     for k in ("inside", "outside", "accum_A"):
         if k in f_st and f_st[k][0] > 0:
-            fl = work[k][1] / (f_st[k][0] * 1e-3) / 1e12
+            fl = work64[k][1] / (f_st[k][0] * 1e-3) / 1e12
             fp64_pipe[k] = {"tflops": fl, "frac_of_dgemm": fl / fp64_peak if fp64_peak else None, "ms": f_st[k][0]}
 
-    cpu = cpu_baseline(wl) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    cpu = (cpu_baseline(wl, max_sites=None if args.config == 1 else 24)
+           if (rank == 0 and world == 1 and not args.no_cpu) else None)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if precision == "fp64" else "tf32x3/f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sites": wl.n_sites, "branches": n - 1, "patterns": aln.num_patterns,
+            "config": {"workload": WORKLOADS[args.config], "sites": wl.n_sites, "branches": n - 1, "patterns": aln.num_patterns,
                        "precision": precision, "l2": "flushed (256 MiB write) before every timed step",
                        "parallelism": f"replicas{world}" if world > 1 else "single"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -429,6 +451,40 @@ def _directions(aln, wl, es):
     return np.stack(out)
 
 
+def run_profile(args) -> None:
+    """Evaluations only (no CPU leg, no API leg, no clock sampling): the command ncu captures."""
+    import torch
+    h, wl, aln, tree = build_inputs(config=args.config)
+    from hyphy3 import _capi
+    ctx = _capi.Context(0)
+    states, masks, weights = aln.pattern_arrays()
+    l2t = h.build_leaf_to_taxon_map(tree, aln)
+    n = tree.num_nodes()
+    is_leaf = np.array([nd.is_leaf for nd in tree.nodes], dtype=np.uint8)
+    pr = _capi.Problem(ctx, np.array(tree.parents, dtype=np.int32), is_leaf,
+                       np.array([l2t[i] if is_leaf[i] else -1 for i in range(n)], dtype=np.int32), states, masks, weights)
+    es = []
+    for om in wl.omegas:
+        p = h.MG94Parameters()
+        p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = wl.theta
+        p.beta = om
+        es.append(h.mg94_eigensystem(aln, p))
+    prec = _capi.PREC_FP64 if args.precision == "fp64" else _capi.PREC_MIXED
+    pr.set_model(pi=aln.codon_frequencies, Q=np.stack([e["Q"] for e in es]), lam=np.stack([e["lam"] for e in es]),
+                 U=np.stack([e["U"] for e in es]), V=np.stack([e["V"] for e in es]), mu=np.array([e["mu"] for e in es]),
+                 class_w=wl.omega_w, rates=list(wl.rates), rate_w=list(wl.rate_w), dQ=_directions(aln, wl, es),
+                 precision=prec)
+    pr.stage_branch_lengths(np.array(tree.get_branch_lengths()))
+    want = _capi.WANT_LNL | _capi.WANT_GRAD_T | _capi.WANT_GRAD_GLOBAL
+    for _ in range(args.warmup + args.steps):
+        pr.eval_resident(want)
+    r = pr.read_result(want)
+    torch.cuda.synchronize()
+    print(f"profile run: precision={args.precision} lnL={r['lnl']:.6f} launches/eval={pr.last_stats()[1]}")
+    pr.close()
+    ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -437,8 +493,13 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["auto", "fp64", "mixed"], default="auto")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile", action="store_true", help="device evaluations only (for ncu)")
+    ap.add_argument("--config", type=int, choices=[1, 3], default=1,
+                    help="1: 64-taxon 3-omega mixture (headline); 3: 1024-taxon, 4 rate x 2 omega classes")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -332,9 +332,10 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     H3G_TRY_CUDA(ctx, A.alloc(&w.Eown, NI * M * Pp));
     H3G_TRY_CUDA(ctx, A.alloc(&w.gt, size_t(M) * n));
     H3G_TRY_CUDA(ctx, A.alloc(&w.Apart, n * M * size_t(w.nchunk) * SP2));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Afull, n * M * SP2));
     H3G_TRY_CUDA(ctx, A.alloc(&w.Hpart, size_t(nmod) * M * n * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * n));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * n));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * n * 4));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * n * 4));
     H3G_TRY_CUDA(ctx, A.alloc(&w.H, size_t(nmod) * SP2));
     H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 4));
     const size_t n_out = 2 + n + K + nmod + M;
@@ -350,8 +351,8 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
         h3g_status st = mixed_alloc(pr->mw, A.ptrs, pr->n, pr->NI, M, pr->Pp);
         if (st != H3G_OK) return fail(ctx, st, "mixed-precision workspace allocation failed");
     }
-    cudaMemsetAsync(w.gc, 0, size_t(std::max(K, 1)) * M * n * sizeof(double), ctx->stream);
-    cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * n * sizeof(double), ctx->stream);
+    cudaMemsetAsync(w.gc, 0, size_t(std::max(K, 1)) * M * n * 4 * sizeof(double), ctx->stream);
+    cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * n * 4 * sizeof(double), ctx->stream);
     cudaMemsetAsync(w.Hpart, 0, size_t(nmod) * M * n * SP2 * sizeof(double), ctx->stream);
     pr->off_out = n;
     pr->off_dir = pr->off_out + n_out;

@@ -73,10 +73,11 @@ struct Work {
     double* rw;              // [M][Pp]   w_p * post_{m,p} / rho_m
     int nchunk, chunk;
     double* Apart;           // [n][M][nchunk][64*64]
+    double* Afull;           // [n][M][64*64] A_{m,b} summed over chunks
     double* gt;              // [M][n]    <A_{m,b}, dP_{m,b}>
     double* Hpart;           // [nmod][M][n][64*64]
-    double* gc;              // [K][M][n] <A_{m,b}, P_k(tau)>
-    double* stg;             // [nmod][M][n] c_k * tau * <A_{m,b}, Q_k P_k(tau)>
+    double* gc;              // [K][M][n][4] <A_{m,b}, P_k(tau)> per row block
+    double* stg;             // [nmod][M][n][4] c_k * tau * <A_{m,b}, Q_k P_k(tau)> per row block
     double* H;               // [nmod][64*64]
     double* dirpart;         // [ndirs][nmod][4] row-block partials
     double* out;             // [2 + n + K + nmod + M] lnl | error flag | grad_t | gc | stg | grad_rate_w

@@ -84,17 +84,17 @@ __device__ __forceinline__ void stage_matrix(double* __restrict__ s, const doubl
 
 // ------------------------------------------------------------------ build P
 // grid (n, M, 4): CTA z owns columns [16z, 16z+16) of P_{m,b} and dP_{m,b}.
-// Each of the 256 threads owns 4 entries (row r, columns c0..c0+3).
+// Thread (r = tid % 64, cg = tid / 64) owns row r, columns 16z + 4cg .. +3.
+// U_k and Q_k are staged transposed so consecutive threads read consecutive rows.
 __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
     extern __shared__ __align__(16) double sm[];
-    double* sU = sm;                 // U_k (64 x 64), later Q_k
-    double* sV = sm + SP2;           // V_k columns of this block (64 x 16)
+    double* sT = sm;                 // U_k^T, later Q_k^T (sT[l * 65 + r]; padded against bank conflicts)
+    double* sV = sm + SP * (SP + 1); // V_k columns of this block (64 x 16)
     double* sPk = sV + SP * 16;      // clamp(P_k) columns of this block (64 x 16)
     __shared__ double se[SP];
     const int b = blockIdx.x, m = blockIdx.y, cb = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
-    const int r = tid >> 2, c0 = (tid & 3) * 4;       // local columns c0..c0+3 of the block
-    const int col0 = cb * 16;
+    const int r = tid & 63, c0 = (tid >> 6) * 4;
     const bool test = md.is_test == nullptr || md.is_test[b] != 0;
     const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
     double accP[4] = {0, 0, 0, 0}, accD[4] = {0, 0, 0, 0};
@@ -104,42 +104,46 @@ __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
         const double rate = md.rates[m];
         const double tau = rate * w.bl[b] * cv;
         __syncthreads();
-        stage_matrix(sU, md.U + size_t(k) * SP2, tid, 256);
-        for (int e = tid; e < SP * 16; e += 256) sV[e] = md.V[size_t(k) * SP2 + (e >> 4) * SP + col0 + (e & 15)];
+        for (int e = tid; e < SP2; e += 256) sT[(e & 63) * (SP + 1) + (e >> 6)] = md.U[size_t(k) * SP2 + e];
+        for (int e = tid; e < SP * 16; e += 256) sV[e] = md.V[size_t(k) * SP2 + (e >> 4) * SP + cb * 16 + (e & 15)];
         if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
         __syncthreads();
         double pk[4] = {0, 0, 0, 0};
+#pragma unroll 4
         for (int l = 0; l < SP; ++l) {
-            const double u = sU[r * SP + l] * se[l];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) pk[q] = fma(u, sV[l * 16 + c0 + q], pk[q]);
+            const double u = sT[l * (SP + 1) + r] * se[l];
+            const double2 v01 = *reinterpret_cast<const double2*>(sV + l * 16 + c0);
+            const double2 v23 = *reinterpret_cast<const double2*>(sV + l * 16 + c0 + 2);
+            pk[0] = fma(u, v01.x, pk[0]); pk[1] = fma(u, v01.y, pk[1]);
+            pk[2] = fma(u, v23.x, pk[2]); pk[3] = fma(u, v23.y, pk[3]);
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) pk[q] = fmax(pk[q], 0.0);
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < 4; ++q) sPk[r * 16 + c0 + q] = pk[q];
-        stage_matrix(sU, md.Q + size_t(k) * SP2, tid, 256);
+        for (int e = tid; e < SP2; e += 256) sT[(e & 63) * (SP + 1) + (e >> 6)] = md.Q[size_t(k) * SP2 + e];
         __syncthreads();
         double qp[4] = {0, 0, 0, 0};
+#pragma unroll 4
         for (int l = 0; l < SP; ++l) {
-            const double qq = sU[r * SP + l];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) qp[q] = fma(qq, sPk[l * 16 + c0 + q], qp[q]);
+            const double qq = sT[l * (SP + 1) + r];
+            const double2 p01 = *reinterpret_cast<const double2*>(sPk + l * 16 + c0);
+            const double2 p23 = *reinterpret_cast<const double2*>(sPk + l * 16 + c0 + 2);
+            qp[0] = fma(qq, p01.x, qp[0]); qp[1] = fma(qq, p01.y, qp[1]);
+            qp[2] = fma(qq, p23.x, qp[2]); qp[3] = fma(qq, p23.y, qp[3]);
         }
         const double sc = cw * rate * cv;
 #pragma unroll
         for (int q = 0; q < 4; ++q) { accP[q] = fma(cw, pk[q], accP[q]); accD[q] = fma(sc, qp[q], accD[q]); }
     }
-    double* P = w.P + mat_off(m, b, t.n);
-    double* PT = w.PT + mat_off(m, b, t.n);
-    double* dP = w.dP + mat_off(m, b, t.n);
+    const size_t o = mat_off(m, b, t.n);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const int c = col0 + c0 + q;
-        P[r * SP + c] = accP[q];
-        PT[c * SP + r] = accP[q];
-        dP[r * SP + c] = accD[q];
+        const int col = cb * 16 + c0 + q;
+        w.P[o + r * SP + col] = accP[q];
+        w.PT[o + col * SP + r] = accP[q];
+        w.dP[o + r * SP + col] = accD[q];
     }
 }
 
@@ -147,9 +151,9 @@ __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
 __global__ void k_rowsum(Topo t, Model md, Work w) {
     const int b = blockIdx.x, m = blockIdx.y, r = threadIdx.x;
     if (b == t.root) return;
-    const double* P = w.P + mat_off(m, b, t.n) + r * SP;
+    const double* PT = w.PT + mat_off(m, b, t.n) + r;
     double s = 0.0;
-    for (int j = 0; j < SP; ++j) s += P[j];
+    for (int j = 0; j < SP; ++j) s += PT[j * SP];     // sum_j P[r][j], read along PT rows
     w.rs[(size_t(m) * t.n + b) * SP + r] = s;
 }
 
@@ -462,83 +466,93 @@ __device__ __forceinline__ double block_sum_256(double x, double* red) {
     return s;   // valid on thread 0
 }
 
-// ------------------------------------------------------------------ frechet
-// grid (n, M, max(K,1)): CTA z handles model k = z on a test branch (k = K, z = 0,
-// on a background branch); z = 0 also writes <A, dP>.  block 256, dynamic smem 3 * 64 * 64 doubles.
-__global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int want_global) {
-    extern __shared__ __align__(16) double sm[];
-    double* sA = sm;
-    double* sB = sm + SP2;
-    double* sT = sm + 2 * SP2;
+// A_{m,b} = sum of the chunk partials in chunk order, and dlnL/dt_b's term
+// <A_{m,b}, dP_{m,b}>.  grid (n, M), block 256.
+__global__ void __launch_bounds__(256) k_areduce(Topo t, Model md, Work w) {
     __shared__ double red[8];
-    __shared__ double se[SP];
-    const int b = blockIdx.x, m = blockIdx.y, z = blockIdx.z, tid = threadIdx.x, n = t.n, M = md.M;
+    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x, n = t.n, M = md.M;
     if (b == t.root) return;
-    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-    const bool has_model = test ? z < md.K : z == 0;
-    if (!(z == 0 || (want_global && has_model))) return;
     const double* Ap = w.Apart + (size_t(b) * M + m) * w.nchunk * SP2;
+    const double* dP = w.dP + mat_off(m, b, n);
+    double* Af = w.Afull + (size_t(b) * M + m) * SP2;
+    double g = 0.0;
     for (int e = tid; e < SP2; e += 256) {
         double s = 0.0;
         for (int ck = 0; ck < w.nchunk; ++ck) s += Ap[size_t(ck) * SP2 + e];
-        sA[e] = s;
+        Af[e] = s;
+        g = fma(s, dP[e], g);
     }
-    __syncthreads();
-    if (z == 0) {
-        const double* dP = w.dP + mat_off(m, b, n);
-        double g = 0.0;
-        for (int e = tid; e < SP2; e += 256) g = fma(sA[e], dP[e], g);
-        g = block_sum_256(g, red);
-        if (tid == 0) w.gt[size_t(m) * n + b] = g;
-    }
+    g = block_sum_256(g, red);
+    if (tid == 0) w.gt[size_t(m) * n + b] = g;
+}
+
+// ------------------------------------------------------------------ frechet
+// grid (n, M, 4 * max(K,1)): CTA (b, m, 4z + rb) handles model k = z on a test
+// branch (k = K, z = 0, on a background branch) and rows [16rb, 16rb+16) of the
+// spectral transform U^T A V^T of the reduced A_{m,b}.
+// block 256, dynamic smem (64*64 + 64*16 + 16*64 + 64*64) doubles.
+__global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int want_global) {
+    extern __shared__ __align__(16) double sm[];
+    double* sA = sm;                 // A_{m,b}
+    double* sUc = sA + SP2;          // U_k[:, rows]  (64 x 16)
+    double* sT = sUc + SP * 16;      // T = U_k[:, rows]^T A  (16 x 64)
+    double* sV = sT + 16 * SP;       // V_k^T, padded rows (sV[l * 65 + c] = V[c][l])
+    __shared__ double red[8];
+    __shared__ double se[SP];
+    const int b = blockIdx.x, m = blockIdx.y, z = blockIdx.z >> 2, rb = blockIdx.z & 3;
+    const int tid = threadIdx.x, n = t.n, M = md.M;
+    if (b == t.root) return;
+    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+    const bool has_model = test ? z < md.K : z == 0;
     if (!want_global || !has_model) return;
+    stage_matrix(sA, w.Afull + (size_t(b) * M + m) * SP2, tid, 256);
     const int k = test ? z : md.K;
-    const int r = tid >> 2, c0 = (tid & 3) * 16;
+    const int r0 = 16 * rb;
     const double cw = test ? md.class_w[k] : 1.0;
     const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
-    __syncthreads();
-    stage_matrix(sB, md.U + size_t(k) * SP2, tid, 256);
+    for (int e = tid; e < SP * 16; e += 256) sUc[e] = md.U[size_t(k) * SP2 + (e >> 4) * SP + r0 + (e & 15)];
+    // V transposed (sV[l][c] = V[c][l]) so that the T V^T loop reads along rows
+    for (int e = tid; e < SP2; e += 256) sV[(e & 63) * (SP + 1) + (e >> 6)] = md.V[size_t(k) * SP2 + e];
     if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
     __syncthreads();
-    // T = U^T A
-    double acc[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    const int r = tid >> 4, c0 = (tid & 15) * 4;   // local row r (0..15), columns c0..c0+3
+    // T[r][c] = sum_l U[l][r0 + r] A[l][c]
+    double acc[4] = {0, 0, 0, 0};
     for (int l = 0; l < SP; ++l) {
-        const double u = sB[l * SP + r];
+        const double u = sUc[l * 16 + r];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma(u, sA[l * SP + c0 + q], acc[q]);
+        for (int q = 0; q < 4; ++q) acc[q] = fma(u, sA[l * SP + c0 + q], acc[q]);
     }
 #pragma unroll
-    for (int q = 0; q < 16; ++q) sT[r * SP + c0 + q] = acc[q];
+    for (int q = 0; q < 4; ++q) sT[r * SP + c0 + q] = acc[q];
     __syncthreads();
-    stage_matrix(sB, md.V + size_t(k) * SP2, tid, 256);
-    __syncthreads();
-    // At = T V^T
+    // At[r][c] = sum_l T[r][l] V[c][l]
 #pragma unroll
-    for (int q = 0; q < 16; ++q) acc[q] = 0.0;
+    for (int q = 0; q < 4; ++q) acc[q] = 0.0;
     for (int l = 0; l < SP; ++l) {
         const double x = sT[r * SP + l];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) acc[q] = fma(x, sB[(c0 + q) * SP + l], acc[q]);
+        for (int q = 0; q < 4; ++q) acc[q] = fma(x, sV[l * (SP + 1) + c0 + q], acc[q]);
     }
     const double* lam = md.lam + size_t(k) * SP;
-    const double li = lam[r], ei = se[r];
+    const int gi = r0 + r;
+    const double li = lam[gi], ei = se[gi];
     double* Hp = w.Hpart + ((size_t(k) * M + m) * n + b) * SP2;
     double dg = 0.0, dq = 0.0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < 4; ++q) {
         const int j = c0 + q;
         const double lj = lam[j], ej = se[j], d = li - lj;
         const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
-        Hp[r * SP + j] = cw * acc[q] * E;
-        if (j == r) { dg = ei * acc[q]; dq = li * ei * acc[q]; }
+        Hp[gi * SP + j] = cw * acc[q] * E;
+        if (j == gi) { dg = ei * acc[q]; dq = li * ei * acc[q]; }
     }
     dg = block_sum_256(dg, red);
     dq = block_sum_256(dq, red);
     if (tid == 0) {
-        if (test) w.gc[(size_t(k) * M + m) * n + b] = dg;
-        w.stg[(size_t(k) * M + m) * n + b] = cw * tau * dq;
+        const size_t o = ((size_t(k) * M + m) * n + b) * 4 + rb;
+        if (test) w.gc[o] = dg;
+        w.stg[o] = cw * tau * dq;
     }
 }
 
@@ -632,8 +646,10 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
             if (b == t.root) continue;
             const bool test = md.is_test == nullptr || md.is_test[b] != 0;
             if ((k < md.K) != test) continue;
-            if (k < md.K) a += w.gc[size_t(k) * M * n + idx];
-            z += w.stg[size_t(k) * M * n + idx];
+            for (int rb = 0; rb < 4; ++rb) {
+                if (k < md.K) a += w.gc[(size_t(k) * M * n + idx) * 4 + rb];
+                z += w.stg[(size_t(k) * M * n + idx) * 4 + rb];
+            }
         }
         a = block_sum_256(a, red);
         z = block_sum_256(z, red);
@@ -653,14 +669,15 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
 // ------------------------------------------------------------------ launch
 static size_t smem_bytes(int mats) { return size_t(mats) * SP2 * sizeof(double); }
 static const size_t kPruneSmem = (SP2 + SP * kTileP + kGroups * kTileP) * sizeof(double);
-static const size_t kBuildSmem = (SP2 + 2 * SP * 16) * sizeof(double);
+static const size_t kBuildSmem = (SP * (SP + 1) + 2 * SP * 16) * sizeof(double);
 static const size_t kDirSmem = (2 * SP2 + 16 * SP) * sizeof(double);
+static const size_t kFrechetSmem = (SP2 + SP * (SP + 1) + 2 * 16 * SP) * sizeof(double);
 
 void fp64_configure() {
     cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
     cudaFuncSetAttribute(k_inside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
     cudaFuncSetAttribute(k_outside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
-    cudaFuncSetAttribute(k_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_bytes(3)));
+    cudaFuncSetAttribute(k_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFrechetSmem));
     cudaFuncSetAttribute(k_dir, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kDirSmem));
 }
 
@@ -690,8 +707,10 @@ int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream
     return 1;
 }
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {
-    k_frechet<<<dim3(t.n, md.M, want_global ? (md.K > 1 ? md.K : 1) : 1), 256, smem_bytes(3), s>>>(t, md, w, want_global);
-    return 1;
+    k_areduce<<<dim3(t.n, md.M), 256, 0, s>>>(t, md, w);
+    if (!want_global) return 1;
+    k_frechet<<<dim3(t.n, md.M, 4 * (md.K > 1 ? md.K : 1)), 256, kFrechetSmem, s>>>(t, md, w, want_global);
+    return 2;
 }
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
     k_hsum<<<dim3(md.nmod, SP2 / 256), 256, 0, s>>>(t, md, w);

@@ -1,9 +1,10 @@
 // h3g_mixed.cu — split-precision pruning on the sm_100a tensor cores.
 //
-// One CTA = 128 patterns x one node (inside) or one child (outside); thread t
-// owns pattern row t, which is also TMEM lane t of the accumulator, so the
-// per-pattern rescaling, the elementwise products with sibling messages and the
-// epilogue all stay in registers of one thread.  The 61x61 contraction is a
+// One CTA = 128 patterns x one node (inside) or one child (outside), 512
+// threads: four threads share each pattern row (16 states each); the row is
+// also TMEM lane r of the accumulator, read back by the warp that owns that
+// lane quadrant.  Per-pattern rescaling combines the four partial maxima
+// through shared memory.  The 61x61 contraction is a
 // tcgen05.mma (M=128 patterns, N=64 states, K=64 states) issued by one thread:
 // A = the CTA's partial tile, written by the threads into shared memory as a
 // K-major BF16 hi/mid/lo triple; B = the branch's P (or P^T) tile, prepared
@@ -24,79 +25,117 @@ constexpr int MT = 128;                       // patterns per CTA = MMA M
 constexpr uint32_t kIdesc = tc::idesc_bf16(MT, SP);
 constexpr size_t kTileBytes = size_t(MT) * SP * 2;       // 16 KB per BF16 term
 constexpr size_t kBBytes = size_t(SP) * SP * 2;          // 8 KB per BF16 term
-constexpr size_t kMxSmem = 3 * kTileBytes + 3 * kBBytes + 64;   // A terms, B terms, barriers
 constexpr int kKSteps = SP / 16;                                 // K = 16 per kind::f16 MMA
 constexpr uint32_t kTmemCols = kKSteps * SP;                     // one 64-column accumulator per K step
 
 __device__ __forceinline__ size_t mat_off_f(int m, int b, int n) { return (size_t(m) * n + b) * SP2; }
 
+// Thread layout of the pruning CTAs: 16 warps; warp w serves TMEM lane quadrant
+// q = w % 4 (patterns 32q .. 32q+31 of the tile, lane = pattern) and state group
+// g = w / 4 (states 16g .. 16g+15).  Four threads share one pattern row.
+constexpr int kThreads = 512;
+constexpr int kSG = 16;                                           // states per thread
+constexpr size_t kMxSmem = 3 * kTileBytes + 3 * kBBytes + 4 * MT * sizeof(float) + 64;
+
+struct Lane {
+    int r;      // row in the tile (pattern), also the TMEM lane
+    int g;      // state group
+    int q;      // lane quadrant
+    int warp;
+};
+__device__ __forceinline__ Lane lane_of(int tid) {
+    Lane l;
+    l.warp = tid >> 5;
+    l.q = l.warp & 3;
+    l.g = l.warp >> 2;
+    l.r = 32 * l.q + (tid & 31);
+    return l;
+}
+
 // Exact power-of-two scale factor 2^k for |k| <= 126.
 __device__ __forceinline__ float pow2f(int k) { return __int_as_float((127 + k) << 23); }
 
-// Normalise v to a maximum in [0.5, 1); returns the shift s (v_new = v * 2^s).
-__device__ __forceinline__ int renorm_row(float (&v)[SP]) {
-    float mx = 0.f;
-#pragma unroll
-    for (int i = 0; i < SP; ++i) mx = fmaxf(mx, v[i]);
-    if (!(mx > 0.f) || !(mx < INFINITY)) return 0;
-    const int sh = -ilogbf(mx) - 1;
+__device__ __forceinline__ void scale_pow2(float (&v)[kSG], int sh) {
     for (int rem = sh; rem != 0;) {
         const int step = rem > 126 ? 126 : (rem < -126 ? -126 : rem);
         const float f = pow2f(step);
 #pragma unroll
-        for (int i = 0; i < SP; ++i) v[i] *= f;
+        for (int i = 0; i < kSG; ++i) v[i] *= f;
         rem -= step;
     }
+}
+
+// Normalise the pattern row (spread over the 4 state groups) to a maximum in
+// [0.5, 1); returns the shift s (v_new = v * 2^s), identical on all 4 threads.
+__device__ __forceinline__ int renorm_row(float (&v)[kSG], float* smax, const Lane& l) {
+    float mx = 0.f;
+#pragma unroll
+    for (int i = 0; i < kSG; ++i) mx = fmaxf(mx, v[i]);
+    smax[l.g * MT + l.r] = mx;
+    __syncthreads();
+    mx = fmaxf(fmaxf(smax[l.r], smax[MT + l.r]), fmaxf(smax[2 * MT + l.r], smax[3 * MT + l.r]));
+    __syncthreads();
+    if (!(mx > 0.f) || !(mx < INFINITY)) return 0;
+    const int sh = -ilogbf(mx) - 1;
+    scale_pow2(v, sh);
     return sh;
 }
 
-// v *= P_c * leaf_vector(c, p) in FP32.
-__device__ __forceinline__ void mul_leaf_row(float (&v)[SP], const Topo& t, const MixedWork& mw, int m, int c, int p) {
+// v *= (P_c * leaf_vector(c, p)) restricted to states 16g .. 16g+15, in FP32.
+__device__ __forceinline__ void mul_leaf(float (&v)[kSG], const Topo& t, const MixedWork& mw, int m, int c, int p, int g) {
     const int tx = t.taxon[c];
     const float* PTc = mw.PT32 + mat_off_f(m, c, t.n);
     const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
     const float* src;
     if (st >= 0) {
-        src = PTc + st * SP;
+        src = PTc + st * SP + kSG * g;
     } else {
         const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * t.Pp + p];
         if (mk == 0 || (mk & t.all_mask) == t.all_mask) {
-            src = mw.rs32 + (size_t(m) * t.n + c) * SP;
+            src = mw.rs32 + (size_t(m) * t.n + c) * SP + kSG * g;
         } else {
+            float acc[kSG];
 #pragma unroll
-            for (int i = 0; i < SP; ++i) {
-                float s = 0.f;
-                for (uint64_t b = mk; b; b &= b - 1) s += __ldg(PTc + (__ffsll((long long)b) - 1) * SP + i);
-                v[i] *= s;
+            for (int i = 0; i < kSG; ++i) acc[i] = 0.f;
+            for (uint64_t b = mk; b; b &= b - 1) {
+                const float4* r4 = reinterpret_cast<const float4*>(PTc + (__ffsll((long long)b) - 1) * SP + kSG * g);
+#pragma unroll
+                for (int q4 = 0; q4 < kSG / 4; ++q4) {
+                    const float4 x = __ldg(r4 + q4);
+                    acc[4 * q4] += x.x; acc[4 * q4 + 1] += x.y; acc[4 * q4 + 2] += x.z; acc[4 * q4 + 3] += x.w;
+                }
             }
+#pragma unroll
+            for (int i = 0; i < kSG; ++i) v[i] *= acc[i];
             return;
         }
     }
     const float4* s4 = reinterpret_cast<const float4*>(src);
 #pragma unroll
-    for (int q = 0; q < SP / 4; ++q) {
-        const float4 x = __ldg(s4 + q);
-        v[4 * q] *= x.x; v[4 * q + 1] *= x.y; v[4 * q + 2] *= x.z; v[4 * q + 3] *= x.w;
+    for (int q4 = 0; q4 < kSG / 4; ++q4) {
+        const float4 x = __ldg(s4 + q4);
+        v[4 * q4] *= x.x; v[4 * q4 + 1] *= x.y; v[4 * q4 + 2] *= x.z; v[4 * q4 + 3] *= x.w;
     }
 }
 
-__device__ __forceinline__ void load_col(float (&v)[SP], const float* src, size_t stride) {
+__device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
-    for (int i = 0; i < SP; ++i) v[i] = src[i * stride];
+    for (int i = 0; i < kSG; ++i) v[i] = src[i * stride];
 }
-__device__ __forceinline__ void mul_col(float (&v)[SP], const float* src, size_t stride) {
+__device__ __forceinline__ void mul_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
-    for (int i = 0; i < SP; ++i) v[i] *= src[i * stride];
+    for (int i = 0; i < kSG; ++i) v[i] *= src[i * stride];
 }
-__device__ __forceinline__ void store_col(const float (&v)[SP], float* dst, size_t stride) {
+__device__ __forceinline__ void store_part(const float (&v)[kSG], float* dst, size_t stride) {
 #pragma unroll
-    for (int i = 0; i < SP; ++i) dst[i * stride] = v[i];
+    for (int i = 0; i < kSG; ++i) dst[i * stride] = v[i];
 }
 
 // Shared-memory block of one tensor-core contraction.
 struct TcTile {
     unsigned char* A[3];   // BF16 hi / mid / lo of the CTA's 128 x 64 partial tile
     unsigned char* B[3];   // BF16 hi / mid / lo of the 64 x 64 transition tile
+    float* smax;           // [4][128] per-group row maxima
     uint64_t* bars;        // [0] B tile arrival, [1] MMA completion
     uint32_t* slot;        // TMEM base address written by tcgen05.alloc
 };
@@ -105,7 +144,8 @@ __device__ __forceinline__ TcTile carve(unsigned char* sm) {
     TcTile s;
     for (int q = 0; q < 3; ++q) s.A[q] = sm + q * kTileBytes;
     for (int q = 0; q < 3; ++q) s.B[q] = sm + 3 * kTileBytes + q * kBBytes;
-    s.bars = reinterpret_cast<uint64_t*>(sm + 3 * kTileBytes + 3 * kBBytes);
+    s.smax = reinterpret_cast<float*>(sm + 3 * kTileBytes + 3 * kBBytes);
+    s.bars = reinterpret_cast<uint64_t*>(s.smax + 4 * MT);
     s.slot = reinterpret_cast<uint32_t*>(s.bars + 2);
     return s;
 }
@@ -128,11 +168,10 @@ __device__ __forceinline__ void tc_begin(const TcTile& s, uint16_t* const (&b)[3
     }
 }
 
-// Write this thread's row (64 FP32 values) into the K-major A tiles as a BF16 split.
-__device__ __forceinline__ void tc_write_row(const TcTile& s, const float (&v)[SP]) {
-    const int r = threadIdx.x;
+// Write this thread's 16 states of its row into the K-major A tiles as a BF16 split.
+__device__ __forceinline__ void tc_write_part(const TcTile& s, const float (&v)[kSG], const Lane& l) {
 #pragma unroll
-    for (int kc = 0; kc < SP / 8; ++kc) {
+    for (int kc = 0; kc < kSG / 8; ++kc) {
         uint32_t w[3][4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -142,16 +181,17 @@ __device__ __forceinline__ void tc_write_row(const TcTile& s, const float (&v)[S
             w[1][e] = uint32_t(x0.mid) | (uint32_t(x1.mid) << 16);
             w[2][e] = uint32_t(x0.lo) | (uint32_t(x1.lo) << 16);
         }
-        const uint32_t off = tc::kmajor_off16(MT, r, 8 * kc);
+        const uint32_t off = tc::kmajor_off16(MT, l.r, kSG * l.g + 8 * kc);
 #pragma unroll
         for (int q = 0; q < 3; ++q)
             *reinterpret_cast<uint4*>(s.A[q] + off) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
     }
 }
 
-// out = A * B^T for this thread's row: issue (one thread), wait (all), read TMEM.
-__device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[SP], int* err) {
-    const int tid = threadIdx.x, warp = tid >> 5;
+// out = A * B^T for this thread's row and state group: issue (one thread),
+// wait (all), read the four per-K-step accumulators from TMEM and sum in FP64.
+__device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const Lane& l, int* err) {
+    const int tid = threadIdx.x;
     tc::fence_async_smem();
     tc::tc_fence_before();
     __syncthreads();
@@ -163,8 +203,7 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[SP], int* err
             const uint32_t lboA = (MT / 8) * 128, lboB = (SP / 8) * 128;
             // Each K step accumulates into its own TMEM columns: the five small split
             // products first (their rounding is ~2^-8 below the result), hi*hi last,
-            // so every accumulator takes at most one add at full magnitude; the
-            // four accumulators are summed in FP64 in the epilogue.
+            // so every accumulator takes at most one add at full magnitude.
             const int pa[6] = {1, 2, 0, 1, 0, 0}, pb[6] = {1, 0, 2, 0, 1, 0};   // mm lh hl mh hm hh
 #pragma unroll
             for (int ks = 0; ks < kKSteps; ++ks) {
@@ -182,27 +221,21 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[SP], int* err
     }
     if (!tc::mbar_wait(&s.bars[1], 0) && (tid & 31) == 0) atomicOr(err, 2);
     tc::tc_fence_after();
-    const uint32_t row = tmem + (uint32_t(warp * 32) << 16);
+    const uint32_t row = tmem + (uint32_t(32 * l.q) << 16) + uint32_t(kSG * l.g);
+    float t16[kKSteps][16];
 #pragma unroll
-    for (int c4 = 0; c4 < SP / 16; ++c4) {
-        double acc[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) acc[i] = 0.0;
-#pragma unroll
-        for (int ks = 0; ks < kKSteps; ++ks) {
-            float t16[16];
-            tc::tmem_ld16(row + uint32_t(ks * SP + c4 * 16), t16);
-            tc::tmem_wait_ld();
-#pragma unroll
-            for (int i = 0; i < 16; ++i) acc[i] += double(t16[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < 16; ++i) o[c4 * 16 + i] = float(acc[i]);
-    }
+    for (int ks = 0; ks < kKSteps; ++ks) tc::tmem_ld16(row + uint32_t(ks * SP), t16[ks]);
     tc::tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < kSG; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < kKSteps; ++ks) acc += double(t16[ks][i]);
+        o[i] = float(acc);
+    }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    if (l.warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
 // ------------------------------------------------------------ P preparation
@@ -230,40 +263,42 @@ __global__ void __launch_bounds__(256) k_prep_mx(Topo t, Model md, Work w, Mixed
 }
 
 // ------------------------------------------------------------------ inside
-// grid (Pp/128, nodes in level, M), block 128.
-__global__ void __launch_bounds__(MT) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ nodes) {
+// grid (Pp/128, nodes in level, M), block 512.
+__global__ void __launch_bounds__(kThreads) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ nodes) {
     extern __shared__ __align__(1024) unsigned char smraw[];
     const TcTile s = carve(smraw);
-    const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
-    const int p = blockIdx.x * MT + tid;
+    const Lane l = lane_of(threadIdx.x);
+    const int u = nodes[blockIdx.y], m = blockIdx.z;
+    const int p = blockIdx.x * MT + l.r;
     const int iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
+    const size_t so = size_t(kSG * l.g) * Pp + p;     // this thread's first state of the pattern column
     const bool root = u == t.root;
     if (!root) tc_begin(s, mw.Bp, mat_off_f(m, u, t.n));
-    float v[SP];
+    float v[kSG];
 #pragma unroll
-    for (int i = 0; i < SP; ++i) v[i] = i < t.S ? 1.f : 0.f;
+    for (int i = 0; i < kSG; ++i) v[i] = (kSG * l.g + i) < t.S ? 1.f : 0.f;
     int E = 0;
     for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
         const int c = t.ch[k];
         if (t.leaf[c]) {
-            mul_leaf_row(v, t, mw, m, c, p);
+            mul_leaf(v, t, mw, m, c, p, l.g);
         } else {
             const int ic = t.iidx[c];
-            mul_col(v, mw.Ms + part_off(ic, m, M, t.Pp) + p, Pp);
+            mul_part(v, mw.Ms + part_off(ic, m, M, t.Pp) + so, Pp);
             E += mw.EM[col_off(ic, m, M, t.Pp) + p];
         }
-        E += renorm_row(v);
+        E += renorm_row(v, s.smax, l);
     }
-    store_col(v, mw.D + part_off(iu, m, M, t.Pp) + p, Pp);
-    mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
+    store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
+    if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
     if (root) return;
-    tc_write_row(s, v);
-    float o[SP];
-    tc_run(s, o, w.err);
-    const int sh = renorm_row(o);
-    store_col(o, mw.Ms + part_off(iu, m, M, t.Pp) + p, Pp);
-    mw.EM[col_off(iu, m, M, t.Pp) + p] = E + sh;
+    tc_write_part(s, v, l);
+    float o[kSG];
+    tc_run(s, o, l, w.err);
+    const int sh = renorm_row(o, s.smax, l);
+    store_part(o, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
+    if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E + sh;
 }
 
 // --------------------------------------------------------------------- root
@@ -308,64 +343,92 @@ __global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
 }
 
 // ------------------------------------------------------------------ outside
-// grid (Pp/128, children in level, M), block 128.
-__global__ void __launch_bounds__(MT) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ kids) {
+// grid (Pp/128, children in level, M), block 512.
+__global__ void __launch_bounds__(kThreads) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ kids) {
     extern __shared__ __align__(1024) unsigned char smraw[];
     const TcTile s = carve(smraw);
-    const int c = kids[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
-    const int p = blockIdx.x * MT + tid;
+    const Lane l = lane_of(threadIdx.x);
+    const int c = kids[blockIdx.y], m = blockIdx.z;
+    const int p = blockIdx.x * MT + l.r;
     const int u = t.parent[c], iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
+    const size_t so = size_t(kSG * l.g) * Pp + p;
     const bool internal = !t.leaf[c];
     if (internal) tc_begin(s, mw.Bpt, mat_off_f(m, c, t.n));
-    float v[SP];
+    float v[kSG];
     int EV = 0;
     if (u == t.root) {
 #pragma unroll
-        for (int i = 0; i < SP; ++i) v[i] = float(md.pi[i]);
-        EV = renorm_row(v);
+        for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
+        EV = renorm_row(v, s.smax, l);
     } else {
-        load_col(v, mw.U + part_off(iu, m, M, t.Pp) + p, Pp);
+        load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
         EV = mw.EU[col_off(iu, m, M, t.Pp) + p];
     }
     for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
         const int sb = t.ch[k];
         if (sb == c) continue;
         if (t.leaf[sb]) {
-            mul_leaf_row(v, t, mw, m, sb, p);
+            mul_leaf(v, t, mw, m, sb, p, l.g);
         } else {
-            mul_col(v, mw.Ms + part_off(t.iidx[sb], m, M, t.Pp) + p, Pp);
+            mul_part(v, mw.Ms + part_off(t.iidx[sb], m, M, t.Pp) + so, Pp);
             EV += mw.EM[col_off(t.iidx[sb], m, M, t.Pp) + p];
         }
-        EV += renorm_row(v);
+        EV += renorm_row(v, s.smax, l);
     }
     // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
     const int ir = t.iidx[t.root];
     const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
     const int EDc = internal ? mw.ED[col_off(t.iidx[c], m, M, t.Pp) + p] : 0;
     const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
-    float* vf = mw.Vf + part_off(c, m, M, t.Pp) + p;
+    float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
 #pragma unroll
-    for (int i = 0; i < SP; ++i) vf[i * Pp] = float(double(v[i]) * scale);
+    for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
     if (!internal) return;
-    tc_write_row(s, v);
-    float o[SP];
-    tc_run(s, o, w.err);
-    const int sh = renorm_row(o);
-    store_col(o, mw.U + part_off(t.iidx[c], m, M, t.Pp) + p, Pp);
-    mw.EU[col_off(t.iidx[c], m, M, t.Pp) + p] = EV + sh;
+    tc_write_part(s, v, l);
+    float o[kSG];
+    tc_run(s, o, l, w.err);
+    const int sh = renorm_row(o, s.smax, l);
+    store_part(o, mw.U + part_off(t.iidx[c], m, M, t.Pp) + so, Pp);
+    if (l.g == 0) mw.EU[col_off(t.iidx[c], m, M, t.Pp) + p] = EV + sh;
 }
 
 // ------------------------------------------------------------------ accum A
 // A_{m,b,chunk} = sum_p Vf D^T with FP32 products and FP32 accumulation inside
-// the chunk; chunks are summed in FP64 afterwards.  grid (n, M, nchunk), block 256.
+// the chunk; chunks are summed in FP64 afterwards.  The next 32-pattern tile is
+// fetched into registers while the current one is multiplied.
+// grid (n, M, nchunk), block 256.
+__device__ __forceinline__ void fetch_ad(const Topo& t, const float* Vb, const float* Db, bool lf, int tx, int p0, int p_end,
+                                         int tid, float (&rv)[8], float (&rd)[8]) {
+    const size_t Pp = size_t(t.Pp);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int e = tid + 256 * q, pp = e & 31, i = e >> 5, p = p0 + pp;
+        const bool in = p < p_end;
+        rv[q] = in ? Vb[i * Pp + p] : 0.f;
+        float d = 0.f;
+        if (in) {
+            if (!lf) {
+                d = Db[i * Pp + p];
+            } else if (i < t.S) {
+                const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
+                if (st >= 0) d = (st == i) ? 1.f : 0.f;
+                else {
+                    const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * Pp + p];
+                    d = (mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> i) & 1)) ? 1.f : 0.f;
+                }
+            }
+        }
+        rd[q] = d;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
     __shared__ __align__(16) float sV[32][SP + 4];
     __shared__ __align__(16) float sD[32][SP + 4];
     const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
     const int M = md.M;
-    const size_t Pp = size_t(t.Pp);
     const int ti = tid & 15, tj = tid >> 4;
     const int p_begin = ck * w.chunk, p_end = min(t.Pp, p_begin + w.chunk);
     const bool lf = t.leaf[b];
@@ -377,27 +440,18 @@ __global__ void __launch_bounds__(256) k_accumA_mx(Topo t, Model md, Work w, Mix
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][c] = 0.f;
+    float rv[8], rd[8];
+    fetch_ad(t, Vb, Db, lf, tx, p_begin, p_end, tid, rv, rd);
     for (int p0 = p_begin; p0 < p_end; p0 += 32) {
-        for (int e = tid; e < 32 * SP; e += 256) {
-            const int pp = e & 31, i = e >> 5, p = p0 + pp;
-            const bool in = p < p_end;
-            sV[pp][i] = in ? Vb[i * Pp + p] : 0.f;
-            float d = 0.f;
-            if (in) {
-                if (!lf) {
-                    d = Db[i * Pp + p];
-                } else if (i < t.S) {
-                    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
-                    if (st >= 0) d = (st == i) ? 1.f : 0.f;
-                    else {
-                        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * Pp + p];
-                        d = (mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> i) & 1)) ? 1.f : 0.f;
-                    }
-                }
-            }
-            sD[pp][i] = d;
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int e = tid + 256 * q;
+            sV[e & 31][e >> 5] = rv[q];
+            sD[e & 31][e >> 5] = rd[q];
         }
         __syncthreads();
+        if (p0 + 32 < p_end) fetch_ad(t, Vb, Db, lf, tx, p0 + 32, p_end, tid, rv, rd);
 #pragma unroll 8
         for (int pp = 0; pp < 32; ++pp) {
             const float4 av = *reinterpret_cast<const float4*>(&sV[pp][4 * ti]);
@@ -408,7 +462,6 @@ __global__ void __launch_bounds__(256) k_accumA_mx(Topo t, Model md, Work w, Mix
 #pragma unroll
                 for (int c = 0; c < 4; ++c) acc[a][c] = fmaf(a4[a], b4[c], acc[a][c]);
         }
-        __syncthreads();
     }
     double* dst = w.Apart + ((size_t(b) * M + m) * w.nchunk + ck) * SP2;
 #pragma unroll
@@ -447,7 +500,7 @@ int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork
     return 1;
 }
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s) {
-    k_inside_mx<<<dim3(t.Pp / MT, count, md.M), MT, kMxSmem, s>>>(t, md, w, mw, d_nodes);
+    k_inside_mx<<<dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s>>>(t, md, w, mw, d_nodes);
     return 1;
 }
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
@@ -455,7 +508,7 @@ int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const Mixed
     return 1;
 }
 int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s) {
-    k_outside_mx<<<dim3(t.Pp / MT, count, md.M), MT, kMxSmem, s>>>(t, md, w, mw, d_kids);
+    k_outside_mx<<<dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s>>>(t, md, w, mw, d_kids);
     return 1;
 }
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {

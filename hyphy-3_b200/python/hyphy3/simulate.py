@@ -54,15 +54,24 @@ def mg94_generator(theta, omega, pos_freq, alpha=1.0):
     return Q, pi / pi.sum()
 
 
+class ReversibleExp:
+    """exp(Q t) for a reversible Q via one symmetrised eigendecomposition."""
+
+    def __init__(self, Q, pi):
+        s = np.sqrt(np.maximum(pi, 1e-12))
+        A = (s[:, None] * Q) / s[None, :]
+        lam, E = np.linalg.eigh(0.5 * (A + A.T))
+        self.lam = np.minimum(lam, 0.0)
+        self.L = E / s[:, None]
+        self.R = E.T * s[None, :]
+
+    def __call__(self, t):
+        return np.maximum(self.L @ (np.exp(self.lam * t)[:, None] * self.R), 0.0)
+
+
 def expm_sym(Q, pi, t):
     """exp(Q t) for a reversible Q via the symmetrised eigenproblem."""
-    s = np.sqrt(np.maximum(pi, 1e-12))
-    A = (s[:, None] * Q) / s[None, :]
-    A = 0.5 * (A + A.T)
-    lam, E = np.linalg.eigh(A)
-    lam = np.minimum(lam, 0.0)
-    P = (E / s[:, None]) @ (np.exp(lam * t)[:, None] * (E.T * s[None, :]))
-    return np.maximum(P, 0.0)
+    return ReversibleExp(Q, pi)(t)
 
 
 @dataclasses.dataclass
@@ -162,6 +171,7 @@ def simulate_alignment(tree: TreeSpec, n_sites: int, rng: np.random.Generator, *
     site_om = rng.choice(len(omegas), size=n_sites, p=np.asarray(omega_w) / np.sum(omega_w))
     site_rt = rng.choice(len(rates), size=n_sites, p=np.asarray(rate_w) / np.sum(rate_w))
     gens = [mg94_generator(theta, om, pos_freq) for om in omegas]
+    exps = [ReversibleExp(Q, pik) for Q, pik in gens]
     pi = gens[0][1]
     states = np.zeros((n, n_sites), dtype=np.int64)
     states[root] = rng.choice(len(pi), size=n_sites, p=pi)
@@ -173,7 +183,7 @@ def simulate_alignment(tree: TreeSpec, n_sites: int, rng: np.random.Generator, *
                 sel = np.flatnonzero((site_om == k) & (site_rt == m))
                 if sel.size == 0:
                     continue
-                cum = np.cumsum(expm_sym(Q, pik, r * tree.length[u]), axis=1)
+                cum = np.cumsum(exps[k](r * tree.length[u]), axis=1)
                 cum /= cum[:, -1:]
                 rows = cum[states[par, sel]]
                 states[u, sel] = np.minimum((rows < u_rand[sel, None]).sum(1), len(pi) - 1)
