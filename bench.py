@@ -52,10 +52,10 @@ WORKLOADS = {
 }
 
 
-def build_inputs(seed_offset: int = 0, config: int = 1):
+def build_inputs(seed_offset: int = 0, config: int = 1, sites: int | None = None):
     import _hyphy3 as h
     from hyphy3.simulate import make_workload
-    wl = make_workload(config)
+    wl = make_workload(config, n_sites=sites)
     if seed_offset:
         # independent replica gene for another rank: same shapes, different draw
         import hyphy3.simulate as sim
@@ -454,7 +454,7 @@ def _directions(aln, wl, es):
 def run_profile(args) -> None:
     """Evaluations only (no CPU leg, no API leg, no clock sampling): the command ncu captures."""
     import torch
-    h, wl, aln, tree = build_inputs(config=args.config)
+    h, wl, aln, tree = build_inputs(config=args.config, sites=args.sites)
     from hyphy3 import _capi
     ctx = _capi.Context(0)
     states, masks, weights = aln.pattern_arrays()
@@ -494,6 +494,7 @@ def main() -> None:
     ap.add_argument("--precision", choices=["auto", "fp64", "mixed"], default="auto")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true", help="device evaluations only (for ncu)")
+    ap.add_argument("--sites", type=int, default=None, help="--profile only: shrink the alignment to this many codons")
     ap.add_argument("--config", type=int, choices=[1, 3], default=1,
                     help="1: 64-taxon 3-omega mixture (headline); 3: 1024-taxon, 4 rate x 2 omega classes")
     args = ap.parse_args()

@@ -75,6 +75,7 @@ struct h3g_problem {
     size_t model_key[5] = {0, 0, 0, 0, 0};
     uint64_t model_hash = 0;
     double *m_pi = nullptr, *m_Q = nullptr, *m_lam = nullptr, *m_U = nullptr, *m_V = nullptr, *m_mu = nullptr;
+    double *m_UT = nullptr, *m_QT = nullptr;
     double *m_cw = nullptr, *m_rt = nullptr, *m_rw = nullptr, *m_dQ = nullptr;
     uint8_t* m_it = nullptr;
     // captured evaluation graphs, keyed by (want, with host copies)
@@ -333,9 +334,12 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     H3G_TRY_CUDA(ctx, A.alloc(&w.gt, size_t(M) * n));
     H3G_TRY_CUDA(ctx, A.alloc(&w.Apart, n * M * size_t(w.nchunk) * SP2));
     H3G_TRY_CUDA(ctx, A.alloc(&w.Afull, n * M * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.Hpart, size_t(nmod) * M * n * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * n * 4));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * n * 4));
+    // Frechet branch groups: about two CTAs per SM over (group, rate class, model)
+    w.ngroups = int(std::max<size_t>(1, std::min<size_t>(n, (296 + size_t(M) * nmod - 1) / (size_t(M) * nmod))));
+    const size_t G = size_t(w.ngroups);
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Hpart, size_t(nmod) * M * G * SP2));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * G));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * G));
     H3G_TRY_CUDA(ctx, A.alloc(&w.H, size_t(nmod) * SP2));
     H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 4));
     const size_t n_out = 2 + n + K + nmod + M;
@@ -351,9 +355,8 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
         h3g_status st = mixed_alloc(pr->mw, A.ptrs, pr->n, pr->NI, M, pr->Pp);
         if (st != H3G_OK) return fail(ctx, st, "mixed-precision workspace allocation failed");
     }
-    cudaMemsetAsync(w.gc, 0, size_t(std::max(K, 1)) * M * n * 4 * sizeof(double), ctx->stream);
-    cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * n * 4 * sizeof(double), ctx->stream);
-    cudaMemsetAsync(w.Hpart, 0, size_t(nmod) * M * n * SP2 * sizeof(double), ctx->stream);
+    cudaMemsetAsync(w.gc, 0, size_t(std::max(K, 1)) * M * G * sizeof(double), ctx->stream);
+    cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * G * sizeof(double), ctx->stream);
     pr->off_out = n;
     pr->off_dir = pr->off_out + n_out;
     pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod * 4;
@@ -418,12 +421,18 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         if (pr->precision != d->precision) { pr->drop_graphs(); pr->work_mem.release(); pr->w = Work{}; }
         pr->precision = d->precision;
         std::vector<double> pi(SP, 0.0), Q(size_t(nm) * SP2), U(size_t(nm) * SP2), V(size_t(nm) * SP2), lam(size_t(nm) * SP, 0.0);
+        std::vector<double> UT(size_t(nm) * SP2), QT(size_t(nm) * SP2);
         std::copy(d->pi, d->pi + S, pi.begin());
         for (int k = 0; k < nm; ++k) {
             pad_matrix(d->Q + size_t(k) * S * S, S, &Q[size_t(k) * SP2]);
             pad_matrix(d->U + size_t(k) * S * S, S, &U[size_t(k) * SP2]);
             pad_matrix(d->V + size_t(k) * S * S, S, &V[size_t(k) * SP2]);
             std::copy(d->lam + size_t(k) * S, d->lam + size_t(k) * S + S, &lam[size_t(k) * SP]);
+            for (int i = 0; i < SP; ++i)
+                for (int j = 0; j < SP; ++j) {
+                    UT[size_t(k) * SP2 + size_t(j) * SP + i] = U[size_t(k) * SP2 + size_t(i) * SP + j];
+                    QT[size_t(k) * SP2 + size_t(j) * SP + i] = Q[size_t(k) * SP2 + size_t(i) * SP + j];
+                }
         }
         std::vector<double> mu(nm, 1.0);
         if (d->mu) std::copy(d->mu, d->mu + nm, mu.begin());
@@ -442,6 +451,8 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_Q, Q.size()));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_lam, lam.size()));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_U, U.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_UT, UT.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_QT, QT.size()));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_V, V.size()));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_mu, mu.size()));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_cw, d->K));
@@ -456,6 +467,8 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_Q, Q.data(), Q.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_lam, lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_U, U.data(), U.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_UT, UT.data(), UT.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_QT, QT.data(), QT.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_V, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_mu, mu.data(), mu.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_cw, d->class_w, d->K * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -467,6 +480,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         md.M = d->M; md.K = d->K; md.has_bg = d->has_bg; md.nmod = nm; md.time_mode = d->time_mode; md.ndirs = d->n_dirs;
         md.sentinel = d->zero_l_sentinel;
         md.pi = pr->m_pi; md.Q = pr->m_Q; md.lam = pr->m_lam; md.U = pr->m_U; md.V = pr->m_V; md.mu = pr->m_mu;
+        md.UT = pr->m_UT; md.QT = pr->m_QT;
         md.class_w = pr->m_cw; md.rates = pr->m_rt; md.rate_w = pr->m_rw; md.is_test = d->is_test ? pr->m_it : nullptr;
         md.dQ = pr->m_dQ;
         if (std::memcmp(&md, &pr->md, sizeof(Model)) != 0) pr->drop_graphs();

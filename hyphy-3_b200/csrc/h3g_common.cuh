@@ -44,8 +44,10 @@ struct Model {
     int M, K, has_bg, nmod, time_mode, ndirs, sentinel;
     const double* pi;        // [64]
     const double* Q;         // [nmod][64*64]
+    const double* QT;        // [nmod][64*64] transpose of Q
     const double* lam;       // [nmod][64]
     const double* U;         // [nmod][64*64]
+    const double* UT;        // [nmod][64*64] transpose of U
     const double* V;         // [nmod][64*64]
     const double* mu;        // [nmod]
     const double* class_w;   // [K]
@@ -75,9 +77,10 @@ struct Work {
     double* Apart;           // [n][M][nchunk][64*64]
     double* Afull;           // [n][M][64*64] A_{m,b} summed over chunks
     double* gt;              // [M][n]    <A_{m,b}, dP_{m,b}>
-    double* Hpart;           // [nmod][M][n][64*64]
-    double* gc;              // [K][M][n][4] <A_{m,b}, P_k(tau)> per row block
-    double* stg;             // [nmod][M][n][4] c_k * tau * <A_{m,b}, Q_k P_k(tau)> per row block
+    int ngroups;             // branch groups G of the Frechet kernel
+    double* Hpart;           // [nmod][M][G][64*64] per-CTA partial H
+    double* gc;              // [K][M][G] <A_{m,b}, P_k(tau)> summed over a branch group
+    double* stg;             // [nmod][M][G] c_k * tau * <A_{m,b}, Q_k P_k(tau)> summed over a branch group
     double* H;               // [nmod][64*64]
     double* dirpart;         // [ndirs][nmod][4] row-block partials
     double* out;             // [2 + n + K + nmod + M] lnl | error flag | grad_t | gc | stg | grad_rate_w

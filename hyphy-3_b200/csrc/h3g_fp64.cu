@@ -487,86 +487,115 @@ __global__ void __launch_bounds__(256) k_areduce(Topo t, Model md, Work w) {
 }
 
 // ------------------------------------------------------------------ frechet
-// grid (n, M, 4 * max(K,1)): CTA (b, m, 4z + rb) handles model k = z on a test
-// branch (k = K, z = 0, on a background branch) and rows [16rb, 16rb+16) of the
-// spectral transform U^T A V^T of the reduced A_{m,b}.
-// block 256, dynamic smem (64*64 + 64*16 + 16*64 + 64*64) doubles.
-__global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int want_global) {
+// grid (G, M, nmod): CTA (g, m, k) walks the branches b = g, g+G, ... that use
+// model k (test branches for k < K, background branches for k = K), computes
+// the spectral transform At = U_k^T A_{m,b} V_k^T and accumulates
+// H += c_k At o E(lambda, tau_b) in registers (likelihood.hpp:1428-1471), plus
+// the diagonal sums for d/dc_k and the d mu term.  Thread t owns the 4x4 block
+// rows 4(t/16).., columns 4(t%16).. of every 64x64 product, so shared-memory
+// reads are consecutive (or broadcast) across a warp.
+// block 256, dynamic smem (64*64 (A) + 64*64 (T^T) + 64*64 (V^T)) doubles; U_k is read through L1.
+__global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G) {
     extern __shared__ __align__(16) double sm[];
-    double* sA = sm;                 // A_{m,b}
-    double* sUc = sA + SP2;          // U_k[:, rows]  (64 x 16)
-    double* sT = sUc + SP * 16;      // T = U_k[:, rows]^T A  (16 x 64)
-    double* sV = sT + 16 * SP;       // V_k^T, padded rows (sV[l * 65 + c] = V[c][l])
-    __shared__ double red[8];
+    double* sA = sm;                  // A_{m,b}
+    double* sTT = sA + SP2;           // (U^T A)^T : sTT[l][r] = T[r][l]
+    double* sVT = sTT + SP2;          // V_k^T : sVT[l][c] = V[c][l]
     __shared__ double se[SP];
-    const int b = blockIdx.x, m = blockIdx.y, z = blockIdx.z >> 2, rb = blockIdx.z & 3;
-    const int tid = threadIdx.x, n = t.n, M = md.M;
-    if (b == t.root) return;
-    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-    const bool has_model = test ? z < md.K : z == 0;
-    if (!want_global || !has_model) return;
-    stage_matrix(sA, w.Afull + (size_t(b) * M + m) * SP2, tid, 256);
-    const int k = test ? z : md.K;
-    const int r0 = 16 * rb;
-    const double cw = test ? md.class_w[k] : 1.0;
-    const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
-    for (int e = tid; e < SP * 16; e += 256) sUc[e] = md.U[size_t(k) * SP2 + (e >> 4) * SP + r0 + (e & 15)];
-    // V transposed (sV[l][c] = V[c][l]) so that the T V^T loop reads along rows
-    for (int e = tid; e < SP2; e += 256) sV[(e & 63) * (SP + 1) + (e >> 6)] = md.V[size_t(k) * SP2 + e];
-    if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
-    __syncthreads();
-    const int r = tid >> 4, c0 = (tid & 15) * 4;   // local row r (0..15), columns c0..c0+3
-    // T[r][c] = sum_l U[l][r0 + r] A[l][c]
-    double acc[4] = {0, 0, 0, 0};
-    for (int l = 0; l < SP; ++l) {
-        const double u = sUc[l * 16 + r];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = fma(u, sA[l * SP + c0 + q], acc[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) sT[r * SP + c0 + q] = acc[q];
-    __syncthreads();
-    // At[r][c] = sum_l T[r][l] V[c][l]
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = 0.0;
-    for (int l = 0; l < SP; ++l) {
-        const double x = sT[r * SP + l];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = fma(x, sV[l * (SP + 1) + c0 + q], acc[q]);
+    __shared__ double red[8];
+    const int g = blockIdx.x, m = blockIdx.y, k = blockIdx.z, tid = threadIdx.x, n = t.n, M = md.M;
+    const int r0 = 4 * (tid >> 4), c0 = 4 * (tid & 15);
+    const double* gU = md.U + size_t(k) * SP2;       // U_k, read through L1
+    for (int e = tid; e < SP2; e += 256) {
+        const int c = e >> 6, l = e & 63;                 // V[c][l], coalesced read
+        sVT[l * SP + c] = md.V[size_t(k) * SP2 + e];
     }
     const double* lam = md.lam + size_t(k) * SP;
-    const int gi = r0 + r;
-    const double li = lam[gi], ei = se[gi];
-    double* Hp = w.Hpart + ((size_t(k) * M + m) * n + b) * SP2;
-    double dg = 0.0, dq = 0.0;
+    double H[4][4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = c0 + q;
-        const double lj = lam[j], ej = se[j], d = li - lj;
-        const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
-        Hp[gi * SP + j] = cw * acc[q] * E;
-        if (j == gi) { dg = ei * acc[q]; dq = li * ei * acc[q]; }
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) H[a][c] = 0.0;
+    double dg = 0.0, dq = 0.0;
+    for (int b = g; b < n; b += G) {
+        if (b == t.root) continue;
+        const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+        if ((k < md.K) != test) continue;
+        const double cw = test ? md.class_w[k] : 1.0;
+        const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
+        __syncthreads();
+        stage_matrix(sA, w.Afull + (size_t(b) * M + m) * SP2, tid, 256);
+        if (tid < SP) se[tid] = exp(lam[tid] * tau);
+        __syncthreads();
+        double acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+        for (int l = 0; l < SP; ++l) {          // T[r][c] = sum_l U[l][r] A[l][c]
+            const double2 u01 = __ldg(reinterpret_cast<const double2*>(gU + l * SP + r0));
+            const double2 u23 = __ldg(reinterpret_cast<const double2*>(gU + l * SP + r0 + 2));
+            const double2 a01 = *reinterpret_cast<const double2*>(sA + l * SP + c0);
+            const double2 a23 = *reinterpret_cast<const double2*>(sA + l * SP + c0 + 2);
+            const double uu[4] = {u01.x, u01.y, u23.x, u23.y}, aa[4] = {a01.x, a01.y, a23.x, a23.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] = fma(uu[a], aa[c], acc[a][c]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) sTT[(c0 + c) * SP + r0 + a] = acc[a][c];
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+        for (int l = 0; l < SP; ++l) {          // At[r][c] = sum_l T[r][l] V[c][l]
+            const double2 t01 = *reinterpret_cast<const double2*>(sTT + l * SP + r0);
+            const double2 t23 = *reinterpret_cast<const double2*>(sTT + l * SP + r0 + 2);
+            const double2 v01 = *reinterpret_cast<const double2*>(sVT + l * SP + c0);
+            const double2 v23 = *reinterpret_cast<const double2*>(sVT + l * SP + c0 + 2);
+            const double tt[4] = {t01.x, t01.y, t23.x, t23.y}, vv[4] = {v01.x, v01.y, v23.x, v23.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] = fma(tt[a], vv[c], acc[a][c]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = r0 + a;
+            const double li = lam[i], ei = se[i];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int j = c0 + c;
+                const double d = li - lam[j], ej = se[j];
+                const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
+                H[a][c] = fma(cw * acc[a][c], E, H[a][c]);
+                if (i == j) { if (test) dg += ei * acc[a][c]; dq += cw * tau * li * ei * acc[a][c]; }
+            }
+        }
     }
+    double* Hp = w.Hpart + ((size_t(k) * M + m) * G + g) * SP2;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) Hp[(r0 + a) * SP + c0 + c] = H[a][c];
     dg = block_sum_256(dg, red);
     dq = block_sum_256(dq, red);
     if (tid == 0) {
-        const size_t o = ((size_t(k) * M + m) * n + b) * 4 + rb;
-        if (test) w.gc[o] = dg;
-        w.stg[o] = cw * tau * dq;
+        const size_t o = (size_t(k) * M + m) * G + g;
+        if (k < md.K) w.gc[o] = dg;
+        w.stg[o] = dq;
     }
 }
 
-// H_k[e] = sum over (m, b) using model k, fixed order.  grid (nmod, 16), block 256.
-__global__ void k_hsum(Topo t, Model md, Work w) {
-    const int k = blockIdx.x, e = blockIdx.y * 256 + threadIdx.x, n = t.n, M = md.M;
+// H_k[e] = sum over (m, g) of the per-CTA partials, fixed order.  grid (nmod, 16), block 256.
+__global__ void k_hsum(Topo t, Model md, Work w, int G) {
+    const int k = blockIdx.x, e = blockIdx.y * 256 + threadIdx.x, M = md.M;
     double s = 0.0;
     for (int m = 0; m < M; ++m)
-        for (int b = 0; b < n; ++b) {
-            if (b == t.root) continue;
-            const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-            if ((k < md.K) != test) continue;
-            s += w.Hpart[((size_t(k) * M + m) * n + b) * SP2 + e];
-        }
+        for (int g = 0; g < G; ++g) s += w.Hpart[((size_t(k) * M + m) * G + g) * SP2 + e];
     w.H[size_t(k) * SP2 + e] = s;
 }
 
@@ -641,15 +670,9 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
     }
     for (int k = 0; k < md.nmod; ++k) {
         double a = 0.0, z = 0.0;
-        for (int idx = tid; idx < M * n; idx += 256) {
-            const int b = idx % n;
-            if (b == t.root) continue;
-            const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-            if ((k < md.K) != test) continue;
-            for (int rb = 0; rb < 4; ++rb) {
-                if (k < md.K) a += w.gc[(size_t(k) * M * n + idx) * 4 + rb];
-                z += w.stg[(size_t(k) * M * n + idx) * 4 + rb];
-            }
+        for (int idx = tid; idx < M * w.ngroups; idx += 256) {
+            if (k < md.K) a += w.gc[size_t(k) * M * w.ngroups + idx];
+            z += w.stg[size_t(k) * M * w.ngroups + idx];
         }
         a = block_sum_256(a, red);
         z = block_sum_256(z, red);
@@ -669,9 +692,9 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
 // ------------------------------------------------------------------ launch
 static size_t smem_bytes(int mats) { return size_t(mats) * SP2 * sizeof(double); }
 static const size_t kPruneSmem = (SP2 + SP * kTileP + kGroups * kTileP) * sizeof(double);
-static const size_t kBuildSmem = (SP * (SP + 1) + 2 * SP * 16) * sizeof(double);
 static const size_t kDirSmem = (2 * SP2 + 16 * SP) * sizeof(double);
-static const size_t kFrechetSmem = (SP2 + SP * (SP + 1) + 2 * 16 * SP) * sizeof(double);
+static const size_t kBuildSmem = (SP * (SP + 1) + 2 * SP * 16) * sizeof(double);
+static const size_t kFrechetSmem = (3 * SP2) * sizeof(double);
 
 void fp64_configure() {
     cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
@@ -709,11 +732,11 @@ int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {
     k_areduce<<<dim3(t.n, md.M), 256, 0, s>>>(t, md, w);
     if (!want_global) return 1;
-    k_frechet<<<dim3(t.n, md.M, 4 * (md.K > 1 ? md.K : 1)), 256, kFrechetSmem, s>>>(t, md, w, want_global);
+    k_frechet<<<dim3(w.ngroups, md.M, md.nmod), 256, kFrechetSmem, s>>>(t, md, w, w.ngroups);
     return 2;
 }
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    k_hsum<<<dim3(md.nmod, SP2 / 256), 256, 0, s>>>(t, md, w);
+    k_hsum<<<dim3(md.nmod, SP2 / 256), 256, 0, s>>>(t, md, w, w.ngroups);
     return 1;
 }
 int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
