@@ -394,80 +394,227 @@ __global__ void __launch_bounds__(kThreads) k_outside_mx(Topo t, Model md, Work 
 }
 
 // ------------------------------------------------------------------ accum A
-// A_{m,b,chunk} = sum_p Vf D^T with FP32 products and FP32 accumulation inside
-// the chunk; chunks are summed in FP64 afterwards.  The next 32-pattern tile is
-// fetched into registers while the current one is multiplied.
-// grid (n, M, nchunk), block 256.
-__device__ __forceinline__ void fetch_ad(const Topo& t, const float* Vb, const float* Db, bool lf, int tx, int p0, int p_end,
-                                         int tid, float (&rv)[8], float (&rd)[8]) {
-    const size_t Pp = size_t(t.Pp);
+// A_{m,b,chunk}[i][j] = sum_p Vf[i][p] D[j][p] on the tensor cores: the K
+// dimension of the MMA is the pattern axis.  Both operands are split into
+// BF16 hi/mid/lo; the V terms are stacked as one 192-row K-major tile
+// [lo | hi | mid], so two M=128 operands cover all six leading products with
+// four MMAs per K step (N = 64 states of D):
+//   acc0 += [hi; mid] x D_hi      rows 0-63: hi*hi   rows 64-127: mid*hi
+//   acc1 += [hi; mid] x D_mid                hi*mid              mid*mid
+//   acc2 += [lo; hi]  x D_hi                 lo*hi               (unused)
+//   acc3 += [lo; hi]  x D_lo                 (unused)            hi*lo
+// A[i][.] = acc0[i] + acc1[i] + acc2[i] + acc0[64+i] + acc1[64+i] + acc3[64+i].
+// Leaf branches have 0/1 leaf vectors (exact in BF16): only acc0 and acc2.
+// Every kADrain tiles the accumulators are drained into FP64 registers, so no
+// FP32 accumulator takes more than 4 * kADrain additions.
+// 64-pattern tiles, two shared-memory stages: the global loads of tile k+1
+// are in flight while the MMAs of tile k run.
+// grid (n, M, nchunk), block 256 (8 warps: lane quadrant w % 4, column half w / 4).
+constexpr int kAT = 64;                                   // patterns per tile (MMA K per tile)
+constexpr int kADrain = 4;                                // tiles per FP32 accumulation group
+constexpr uint32_t kVRows = 3 * SP;                       // stacked V terms
+constexpr uint32_t kVLbo = (kVRows / 8) * 128;            // K-chunk stride in the V stack
+constexpr uint32_t kDLbo = (SP / 8) * 128;                // K-chunk stride in a D term
+constexpr size_t kVStage = size_t(kVRows) * kAT * 2;      // 24 KB
+constexpr size_t kDTerm = size_t(SP) * kAT * 2;           // 8 KB
+constexpr size_t kStage = kVStage + 3 * kDTerm;           // 48 KB
+constexpr size_t kAccSmem = 2 * kStage + 64;
+
+struct Split8 { uint4 hi, mid, lo; };
+__device__ __forceinline__ Split8 split8(const float (&x)[8]) {
+    uint32_t h[4], md[4], lo[4];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int e = tid + 256 * q, pp = e & 31, i = e >> 5, p = p0 + pp;
-        const bool in = p < p_end;
-        rv[q] = in ? Vb[i * Pp + p] : 0.f;
-        float d = 0.f;
-        if (in) {
-            if (!lf) {
-                d = Db[i * Pp + p];
-            } else if (i < t.S) {
-                const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
-                if (st >= 0) d = (st == i) ? 1.f : 0.f;
-                else {
-                    const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * Pp + p];
-                    d = (mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> i) & 1)) ? 1.f : 0.f;
-                }
-            }
+    for (int e = 0; e < 4; ++e) {
+        const tc::Bf16x3 a = tc::split3(x[2 * e]), b = tc::split3(x[2 * e + 1]);
+        h[e] = uint32_t(a.hi) | (uint32_t(b.hi) << 16);
+        md[e] = uint32_t(a.mid) | (uint32_t(b.mid) << 16);
+        lo[e] = uint32_t(a.lo) | (uint32_t(b.lo) << 16);
+    }
+    return {make_uint4(h[0], h[1], h[2], h[3]), make_uint4(md[0], md[1], md[2], md[3]), make_uint4(lo[0], lo[1], lo[2], lo[3])};
+}
+
+// The 8 patterns [p, p+8) of state row j of a leaf's 0/1 vector.
+__device__ __forceinline__ void leaf_row8(const Topo& t, int tx, int j, int p, float (&d)[8]) {
+    if (j >= t.S) {
+#pragma unroll
+        for (int x = 0; x < 8; ++x) d[x] = 0.f;
+        return;
+    }
+    if (tx < 0) {
+#pragma unroll
+        for (int x = 0; x < 8; ++x) d[x] = 1.f;
+        return;
+    }
+    const size_t base = size_t(tx) * t.Pp + p;
+    const uint64_t st8 = __ldg(reinterpret_cast<const unsigned long long*>(t.states + base));
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+        const int st = int(int8_t(uint8_t(st8 >> (8 * x))));
+        bool on;
+        if (st >= 0) {
+            on = st == j;
+        } else {
+            const uint64_t mk = __ldg(reinterpret_cast<const unsigned long long*>(t.masks + base + x));
+            on = mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> j) & 1);
         }
-        rd[q] = d;
+        d[x] = on ? 1.f : 0.f;
     }
 }
 
-__global__ void __launch_bounds__(256) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
-    __shared__ __align__(16) float sV[32][SP + 4];
-    __shared__ __align__(16) float sD[32][SP + 4];
+__global__ void __launch_bounds__(256, 2) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
+    extern __shared__ __align__(1024) unsigned char smraw[];
     const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
-    const int M = md.M;
-    const int ti = tid & 15, tj = tid >> 4;
+    const int M = md.M, warp = tid >> 5, lane = tid & 31;
+    const size_t Pp = size_t(t.Pp);
     const int p_begin = ck * w.chunk, p_end = min(t.Pp, p_begin + w.chunk);
+    const int ntile = (p_end - p_begin) / kAT;
     const bool lf = t.leaf[b];
     const int tx = lf ? t.taxon[b] : -1;
     const float* Vb = mw.Vf + part_off(b, m, M, t.Pp);
     const float* Db = lf ? nullptr : mw.D + part_off(t.iidx[b], m, M, t.Pp);
-    float acc[4][4];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + 2 * kStage);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 2);
+    if (tid == 0) {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        tc::mbar_fence_init();
+    }
+    if (warp == 0) tc::tmem_alloc(slot, 256);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *slot;
+
+    // load items: e = tid + 256 q; state row 8 (e / 64) + e % 8, 8-pattern chunk (e / 8) % 8
+    int row[2], kc[2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int q = 0; q < 2; ++q) {
+        const int e = tid + 256 * q;
+        row[q] = 8 * (e >> 6) + (e & 7);
+        kc[q] = (e >> 3) & 7;
+    }
+    float rv[2][8], rd[2][8];
+    auto fetch = [&](int tile) {
+        const int p0 = p_begin + tile * kAT;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[a][c] = 0.f;
-    float rv[8], rd[8];
-    fetch_ad(t, Vb, Db, lf, tx, p_begin, p_end, tid, rv, rd);
-    for (int p0 = p_begin; p0 < p_end; p0 += 32) {
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int e = tid + 256 * q;
-            sV[e & 31][e >> 5] = rv[q];
-            sD[e & 31][e >> 5] = rd[q];
+        for (int q = 0; q < 2; ++q) {
+            const int p = p0 + 8 * kc[q];
+            const float4* v4 = reinterpret_cast<const float4*>(Vb + size_t(row[q]) * Pp + p);
+            const float4 a = __ldcs(v4), c = __ldcs(v4 + 1);
+            rv[q][0] = a.x; rv[q][1] = a.y; rv[q][2] = a.z; rv[q][3] = a.w;
+            rv[q][4] = c.x; rv[q][5] = c.y; rv[q][6] = c.z; rv[q][7] = c.w;
+            if (lf) {
+                leaf_row8(t, tx, row[q], p, rd[q]);
+            } else {
+                const float4* d4 = reinterpret_cast<const float4*>(Db + size_t(row[q]) * Pp + p);
+                const float4 x = __ldcs(d4), y = __ldcs(d4 + 1);
+                rd[q][0] = x.x; rd[q][1] = x.y; rd[q][2] = x.z; rd[q][3] = x.w;
+                rd[q][4] = y.x; rd[q][5] = y.y; rd[q][6] = y.z; rd[q][7] = y.w;
+            }
         }
+    };
+
+    // drain mapping: TMEM lane quadrant lq (rows 32 lq ..), column half ch
+    const int lq = warp & 3, ch = warp >> 2;
+    const bool top = lq < 2;
+    double dacc[32];
+#pragma unroll
+    for (int x = 0; x < 32; ++x) dacc[x] = 0.0;
+
+    fetch(0);
+    for (int kt = 0; kt < ntile; ++kt) {
+        const int st = kt & 1;
+        unsigned char* VS = smraw + st * kStage;
+        unsigned char* DS = VS + kVStage;
+        if (kt >= 2 && !tc::mbar_wait(&bars[st], uint32_t(((kt - 2) >> 1) & 1)) && lane == 0) atomicOr(w.err, 4);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const uint32_t rg = uint32_t(row[q] >> 3) * 128 + uint32_t(row[q] & 7) * 16;
+            const Split8 sv = split8(rv[q]);
+            *reinterpret_cast<uint4*>(VS + kc[q] * kVLbo + 0 * 1024 + rg) = sv.lo;
+            *reinterpret_cast<uint4*>(VS + kc[q] * kVLbo + 1 * 1024 + rg) = sv.hi;
+            *reinterpret_cast<uint4*>(VS + kc[q] * kVLbo + 2 * 1024 + rg) = sv.mid;
+            if (lf) {
+                uint32_t h[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    h[e] = uint32_t(tc::bf16_bits(rd[q][2 * e])) | (uint32_t(tc::bf16_bits(rd[q][2 * e + 1])) << 16);
+                *reinterpret_cast<uint4*>(DS + kc[q] * kDLbo + rg) = make_uint4(h[0], h[1], h[2], h[3]);
+            } else {
+                const Split8 sd = split8(rd[q]);
+                *reinterpret_cast<uint4*>(DS + kc[q] * kDLbo + rg) = sd.hi;
+                *reinterpret_cast<uint4*>(DS + kDTerm + kc[q] * kDLbo + rg) = sd.mid;
+                *reinterpret_cast<uint4*>(DS + 2 * kDTerm + kc[q] * kDLbo + rg) = sd.lo;
+            }
+        }
+        tc::fence_async_smem();
+        tc::tc_fence_before();
         __syncthreads();
-        if (p0 + 32 < p_end) fetch_ad(t, Vb, Db, lf, tx, p0 + 32, p_end, tid, rv, rd);
-#pragma unroll 8
-        for (int pp = 0; pp < 32; ++pp) {
-            const float4 av = *reinterpret_cast<const float4*>(&sV[pp][4 * ti]);
-            const float4 bv = *reinterpret_cast<const float4*>(&sD[pp][4 * tj]);
-            const float a4[4] = {av.x, av.y, av.z, av.w}, b4[4] = {bv.x, bv.y, bv.z, bv.w};
+        tc::tc_fence_after();
+        if (tid == 0) {
+            const uint32_t vs = tc::smem_u32(VS), ds = tc::smem_u32(DS);
+            const bool first = (kt % kADrain) == 0;
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
+            for (int ks = 0; ks < kAT / 16; ++ks) {
+                const uint32_t acc = (first && ks == 0) ? 0u : 1u;
+                const uint64_t a1 = tc::smem_desc(vs + 1024 + 2 * ks * kVLbo, kVLbo, 128);   // [hi; mid]
+                const uint64_t a2 = tc::smem_desc(vs + 2 * ks * kVLbo, kVLbo, 128);          // [lo; hi]
+                const uint64_t bh = tc::smem_desc(ds + 2 * ks * kDLbo, kDLbo, 128);
+                tc::mma_bf16(tmem + 0, a1, bh, kIdesc, acc);
+                tc::mma_bf16(tmem + 128, a2, bh, kIdesc, acc);
+                if (!lf) {
+                    const uint64_t bm = tc::smem_desc(ds + uint32_t(kDTerm) + 2 * ks * kDLbo, kDLbo, 128);
+                    const uint64_t bl = tc::smem_desc(ds + uint32_t(2 * kDTerm) + 2 * ks * kDLbo, kDLbo, 128);
+                    tc::mma_bf16(tmem + 64, a1, bm, kIdesc, acc);
+                    tc::mma_bf16(tmem + 192, a2, bl, kIdesc, acc);
+                }
+            }
+            tc::mma_commit(&bars[st]);
+        }
+        if (kt + 1 < ntile) fetch(kt + 1);
+        if ((kt % kADrain) == kADrain - 1 || kt == ntile - 1) {
+            if (!tc::mbar_wait(&bars[st], uint32_t((kt >> 1) & 1)) && lane == 0) atomicOr(w.err, 8);
+            tc::tc_fence_after();
+            const uint32_t rowaddr = tmem + (uint32_t(32 * lq) << 16) + uint32_t(32 * ch);
+            // acc0, acc1 (internal branches) and acc2 (top rows) / acc3 (bottom rows, internal branches)
+            const uint32_t cols[3] = {0u, 64u, top ? 128u : 192u};
+            const bool use[3] = {true, !lf, top || !lf};
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[a][c] = fmaf(a4[a], b4[c], acc[a][c]);
+            for (int a = 0; a < 3; ++a) {
+                if (!use[a]) continue;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    float v16[16];
+                    tc::tmem_ld16(rowaddr + cols[a] + 16 * h, v16);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int x = 0; x < 16; ++x) dacc[16 * h + x] += double(v16[x]);
+                }
+            }
+            tc::tc_fence_before();
+            __syncthreads();
+            tc::tc_fence_after();
         }
     }
+    // combine the two halves of each state row in shared memory (stages are idle now), write coalesced
+    double* sA = reinterpret_cast<double*>(smraw);              // [64][65]
+    const int i = 32 * lq + lane - (top ? 0 : 64);
+    if (!top) {
+#pragma unroll
+        for (int x = 0; x < 32; ++x) sA[i * 65 + 32 * ch + x] = dacc[x];
+    }
+    __syncthreads();
+    if (top) {
+#pragma unroll
+        for (int x = 0; x < 32; ++x) sA[i * 65 + 32 * ch + x] += dacc[x];
+    }
+    __syncthreads();
     double* dst = w.Apart + ((size_t(b) * M + m) * w.nchunk + ck) * SP2;
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) dst[(4 * ti + a) * SP + 4 * tj + c] = double(acc[a][c]);
+    for (int e = tid; e < SP2; e += 256) dst[e] = sA[(e >> 6) * 65 + (e & 63)];
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 256);
 }
 
 }  // namespace
@@ -475,6 +622,7 @@ __global__ void __launch_bounds__(256) k_accumA_mx(Topo t, Model md, Work w, Mix
 bool mixed_available() { return true; }
 
 void mixed_configure() {
+    cudaFuncSetAttribute(k_accumA_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAccSmem));
     cudaFuncSetAttribute(k_inside_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMxSmem));
     cudaFuncSetAttribute(k_outside_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMxSmem));
 }
@@ -512,7 +660,7 @@ int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const Mi
     return 1;
 }
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
-    k_accumA_mx<<<dim3(t.n, md.M, w.nchunk), 256, 0, s>>>(t, md, w, mw);
+    k_accumA_mx<<<dim3(t.n, md.M, w.nchunk), 256, kAccSmem, s>>>(t, md, w, mw);
     return 1;
 }
 

@@ -55,6 +55,16 @@ PYBIND11_MODULE(h3oracle, m) {
         .def_static("from_sequences", [](const std::vector<std::string>& names, const std::vector<std::string>& seqs, const std::string& code) {
             Alignment a; a.names = names; a.seqs = seqs; a.finalize(code); return a;
         }, py::arg("names"), py::arg("seqs"), py::arg("code") = "Universal")
+        .def("subset_patterns", [](const Alignment& a, int begin, int end) {
+            // patterns [begin, end) with the full alignment's frequencies (pattern-sharding tests)
+            if (begin < 0 || end > a.P || begin > end) throw std::out_of_range("pattern range");
+            Alignment b = a;
+            b.P = end - begin;
+            b.states.assign(a.states.begin() + size_t(begin) * a.T, a.states.begin() + size_t(end) * a.T);
+            b.masks.assign(a.masks.begin() + size_t(begin) * a.T, a.masks.begin() + size_t(end) * a.T);
+            b.weights.assign(a.weights.begin() + begin, a.weights.begin() + end);
+            return b;
+        }, py::arg("begin"), py::arg("end"))
         .def_readonly("names", &Alignment::names)
         .def_readonly("embedded_tree", &Alignment::embedded_tree)
         .def_readonly("num_taxa", &Alignment::T)
