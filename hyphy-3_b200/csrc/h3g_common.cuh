@@ -21,6 +21,33 @@
 
 namespace h3g {
 
+// Programmatic dependent launch: every evaluation kernel is launched with
+// programmatic stream serialisation, so its CTAs may start while the previous
+// kernel drains.  Each kernel first waits for the previous grid to complete
+// (and its writes to become visible) before touching global memory, then lets
+// the next kernel's CTAs launch into the SM space its own CTAs leave free.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+bool pdl_enabled();   // false when H3G_NO_PDL=1
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 constexpr int SP = 64;       // padded state count (61 sense codons -> 64)
 constexpr int SP2 = SP * SP; // one padded matrix
 constexpr int TP = 128;      // pattern padding granule (the mixed path's CTA tile)

@@ -14,6 +14,7 @@
 //                  (likelihood.hpp:1428-1471)
 //   k_hsum, k_dir, k_small   fixed-order reductions -> lnL, gradients
 // All reductions run in a fixed order, so repeated evaluations are bit-identical.
+#include <cstdlib>
 #include "h3g_common.cuh"
 #include "h3g_kernels.h"
 
@@ -87,6 +88,7 @@ __device__ __forceinline__ void stage_matrix(double* __restrict__ s, const doubl
 // Thread (r = tid % 64, cg = tid / 64) owns row r, columns 16z + 4cg .. +3.
 // U_k and Q_k are staged transposed so consecutive threads read consecutive rows.
 __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
+    pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* sT = sm;                 // U_k^T, later Q_k^T (sT[l * 65 + r]; padded against bank conflicts)
     double* sV = sm + SP * (SP + 1); // V_k columns of this block (64 x 16)
@@ -149,6 +151,7 @@ __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
 
 // Row sums of P_{m,b} (the message of a leaf with missing data).  grid (n, M), block 64.
 __global__ void k_rowsum(Topo t, Model md, Work w) {
+    pdl_enter();
     const int b = blockIdx.x, m = blockIdx.y, r = threadIdx.x;
     if (b == t.root) return;
     const double* PT = w.PT + mat_off(m, b, t.n) + r;
@@ -159,6 +162,7 @@ __global__ void k_rowsum(Topo t, Model md, Work w) {
 
 // Caller-supplied P (compute_tree_log_likelihood_from_P): derive PT and row sums.
 __global__ void k_prep_given_P(Topo t, Work w) {
+    pdl_enter();
     const int b = blockIdx.x, tid = threadIdx.x;
     if (b == t.root) return;
     const double* P = w.P + mat_off(0, b, t.n);
@@ -241,6 +245,7 @@ __device__ __forceinline__ void tile_matvec8(const double* __restrict__ sM, cons
 
 // grid (Pp/32, nodes in level, M), block 256, dynamic smem (64*64 + 64*32 + 8*32) doubles.
 __global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const int* __restrict__ nodes) {
+    pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* sPT = sm;                    // PT_u
     double* sD = sm + SP2;               // D_u tile [64][32]
@@ -290,6 +295,7 @@ __global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const 
 
 // --------------------------------------------------------------------- root
 __global__ void k_root(Topo t, Model md, Work w) {
+    pdl_enter();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= t.Pp) return;
     const int ir = t.iidx[t.root], M = md.M;
@@ -338,6 +344,7 @@ __global__ void k_root(Topo t, Model md, Work w) {
 // V_c = 2^{e_u} U_u o prod_{s != c} (P_s D_s), then U_c = P_c^T V_c for internal c.
 // grid (Pp/32, children in level, M), block 256, dynamic smem (64*64 + 64*32 + 8*32) doubles.
 __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const int* __restrict__ kids, int want_v) {
+    pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* sP = sm;                     // P_c row-major
     double* sV = sm + SP2;               // V_c tile [64][32]
@@ -396,6 +403,7 @@ __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const
 // ------------------------------------------------------------------ accum A
 // A_{m,b,chunk} = sum_{p in chunk} Vf_b[:, p] D_b[:, p]^T.  grid (n, M, nchunk), block 256.
 __global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w) {
+    pdl_enter();
     __shared__ __align__(16) double sV[32][SP + 2];
     __shared__ __align__(16) double sD[32][SP + 2];
     const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
@@ -469,6 +477,7 @@ __device__ __forceinline__ double block_sum_256(double x, double* red) {
 // A_{m,b} = sum of the chunk partials in chunk order, and dlnL/dt_b's term
 // <A_{m,b}, dP_{m,b}>.  grid (n, M), block 256.
 __global__ void __launch_bounds__(256) k_areduce(Topo t, Model md, Work w) {
+    pdl_enter();
     __shared__ double red[8];
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x, n = t.n, M = md.M;
     if (b == t.root) return;
@@ -496,6 +505,7 @@ __global__ void __launch_bounds__(256) k_areduce(Topo t, Model md, Work w) {
 // reads are consecutive (or broadcast) across a warp.
 // block 256, dynamic smem (64*64 (A) + 64*64 (T^T) + 64*64 (V^T)) doubles; U_k is read through L1.
 __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G) {
+    pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* sA = sm;                  // A_{m,b}
     double* sTT = sA + SP2;           // (U^T A)^T : sTT[l][r] = T[r][l]
@@ -592,6 +602,7 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
 
 // H_k[e] = sum over (m, g) of the per-CTA partials, fixed order.  grid (nmod, 16), block 256.
 __global__ void k_hsum(Topo t, Model md, Work w, int G) {
+    pdl_enter();
     const int k = blockIdx.x, e = blockIdx.y * 256 + threadIdx.x, M = md.M;
     double s = 0.0;
     for (int m = 0; m < M; ++m)
@@ -603,6 +614,7 @@ __global__ void k_hsum(Topo t, Model md, Work w, int G) {
 // (V_k dQ U_k) o H_k, minus (block 0, normalized time) dmu/mu * stg_k.
 // grid (ndirs, nmod, 4), block 256, dynamic smem (64*64 + 16*64 + 64*64) doubles.
 __global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
+    pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* sX = sm;                 // dQ, later U_k
     double* sY = sm + SP2;           // (V dQ)[rows, :]
@@ -651,6 +663,7 @@ __global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
 // Fixed-order reductions of the small per-branch / per-pattern partials.
 // One block of 256 threads.
 __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int grads) {
+    pdl_enter();
     __shared__ double red[8];
     const int tid = threadIdx.x, n = t.n, M = md.M;
     // lnL: per-thread Neumaier over a strided slice, then a fixed tree
@@ -705,48 +718,53 @@ void fp64_configure() {
 }
 
 int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    k_build_P<<<dim3(t.n, md.M, 4), 256, kBuildSmem, s>>>(t, md, w);
-    k_rowsum<<<dim3(t.n, md.M), SP, 0, s>>>(t, md, w);
+    launch_k(k_build_P, dim3(t.n, md.M, 4), 256, kBuildSmem, s, t, md, w);
+    launch_k(k_rowsum, dim3(t.n, md.M), SP, 0, s, t, md, w);
     return 2;
 }
 int launch_prep_given_P(const Topo& t, const Work& w, cudaStream_t s) {
-    k_prep_given_P<<<t.n, 256, 0, s>>>(t, w);
+    launch_k(k_prep_given_P, t.n, 256, 0, s, t, w);
     return 1;
 }
 int launch_inside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, cudaStream_t s) {
-    k_inside<<<dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s>>>(t, md, w, d_nodes);
+    launch_k(k_inside, dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s, t, md, w, d_nodes);
     return 1;
 }
 int launch_root(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    k_root<<<(t.Pp + 127) / 128, 128, 0, s>>>(t, md, w);
+    launch_k(k_root, (t.Pp + 127) / 128, 128, 0, s, t, md, w);
     return 1;
 }
 int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_kids, int count, int want_v, cudaStream_t s) {
-    k_outside<<<dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s>>>(t, md, w, d_kids, want_v);
+    launch_k(k_outside, dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s, t, md, w, d_kids, want_v);
     return 1;
 }
 int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    k_accumA<<<dim3(t.n, md.M, w.nchunk), 256, 0, s>>>(t, md, w);
+    launch_k(k_accumA, dim3(t.n, md.M, w.nchunk), 256, 0, s, t, md, w);
     return 1;
 }
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {
-    k_areduce<<<dim3(t.n, md.M), 256, 0, s>>>(t, md, w);
+    launch_k(k_areduce, dim3(t.n, md.M), 256, 0, s, t, md, w);
     if (!want_global) return 1;
-    k_frechet<<<dim3(w.ngroups, md.M, md.nmod), 256, kFrechetSmem, s>>>(t, md, w, w.ngroups);
+    launch_k(k_frechet, dim3(w.ngroups, md.M, md.nmod), 256, kFrechetSmem, s, t, md, w, w.ngroups);
     return 2;
 }
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    k_hsum<<<dim3(md.nmod, SP2 / 256), 256, 0, s>>>(t, md, w, w.ngroups);
+    launch_k(k_hsum, dim3(md.nmod, SP2 / 256), 256, 0, s, t, md, w, w.ngroups);
     return 1;
 }
 int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
     if (md.ndirs <= 0) return 0;
-    k_dir<<<dim3(md.ndirs, md.nmod, 4), 256, kDirSmem, s>>>(t, md, w);
+    launch_k(k_dir, dim3(md.ndirs, md.nmod, 4), 256, kDirSmem, s, t, md, w);
     return 1;
 }
 int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s) {
-    k_small<<<1, 256, 0, s>>>(t, md, w, grads);
+    launch_k(k_small, 1, 256, 0, s, t, md, w, grads);
     return 1;
+}
+
+bool pdl_enabled() {
+    static const bool on = [] { const char* e = std::getenv("H3G_NO_PDL"); return !(e && e[0] == '1'); }();
+    return on;
 }
 
 }  // namespace h3g

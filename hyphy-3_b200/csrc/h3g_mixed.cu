@@ -118,6 +118,67 @@ __device__ __forceinline__ void mul_leaf(float (&v)[kSG], const Topo& t, const M
     }
 }
 
+// Where this thread's 16 states of a child's message live: a contiguous
+// row of PT32 / rs32 for a leaf (one-hot or fully ambiguous codon), a masked
+// sum of PT32 rows (partially ambiguous codon), or the child's stored message
+// (stride Pp) with its exponent.  Splitting address resolution from the loads
+// lets a thread put the loads of two children in flight together.
+struct MsgSrc {
+    const float* src;
+    size_t stride;      // 1 (leaf row) or Pp (stored message)
+    uint64_t mk;        // != 0: masked sum of PT32 rows starting at src
+    int E;              // exponent of a stored message
+};
+__device__ __forceinline__ MsgSrc msg_src(const Topo& t, const MixedWork& mw, int m, int M, int c, int p, int g, size_t so) {
+    MsgSrc r{nullptr, 1, 0, 0};
+    if (t.leaf[c]) {
+        const int tx = t.taxon[c];
+        const float* PTc = mw.PT32 + mat_off_f(m, c, t.n);
+        const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
+        if (st >= 0) {
+            r.src = PTc + st * SP + kSG * g;
+        } else {
+            const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * t.Pp + p];
+            if (mk == 0 || (mk & t.all_mask) == t.all_mask) {
+                r.src = mw.rs32 + (size_t(m) * t.n + c) * SP + kSG * g;
+            } else {
+                r.src = PTc + kSG * g;
+                r.mk = mk;
+            }
+        }
+    } else {
+        const int ic = t.iidx[c];
+        r.src = mw.Ms + part_off(ic, m, M, t.Pp) + so;
+        r.stride = size_t(t.Pp);
+        r.E = mw.EM[col_off(ic, m, M, t.Pp) + p];
+    }
+    return r;
+}
+__device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
+    if (r.stride != 1) {
+#pragma unroll
+        for (int i = 0; i < kSG; ++i) a[i] = r.src[i * r.stride];
+    } else if (r.mk == 0) {
+        const float4* s4 = reinterpret_cast<const float4*>(r.src);
+#pragma unroll
+        for (int q4 = 0; q4 < kSG / 4; ++q4) {
+            const float4 x = __ldg(s4 + q4);
+            a[4 * q4] = x.x; a[4 * q4 + 1] = x.y; a[4 * q4 + 2] = x.z; a[4 * q4 + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kSG; ++i) a[i] = 0.f;
+        for (uint64_t b = r.mk; b; b &= b - 1) {
+            const float4* r4 = reinterpret_cast<const float4*>(r.src + (__ffsll((long long)b) - 1) * SP);
+#pragma unroll
+            for (int q4 = 0; q4 < kSG / 4; ++q4) {
+                const float4 x = __ldg(r4 + q4);
+                a[4 * q4] += x.x; a[4 * q4 + 1] += x.y; a[4 * q4 + 2] += x.z; a[4 * q4 + 3] += x.w;
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
     for (int i = 0; i < kSG; ++i) v[i] = src[i * stride];
@@ -174,13 +235,7 @@ __device__ __forceinline__ void tc_write_part(const TcTile& s, const float (&v)[
     for (int kc = 0; kc < kSG / 8; ++kc) {
         uint32_t w[3][4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const tc::Bf16x3 x0 = tc::split3(v[8 * kc + 2 * e]);
-            const tc::Bf16x3 x1 = tc::split3(v[8 * kc + 2 * e + 1]);
-            w[0][e] = uint32_t(x0.hi) | (uint32_t(x1.hi) << 16);
-            w[1][e] = uint32_t(x0.mid) | (uint32_t(x1.mid) << 16);
-            w[2][e] = uint32_t(x0.lo) | (uint32_t(x1.lo) << 16);
-        }
+        for (int e = 0; e < 4; ++e) tc::split3x2(v[8 * kc + 2 * e], v[8 * kc + 2 * e + 1], w[0][e], w[1][e], w[2][e]);
         const uint32_t off = tc::kmajor_off16(MT, l.r, kSG * l.g + 8 * kc);
 #pragma unroll
         for (int q = 0; q < 3; ++q)
@@ -241,6 +296,7 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
 // ------------------------------------------------------------ P preparation
 // grid (n, M), block 256: BF16 hi/mid/lo tiles of P and P^T, FP32 P^T and row sums.
 __global__ void __launch_bounds__(256) k_prep_mx(Topo t, Model md, Work w, MixedWork mw) {
+    pdl_enter();
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
     if (b == t.root) return;
     const double* P = w.P + mat_off(m, b, t.n);
@@ -264,7 +320,8 @@ __global__ void __launch_bounds__(256) k_prep_mx(Topo t, Model md, Work w, Mixed
 
 // ------------------------------------------------------------------ inside
 // grid (Pp/128, nodes in level, M), block 512.
-__global__ void __launch_bounds__(kThreads) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ nodes) {
+__global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ nodes) {
+    pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
@@ -275,20 +332,34 @@ __global__ void __launch_bounds__(kThreads) k_inside_mx(Topo t, Model md, Work w
     const size_t so = size_t(kSG * l.g) * Pp + p;     // this thread's first state of the pattern column
     const bool root = u == t.root;
     if (!root) tc_begin(s, mw.Bp, mat_off_f(m, u, t.n));
+    // the first two children's messages load together (padding states are zero in every
+    // message), then one product and one renormalisation; further children one at a time
     float v[kSG];
-#pragma unroll
-    for (int i = 0; i < kSG; ++i) v[i] = (kSG * l.g + i) < t.S ? 1.f : 0.f;
     int E = 0;
-    for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
-        const int c = t.ch[k];
-        if (t.leaf[c]) {
-            mul_leaf(v, t, mw, m, c, p, l.g);
+    const int k0 = t.ch_off[u], k1 = t.ch_off[u + 1];
+    {
+        const MsgSrc s0 = msg_src(t, mw, m, M, t.ch[k0], p, l.g, so);
+        E = s0.E;
+        if (k0 + 1 < k1) {
+            const MsgSrc s1 = msg_src(t, mw, m, M, t.ch[k0 + 1], p, l.g, so);
+            float b[kSG];
+            msg_load(s0, v);
+            msg_load(s1, b);
+#pragma unroll
+            for (int i = 0; i < kSG; ++i) v[i] *= b[i];
+            E += s1.E;
         } else {
-            const int ic = t.iidx[c];
-            mul_part(v, mw.Ms + part_off(ic, m, M, t.Pp) + so, Pp);
-            E += mw.EM[col_off(ic, m, M, t.Pp) + p];
+            msg_load(s0, v);
         }
         E += renorm_row(v, s.smax, l);
+    }
+    for (int k = k0 + 2; k < k1; ++k) {
+        const MsgSrc sr = msg_src(t, mw, m, M, t.ch[k], p, l.g, so);
+        float a[kSG];
+        msg_load(sr, a);
+#pragma unroll
+        for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+        E += sr.E + renorm_row(v, s.smax, l);
     }
     store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
     if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
@@ -303,6 +374,7 @@ __global__ void __launch_bounds__(kThreads) k_inside_mx(Topo t, Model md, Work w
 
 // --------------------------------------------------------------------- root
 __global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
+    pdl_enter();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= t.Pp) return;
     const int ir = t.iidx[t.root], M = md.M;
@@ -344,7 +416,8 @@ __global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
 
 // ------------------------------------------------------------------ outside
 // grid (Pp/128, children in level, M), block 512.
-__global__ void __launch_bounds__(kThreads) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ kids) {
+__global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ kids) {
+    pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
@@ -355,26 +428,37 @@ __global__ void __launch_bounds__(kThreads) k_outside_mx(Topo t, Model md, Work 
     const size_t so = size_t(kSG * l.g) * Pp + p;
     const bool internal = !t.leaf[c];
     if (internal) tc_begin(s, mw.Bpt, mat_off_f(m, c, t.n));
+    // the parent's outside vector (pi at the root) and the first sibling's message load together
     float v[kSG];
     int EV = 0;
-    if (u == t.root) {
+    const int k0 = t.ch_off[u], k1 = t.ch_off[u + 1];
+    int k = k0;
+    while (k < k1 && t.ch[k] == c) ++k;
+    {
+        float a[kSG];
+        const MsgSrc s0 = msg_src(t, mw, m, M, t.ch[k], p, l.g, so);
+        if (u == t.root) {
 #pragma unroll
-        for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
-        EV = renorm_row(v, s.smax, l);
-    } else {
-        load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
-        EV = mw.EU[col_off(iu, m, M, t.Pp) + p];
+            for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
+        } else {
+            load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
+            EV = mw.EU[col_off(iu, m, M, t.Pp) + p];
+        }
+        msg_load(s0, a);
+#pragma unroll
+        for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+        EV += s0.E + renorm_row(v, s.smax, l);
+        ++k;
     }
-    for (int k = t.ch_off[u]; k < t.ch_off[u + 1]; ++k) {
+    for (; k < k1; ++k) {
         const int sb = t.ch[k];
         if (sb == c) continue;
-        if (t.leaf[sb]) {
-            mul_leaf(v, t, mw, m, sb, p, l.g);
-        } else {
-            mul_part(v, mw.Ms + part_off(t.iidx[sb], m, M, t.Pp) + so, Pp);
-            EV += mw.EM[col_off(t.iidx[sb], m, M, t.Pp) + p];
-        }
-        EV += renorm_row(v, s.smax, l);
+        const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
+        float a[kSG];
+        msg_load(sr, a);
+#pragma unroll
+        for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+        EV += sr.E + renorm_row(v, s.smax, l);
     }
     // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
     const int ir = t.iidx[t.root];
@@ -407,29 +491,33 @@ __global__ void __launch_bounds__(kThreads) k_outside_mx(Topo t, Model md, Work 
 // Leaf branches have 0/1 leaf vectors (exact in BF16): only acc0 and acc2.
 // Every kADrain tiles the accumulators are drained into FP64 registers, so no
 // FP32 accumulator takes more than 4 * kADrain additions.
-// 64-pattern tiles, two shared-memory stages: the global loads of tile k+1
-// are in flight while the MMAs of tile k run.
-// grid (n, M, nchunk), block 256 (8 warps: lane quadrant w % 4, column half w / 4).
+//
+// Pipeline (one CTA per SM, 16 warps): the FP32 V and D tiles of 64 patterns
+// stream into a kRing-deep shared-memory ring by 16-byte cp.async (one commit
+// group per tile); the threads split the oldest ring slot into one of two
+// BF16 MMA stages; one thread issues the MMAs of that stage asynchronously.
+// Copies for tile k+2, the split of tile k and the MMAs of tile k-1 overlap.
+// grid (n, M, nchunk), block 512 (warp w: TMEM lane quadrant w % 4, column quarter w / 4).
+constexpr int kAccThreads = 512;
 constexpr int kAT = 64;                                   // patterns per tile (MMA K per tile)
 constexpr int kADrain = 4;                                // tiles per FP32 accumulation group
+constexpr int kRing = 3;                                  // FP32 tiles in flight
 constexpr uint32_t kVRows = 3 * SP;                       // stacked V terms
 constexpr uint32_t kVLbo = (kVRows / 8) * 128;            // K-chunk stride in the V stack
 constexpr uint32_t kDLbo = (SP / 8) * 128;                // K-chunk stride in a D term
 constexpr size_t kVStage = size_t(kVRows) * kAT * 2;      // 24 KB
 constexpr size_t kDTerm = size_t(SP) * kAT * 2;           // 8 KB
-constexpr size_t kStage = kVStage + 3 * kDTerm;           // 48 KB
-constexpr size_t kAccSmem = 2 * kStage + 64;
+constexpr size_t kStage = kVStage + 3 * kDTerm;           // 48 KB per BF16 MMA stage
+constexpr uint32_t kRawRow = kAT * 4 + 16;                // padded FP32 row: conflict-free 16-byte reads
+constexpr size_t kRawOp = size_t(SP) * kRawRow;           // 17 KB per operand
+constexpr size_t kRawSlot = 2 * kRawOp;                   // V and D
+constexpr size_t kAccSmem = 2 * kStage + kRing * kRawSlot + 8 * 2 + 16;
 
 struct Split8 { uint4 hi, mid, lo; };
 __device__ __forceinline__ Split8 split8(const float (&x)[8]) {
     uint32_t h[4], md[4], lo[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        const tc::Bf16x3 a = tc::split3(x[2 * e]), b = tc::split3(x[2 * e + 1]);
-        h[e] = uint32_t(a.hi) | (uint32_t(b.hi) << 16);
-        md[e] = uint32_t(a.mid) | (uint32_t(b.mid) << 16);
-        lo[e] = uint32_t(a.lo) | (uint32_t(b.lo) << 16);
-    }
+    for (int e = 0; e < 4; ++e) tc::split3x2(x[2 * e], x[2 * e + 1], h[e], md[e], lo[e]);
     return {make_uint4(h[0], h[1], h[2], h[3]), make_uint4(md[0], md[1], md[2], md[3]), make_uint4(lo[0], lo[1], lo[2], lo[3])};
 }
 
@@ -461,7 +549,21 @@ __device__ __forceinline__ void leaf_row8(const Topo& t, int tx, int j, int p, f
     }
 }
 
-__global__ void __launch_bounds__(256, 2) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void ld_row8(const unsigned char* raw, int row, int kc, float (&x)[8]) {
+    const float4* r = reinterpret_cast<const float4*>(raw + row * kRawRow + kc * 32);
+    const float4 a = r[0], b = r[1];
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+
+__global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
+    pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
     const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
@@ -473,11 +575,11 @@ __global__ void __launch_bounds__(256, 2) k_accumA_mx(Topo t, Model md, Work w, 
     const int tx = lf ? t.taxon[b] : -1;
     const float* Vb = mw.Vf + part_off(b, m, M, t.Pp);
     const float* Db = lf ? nullptr : mw.D + part_off(t.iidx[b], m, M, t.Pp);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + 2 * kStage);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 2);
+    unsigned char* ring = smraw + 2 * kStage;
+    uint64_t* mma_bar = reinterpret_cast<uint64_t*>(ring + kRing * kRawSlot);   // [2]
+    uint32_t* slot = reinterpret_cast<uint32_t*>(mma_bar + 2);
     if (tid == 0) {
-        tc::mbar_init(&bars[0], 1);
-        tc::mbar_init(&bars[1], 1);
+        for (int q = 0; q < 2; ++q) tc::mbar_init(&mma_bar[q], 1);
         tc::mbar_fence_init();
     }
     if (warp == 0) tc::tmem_alloc(slot, 256);
@@ -486,66 +588,61 @@ __global__ void __launch_bounds__(256, 2) k_accumA_mx(Topo t, Model md, Work w, 
     tc::tc_fence_after();
     const uint32_t tmem = *slot;
 
-    // load items: e = tid + 256 q; state row 8 (e / 64) + e % 8, 8-pattern chunk (e / 8) % 8
-    int row[2], kc[2];
+    // all threads stream tile `tile` into ring slot tile % kRing with 16-byte cp.async
+    // (256-byte state-row segments, two rows per warp instruction); one commit group per tile
+    auto produce = [&](int tile) {
+        if (tile < ntile) {
+            unsigned char* dst = ring + (tile % kRing) * kRawSlot;
+            const size_t p0 = size_t(p_begin) + size_t(tile) * kAT;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int e = tid + 256 * q;
-        row[q] = 8 * (e >> 6) + (e & 7);
-        kc[q] = (e >> 3) & 7;
-    }
-    float rv[2][8], rd[2][8];
-    auto fetch = [&](int tile) {
-        const int p0 = p_begin + tile * kAT;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int p = p0 + 8 * kc[q];
-            const float4* v4 = reinterpret_cast<const float4*>(Vb + size_t(row[q]) * Pp + p);
-            const float4 a = __ldcs(v4), c = __ldcs(v4 + 1);
-            rv[q][0] = a.x; rv[q][1] = a.y; rv[q][2] = a.z; rv[q][3] = a.w;
-            rv[q][4] = c.x; rv[q][5] = c.y; rv[q][6] = c.z; rv[q][7] = c.w;
-            if (lf) {
-                leaf_row8(t, tx, row[q], p, rd[q]);
-            } else {
-                const float4* d4 = reinterpret_cast<const float4*>(Db + size_t(row[q]) * Pp + p);
-                const float4 x = __ldcs(d4), y = __ldcs(d4 + 1);
-                rd[q][0] = x.x; rd[q][1] = x.y; rd[q][2] = x.z; rd[q][3] = x.w;
-                rd[q][4] = y.x; rd[q][5] = y.y; rd[q][6] = y.z; rd[q][7] = y.w;
+            for (int q = 0; q < 2; ++q) {
+                const int c = tid + kAccThreads * q, r = c >> 4, c16 = c & 15;
+                cp_async16(dst + r * kRawRow + c16 * 16, Vb + size_t(r) * Pp + p0 + 4 * c16);
+                if (!lf) cp_async16(dst + kRawOp + r * kRawRow + c16 * 16, Db + size_t(r) * Pp + p0 + 4 * c16);
             }
         }
+        cp_async_commit();
     };
 
-    // drain mapping: TMEM lane quadrant lq (rows 32 lq ..), column half ch
-    const int lq = warp & 3, ch = warp >> 2;
+    // split item of this thread: state row 8 (tid / 64) + tid % 8, 8-pattern chunk (tid / 8) % 8
+    const int row = 8 * (tid >> 6) + (tid & 7), kc = (tid >> 3) & 7;
+    const int lq = warp & 3, cq = warp >> 2;
     const bool top = lq < 2;
-    double dacc[32];
+    double dacc[16];
 #pragma unroll
-    for (int x = 0; x < 32; ++x) dacc[x] = 0.0;
+    for (int x = 0; x < 16; ++x) dacc[x] = 0.0;
 
-    fetch(0);
+    for (int q = 0; q < kRing - 1; ++q) produce(q);
     for (int kt = 0; kt < ntile; ++kt) {
-        const int st = kt & 1;
+        const int st = kt & 1, sl = kt % kRing;
+        produce(kt + kRing - 1);                 // slot of tile kt-1, released by the barrier of iteration kt-1
+        cp_async_wait<kRing - 1>();              // this thread's copies of tile kt have landed
+        __syncthreads();                         // ... and everyone else's
         unsigned char* VS = smraw + st * kStage;
         unsigned char* DS = VS + kVStage;
-        if (kt >= 2 && !tc::mbar_wait(&bars[st], uint32_t(((kt - 2) >> 1) & 1)) && lane == 0) atomicOr(w.err, 4);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const uint32_t rg = uint32_t(row[q] >> 3) * 128 + uint32_t(row[q] & 7) * 16;
-            const Split8 sv = split8(rv[q]);
-            *reinterpret_cast<uint4*>(VS + kc[q] * kVLbo + 0 * 1024 + rg) = sv.lo;
-            *reinterpret_cast<uint4*>(VS + kc[q] * kVLbo + 1 * 1024 + rg) = sv.hi;
-            *reinterpret_cast<uint4*>(VS + kc[q] * kVLbo + 2 * 1024 + rg) = sv.mid;
+        const unsigned char* raw = ring + sl * kRawSlot;
+        if (kt >= 2 && !tc::mbar_wait(&mma_bar[st], uint32_t(((kt - 2) >> 1) & 1)) && lane == 0) atomicOr(w.err, 4);
+        const int p0 = p_begin + kt * kAT;
+        {
+            const uint32_t rg = uint32_t(row >> 3) * 128 + uint32_t(row & 7) * 16;
+            float x[8];
+            ld_row8(raw, row, kc, x);
+            const Split8 sv = split8(x);
+            *reinterpret_cast<uint4*>(VS + kc * kVLbo + 0 * 1024 + rg) = sv.lo;
+            *reinterpret_cast<uint4*>(VS + kc * kVLbo + 1 * 1024 + rg) = sv.hi;
+            *reinterpret_cast<uint4*>(VS + kc * kVLbo + 2 * 1024 + rg) = sv.mid;
             if (lf) {
+                leaf_row8(t, tx, row, p0 + 8 * kc, x);
                 uint32_t h[4];
 #pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    h[e] = uint32_t(tc::bf16_bits(rd[q][2 * e])) | (uint32_t(tc::bf16_bits(rd[q][2 * e + 1])) << 16);
-                *reinterpret_cast<uint4*>(DS + kc[q] * kDLbo + rg) = make_uint4(h[0], h[1], h[2], h[3]);
+                for (int e = 0; e < 4; ++e) h[e] = tc::bf16x2_bits(x[2 * e], x[2 * e + 1]);
+                *reinterpret_cast<uint4*>(DS + kc * kDLbo + rg) = make_uint4(h[0], h[1], h[2], h[3]);
             } else {
-                const Split8 sd = split8(rd[q]);
-                *reinterpret_cast<uint4*>(DS + kc[q] * kDLbo + rg) = sd.hi;
-                *reinterpret_cast<uint4*>(DS + kDTerm + kc[q] * kDLbo + rg) = sd.mid;
-                *reinterpret_cast<uint4*>(DS + 2 * kDTerm + kc[q] * kDLbo + rg) = sd.lo;
+                ld_row8(raw + kRawOp, row, kc, x);
+                const Split8 sd = split8(x);
+                *reinterpret_cast<uint4*>(DS + kc * kDLbo + rg) = sd.hi;
+                *reinterpret_cast<uint4*>(DS + kDTerm + kc * kDLbo + rg) = sd.mid;
+                *reinterpret_cast<uint4*>(DS + 2 * kDTerm + kc * kDLbo + rg) = sd.lo;
             }
         }
         tc::fence_async_smem();
@@ -570,27 +667,23 @@ __global__ void __launch_bounds__(256, 2) k_accumA_mx(Topo t, Model md, Work w, 
                     tc::mma_bf16(tmem + 192, a2, bl, kIdesc, acc);
                 }
             }
-            tc::mma_commit(&bars[st]);
+            tc::mma_commit(&mma_bar[st]);
         }
-        if (kt + 1 < ntile) fetch(kt + 1);
         if ((kt % kADrain) == kADrain - 1 || kt == ntile - 1) {
-            if (!tc::mbar_wait(&bars[st], uint32_t((kt >> 1) & 1)) && lane == 0) atomicOr(w.err, 8);
+            if (!tc::mbar_wait(&mma_bar[st], uint32_t((kt >> 1) & 1)) && lane == 0) atomicOr(w.err, 8);
             tc::tc_fence_after();
-            const uint32_t rowaddr = tmem + (uint32_t(32 * lq) << 16) + uint32_t(32 * ch);
+            const uint32_t rowaddr = tmem + (uint32_t(32 * lq) << 16) + uint32_t(16 * cq);
             // acc0, acc1 (internal branches) and acc2 (top rows) / acc3 (bottom rows, internal branches)
             const uint32_t cols[3] = {0u, 64u, top ? 128u : 192u};
             const bool use[3] = {true, !lf, top || !lf};
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 if (!use[a]) continue;
+                float v16[16];
+                tc::tmem_ld16(rowaddr + cols[a], v16);
+                tc::tmem_wait_ld();
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    float v16[16];
-                    tc::tmem_ld16(rowaddr + cols[a] + 16 * h, v16);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int x = 0; x < 16; ++x) dacc[16 * h + x] += double(v16[x]);
-                }
+                for (int x = 0; x < 16; ++x) dacc[x] += double(v16[x]);
             }
             tc::tc_fence_before();
             __syncthreads();
@@ -602,16 +695,16 @@ __global__ void __launch_bounds__(256, 2) k_accumA_mx(Topo t, Model md, Work w, 
     const int i = 32 * lq + lane - (top ? 0 : 64);
     if (!top) {
 #pragma unroll
-        for (int x = 0; x < 32; ++x) sA[i * 65 + 32 * ch + x] = dacc[x];
+        for (int x = 0; x < 16; ++x) sA[i * 65 + 16 * cq + x] = dacc[x];
     }
     __syncthreads();
     if (top) {
 #pragma unroll
-        for (int x = 0; x < 32; ++x) sA[i * 65 + 32 * ch + x] += dacc[x];
+        for (int x = 0; x < 16; ++x) sA[i * 65 + 16 * cq + x] += dacc[x];
     }
     __syncthreads();
     double* dst = w.Apart + ((size_t(b) * M + m) * w.nchunk + ck) * SP2;
-    for (int e = tid; e < SP2; e += 256) dst[e] = sA[(e >> 6) * 65 + (e & 63)];
+    for (int e = tid; e < SP2; e += kAccThreads) dst[e] = sA[(e >> 6) * 65 + (e & 63)];
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, 256);
@@ -644,23 +737,23 @@ h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, 
 }
 
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
-    k_prep_mx<<<dim3(t.n, md.M), 256, 0, s>>>(t, md, w, mw);
+    launch_k(k_prep_mx, dim3(t.n, md.M), 256, 0, s, t, md, w, mw);
     return 1;
 }
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s) {
-    k_inside_mx<<<dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s>>>(t, md, w, mw, d_nodes);
+    launch_k(k_inside_mx, dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s, t, md, w, mw, d_nodes);
     return 1;
 }
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
-    k_root_mx<<<(t.Pp + 127) / 128, 128, 0, s>>>(t, md, w, mw);
+    launch_k(k_root_mx, (t.Pp + 127) / 128, 128, 0, s, t, md, w, mw);
     return 1;
 }
 int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s) {
-    k_outside_mx<<<dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s>>>(t, md, w, mw, d_kids);
+    launch_k(k_outside_mx, dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s, t, md, w, mw, d_kids);
     return 1;
 }
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
-    k_accumA_mx<<<dim3(t.n, md.M, w.nchunk), 256, kAccSmem, s>>>(t, md, w, mw);
+    launch_k(k_accumA_mx, dim3(t.n, md.M, w.nchunk), kAccThreads, kAccSmem, s, t, md, w, mw);
     return 1;
 }
 

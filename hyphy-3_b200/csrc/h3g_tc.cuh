@@ -36,6 +36,23 @@ __device__ __forceinline__ Bf16x3 split3(float x) {
     return s;
 }
 
+// Packed form of the split for two values: cvt.rn.bf16x2 rounds each half
+// exactly like cvt.rn.bf16.f32, so the terms equal split3's.  Returns the
+// hi / mid / lo words with x0 in the low and x1 in the high 16 bits.
+__device__ __forceinline__ uint32_t bf16x2_bits(float x0, float x1) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(x1), "f"(x0));
+    return r;
+}
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+__device__ __forceinline__ void split3x2(float x0, float x1, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
+    hi = bf16x2_bits(x0, x1);
+    const float r0 = x0 - bf16_lo(hi), r1 = x1 - bf16_hi(hi);
+    mid = bf16x2_bits(r0, r1);
+    lo = bf16x2_bits(r0 - bf16_lo(mid), r1 - bf16_hi(mid));
+}
+
 // ---- mbarrier
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
