@@ -521,8 +521,10 @@ __device__ __forceinline__ Split8 split8(const float (&x)[8]) {
     return {make_uint4(h[0], h[1], h[2], h[3]), make_uint4(md[0], md[1], md[2], md[3]), make_uint4(lo[0], lo[1], lo[2], lo[3])};
 }
 
-// The 8 patterns [p, p+8) of state row j of a leaf's 0/1 vector.
-__device__ __forceinline__ void leaf_row8(const Topo& t, int tx, int j, int p, float (&d)[8]) {
+// The 8 patterns of state row j of a leaf's 0/1 vector, from the tile's states
+// (8 bytes at st) and masks (8 words at mk) staged in shared memory.
+__device__ __forceinline__ void leaf_row8_smem(const Topo& t, int tx, int j, const unsigned char* st, const uint64_t* mk,
+                                               float (&d)[8]) {
     if (j >= t.S) {
 #pragma unroll
         for (int x = 0; x < 8; ++x) d[x] = 0.f;
@@ -533,17 +535,16 @@ __device__ __forceinline__ void leaf_row8(const Topo& t, int tx, int j, int p, f
         for (int x = 0; x < 8; ++x) d[x] = 1.f;
         return;
     }
-    const size_t base = size_t(tx) * t.Pp + p;
-    const uint64_t st8 = __ldg(reinterpret_cast<const unsigned long long*>(t.states + base));
+    const uint64_t st8 = *reinterpret_cast<const uint64_t*>(st);
 #pragma unroll
     for (int x = 0; x < 8; ++x) {
-        const int st = int(int8_t(uint8_t(st8 >> (8 * x))));
+        const int s = int(int8_t(uint8_t(st8 >> (8 * x))));
         bool on;
-        if (st >= 0) {
-            on = st == j;
+        if (s >= 0) {
+            on = s == j;
         } else {
-            const uint64_t mk = __ldg(reinterpret_cast<const unsigned long long*>(t.masks + base + x));
-            on = mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> j) & 1);
+            const uint64_t m = mk[x];
+            on = m == 0 || (m & t.all_mask) == t.all_mask || ((m >> j) & 1);
         }
         d[x] = on ? 1.f : 0.f;
     }
@@ -600,6 +601,12 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
                 cp_async16(dst + r * kRawRow + c16 * 16, Vb + size_t(r) * Pp + p0 + 4 * c16);
                 if (!lf) cp_async16(dst + kRawOp + r * kRawRow + c16 * 16, Db + size_t(r) * Pp + p0 + 4 * c16);
             }
+            if (lf && tx >= 0 && tid < 36) {
+                // a leaf's states (64 B) and masks (512 B) of the tile, in the unused D area of the slot
+                const size_t o = size_t(tx) * Pp + p0;
+                if (tid < 4) cp_async16(dst + kRawOp + tid * 16, t.states + o + 16 * tid);
+                else cp_async16(dst + kRawOp + 64 + (tid - 4) * 16, t.masks + o + 2 * (tid - 4));
+            }
         }
         cp_async_commit();
     };
@@ -632,7 +639,7 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
             *reinterpret_cast<uint4*>(VS + kc * kVLbo + 1 * 1024 + rg) = sv.hi;
             *reinterpret_cast<uint4*>(VS + kc * kVLbo + 2 * 1024 + rg) = sv.mid;
             if (lf) {
-                leaf_row8(t, tx, row, p0 + 8 * kc, x);
+                leaf_row8_smem(t, tx, row, raw + kRawOp + 8 * kc, reinterpret_cast<const uint64_t*>(raw + kRawOp + 64) + 8 * kc, x);
                 uint32_t h[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) h[e] = tc::bf16x2_bits(x[2 * e], x[2 * e + 1]);
