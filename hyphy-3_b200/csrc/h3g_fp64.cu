@@ -84,68 +84,112 @@ __device__ __forceinline__ void stage_matrix(double* __restrict__ s, const doubl
 }
 
 // ------------------------------------------------------------------ build P
-// grid (n, M, 4): CTA z owns columns [16z, 16z+16) of P_{m,b} and dP_{m,b}.
-// Thread (r = tid % 64, cg = tid / 64) owns row r, columns 16z + 4cg .. +3.
-// U_k and Q_k are staged transposed so consecutive threads read consecutive rows.
+// grid (n, M): one CTA per branch and rate class computes the whole 64x64
+// P_{m,b} = sum_k c_k clamp(U_k diag(e^{lam_k tau}) V_k) and
+// dP_{m,b} = sum_k c_k r_m conv_k Q_k clamp(P_k), model by model.  Thread t owns
+// the 4x4 block rows 4(t/16).., columns 4(t%16)..; operands are staged in
+// shared memory so every k step reads two contiguous 32-byte row pieces
+// (a broadcast of the two row blocks of the warp and 16 consecutive column blocks).
+// dynamic smem: UE (U^T scaled by e, then Q^T), V, clamp(P_k): 3 x 64 x 64 doubles.
 __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    double* sT = sm;                 // U_k^T, later Q_k^T (sT[l * 65 + r]; padded against bank conflicts)
-    double* sV = sm + SP * (SP + 1); // V_k columns of this block (64 x 16)
-    double* sPk = sV + SP * 16;      // clamp(P_k) columns of this block (64 x 16)
+    double* sUE = sm;             // sUE[l][r] = U[r][l] e_l, later Q^T: sUE[l][r] = Q[r][l]
+    double* sV = sm + SP2;        // sV[l][c] = V[l][c]
+    double* sPk = sm + 2 * SP2;   // sPk[l][c] = clamp(P_k)[l][c]
     __shared__ double se[SP];
-    const int b = blockIdx.x, m = blockIdx.y, cb = blockIdx.z, tid = threadIdx.x;
+    const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
     if (b == t.root) return;
-    const int r = tid & 63, c0 = (tid >> 6) * 4;
+    const int r0 = 4 * (tid >> 4), c0 = 4 * (tid & 15);
     const bool test = md.is_test == nullptr || md.is_test[b] != 0;
     const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
-    double accP[4] = {0, 0, 0, 0}, accD[4] = {0, 0, 0, 0};
+    double accP[4][4], accD[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) accP[a][c] = accD[a][c] = 0.0;
     for (int k = k0; k < k1; ++k) {
         const double cw = test ? md.class_w[k] : 1.0;
         const double cv = time_conv(md, k);
         const double rate = md.rates[m];
         const double tau = rate * w.bl[b] * cv;
         __syncthreads();
-        for (int e = tid; e < SP2; e += 256) sT[(e & 63) * (SP + 1) + (e >> 6)] = md.U[size_t(k) * SP2 + e];
-        for (int e = tid; e < SP * 16; e += 256) sV[e] = md.V[size_t(k) * SP2 + (e >> 4) * SP + cb * 16 + (e & 15)];
         if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
+        stage_matrix(sV, md.V + size_t(k) * SP2, tid, 256);
         __syncthreads();
-        double pk[4] = {0, 0, 0, 0};
+        {
+            const double2* g2 = reinterpret_cast<const double2*>(md.UT + size_t(k) * SP2);
+            double2* s2 = reinterpret_cast<double2*>(sUE);
+            for (int e = tid; e < SP2 / 2; e += 256) {
+                const double f = se[e >> 5];           // row l = (2e) / 64 of U^T
+                double2 x = __ldg(g2 + e);
+                x.x *= f; x.y *= f;
+                s2[e] = x;
+            }
+        }
+        __syncthreads();
+        double pk[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) pk[a][c] = 0.0;
 #pragma unroll 4
         for (int l = 0; l < SP; ++l) {
-            const double u = sT[l * (SP + 1) + r] * se[l];
-            const double2 v01 = *reinterpret_cast<const double2*>(sV + l * 16 + c0);
-            const double2 v23 = *reinterpret_cast<const double2*>(sV + l * 16 + c0 + 2);
-            pk[0] = fma(u, v01.x, pk[0]); pk[1] = fma(u, v01.y, pk[1]);
-            pk[2] = fma(u, v23.x, pk[2]); pk[3] = fma(u, v23.y, pk[3]);
+            const double2 u01 = *reinterpret_cast<const double2*>(sUE + l * SP + r0);
+            const double2 u23 = *reinterpret_cast<const double2*>(sUE + l * SP + r0 + 2);
+            const double2 v01 = *reinterpret_cast<const double2*>(sV + l * SP + c0);
+            const double2 v23 = *reinterpret_cast<const double2*>(sV + l * SP + c0 + 2);
+            const double uu[4] = {u01.x, u01.y, u23.x, u23.y}, vv[4] = {v01.x, v01.y, v23.x, v23.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) pk[a][c] = fma(uu[a], vv[c], pk[a][c]);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) pk[q] = fmax(pk[q], 0.0);
+        for (int a = 0; a < 4; ++a) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                pk[a][c] = fmax(pk[a][c], 0.0);
+                accP[a][c] = fma(cw, pk[a][c], accP[a][c]);
+            }
+            *reinterpret_cast<double2*>(sPk + (r0 + a) * SP + c0) = make_double2(pk[a][0], pk[a][1]);
+            *reinterpret_cast<double2*>(sPk + (r0 + a) * SP + c0 + 2) = make_double2(pk[a][2], pk[a][3]);
+        }
+        __syncthreads();
+        stage_matrix(sUE, md.QT + size_t(k) * SP2, tid, 256);
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < 4; ++q) sPk[r * 16 + c0 + q] = pk[q];
-        for (int e = tid; e < SP2; e += 256) sT[(e & 63) * (SP + 1) + (e >> 6)] = md.Q[size_t(k) * SP2 + e];
-        __syncthreads();
-        double qp[4] = {0, 0, 0, 0};
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) pk[a][c] = 0.0;
 #pragma unroll 4
-        for (int l = 0; l < SP; ++l) {
-            const double qq = sT[l * (SP + 1) + r];
-            const double2 p01 = *reinterpret_cast<const double2*>(sPk + l * 16 + c0);
-            const double2 p23 = *reinterpret_cast<const double2*>(sPk + l * 16 + c0 + 2);
-            qp[0] = fma(qq, p01.x, qp[0]); qp[1] = fma(qq, p01.y, qp[1]);
-            qp[2] = fma(qq, p23.x, qp[2]); qp[3] = fma(qq, p23.y, qp[3]);
+        for (int l = 0; l < SP; ++l) {            // (Q clamp(P_k))[r][c] = sum_l Q[r][l] P_k[l][c]
+            const double2 q01 = *reinterpret_cast<const double2*>(sUE + l * SP + r0);
+            const double2 q23 = *reinterpret_cast<const double2*>(sUE + l * SP + r0 + 2);
+            const double2 p01 = *reinterpret_cast<const double2*>(sPk + l * SP + c0);
+            const double2 p23 = *reinterpret_cast<const double2*>(sPk + l * SP + c0 + 2);
+            const double qq[4] = {q01.x, q01.y, q23.x, q23.y}, pp[4] = {p01.x, p01.y, p23.x, p23.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) pk[a][c] = fma(qq[a], pp[c], pk[a][c]);
         }
         const double sc = cw * rate * cv;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) { accP[q] = fma(cw, pk[q], accP[q]); accD[q] = fma(sc, qp[q], accD[q]); }
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) accD[a][c] = fma(sc, pk[a][c], accD[a][c]);
     }
     const size_t o = mat_off(m, b, t.n);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int col = cb * 16 + c0 + q;
-        w.P[o + r * SP + col] = accP[q];
-        w.PT[o + col * SP + r] = accP[q];
-        w.dP[o + r * SP + col] = accD[q];
+    for (int a = 0; a < 4; ++a) {
+        const int r = r0 + a;
+        *reinterpret_cast<double2*>(w.P + o + r * SP + c0) = make_double2(accP[a][0], accP[a][1]);
+        *reinterpret_cast<double2*>(w.P + o + r * SP + c0 + 2) = make_double2(accP[a][2], accP[a][3]);
+        *reinterpret_cast<double2*>(w.dP + o + r * SP + c0) = make_double2(accD[a][0], accD[a][1]);
+        *reinterpret_cast<double2*>(w.dP + o + r * SP + c0 + 2) = make_double2(accD[a][2], accD[a][3]);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) w.PT[o + (c0 + c) * SP + r] = accP[a][c];
     }
 }
 
@@ -503,18 +547,19 @@ __global__ void __launch_bounds__(256) k_areduce(Topo t, Model md, Work w) {
 // the diagonal sums for d/dc_k and the d mu term.  Thread t owns the 4x4 block
 // rows 4(t/16).., columns 4(t%16).. of every 64x64 product, so shared-memory
 // reads are consecutive (or broadcast) across a warp.
-// block 256, dynamic smem (64*64 (A) + 64*64 (T^T) + 64*64 (V^T)) doubles; U_k is read through L1.
+// block 256, dynamic smem (64*64 (A, then T^T) + 64*64 (V^T) + 64*64 (U_k)) doubles.
 __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    double* sA = sm;                  // A_{m,b}
-    double* sTT = sA + SP2;           // (U^T A)^T : sTT[l][r] = T[r][l]
-    double* sVT = sTT + SP2;          // V_k^T : sVT[l][c] = V[c][l]
+    double* sA = sm;                  // A_{m,b}, then (U^T A)^T : sTT[l][r] = T[r][l]
+    double* sTT = sA;
+    double* sVT = sm + SP2;           // V_k^T : sVT[l][c] = V[c][l]
+    double* sU = sm + 2 * SP2;        // U_k
     __shared__ double se[SP];
     __shared__ double red[8];
     const int g = blockIdx.x, m = blockIdx.y, k = blockIdx.z, tid = threadIdx.x, n = t.n, M = md.M;
     const int r0 = 4 * (tid >> 4), c0 = 4 * (tid & 15);
-    const double* gU = md.U + size_t(k) * SP2;       // U_k, read through L1
+    stage_matrix(sU, md.U + size_t(k) * SP2, tid, 256);
     for (int e = tid; e < SP2; e += 256) {
         const int c = e >> 6, l = e & 63;                 // V[c][l], coalesced read
         sVT[l * SP + c] = md.V[size_t(k) * SP2 + e];
@@ -541,9 +586,10 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
         for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+#pragma unroll 4
         for (int l = 0; l < SP; ++l) {          // T[r][c] = sum_l U[l][r] A[l][c]
-            const double2 u01 = __ldg(reinterpret_cast<const double2*>(gU + l * SP + r0));
-            const double2 u23 = __ldg(reinterpret_cast<const double2*>(gU + l * SP + r0 + 2));
+            const double2 u01 = *reinterpret_cast<const double2*>(sU + l * SP + r0);
+            const double2 u23 = *reinterpret_cast<const double2*>(sU + l * SP + r0 + 2);
             const double2 a01 = *reinterpret_cast<const double2*>(sA + l * SP + c0);
             const double2 a23 = *reinterpret_cast<const double2*>(sA + l * SP + c0 + 2);
             const double uu[4] = {u01.x, u01.y, u23.x, u23.y}, aa[4] = {a01.x, a01.y, a23.x, a23.y};
@@ -552,6 +598,7 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
 #pragma unroll
                 for (int c = 0; c < 4; ++c) acc[a][c] = fma(uu[a], aa[c], acc[a][c]);
         }
+        __syncthreads();                        // every thread is done with A: T^T overwrites it
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -561,6 +608,7 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
         for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+#pragma unroll 4
         for (int l = 0; l < SP; ++l) {          // At[r][c] = sum_l T[r][l] V[c][l]
             const double2 t01 = *reinterpret_cast<const double2*>(sTT + l * SP + r0);
             const double2 t23 = *reinterpret_cast<const double2*>(sTT + l * SP + r0 + 2);
@@ -706,7 +754,7 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
 static size_t smem_bytes(int mats) { return size_t(mats) * SP2 * sizeof(double); }
 static const size_t kPruneSmem = (SP2 + SP * kTileP + kGroups * kTileP) * sizeof(double);
 static const size_t kDirSmem = (2 * SP2 + 16 * SP) * sizeof(double);
-static const size_t kBuildSmem = (SP * (SP + 1) + 2 * SP * 16) * sizeof(double);
+static const size_t kBuildSmem = (3 * SP2) * sizeof(double);
 static const size_t kFrechetSmem = (3 * SP2) * sizeof(double);
 
 void fp64_configure() {
@@ -718,7 +766,7 @@ void fp64_configure() {
 }
 
 int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    launch_k(k_build_P, dim3(t.n, md.M, 4), 256, kBuildSmem, s, t, md, w);
+    launch_k(k_build_P, dim3(t.n, md.M), 256, kBuildSmem, s, t, md, w);
     launch_k(k_rowsum, dim3(t.n, md.M), SP, 0, s, t, md, w);
     return 2;
 }
