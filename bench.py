@@ -52,6 +52,19 @@ WORKLOADS = {
 }
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of each pruning stage per evaluation,
+# summed over the stage's launches in the ncu launch list of `bench.py --profile` (one evaluation,
+# --clock-control none).  The 1024-taxon workload is captured on its 512-codon prefix and scaled by
+# the padded pattern count (5120 / 512): these stages stream per-pattern partials, so their traffic is
+# proportional to the patterns processed.
+MEASURED_TRAFFIC = {
+    (1, "mixed"): {"inside": 19.5e6, "outside": 36.2e6, "accum_A": 49.4e6},
+    (1, "fp64"): {"inside": 36.5e6, "outside": 68.7e6, "accum_A": 98.3e6},
+    (3, "mixed"): {"inside": 13.548e9, "outside": 22.313e9, "accum_A": 18.797e9},
+    (3, "fp64"): {"inside": 29.259e9, "outside": 48.234e9, "accum_A": 34.723e9},
+}
+
+
 def build_inputs(seed_offset: int = 0, config: int = 1, sites: int | None = None):
     import _hyphy3 as h
     from hyphy3.simulate import make_workload
@@ -366,8 +379,10 @@ def run_ours(args) -> None:
     dom = max(("inside", "outside", "accum_A"), key=lambda k: stg.get(k, (0.0, 0))[0])
     dom_ms, dom_launches = stg[dom]
     dom_bytes, dom_flops = work[dom]
+    traffic = MEASURED_TRAFFIC.get((args.config, precision), {}).get(dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_bytes / (dom_ms * 1e-3) / 1e9, "peak": hbm_peak,
-                "unit": "GB/s", "frac": dom_bytes / (dom_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None,
+                "unit": "GB/s", "frac": dom_bytes / (dom_ms * 1e-3) / 1e9 / hbm_peak, "traffic": traffic,
+                "traffic_unit": "bytes per evaluation (all launches of the stage), from ncu",
                 "peak_source": "measured" if peaks else "fallback",
                 "algorithmic_bytes_per_eval": dom_bytes, "stage_ms": dom_ms, "launches_per_eval": dom_launches}
     fp64_peak = fp64_dgemm_peak() if rank == 0 else None
@@ -384,7 +399,7 @@ def run_ours(args) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if precision == "fp64" else "tf32x3/f32", "data": "synthetic",
+            "dtype": "f64" if precision == "fp64" else "bf16x3/f32", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.config], "sites": wl.n_sites, "branches": n - 1, "patterns": aln.num_patterns,
                        "precision": precision, "l2": "flushed (256 MiB write) before every timed step",
                        "parallelism": f"replicas{world}" if world > 1 else "single"},
@@ -488,7 +503,7 @@ def run_profile(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["auto", "fp64", "mixed"], default="auto")
