@@ -200,6 +200,7 @@ struct Alignment {
     std::vector<int8_t> states;
     std::vector<uint64_t> masks;
     std::vector<double> weights;
+    std::vector<int> site_pattern;    // alignment.hpp site_to_pattern
     double nuc_freq[4] = {0, 0, 0, 0};
     double pos_freq[3][4] = {};   // CF3x4-corrected (alignment.hpp:1017)
     std::vector<double> pi;       // codon_frequencies_f3x4
@@ -224,18 +225,20 @@ struct Alignment {
         frequencies();
         // first-occurrence pattern order
         std::map<std::pair<std::vector<int8_t>, std::vector<uint64_t>>, int> seen;
-        states.clear(); masks.clear(); weights.clear(); P = 0;
+        states.clear(); masks.clear(); weights.clear(); site_pattern.clear(); P = 0;
         std::vector<int8_t> ks(T); std::vector<uint64_t> km(T);
         for (int c = 0; c < n_codons; ++c) {
             for (int t = 0; t < T; ++t) { ks[t] = cs[size_t(t) * n_codons + c]; km[t] = cm[size_t(t) * n_codons + c]; }
             auto key = std::make_pair(ks, km);
             auto it = seen.find(key);
             if (it == seen.end()) {
+                site_pattern.push_back(P);
                 seen.emplace(key, P++);
                 states.insert(states.end(), ks.begin(), ks.end());
                 masks.insert(masks.end(), km.begin(), km.end());
                 weights.push_back(1.0);
             } else {
+                site_pattern.push_back(it->second);
                 weights[it->second] += 1.0;
             }
         }
@@ -1007,6 +1010,179 @@ inline MixResult joint_frechet_gradients(const Tree& tr, const Alignment& a, con
         sp.has_bg = true; sp.bg = p; sp.bg.beta = omega_bg; sp.is_test = *is_test;
     }
     return mixture_eval(tr, a, sp, bl);
+}
+
+
+// ------------------------------------------------------------------ FEL
+// Per-site fixed-effects likelihood fits (analyses/fel.hpp:230-446, fast path
+// with every branch tested) and the two scalar optimisers it uses
+// (opt/nelder_mead.hpp:24-105 Brent1D, :111-229 NelderMead2D), restated.
+
+// opt/nelder_mead.hpp:24-105 — Brent's parabolic / golden-section minimiser on [min(ax,cx), max(ax,cx)]
+template <class F>
+inline std::pair<double, double> brent1d(F&& f, double ax, double bx, double cx, double tol = 1e-4, int max_iter = 60) {
+    const double CGOLD = 0.3819660, ZEPS = 1e-10;
+    double a = std::min(ax, cx), b = std::max(ax, cx);
+    double v = bx, w = v, x = v, e = 0.0;
+    double fx = f(x), fv = fx, fw = fx;
+    for (int iter = 0; iter < max_iter; ++iter) {
+        const double xm = 0.5 * (a + b), tol1 = tol * std::fabs(x) + ZEPS, tol2 = 2.0 * tol1;
+        if (std::fabs(x - xm) <= (tol2 - 0.5 * (b - a))) break;
+        double d = 0.0;
+        if (std::fabs(e) > tol1) {
+            double r = (x - w) * (fx - fv), q = (x - v) * (fx - fw), pp = (x - v) * q - (x - w) * r;
+            q = 2.0 * (q - r);
+            if (q > 0.0) pp = -pp;
+            q = std::fabs(q);
+            const double etemp = e;
+            e = d;
+            if (std::fabs(pp) >= std::fabs(0.5 * q * etemp) || pp <= q * (a - x) || pp >= q * (b - x)) {
+                e = (x >= xm) ? a - x : b - x;
+                d = CGOLD * e;
+            } else {
+                d = pp / q;
+                const double u = x + d;
+                if (u - a < tol2 || b - u < tol2) d = (xm - x >= 0.0) ? std::fabs(tol1) : -std::fabs(tol1);
+            }
+        } else {
+            e = (x >= xm) ? a - x : b - x;
+            d = CGOLD * e;
+        }
+        const double u = (std::fabs(d) >= tol1) ? x + d : x + ((d >= 0.0) ? std::fabs(tol1) : -std::fabs(tol1));
+        const double fu = f(u);
+        if (fu <= fx) {
+            if (u >= x) a = x; else b = x;
+            v = w; fv = fw; w = x; fw = fx; x = u; fx = fu;
+        } else {
+            if (u < x) a = u; else b = u;
+            if (fu <= fw || w == x) { v = w; fv = fw; w = u; fw = fu; }
+            else if (fu <= fv || v == x || v == w) { v = u; fv = fu; }
+        }
+    }
+    return {x, fx};
+}
+
+struct NMPoint { double a = 0, b = 0, f = 0; };
+
+// stable order of three simplex vertices by f (what std::sort does on three elements in libstdc++)
+inline void sort3(std::array<NMPoint, 3>& s) {
+    for (int i = 1; i < 3; ++i) {
+        NMPoint v = s[i]; int j = i;
+        while (j > 0 && v.f < s[j - 1].f) { s[j] = s[j - 1]; --j; }
+        s[j] = v;
+    }
+}
+
+// opt/nelder_mead.hpp:111-229 — bounded 2-D Nelder-Mead
+template <class F>
+inline NMPoint nelder_mead2d(F&& f, double init_a, double init_b, double lb = 1e-4, double ub = 1000.0,
+                             double tol = 1e-4, int max_iter = 100) {
+    auto clamp = [&](double v) { return std::clamp(v, lb, ub); };
+    auto eval = [&](double a, double b) { const double ca = clamp(a), cb = clamp(b); return NMPoint{ca, cb, f(ca, cb)}; };
+    const double step_a = std::max(0.1, 0.2 * init_a), step_b = std::max(0.1, 0.2 * init_b);
+    std::array<NMPoint, 3> s = {eval(init_a, init_b), eval(init_a + step_a, init_b), eval(init_a, init_b + step_b)};
+    const double alpha = 1.0, gamma = 2.0, rho = 0.5, sigma = 0.5;
+    for (int iter = 0; iter < max_iter; ++iter) {
+        sort3(s);
+        if (std::fabs(s[2].f - s[0].f) < tol && std::fabs(s[2].a - s[0].a) < tol && std::fabs(s[2].b - s[0].b) < tol) break;
+        const double c_a = 0.5 * (s[0].a + s[1].a), c_b = 0.5 * (s[0].b + s[1].b);
+        const NMPoint r = eval(c_a + alpha * (c_a - s[2].a), c_b + alpha * (c_b - s[2].b));
+        if (r.f < s[0].f) {
+            const NMPoint e = eval(c_a + gamma * (r.a - c_a), c_b + gamma * (r.b - c_b));
+            s[2] = (e.f < r.f) ? e : r;
+        } else if (r.f < s[1].f) {
+            s[2] = r;
+        } else {
+            const bool outside = r.f < s[2].f;
+            const NMPoint c = outside ? eval(c_a + rho * (r.a - c_a), c_b + rho * (r.b - c_b))
+                                      : eval(c_a + rho * (s[2].a - c_a), c_b + rho * (s[2].b - c_b));
+            const double ref_f = outside ? r.f : s[2].f;
+            if (c.f < ref_f) {
+                s[2] = c;
+            } else {
+                s[1] = eval(s[0].a + sigma * (s[1].a - s[0].a), s[0].b + sigma * (s[1].b - s[0].b));
+                s[2] = eval(s[0].a + sigma * (s[2].a - s[0].a), s[0].b + sigma * (s[2].b - s[0].b));
+            }
+        }
+    }
+    sort3(s);
+    return s[0];
+}
+
+struct FelSite {
+    double alpha = 0, beta = 0, alpha_null = 0, lrt = 0, p_value = 1, total_bl = 0, lnl_alt = 0, lnl_null = 0;
+    int evals = 0;
+};
+struct FelRun {
+    double conversion = 1.0, tested_length = 0.0;
+    std::vector<double> bl;           // branch lengths in FEL time (x conversion)
+    std::vector<FelSite> patterns;
+};
+
+// fel.hpp:230-273 (every branch tested): t_b <- t_b * 3 / scale_factor(base model)
+inline FelRun fel_prepare(const Tree& tr, const Alignment& a, const Params& base) {
+    FelRun r;
+    MG94 m0; m0.update(base, a.pos_freq, a.pi, a.code);
+    r.conversion = m0.mu > 1e-12 ? 3.0 / m0.mu : 1.0;
+    r.bl.assign(tr.n(), 0.0);
+    for (int i = 0; i < tr.n(); ++i) if (i != tr.root) { r.tested_length += tr.bl[i]; r.bl[i] = tr.bl[i] * r.conversion; }
+    return r;
+}
+
+// fel.hpp:326-446 (analyze_pattern, num_background == 0)
+inline FelSite fel_pattern(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
+                           const FelRun& run, int p) {
+    FelSite res;
+    int first = -1; bool invariant = true;
+    for (int t = 0; t < a.T; ++t) {
+        const int st = a.states[size_t(p) * a.T + t];
+        if (st >= 0) { if (first == -1) first = st; else if (st != first) { invariant = false; break; } }
+    }
+    if (invariant) return res;
+    const int S = a.code.S, n = tr.n();
+    MG94 mg; double cached = -1.0;
+    std::vector<Mat> Pb(n, Mat::eye(S));
+    Pass w;
+    auto lnl = [&](double aa, double bb) {
+        ++res.evals;
+        const double as = std::max(aa, 1e-12), om = bb / as;
+        if (std::fabs(om - cached) > 1e-12) {
+            Params q = base; q.alpha = 1.0; q.beta = om;
+            mg.update(q, a.pos_freq, a.pi, a.code);
+            cached = om;
+        }
+        for (int i = 0; i < n; ++i) if (i != tr.root) Pb[i] = mg.P(as * run.bl[i]);
+        inside_outside(tr, a, p, l2t, Pb, mg.pi, S, w, false);
+        return w.logL;
+    };
+    static const double grid[12][2] = {{0.01, 0.1}, {1.0, 0.1}, {1.0, 0.5}, {1.0, 1.0}, {1.0, 5.0}, {10.0, 0.1},
+                                       {0.01, 0.5}, {0.01, 5.0}, {10.0, 0.5}, {10.0, 1.0}, {10.0, 50.0}, {100.0, 1.0}};
+    double best = -1e20, ba = 1.0, bb = 1.0;
+    for (auto& g : grid) { const double l = lnl(g[0], g[1]); if (l > best) { best = l; ba = g[0]; bb = g[1]; } }
+    const NMPoint alt = nelder_mead2d([&](double x, double y) { return -lnl(x, y); }, ba, bb, 1e-4, 1000.0, 1e-4, 100);
+    res.alpha = alt.a; res.beta = alt.b; res.lnl_alt = -alt.f;
+    const double init_null = (std::min(res.alpha, 100.0) + 3.0 * std::min(res.beta, 100.0)) / 4.0;
+    double best_null = lnl(init_null, init_null), best_na = init_null;
+    for (double c : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0}) { const double l = lnl(c, c); if (l > best_null) { best_null = l; best_na = c; } }
+    const auto nul = brent1d([&](double x) { return -lnl(x, x); }, 1e-4, std::clamp(best_na, 0.01, 45.0), 50.0, 1e-4, 60);
+    res.alpha_null = nul.first; res.lnl_null = -nul.second;
+    double lrt = 0.0;
+    if (res.lnl_alt > -1e10 && res.lnl_null > -1e10) lrt = std::max(0.0, 2.0 * (res.lnl_alt - res.lnl_null));
+    res.lrt = lrt;
+    res.p_value = std::erfc(std::sqrt(lrt / 2.0));
+    res.total_bl = res.alpha_null * run.tested_length;
+    return res;
+}
+
+// fel.hpp:778-833 (run): every pattern, in parallel
+inline FelRun fel_run(const Tree& tr, const Alignment& a, const Params& base, int max_patterns = -1) {
+    FelRun run = fel_prepare(tr, a, base);
+    const auto l2t = leaf_map(tr, a);
+    const int P = max_patterns < 0 ? a.P : std::min(a.P, max_patterns);
+    run.patterns.assign(P, FelSite{});
+    #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(P))
+    for (int p = 0; p < P; ++p) run.patterns[p] = fel_pattern(tr, a, l2t, base, run, p);
+    return run;
 }
 
 } // namespace h3o

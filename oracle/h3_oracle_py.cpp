@@ -71,6 +71,7 @@ PYBIND11_MODULE(h3oracle, m) {
         .def_readonly("num_patterns", &Alignment::P)
         .def_readonly("num_codons", &Alignment::n_codons)
         .def_readonly("weights", &Alignment::weights)
+        .def_readonly("site_pattern", &Alignment::site_pattern)
         .def_readonly("pi", &Alignment::pi)
         .def_property_readonly("nuc_freq", [](const Alignment& a) { return std::vector<double>(a.nuc_freq, a.nuc_freq + 4); })
         .def_property_readonly("pos_freq", [](const Alignment& a) {
@@ -159,6 +160,27 @@ PYBIND11_MODULE(h3oracle, m) {
        py::arg("is_test") = std::vector<bool>{}, py::arg("rates") = std::vector<double>{}, py::arg("rate_w") = std::vector<double>{},
        py::arg("branch_lengths") = std::vector<double>{}, py::arg("normalized_time") = false, py::arg("want_global") = false,
        py::arg("zero_l_sentinel") = false);
+    m.def("fel_run", [](const Tree& t, const Alignment& a, const py::dict& p, int max_patterns) {
+        const Params pp = params_from(p);
+        FelRun r;
+        { py::gil_scoped_release rel; r = fel_run(t, a, pp, max_patterns); }
+        const size_t P = r.patterns.size();
+        py::dict d;
+        auto col = [&](auto get) { py::array_t<double> x(P); for (size_t i = 0; i < P; ++i) x.mutable_data()[i] = get(r.patterns[i]); return x; };
+        d["alpha"] = col([](const FelSite& s) { return s.alpha; });
+        d["beta"] = col([](const FelSite& s) { return s.beta; });
+        d["alpha_null"] = col([](const FelSite& s) { return s.alpha_null; });
+        d["lrt"] = col([](const FelSite& s) { return s.lrt; });
+        d["p_value"] = col([](const FelSite& s) { return s.p_value; });
+        d["total_branch_length"] = col([](const FelSite& s) { return s.total_bl; });
+        d["log_l_alt"] = col([](const FelSite& s) { return s.lnl_alt; });
+        d["log_l_null"] = col([](const FelSite& s) { return s.lnl_null; });
+        d["evals"] = col([](const FelSite& s) { return double(s.evals); });
+        d["conversion"] = r.conversion;
+        d["tested_length"] = r.tested_length;
+        d["branch_lengths"] = r.bl;
+        return d;
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("max_patterns") = -1);
     m.def("set_threads", [](int n) {
 #ifdef _OPENMP
         omp_set_num_threads(n);

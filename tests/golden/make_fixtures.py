@@ -22,6 +22,9 @@ FILES = {
     # CD2 full alignment with embedded tree (tests/test_fel_cd2_parity.cpp)
     "CD2.nex": "benchmarks/data/CD2.nex",
     "cd2_reduced_point_truth.json": "benchmarks/ground_truth/cd2_reduced_point_truth.json",
+    # FEL parity on CD2 with matched branch lengths: tests/test_fel_cd2_parity.cpp:66-118
+    "cd2.fna": "benchmarks/data/cd2.fna",
+    "cd2_fitted.nwk": "benchmarks/data/cd2_fitted.nwk",
 }
 
 
@@ -56,6 +59,20 @@ def main(ref: str) -> None:
             "branch_length": 0.05, "fd_eps": 1e-6, "rel_err": 1e-5,
             "num_taxa": 23, "num_codons": 254, "num_nodes": 44,
         },
+    }
+    # HyPhy 2.5 FEL per-site table for CD2 (columns alpha, beta, alpha=beta, LRT, p-value, total branch
+    # length); only the MLE content of benchmarks/ground_truth/cd2_fel.json is kept
+    fel = json.loads((ref_root / "benchmarks/ground_truth/cd2_fel.json").read_text())
+    known["cd2_fel"] = {
+        "source": "benchmarks/ground_truth/cd2_fel.json (HyPhy 2.5); compared in tests/test_fel_cd2_parity.cpp:66-118",
+        "headers": [h[0] for h in fel["MLE"]["headers"]],
+        "mle": fel["MLE"]["content"]["0"],
+        # tests/test_fel_cd2_parity.cpp:71-77
+        "params": {"alpha": 1.0, "beta": 1.012387352492807,
+                   "theta": [0.5521777318173139, 0.2653120245806623, 0.4932059218537349, 1.03133955537726,
+                             0.3054313963126315]},
+        # tests/test_fel_cd2_parity.cpp:113-116
+        "min_pearson_lrt": 0.998, "min_spearman_lrt": 0.995, "min_pearson_p": 0.993, "min_spearman_p": 0.995,
     }
     (out / "known_answers.json").write_text(json.dumps(known, indent=1) + "\n")
 
