@@ -1,6 +1,6 @@
 """Build the B200 library and its Python binding in-tree.
 
-    libh3g.so     hyphy-3_b200/lib/      CUDA kernels + C ABI (nvcc, sm_100a)
+    libh3g.so     hyphy-3_b200/lib/      CUDA kernels + C ABI (nvcc, sm_100a) and host C++20 drivers (g++)
     _hyphy3*.so   hyphy-3_b200/python/   pybind11 module over include/hyphy/core/likelihood_gpu.hpp
 
 Objects go to hyphy-3_b200/_build/.  Rebuilds only what is older than its
@@ -46,6 +46,7 @@ def build(force: bool = False) -> dict[str, pathlib.Path]:
     LIB.mkdir(exist_ok=True)
     headers = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "h3g.h"]
     sources = sorted(CSRC.glob("*.cu"))
+    host_sources = sorted(CSRC.glob("*.cpp"))       # host-only parts (C++20), built by the host compiler
     objs = []
     jobs = []
     for src in sources:
@@ -53,6 +54,12 @@ def build(force: bool = False) -> dict[str, pathlib.Path]:
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
             jobs.append([NVCC] + NVFLAGS + ["-c", str(src), "-o", str(obj)])
+    for src in host_sources:
+        obj = BUILD / (src.stem + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + headers):
+            jobs.append([HOSTCXX, "-O2", "-std=c++20", "-fPIC", "-Wall", "-Wextra", "-I/usr/local/cuda/include",
+                         f"-I{ROOT / 'include'}", "-c", str(src), "-o", str(obj)])
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
         list(ex.map(_run, jobs))
     lib = LIB / "libh3g.so"

@@ -11,6 +11,7 @@
 
 #include "../../include/h3g.h"
 #include "h3g_common.cuh"
+#include "h3g_fel.h"
 #include "h3g_kernels.h"
 #include "h3g_mixed.h"
 
@@ -47,6 +48,7 @@ struct h3g_problem {
     int n = 0, root = -1, T = 0, P = 0, Pp = 0, NI = 0, max_state = -1;
     std::vector<int> ch_off, ch, iidx, taxon, in_off, out_off, in_nodes, out_nodes, parent_h;
     std::vector<uint8_t> leaf;
+    std::vector<int8_t> states_pm;     // [P][T] as uploaded (per-pattern checks on the host)
     DevArena topo_mem, model_mem, work_mem;
     int *d_ch_off = nullptr, *d_ch = nullptr, *d_iidx = nullptr, *d_taxon = nullptr, *d_in_nodes = nullptr, *d_out_nodes = nullptr;
     int* d_parent = nullptr;
@@ -226,6 +228,7 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
             pr->out_off.push_back(int(pr->out_nodes.size()));
         }
         pr->parent_h.assign(parent, parent + n);
+        if (n_patterns > 0) pr->states_pm.assign(states, states + size_t(n_patterns) * n_taxa);
         // patterns, taxon-major with padding (missing data, weight 0)
         const int Pp = pr->Pp, T = n_taxa;
         std::vector<int8_t> st(size_t(std::max(T, 1)) * Pp, int8_t(-1));
@@ -280,6 +283,33 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
         return fail(ctx, H3G_ERR_ARG, e.what());
     }
 }
+
+namespace h3g {
+
+Topo problem_topo(h3g_problem* pr, int S) {
+    Topo t = pr->topo();
+    t.S = S;
+    t.all_mask = S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1);
+    return t;
+}
+
+cudaStream_t problem_stream(h3g_problem* pr) { return pr->ctx->stream; }
+
+bool fel_problem_view(h3g_problem* pr, FelProblemView* v) {
+    if (!pr || !v) return false;
+    v->n = pr->n; v->root = pr->root; v->T = pr->T; v->P = pr->P;
+    v->parent = pr->parent_h.data(); v->leaf = pr->leaf.data(); v->taxon = pr->taxon.data();
+    v->ch_off = pr->ch_off.data(); v->ch = pr->ch.data();
+    v->states = pr->states_pm.data();
+    v->device = pr->ctx->device;
+    return true;
+}
+
+void fel_set_error(h3g_problem* pr, const std::string& msg) {
+    if (pr && pr->ctx) pr->ctx->err = msg;
+}
+
+}  // namespace h3g
 
 extern "C" h3g_status h3g_problem_destroy(h3g_problem* prob) {
     if (!prob) return H3G_ERR_ARG;

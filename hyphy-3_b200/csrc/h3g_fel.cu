@@ -1,0 +1,427 @@
+// h3g_fel.cu — batched device evaluator for FEL per-site fits.
+//
+// The reference evaluates one pattern at a time on the CPU: for every trial
+// (alpha, beta) it re-eigensolves MG94 at omega = beta / alpha, builds the
+// transition matrix of every branch and prunes the single pattern
+// (analyses/fel.hpp:276-308, :365-383).  Here one optimiser step of every
+// pattern is evaluated in one batch:
+//
+//   k_fel_eig   one CTA per distinct omega of the batch: the symmetric form
+//               of Q(omega) = Qs + omega Qn is diagonalised by the parallel
+//               (round-robin) cyclic Jacobi method in shared memory; the
+//               slot receives lambda (clamped <= 0), U_pi and V_pi.
+//   k_fel_lnl   one CTA per request: single-pattern pruning in the spectral
+//               domain.  The message of branch b is
+//               U (e^{lambda a t_b} o (V L_b)), two 64x64 mat-vecs from shared
+//               memory, so no transition matrix is ever formed.  The tree is
+//               walked depth-first; open partials live on a per-CTA stack,
+//               with power-of-two rescaling when a partial falls below 2^-256.
+//
+// Everything is FP64: FEL results are compared with the reference's.
+#include <algorithm>
+#include <cmath>
+#include <new>
+#include <type_traits>
+#include <vector>
+
+#include "h3g_common.cuh"
+#include "h3g_fel.h"
+
+namespace h3g {
+
+Topo problem_topo(h3g_problem* pr, int S);         // h3g_capi.cu
+cudaStream_t problem_stream(h3g_problem* pr);      // h3g_capi.cu
+
+namespace {
+
+constexpr int kFT = 256;                  // threads per CTA
+constexpr int LD = SP + 1;                // padded row stride: column walks hit 32 distinct banks
+constexpr int kMaxSweeps = 30;
+constexpr int kMaxDepth = 1024;           // open internal nodes on the traversal stack
+constexpr size_t kEigSmem = size_t(2) * SP * LD * sizeof(double);
+constexpr size_t kLnlSmem = (size_t(2) * SP * LD + 4 * SP + 3 * SP) * sizeof(double);
+
+struct FelModel {
+    int S;
+    const double* Qs;     // [S][S]
+    const double* Qn;     // [S][S]
+    const double* sq;     // [64] sqrt(max(pi, 1e-12)), 0 on padding
+    const double* isq;    // [64] 1 / sq, 0 on padding
+    const double* pi;     // [64]
+    double* lam;          // [slots][64]
+    double* U;            // [slots][64*64]
+    double* V;            // [slots][64*64]
+};
+
+__device__ __forceinline__ double block_sum_or_max(double v, double* red, bool is_max) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = is_max ? fmax(v, w) : v + w;
+    }
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) red[warp] = v;
+    __syncthreads();
+    double r = red[0];
+    for (int k = 1; k < kFT / 32; ++k) r = is_max ? fmax(r, red[k]) : r + red[k];
+    __syncthreads();
+    return r;
+}
+
+// ----------------------------------------------------------------- eigensystems
+// grid n_eig, block 256.  Jacobi rotations as in Golub & Van Loan (Alg. 8.5.3);
+// one sweep = 63 rounds of 32 disjoint pairs (circle schedule), each round
+// A <- A J (columns) then A <- J^T A (rows), E <- E J.
+__global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __restrict__ omega, const int* __restrict__ slot) {
+    pdl_enter();
+    extern __shared__ __align__(16) double sm[];
+    double* A = sm;
+    double* E = sm + SP * LD;
+    __shared__ double rc[32], rsn[32], red[kFT / 32];
+    __shared__ int rp[32], rq[32], rot[32];
+    const int tid = threadIdx.x, S = f.S;
+    const double om = omega[blockIdx.x];
+    const int sl = slot[blockIdx.x];
+    for (int e = tid; e < SP2; e += kFT) {
+        const int i = e >> 6, j = e & 63;
+        double v = 0.0;
+        if (i < S && j < S && i != j) v = f.sq[i] * (f.Qs[i * S + j] + om * f.Qn[i * S + j]) * f.isq[j];
+        A[i * LD + j] = v;
+        E[i * LD + j] = i == j ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    if (tid < S) {
+        double row = 0.0;
+        for (int j = 0; j < S; ++j)
+            if (j != tid) row += f.Qs[tid * S + j] + om * f.Qn[tid * S + j];
+        A[tid * LD + tid] = -row;
+    }
+    __syncthreads();
+    for (int e = tid; e < SP2; e += kFT) {        // symmetric part (rate_matrix.hpp:236-237)
+        const int i = e >> 6, j = e & 63;
+        if (i < j) {
+            const double m = 0.5 * (A[i * LD + j] + A[j * LD + i]);
+            A[i * LD + j] = m;
+            A[j * LD + i] = m;
+        }
+    }
+    __syncthreads();
+    for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int e = tid; e < SP2; e += kFT) {
+            const int i = e >> 6, j = e & 63;
+            const double x = A[i * LD + j] * A[i * LD + j];
+            tot += x;
+            if (i != j) off += x;
+        }
+        off = block_sum_or_max(off, red, false);
+        tot = block_sum_or_max(tot, red, false);
+        if (off <= 1e-30 * tot || off == 0.0) break;
+        for (int round = 0; round < SP - 1; ++round) {
+            if (tid < 32) {
+                int p, q;
+                if (tid == 0) { p = SP - 1; q = round; }
+                else { p = (round + tid) % (SP - 1); q = (round - tid + (SP - 1)) % (SP - 1); }
+                if (p > q) { const int tmp = p; p = q; q = tmp; }
+                const double apq = A[p * LD + q];
+                double c = 1.0, s = 0.0;
+                const bool active = fabs(apq) >= 1e-300;
+                if (active) {
+                    const double tau = (A[q * LD + q] - A[p * LD + p]) / (2.0 * apq);
+                    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                    c = 1.0 / sqrt(1.0 + tt * tt);
+                    s = tt * c;
+                }
+                rp[tid] = p; rq[tid] = q; rc[tid] = c; rsn[tid] = s; rot[tid] = active;
+            }
+            __syncthreads();
+            for (int e = tid; e < 32 * SP; e += kFT) {      // columns p, q of A and E
+                const int k = e >> 6, i = e & 63;
+                if (!rot[k]) continue;
+                const int p = rp[k], q = rq[k];
+                const double c = rc[k], s = rsn[k];
+                const double akp = A[i * LD + p], akq = A[i * LD + q];
+                A[i * LD + p] = c * akp - s * akq;
+                A[i * LD + q] = s * akp + c * akq;
+                const double ekp = E[i * LD + p], ekq = E[i * LD + q];
+                E[i * LD + p] = c * ekp - s * ekq;
+                E[i * LD + q] = s * ekp + c * ekq;
+            }
+            __syncthreads();
+            for (int e = tid; e < 32 * SP; e += kFT) {      // rows p, q of A
+                const int k = e >> 6, j = e & 63;
+                if (!rot[k]) continue;
+                const int p = rp[k], q = rq[k];
+                const double c = rc[k], s = rsn[k];
+                const double apk = A[p * LD + j], aqk = A[q * LD + j];
+                A[p * LD + j] = c * apk - s * aqk;
+                A[q * LD + j] = s * apk + c * aqk;
+            }
+            __syncthreads();
+        }
+    }
+    double* lam = f.lam + size_t(sl) * SP;
+    double* U = f.U + size_t(sl) * SP2;
+    double* V = f.V + size_t(sl) * SP2;
+    if (tid < SP) lam[tid] = fmin(A[tid * LD + tid], 0.0);
+    for (int e = tid; e < SP2; e += kFT) {
+        const int a = e >> 6, b = e & 63;
+        U[e] = f.isq[a] * E[a * LD + b];                  // U_pi[i = a][k = b]
+        V[e] = E[b * LD + a] * f.sq[b];                   // V_pi[k = a][j = b]
+    }
+}
+
+// ---------------------------------------------------------------- likelihoods
+// grid n_req, block 256.  ev: depth-first events, 2 node + 1 = open internal
+// node, 2 node = close node (its message goes to the parent).
+__global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const double* __restrict__ bl, const int* __restrict__ ev,
+                                                 int n_ev, int depth, double* __restrict__ stack,
+                                                 const int* __restrict__ pattern, const double* __restrict__ avec,
+                                                 const int* __restrict__ slot, double* __restrict__ out) {
+    pdl_enter();
+    extern __shared__ __align__(16) double sm[];
+    double* sU = sm;
+    double* sV = sU + SP * LD;
+    double* part = sV + SP * LD;     // [4][64]
+    double* x = part + 4 * SP;
+    double* sL = x + SP;
+    double* lam = sL + SP;
+    __shared__ int sexp[kMaxDepth];
+    __shared__ double red[kFT / 32];
+    const int tid = threadIdx.x, S = t.S, r = blockIdx.x;
+    const int p = pattern[r], sl = slot[r];
+    const double a = avec[r];
+    const double* gU = f.U + size_t(sl) * SP2;
+    const double* gV = f.V + size_t(sl) * SP2;
+    for (int e = tid; e < SP2; e += kFT) {
+        const int i = e >> 6, j = e & 63;
+        sU[i * LD + j] = gU[e];
+        sV[i * LD + j] = gV[e];
+    }
+    if (tid < SP) lam[tid] = f.lam[size_t(sl) * SP + tid] * a;
+    double* stk = stack + size_t(r) * depth * SP;
+    const int row = tid & 63, qd = tid >> 6;
+    int sp = -1;
+    __syncthreads();
+    for (int k = 0; k < n_ev; ++k) {
+        const int code = ev[k], node = code >> 1;
+        if (code & 1) {                                    // open an internal node: partial = 1
+            ++sp;
+            if (tid < SP) stk[sp * SP + tid] = tid < S ? 1.0 : 0.0;
+            if (tid == 0) sexp[sp] = 0;
+            continue;
+        }
+        int Ev = 0;
+        if (t.leaf[node]) {                                // x = V * leaf vector
+            if (tid < SP) {
+                const int tx = t.taxon[node];
+                int st = -1;
+                uint64_t mk = t.all_mask;
+                if (tx >= 0) {
+                    st = t.states[size_t(tx) * t.Pp + p];
+                    if (st < 0) mk = t.masks[size_t(tx) * t.Pp + p];
+                }
+                double s = 0.0;
+                if (st >= 0) {
+                    s = sV[tid * LD + st];
+                } else {
+                    const bool all = mk == 0 || (mk & t.all_mask) == t.all_mask;
+                    for (int j = 0; j < S; ++j)
+                        if (all || ((mk >> j) & 1)) s += sV[tid * LD + j];
+                }
+                x[tid] = s;
+            }
+        } else {                                           // x = V * L(node), pop it
+            if (tid < SP) sL[tid] = stk[sp * SP + tid];
+            __syncthreads();
+            Ev = sexp[sp];
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) s = fma(sV[row * LD + 16 * qd + j], sL[16 * qd + j], s);
+            part[qd * SP + row] = s;
+            __syncthreads();
+            if (tid < SP) x[tid] = (part[tid] + part[SP + tid]) + (part[2 * SP + tid] + part[3 * SP + tid]);
+            --sp;
+        }
+        if (tid < SP) x[tid] *= exp(lam[tid] * bl[node]);
+        __syncthreads();
+        {                                                  // m = U x, into the parent's partial
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) s = fma(sU[row * LD + 16 * qd + j], x[16 * qd + j], s);
+            part[qd * SP + row] = s;
+        }
+        __syncthreads();
+        double v = 0.0;
+        if (tid < SP) {
+            const double m = tid < S ? fmax((part[tid] + part[SP + tid]) + (part[2 * SP + tid] + part[3 * SP + tid]), 0.0) : 0.0;
+            v = stk[sp * SP + tid] * m;
+            stk[sp * SP + tid] = v;
+        }
+        const double mx = block_sum_or_max(v, red, true);
+        if (mx > 0.0 && mx < 0x1p-256) {
+            if (tid < SP) stk[sp * SP + tid] = v * 0x1p256;
+            if (tid == 0) sexp[sp] += 256;
+        }
+        if (tid == 0) sexp[sp] += Ev;
+    }
+    // root: lnL = log(pi . L) - E ln 2, or the reference's -1e20 for L <= 0
+    double v = 0.0;
+    if (tid < S) v = f.pi[tid] * stk[tid];
+    const double L = block_sum_or_max(v, red, false);
+    if (tid == 0) out[r] = L > 0.0 ? log(L) - double(sexp[0]) * 0.69314718055994530942 : -1e20;
+}
+
+}  // namespace
+
+struct FelDevice {
+    h3g_problem* pr = nullptr;
+    cudaStream_t s = nullptr;
+    int S = 0, n = 0, n_ev = 0, depth = 1, max_req = 0, n_slots = 0;
+    Topo t{};
+    FelModel f{};
+    double* d_bl = nullptr;
+    int* d_ev = nullptr;
+    double* d_stack = nullptr;
+    unsigned char* d_req = nullptr;       // [om | a | eslot | pat | slot]
+    unsigned char* h_req = nullptr;       // pinned mirror
+    double* d_out = nullptr;
+    double* h_out = nullptr;
+    std::vector<void*> owned;
+    ~FelDevice() {
+        for (void* p : owned) cudaFree(p);
+        if (h_req) cudaFreeHost(h_req);
+        if (h_out) cudaFreeHost(h_out);
+    }
+    size_t off_a() const { return size_t(max_req) * sizeof(double); }
+    size_t off_eslot() const { return 2 * size_t(max_req) * sizeof(double); }
+    size_t off_pat() const { return off_eslot() + size_t(max_req) * sizeof(int); }
+    size_t off_slot() const { return off_pat() + size_t(max_req) * sizeof(int); }
+    size_t req_bytes() const { return off_slot() + size_t(max_req) * sizeof(int); }
+};
+
+FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
+                             const double* branch_lengths, int max_requests, int n_slots, std::string* err) {
+    FelProblemView v;
+    if (!fel_problem_view(pr, &v)) { *err = "invalid problem"; return nullptr; }
+    auto* d = new (std::nothrow) FelDevice;
+    if (!d) { *err = "host allocation failed"; return nullptr; }
+    d->pr = pr;
+    d->s = problem_stream(pr);
+    d->S = S;
+    d->n = v.n;
+    d->max_req = std::max(1, max_requests);
+    d->n_slots = std::max(1, n_slots);
+    d->t = problem_topo(pr, S);
+    // depth-first events in the reference's child order
+    std::vector<int> ev;
+    ev.reserve(2 * size_t(v.n));
+    int open = 0, deepest = 1;
+    std::vector<std::pair<int, int>> stk{{v.root, 0}};
+    ev.push_back(2 * v.root + 1);
+    open = 1;
+    while (!stk.empty()) {
+        auto& [u, k] = stk.back();
+        if (k < v.ch_off[u + 1] - v.ch_off[u]) {
+            const int c = v.ch[v.ch_off[u] + k++];
+            if (v.leaf[c]) {
+                ev.push_back(2 * c);
+            } else {
+                ev.push_back(2 * c + 1);
+                deepest = std::max(deepest, ++open);
+                stk.push_back({c, 0});
+            }
+        } else {
+            if (u != v.root) { ev.push_back(2 * u); --open; }
+            stk.pop_back();
+        }
+    }
+    if (deepest > kMaxDepth) { *err = "tree deeper than 1024 internal levels"; delete d; return nullptr; }
+    d->n_ev = int(ev.size());
+    d->depth = deepest;
+    std::vector<double> sq(SP, 0.0), isq(SP, 0.0), pp(SP, 0.0);
+    for (int i = 0; i < S; ++i) {
+        sq[i] = std::sqrt(std::max(pi[i], 1e-12));
+        isq[i] = 1.0 / sq[i];
+        pp[i] = pi[i];
+    }
+    auto take = [&](auto** ptr, size_t count) -> bool {
+        void* q = nullptr;
+        if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**ptr)) != cudaSuccess) return false;
+        d->owned.push_back(q);
+        *ptr = static_cast<std::remove_reference_t<decltype(*ptr)>>(q);
+        return true;
+    };
+    double *qs = nullptr, *qn = nullptr, *dsq = nullptr, *disq = nullptr, *dpi = nullptr;
+    bool ok = take(&qs, size_t(S) * S) && take(&qn, size_t(S) * S) && take(&dsq, SP) && take(&disq, SP) && take(&dpi, SP) &&
+              take(&d->f.lam, size_t(d->n_slots) * SP) && take(&d->f.U, size_t(d->n_slots) * SP2) &&
+              take(&d->f.V, size_t(d->n_slots) * SP2) && take(&d->d_bl, v.n) && take(&d->d_ev, ev.size()) &&
+              take(&d->d_stack, size_t(d->max_req) * d->depth * SP) && take(&d->d_out, d->max_req);
+    void* rq = nullptr;
+    ok = ok && cudaMalloc(&rq, d->req_bytes()) == cudaSuccess;
+    if (rq) d->owned.push_back(rq);
+    d->d_req = static_cast<unsigned char*>(rq);
+    ok = ok && cudaMallocHost(reinterpret_cast<void**>(&d->h_req), d->req_bytes()) == cudaSuccess &&
+         cudaMallocHost(reinterpret_cast<void**>(&d->h_out), d->max_req * sizeof(double)) == cudaSuccess;
+    if (!ok) { *err = "device allocation failed"; delete d; return nullptr; }
+    d->f.S = S; d->f.Qs = qs; d->f.Qn = qn; d->f.sq = dsq; d->f.isq = disq; d->f.pi = dpi;
+    cudaStream_t s = d->s;
+    ok = cudaMemcpyAsync(qs, Qs, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(qn, Qn, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(dsq, sq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(disq, isq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(dpi, pp.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_bl, branch_lengths, v.n * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess;
+    static bool configured = false;
+    if (ok && !configured) {
+        ok = cudaFuncSetAttribute(k_fel_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEigSmem)) == cudaSuccess &&
+             cudaFuncSetAttribute(k_fel_lnl, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLnlSmem)) == cudaSuccess;
+        configured = ok;
+    }
+    if (!ok) { *err = std::string("FEL set-up: ") + cudaGetErrorString(cudaGetLastError()); delete d; return nullptr; }
+    return d;
+}
+
+bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, int n_req,
+                     const int* req_pattern, const double* req_a, const int* req_slot, double* lnl_out, std::string* err) {
+    if (n_eig > d->max_req || n_req > d->max_req || n_eig < 0 || n_req < 0) { *err = "FEL batch too large"; return false; }
+    if (n_req == 0) return true;
+    for (int i = 0; i < n_eig; ++i)
+        if (eig_slot[i] < 0 || eig_slot[i] >= d->n_slots) { *err = "FEL eigensystem slot out of range"; return false; }
+    for (int i = 0; i < n_req; ++i)
+        if (req_slot[i] < 0 || req_slot[i] >= d->n_slots || req_pattern[i] < 0 || req_pattern[i] >= d->t.P) {
+            *err = "FEL request out of range";
+            return false;
+        }
+    unsigned char* h = d->h_req;
+    std::copy(eig_omega, eig_omega + n_eig, reinterpret_cast<double*>(h));
+    std::copy(req_a, req_a + n_req, reinterpret_cast<double*>(h + d->off_a()));
+    std::copy(eig_slot, eig_slot + n_eig, reinterpret_cast<int*>(h + d->off_eslot()));
+    std::copy(req_pattern, req_pattern + n_req, reinterpret_cast<int*>(h + d->off_pat()));
+    std::copy(req_slot, req_slot + n_req, reinterpret_cast<int*>(h + d->off_slot()));
+    cudaStream_t s = d->s;
+    bool ok = cudaMemcpyAsync(d->d_req, h, d->req_bytes(), cudaMemcpyHostToDevice, s) == cudaSuccess;
+    unsigned char* q = d->d_req;
+    if (ok && n_eig > 0)
+        launch_k(k_fel_eig, n_eig, kFT, kEigSmem, s, d->f, reinterpret_cast<const double*>(q),
+                 reinterpret_cast<const int*>(q + d->off_eslot()));
+    if (ok)
+        launch_k(k_fel_lnl, n_req, kFT, kLnlSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
+                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack,
+                 reinterpret_cast<const int*>(q + d->off_pat()), reinterpret_cast<const double*>(q + d->off_a()),
+                 reinterpret_cast<const int*>(q + d->off_slot()), d->d_out);
+    ok = ok && cudaGetLastError() == cudaSuccess &&
+         cudaMemcpyAsync(d->h_out, d->d_out, n_req * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) { *err = std::string("FEL batch: ") + cudaGetErrorString(cudaGetLastError()); return false; }
+    std::copy(d->h_out, d->h_out + n_req, lnl_out);
+    return true;
+}
+
+void fel_device_destroy(FelDevice* d) {
+    if (d && d->s) cudaStreamSynchronize(d->s);
+    delete d;
+}
+
+}  // namespace h3g

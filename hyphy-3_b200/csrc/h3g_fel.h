@@ -1,0 +1,37 @@
+// h3g_fel.h — FEL per-site fits: the batched device evaluator (h3g_fel.cu) and
+// the host driver that runs one optimiser per pattern (h3g_fel_driver.cpp).
+// Plain C++ (no device code), so the driver builds with the host compiler.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/h3g.h"
+
+namespace h3g {
+
+// Host view of an uploaded problem (h3g_capi.cu).
+struct FelProblemView {
+    int n = 0, root = -1, T = 0, P = 0;
+    const int* parent = nullptr;      // [n]
+    const uint8_t* leaf = nullptr;    // [n]
+    const int* taxon = nullptr;       // [n] alignment row of each leaf, -1 otherwise
+    const int* ch_off = nullptr;      // [n + 1] children CSR
+    const int* ch = nullptr;
+    const int8_t* states = nullptr;   // [P][T] as uploaded
+    int device = 0;
+};
+bool fel_problem_view(h3g_problem* pr, FelProblemView* v);
+void fel_set_error(h3g_problem* pr, const std::string& msg);
+
+// Device evaluator.  Eigensystem slots hold (lambda, U, V) of
+// Q(omega) = Qs + omega Qn; a request evaluates one pattern's log-likelihood
+// at time scale a with the eigensystem in its slot.
+struct FelDevice;
+FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
+                             const double* branch_lengths, int max_requests, int n_slots, std::string* err);
+bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, int n_req,
+                     const int* req_pattern, const double* req_a, const int* req_slot, double* lnl_out, std::string* err);
+void fel_device_destroy(FelDevice* d);
+
+}  // namespace h3g

@@ -25,7 +25,7 @@ EXPORTED = [
     "h3g_ctx_create", "h3g_ctx_destroy", "h3g_last_error", "h3g_version", "h3g_problem_create",
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
-    "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc",
+    "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -39,6 +39,15 @@ class ModelDesc(C.Structure):
         ("M", C.c_int), ("rates", _dp), ("rate_w", _dp), ("time_mode", C.c_int), ("n_dirs", C.c_int),
         ("dQ", _dp), ("precision", C.c_int), ("zero_l_sentinel", C.c_int),
     ]
+
+
+class FelModel(C.Structure):
+    _fields_ = [("S", C.c_int), ("pi", _dp), ("Qs", _dp), ("Qn", _dp)]
+
+
+class FelResult(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("beta", C.c_double), ("alpha_null", C.c_double), ("log_l_alt", C.c_double),
+                ("log_l_null", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double), ("evaluations", C.c_int)]
 
 
 class Result(C.Structure):
@@ -78,6 +87,7 @@ def load() -> C.CDLL:
         lib.h3g_eval_from_P_noalloc.argtypes = [C.c_int, vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_uint8),
                                                 C.POINTER(C.c_int32), C.c_int, C.c_int, C.POINTER(C.c_int8),
                                                 C.POINTER(C.c_uint64), _dp, C.c_int, _dp, _dp, _dp, _dp]
+        lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
         for name in EXPORTED:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         lib.h3g_version.restype = C.c_char_p
@@ -206,6 +216,18 @@ class Problem:
         self.ctx.check(self.ctx.lib.h3g_branch_length_gradients(
             self.h, int(pi.size), _ptr(pi), _ptr(Q), _ptr(lam), _ptr(U), _ptr(V), _ptr(bl), precision, C.byref(lnl), _ptr(g)))
         return lnl.value, g
+
+    def fel_run(self, *, pi, Qs, Qn, branch_lengths) -> dict:
+        """FEL per-pattern fits (h3g_fel_run); branch lengths in FEL time.  Returns arrays per pattern."""
+        pi, Qs, Qn, bl = _f64(pi), _f64(Qs), _f64(Qn), _f64(branch_lengths)
+        S = int(pi.size)
+        if Qs.shape != (S, S) or Qn.shape != (S, S) or bl.size != self.n:
+            raise ValueError("Qs, Qn must be S x S and branch_lengths one per node")
+        m = FelModel(S=S, pi=_ptr(pi), Qs=_ptr(Qs), Qn=_ptr(Qn))
+        res = (FelResult * max(self.P, 1))()
+        self.ctx.check(self.ctx.lib.h3g_fel_run(self.h, C.byref(m), _ptr(bl), res))
+        names = [f[0] for f in FelResult._fields_]
+        return {k: np.array([getattr(res[i], k) for i in range(self.P)]) for k in names}
 
     def _result_struct(self, out):
         return Result(site_lnl=_ptr(out["site_lnl"]), grad_t=_ptr(out["grad_t"]), grad_dir=_ptr(out["grad_dir"]),

@@ -183,6 +183,37 @@ h3g_status h3g_eval_from_P_noalloc(int device, void* cuda_stream, int n_nodes, c
                                    const int8_t* states, const uint64_t* masks, const double* weights, int S,
                                    const double* P, const double* pi, double* lnl, double* site_lnl);
 
+/* ---------------------------------------------------------------- FEL
+ * Fixed-effects likelihood per-site fits on the device, replacing
+ * FELAnalyzer::analyze_pattern / run (include/hyphy/analyses/fel.hpp:326-446,
+ * :778-833) for the case where every branch is tested.  Per pattern: the
+ * 12-point (alpha, beta) grid, the bounded 2-D Nelder-Mead of the alternative
+ * model, the null grid and Brent search on alpha = beta, then LRT and
+ * p = erfc(sqrt(LRT / 2)).  Each likelihood evaluation uses the MG94 model
+ * Q = Qs + (beta / alpha) Qn with time scaled by alpha, exactly as the
+ * reference; all patterns advance together, one batched device evaluation
+ * (eigensystems + single-pattern pruning) per optimiser step. */
+typedef struct {
+    int S;                    /* states (<= 64; 61 for the universal code) */
+    const double* pi;         /* S codon frequencies (root prior) */
+    const double* Qs;         /* S * S synonymous rates of the base model at alpha = 1, beta = 0 (diagonal ignored) */
+    const double* Qn;         /* S * S non-synonymous rates at alpha = 0, beta = 1 (diagonal ignored) */
+} h3g_fel_model;
+
+typedef struct {
+    double alpha, beta;       /* alternative-model MLE */
+    double alpha_null;        /* null-model (alpha = beta) MLE */
+    double log_l_alt, log_l_null;
+    double lrt, p_value;
+    int evaluations;          /* likelihood evaluations used; 0 for an invariant pattern (not fitted) */
+} h3g_fel_result;
+
+/* Fit every pattern of prob.  branch_lengths[n_nodes] are in the reference's
+ * FEL time (input length x 3 / mean rate of the base model, fel.hpp:230-273);
+ * out[n_patterns].  Blocks until done.  The problem's installed model (if
+ * any) is left untouched. */
+h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths, h3g_fel_result* out);
+
 #ifdef __cplusplus
 }
 #endif
