@@ -5,6 +5,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include "hyphy/analyses/fel_gpu.hpp"
 #include "hyphy/core/likelihood_gpu.hpp"
 
 namespace py = pybind11;
@@ -226,4 +227,42 @@ PYBIND11_MODULE(_hyphy3, m) {
     }, "precision"_a);
     m.def("get_precision", []() { return LikelihoodEngine::get_precision() == H3G_PREC_MIXED ? "mixed" : "fp64"; });
     m.def("library_version", []() { return std::string(h3g_version()); });
+
+    // FEL (bindings.cpp:121-188 of the reference): settings, per-site results, analyzer
+    using hyphy::analyses::FELAnalyzer;
+    using hyphy::analyses::FELSettings;
+    using hyphy::analyses::SiteResult;
+    py::class_<FELSettings>(m, "FELSettings")
+        .def(py::init<>())
+        .def_readwrite("p_value_threshold", &FELSettings::p_value_threshold)
+        .def_readwrite("full_model", &FELSettings::full_model)
+        .def_readwrite("srv", &FELSettings::srv)
+        .def_readwrite("test_branches", &FELSettings::test_branches)
+        .def_readwrite("test_branch_regex", &FELSettings::test_branch_regex)
+        .def_readwrite("test_branch_names", &FELSettings::test_branch_names);
+    py::class_<SiteResult>(m, "FELSiteResult")
+        .def_readonly("site_index", &SiteResult::site_index)
+        .def_readonly("alpha", &SiteResult::alpha)
+        .def_readonly("beta", &SiteResult::beta)
+        .def_readonly("beta_nuisance", &SiteResult::beta_nuisance)
+        .def_readonly("beta_background", &SiteResult::beta_nuisance)
+        .def_readonly("alpha_null", &SiteResult::alpha_null)
+        .def_readonly("lrt", &SiteResult::lrt)
+        .def_readonly("p_value", &SiteResult::p_value)
+        .def_readonly("total_branch_length", &SiteResult::total_branch_length)
+        .def_readonly("log_l_alt", &SiteResult::log_l_alt)
+        .def_readonly("log_l_null", &SiteResult::log_l_null)
+        .def_readonly("evaluations", &SiteResult::evaluations);
+    py::class_<FELAnalyzer>(m, "FELAnalyzer")
+        .def(py::init([](Tree tree, Alignment aln, const MG94Parameters& params, const FELSettings& settings) {
+                 return FELAnalyzer(std::move(tree), std::move(aln), params, settings);
+             }),
+             "tree"_a, "alignment"_a, "params"_a = MG94Parameters{}, "settings"_a = FELSettings{})
+        .def("run", [](FELAnalyzer& f, bool show_progress, bool force_progress) {
+                 py::gil_scoped_release rel;
+                 return f.run(show_progress, force_progress);
+             }, "show_progress"_a = false, "force_progress"_a = false)
+        .def_readonly("conversion_factor", &FELAnalyzer::conversion_factor)
+        .def_readonly("baseline_tree_length", &FELAnalyzer::baseline_tree_length)
+        .def_readonly("site_results", &FELAnalyzer::site_results);
 }

@@ -15,6 +15,9 @@ if _pydir not in sys.path:
 
 from _hyphy3 import (  # noqa: E402
     Alignment,
+    FELAnalyzer,
+    FELSettings,
+    FELSiteResult,
     GeneticCode,
     MG94Parameters,
     Tree,
@@ -35,7 +38,7 @@ from . import autograd  # noqa: E402
 
 __version__ = "3.0.0"
 __all__ = [
-    "Alignment", "GeneticCode", "MG94Parameters", "Tree", "TreeNode", "build_leaf_to_taxon_map",
+    "Alignment", "FELAnalyzer", "FELSettings", "FELSiteResult", "GeneticCode", "MG94Parameters", "Tree", "TreeNode", "build_leaf_to_taxon_map",
     "compute_branch_length_gradients", "compute_joint_frechet_gradients", "compute_mg94_log_likelihood",
     "compute_mixture_gradients", "compute_tree_log_likelihood_from_P", "get_precision", "library_version",
     "mg94_eigensystem", "set_precision", "autograd",

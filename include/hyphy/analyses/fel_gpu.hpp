@@ -1,0 +1,128 @@
+// fel_gpu.hpp — drop-in FELAnalyzer (include/hyphy/analyses/fel.hpp) whose
+// per-site fits run on the device through h3g_fel_run.
+//
+// Same constructor and run() as the reference class: the constructor converts
+// branch lengths to the FEL time scale (t x 3 / mean rate of the base MG94
+// model, fel.hpp:230-273); run() fits every site pattern (fel.hpp:326-446)
+// and maps patterns back to sites (fel.hpp:778-833).  Only the path where every
+// branch is tested (FELSettings::test_branches == "All", no regex, no names)
+// is on the device; any other selection throws std::runtime_error.  Ancestral
+// substitution summaries (SiteResult::subs in the reference) are not produced.
+#pragma once
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../core/likelihood_gpu.hpp"
+
+namespace hyphy::analyses {
+
+using hyphy::core::Alignment;
+using hyphy::core::MG94Matrix;
+using hyphy::core::MG94Parameters;
+using hyphy::core::Scalar;
+using hyphy::core::Tree;
+
+struct FELSettings {
+    Scalar p_value_threshold = 0.1;
+    bool full_model = true;
+    bool srv = true;
+    std::string test_branches = "All";
+    std::string test_branch_regex = "";
+    std::vector<std::string> test_branch_names = {};
+};
+
+struct SiteResult {
+    size_t site_index = 0;
+    Scalar alpha = 0.0;
+    Scalar beta = 0.0;
+    Scalar beta_nuisance = 0.0;
+    Scalar alpha_null = 0.0;
+    Scalar lrt = 0.0;
+    Scalar p_value = 1.0;
+    Scalar total_branch_length = 0.0;
+    Scalar log_l_alt = 0.0;
+    Scalar log_l_null = 0.0;
+    int evaluations = 0;          // likelihood evaluations of the pattern's search (0: invariant)
+};
+
+class FELAnalyzer {
+public:
+    Tree tree;
+    Alignment aln;
+    MG94Parameters base_params;
+    FELSettings settings;
+    Scalar p_value_threshold = 0.1;
+    Scalar baseline_tree_length = 0.0;
+    Scalar baseline_tested_tree_length = 0.0;
+    Scalar conversion_factor = 1.0;
+    std::vector<SiteResult> site_results;
+
+    FELAnalyzer(Tree t, Alignment a, MG94Parameters params = MG94Parameters{}, FELSettings s = FELSettings{}, Scalar bg_om = -1.0)
+        : tree(std::move(t)), aln(std::move(a)), base_params(params), settings(std::move(s)) {
+        (void)bg_om;
+        if (settings.test_branches != "All" || !settings.test_branch_regex.empty() || !settings.test_branch_names.empty())
+            throw std::runtime_error("FELAnalyzer (device): only the all-branches-tested analysis is supported");
+        p_value_threshold = settings.p_value_threshold;
+        prepare_branch_lengths();
+    }
+
+    // fel.hpp:230-273 with every branch tested
+    void prepare_branch_lengths() {
+        const auto& code = aln.code ? *aln.code : *hyphy::core::GeneticCode::universal();
+        MG94Matrix base;
+        base.update(base_params, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        conversion_factor = base.scale_factor > 1e-12 ? 3.0 / base.scale_factor : 1.0;
+        baseline_tree_length = baseline_tested_tree_length = 0.0;
+        for (auto& node : tree.nodes) {
+            if (node.id == tree.root_id) continue;
+            baseline_tree_length += node.branch_length;
+            baseline_tested_tree_length += node.branch_length;
+            node.branch_length *= conversion_factor;
+        }
+    }
+
+    std::vector<SiteResult> run(bool show_progress = false, bool force_progress = false) {
+        (void)show_progress; (void)force_progress;
+        auto& eng = hyphy::core::gpu_detail::Engine::get();
+        const auto l2t = hyphy::core::LikelihoodEngine::build_leaf_to_taxon_map(tree, aln);
+        h3g_problem* pr = eng.problem(tree, aln, l2t);
+        const auto& code = aln.code ? *aln.code : *hyphy::core::GeneticCode::universal();
+        const int S = code.num_sense_codons;
+        MG94Parameters ps = base_params, pn = base_params;
+        ps.alpha = 1.0; ps.beta = 0.0;
+        pn.alpha = 0.0; pn.beta = 1.0;
+        MG94Matrix ms, mn;
+        ms.update(ps, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        mn.update(pn, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        const size_t nS = static_cast<size_t>(S);
+        std::vector<double> pi(nS), qs(nS * nS), qn(nS * nS), bl(tree.num_nodes(), 0.0);
+        for (int i = 0; i < S; ++i) {
+            pi[size_t(i)] = aln.codon_frequencies_f3x4[size_t(i)];
+            for (int j = 0; j < S; ++j) {
+                qs[size_t(i) * S + j] = i == j ? 0.0 : ms.Q(i, j);
+                qn[size_t(i) * S + j] = i == j ? 0.0 : mn.Q(i, j);
+            }
+        }
+        for (const auto& node : tree.nodes)
+            if (node.id != tree.root_id) bl[size_t(node.id)] = node.branch_length;
+        h3g_fel_model m{S, pi.data(), qs.data(), qn.data()};
+        std::vector<h3g_fel_result> res(aln.patterns.size());
+        eng.check(h3g_fel_run(pr, &m, bl.data(), res.data()));
+        site_results.assign(aln.num_codons, SiteResult{});
+        for (size_t s = 0; s < aln.num_codons; ++s) {
+            const auto& r = res[aln.site_to_pattern[s]];
+            SiteResult& o = site_results[s];
+            o.site_index = s;
+            o.alpha = r.alpha; o.beta = r.beta; o.alpha_null = r.alpha_null;
+            o.lrt = r.lrt; o.p_value = r.p_value;
+            o.log_l_alt = r.log_l_alt; o.log_l_null = r.log_l_null;
+            o.total_branch_length = r.alpha_null * baseline_tested_tree_length;
+            o.evaluations = r.evaluations;
+        }
+        return site_results;
+    }
+};
+
+}  // namespace hyphy::analyses

@@ -91,3 +91,32 @@ def test_fel_rejects_bad_arguments(ctx, oracle, golden_dir):
         pr.fel_run(pi=pi, Qs=-qs, Qn=qn, branch_lengths=bl)
     out = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)
     assert np.all(out["lrt"] >= 0) and np.all((out["p_value"] >= 0) & (out["p_value"] <= 1))
+
+
+def test_fel_analyzer_api_matches_reference_test(oracle, golden_dir):
+    """hyphy3.FELAnalyzer(tree, aln, params).run(): the reference's CD2 parity case, site by site."""
+    import _hyphy3 as h3
+    k = json.loads((golden_dir / "known_answers.json").read_text())["cd2_fel"]
+    a = h3.Alignment.load(str(golden_dir / "cd2.fna"))
+    t = h3.Tree.from_newick_file(str(golden_dir / "cd2_fitted.nwk"))
+    p = h3.MG94Parameters()
+    p.alpha, p.beta = k["params"]["alpha"], k["params"]["beta"]
+    p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = k["params"]["theta"]
+    res = h3.FELAnalyzer(t, a, p).run()
+    assert len(res) == 187
+    lrt = np.array([r.lrt for r in res])
+    pv = np.array([r.p_value for r in res])
+    mle = np.array(k["mle"])
+    assert np.corrcoef(lrt, mle[:, 3])[0, 1] > k["min_pearson_lrt"]
+    assert np.corrcoef(pv, mle[:, 4])[0, 1] > k["min_pearson_p"]
+    oa = oracle.Alignment.load(str(golden_dir / "cd2.fna"))
+    ot = oracle.Tree.parse((golden_dir / "cd2_fitted.nwk").read_text())
+    ref = oracle.fel_run(ot, oa, k["params"])
+    sp = np.array(oa.site_pattern)
+    np.testing.assert_allclose(lrt, np.asarray(ref["lrt"])[sp], rtol=0, atol=2e-4)
+    np.testing.assert_allclose([r.total_branch_length for r in res], np.asarray(ref["total_branch_length"])[sp],
+                               rtol=1e-3, atol=1e-6)
+    with pytest.raises(RuntimeError):
+        s = h3.FELSettings()
+        s.test_branches = "Internal"
+        h3.FELAnalyzer(t, a, p, s)
