@@ -309,6 +309,11 @@ void fel_set_error(h3g_problem* pr, const std::string& msg) {
     if (pr && pr->ctx) pr->ctx->err = msg;
 }
 
+void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h) {
+    pr->last_h2d = h2d;
+    pr->last_d2h = d2h;
+}
+
 }  // namespace h3g
 
 extern "C" h3g_status h3g_problem_destroy(h3g_problem* prob) {

@@ -282,21 +282,18 @@ struct FelDevice {
     double* d_bl = nullptr;
     int* d_ev = nullptr;
     double* d_stack = nullptr;
-    unsigned char* d_req = nullptr;       // [om | a | eslot | pat | slot]
+    unsigned char* d_req = nullptr;       // per batch: [om | a | eslot | pat | slot], packed to the batch's sizes
     unsigned char* h_req = nullptr;       // pinned mirror
     double* d_out = nullptr;
     double* h_out = nullptr;
+    size_t h2d = 0, d2h = 0;              // bytes moved by the batches so far
     std::vector<void*> owned;
     ~FelDevice() {
         for (void* p : owned) cudaFree(p);
         if (h_req) cudaFreeHost(h_req);
         if (h_out) cudaFreeHost(h_out);
     }
-    size_t off_a() const { return size_t(max_req) * sizeof(double); }
-    size_t off_eslot() const { return 2 * size_t(max_req) * sizeof(double); }
-    size_t off_pat() const { return off_eslot() + size_t(max_req) * sizeof(int); }
-    size_t off_slot() const { return off_pat() + size_t(max_req) * sizeof(int); }
-    size_t req_bytes() const { return off_slot() + size_t(max_req) * sizeof(int); }
+    size_t req_bytes() const { return 2 * size_t(max_req) * sizeof(double) + 3 * size_t(max_req) * sizeof(int); }
 };
 
 FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
@@ -394,29 +391,40 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int
             *err = "FEL request out of range";
             return false;
         }
+    // one host-to-device copy of exactly this batch's arrays
+    const size_t o_a = size_t(n_eig) * sizeof(double), o_es = o_a + size_t(n_req) * sizeof(double);
+    const size_t o_pat = o_es + size_t(n_eig) * sizeof(int), o_sl = o_pat + size_t(n_req) * sizeof(int);
+    const size_t bytes = o_sl + size_t(n_req) * sizeof(int);
     unsigned char* h = d->h_req;
     std::copy(eig_omega, eig_omega + n_eig, reinterpret_cast<double*>(h));
-    std::copy(req_a, req_a + n_req, reinterpret_cast<double*>(h + d->off_a()));
-    std::copy(eig_slot, eig_slot + n_eig, reinterpret_cast<int*>(h + d->off_eslot()));
-    std::copy(req_pattern, req_pattern + n_req, reinterpret_cast<int*>(h + d->off_pat()));
-    std::copy(req_slot, req_slot + n_req, reinterpret_cast<int*>(h + d->off_slot()));
+    std::copy(req_a, req_a + n_req, reinterpret_cast<double*>(h + o_a));
+    std::copy(eig_slot, eig_slot + n_eig, reinterpret_cast<int*>(h + o_es));
+    std::copy(req_pattern, req_pattern + n_req, reinterpret_cast<int*>(h + o_pat));
+    std::copy(req_slot, req_slot + n_req, reinterpret_cast<int*>(h + o_sl));
     cudaStream_t s = d->s;
-    bool ok = cudaMemcpyAsync(d->d_req, h, d->req_bytes(), cudaMemcpyHostToDevice, s) == cudaSuccess;
+    bool ok = cudaMemcpyAsync(d->d_req, h, bytes, cudaMemcpyHostToDevice, s) == cudaSuccess;
     unsigned char* q = d->d_req;
     if (ok && n_eig > 0)
         launch_k(k_fel_eig, n_eig, kFT, kEigSmem, s, d->f, reinterpret_cast<const double*>(q),
-                 reinterpret_cast<const int*>(q + d->off_eslot()));
+                 reinterpret_cast<const int*>(q + o_es));
     if (ok)
         launch_k(k_fel_lnl, n_req, kFT, kLnlSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
                  static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack,
-                 reinterpret_cast<const int*>(q + d->off_pat()), reinterpret_cast<const double*>(q + d->off_a()),
-                 reinterpret_cast<const int*>(q + d->off_slot()), d->d_out);
+                 reinterpret_cast<const int*>(q + o_pat), reinterpret_cast<const double*>(q + o_a),
+                 reinterpret_cast<const int*>(q + o_sl), d->d_out);
+    d->h2d += bytes;
+    d->d2h += size_t(n_req) * sizeof(double);
     ok = ok && cudaGetLastError() == cudaSuccess &&
          cudaMemcpyAsync(d->h_out, d->d_out, n_req * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
          cudaStreamSynchronize(s) == cudaSuccess;
     if (!ok) { *err = std::string("FEL batch: ") + cudaGetErrorString(cudaGetLastError()); return false; }
     std::copy(d->h_out, d->h_out + n_req, lnl_out);
     return true;
+}
+
+void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h) {
+    *h2d = d->h2d;
+    *d2h = d->d2h;
 }
 
 void fel_device_destroy(FelDevice* d) {

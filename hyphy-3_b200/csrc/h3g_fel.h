@@ -3,6 +3,7 @@
 // Plain C++ (no device code), so the driver builds with the host compiler.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <string>
 
@@ -32,6 +33,9 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
                              const double* branch_lengths, int max_requests, int n_slots, std::string* err);
 bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, int n_req,
                      const int* req_pattern, const double* req_a, const int* req_slot, double* lnl_out, std::string* err);
+void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h);   // bytes moved by the batches
 void fel_device_destroy(FelDevice* d);
+// record a whole run's transfers where h3g_last_eval_transfer reports them (h3g_capi.cu)
+void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h);
 
 }  // namespace h3g

@@ -328,8 +328,12 @@ extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, con
                 }
             }
         }
+        size_t h2d = 0, d2h = 0;
+        fel_device_transfer(dev, &h2d, &d2h);
         fel_device_destroy(dev);
         if (st != H3G_OK) return st;
+        // the run's own inputs and outputs: model, branch lengths, per-pattern results
+        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h);
         for (int i = 0; i < N; ++i) {
             if (!fits[i].h.done()) { fel_set_error(prob, "h3g_fel_run: a pattern did not finish"); return H3G_ERR_STATE; }
             out[sites[i].pattern] = sites[i].res;
