@@ -71,7 +71,12 @@ __device__ __forceinline__ double block_sum_or_max(double v, double* red, bool i
 // grid n_eig, block 256.  Jacobi rotations as in Golub & Van Loan (Alg. 8.5.3);
 // one sweep = 63 rounds of 32 disjoint pairs (circle schedule), each round
 // A <- A J (columns) then A <- J^T A (rows), E <- E J.
-__global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __restrict__ omega, const int* __restrict__ slot) {
+// Warm start: when prev[r] >= 0 the eigenvectors E0 of that slot (E0 = D^1/2 U)
+// are the starting basis: A <- E0^T A E0, E <- E0.  A pattern's next omega is
+// usually close to its last one, so the rotated matrix is nearly diagonal and
+// the sweeps needed drop from ~8 to 2-3.
+__global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __restrict__ omega, const int* __restrict__ slot,
+                                                 const int* __restrict__ prev) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* A = sm;
@@ -105,6 +110,48 @@ __global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __res
         }
     }
     __syncthreads();
+    const int pv = prev[blockIdx.x];
+    if (pv >= 0) {
+        const double* U0 = f.U + size_t(pv) * SP2;
+        for (int e = tid; e < SP2; e += kFT) {
+            const int i = e >> 6, k = e & 63;
+            E[i * LD + k] = i < S ? f.sq[i] * U0[e] : (i == k ? 1.0 : 0.0);
+        }
+        __syncthreads();
+        const int i = tid & 63, kq = (tid >> 6) * 16;
+        double acc[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) acc[m] = 0.0;
+        for (int j = 0; j < SP; ++j) {                   // T = A E0, row i, columns kq..kq+15
+            const double aij = A[i * LD + j];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) acc[m] = fma(aij, E[j * LD + kq + m], acc[m]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) A[i * LD + kq + m] = acc[m];
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) acc[m] = 0.0;
+        for (int j = 0; j < SP; ++j) {                   // B = E0^T T, row k = i, columns kq..kq+15
+            const double ejk = E[j * LD + i];
+#pragma unroll
+            for (int m = 0; m < 16; ++m) acc[m] = fma(ejk, A[j * LD + kq + m], acc[m]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) A[i * LD + kq + m] = acc[m];
+        __syncthreads();
+        for (int e = tid; e < SP2; e += kFT) {           // re-symmetrise the rounding
+            const int a = e >> 6, b = e & 63;
+            if (a < b) {
+                const double m = 0.5 * (A[a * LD + b] + A[b * LD + a]);
+                A[a * LD + b] = m;
+                A[b * LD + a] = m;
+            }
+        }
+        __syncthreads();
+    }
     for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
         double off = 0.0, tot = 0.0;
         for (int e = tid; e < SP2; e += kFT) {
@@ -251,19 +298,25 @@ __global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const doubl
             part[qd * SP + row] = s;
         }
         __syncthreads();
-        double v = 0.0;
         if (tid < SP) {
+            // the two warps that own the partial multiply, take its maximum between
+            // themselves (named barrier 1, 64 threads) and rescale; the other warps go on
             const double m = tid < S ? fmax((part[tid] + part[SP + tid]) + (part[2 * SP + tid] + part[3 * SP + tid]), 0.0) : 0.0;
-            v = stk[sp * SP + tid] * m;
+            double v = stk[sp * SP + tid] * m;
+            double w = v;
+            for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+            if ((tid & 31) == 0) red[tid >> 5] = w;
+            asm volatile("bar.sync 1, 64;" ::: "memory");
+            const double mx = fmax(red[0], red[1]);
+            if (mx > 0.0 && mx < 0x1p-256) {
+                v *= 0x1p256;
+                if (tid == 0) sexp[sp] += 256;
+            }
             stk[sp * SP + tid] = v;
+            if (tid == 0) sexp[sp] += Ev;
         }
-        const double mx = block_sum_or_max(v, red, true);
-        if (mx > 0.0 && mx < 0x1p-256) {
-            if (tid < SP) stk[sp * SP + tid] = v * 0x1p256;
-            if (tid == 0) sexp[sp] += 256;
-        }
-        if (tid == 0) sexp[sp] += Ev;
     }
+    __syncthreads();
     // root: lnL = log(pi . L) - E ln 2, or the reference's -1e20 for L <= 0
     double v = 0.0;
     if (tid < S) v = f.pi[tid] * stk[tid];
@@ -282,7 +335,7 @@ struct FelDevice {
     double* d_bl = nullptr;
     int* d_ev = nullptr;
     double* d_stack = nullptr;
-    unsigned char* d_req = nullptr;       // per batch: [om | a | eslot | pat | slot], packed to the batch's sizes
+    unsigned char* d_req = nullptr;       // per batch: [om | a | eslot | eprev | pat | slot], packed to the batch's sizes
     unsigned char* h_req = nullptr;       // pinned mirror
     double* d_out = nullptr;
     double* h_out = nullptr;
@@ -293,7 +346,7 @@ struct FelDevice {
         if (h_req) cudaFreeHost(h_req);
         if (h_out) cudaFreeHost(h_out);
     }
-    size_t req_bytes() const { return 2 * size_t(max_req) * sizeof(double) + 3 * size_t(max_req) * sizeof(int); }
+    size_t req_bytes() const { return 2 * size_t(max_req) * sizeof(double) + 4 * size_t(max_req) * sizeof(int); }
 };
 
 FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
@@ -380,12 +433,15 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     return d;
 }
 
-bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, int n_req,
+bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                      const int* req_pattern, const double* req_a, const int* req_slot, double* lnl_out, std::string* err) {
     if (n_eig > d->max_req || n_req > d->max_req || n_eig < 0 || n_req < 0) { *err = "FEL batch too large"; return false; }
     if (n_req == 0) return true;
     for (int i = 0; i < n_eig; ++i)
-        if (eig_slot[i] < 0 || eig_slot[i] >= d->n_slots) { *err = "FEL eigensystem slot out of range"; return false; }
+        if (eig_slot[i] < 0 || eig_slot[i] >= d->n_slots || eig_prev[i] < -1 || eig_prev[i] >= d->n_slots) {
+            *err = "FEL eigensystem slot out of range";
+            return false;
+        }
     for (int i = 0; i < n_req; ++i)
         if (req_slot[i] < 0 || req_slot[i] >= d->n_slots || req_pattern[i] < 0 || req_pattern[i] >= d->t.P) {
             *err = "FEL request out of range";
@@ -393,12 +449,14 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int
         }
     // one host-to-device copy of exactly this batch's arrays
     const size_t o_a = size_t(n_eig) * sizeof(double), o_es = o_a + size_t(n_req) * sizeof(double);
-    const size_t o_pat = o_es + size_t(n_eig) * sizeof(int), o_sl = o_pat + size_t(n_req) * sizeof(int);
+    const size_t o_pv = o_es + size_t(n_eig) * sizeof(int), o_pat = o_pv + size_t(n_eig) * sizeof(int);
+    const size_t o_sl = o_pat + size_t(n_req) * sizeof(int);
     const size_t bytes = o_sl + size_t(n_req) * sizeof(int);
     unsigned char* h = d->h_req;
     std::copy(eig_omega, eig_omega + n_eig, reinterpret_cast<double*>(h));
     std::copy(req_a, req_a + n_req, reinterpret_cast<double*>(h + o_a));
     std::copy(eig_slot, eig_slot + n_eig, reinterpret_cast<int*>(h + o_es));
+    std::copy(eig_prev, eig_prev + n_eig, reinterpret_cast<int*>(h + o_pv));
     std::copy(req_pattern, req_pattern + n_req, reinterpret_cast<int*>(h + o_pat));
     std::copy(req_slot, req_slot + n_req, reinterpret_cast<int*>(h + o_sl));
     cudaStream_t s = d->s;
@@ -406,7 +464,7 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int
     unsigned char* q = d->d_req;
     if (ok && n_eig > 0)
         launch_k(k_fel_eig, n_eig, kFT, kEigSmem, s, d->f, reinterpret_cast<const double*>(q),
-                 reinterpret_cast<const int*>(q + o_es));
+                 reinterpret_cast<const int*>(q + o_es), reinterpret_cast<const int*>(q + o_pv));
     if (ok)
         launch_k(k_fel_lnl, n_req, kFT, kLnlSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
                  static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack,

@@ -31,7 +31,8 @@ void fel_set_error(h3g_problem* pr, const std::string& msg);
 struct FelDevice;
 FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
                              const double* branch_lengths, int max_requests, int n_slots, std::string* err);
-bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, int n_req,
+// eig_prev[i] >= 0: slot whose eigenvectors start the solve (warm start), -1: from the identity
+bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                      const int* req_pattern, const double* req_a, const int* req_slot, double* lnl_out, std::string* err);
 void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h);   // bytes moved by the batches
 void fel_device_destroy(FelDevice* d);

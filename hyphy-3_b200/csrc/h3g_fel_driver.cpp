@@ -269,12 +269,13 @@ extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, con
         for (auto& s : sites) fits.push_back(fit_pattern(s));
         for (auto& f : fits) f.h.resume();                 // run to the first evaluation
         std::unordered_map<uint64_t, int> shared;          // omega bits -> shared slot
-        std::vector<int> req_site, req_pat, req_slot, eig_slot;
+        std::vector<int> req_site, req_pat, req_slot, eig_slot, eig_prev;
         std::vector<double> req_a, eig_om, lnl;
         std::unordered_map<uint64_t, int> count;
         h3g_status st = H3G_OK;
         while (st == H3G_OK) {
             req_site.clear(); req_pat.clear(); req_slot.clear(); req_a.clear(); eig_slot.clear(); eig_om.clear();
+            eig_prev.clear();
             count.clear();
             for (int i = 0; i < N; ++i) {
                 if (!sites[i].pending) continue;
@@ -300,6 +301,8 @@ extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, con
                         eig_slot.push_back(slot);
                         s.slot = slot;
                     } else {
+                        eig_prev.resize(eig_slot.size(), -1);
+                        eig_prev.push_back(s.slot);        // warm start from the pattern's last eigensystem
                         s.slot = kSharedSlots + i;
                         eig_om.push_back(om);
                         eig_slot.push_back(s.slot);
@@ -310,7 +313,8 @@ extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, con
                 req_slot.push_back(s.slot);
             }
             lnl.assign(req_site.size(), 0.0);
-            if (!fel_device_eval(dev, int(eig_om.size()), eig_om.data(), eig_slot.data(), int(req_site.size()), req_pat.data(),
+            eig_prev.resize(eig_slot.size(), -1);          // new shared slots start from the identity
+            if (!fel_device_eval(dev, int(eig_om.size()), eig_om.data(), eig_slot.data(), eig_prev.data(), int(req_site.size()), req_pat.data(),
                                  req_a.data(), req_slot.data(), lnl.data(), &err)) {
                 fel_set_error(prob, "h3g_fel_run: " + err);
                 st = H3G_ERR_CUDA;
