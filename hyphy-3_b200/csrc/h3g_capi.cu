@@ -53,6 +53,9 @@ struct h3g_problem {
     int *d_ch_off = nullptr, *d_ch = nullptr, *d_iidx = nullptr, *d_taxon = nullptr, *d_in_nodes = nullptr, *d_out_nodes = nullptr;
     int* d_parent = nullptr;
     uint8_t* d_leaf = nullptr;
+    int2* d_kdesc = nullptr;
+    int4* d_in_info = nullptr;
+    int4* d_out_info = nullptr;
     int8_t* d_states = nullptr;
     uint64_t* d_masks = nullptr;
     double* d_w = nullptr;
@@ -98,6 +101,7 @@ struct h3g_problem {
         t.n = n; t.root = root; t.NI = NI; t.T = T; t.P = P; t.Pp = Pp; t.S = S;
         t.ch_off = d_ch_off; t.ch = d_ch; t.parent = d_parent; t.iidx = d_iidx; t.leaf = d_leaf; t.taxon = d_taxon;
         t.states = d_states; t.masks = d_masks; t.w = d_w;
+        t.kdesc = d_kdesc; t.in_info = d_in_info; t.out_info = d_out_info;
         t.all_mask = S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1);
         return t;
     }
@@ -255,6 +259,29 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_leaf, n));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_in_nodes, std::max<size_t>(pr->in_nodes.size(), 1)));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_out_nodes, std::max<size_t>(pr->out_nodes.size(), 1)));
+        // descriptors for the persistent passes
+        std::vector<int2> kdesc(std::max<size_t>(pr->ch.size(), 1));
+        for (size_t j = 0; j < pr->ch.size(); ++j) {
+            const int c = pr->ch[j];
+            kdesc[j] = make_int2(c, is_leaf[c] ? pr->taxon[c] : -(2 + pr->iidx[c]));
+        }
+        std::vector<int4> in_info(std::max<size_t>(pr->in_nodes.size(), 1));
+        for (size_t k = 0; k < pr->in_nodes.size(); ++k) {
+            const int u = pr->in_nodes[k];
+            in_info[k] = make_int4(u, pr->iidx[u], pr->ch_off[u], pr->ch_off[u + 1]);
+        }
+        std::vector<int4> out_info(2 * std::max<size_t>(pr->out_nodes.size(), 1));
+        for (size_t k = 0; k < pr->out_nodes.size(); ++k) {
+            const int c = pr->out_nodes[k], u = parent[c];
+            out_info[2 * k] = make_int4(c, u, pr->iidx[u], is_leaf[c] ? -1 : pr->iidx[c]);
+            out_info[2 * k + 1] = make_int4(pr->ch_off[u], pr->ch_off[u + 1], 0, 0);
+        }
+        H3G_TRY_CUDA(ctx, A.alloc(&pr->d_kdesc, kdesc.size()));
+        H3G_TRY_CUDA(ctx, A.alloc(&pr->d_in_info, in_info.size()));
+        H3G_TRY_CUDA(ctx, A.alloc(&pr->d_out_info, out_info.size()));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_kdesc, kdesc.data(), kdesc.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_in_info, in_info.data(), in_info.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_out_info, out_info.data(), out_info.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_states, st.size()));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_masks, mk.size()));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_w, wt.size()));
@@ -559,21 +586,28 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
     mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
     if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, pr->mw, s));
     int l = 0;
-    for (size_t lv = 0; lv + 1 < pr->in_off.size(); ++lv) {
-        const int cnt = pr->in_off[lv + 1] - pr->in_off[lv];
-        if (!cnt) continue;
-        const int* nodes = pr->d_in_nodes + pr->in_off[lv];
-        l += mixed ? launch_inside_mixed(t, md, w, pr->mw, nodes, cnt, s) : launch_inside_fp64(t, md, w, nodes, cnt, s);
+    if (mixed) {
+        // one persistent launch over every level, per-tile dependencies
+        l = launch_inside_mixed(t, md, w, pr->mw, pr->d_in_nodes, int(pr->in_nodes.size()), s);
+    } else {
+        for (size_t lv = 0; lv + 1 < pr->in_off.size(); ++lv) {
+            const int cnt = pr->in_off[lv + 1] - pr->in_off[lv];
+            if (!cnt) continue;
+            l += launch_inside_fp64(t, md, w, pr->d_in_nodes + pr->in_off[lv], cnt, s);
+        }
     }
     mark(ST_INSIDE, l);
     mark(ST_ROOT, mixed ? launch_root_mixed(t, md, w, pr->mw, s) : launch_root(t, md, w, s));
     if (grads) {
         l = 0;
-        for (size_t lv = 0; lv + 1 < pr->out_off.size(); ++lv) {
-            const int cnt = pr->out_off[lv + 1] - pr->out_off[lv];
-            if (!cnt) continue;
-            const int* nodes = pr->d_out_nodes + pr->out_off[lv];
-            l += mixed ? launch_outside_mixed(t, md, w, pr->mw, nodes, cnt, s) : launch_outside_fp64(t, md, w, nodes, cnt, 1, s);
+        if (mixed) {
+            l = launch_outside_mixed(t, md, w, pr->mw, pr->d_out_nodes, int(pr->out_nodes.size()), s);
+        } else {
+            for (size_t lv = 0; lv + 1 < pr->out_off.size(); ++lv) {
+                const int cnt = pr->out_off[lv + 1] - pr->out_off[lv];
+                if (!cnt) continue;
+                l += launch_outside_fp64(t, md, w, pr->d_out_nodes + pr->out_off[lv], cnt, 1, s);
+            }
         }
         mark(ST_OUTSIDE, l);
         mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, pr->mw, s) : launch_accumA_fp64(t, md, w, s));

@@ -65,6 +65,10 @@ struct Topo {
     const uint64_t* masks;   // [T][Pp]
     const double* w;         // [Pp] pattern weights, 0 on padding
     uint64_t all_mask;
+    // per-item descriptors of the persistent passes, one load each instead of a chain of lookups
+    const int2* kdesc;       // [children CSR] {child, code}: code = taxon (>= 0) or -1 for a leaf, -(2 + iidx) for an internal child
+    const int4* in_info;     // [internal nodes, inside order] {u, iidx[u], first child slot, end}
+    const int4* out_info;    // [2 x children, outside order] {c, u, iidx[u], iidx[c] or -1}, {first sibling slot, end, 0, 0}
 };
 
 struct Model {

@@ -129,10 +129,11 @@ struct MsgSrc {
     uint64_t mk;        // != 0: masked sum of PT32 rows starting at src
     int E;              // exponent of a stored message
 };
-__device__ __forceinline__ MsgSrc msg_src(const Topo& t, const MixedWork& mw, int m, int M, int c, int p, int g, size_t so) {
+__device__ __forceinline__ MsgSrc msg_src(const Topo& t, const MixedWork& mw, int m, int M, int2 d, int p, int g, size_t so) {
     MsgSrc r{nullptr, 1, 0, 0};
-    if (t.leaf[c]) {
-        const int tx = t.taxon[c];
+    const int c = d.x;
+    if (d.y >= -1) {
+        const int tx = d.y;
         const float* PTc = mw.PT32 + mat_off_f(m, c, t.n);
         const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
         if (st >= 0) {
@@ -147,17 +148,17 @@ __device__ __forceinline__ MsgSrc msg_src(const Topo& t, const MixedWork& mw, in
             }
         }
     } else {
-        const int ic = t.iidx[c];
+        const int ic = -(d.y + 2);
         r.src = mw.Ms + part_off(ic, m, M, t.Pp) + so;
         r.stride = size_t(t.Pp);
-        r.E = mw.EM[col_off(ic, m, M, t.Pp) + p];
+        r.E = __ldcg(mw.EM + col_off(ic, m, M, t.Pp) + p);
     }
     return r;
 }
 __device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
-    if (r.stride != 1) {
+    if (r.stride != 1) {                // a message written by another CTA of this launch: read through L2
 #pragma unroll
-        for (int i = 0; i < kSG; ++i) a[i] = r.src[i * r.stride];
+        for (int i = 0; i < kSG; ++i) a[i] = __ldcg(r.src + i * r.stride);
     } else if (r.mk == 0) {
         const float4* s4 = reinterpret_cast<const float4*>(r.src);
 #pragma unroll
@@ -181,7 +182,7 @@ __device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
 
 __device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
-    for (int i = 0; i < kSG; ++i) v[i] = src[i * stride];
+    for (int i = 0; i < kSG; ++i) v[i] = __ldcg(src + i * stride);
 }
 __device__ __forceinline__ void mul_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
@@ -211,8 +212,8 @@ __device__ __forceinline__ TcTile carve(unsigned char* sm) {
     return s;
 }
 
-// Barriers, TMEM and the B tile terms for one contraction.  All threads call.
-__device__ __forceinline__ void tc_begin(const TcTile& s, uint16_t* const (&b)[3], size_t off) {
+// Once per persistent CTA: barriers and TMEM.  All threads call.
+__device__ __forceinline__ void tc_setup(const TcTile& s) {
     const int tid = threadIdx.x;
     if (tid == 0) {
         tc::mbar_init(&s.bars[0], 1);
@@ -223,7 +224,17 @@ __device__ __forceinline__ void tc_begin(const TcTile& s, uint16_t* const (&b)[3
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
-    if (tid == 0) {
+}
+__device__ __forceinline__ void tc_teardown(const TcTile& s) {
+    tc::tc_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) tc::tmem_dealloc(*s.slot, kTmemCols);
+}
+// Per item: bring the branch's B tile terms in with the bulk-copy engine (thread 0).
+// The previous item's MMAs, the last readers of the B tiles, completed in its tc_run.
+__device__ __forceinline__ void tc_load_b(const TcTile& s, uint16_t* const (&b)[3], size_t off) {
+    if (threadIdx.x == 0) {
+        tc::fence_async_smem();
         tc::mbar_expect_tx(&s.bars[0], uint32_t(3 * kBBytes));
         for (int q = 0; q < 3; ++q) tc::bulk_g2s(s.B[q], b[q] + off, uint32_t(kBBytes), &s.bars[0]);
     }
@@ -245,7 +256,7 @@ __device__ __forceinline__ void tc_write_part(const TcTile& s, const float (&v)[
 
 // out = A * B^T for this thread's row and state group: issue (one thread),
 // wait (all), read the four per-K-step accumulators from TMEM and sum in FP64.
-__device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const Lane& l, int* err) {
+__device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const Lane& l, int* err, uint32_t phase) {
     const int tid = threadIdx.x;
     tc::fence_async_smem();
     tc::tc_fence_before();
@@ -253,7 +264,7 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
     tc::tc_fence_after();
     const uint32_t tmem = *s.slot;
     if (tid == 0) {
-        const bool got_b = tc::mbar_wait(&s.bars[0], 0);
+        const bool got_b = tc::mbar_wait(&s.bars[0], phase);
         if (got_b) {
             const uint32_t lboA = (MT / 8) * 128, lboB = (SP / 8) * 128;
             // Each K step accumulates into its own TMEM columns: the five small split
@@ -274,7 +285,7 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
         }
         tc::mma_commit(&s.bars[1]);
     }
-    if (!tc::mbar_wait(&s.bars[1], 0) && (tid & 31) == 0) atomicOr(err, 2);
+    if (!tc::mbar_wait(&s.bars[1], phase) && (tid & 31) == 0) atomicOr(err, 2);
     tc::tc_fence_after();
     const uint32_t row = tmem + (uint32_t(32 * l.q) << 16) + uint32_t(kSG * l.g);
     float t16[kKSteps][16];
@@ -290,7 +301,7 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (l.warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
+    tc::tc_fence_after();
 }
 
 // ------------------------------------------------------------ P preparation
@@ -298,6 +309,11 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
 __global__ void __launch_bounds__(256) k_prep_mx(Topo t, Model md, Work w, MixedWork mw) {
     pdl_enter();
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
+    if (b == 0 && m == 0 && tid == 0) {        // a new evaluation: new epoch, fresh item counters
+        mw.sync[0] += 1;
+        mw.sync[1] = 0;
+        mw.sync[2] = 0;
+    }
     if (b == t.root) return;
     const double* P = w.P + mat_off(m, b, t.n);
     const size_t o = mat_off_f(m, b, t.n);
@@ -318,58 +334,123 @@ __global__ void __launch_bounds__(256) k_prep_mx(Topo t, Model md, Work w, Mixed
     if (tid < SP) mw.rs32[(size_t(m) * t.n + b) * SP + tid] = float(w.rs[(size_t(m) * t.n + b) * SP + tid]);
 }
 
+// --------------------------------------------------- persistent pass machinery
+// The inside and outside passes are each ONE launch of persistent CTAs (two per
+// SM).  A work item is (node, rate class, 128-pattern tile); items are claimed
+// from a counter in tree order (children before parents for the inside pass,
+// parents before children for the outside pass), so an item only ever waits for
+// items that running CTAs have already claimed.  An item waits for the items
+// it reads with a per-(node, class, tile) flag that holds the evaluation's
+// epoch once the item's partials are in memory.  This replaces one launch and
+// one grid-wide wait per tree level with per-tile dependencies.
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// next item for this CTA (all threads call)
+__device__ __forceinline__ int claim(int* ctr, int* s_item) {
+    __syncthreads();
+    if (threadIdx.x == 0) *s_item = atomicAdd(ctr, 1);
+    __syncthreads();
+    return *s_item;
+}
+// thread 0: bounded wait until an item's flag holds this evaluation's epoch
+__device__ __forceinline__ void wait_item(const int* flag, int epoch, int* err) {
+    for (uint32_t it = 0; ld_acquire(flag) != epoch; ++it) {
+        if (it > (1u << 22)) { atomicOr(err, 32); return; }
+        __nanosleep(64);
+    }
+}
+// all threads: the item's partials are stored; make them visible, raise its flag, and
+// claim the CTA's next item in the same step (the item being published waits for nothing
+// more, so holding the next claim meanwhile cannot block anyone)
+__device__ __forceinline__ int publish_and_claim(int* flag, int epoch, int* ctr, int* s_item) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int next = atomicAdd(ctr, 1);
+        __threadfence();
+        st_release(flag, epoch);
+        *s_item = next;
+    }
+    __syncthreads();
+    return *s_item;
+}
+
 // ------------------------------------------------------------------ inside
-// grid (Pp/128, nodes in level, M), block 512.
-__global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ nodes) {
+// Persistent: grid min(items, 2 x SMs), block 512; items (node k, m, tile) in the
+// order of t.in_info (internal nodes by increasing height, the root last).
+__global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
+    __shared__ int s_item;
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
-    const int u = nodes[blockIdx.y], m = blockIdx.z;
-    const int p = blockIdx.x * MT + l.r;
-    const int iu = t.iidx[u], M = md.M;
+    const int M = md.M, ntile = t.Pp / MT;
     const size_t Pp = size_t(t.Pp);
-    const size_t so = size_t(kSG * l.g) * Pp + p;     // this thread's first state of the pattern column
-    const bool root = u == t.root;
-    if (!root) tc_begin(s, mw.Bp, mat_off_f(m, u, t.n));
-    // the first two children's messages load together (padding states are zero in every
-    // message), then one product and one renormalisation; further children one at a time
-    float v[kSG];
-    int E = 0;
-    const int k0 = t.ch_off[u], k1 = t.ch_off[u + 1];
-    {
-        const MsgSrc s0 = msg_src(t, mw, m, M, t.ch[k0], p, l.g, so);
-        E = s0.E;
-        if (k0 + 1 < k1) {
-            const MsgSrc s1 = msg_src(t, mw, m, M, t.ch[k0 + 1], p, l.g, so);
-            float b[kSG];
-            msg_load(s0, v);
-            msg_load(s1, b);
+    const int epoch = __ldcg(mw.sync);
+    tc_setup(s);
+    uint32_t phase = 0;
+    int item = claim(mw.sync + 1, &s_item);
+    while (item < n_items) {
+        const int tile = item % ntile, rest = item / ntile, m = rest % M;
+        const int4 info = t.in_info[rest / M];
+        const int u = info.x, iu = info.y, k0 = info.z, k1 = info.w;
+        const int p = tile * MT + l.r;
+        const size_t so = size_t(kSG * l.g) * Pp + p;     // this thread's first state of the pattern column
+        const bool root = u == t.root;
+        if (!root) tc_load_b(s, mw.Bp, mat_off_f(m, u, t.n));
+        if (threadIdx.x == 0)
+            for (int k = k0; k < k1; ++k) {
+                const int code = t.kdesc[k].y;
+                if (code <= -2) wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err);
+            }
+        __syncthreads();
+        // the first two children's messages load together (padding states are zero in every
+        // message), then one product and one renormalisation; further children one at a time
+        float v[kSG];
+        int E = 0;
+        {
+            const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k0], p, l.g, so);
+            E = s0.E;
+            if (k0 + 1 < k1) {
+                const MsgSrc s1 = msg_src(t, mw, m, M, t.kdesc[k0 + 1], p, l.g, so);
+                float b[kSG];
+                msg_load(s0, v);
+                msg_load(s1, b);
 #pragma unroll
-            for (int i = 0; i < kSG; ++i) v[i] *= b[i];
-            E += s1.E;
-        } else {
-            msg_load(s0, v);
+                for (int i = 0; i < kSG; ++i) v[i] *= b[i];
+                E += s1.E;
+            } else {
+                msg_load(s0, v);
+            }
+            E += renorm_row(v, s.smax, l);
         }
-        E += renorm_row(v, s.smax, l);
-    }
-    for (int k = k0 + 2; k < k1; ++k) {
-        const MsgSrc sr = msg_src(t, mw, m, M, t.ch[k], p, l.g, so);
-        float a[kSG];
-        msg_load(sr, a);
+        for (int k = k0 + 2; k < k1; ++k) {
+            const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
+            float a[kSG];
+            msg_load(sr, a);
 #pragma unroll
-        for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-        E += sr.E + renorm_row(v, s.smax, l);
+            for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+            E += sr.E + renorm_row(v, s.smax, l);
+        }
+        store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
+        if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
+        if (!root) {
+            tc_write_part(s, v, l);
+            float o[kSG];
+            tc_run(s, o, l, w.err, phase);
+            phase ^= 1u;
+            const int sh = renorm_row(o, s.smax, l);
+            store_part(o, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
+            if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E + sh;
+        }
+        item = publish_and_claim(mw.flag_in + (size_t(iu) * M + m) * ntile + tile, epoch, mw.sync + 1, &s_item);
     }
-    store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
-    if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
-    if (root) return;
-    tc_write_part(s, v, l);
-    float o[kSG];
-    tc_run(s, o, l, w.err);
-    const int sh = renorm_row(o, s.smax, l);
-    store_part(o, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
-    if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E + sh;
+    tc_teardown(s);
 }
 
 // --------------------------------------------------------------------- root
@@ -415,66 +496,83 @@ __global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
 }
 
 // ------------------------------------------------------------------ outside
-// grid (Pp/128, children in level, M), block 512.
-__global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, const int* __restrict__ kids) {
+// Persistent like the inside pass; items (child k, m, tile) in the order of t.out_info
+// (children of the root first, then by increasing depth of the parent).
+__global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
+    __shared__ int s_item;
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
-    const int c = kids[blockIdx.y], m = blockIdx.z;
-    const int p = blockIdx.x * MT + l.r;
-    const int u = t.parent[c], iu = t.iidx[u], M = md.M;
+    const int M = md.M, ntile = t.Pp / MT;
     const size_t Pp = size_t(t.Pp);
-    const size_t so = size_t(kSG * l.g) * Pp + p;
-    const bool internal = !t.leaf[c];
-    if (internal) tc_begin(s, mw.Bpt, mat_off_f(m, c, t.n));
-    // the parent's outside vector (pi at the root) and the first sibling's message load together
-    float v[kSG];
-    int EV = 0;
-    const int k0 = t.ch_off[u], k1 = t.ch_off[u + 1];
-    int k = k0;
-    while (k < k1 && t.ch[k] == c) ++k;
-    {
-        float a[kSG];
-        const MsgSrc s0 = msg_src(t, mw, m, M, t.ch[k], p, l.g, so);
-        if (u == t.root) {
-#pragma unroll
-            for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
-        } else {
-            load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
-            EV = mw.EU[col_off(iu, m, M, t.Pp) + p];
-        }
-        msg_load(s0, a);
-#pragma unroll
-        for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-        EV += s0.E + renorm_row(v, s.smax, l);
-        ++k;
-    }
-    for (; k < k1; ++k) {
-        const int sb = t.ch[k];
-        if (sb == c) continue;
-        const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
-        float a[kSG];
-        msg_load(sr, a);
-#pragma unroll
-        for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-        EV += sr.E + renorm_row(v, s.smax, l);
-    }
-    // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
+    const int epoch = __ldcg(mw.sync);
     const int ir = t.iidx[t.root];
-    const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
-    const int EDc = internal ? mw.ED[col_off(t.iidx[c], m, M, t.Pp) + p] : 0;
-    const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
-    float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
+    tc_setup(s);
+    uint32_t phase = 0;
+    int item = claim(mw.sync + 2, &s_item);
+    while (item < n_items) {
+        const int tile = item % ntile, rest = item / ntile, m = rest % M;
+        const int4 oi = t.out_info[2 * (rest / M)], oj = t.out_info[2 * (rest / M) + 1];
+        const int c = oi.x, u = oi.y, iu = oi.z, ic = oi.w, k0 = oj.x, k1 = oj.y;
+        const int p = tile * MT + l.r;
+        const size_t so = size_t(kSG * l.g) * Pp + p;
+        const bool internal = ic >= 0;
+        if (internal) tc_load_b(s, mw.Bpt, mat_off_f(m, c, t.n));
+        if (threadIdx.x == 0 && u != t.root) wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err);
+        __syncthreads();
+        // the parent's outside vector (pi at the root) and the first sibling's message load together
+        float v[kSG];
+        int EV = 0;
+        int k = k0;
+        while (k < k1 && t.kdesc[k].x == c) ++k;
+        {
+            float a[kSG];
+            const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
+            if (u == t.root) {
 #pragma unroll
-    for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
-    if (!internal) return;
-    tc_write_part(s, v, l);
-    float o[kSG];
-    tc_run(s, o, l, w.err);
-    const int sh = renorm_row(o, s.smax, l);
-    store_part(o, mw.U + part_off(t.iidx[c], m, M, t.Pp) + so, Pp);
-    if (l.g == 0) mw.EU[col_off(t.iidx[c], m, M, t.Pp) + p] = EV + sh;
+                for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
+            } else {
+                load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
+                EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
+            }
+            msg_load(s0, a);
+#pragma unroll
+            for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+            EV += s0.E + renorm_row(v, s.smax, l);
+            ++k;
+        }
+        for (; k < k1; ++k) {
+            const int2 sb = t.kdesc[k];
+            if (sb.x == c) continue;
+            const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
+            float a[kSG];
+            msg_load(sr, a);
+#pragma unroll
+            for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+            EV += sr.E + renorm_row(v, s.smax, l);
+        }
+        // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
+        const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
+        const int EDc = internal ? mw.ED[col_off(ic, m, M, t.Pp) + p] : 0;
+        const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
+        float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
+#pragma unroll
+        for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
+        if (!internal) {
+            item = claim(mw.sync + 2, &s_item);
+            continue;
+        }
+        tc_write_part(s, v, l);
+        float o[kSG];
+        tc_run(s, o, l, w.err, phase);
+        phase ^= 1u;
+        const int sh = renorm_row(o, s.smax, l);
+        store_part(o, mw.U + part_off(ic, m, M, t.Pp) + so, Pp);
+        if (l.g == 0) mw.EU[col_off(ic, m, M, t.Pp) + p] = EV + sh;
+        item = publish_and_claim(mw.flag_out + (size_t(ic) * M + m) * ntile + tile, epoch, mw.sync + 2, &s_item);
+    }
+    tc_teardown(s);
 }
 
 // ------------------------------------------------------------------ accum A
@@ -740,6 +838,10 @@ h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, 
               take(&mw.ED, cols) && take(&mw.EM, cols) && take(&mw.EU, cols) && take(&mw.PT32, mats) &&
               take(&mw.rs32, size_t(M) * n * SP);
     for (int q = 0; q < 3 && ok; ++q) ok = take(&mw.Bp[q], mats) && take(&mw.Bpt[q], mats);
+    const size_t flags = size_t(NI) * M * (Pp / MT);
+    ok = ok && take(&mw.flag_in, flags) && take(&mw.flag_out, flags) && take(&mw.sync, 4);
+    ok = ok && cudaMemset(mw.flag_in, 0, flags * sizeof(int)) == cudaSuccess &&
+         cudaMemset(mw.flag_out, 0, flags * sizeof(int)) == cudaSuccess && cudaMemset(mw.sync, 0, 4 * sizeof(int)) == cudaSuccess;
     return ok ? H3G_OK : H3G_ERR_OOM;
 }
 
@@ -747,8 +849,19 @@ int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork
     launch_k(k_prep_mx, dim3(t.n, md.M), 256, 0, s, t, md, w, mw);
     return 1;
 }
+static int persistent_ctas(int items) {
+    static int sms = [] {
+        int dev = 0, v = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v;
+    }();
+    return std::max(1, std::min(items, 2 * sms));
+}
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s) {
-    launch_k(k_inside_mx, dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s, t, md, w, mw, d_nodes);
+    const int items = count * md.M * (t.Pp / MT);
+    (void)d_nodes;     // the item order is t.in_info's
+    launch_k(k_inside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items);
     return 1;
 }
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
@@ -756,7 +869,9 @@ int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const Mixed
     return 1;
 }
 int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s) {
-    launch_k(k_outside_mx, dim3(t.Pp / MT, count, md.M), kThreads, kMxSmem, s, t, md, w, mw, d_kids);
+    const int items = count * md.M * (t.Pp / MT);
+    (void)d_kids;      // the item order is t.out_info's
+    launch_k(k_outside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items);
     return 1;
 }
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {

@@ -28,6 +28,9 @@ struct MixedWork {
     uint16_t* Bpt[3] = {nullptr, nullptr, nullptr};  // same for P^T
     float* PT32 = nullptr;   // [M][n][64*64]    FP32 P^T row-major (leaf messages)
     float* rs32 = nullptr;   // [M][n][64]       FP32 row sums of P
+    int* flag_in = nullptr;  // [NI][M][Pp/128]  epoch of the evaluation whose inside item is stored
+    int* flag_out = nullptr; // [NI][M][Pp/128]  same for the outside item (U of an internal node)
+    int* sync = nullptr;     // [4]              epoch, inside and outside item counters
 };
 
 bool mixed_available();
