@@ -72,6 +72,8 @@ struct h3g_problem {
     size_t h_pin_count = 0;
     double* d_bl = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t s2 = nullptr;                       // side stream: model-only work beside the pruning passes
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     float last_ms = 0.f;
     int last_launches = 0;
     size_t last_h2d = 0, last_d2h = 0;
@@ -95,6 +97,9 @@ struct h3g_problem {
         if (h_pin) cudaFreeHost(h_pin);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (s2) cudaStreamDestroy(s2);
     }
     Topo topo() const {
         Topo t;
@@ -301,6 +306,9 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
         H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
         H3G_TRY_CUDA(ctx, cudaEventCreate(&pr->ev0));
         H3G_TRY_CUDA(ctx, cudaEventCreate(&pr->ev1));
+        H3G_TRY_CUDA(ctx, cudaStreamCreateWithFlags(&pr->s2, cudaStreamNonBlocking));
+        H3G_TRY_CUDA(ctx, cudaEventCreateWithFlags(&pr->ev_fork, cudaEventDisableTiming));
+        H3G_TRY_CUDA(ctx, cudaEventCreateWithFlags(&pr->ev_join, cudaEventDisableTiming));
         *out = guard.release();
         ctx->live_problems++;
         return H3G_OK;
@@ -403,7 +411,8 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * G));
     H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * G));
     H3G_TRY_CUDA(ctx, A.alloc(&w.H, size_t(nmod) * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 4));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 17));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.G, size_t(std::max(ndirs, 1)) * nmod * SP2));
     const size_t n_out = 2 + n + K + nmod + M;
     H3G_TRY_CUDA(ctx, A.alloc(&w.out, n_out));
     H3G_TRY_CUDA(ctx, A.alloc(&w.err, 1));
@@ -421,7 +430,7 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * G * sizeof(double), ctx->stream);
     pr->off_out = n;
     pr->off_dir = pr->off_out + n_out;
-    pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod * 4;
+    pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod * 17;
     pr->h_pin_count = pr->off_site + size_t(std::max(pr->P, 1));
     H3G_TRY_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&pr->h_pin), pr->h_pin_count * sizeof(double)));
     return H3G_OK;
@@ -583,6 +592,14 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
         if (mk && launched) { cudaEventRecord(mk->ev[st + 1], s); mk->seen[st] = true; mk->launches[st] += launched; }
     };
     if (mk) cudaEventRecord(mk->ev[0], s);
+    // model-only directional products on the side stream, joined before their contraction
+    const bool side = global && md.ndirs > 0;
+    if (side) {
+        cudaEventRecord(pr->ev_fork, s);
+        cudaStreamWaitEvent(pr->s2, pr->ev_fork, 0);
+        L += launch_dir(t, md, w, pr->s2);
+        cudaEventRecord(pr->ev_join, pr->s2);
+    }
     mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
     if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, pr->mw, s));
     int l = 0;
@@ -612,10 +629,11 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
         mark(ST_OUTSIDE, l);
         mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, pr->mw, s) : launch_accumA_fp64(t, md, w, s));
         mark(ST_FRECHET, launch_frechet(t, md, w, global ? 1 : 0, s));
+        if (side) cudaStreamWaitEvent(s, pr->ev_join, 0);
         if (global) mark(ST_HSUM, launch_global(t, md, w, s));
     }
+    if (side && !grads) cudaStreamWaitEvent(s, pr->ev_join, 0);
     mark(ST_SMALL, launch_small(t, md, w, grads ? 1 : 0, s));
-    if (global) mark(ST_DIR, launch_dir(t, md, w, s));
     return L;
 }
 
@@ -631,7 +649,7 @@ static size_t enqueue_readback(h3g_problem* pr, unsigned want) {
     size_t bytes = n_out_of(pr) * sizeof(double);
     cudaMemcpyAsync(pr->h_pin + pr->off_out, pr->w.out, bytes, cudaMemcpyDeviceToHost, s);
     if ((want & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) {
-        const size_t b = size_t(pr->ndirs) * pr->nmod * 4 * sizeof(double);
+        const size_t b = size_t(pr->ndirs) * pr->nmod * 17 * sizeof(double);
         cudaMemcpyAsync(pr->h_pin + pr->off_dir, pr->w.dirpart, b, cudaMemcpyDeviceToHost, s);
         bytes += b;
     }
@@ -683,7 +701,7 @@ static h3g_status run_eval(h3g_problem* pr, unsigned want, bool copies) {
     pr->last_d2h = 0;
     if (copies) {
         pr->last_d2h = n_out_of(pr) * sizeof(double);
-        if ((key & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) pr->last_d2h += size_t(pr->ndirs) * pr->nmod * 4 * sizeof(double);
+        if ((key & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) pr->last_d2h += size_t(pr->ndirs) * pr->nmod * 17 * sizeof(double);
         if ((key & H3G_WANT_SITE_LNL) && pr->P > 0) pr->last_d2h += size_t(pr->P) * sizeof(double);
     }
     return H3G_OK;
@@ -702,12 +720,19 @@ static void unpack_result(h3g_problem* pr, unsigned want, h3g_result* out) {
     if (out->grad_class_w) for (int k = 0; k < pr->K; ++k) out->grad_class_w[k] = global ? hout[2 + n + k] : 0.0;
     if (out->grad_rate_w) for (int m = 0; m < pr->M; ++m) out->grad_rate_w[m] = grads ? hout[2 + n + pr->K + pr->nmod + m] : 0.0;
     if (out->grad_dir) {
+        // sum_k sum (V dQ U) o H_k, minus (normalised time) sum_k dmu_k / mu_k * sum_b tau_b dL/dtau_b
         const double* dir = pr->h_pin + pr->off_dir;
         for (int x = 0; x < pr->ndirs; ++x) {
             double g = 0.0;
             if (global)
-                for (int k = 0; k < pr->nmod; ++k)
-                    for (int rb = 0; rb < 4; ++rb) g += dir[(size_t(x) * pr->nmod + k) * 4 + rb];
+                for (int k = 0; k < pr->nmod; ++k) {
+                    const double* d = dir + (size_t(x) * pr->nmod + k) * 17;
+                    double v = 0.0;
+                    for (int b = 0; b < 16; ++b) v += d[b];
+                    if (pr->time_mode == H3G_TIME_NORMALIZED)
+                        v -= d[16] / std::max(pr->h_mu[size_t(k)], 1e-12) * hout[2 + n + pr->K + k];
+                    g += v;
+                }
             out->grad_dir[x] = g;
         }
     }

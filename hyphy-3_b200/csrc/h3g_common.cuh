@@ -113,7 +113,8 @@ struct Work {
     double* gc;              // [K][M][G] <A_{m,b}, P_k(tau)> summed over a branch group
     double* stg;             // [nmod][M][G] c_k * tau * <A_{m,b}, Q_k P_k(tau)> summed over a branch group
     double* H;               // [nmod][64*64]
-    double* dirpart;         // [ndirs][nmod][4] row-block partials
+    double* dirpart;         // [ndirs][nmod][17]: 16 partials of sum (V dQ U) o H, then d mu = -sum pi_i dQ_ii
+    double* G;               // [ndirs][nmod][64*64] V_k dQ_x U_k (depends on the model only)
     double* out;             // [2 + n + K + nmod + M] lnl | error flag | grad_t | gc | stg | grad_rate_w
     int* err;                // sticky device error flags (bounded waits that expired)
 };

@@ -648,19 +648,36 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
     }
 }
 
-// H_k[e] = sum over (m, g) of the per-CTA partials, fixed order.  grid (nmod, 16), block 256.
-__global__ void k_hsum(Topo t, Model md, Work w, int G) {
+// H_k[e] = sum over (m, g) of the per-CTA partials (fixed order: four interleaved
+// running sums, combined pairwise), then the directional contractions
+// dirpart[x][k][block] = sum over this block's 256 entries of H_k o G_{x,k}.
+// grid (nmod, 16), block 256.
+__global__ void __launch_bounds__(256) k_hsum(Topo t, Model md, Work w, int G) {
     pdl_enter();
-    const int k = blockIdx.x, e = blockIdx.y * 256 + threadIdx.x, M = md.M;
-    double s = 0.0;
-    for (int m = 0; m < M; ++m)
-        for (int g = 0; g < G; ++g) s += w.Hpart[((size_t(k) * M + m) * G + g) * SP2 + e];
-    w.H[size_t(k) * SP2 + e] = s;
+    __shared__ double red[8];
+    const int k = blockIdx.x, e = blockIdx.y * 256 + threadIdx.x, M = md.M, nt = M * G;
+    const double* hp = w.Hpart + size_t(k) * nt * SP2 + e;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int i = 0;
+    for (; i + 4 <= nt; i += 4) {
+        s0 += hp[size_t(i) * SP2];
+        s1 += hp[size_t(i + 1) * SP2];
+        s2 += hp[size_t(i + 2) * SP2];
+        s3 += hp[size_t(i + 3) * SP2];
+    }
+    for (; i < nt; ++i) s0 += hp[size_t(i) * SP2];
+    const double h = (s0 + s1) + (s2 + s3);
+    w.H[size_t(k) * SP2 + e] = h;
+    for (int x = 0; x < md.ndirs; ++x) {
+        const double v = block_sum_256(h * w.G[(size_t(x) * md.nmod + k) * SP2 + e], red);
+        if (threadIdx.x == 0) w.dirpart[(size_t(x) * md.nmod + k) * 17 + blockIdx.y] = v;
+    }
 }
 
-// per (direction x, model k, row block rb): sum over rows [16rb, 16rb+16) of
-// (V_k dQ U_k) o H_k, minus (block 0, normalized time) dmu/mu * stg_k.
-// grid (ndirs, nmod, 4), block 256, dynamic smem (64*64 + 16*64 + 64*64) doubles.
+// G_{x,k} = V_k dQ_{x,k} U_k, rows [16rb, 16rb+16); block 0 also stores
+// d mu = -sum_i pi_i dQ_ii.  Depends on the model only, so it runs on a side
+// stream alongside the pruning passes.  grid (ndirs, nmod, 4), block 256,
+// dynamic smem (64*64 + 16*64 + 16*64) doubles.
 __global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
@@ -694,18 +711,11 @@ __global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[q] = fma(a, sX[l * SP + c0 + q], acc[q]);
     }
-    const double* H = w.H + size_t(k) * SP2 + size_t(16 * rb) * SP;
-    double g = 0.0;
+    double* Gx = w.G + (size_t(x) * md.nmod + k) * SP2 + size_t(16 * rb + r) * SP + c0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) g = fma(acc[q], H[r * SP + c0 + q], g);
-    g = block_sum_256(g, red);
+    for (int q = 0; q < 4; ++q) Gx[q] = acc[q];
     dmu = block_sum_256(dmu, red);
-    if (tid == 0) {
-        double v = g;
-        // stg_k total sits in out[] after k_small: out[2 + n + K + k]
-        if (rb == 0 && md.time_mode == 1) v -= dmu / fmax(md.mu[k], 1e-12) * w.out[2 + t.n + md.K + k];
-        w.dirpart[(size_t(x) * md.nmod + k) * 4 + rb] = v;
-    }
+    if (rb == 0 && tid == 0) w.dirpart[(size_t(x) * md.nmod + k) * 17 + 16] = dmu;
 }
 
 // Fixed-order reductions of the small per-branch / per-pattern partials.
