@@ -6,6 +6,7 @@
 #include <pybind11/stl.h>
 
 #include "hyphy/analyses/fel_gpu.hpp"
+#include "hyphy/opt/optimizer_gpu.hpp"
 #include "hyphy/core/likelihood_gpu.hpp"
 
 namespace py = pybind11;
@@ -227,6 +228,28 @@ PYBIND11_MODULE(_hyphy3, m) {
     }, "precision"_a);
     m.def("get_precision", []() { return LikelihoodEngine::get_precision() == H3G_PREC_MIXED ? "mixed" : "fp64"; });
     m.def("library_version", []() { return std::string(h3g_version()); });
+
+    // MG94 global fits (optimizer.hpp:741-1135)
+    using hyphy::opt::FitResult;
+    using hyphy::opt::MG94Fitter;
+    py::class_<FitResult>(m, "FitResult")
+        .def_readonly("log_likelihood", &FitResult::log_likelihood)
+        .def_readonly("x_opt", &FitResult::x_opt)
+        .def_readonly("param_names", &FitResult::param_names)
+        .def_readonly("iterations", &FitResult::iterations)
+        .def_readonly("converged", &FitResult::converged)
+        .def_readonly("tree", &FitResult::tree)
+        .def_readonly("params", &FitResult::params);
+    py::class_<MG94Fitter>(m, "MG94Fitter")
+        .def(py::init([](Tree t, Alignment a) { return MG94Fitter(std::move(t), std::move(a)); }), "tree"_a, "alignment"_a)
+        .def("fit_omega_and_scale", [](MG94Fitter& f, Scalar init_omega, const MG94Parameters& base) {
+                 py::gil_scoped_release rel;
+                 return f.fit_omega_and_scale(init_omega, base);
+             }, "init_omega"_a = 1.0, "base_params"_a = MG94Parameters{})
+        .def("fit_full_model", [](MG94Fitter& f, Scalar init_omega, const MG94Parameters& base, int max_iters, Scalar tolerance) {
+                 py::gil_scoped_release rel;
+                 return f.fit_full_model(init_omega, base, nullptr, max_iters, tolerance);
+             }, "init_omega"_a = 1.0, "base_params"_a = MG94Parameters{}, "max_iters"_a = 250, "tolerance"_a = 1e-5);
 
     // FEL (bindings.cpp:121-188 of the reference): settings, per-site results, analyzer
     using hyphy::analyses::FELAnalyzer;

@@ -18,6 +18,8 @@ from _hyphy3 import (  # noqa: E402
     FELAnalyzer,
     FELSettings,
     FELSiteResult,
+    FitResult,
+    MG94Fitter,
     GeneticCode,
     MG94Parameters,
     Tree,
@@ -38,7 +40,7 @@ from . import autograd  # noqa: E402
 
 __version__ = "3.0.0"
 __all__ = [
-    "Alignment", "FELAnalyzer", "FELSettings", "FELSiteResult", "GeneticCode", "MG94Parameters", "Tree", "TreeNode", "build_leaf_to_taxon_map",
+    "Alignment", "FELAnalyzer", "FELSettings", "FELSiteResult", "FitResult", "MG94Fitter", "GeneticCode", "MG94Parameters", "Tree", "TreeNode", "build_leaf_to_taxon_map",
     "compute_branch_length_gradients", "compute_joint_frechet_gradients", "compute_mg94_log_likelihood",
     "compute_mixture_gradients", "compute_tree_log_likelihood_from_P", "get_precision", "library_version",
     "mg94_eigensystem", "set_precision", "autograd",

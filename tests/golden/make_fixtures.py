@@ -60,6 +60,11 @@ def main(ref: str) -> None:
             "num_taxa": 23, "num_codons": 254, "num_nodes": 44,
         },
     }
+    # global MG94 fit of adh (full model: every branch, omega, GTR rates): python/tests/test_python_autograd.py:46-55
+    known["adh_global_fit"] = {
+        "source": "python/tests/test_python_autograd.py:46-55 (FELAnalyzer.create_and_fit global_log_l, delta 5)",
+        "full_model_logl": -4686.73, "delta": 5.0,
+    }
     # HyPhy 2.5 FEL per-site table for CD2 (columns alpha, beta, alpha=beta, LRT, p-value, total branch
     # length); only the MLE content of benchmarks/ground_truth/cd2_fel.json is kept
     fel = json.loads((ref_root / "benchmarks/ground_truth/cd2_fel.json").read_text())
