@@ -136,6 +136,33 @@ public:
             leaf[size_t(nd.id)] = nd.is_leaf ? 1 : 0;
             if (nd.is_leaf && l2t[size_t(nd.id)] != size_t(-1)) taxon[size_t(nd.id)] = int32_t(l2t[size_t(nd.id)]);
         }
+        // content fingerprint straight from the patterns (arrays are only built on a miss);
+        // a mask only matters where the state is unresolved, so only those masks are hashed
+        uint64_t h = 1469598103934665603ull;
+        h = fnv(h, parent.data(), parent.size() * 4);
+        h = fnv(h, leaf.data(), leaf.size());
+        h = fnv(h, taxon.data(), taxon.size() * 4);
+        {
+            uint64_t lane[4] = {h, h ^ 0x243F6A8885A308D3ull, h ^ 0x13198A2E03707344ull, h ^ 0xA4093822299F31D0ull};
+            for (int p = 0; p < P; ++p) {
+                const auto& sp = aln.patterns[size_t(p)];
+                uint64_t& l = lane[p & 3];
+                l = fnv(l, sp.states.data(), sp.states.size());
+                for (size_t t = 0; t < sp.states.size(); ++t)
+                    if (sp.states[t] < 0) {
+                        const uint64_t m = t < sp.ambiguous_masks.size() ? sp.ambiguous_masks[t] : 0;
+                        l = fnv(l, &m, 8);
+                    }
+                const double wt = double(sp.weight);
+                l = fnv(l, &wt, 8);
+            }
+            for (uint64_t l : lane) h = fnv(h, &l, 8);
+        }
+        for (auto it = problems_.begin(); it != problems_.end(); ++it)
+            if (it->key == h && it->n == n && it->P == P) {
+                problems_.splice(problems_.begin(), problems_, it);
+                return problems_.front().prob;
+            }
         std::vector<int8_t> st(size_t(P) * T);
         std::vector<uint64_t> mk(size_t(P) * T);
         std::vector<double> w(P);
@@ -147,18 +174,6 @@ public:
                 mk[size_t(p) * T + t] = size_t(t) < sp.ambiguous_masks.size() ? sp.ambiguous_masks[size_t(t)] : 0;
             }
         }
-        uint64_t h = 1469598103934665603ull;
-        h = fnv(h, parent.data(), parent.size() * 4);
-        h = fnv(h, leaf.data(), leaf.size());
-        h = fnv(h, taxon.data(), taxon.size() * 4);
-        h = fnv(h, st.data(), st.size());
-        h = fnv(h, mk.data(), mk.size() * 8);
-        h = fnv(h, w.data(), w.size() * 8);
-        for (auto it = problems_.begin(); it != problems_.end(); ++it)
-            if (it->key == h && it->n == n && it->P == P) {
-                problems_.splice(problems_.begin(), problems_, it);
-                return problems_.front().prob;
-            }
         h3g_problem* pr = nullptr;
         check(h3g_problem_create(ctx(), n, parent.data(), leaf.data(), taxon.data(), T, P, st.data(), mk.data(), w.data(), &pr));
         problems_.push_front({h, n, P, pr, 0});
