@@ -39,7 +39,6 @@ constexpr int LD = SP + 1;                // padded row stride: column walks hit
 constexpr int kMaxSweeps = 30;
 constexpr int kMaxDepth = 1024;           // open internal nodes on the traversal stack
 constexpr size_t kEigSmem = size_t(2) * SP * LD * sizeof(double);
-constexpr size_t kLnlSmem = (size_t(2) * SP * LD + 4 * SP + 3 * SP) * sizeof(double);
 
 struct FelModel {
     int S;
@@ -218,47 +217,97 @@ __global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __res
 }
 
 // ---------------------------------------------------------------- likelihoods
-// grid n_req, block 256.  ev: depth-first events, 2 node + 1 = open internal
-// node, 2 node = close node (its message goes to the parent).
-__global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const double* __restrict__ bl, const int* __restrict__ ev,
-                                                 int n_ev, int depth, double* __restrict__ stack,
-                                                 const int* __restrict__ pattern, const double* __restrict__ avec,
-                                                 const int* __restrict__ slot, double* __restrict__ out) {
-    pdl_enter();
-    extern __shared__ __align__(16) double sm[];
-    double* sU = sm;
-    double* sV = sU + SP * LD;
-    double* part = sV + SP * LD;     // [4][64]
-    double* x = part + 4 * SP;
-    double* sL = x + SP;
-    double* lam = sL + SP;
-    __shared__ int sexp[kMaxDepth];
-    __shared__ double red[kFT / 32];
-    const int tid = threadIdx.x, S = t.S, r = blockIdx.x;
-    const int p = pattern[r], sl = slot[r];
-    const double a = avec[r];
-    const double* gU = f.U + size_t(sl) * SP2;
-    const double* gV = f.V + size_t(sl) * SP2;
-    for (int e = tid; e < SP2; e += kFT) {
-        const int i = e >> 6, j = e & 63;
-        sU[i * LD + j] = gU[e];
-        sV[i * LD + j] = gV[e];
+// A request evaluates one pattern with NC eigensystems mixed at the
+// transition-matrix level, P_b = sum_c w_c U_c diag(e^{lambda_c a t_b}) V_c:
+// NC = 1 for FEL (one omega), NC = 2 for MEME (the p1 / p+ components,
+// meme.hpp:221-245).  The message of branch b is sum_c w_c U_c (e_c o (V_c L_b)).
+struct FelReqs {
+    const int* pattern;
+    const double* a;      // time scale (the site's alpha)
+    const int* slot;      // eigensystem of component 0
+    const int* slot2;     // component 1 (NC = 2)
+    const double* w1;     // weight of component 0 (NC = 2); component 1 gets 1 - w1
+};
+
+template <int NC>
+struct Spectral {
+    double* U[NC];        // shared [64][LD]
+    double* V[NC];
+    double* part[NC];     // [4][64] quarter sums of a mat-vec
+    double* x[NC];        // [64]
+    double* lam[NC];      // [64] lambda * a
+    double w[NC];
+};
+
+constexpr size_t spectral_doubles(int nc) { return size_t(nc) * (2 * SP * LD + 6 * SP); }
+constexpr size_t lnl_smem(int nc) { return (spectral_doubles(nc) + SP) * sizeof(double); }
+constexpr size_t kEbfSmem = (spectral_doubles(2) + 3 * SP) * sizeof(double);
+
+// carve shared memory and stage request r's eigensystems; returns the first free double
+template <int NC>
+__device__ double* spectral_setup(Spectral<NC>& sp, double* sm, const FelModel& f, const FelReqs& q, int r) {
+    const int tid = threadIdx.x;
+    double* z = sm;
+    int sl[NC];
+    sl[0] = q.slot[r];
+    if constexpr (NC == 2) {
+        sl[1] = q.slot2[r];
+        sp.w[0] = q.w1[r];
+        sp.w[1] = 1.0 - q.w1[r];
+    } else {
+        sp.w[0] = 1.0;
     }
-    if (tid < SP) lam[tid] = f.lam[size_t(sl) * SP + tid] * a;
-    double* stk = stack + size_t(r) * depth * SP;
-    const int row = tid & 63, qd = tid >> 6;
-    int sp = -1;
-    __syncthreads();
+    const double a = q.a[r];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        sp.U[c] = z; z += SP * LD;
+        sp.V[c] = z; z += SP * LD;
+        sp.part[c] = z; z += 4 * SP;
+        sp.x[c] = z; z += SP;
+        sp.lam[c] = z; z += SP;
+        const double* gU = f.U + size_t(sl[c]) * SP2;
+        const double* gV = f.V + size_t(sl[c]) * SP2;
+        for (int e = tid; e < SP2; e += kFT) {
+            const int i = e >> 6, j = e & 63;
+            sp.U[c][i * LD + j] = gU[e];
+            sp.V[c][i * LD + j] = gV[e];
+        }
+        if (tid < SP) sp.lam[c][tid] = f.lam[size_t(sl[c]) * SP + tid] * a;
+    }
+    return z;
+}
+
+// maximum over the 64 threads that own a state vector (named barrier 1)
+__device__ __forceinline__ double max64(double v, double* r2) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) r2[threadIdx.x >> 5] = v;
+    asm volatile("bar.sync 1, 64;" ::: "memory");
+    const double m = fmax(r2[0], r2[1]);
+    asm volatile("bar.sync 1, 64;" ::: "memory");
+    return m;
+}
+
+// Depth-first pruning of pattern p (ev: 2 node + 1 opens an internal node,
+// 2 node closes a node and sends its message to the parent's partial).  Open
+// partials live on stk with power-of-two exponents in sexp.  STORE: the
+// component messages of every non-root node are written to msg[node][c][64]
+// (the outside pass of k_meme_ebf reads them).  On return stk[0..63] holds the
+// root partial and sexp[0] its exponent.
+template <int NC, bool STORE>
+__device__ void prune(const Spectral<NC>& sp, double* sL, const Topo& t, const double* __restrict__ bl,
+                      const int* __restrict__ ev, int n_ev, double* stk, int* sexp, double* red, int p, double* msg) {
+    const int tid = threadIdx.x, S = t.S, row = tid & 63, qd = tid >> 6;
+    int sp_ = -1;
     for (int k = 0; k < n_ev; ++k) {
         const int code = ev[k], node = code >> 1;
         if (code & 1) {                                    // open an internal node: partial = 1
-            ++sp;
-            if (tid < SP) stk[sp * SP + tid] = tid < S ? 1.0 : 0.0;
-            if (tid == 0) sexp[sp] = 0;
+            ++sp_;
+            if (tid < SP) stk[sp_ * SP + tid] = tid < S ? 1.0 : 0.0;
+            if (tid == 0) sexp[sp_] = 0;
             continue;
         }
         int Ev = 0;
-        if (t.leaf[node]) {                                // x = V * leaf vector
+        if (t.leaf[node]) {                                // x_c = V_c * leaf vector
             if (tid < SP) {
                 const int tx = t.taxon[node];
                 int st = -1;
@@ -267,42 +316,63 @@ __global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const doubl
                     st = t.states[size_t(tx) * t.Pp + p];
                     if (st < 0) mk = t.masks[size_t(tx) * t.Pp + p];
                 }
-                double s = 0.0;
-                if (st >= 0) {
-                    s = sV[tid * LD + st];
-                } else {
-                    const bool all = mk == 0 || (mk & t.all_mask) == t.all_mask;
-                    for (int j = 0; j < S; ++j)
-                        if (all || ((mk >> j) & 1)) s += sV[tid * LD + j];
+                const bool all = mk == 0 || (mk & t.all_mask) == t.all_mask;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    double s = 0.0;
+                    if (st >= 0) {
+                        s = sp.V[c][tid * LD + st];
+                    } else {
+                        for (int j = 0; j < S; ++j)
+                            if (all || ((mk >> j) & 1)) s += sp.V[c][tid * LD + j];
+                    }
+                    sp.x[c][tid] = s;
                 }
-                x[tid] = s;
             }
-        } else {                                           // x = V * L(node), pop it
-            if (tid < SP) sL[tid] = stk[sp * SP + tid];
+        } else {                                           // x_c = V_c * L(node), pop it
+            if (tid < SP) sL[tid] = stk[sp_ * SP + tid];
             __syncthreads();
-            Ev = sexp[sp];
-            double s = 0.0;
+            Ev = sexp[sp_];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) s = fma(sV[row * LD + 16 * qd + j], sL[16 * qd + j], s);
-            part[qd * SP + row] = s;
+            for (int c = 0; c < NC; ++c) {
+                double s = 0.0;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) s = fma(sp.V[c][row * LD + 16 * qd + j], sL[16 * qd + j], s);
+                sp.part[c][qd * SP + row] = s;
+            }
             __syncthreads();
-            if (tid < SP) x[tid] = (part[tid] + part[SP + tid]) + (part[2 * SP + tid] + part[3 * SP + tid]);
-            --sp;
+            if (tid < SP) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    sp.x[c][tid] = (sp.part[c][tid] + sp.part[c][SP + tid]) + (sp.part[c][2 * SP + tid] + sp.part[c][3 * SP + tid]);
+            }
+            --sp_;
         }
-        if (tid < SP) x[tid] *= exp(lam[tid] * bl[node]);
+        if (tid < SP) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) sp.x[c][tid] *= exp(sp.lam[c][tid] * bl[node]);
+        }
         __syncthreads();
-        {                                                  // m = U x, into the parent's partial
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {                     // U_c x_c
             double s = 0.0;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) s = fma(sU[row * LD + 16 * qd + j], x[16 * qd + j], s);
-            part[qd * SP + row] = s;
+            for (int j = 0; j < 16; ++j) s = fma(sp.U[c][row * LD + 16 * qd + j], sp.x[c][16 * qd + j], s);
+            sp.part[c][qd * SP + row] = s;
         }
         __syncthreads();
         if (tid < SP) {
             // the two warps that own the partial multiply, take its maximum between
             // themselves (named barrier 1, 64 threads) and rescale; the other warps go on
-            const double m = tid < S ? fmax((part[tid] + part[SP + tid]) + (part[2 * SP + tid] + part[3 * SP + tid]), 0.0) : 0.0;
-            double v = stk[sp * SP + tid] * m;
+            double m = 0.0;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const double mc = (sp.part[c][tid] + sp.part[c][SP + tid]) + (sp.part[c][2 * SP + tid] + sp.part[c][3 * SP + tid]);
+                m += sp.w[c] * mc;
+                if constexpr (STORE) msg[(size_t(node) * 3 + c) * SP + tid] = tid < S ? fmax(mc, 0.0) : 0.0;
+            }
+            m = tid < S ? fmax(m, 0.0) : 0.0;
+            double v = stk[sp_ * SP + tid] * m;
             double w = v;
             for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
             if ((tid & 31) == 0) red[tid >> 5] = w;
@@ -310,18 +380,143 @@ __global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const doubl
             const double mx = fmax(red[0], red[1]);
             if (mx > 0.0 && mx < 0x1p-256) {
                 v *= 0x1p256;
-                if (tid == 0) sexp[sp] += 256;
+                if (tid == 0) sexp[sp_] += 256;
             }
-            stk[sp * SP + tid] = v;
-            if (tid == 0) sexp[sp] += Ev;
+            stk[sp_ * SP + tid] = v;
+            if (tid == 0) sexp[sp_] += Ev;
         }
     }
     __syncthreads();
-    // root: lnL = log(pi . L) - E ln 2, or the reference's -1e20 for L <= 0
+}
+
+// grid n_req, block 256: log-likelihood of each request, or the reference's -1e20 for L <= 0
+template <int NC>
+__global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const double* __restrict__ bl, const int* __restrict__ ev,
+                                                 int n_ev, int depth, double* __restrict__ stack, FelReqs q,
+                                                 double* __restrict__ out) {
+    pdl_enter();
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int sexp[kMaxDepth];
+    __shared__ double red[kFT / 32];
+    const int tid = threadIdx.x, S = t.S, r = blockIdx.x;
+    Spectral<NC> sp;
+    double* sL = spectral_setup<NC>(sp, sm, f, q, r);
+    double* stk = stack + size_t(r) * depth * SP;
+    __syncthreads();
+    prune<NC, false>(sp, sL, t, bl, ev, n_ev, stk, sexp, red, q.pattern[r], nullptr);
     double v = 0.0;
     if (tid < S) v = f.pi[tid] * stk[tid];
     const double L = block_sum_or_max(v, red, false);
     if (tid == 0) out[r] = L > 0.0 ? log(L) - double(sexp[0]) * 0.69314718055994530942 : -1e20;
+}
+
+// grid n_req, block 256: MEME's empirical Bayes factors (meme.hpp:484-588).  For
+// every branch b the reference re-prunes the pattern twice, with b alone in
+// class 1 and alone in class +; the likelihood is linear in b's message, so
+// both follow from one inside-outside pass: L_c(b) = top_b . M_c(b), where
+// top_b = O_parent o (product of b's siblings' messages) and O is the outside
+// vector (pi at the root, P_mix^T top below).  Every vector may carry any
+// positive factor common to both classes, so the outside pass normalises by
+// the maximum instead of tracking exponents.  ebf[r][b] for every non-root b.
+__global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const double* __restrict__ bl, const int* __restrict__ ev,
+                                                  int n_ev, int depth, double* __restrict__ stack, FelReqs q,
+                                                  double* __restrict__ msg_all, double* __restrict__ ebf_all) {
+    pdl_enter();
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int sexp[kMaxDepth];
+    __shared__ double red[kFT / 32], r2[2], r4[4];
+    const int tid = threadIdx.x, S = t.S, r = blockIdx.x, n = t.n, row = tid & 63, qd = tid >> 6;
+    Spectral<2> sp;
+    double* sL = spectral_setup<2>(sp, sm, f, q, r);
+    double* ou = sL + SP;                                  // outside vector of the open node
+    double* top = ou + SP;
+    double* stk = stack + size_t(r) * depth * SP;
+    double* msg = msg_all + size_t(r) * n * 3 * SP;        // [node][M_1 | M_+ | O or prefix][64]
+    double* ebf = ebf_all + size_t(r) * n;
+    __syncthreads();
+    prune<2, true>(sp, sL, t, bl, ev, n_ev, stk, sexp, red, q.pattern[r], msg);
+    const double w0 = sp.w[0], w1 = sp.w[1];
+    if (tid == 0) ebf[t.root] = 1.0;
+    for (int k = 0; k < n_ev; ++k) {                       // internal nodes in pre-order
+        const int code = ev[k];
+        if (!(code & 1)) continue;
+        const int u = code >> 1;
+        if (tid < SP) ou[tid] = tid >= S ? 0.0 : (u == t.root ? f.pi[tid] : msg[(size_t(u) * 3 + 2) * SP + tid]);
+        const int c0 = t.ch_off[u], c1 = t.ch_off[u + 1];
+        if (tid < SP) {                                    // prefix products into each child's third slot
+            double acc = ou[tid];
+            for (int i = c0; i < c1; ++i) {
+                const size_t b = size_t(t.ch[i]) * 3 * SP;
+                msg[b + 2 * SP + tid] = acc;
+                acc *= w0 * msg[b + tid] + w1 * msg[b + SP + tid];
+                const double mx = max64(acc, r2);
+                if (mx > 0.0) acc /= mx;
+            }
+        }
+        __syncthreads();
+        double suf = tid < S ? 1.0 : 0.0;
+        for (int i = c1 - 1; i >= c0; --i) {               // suffix products, children in reverse
+            const int c = t.ch[i];
+            const size_t b = size_t(c) * 3 * SP;
+            if (tid < SP) {
+                double tv = msg[b + 2 * SP + tid] * suf;
+                const double mx = max64(tv, r2);
+                if (mx > 0.0) tv /= mx;
+                top[tid] = tv;
+                double s1 = tv * msg[b + tid], s2 = tv * msg[b + SP + tid];
+                for (int o = 16; o > 0; o >>= 1) {
+                    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                }
+                if ((tid & 31) == 0) { r4[2 * (tid >> 5)] = s1; r4[2 * (tid >> 5) + 1] = s2; }
+                asm volatile("bar.sync 1, 64;" ::: "memory");
+                if (tid == 0) {
+                    const double L1 = r4[0] + r4[2], Lp = r4[1] + r4[3];
+                    double e = 0.0;
+                    if (L1 > 0.0 && Lp > 0.0) e = exp(fmin(fmax(log(Lp) - log(L1), -50.0), 50.0));
+                    else if (!(L1 > 0.0) && Lp > 0.0) e = 1e6;
+                    ebf[c] = e;
+                }
+                suf *= w0 * msg[b + tid] + w1 * msg[b + SP + tid];
+                const double ms = max64(suf, r2);
+                if (ms > 0.0) suf /= ms;
+            }
+            __syncthreads();
+            if (!t.leaf[c]) {                              // O_c = sum_k w_k V_k^T (e_k o (U_k^T top))
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) s = fma(sp.U[m][(16 * qd + j) * LD + row], top[16 * qd + j], s);
+                    sp.part[m][qd * SP + row] = s;
+                }
+                __syncthreads();
+                if (tid < SP) {
+#pragma unroll
+                    for (int m = 0; m < 2; ++m)
+                        sp.x[m][tid] = ((sp.part[m][tid] + sp.part[m][SP + tid]) + (sp.part[m][2 * SP + tid] + sp.part[m][3 * SP + tid])) *
+                                       exp(sp.lam[m][tid] * bl[c]);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) s = fma(sp.V[m][(16 * qd + j) * LD + row], sp.x[m][16 * qd + j], s);
+                    sp.part[m][qd * SP + row] = s;
+                }
+                __syncthreads();
+                if (tid < SP) {
+                    double o = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 2; ++m)
+                        o += sp.w[m] * ((sp.part[m][tid] + sp.part[m][SP + tid]) + (sp.part[m][2 * SP + tid] + sp.part[m][3 * SP + tid]));
+                    msg[b + 2 * SP + tid] = tid < S ? fmax(o, 0.0) : 0.0;
+                }
+                __syncthreads();
+            }
+        }
+    }
 }
 
 }  // namespace
@@ -335,19 +530,27 @@ struct FelDevice {
     double* d_bl = nullptr;
     int* d_ev = nullptr;
     double* d_stack = nullptr;
-    unsigned char* d_req = nullptr;       // per batch: [om | a | eslot | eprev | pat | slot], packed to the batch's sizes
+    unsigned char* d_req = nullptr;       // per batch: [om | a | w1 | eslot | eprev | pat | slot | slot2], packed to the batch's sizes
     unsigned char* h_req = nullptr;       // pinned mirror
     double* d_out = nullptr;
     double* h_out = nullptr;
+    double* d_msg = nullptr;              // EBF pass: [kEbfChunk][n][3][64], allocated on first use
+    double* d_ebf = nullptr;              // [kEbfChunk][n]
+    double* h_ebf = nullptr;
     size_t h2d = 0, d2h = 0;              // bytes moved by the batches so far
     std::vector<void*> owned;
+    std::vector<int> order;               // one-component requests first, then two-component ones
     ~FelDevice() {
         for (void* p : owned) cudaFree(p);
         if (h_req) cudaFreeHost(h_req);
         if (h_out) cudaFreeHost(h_out);
+        if (h_ebf) cudaFreeHost(h_ebf);
     }
-    size_t req_bytes() const { return 2 * size_t(max_req) * sizeof(double) + 4 * size_t(max_req) * sizeof(int); }
+    // a batch holds up to max_req requests and two eigensolves per request
+    size_t req_bytes() const { return 4 * size_t(max_req) * sizeof(double) + 7 * size_t(max_req) * sizeof(int); }
 };
+
+constexpr int kEbfChunk = 256;
 
 FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
                              const double* branch_lengths, int max_requests, int n_slots, std::string* err) {
@@ -362,7 +565,7 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     d->max_req = std::max(1, max_requests);
     d->n_slots = std::max(1, n_slots);
     d->t = problem_topo(pr, S);
-    // depth-first events in the reference's child order
+    // depth-first events in the children CSR order
     std::vector<int> ev;
     ev.reserve(2 * size_t(v.n));
     int open = 0, deepest = 1;
@@ -426,59 +629,144 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     static bool configured = false;
     if (ok && !configured) {
         ok = cudaFuncSetAttribute(k_fel_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEigSmem)) == cudaSuccess &&
-             cudaFuncSetAttribute(k_fel_lnl, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLnlSmem)) == cudaSuccess;
+             cudaFuncSetAttribute(k_fel_lnl<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lnl_smem(1))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_fel_lnl<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lnl_smem(2))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_meme_ebf, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEbfSmem)) == cudaSuccess;
         configured = ok;
     }
     if (!ok) { *err = std::string("FEL set-up: ") + cudaGetErrorString(cudaGetLastError()); delete d; return nullptr; }
     return d;
 }
 
-bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
-                     const int* req_pattern, const double* req_a, const int* req_slot, double* lnl_out, std::string* err) {
-    if (n_eig > d->max_req || n_req > d->max_req || n_eig < 0 || n_req < 0) { *err = "FEL batch too large"; return false; }
-    if (n_req == 0) return true;
+namespace {
+
+// Validate a batch, pack it into one host-to-device copy in `order` and launch
+// the eigensolves.  Returns the request views (in packed order) through q.
+bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
+                 const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2, const double* req_w1,
+                 const std::vector<int>& order, FelReqs* q, std::string* err) {
+    if (n_eig > 2 * d->max_req || n_req > d->max_req || n_eig < 0 || n_req < 0) { *err = "FEL batch too large"; return false; }
     for (int i = 0; i < n_eig; ++i)
         if (eig_slot[i] < 0 || eig_slot[i] >= d->n_slots || eig_prev[i] < -1 || eig_prev[i] >= d->n_slots) {
             *err = "FEL eigensystem slot out of range";
             return false;
         }
-    for (int i = 0; i < n_req; ++i)
-        if (req_slot[i] < 0 || req_slot[i] >= d->n_slots || req_pattern[i] < 0 || req_pattern[i] >= d->t.P) {
+    for (int i = 0; i < n_req; ++i) {
+        const bool mix = req_slot2 && req_slot2[i] >= 0;
+        if (req_slot[i] < 0 || req_slot[i] >= d->n_slots || req_pattern[i] < 0 || req_pattern[i] >= d->t.P ||
+            (mix && req_slot2[i] >= d->n_slots) || !(req_a[i] > 0.0) || (req_w1 && !(req_w1[i] >= 0.0 && req_w1[i] <= 1.0))) {
             *err = "FEL request out of range";
             return false;
         }
-    // one host-to-device copy of exactly this batch's arrays
-    const size_t o_a = size_t(n_eig) * sizeof(double), o_es = o_a + size_t(n_req) * sizeof(double);
-    const size_t o_pv = o_es + size_t(n_eig) * sizeof(int), o_pat = o_pv + size_t(n_eig) * sizeof(int);
-    const size_t o_sl = o_pat + size_t(n_req) * sizeof(int);
-    const size_t bytes = o_sl + size_t(n_req) * sizeof(int);
+    }
+    const size_t o_a = size_t(n_eig) * sizeof(double), o_w = o_a + size_t(n_req) * sizeof(double);
+    const size_t o_es = o_w + size_t(n_req) * sizeof(double), o_pv = o_es + size_t(n_eig) * sizeof(int);
+    const size_t o_pat = o_pv + size_t(n_eig) * sizeof(int), o_sl = o_pat + size_t(n_req) * sizeof(int);
+    const size_t o_s2 = o_sl + size_t(n_req) * sizeof(int);
+    const size_t bytes = o_s2 + size_t(n_req) * sizeof(int);
     unsigned char* h = d->h_req;
     std::copy(eig_omega, eig_omega + n_eig, reinterpret_cast<double*>(h));
-    std::copy(req_a, req_a + n_req, reinterpret_cast<double*>(h + o_a));
     std::copy(eig_slot, eig_slot + n_eig, reinterpret_cast<int*>(h + o_es));
     std::copy(eig_prev, eig_prev + n_eig, reinterpret_cast<int*>(h + o_pv));
-    std::copy(req_pattern, req_pattern + n_req, reinterpret_cast<int*>(h + o_pat));
-    std::copy(req_slot, req_slot + n_req, reinterpret_cast<int*>(h + o_sl));
+    for (int k = 0; k < n_req; ++k) {
+        const int i = order[k];
+        reinterpret_cast<double*>(h + o_a)[k] = req_a[i];
+        reinterpret_cast<double*>(h + o_w)[k] = req_w1 ? req_w1[i] : 1.0;
+        reinterpret_cast<int*>(h + o_pat)[k] = req_pattern[i];
+        reinterpret_cast<int*>(h + o_sl)[k] = req_slot[i];
+        reinterpret_cast<int*>(h + o_s2)[k] = req_slot2 ? req_slot2[i] : -1;
+    }
     cudaStream_t s = d->s;
-    bool ok = cudaMemcpyAsync(d->d_req, h, bytes, cudaMemcpyHostToDevice, s) == cudaSuccess;
-    unsigned char* q = d->d_req;
-    if (ok && n_eig > 0)
-        launch_k(k_fel_eig, n_eig, kFT, kEigSmem, s, d->f, reinterpret_cast<const double*>(q),
-                 reinterpret_cast<const int*>(q + o_es), reinterpret_cast<const int*>(q + o_pv));
-    if (ok)
-        launch_k(k_fel_lnl, n_req, kFT, kLnlSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
-                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack,
-                 reinterpret_cast<const int*>(q + o_pat), reinterpret_cast<const double*>(q + o_a),
-                 reinterpret_cast<const int*>(q + o_sl), d->d_out);
+    if (cudaMemcpyAsync(d->d_req, h, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        *err = std::string("FEL batch copy: ") + cudaGetErrorString(cudaGetLastError());
+        return false;
+    }
     d->h2d += bytes;
-    d->d2h += size_t(n_req) * sizeof(double);
-    ok = ok && cudaGetLastError() == cudaSuccess &&
-         cudaMemcpyAsync(d->h_out, d->d_out, n_req * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-         cudaStreamSynchronize(s) == cudaSuccess;
-    if (!ok) { *err = std::string("FEL batch: ") + cudaGetErrorString(cudaGetLastError()); return false; }
-    std::copy(d->h_out, d->h_out + n_req, lnl_out);
+    unsigned char* g = d->d_req;
+    if (n_eig > 0)
+        launch_k(k_fel_eig, n_eig, kFT, kEigSmem, s, d->f, reinterpret_cast<const double*>(g),
+                 reinterpret_cast<const int*>(g + o_es), reinterpret_cast<const int*>(g + o_pv));
+    *q = FelReqs{reinterpret_cast<const int*>(g + o_pat), reinterpret_cast<const double*>(g + o_a),
+                 reinterpret_cast<const int*>(g + o_sl), reinterpret_cast<const int*>(g + o_s2),
+                 reinterpret_cast<const double*>(g + o_w)};
     return true;
 }
+
+FelReqs offset(const FelReqs& q, int k) {
+    return FelReqs{q.pattern + k, q.a + k, q.slot + k, q.slot2 + k, q.w1 + k};
+}
+
+}  // namespace
+
+bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
+                     const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
+                     const double* req_w1, double* lnl_out, std::string* err) {
+    if (n_req == 0 && n_eig == 0) return true;
+    auto& order = d->order;
+    order.clear();
+    for (int i = 0; i < n_req; ++i)
+        if (!(req_slot2 && req_slot2[i] >= 0)) order.push_back(i);
+    const int n1 = int(order.size());
+    for (int i = 0; i < n_req; ++i)
+        if (req_slot2 && req_slot2[i] >= 0) order.push_back(i);
+    FelReqs q{};
+    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, order, &q, err))
+        return false;
+    cudaStream_t s = d->s;
+    if (n1 > 0)
+        launch_k(k_fel_lnl<1>, n1, kFT, lnl_smem(1), s, d->f, d->t, static_cast<const double*>(d->d_bl),
+                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack, q, d->d_out);
+    if (n_req > n1)
+        launch_k(k_fel_lnl<2>, n_req - n1, kFT, lnl_smem(2), s, d->f, d->t, static_cast<const double*>(d->d_bl),
+                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack + size_t(n1) * d->depth * SP,
+                 offset(q, n1), d->d_out + n1);
+    d->d2h += size_t(n_req) * sizeof(double);
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    (n_req == 0 || cudaMemcpyAsync(d->h_out, d->d_out, n_req * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess) &&
+                    cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) { *err = std::string("FEL batch: ") + cudaGetErrorString(cudaGetLastError()); return false; }
+    for (int k = 0; k < n_req; ++k) lnl_out[order[k]] = d->h_out[k];
+    return true;
+}
+
+bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
+                    const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
+                    const double* req_w1, double* ebf_out, std::string* err) {
+    if (n_req > kEbfChunk) { *err = "EBF batch larger than 256 requests"; return false; }
+    for (int i = 0; i < n_req; ++i)
+        if (req_slot2[i] < 0) { *err = "EBF request needs two components"; return false; }
+    if (!d->d_msg) {
+        void *m = nullptr, *e = nullptr;
+        bool ok = cudaMalloc(&m, size_t(kEbfChunk) * d->n * 3 * SP * sizeof(double)) == cudaSuccess;
+        if (m) d->owned.push_back(m);
+        ok = ok && cudaMalloc(&e, size_t(kEbfChunk) * d->n * sizeof(double)) == cudaSuccess;
+        if (e) d->owned.push_back(e);
+        ok = ok && cudaMallocHost(reinterpret_cast<void**>(&d->h_ebf), size_t(kEbfChunk) * d->n * sizeof(double)) == cudaSuccess;
+        if (!ok) { *err = "EBF scratch allocation failed"; return false; }
+        d->d_msg = static_cast<double*>(m);
+        d->d_ebf = static_cast<double*>(e);
+    }
+    auto& order = d->order;
+    order.resize(n_req);
+    for (int i = 0; i < n_req; ++i) order[i] = i;
+    FelReqs q{};
+    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, order, &q, err))
+        return false;
+    cudaStream_t s = d->s;
+    const size_t bytes = size_t(n_req) * d->n * sizeof(double);
+    if (n_req > 0)
+        launch_k(k_meme_ebf, n_req, kFT, kEbfSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
+                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack, q, d->d_msg, d->d_ebf);
+    d->d2h += bytes;
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    (n_req == 0 || cudaMemcpyAsync(d->h_ebf, d->d_ebf, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess) &&
+                    cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) { *err = std::string("EBF batch: ") + cudaGetErrorString(cudaGetLastError()); return false; }
+    std::copy(d->h_ebf, d->h_ebf + size_t(n_req) * d->n, ebf_out);
+    return true;
+}
+
+int fel_device_max_ebf(const FelDevice* d) { return std::min(kEbfChunk, d->max_req); }
 
 void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h) {
     *h2d = d->h2d;

@@ -3,12 +3,12 @@
 //
 // Each pattern runs the reference's search (analyses/fel.hpp:326-446 with
 // every branch tested; optimisers from opt/nelder_mead.hpp:24-229) written as
-// a C++20 coroutine: every likelihood evaluation is a co_await that parks the
-// pattern with its requested (alpha, beta).  The driver gathers the parked
-// requests of all patterns, evaluates them in one device batch
-// (h3g_fel.cu), hands each pattern its log-likelihood and resumes it.  The
-// search path of a pattern is therefore exactly the reference's; only the
-// likelihood evaluations are batched.
+// a C++20 coroutine (h3g_sitefit.h): every likelihood evaluation is a
+// co_await that parks the pattern with its requested (alpha, beta); the
+// lockstep loop evaluates the parked requests of all patterns in one device
+// batch (h3g_fel.cu) and resumes them.  The search path of a pattern is
+// therefore exactly the reference's; only the likelihood evaluations are
+// batched.
 //
 // Eigensystems: a pattern keeps its current eigensystem while
 // |omega - cached omega| <= 1e-12 (the reference's per-pattern cache,
@@ -17,55 +17,26 @@
 // into a shared slot.
 #include <algorithm>
 #include <cmath>
-#include <coroutine>
-#include <cstring>
-#include <exception>
 #include <new>
 #include <string>
-#include <unordered_map>
-#include <utility>
 #include <vector>
 
-#include "h3g_fel.h"
+#include "h3g_sitefit.h"
 
-namespace h3g {
+namespace h3g::sitefit {
 namespace {
 
-constexpr int kSharedSlots = 64;
-
-struct Site {
-    int pattern = 0;
-    bool pending = false;
-    double a = 0.0, b = 0.0, lnl = 0.0;
-    double cached_omega = -1.0;
-    int slot = -1;
-    h3g_fel_result res{};
-};
-
-struct Fit {
-    struct promise_type {
-        std::exception_ptr error;
-        Fit get_return_object() { return Fit{std::coroutine_handle<promise_type>::from_promise(*this)}; }
-        std::suspend_always initial_suspend() noexcept { return {}; }
-        std::suspend_always final_suspend() noexcept { return {}; }
-        void return_void() {}
-        void unhandled_exception() { error = std::current_exception(); }
-    };
-    std::coroutine_handle<promise_type> h;
-    explicit Fit(std::coroutine_handle<promise_type> hh) : h(hh) {}
-    Fit(Fit&& o) noexcept : h(std::exchange(o.h, {})) {}
-    Fit& operator=(Fit&&) = delete;
-    ~Fit() { if (h) h.destroy(); }
-};
-
-// co_await Lnl{site, a, b}: log-likelihood of the site's pattern at (a, b)
+// co_await Lnl{site, alpha, beta}: FEL's likelihood at (alpha, beta): time scale
+// alpha, omega = beta / alpha
 struct Lnl {
     Site& s;
     double a, b;
-    bool await_ready() const noexcept { return false; }
-    void await_suspend(std::coroutine_handle<>) noexcept { s.pending = true; s.a = a; s.b = b; }
-    double await_resume() const noexcept { ++s.res.evaluations; return s.lnl; }
+    Eval ev() const {
+        const double as = std::max(a, 1e-12);
+        return Eval{s, Req{as, b / as, -1.0, 1.0, 0.0}};
+    }
 };
+inline Eval operator co_await(const Lnl& l) { return l.ev(); }
 
 struct Vertex { double a, b, f; };
 
@@ -79,8 +50,10 @@ void sort3(Vertex (&v)[3]) {
     }
 }
 
+}  // namespace
+
 // The reference's per-pattern search, one likelihood per co_await.
-Fit fit_pattern(Site& s) {
+Fit fel_search(Site& s, h3g_fel_result& res) {
     // 12-point start grid (fel.hpp:385-401)
     static const double grid[12][2] = {{0.01, 0.1}, {1.0, 0.1}, {1.0, 0.5}, {1.0, 1.0}, {1.0, 5.0}, {10.0, 0.1},
                                        {0.01, 0.5}, {0.01, 5.0}, {10.0, 0.5}, {10.0, 1.0}, {10.0, 50.0}, {100.0, 1.0}};
@@ -135,12 +108,12 @@ Fit fit_pattern(Site& s) {
         }
 #undef H3G_NM_EVAL
         sort3(v);
-        s.res.alpha = v[0].a;
-        s.res.beta = v[0].b;
-        s.res.log_l_alt = -v[0].f;
+        res.alpha = v[0].a;
+        res.beta = v[0].b;
+        res.log_l_alt = -v[0].f;
     }
     // null model alpha = beta: start grid, then Brent on [1e-4, 50] (fel.hpp:415-434)
-    const double init_null = (std::min(s.res.alpha, 100.0) + 3.0 * std::min(s.res.beta, 100.0)) / 4.0;
+    const double init_null = (std::min(res.alpha, 100.0) + 3.0 * std::min(res.beta, 100.0)) / 4.0;
     double best_null = co_await Lnl{s, init_null, init_null}, best_na = init_null;
     for (double c : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0}) {
         const double l = co_await Lnl{s, c, c};
@@ -188,160 +161,104 @@ Fit fit_pattern(Site& s) {
                 else if (fu <= fv || v == x || v == w) { v = u; fv = fu; }
             }
         }
-        s.res.alpha_null = x;
-        s.res.log_l_null = -fx;
+        res.alpha_null = x;
+        res.log_l_null = -fx;
     }
     double lrt = 0.0;
-    if (s.res.log_l_alt > -1e10 && s.res.log_l_null > -1e10) lrt = std::max(0.0, 2.0 * (s.res.log_l_alt - s.res.log_l_null));
-    s.res.lrt = lrt;
-    s.res.p_value = std::erfc(std::sqrt(lrt / 2.0));
+    if (res.log_l_alt > -1e10 && res.log_l_null > -1e10) lrt = std::max(0.0, 2.0 * (res.log_l_alt - res.log_l_null));
+    res.lrt = lrt;
+    res.p_value = std::erfc(std::sqrt(lrt / 2.0));
+    res.evaluations = s.evaluations;
 }
 
-uint64_t bits_of(double x) {
-    uint64_t u;
-    std::memcpy(&u, &x, sizeof u);
-    return u;
+h3g_status prepare_site_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths, const char* who,
+                            FelProblemView* pv, std::vector<int>* variable) {
+    const std::string w(who);
+    FelProblemView& v = *pv;
+    if (!m || !branch_lengths || !fel_problem_view(prob, &v)) {
+        fel_set_error(prob, w + ": null argument");
+        return H3G_ERR_ARG;
+    }
+    const int S = m->S;
+    if (S < 2 || S > 64 || !m->pi || !m->Qs || !m->Qn) {
+        fel_set_error(prob, w + ": model needs 2 <= S <= 64, pi, Qs and Qn");
+        return H3G_ERR_ARG;
+    }
+    for (int i = 0; i < S; ++i)
+        if (!std::isfinite(m->pi[i]) || m->pi[i] < 0.0) { fel_set_error(prob, w + ": pi must be finite and >= 0"); return H3G_ERR_NUMERIC; }
+    for (int e = 0; e < S * S; ++e)
+        if (!std::isfinite(m->Qs[e]) || !std::isfinite(m->Qn[e]) || m->Qs[e] < 0.0 || m->Qn[e] < 0.0) {
+            if (e / S == e % S) continue;
+            fel_set_error(prob, w + ": rates must be finite and >= 0");
+            return H3G_ERR_NUMERIC;
+        }
+    for (int i = 0; i < v.n; ++i)
+        if (i != v.root && (!std::isfinite(branch_lengths[i]) || branch_lengths[i] < 0.0)) {
+            fel_set_error(prob, w + ": branch lengths must be finite and >= 0");
+            return H3G_ERR_NUMERIC;
+        }
+    if (v.P > 0 && v.T > 0) {
+        int max_state = -1;
+        for (size_t e = 0; e < size_t(v.P) * v.T; ++e) max_state = std::max<int>(max_state, v.states[e]);
+        if (max_state >= S) { fel_set_error(prob, w + ": a pattern state is >= S"); return H3G_ERR_ARG; }
+    }
+    variable->clear();
+    for (int p = 0; p < v.P; ++p) {
+        int first = -1;
+        bool invariant = true;
+        for (int t = 0; t < v.T; ++t) {
+            const int st = v.states[size_t(p) * v.T + t];
+            if (st < 0) continue;
+            if (first < 0) first = st;
+            else if (st != first) { invariant = false; break; }
+        }
+        if (!invariant) variable->push_back(p);
+    }
+    return H3G_OK;
 }
 
-}  // namespace
-}  // namespace h3g
+}  // namespace h3g::sitefit
 
 using namespace h3g;
+using namespace h3g::sitefit;
 
 extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths,
                                   h3g_fel_result* out) {
     if (!prob) return H3G_ERR_ARG;
     try {
         FelProblemView v;
-        if (!m || !branch_lengths || !out || !fel_problem_view(prob, &v)) {
-            fel_set_error(prob, "h3g_fel_run: null argument");
-            return H3G_ERR_ARG;
-        }
-        const int S = m->S;
-        if (S < 2 || S > 64 || !m->pi || !m->Qs || !m->Qn) {
-            fel_set_error(prob, "h3g_fel_run: model needs 2 <= S <= 64, pi, Qs and Qn");
-            return H3G_ERR_ARG;
-        }
-        for (int i = 0; i < S; ++i)
-            if (!std::isfinite(m->pi[i]) || m->pi[i] < 0.0) { fel_set_error(prob, "h3g_fel_run: pi must be finite and >= 0"); return H3G_ERR_NUMERIC; }
-        for (int e = 0; e < S * S; ++e)
-            if (!std::isfinite(m->Qs[e]) || !std::isfinite(m->Qn[e]) || m->Qs[e] < 0.0 || m->Qn[e] < 0.0) {
-                if (e / S == e % S) continue;
-                fel_set_error(prob, "h3g_fel_run: rates must be finite and >= 0");
-                return H3G_ERR_NUMERIC;
-            }
-        for (int i = 0; i < v.n; ++i)
-            if (i != v.root && (!std::isfinite(branch_lengths[i]) || branch_lengths[i] < 0.0)) {
-                fel_set_error(prob, "h3g_fel_run: branch lengths must be finite and >= 0");
-                return H3G_ERR_NUMERIC;
-            }
-        if (v.P > 0 && v.T > 0) {
-            int max_state = -1;
-            for (size_t e = 0; e < size_t(v.P) * v.T; ++e) max_state = std::max<int>(max_state, v.states[e]);
-            if (max_state >= S) { fel_set_error(prob, "h3g_fel_run: a pattern state is >= S"); return H3G_ERR_ARG; }
-        }
-        // invariant patterns (all resolved states equal) are not fitted (fel.hpp:333-356)
-        std::vector<Site> sites;
-        sites.reserve(v.P);
-        for (int p = 0; p < v.P; ++p) {
-            out[p] = h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0};
-            int first = -1;
-            bool invariant = true;
-            for (int t = 0; t < v.T; ++t) {
-                const int st = v.states[size_t(p) * v.T + t];
-                if (st < 0) continue;
-                if (first < 0) first = st;
-                else if (st != first) { invariant = false; break; }
-            }
-            if (!invariant) {
-                Site s;
-                s.pattern = p;
-                sites.push_back(s);
-            }
-        }
-        const int N = int(sites.size());
+        std::vector<int> variable;
+        if (!out) { fel_set_error(prob, "h3g_fel_run: null argument"); return H3G_ERR_ARG; }
+        const h3g_status pst = prepare_site_run(prob, m, branch_lengths, "h3g_fel_run", &v, &variable);
+        if (pst != H3G_OK) return pst;
+        for (int p = 0; p < v.P; ++p) out[p] = h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0};
+        const int N = int(variable.size());
         if (N == 0) return H3G_OK;
+        const int S = m->S;
         std::string err;
-        FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, N, kSharedSlots + N, &err);
+        LockstepOptions opt;
+        opt.cache_tol = 1e-12;              // fel.hpp:368-376
+        opt.max_requests = N;               // one request per pattern at a time
+        opt.temp_slots = 0;
+        FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, opt.max_requests,
+                                           slots_needed(N, opt.temp_slots), &err);
         if (!dev) { fel_set_error(prob, "h3g_fel_run: " + err); return H3G_ERR_CUDA; }
+        std::vector<Site> sites(N);
+        std::vector<h3g_fel_result> res(N, h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0});
         std::vector<Fit> fits;
         fits.reserve(N);
-        for (auto& s : sites) fits.push_back(fit_pattern(s));
-        for (auto& f : fits) f.h.resume();                 // run to the first evaluation
-        std::unordered_map<uint64_t, int> shared;          // omega bits -> shared slot
-        std::vector<int> req_site, req_pat, req_slot, eig_slot, eig_prev;
-        std::vector<double> req_a, eig_om, lnl;
-        std::unordered_map<uint64_t, int> count;
-        h3g_status st = H3G_OK;
-        while (st == H3G_OK) {
-            req_site.clear(); req_pat.clear(); req_slot.clear(); req_a.clear(); eig_slot.clear(); eig_om.clear();
-            eig_prev.clear();
-            count.clear();
-            for (int i = 0; i < N; ++i) {
-                if (!sites[i].pending) continue;
-                req_site.push_back(i);
-                Site& s = sites[i];
-                const double om = s.b / std::max(s.a, 1e-12);
-                if (!(s.slot >= 0 && std::fabs(om - s.cached_omega) <= 1e-12)) ++count[bits_of(om)];
-            }
-            if (req_site.empty()) break;
-            for (int i : req_site) {
-                Site& s = sites[i];
-                const double as = std::max(s.a, 1e-12), om = s.b / as;
-                if (!(s.slot >= 0 && std::fabs(om - s.cached_omega) <= 1e-12)) {
-                    s.cached_omega = om;
-                    const uint64_t key = bits_of(om);
-                    auto it = shared.find(key);
-                    if (it != shared.end()) {
-                        s.slot = it->second;
-                    } else if (count[key] >= 2 && int(shared.size()) < kSharedSlots) {
-                        const int slot = int(shared.size());
-                        shared.emplace(key, slot);
-                        eig_om.push_back(om);
-                        eig_slot.push_back(slot);
-                        s.slot = slot;
-                    } else {
-                        eig_prev.resize(eig_slot.size(), -1);
-                        eig_prev.push_back(s.slot);        // warm start from the pattern's last eigensystem
-                        s.slot = kSharedSlots + i;
-                        eig_om.push_back(om);
-                        eig_slot.push_back(s.slot);
-                    }
-                }
-                req_pat.push_back(s.pattern);
-                req_a.push_back(as);
-                req_slot.push_back(s.slot);
-            }
-            lnl.assign(req_site.size(), 0.0);
-            eig_prev.resize(eig_slot.size(), -1);          // new shared slots start from the identity
-            if (!fel_device_eval(dev, int(eig_om.size()), eig_om.data(), eig_slot.data(), eig_prev.data(), int(req_site.size()), req_pat.data(),
-                                 req_a.data(), req_slot.data(), lnl.data(), &err)) {
-                fel_set_error(prob, "h3g_fel_run: " + err);
-                st = H3G_ERR_CUDA;
-                break;
-            }
-            for (size_t r = 0; r < req_site.size(); ++r) {
-                Site& s = sites[req_site[r]];
-                s.lnl = lnl[r];
-                s.pending = false;
-                fits[req_site[r]].h.resume();
-                if (fits[req_site[r]].h.promise().error) {
-                    fel_set_error(prob, "h3g_fel_run: optimiser failed");
-                    st = H3G_ERR_NUMERIC;
-                    break;
-                }
-            }
+        for (int i = 0; i < N; ++i) {
+            sites[i].pattern = variable[i];
+            fits.push_back(fel_search(sites[i], res[i]));
         }
+        const h3g_status st = run_lockstep(dev, sites, fits, opt, &err);
         size_t h2d = 0, d2h = 0;
         fel_device_transfer(dev, &h2d, &d2h);
         fel_device_destroy(dev);
-        if (st != H3G_OK) return st;
+        if (st != H3G_OK) { fel_set_error(prob, "h3g_fel_run: " + err); return st; }
         // the run's own inputs and outputs: model, branch lengths, per-pattern results
         fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h);
-        for (int i = 0; i < N; ++i) {
-            if (!fits[i].h.done()) { fel_set_error(prob, "h3g_fel_run: a pattern did not finish"); return H3G_ERR_STATE; }
-            out[sites[i].pattern] = sites[i].res;
-        }
+        for (int i = 0; i < N; ++i) out[variable[i]] = res[i];
         return H3G_OK;
     } catch (const std::bad_alloc&) {
         fel_set_error(prob, "h3g_fel_run: host allocation failed");

@@ -6,6 +6,7 @@
 #include <pybind11/stl.h>
 
 #include "hyphy/analyses/fel_gpu.hpp"
+#include "hyphy/analyses/meme_gpu.hpp"
 #include "hyphy/opt/optimizer_gpu.hpp"
 #include "hyphy/core/likelihood_gpu.hpp"
 
@@ -288,4 +289,40 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("conversion_factor", &FELAnalyzer::conversion_factor)
         .def_readonly("baseline_tree_length", &FELAnalyzer::baseline_tree_length)
         .def_readonly("site_results", &FELAnalyzer::site_results);
+
+    // MEME (bindings.cpp of the reference: MEMESiteResult / MEMEAnalyzer)
+    using hyphy::analyses::MEMEAnalyzer;
+    using hyphy::analyses::MEMESiteResult;
+    py::class_<MEMESiteResult>(m, "MEMESiteResult")
+        .def_readonly("site_index", &MEMESiteResult::site_index)
+        .def_readonly("alpha", &MEMESiteResult::alpha)
+        .def_readonly("beta1", &MEMESiteResult::beta1)
+        .def_readonly("p1", &MEMESiteResult::p1)
+        .def_readonly("beta_plus", &MEMESiteResult::beta_plus)
+        .def_readonly("p_plus", &MEMESiteResult::p_plus)
+        .def_readonly("lrt", &MEMESiteResult::lrt)
+        .def_readonly("p_value", &MEMESiteResult::p_value)
+        .def_readonly("branches_under_selection", &MEMESiteResult::branches_under_selection)
+        .def_readonly("total_branch_length", &MEMESiteResult::total_branch_length)
+        .def_readonly("log_l_meme", &MEMESiteResult::log_l_meme)
+        .def_readonly("log_l_fel", &MEMESiteResult::log_l_fel)
+        .def_readonly("p_value_meme_vs_fel", &MEMESiteResult::p_value_meme_vs_fel)
+        .def_readonly("fel_alpha", &MEMESiteResult::fel_alpha)
+        .def_readonly("fel_beta", &MEMESiteResult::fel_beta)
+        .def_readonly("beta_bg", &MEMESiteResult::beta_bg)
+        .def_readonly("branch_ebf", &MEMESiteResult::branch_ebf)
+        .def_readonly("evaluations", &MEMESiteResult::evaluations);
+    py::class_<MEMEAnalyzer>(m, "MEMEAnalyzer")
+        .def(py::init([](Tree tree, Alignment aln, const MG94Parameters& params, std::string branches) {
+                 return MEMEAnalyzer(std::move(tree), std::move(aln), params, std::move(branches));
+             }),
+             "tree"_a, "alignment"_a, "params"_a = MG94Parameters{}, "branches"_a = "All")
+        .def("run", [](MEMEAnalyzer& f, bool show_progress, bool force_progress) {
+                 py::gil_scoped_release rel;
+                 return f.run(show_progress, force_progress);
+             }, "show_progress"_a = false, "force_progress"_a = false)
+        .def_readwrite("p_value_threshold", &MEMEAnalyzer::p_value_threshold)
+        .def_readonly("conversion_factor", &MEMEAnalyzer::conversion_factor)
+        .def_readonly("baseline_tree_length", &MEMEAnalyzer::baseline_tree_length)
+        .def_readonly("site_results", &MEMEAnalyzer::site_results);
 }

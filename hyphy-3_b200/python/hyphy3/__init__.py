@@ -2,8 +2,9 @@
 
 Re-exports the core types and likelihood entry points of the reference
 package (python/hyphy3/__init__.py) from the device-backed _hyphy3 module.
-The analysis drivers (FEL, BUSTED, ... analyzers) are not part of this
-package; only the likelihood / gradient core is.
+Of the analysis drivers, FELAnalyzer and MEMEAnalyzer (every branch tested)
+and MG94Fitter run on the device; the others (BUSTED EM, aBSREL, RELAX, ...)
+are not part of this package.
 """
 import os
 import sys
@@ -19,6 +20,8 @@ from _hyphy3 import (  # noqa: E402
     FELSettings,
     FELSiteResult,
     FitResult,
+    MEMEAnalyzer,
+    MEMESiteResult,
     MG94Fitter,
     GeneticCode,
     MG94Parameters,

@@ -25,7 +25,7 @@ EXPORTED = [
     "h3g_ctx_create", "h3g_ctx_destroy", "h3g_last_error", "h3g_version", "h3g_problem_create",
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
-    "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run",
+    "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -48,6 +48,14 @@ class FelModel(C.Structure):
 class FelResult(C.Structure):
     _fields_ = [("alpha", C.c_double), ("beta", C.c_double), ("alpha_null", C.c_double), ("log_l_alt", C.c_double),
                 ("log_l_null", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double), ("evaluations", C.c_int)]
+
+
+class MemeResult(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("beta1", C.c_double), ("p1", C.c_double), ("beta_plus", C.c_double),
+                ("p_plus", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double),
+                ("branches_under_selection", C.c_int), ("total_branch_length", C.c_double),
+                ("log_l_meme", C.c_double), ("log_l_fel", C.c_double), ("p_value_meme_vs_fel", C.c_double),
+                ("fel_alpha", C.c_double), ("fel_beta", C.c_double), ("evaluations", C.c_int)]
 
 
 class Result(C.Structure):
@@ -88,6 +96,7 @@ def load() -> C.CDLL:
                                                 C.POINTER(C.c_int32), C.c_int, C.c_int, C.POINTER(C.c_int8),
                                                 C.POINTER(C.c_uint64), _dp, C.c_int, _dp, _dp, _dp, _dp]
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
+        lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         for name in EXPORTED:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         lib.h3g_version.restype = C.c_char_p
@@ -228,6 +237,23 @@ class Problem:
         self.ctx.check(self.ctx.lib.h3g_fel_run(self.h, C.byref(m), _ptr(bl), res))
         names = [f[0] for f in FelResult._fields_]
         return {k: np.array([getattr(res[i], k) for i in range(self.P)]) for k in names}
+
+    def meme_run(self, *, pi, Qs, Qn, branch_lengths, with_ebf: bool = True) -> dict:
+        """MEME per-pattern fits (h3g_meme_run); branch lengths in FEL time.  Returns arrays per pattern
+        and, with with_ebf, "branch_ebf" [n_patterns, n_nodes]."""
+        pi, Qs, Qn, bl = _f64(pi), _f64(Qs), _f64(Qn), _f64(branch_lengths)
+        S = int(pi.size)
+        if Qs.shape != (S, S) or Qn.shape != (S, S) or bl.size != self.n:
+            raise ValueError("Qs, Qn must be S x S and branch_lengths one per node")
+        m = FelModel(S=S, pi=_ptr(pi), Qs=_ptr(Qs), Qn=_ptr(Qn))
+        res = (MemeResult * max(self.P, 1))()
+        ebf = np.zeros((max(self.P, 1), self.n)) if with_ebf else None
+        self.ctx.check(self.ctx.lib.h3g_meme_run(self.h, C.byref(m), _ptr(bl), res, _ptr(ebf) if with_ebf else None))
+        names = [f[0] for f in MemeResult._fields_]
+        out = {k: np.array([getattr(res[i], k) for i in range(self.P)]) for k in names}
+        if with_ebf:
+            out["branch_ebf"] = ebf[: self.P]
+        return out
 
     def _result_struct(self, out):
         return Result(site_lnl=_ptr(out["site_lnl"]), grad_t=_ptr(out["grad_t"]), grad_dir=_ptr(out["grad_dir"]),

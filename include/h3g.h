@@ -215,6 +215,35 @@ typedef struct {
  * whole run moved between host and device. */
 h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths, h3g_fel_result* out);
 
+/* ---------------------------------------------------------------- MEME
+ * Mixed-effects model of episodic selection per site on the device, replacing
+ * MEMEAnalyzer::analyze_pattern / run (include/hyphy/analyses/meme.hpp:166-632,
+ * :634-676) for the case where every branch is tested.  Per pattern: the FEL
+ * fit above as the starting point; the alternative model (alpha, omega1, p1,
+ * beta+) by the bounded 4-D Nelder-Mead from the reference's start grid; when
+ * beta+ > alpha and p+ > 1e-6, the null model (beta+ = alpha) by a 3-D
+ * Nelder-Mead, a warm-started alternative refit when the null is better, the
+ * mixture LRT p-value 2/3 (0.45 erfc(sqrt(LRT/2)) + 0.55 exp(-LRT/2)) and the
+ * empirical Bayes factor of every branch.  A likelihood evaluation mixes the
+ * models of omega1 and beta+ / alpha with weights (p1, 1 - p1) at the
+ * transition-matrix level on every branch, time scaled by alpha. */
+typedef struct {
+    double alpha, beta1, p1, beta_plus, p_plus;   /* MEME MLE (beta1 = alpha omega1) */
+    double lrt, p_value;
+    int branches_under_selection;                 /* branches with EBF >= 100 */
+    double total_branch_length;
+    double log_l_meme, log_l_fel;
+    double p_value_meme_vs_fel;                   /* exp(-LRT(MEME vs FEL) / 2), 1 when MEME is not better */
+    double fel_alpha, fel_beta;
+    int evaluations;          /* likelihood evaluations of the MEME search (FEL excluded); 0 for an invariant pattern */
+} h3g_meme_result;
+
+/* Fit every pattern of prob; branch_lengths as for h3g_fel_run; out[n_patterns].
+ * branch_ebf, when not NULL, receives [n_patterns][n_nodes] empirical Bayes
+ * factors (1 for the root, for invariant patterns and where no EBF is computed). */
+h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths, h3g_meme_result* out,
+                        double* branch_ebf);
+
 #ifdef __cplusplus
 }
 #endif

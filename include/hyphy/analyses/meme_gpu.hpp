@@ -1,0 +1,128 @@
+// meme_gpu.hpp — drop-in MEMEAnalyzer (include/hyphy/analyses/meme.hpp) whose
+// per-site fits run on the device through h3g_meme_run.
+//
+// Same constructor and run() as the reference class: the constructor converts
+// branch lengths to the FEL time scale (t x 3 / mean rate of the base MG94
+// model, meme.hpp:150-164); run() fits every site pattern (the FEL baseline,
+// the 4-D alternative and 3-D null Nelder-Mead searches, LRT, empirical Bayes
+// factors; meme.hpp:166-632) and maps patterns back to sites
+// (meme.hpp:634-676).  Only the analysis where every branch is tested
+// ("All") is on the device; any other branch selection throws
+// std::runtime_error.  create_and_fit (nucleotide GTR fit first) and the
+// ancestral substitution summaries (MEMESiteResult::subs) are not provided.
+#pragma once
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fel_gpu.hpp"
+
+namespace hyphy::analyses {
+
+struct MEMESiteResult {
+    size_t site_index = 0;
+    Scalar alpha = 0.0;
+    Scalar beta1 = 0.0;
+    Scalar p1 = 1.0;
+    Scalar beta_plus = 0.0;
+    Scalar p_plus = 0.0;
+    Scalar lrt = 0.0;
+    Scalar p_value = 1.0;
+    int branches_under_selection = 0;
+    Scalar total_branch_length = 0.0;
+    Scalar log_l_meme = 0.0;
+    Scalar log_l_fel = 0.0;
+    Scalar p_value_meme_vs_fel = 1.0;
+    Scalar fel_alpha = 0.0;
+    Scalar fel_beta = 0.0;
+    Scalar beta_bg = 0.0;
+    std::vector<Scalar> branch_ebf;   // per node id, 1 for the root and where no EBF is computed
+    int evaluations = 0;              // likelihood evaluations of the MEME search (0: invariant)
+};
+
+class MEMEAnalyzer {
+public:
+    Tree tree;
+    Alignment aln;
+    MG94Parameters base_params;
+    FELAnalyzer fel_analyzer;
+    Scalar p_value_threshold = 0.1;
+    Scalar baseline_tree_length = 0.0;
+    Scalar conversion_factor = 1.0;
+    Scalar global_log_l = 0.0;
+    std::vector<MEMESiteResult> site_results;
+    std::string test_branches = "All";
+    size_t num_tested = 0;
+    size_t num_background = 0;
+
+    MEMEAnalyzer(Tree t, Alignment a, MG94Parameters params = MG94Parameters{}, std::string branches_spec = "All")
+        : tree(t), aln(std::move(a)), base_params(params), fel_analyzer(t, aln, params), test_branches(std::move(branches_spec)) {
+        if (test_branches != "All")
+            throw std::runtime_error("MEMEAnalyzer (device): only the all-branches-tested analysis is supported");
+        prepare_branch_lengths();
+        num_tested = tree.num_nodes() - 1;
+        num_background = 0;
+    }
+
+    // meme.hpp:150-164
+    void prepare_branch_lengths() {
+        const auto& code = aln.code ? *aln.code : *hyphy::core::GeneticCode::universal();
+        MG94Matrix base;
+        base.update(base_params, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        conversion_factor = base.scale_factor > 1e-12 ? 3.0 / base.scale_factor : 1.0;
+        baseline_tree_length = 0.0;
+        for (auto& node : tree.nodes) {
+            if (node.id == tree.root_id) continue;
+            baseline_tree_length += node.branch_length;
+            node.branch_length *= conversion_factor;
+        }
+    }
+
+    std::vector<MEMESiteResult> run(bool show_progress = false, bool force_progress = false) {
+        (void)show_progress; (void)force_progress;
+        auto& eng = hyphy::core::gpu_detail::Engine::get();
+        const auto l2t = hyphy::core::LikelihoodEngine::build_leaf_to_taxon_map(tree, aln);
+        h3g_problem* pr = eng.problem(tree, aln, l2t);
+        const auto& code = aln.code ? *aln.code : *hyphy::core::GeneticCode::universal();
+        const int S = code.num_sense_codons;
+        MG94Parameters ps = base_params, pn = base_params;
+        ps.alpha = 1.0; ps.beta = 0.0;
+        pn.alpha = 0.0; pn.beta = 1.0;
+        MG94Matrix ms, mn;
+        ms.update(ps, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        mn.update(pn, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        const size_t nS = static_cast<size_t>(S), n = tree.num_nodes();
+        std::vector<double> pi(nS), qs(nS * nS), qn(nS * nS), bl(n, 0.0);
+        for (int i = 0; i < S; ++i) {
+            pi[size_t(i)] = aln.codon_frequencies_f3x4[size_t(i)];
+            for (int j = 0; j < S; ++j) {
+                qs[size_t(i) * S + j] = i == j ? 0.0 : ms.Q(i, j);
+                qn[size_t(i) * S + j] = i == j ? 0.0 : mn.Q(i, j);
+            }
+        }
+        for (const auto& node : tree.nodes)
+            if (node.id != tree.root_id) bl[size_t(node.id)] = node.branch_length;
+        h3g_fel_model m{S, pi.data(), qs.data(), qn.data()};
+        std::vector<h3g_meme_result> res(aln.patterns.size());
+        std::vector<double> ebf(aln.patterns.size() * n, 1.0);
+        eng.check(h3g_meme_run(pr, &m, bl.data(), res.data(), ebf.data()));
+        site_results.assign(aln.num_codons, MEMESiteResult{});
+        for (size_t s = 0; s < aln.num_codons; ++s) {
+            const size_t p = aln.site_to_pattern[s];
+            const auto& r = res[p];
+            MEMESiteResult& o = site_results[s];
+            o.site_index = s;
+            o.alpha = r.alpha; o.beta1 = r.beta1; o.p1 = r.p1; o.beta_plus = r.beta_plus; o.p_plus = r.p_plus;
+            o.lrt = r.lrt; o.p_value = r.p_value; o.branches_under_selection = r.branches_under_selection;
+            o.total_branch_length = r.total_branch_length;
+            o.log_l_meme = r.log_l_meme; o.log_l_fel = r.log_l_fel; o.p_value_meme_vs_fel = r.p_value_meme_vs_fel;
+            o.fel_alpha = r.fel_alpha; o.fel_beta = r.fel_beta;
+            o.branch_ebf.assign(ebf.begin() + std::ptrdiff_t(p * n), ebf.begin() + std::ptrdiff_t((p + 1) * n));
+            o.evaluations = r.evaluations;
+        }
+        return site_results;
+    }
+};
+
+}  // namespace hyphy::analyses

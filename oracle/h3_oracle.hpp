@@ -21,6 +21,7 @@
 #include <cstdint>
 #include <fstream>
 #include <limits>
+#include <list>
 #include <map>
 #include <sstream>
 #include <stdexcept>
@@ -1182,6 +1183,246 @@ inline FelRun fel_run(const Tree& tr, const Alignment& a, const Params& base, in
     run.patterns.assign(P, FelSite{});
     #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(P))
     for (int p = 0; p < P; ++p) run.patterns[p] = fel_pattern(tr, a, l2t, base, run, p);
+    return run;
+}
+
+// ------------------------------------------------------------------ MEME
+// Mixed-effects model of episodic selection per site (analyses/meme.hpp:166-632,
+// every branch tested), restated with the N-dimensional Nelder-Mead it uses
+// (opt/nelder_mead.hpp:209-357).
+
+template <int D>
+struct NMPointN { std::array<double, D> x{}; double f = 0.0; };
+
+// opt/nelder_mead.hpp:209-357 — bounded Nelder-Mead: the best of init and the grid
+// starts a simplex of D perturbed vertices; reflection 1, expansion 2,
+// contraction 0.5, shrink 0.5; converged when both the f-spread and the
+// coordinate spread of best vs worst vertex are below tol.
+template <int D, class F>
+inline NMPointN<D> nelder_mead_nd(F&& f, const std::array<double, D>& init, const std::array<double, D>& lb,
+                                  const std::array<double, D>& ub, double tol, int max_iter,
+                                  const std::vector<std::array<double, D>>& grid) {
+    using Pt = NMPointN<D>;
+    auto eval = [&](const std::array<double, D>& v) {
+        Pt q;
+        for (int d = 0; d < D; ++d) q.x[d] = std::clamp(v[d], lb[d], ub[d]);
+        q.f = f(q.x);
+        return q;
+    };
+    Pt best = eval(init);
+    for (const auto& g : grid) { Pt q = eval(g); if (q.f < best.f) best = q; }
+    std::array<Pt, D + 1> s;
+    s[0] = best;
+    for (int d = 0; d < D; ++d) {
+        std::array<double, D> x = best.x;
+        const double step = std::max(0.05, 0.2 * std::fabs(best.x[d]));
+        if (best.x[d] + step <= ub[d]) x[d] += step; else x[d] -= step;
+        s[d + 1] = eval(x);
+    }
+    auto by_f = [](const Pt& a, const Pt& b) { return a.f < b.f; };
+    for (int iter = 0; iter < max_iter; ++iter) {
+        std::sort(s.begin(), s.end(), by_f);
+        double dx = 0.0;
+        for (int d = 0; d < D; ++d) dx = std::max(dx, std::fabs(s[D].x[d] - s[0].x[d]));
+        if (std::fabs(s[D].f - s[0].f) < tol && dx < tol) break;
+        std::array<double, D> c{};
+        for (int i = 0; i < D; ++i) for (int d = 0; d < D; ++d) c[d] += s[i].x[d];
+        for (int d = 0; d < D; ++d) c[d] /= double(D);
+        std::array<double, D> xr;
+        for (int d = 0; d < D; ++d) xr[d] = c[d] + 1.0 * (c[d] - s[D].x[d]);
+        const Pt r = eval(xr);
+        if (r.f < s[0].f) {
+            std::array<double, D> xe;
+            for (int d = 0; d < D; ++d) xe[d] = c[d] + 2.0 * (r.x[d] - c[d]);
+            const Pt e = eval(xe);
+            s[D] = (e.f < r.f) ? e : r;
+        } else if (r.f < s[D - 1].f) {
+            s[D] = r;
+        } else {
+            const bool outside = r.f < s[D].f;
+            std::array<double, D> xc;
+            for (int d = 0; d < D; ++d) xc[d] = c[d] + 0.5 * ((outside ? r.x[d] : s[D].x[d]) - c[d]);
+            const Pt cc = eval(xc);
+            if (cc.f < (outside ? r.f : s[D].f)) {
+                s[D] = cc;
+            } else {
+                for (int i = 1; i <= D; ++i) {
+                    std::array<double, D> xs;
+                    for (int d = 0; d < D; ++d) xs[d] = s[0].x[d] + 0.5 * (s[i].x[d] - s[0].x[d]);
+                    s[i] = eval(xs);
+                }
+            }
+        }
+    }
+    std::sort(s.begin(), s.end(), by_f);
+    return s[0];
+}
+
+struct MemeSite {
+    double alpha = 0, beta1 = 0, p1 = 1, beta_plus = 0, p_plus = 0, lrt = 0, p_value = 1;
+    int bus = 0;                      // branches with EBF >= 100
+    double total_bl = 0, lnl_meme = 0, lnl_fel = 0, p_vs_fel = 1, fel_alpha = 0, fel_beta = 0;
+    int evals = 0;
+    std::vector<double> ebf;          // per node, 1 where not computed
+};
+struct MemeRun {
+    FelRun fel;                       // conversion, FEL-time branch lengths, the FEL fit of every pattern
+    double mu_s = 0, mu_n = 0;        // scale factor = alpha mu_s + beta mu_n
+    std::vector<MemeSite> patterns;
+};
+
+// meme.hpp:166-632 with num_background == 0
+inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
+                             const MemeRun& run, int p) {
+    MemeSite res;
+    const int S = a.code.S, n = tr.n();
+    res.ebf.assign(n, 1.0);
+    const FelSite& fel = run.fel.patterns[p];
+    res.fel_alpha = fel.alpha; res.fel_beta = fel.beta; res.lnl_fel = fel.lnl_alt;
+    int first = -1; bool invariant = true;
+    for (int t = 0; t < a.T; ++t) {
+        const int st = a.states[size_t(p) * a.T + t];
+        if (st >= 0) { if (first == -1) first = st; else if (st != first) { invariant = false; break; } }
+    }
+    if (invariant) { res.lnl_fel = 0.0; return res; }
+    // eigensystems of Q(omega) = Qs + omega Qn, reused when omega repeats exactly
+    // (least recently used at the front; a hit moves to the back, so the model
+    // returned by the previous call is never the one evicted)
+    std::list<std::pair<double, MG94>> cache;
+    auto model = [&](double om) -> const MG94& {
+        for (auto it = cache.begin(); it != cache.end(); ++it)
+            if (it->first == om) { cache.splice(cache.end(), cache, it); return cache.back().second; }
+        if (cache.size() >= 8) cache.pop_front();
+        Params q = base; q.alpha = 1.0; q.beta = om;
+        cache.emplace_back(om, MG94{});
+        cache.back().second.update(q, a.pos_freq, a.pi, a.code);
+        return cache.back().second;
+    };
+    std::vector<Mat> P1(n, Mat::eye(S)), Pp(n, Mat::eye(S)), Pm(n, Mat::eye(S));
+    Pass w;
+    auto build = [&](double al, double w1, double p1, double bp) {
+        const double ap = std::max(al, 1e-12);
+        const MG94& m1 = model(w1);
+        const MG94& mp = model(bp / ap);
+        for (int i = 0; i < n; ++i) {
+            if (i == tr.root) continue;
+            P1[i] = m1.P(ap * run.fel.bl[i]);
+            Pp[i] = mp.P(ap * run.fel.bl[i]);
+            for (size_t e = 0; e < Pm[i].a.size(); ++e) Pm[i].a[e] = p1 * P1[i].a[e] + (1.0 - p1) * Pp[i].a[e];
+        }
+    };
+    const std::vector<double>& pi = a.pi;
+    auto lnl = [&](double al, double w1, double p1, double bp) {
+        ++res.evals;
+        build(al, w1, p1, bp);
+        inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
+        return w.logL;
+    };
+    using A4 = std::array<double, 4>;
+    using A3 = std::array<double, 3>;
+    // start grid (meme.hpp:282-312)
+    const double af = std::clamp(fel.alpha, 1e-4, 10000.0), bf = std::clamp(fel.beta, 1e-4, 100000.0);
+    const double w10 = std::clamp(bf / std::max(af, 1e-4), 0.0, 1.0);
+    std::vector<A4> grid;
+    if (af >= bf) {
+        grid = {{af, w10, 0.75, bf}, {af, 0.0, 0.75, bf}, {af, 0.0, 0.95, af * 0.5}, {af, 0.25, 0.85, af * 0.9}};
+        const double bp1 = std::max(af * 1.5, bf * 2.0), bp2 = std::max(af * 2.5, bf * 4.0), bp3 = std::max(af * 4.0, bf * 8.0);
+        for (double pp : {0.05, 0.10, 0.20}) {
+            grid.push_back({af, w10, 1.0 - pp, bp1});
+            grid.push_back({af, w10, 1.0 - pp, bp2});
+            grid.push_back({af, w10, 1.0 - pp, bp3});
+        }
+    } else {
+        grid = {{af, w10, 0.75, bf}, {af, 0.0, 0.75, bf}, {af, 0.25, 0.50, bf * 2.0}, {af, 0.25, 0.75, bf * 5.0},
+                {af, 0.10, 0.90, bf * 15.0}, {af, 0.00, 0.95, bf * 30.0}, {af, 1.00, 0.01, std::max(bf, af * 1.5)}};
+    }
+    const A4 lb4 = {1e-4, 0.0, 1e-6, 1e-4}, ub4 = {10000.0, 1.0, 1.0 - 1e-6, 100000.0};
+    auto obj4 = [&](const A4& x) { return -lnl(x[0], x[1], x[2], x[3]); };
+    // alternative model (meme.hpp:340-354)
+    const auto alt = nelder_mead_nd<4>(obj4, grid[0], lb4, ub4, 1e-5, 800, grid);
+    double omega1 = alt.x[1];
+    res.alpha = alt.x[0]; res.p1 = alt.x[2]; res.beta_plus = alt.x[3];
+    res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1; res.lnl_meme = -alt.f;
+    if (res.beta_plus > res.alpha && res.p_plus > 1e-6) {
+        // null model beta+ = alpha (meme.hpp:404-452)
+        const double an = std::clamp(fel.alpha_null, 1e-4, 50.0);
+        std::vector<A3> ng = {{res.alpha, omega1, res.p1}, {an, 1.0, 0.5}, {an, omega1, res.p1},
+                              {std::clamp(res.alpha, 1e-4, 50.0), 1.0, 0.5}};
+        for (double c : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0, 20.0}) { ng.push_back({c, 0.5, 0.5}); ng.push_back({c, 0.0, 0.9}); }
+        const A3 lb3 = {1e-4, 0.0, 1e-6}, ub3 = {10000.0, 1.0, 1.0 - 1e-6};
+        const auto nul = nelder_mead_nd<3>([&](const A3& x) { return -lnl(x[0], x[1], x[2], x[0]); }, ng[0], lb3, ub3,
+                                           1e-5, 800, ng);
+        const double lnl_null = -nul.f, a_null = nul.x[0], w_null = nul.x[1], p_null = nul.x[2];
+        if (lnl_null > res.lnl_meme && std::isfinite(lnl_null)) {
+            // warm-started alternative (meme.hpp:436-452)
+            const std::vector<A4> wg = {{a_null, w_null, p_null, a_null}, {a_null, w_null, 0.99, a_null}};
+            const auto alt2 = nelder_mead_nd<4>(obj4, wg[0], lb4, ub4, 1e-5, 800, wg);
+            if (-alt2.f > res.lnl_meme) {
+                res.alpha = alt2.x[0]; omega1 = alt2.x[1]; res.p1 = alt2.x[2]; res.beta_plus = alt2.x[3];
+                res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1; res.lnl_meme = -alt2.f;
+            }
+        }
+        // meme.hpp:456-482
+        if (lnl_null <= -1e10 || res.lnl_meme <= -1e10 || !std::isfinite(lnl_null) || !std::isfinite(res.lnl_meme)) {
+            res.lrt = 0.0; res.p_value = 1.0;
+        } else if (lnl_null > res.lnl_meme) {
+            res.alpha = a_null; res.beta1 = a_null * w_null; res.p1 = p_null; res.beta_plus = a_null;
+            res.p_plus = 1.0 - p_null; res.lnl_meme = lnl_null; omega1 = w_null;
+            res.lrt = 0.0; res.p_value = 2.0 / 3.0;
+        } else if (std::fabs(res.lnl_meme - lnl_null) <= 1e-12) {
+            res.lrt = 0.0; res.p_value = 2.0 / 3.0;
+        } else {
+            res.lrt = 2.0 * (res.lnl_meme - lnl_null);
+            res.p_value = (2.0 / 3.0) * (0.45 * std::erfc(std::sqrt(res.lrt / 2.0)) + 0.55 * std::exp(-res.lrt / 2.0));
+        }
+        // empirical Bayes factors: every branch alone in class + vs class 1 (meme.hpp:484-588)
+        build(res.alpha, omega1, res.p1, res.beta_plus);
+        for (int b = 0; b < n; ++b) {
+            if (b == tr.root) continue;
+            const Mat keep = Pm[b];
+            Pm[b] = P1[b];
+            inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
+            const double l1 = w.logL;
+            Pm[b] = Pp[b];
+            inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
+            const double lp = w.logL;
+            Pm[b] = keep;
+            double e = 1.0;
+            if (l1 > -1e10 && lp > -1e10) e = std::exp(std::clamp(lp - l1, -50.0, 50.0));
+            else if (l1 <= -1e10 && lp > -1e10) e = 1e6;
+            else e = 0.0;
+            res.ebf[b] = e;
+            if (e >= 100.0) ++res.bus;
+        }
+    } else {
+        res.lrt = 0.0; res.p_value = 2.0 / 3.0;
+    }
+    // meme.hpp:590-619
+    const double d_fel = 2.0 * (res.lnl_meme - res.lnl_fel);
+    res.p_vs_fel = d_fel > 0.0 ? std::exp(-d_fel / 2.0) : 1.0;
+    const double rate = (res.p1 * (res.alpha * run.mu_s + res.beta1 * run.mu_n) +
+                         res.p_plus * (res.alpha * run.mu_s + res.beta_plus * run.mu_n)) / 3.0;
+    double tbl = 0.0;
+    for (int b = 0; b < n; ++b) if (b != tr.root) tbl += run.fel.bl[b] * rate;
+    res.total_bl = tbl;
+    return res;
+}
+
+// meme.hpp:150-164, :620-660 (run): FEL baseline then MEME for every pattern, in parallel
+inline MemeRun meme_run(const Tree& tr, const Alignment& a, const Params& base, int max_patterns = -1) {
+    MemeRun run;
+    run.fel = fel_run(tr, a, base, max_patterns);
+    Params ps = base; ps.alpha = 1.0; ps.beta = 0.0;
+    Params pn = base; pn.alpha = 0.0; pn.beta = 1.0;
+    MG94 ms, mn;
+    ms.update(ps, a.pos_freq, a.pi, a.code);
+    mn.update(pn, a.pos_freq, a.pi, a.code);
+    run.mu_s = ms.mu; run.mu_n = mn.mu;
+    const auto l2t = leaf_map(tr, a);
+    const int P = int(run.fel.patterns.size());
+    run.patterns.assign(P, MemeSite{});
+    #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(P))
+    for (int p = 0; p < P; ++p) run.patterns[p] = meme_pattern(tr, a, l2t, base, run, p);
     return run;
 }
 

@@ -181,6 +181,39 @@ PYBIND11_MODULE(h3oracle, m) {
         d["branch_lengths"] = r.bl;
         return d;
     }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("max_patterns") = -1);
+    m.def("meme_run", [](const Tree& t, const Alignment& a, const py::dict& p, int max_patterns) {
+        const Params pp = params_from(p);
+        MemeRun r;
+        { py::gil_scoped_release rel; r = meme_run(t, a, pp, max_patterns); }
+        const size_t P = r.patterns.size();
+        py::dict d;
+        auto col = [&](auto get) { py::array_t<double> x(P); for (size_t i = 0; i < P; ++i) x.mutable_data()[i] = get(r.patterns[i]); return x; };
+        d["alpha"] = col([](const MemeSite& s) { return s.alpha; });
+        d["beta1"] = col([](const MemeSite& s) { return s.beta1; });
+        d["p1"] = col([](const MemeSite& s) { return s.p1; });
+        d["beta_plus"] = col([](const MemeSite& s) { return s.beta_plus; });
+        d["p_plus"] = col([](const MemeSite& s) { return s.p_plus; });
+        d["lrt"] = col([](const MemeSite& s) { return s.lrt; });
+        d["p_value"] = col([](const MemeSite& s) { return s.p_value; });
+        d["branches_under_selection"] = col([](const MemeSite& s) { return double(s.bus); });
+        d["total_branch_length"] = col([](const MemeSite& s) { return s.total_bl; });
+        d["log_l_meme"] = col([](const MemeSite& s) { return s.lnl_meme; });
+        d["log_l_fel"] = col([](const MemeSite& s) { return s.lnl_fel; });
+        d["p_value_meme_vs_fel"] = col([](const MemeSite& s) { return s.p_vs_fel; });
+        d["fel_alpha"] = col([](const MemeSite& s) { return s.fel_alpha; });
+        d["fel_beta"] = col([](const MemeSite& s) { return s.fel_beta; });
+        d["evals"] = col([](const MemeSite& s) { return double(s.evals); });
+        const size_t n = size_t(t.n());
+        py::array_t<double> ebf({P, n});
+        for (size_t i = 0; i < P; ++i)
+            for (size_t b = 0; b < n; ++b) ebf.mutable_data()[i * n + b] = r.patterns[i].ebf[b];
+        d["branch_ebf"] = ebf;
+        d["conversion"] = r.fel.conversion;
+        d["branch_lengths"] = r.fel.bl;
+        d["mu_s"] = r.mu_s;
+        d["mu_n"] = r.mu_n;
+        return d;
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("max_patterns") = -1);
     m.def("set_threads", [](int n) {
 #ifdef _OPENMP
         omp_set_num_threads(n);

@@ -10,6 +10,7 @@ Run from the repository root with the reference checked out read-only:
 """
 import json
 import pathlib
+import re
 import shutil
 import sys
 
@@ -79,7 +80,34 @@ def main(ref: str) -> None:
         # tests/test_fel_cd2_parity.cpp:113-116
         "min_pearson_lrt": 0.998, "min_spearman_lrt": 0.995, "min_pearson_p": 0.993, "min_spearman_p": 0.995,
     }
+    # HyPhy 2.5 MEME per-site tables (CD2, ADH) with the global MG94xREV fit they were computed on: the tree with
+    # that fit's branch lengths, omega and the GTR exchangeabilities.  Thresholds: tests/test_meme.cpp:66-150.
+    known["cd2_meme"] = meme_case(ref_root, "cd2_meme_rel.json", "tests/test_meme.cpp:66-104", 0.95, 0.95, 0.95, 0.95)
+    known["adh_meme"] = meme_case(ref_root, "adh_meme_rel.json", "tests/test_meme.cpp:106-144", 0.95, 0.92, 0.95, 0.95)
     (out / "known_answers.json").write_text(json.dumps(known, indent=1) + "\n")
+
+
+def labelled_newick(topology: str, lengths: dict) -> str:
+    """Attach ':length' to every named node of a HyPhy tree string (names only, no lengths)."""
+    return re.sub(r"([A-Za-z_][A-Za-z0-9_]*)", lambda m: f"{m.group(1)}:{lengths[m.group(1)]!r}", topology) + ";"
+
+
+def meme_case(ref_root: pathlib.Path, name: str, test_ref: str, r_lrt, rho_lrt, r_p, rho_p) -> dict:
+    g = json.loads((ref_root / "benchmarks/ground_truth" / name).read_text())
+    fit = g["fits"]["Global MG94xREV"]
+    gtr = g["fits"]["Nucleotide GTR"]["Rate Distributions"]
+    rate = lambda a, b: gtr[f"Substitution rate from nucleotide {a} to nucleotide {b}"]
+    lengths = {k: v["Global MG94xREV"] for k, v in g["branch attributes"]["0"].items()}
+    return {
+        "source": f"benchmarks/ground_truth/{name} (HyPhy 2.5); compared in {test_ref}",
+        "headers": [h[0] for h in g["MLE"]["headers"]],
+        "mle": g["MLE"]["content"]["0"],
+        "newick": labelled_newick(g["input"]["trees"]["0"], lengths),
+        "params": {"alpha": 1.0, "beta": fit["Rate Distributions"]["non-synonymous/synonymous rate ratio for *test*"][0][0],
+                   "theta": [rate("A", "C"), rate("A", "T"), rate("C", "G"), rate("C", "T"), rate("G", "T")]},
+        "global_log_l": fit["Log Likelihood"],
+        "min_pearson_lrt": r_lrt, "min_spearman_lrt": rho_lrt, "min_pearson_p": r_p, "min_spearman_p": rho_p,
+    }
 
 
 if __name__ == "__main__":

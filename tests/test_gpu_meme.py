@@ -1,0 +1,164 @@
+"""MEME per-site fits on the device against the oracle's restatement of the reference (meme.hpp:166-632).
+
+Both run the reference's searches (FEL baseline, 4-D and 3-D bounded
+Nelder-Mead from the same start grids) pattern by pattern.  The device
+evaluates every likelihood by spectral pruning with its own eigensolver, so
+the two agree to rounding on every evaluation; MEME's mixture likelihood is
+multi-modal, so where a rounding-level difference changes one comparison in a
+simplex search the two may settle in different optima.  The runs are held to
+the reference's own acceptance against HyPhy 2.5 (tests/test_meme.cpp) and to
+close agreement with the oracle on most patterns.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from gpu_helpers import problem_from_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from hyphy3 import _capi
+    c = _capi.Context(0)
+    yield c
+    c.close()
+
+
+def _inputs(oracle, aln, params):
+    base = dict(params)
+    qs = oracle.mg94(aln, {**base, "alpha": 1.0, "beta": 0.0})["Q"]
+    qn = oracle.mg94(aln, {**base, "alpha": 0.0, "beta": 1.0})["Q"]
+    np.fill_diagonal(qs, 0.0)
+    np.fill_diagonal(qn, 0.0)
+    return np.asarray(aln.pi), qs, qn
+
+
+def _ranks(v):
+    order = np.argsort(v, kind="stable")
+    r = np.empty(len(v))
+    i = 0
+    while i < len(v):
+        j = i + 1
+        while j < len(v) and abs(v[order[j]] - v[order[i]]) < 1e-12:
+            j += 1
+        r[order[i:j]] = 0.5 * (i + j - 1) + 1.0
+        i = j
+    return r
+
+
+def _hyphy_acceptance(k, lrt, pv):
+    mle = np.array(k["mle"])
+    assert np.corrcoef(lrt, mle[:, 5])[0, 1] >= k["min_pearson_lrt"]
+    assert np.corrcoef(_ranks(lrt), _ranks(mle[:, 5]))[0, 1] >= k["min_spearman_lrt"]
+    assert np.corrcoef(pv, mle[:, 6])[0, 1] >= k["min_pearson_p"]
+    assert np.corrcoef(_ranks(pv), _ranks(mle[:, 6]))[0, 1] >= k["min_spearman_p"]
+
+
+def _case(oracle, golden_dir, name, fasta):
+    k = json.loads((golden_dir / "known_answers.json").read_text())[name]
+    a = oracle.Alignment.load(str(golden_dir / fasta))
+    t = oracle.Tree.parse(k["newick"])
+    return k, a, t
+
+
+@pytest.fixture(scope="module")
+def cd2(ctx, oracle, golden_dir):
+    k, a, t = _case(oracle, golden_dir, "cd2_meme", "cd2.fna")
+    ref = oracle.meme_run(t, a, k["params"])
+    pi, qs, qn = _inputs(oracle, a, k["params"])
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    dev = pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=ref["branch_lengths"])
+    return k, a, t, ref, dev
+
+
+def test_meme_cd2_matches_oracle(cd2):
+    _, _, _, ref, dev = cd2
+    inv = np.asarray(ref["evals"]) == 0
+    assert np.array_equal(dev["evaluations"] == 0, inv)
+    assert np.all(dev["p_value"][inv] == 1.0) and np.all(dev["lrt"][inv] == 0.0)
+    # the FEL baseline: same searches, same optima
+    np.testing.assert_allclose(dev["log_l_fel"], ref["log_l_fel"], rtol=0, atol=1e-4)
+    # MEME: the same optimum on most patterns, never a worse one by more than the search tolerance on many
+    d = np.abs(dev["log_l_meme"] - np.asarray(ref["log_l_meme"]))
+    assert np.mean(d[~inv] <= 1e-3) > 0.9
+    same = (~inv) & (d <= 1e-4)
+    np.testing.assert_allclose(dev["lrt"][same], np.asarray(ref["lrt"])[same], rtol=0, atol=5e-3)
+    assert np.corrcoef(dev["lrt"][~inv], np.asarray(ref["lrt"])[~inv])[0, 1] > 0.99
+    np.testing.assert_allclose(dev["p1"] + dev["p_plus"], 1.0, atol=1e-15)
+    assert np.all((dev["p_value"] >= 0) & (dev["p_value"] <= 1))
+
+
+def test_meme_cd2_ebf_matches_oracle(cd2):
+    _, _, t, ref, dev = cd2
+    e_d, e_r = dev["branch_ebf"], np.asarray(ref["branch_ebf"])
+    assert np.all(e_d[:, t.root] == 1.0) and np.all(e_d >= 0)
+    np.testing.assert_array_equal((e_d >= 100).sum(axis=1), dev["branches_under_selection"])
+    # where both runs report the same MLE the per-branch factors agree (inside-outside on the
+    # device vs two re-prunings per branch in the oracle)
+    close = (np.abs(dev["alpha"] - np.asarray(ref["alpha"])) <= 1e-6 * np.maximum(1.0, dev["alpha"])) & \
+            (np.abs(dev["beta_plus"] - np.asarray(ref["beta_plus"])) <= 1e-6 * np.maximum(1.0, dev["beta_plus"])) & \
+            (np.abs(dev["p1"] - np.asarray(ref["p1"])) <= 1e-6) & (np.asarray(ref["evals"]) > 0)
+    tested = close & (dev["lrt"] > 0)
+    assert tested.sum() >= 5
+    np.testing.assert_allclose(np.log(np.maximum(e_d[tested], 1e-300)), np.log(np.maximum(e_r[tested], 1e-300)),
+                               rtol=0, atol=1e-3)
+    assert np.mean(dev["branches_under_selection"] == np.asarray(ref["branches_under_selection"])) > 0.9
+
+
+def test_meme_cd2_meets_reference_acceptance(cd2):
+    k, a, _, _, dev = cd2
+    sp = np.array(a.site_pattern)
+    _hyphy_acceptance(k, dev["lrt"][sp], dev["p_value"][sp])
+
+
+def test_meme_adh_meets_reference_acceptance(ctx, oracle, golden_dir):
+    """tests/test_meme.cpp:106-144 (ADH, 23 taxa, 254 codons) against HyPhy 2.5, device only."""
+    k, a, t = _case(oracle, golden_dir, "adh_meme", "adh.nex")
+    fel = oracle.fel_run(t, a, k["params"], 0)          # conversion and FEL-time lengths only
+    pi, qs, qn = _inputs(oracle, a, k["params"])
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    dev = pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=fel["branch_lengths"], with_ebf=False)
+    sp = np.array(a.site_pattern)
+    assert len(sp) == 254
+    _hyphy_acceptance(k, dev["lrt"][sp], dev["p_value"][sp])
+
+
+def test_meme_rejects_bad_arguments(ctx, oracle, golden_dir):
+    from hyphy3 import _capi
+    a = oracle.Alignment.load(str(golden_dir / "cd2_reduced.fna"))
+    t = oracle.Tree.parse((golden_dir / "cd2_reduced.nwk").read_text())
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    pi, qs, qn = _inputs(oracle, a, {"alpha": 1.0, "beta": 0.5, "theta": [1, 1, 1, 2, 1]})
+    bl = np.array(t.branch_lengths)
+    bad = bl.copy()
+    bad[1] = -1.0
+    with pytest.raises(_capi.H3GError):
+        pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bad)
+    badpi = pi.copy()
+    badpi[0] = np.inf
+    with pytest.raises(_capi.H3GError):
+        pr.meme_run(pi=badpi, Qs=qs, Qn=qn, branch_lengths=bl)
+    out = pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)
+    assert np.all(out["lrt"] >= 0) and np.all((out["p_value"] >= 0) & (out["p_value"] <= 1))
+
+
+def test_meme_analyzer_api(oracle, golden_dir):
+    """hyphy3.MEMEAnalyzer(tree, aln, params).run() on the reference's CD2 case, site by site."""
+    import _hyphy3 as h3
+    k = json.loads((golden_dir / "known_answers.json").read_text())["cd2_meme"]
+    a = h3.Alignment.load(str(golden_dir / "cd2.fna"))
+    t = h3.Tree.from_newick(k["newick"])
+    p = h3.MG94Parameters()
+    p.alpha, p.beta = k["params"]["alpha"], k["params"]["beta"]
+    p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = k["params"]["theta"]
+    res = h3.MEMEAnalyzer(t, a, p).run()
+    assert len(res) == 187
+    lrt = np.array([r.lrt for r in res])
+    pv = np.array([r.p_value for r in res])
+    _hyphy_acceptance(k, lrt, pv)
+    assert all(len(r.branch_ebf) == t.num_nodes() for r in res)
+    with pytest.raises(RuntimeError):
+        h3.MEMEAnalyzer(t, a, p, "Internal")
