@@ -344,9 +344,11 @@ void fel_set_error(h3g_problem* pr, const std::string& msg) {
     if (pr && pr->ctx) pr->ctx->err = msg;
 }
 
-void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h) {
+void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h, int launches, double ms) {
     pr->last_h2d = h2d;
     pr->last_d2h = d2h;
+    pr->last_launches = launches;
+    pr->last_ms = float(ms);
 }
 
 }  // namespace h3g

@@ -240,7 +240,6 @@ struct Spectral {
 };
 
 constexpr size_t spectral_doubles(int nc) { return size_t(nc) * (2 * SP * LD + 6 * SP); }
-constexpr size_t lnl_smem(int nc) { return (spectral_doubles(nc) + SP) * sizeof(double); }
 constexpr size_t kEbfSmem = (spectral_doubles(2) + 3 * SP) * sizeof(double);
 
 // carve shared memory and stage request r's eigensystems; returns the first free double
@@ -389,25 +388,184 @@ __device__ void prune(const Spectral<NC>& sp, double* sL, const Topo& t, const d
     __syncthreads();
 }
 
-// grid n_req, block 256: log-likelihood of each request, or the reference's -1e20 for L <= 0
+// Level-synchronous pruning, one warp per node: the log-likelihood of each
+// request, or the reference's -1e20 for L <= 0.  Nodes are grouped by height
+// (leaves first, the root last); the nodes of one level are independent, so
+// the warps of a CTA take them in parallel and the chain of dependent steps
+// is the tree's height instead of its node count.  Lane l owns states l and
+// l + 32.  A node's message sum_c w_c U_c (e_c o (V_c D)) goes to the CTA's
+// workspace row; its partial D is the product of its children's rows,
+// rescaled by 2^256 whenever its maximum falls below 2^-256 (exponents summed
+// over the tree).  Persistent: CTA b evaluates requests b, b + grid, ...
+struct LevelPlan {
+    int H;                    // levels: 0 = leaves ... H - 1 = the root alone
+    const int* off;           // [H + 1]
+    const int* nodes;         // [n] nodes ordered by level
+};
+
+constexpr int kLvT = 512;
+constexpr int kLvW = kLvT / 32;
+
+constexpr size_t lv_smem(int nc) {
+    return (size_t(nc) * (2 * SP * LD + SP) + size_t(kLvW) * (nc + 1) * SP) * sizeof(double);
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 template <int NC>
-__global__ void __launch_bounds__(kFT) k_fel_lnl(FelModel f, Topo t, const double* __restrict__ bl, const int* __restrict__ ev,
-                                                 int n_ev, int depth, double* __restrict__ stack, FelReqs q,
-                                                 double* __restrict__ out) {
+__global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const double* __restrict__ bl, LevelPlan lp,
+                                                   double* __restrict__ work, FelReqs q, int n_req, double* __restrict__ out) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    __shared__ int sexp[kMaxDepth];
-    __shared__ double red[kFT / 32];
-    const int tid = threadIdx.x, S = t.S, r = blockIdx.x;
-    Spectral<NC> sp;
-    double* sL = spectral_setup<NC>(sp, sm, f, q, r);
-    double* stk = stack + size_t(r) * depth * SP;
-    __syncthreads();
-    prune<NC, false>(sp, sL, t, bl, ev, n_ev, stk, sexp, red, q.pattern[r], nullptr);
-    double v = 0.0;
-    if (tid < S) v = f.pi[tid] * stk[tid];
-    const double L = block_sum_or_max(v, red, false);
-    if (tid == 0) out[r] = L > 0.0 ? log(L) - double(sexp[0]) * 0.69314718055994530942 : -1e20;
+    __shared__ int sE;
+    __shared__ double sL;
+    double* U[NC];
+    double* V[NC];
+    double* lam[NC];
+    double* z = sm;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        U[c] = z; z += SP * LD;
+        V[c] = z; z += SP * LD;
+        lam[c] = z; z += SP;
+    }
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, S = t.S;
+    double* dv = z + size_t(warp) * (NC + 1) * SP;        // this warp's partial
+    double* xv = dv + SP;                                  // [NC][64] spectral coordinates
+    double* msg = work + size_t(blockIdx.x) * t.n * SP;
+    const int s0 = lane, s1 = lane + 32;
+    for (int r = blockIdx.x; r < n_req; r += gridDim.x) {
+        int sl[NC];
+        double w[NC];
+        sl[0] = q.slot[r];
+        if constexpr (NC == 2) {
+            sl[1] = q.slot2[r];
+            w[0] = q.w1[r];
+            w[1] = 1.0 - q.w1[r];
+        } else {
+            w[0] = 1.0;
+        }
+        const double a = q.a[r];
+        const int p = q.pattern[r];
+        __syncthreads();                                   // the previous request is done with shared memory
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const double* gU = f.U + size_t(sl[c]) * SP2;
+            const double* gV = f.V + size_t(sl[c]) * SP2;
+            for (int e = tid; e < SP2; e += kLvT) {
+                const int i = e >> 6, j = e & 63;
+                U[c][i * LD + j] = gU[e];
+                V[c][i * LD + j] = gV[e];
+            }
+            if (tid < SP) lam[c][tid] = f.lam[size_t(sl[c]) * SP + tid] * a;
+        }
+        if (tid == 0) { sE = 0; sL = 0.0; }
+        __syncthreads();
+        for (int h = 0; h < lp.H; ++h) {
+            const int b1 = lp.off[h + 1];
+            for (int i = lp.off[h] + warp; i < b1; i += kLvW) {
+                const int u = lp.nodes[i];
+                double x[NC][2];
+                if (t.leaf[u]) {                           // x_c = V_c * leaf vector
+                    const int tx = t.taxon[u];
+                    int st = -1;
+                    uint64_t mk = t.all_mask;
+                    if (tx >= 0) {
+                        st = t.states[size_t(tx) * t.Pp + p];
+                        if (st < 0) mk = t.masks[size_t(tx) * t.Pp + p];
+                    }
+                    const bool all = mk == 0 || (mk & t.all_mask) == t.all_mask;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        double a0 = 0.0, a1 = 0.0;
+                        if (st >= 0) {
+                            a0 = V[c][s0 * LD + st];
+                            a1 = V[c][s1 * LD + st];
+                        } else {
+                            for (int j = 0; j < S; ++j)
+                                if (all || ((mk >> j) & 1)) { a0 += V[c][s0 * LD + j]; a1 += V[c][s1 * LD + j]; }
+                        }
+                        x[c][0] = a0;
+                        x[c][1] = a1;
+                    }
+                } else {                                   // D = product of the children's messages
+                    double d0 = s0 < S ? 1.0 : 0.0, d1 = s1 < S ? 1.0 : 0.0;
+                    int E = 0;
+                    const int e1 = t.ch_off[u + 1];
+                    for (int e = t.ch_off[u]; e < e1; ++e) {
+                        const double* mc = msg + size_t(t.ch[e]) * SP;
+                        d0 *= mc[s0];
+                        d1 *= mc[s1];
+                        const double mx = warp_max(fmax(d0, d1));
+                        if (mx > 0.0 && mx < 0x1p-256) {
+                            d0 *= 0x1p256;
+                            d1 *= 0x1p256;
+                            E += 256;
+                        }
+                    }
+                    if (lane == 0 && E) atomicAdd(&sE, E);
+                    if (u == t.root) {                     // L = pi . D
+                        const double v = warp_sum((s0 < S ? f.pi[s0] * d0 : 0.0) + (s1 < S ? f.pi[s1] * d1 : 0.0));
+                        if (lane == 0) sL = v;
+                        continue;
+                    }
+                    dv[s0] = d0;
+                    dv[s1] = d1;
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        double a0 = 0.0, a1 = 0.0;
+                        const double* v0 = V[c] + s0 * LD;
+                        const double* v1 = V[c] + s1 * LD;
+#pragma unroll 16
+                        for (int j = 0; j < SP; ++j) {
+                            const double dj = dv[j];
+                            a0 = fma(v0[j], dj, a0);
+                            a1 = fma(v1[j], dj, a1);
+                        }
+                        x[c][0] = a0;
+                        x[c][1] = a1;
+                    }
+                }
+                const double tb = bl[u];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    xv[c * SP + s0] = x[c][0] * exp(lam[c][s0] * tb);
+                    xv[c * SP + s1] = x[c][1] * exp(lam[c][s1] * tb);
+                }
+                __syncwarp();
+                double m0 = 0.0, m1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    double a0 = 0.0, a1 = 0.0;
+                    const double* u0 = U[c] + s0 * LD;
+                    const double* u1 = U[c] + s1 * LD;
+                    const double* xc = xv + c * SP;
+#pragma unroll 16
+                    for (int j = 0; j < SP; ++j) {
+                        const double xj = xc[j];
+                        a0 = fma(u0[j], xj, a0);
+                        a1 = fma(u1[j], xj, a1);
+                    }
+                    m0 += w[c] * a0;
+                    m1 += w[c] * a1;
+                }
+                __syncwarp();                              // dv / xv are reused by this warp's next node
+                msg[size_t(u) * SP + s0] = s0 < S ? fmax(m0, 0.0) : 0.0;
+                msg[size_t(u) * SP + s1] = s1 < S ? fmax(m1, 0.0) : 0.0;
+            }
+            __syncthreads();                               // this level's messages are visible to the next
+        }
+        if (tid == 0) out[r] = sL > 0.0 ? log(sL) - double(sE) * 0.69314718055994530942 : -1e20;
+    }
 }
 
 // grid n_req, block 256: MEME's empirical Bayes factors (meme.hpp:484-588).  For
@@ -529,7 +687,11 @@ struct FelDevice {
     FelModel f{};
     double* d_bl = nullptr;
     int* d_ev = nullptr;
-    double* d_stack = nullptr;
+    double* d_stack = nullptr;            // EBF pass: [kEbfChunk][depth][64] open partials
+    int* d_lv = nullptr;                  // level plan: [H + 1] offsets, then [n] nodes
+    int H = 0;
+    double* d_work = nullptr;             // level-synchronous pruning: [grid][n][64] messages
+    int grid1 = 1, grid2 = 1;             // persistent CTAs for one / two components
     unsigned char* d_req = nullptr;       // per batch: [om | a | w1 | eslot | eprev | pat | slot | slot2], packed to the batch's sizes
     unsigned char* h_req = nullptr;       // pinned mirror
     double* d_out = nullptr;
@@ -538,6 +700,7 @@ struct FelDevice {
     double* d_ebf = nullptr;              // [kEbfChunk][n]
     double* h_ebf = nullptr;
     size_t h2d = 0, d2h = 0;              // bytes moved by the batches so far
+    int launches = 0;                     // kernels launched so far
     std::vector<void*> owned;
     std::vector<int> order;               // one-component requests first, then two-component ones
     ~FelDevice() {
@@ -591,6 +754,24 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     if (deepest > kMaxDepth) { *err = "tree deeper than 1024 internal levels"; delete d; return nullptr; }
     d->n_ev = int(ev.size());
     d->depth = deepest;
+    // levels by height: a node's children all sit on lower levels; the root alone on the top one
+    std::vector<int> height(v.n, 0);
+    for (int e : ev) {                    // a node closes after all of its descendants
+        if (e & 1) continue;
+        const int u = e >> 1;
+        for (int c = v.ch_off[u]; c < v.ch_off[u + 1]; ++c) height[u] = std::max(height[u], height[v.ch[c]] + 1);
+    }
+    for (int c = v.ch_off[v.root]; c < v.ch_off[v.root + 1]; ++c) height[v.root] = std::max(height[v.root], height[v.ch[c]] + 1);
+    d->H = height[v.root] + 1;
+    std::vector<int> lv(size_t(d->H) + 1 + v.n, 0);
+    for (int u = 0; u < v.n; ++u) ++lv[size_t(height[u]) + 1];
+    for (int h = 0; h < d->H; ++h) lv[size_t(h) + 1] += lv[size_t(h)];
+    {
+        std::vector<int> fill(lv.begin(), lv.begin() + d->H);
+        for (int u = 0; u < v.n; ++u) lv[size_t(d->H) + 1 + size_t(fill[size_t(height[u])]++)] = u;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v.device);
     std::vector<double> sq(SP, 0.0), isq(SP, 0.0), pp(SP, 0.0);
     for (int i = 0; i < S; ++i) {
         sq[i] = std::sqrt(std::max(pi[i], 1e-12));
@@ -608,7 +789,8 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     bool ok = take(&qs, size_t(S) * S) && take(&qn, size_t(S) * S) && take(&dsq, SP) && take(&disq, SP) && take(&dpi, SP) &&
               take(&d->f.lam, size_t(d->n_slots) * SP) && take(&d->f.U, size_t(d->n_slots) * SP2) &&
               take(&d->f.V, size_t(d->n_slots) * SP2) && take(&d->d_bl, v.n) && take(&d->d_ev, ev.size()) &&
-              take(&d->d_stack, size_t(d->max_req) * d->depth * SP) && take(&d->d_out, d->max_req);
+              take(&d->d_stack, size_t(kEbfChunk) * d->depth * SP) && take(&d->d_out, d->max_req) &&
+              take(&d->d_lv, lv.size()) && take(&d->d_work, size_t(2) * std::max(sms, 1) * v.n * SP);
     void* rq = nullptr;
     ok = ok && cudaMalloc(&rq, d->req_bytes()) == cudaSuccess;
     if (rq) d->owned.push_back(rq);
@@ -625,16 +807,22 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
          cudaMemcpyAsync(dpi, pp.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
          cudaMemcpyAsync(d->d_bl, branch_lengths, v.n * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
          cudaMemcpyAsync(d->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_lv, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess &&
          cudaStreamSynchronize(s) == cudaSuccess;
     static bool configured = false;
     if (ok && !configured) {
         ok = cudaFuncSetAttribute(k_fel_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEigSmem)) == cudaSuccess &&
-             cudaFuncSetAttribute(k_fel_lnl<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lnl_smem(1))) == cudaSuccess &&
-             cudaFuncSetAttribute(k_fel_lnl<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lnl_smem(2))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_site_lnl<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(1))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_site_lnl<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(2))) == cudaSuccess &&
              cudaFuncSetAttribute(k_meme_ebf, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEbfSmem)) == cudaSuccess;
         configured = ok;
     }
+    int per1 = 0, per2 = 0;
+    ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_site_lnl<1>, kLvT, lv_smem(1)) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_site_lnl<2>, kLvT, lv_smem(2)) == cudaSuccess;
     if (!ok) { *err = std::string("FEL set-up: ") + cudaGetErrorString(cudaGetLastError()); delete d; return nullptr; }
+    d->grid1 = std::max(1, std::min(per1, 2) * std::max(sms, 1));     // the workspace holds 2 x SMs CTAs
+    d->grid2 = std::max(1, std::min(per2, 2) * std::max(sms, 1));
     return d;
 }
 
@@ -683,9 +871,11 @@ bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* ei
     }
     d->h2d += bytes;
     unsigned char* g = d->d_req;
-    if (n_eig > 0)
+    if (n_eig > 0) {
         launch_k(k_fel_eig, n_eig, kFT, kEigSmem, s, d->f, reinterpret_cast<const double*>(g),
                  reinterpret_cast<const int*>(g + o_es), reinterpret_cast<const int*>(g + o_pv));
+        ++d->launches;
+    }
     *q = FelReqs{reinterpret_cast<const int*>(g + o_pat), reinterpret_cast<const double*>(g + o_a),
                  reinterpret_cast<const int*>(g + o_sl), reinterpret_cast<const int*>(g + o_s2),
                  reinterpret_cast<const double*>(g + o_w)};
@@ -713,13 +903,14 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int
     if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, order, &q, err))
         return false;
     cudaStream_t s = d->s;
+    const LevelPlan lp{d->H, d->d_lv, d->d_lv + d->H + 1};
+    d->launches += (n1 > 0) + (n_req > n1);
     if (n1 > 0)
-        launch_k(k_fel_lnl<1>, n1, kFT, lnl_smem(1), s, d->f, d->t, static_cast<const double*>(d->d_bl),
-                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack, q, d->d_out);
+        launch_k(k_site_lnl<1>, std::min(n1, d->grid1), kLvT, lv_smem(1), s, d->f, d->t, static_cast<const double*>(d->d_bl),
+                 lp, d->d_work, q, n1, d->d_out);
     if (n_req > n1)
-        launch_k(k_fel_lnl<2>, n_req - n1, kFT, lnl_smem(2), s, d->f, d->t, static_cast<const double*>(d->d_bl),
-                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack + size_t(n1) * d->depth * SP,
-                 offset(q, n1), d->d_out + n1);
+        launch_k(k_site_lnl<2>, std::min(n_req - n1, d->grid2), kLvT, lv_smem(2), s, d->f, d->t,
+                 static_cast<const double*>(d->d_bl), lp, d->d_work, offset(q, n1), n_req - n1, d->d_out + n1);
     d->d2h += size_t(n_req) * sizeof(double);
     const bool ok = cudaGetLastError() == cudaSuccess &&
                     (n_req == 0 || cudaMemcpyAsync(d->h_out, d->d_out, n_req * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess) &&
@@ -754,6 +945,7 @@ bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int*
         return false;
     cudaStream_t s = d->s;
     const size_t bytes = size_t(n_req) * d->n * sizeof(double);
+    d->launches += n_req > 0;
     if (n_req > 0)
         launch_k(k_meme_ebf, n_req, kFT, kEbfSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
                  static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack, q, d->d_msg, d->d_ebf);
@@ -768,9 +960,10 @@ bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int*
 
 int fel_device_max_ebf(const FelDevice* d) { return std::min(kEbfChunk, d->max_req); }
 
-void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h) {
+void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h, int* launches) {
     *h2d = d->h2d;
     *d2h = d->d2h;
+    *launches = d->launches;
 }
 
 void fel_device_destroy(FelDevice* d) {

@@ -43,9 +43,10 @@ int fel_device_max_ebf(const FelDevice* d);
 bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                     const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
                     const double* req_w1, double* ebf_out, std::string* err);
-void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h);   // bytes moved by the batches
+void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h, int* launches);   // bytes moved, kernels launched
 void fel_device_destroy(FelDevice* d);
-// record a whole run's transfers where h3g_last_eval_transfer reports them (h3g_capi.cu)
-void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h);
+// record a whole run's transfers, kernel launches and host wall time where
+// h3g_last_eval_transfer / h3g_last_eval_stats report them (h3g_capi.cu)
+void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h, int launches, double ms);
 
 }  // namespace h3g

@@ -16,6 +16,7 @@
 // (the shared start grid, the null model's omega = 1) is diagonalised once
 // into a shared slot.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <new>
 #include <string>
@@ -225,6 +226,7 @@ using namespace h3g::sitefit;
 extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths,
                                   h3g_fel_result* out) {
     if (!prob) return H3G_ERR_ARG;
+    const auto t_start = std::chrono::steady_clock::now();
     try {
         FelProblemView v;
         std::vector<int> variable;
@@ -251,13 +253,16 @@ extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, con
             sites[i].pattern = variable[i];
             fits.push_back(fel_search(sites[i], res[i]));
         }
-        const h3g_status st = run_lockstep(dev, sites, fits, opt, &err);
+        LockstepState state;
+        const h3g_status st = run_lockstep(dev, sites, fits, opt, state, &err);
         size_t h2d = 0, d2h = 0;
-        fel_device_transfer(dev, &h2d, &d2h);
+        int launches = 0;
+        fel_device_transfer(dev, &h2d, &d2h, &launches);
         fel_device_destroy(dev);
         if (st != H3G_OK) { fel_set_error(prob, "h3g_fel_run: " + err); return st; }
         // the run's own inputs and outputs: model, branch lengths, per-pattern results
-        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h);
+        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h, launches,
+                            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
         for (int i = 0; i < N; ++i) out[variable[i]] = res[i];
         return H3G_OK;
     } catch (const std::bad_alloc&) {

@@ -11,6 +11,7 @@
 // A likelihood evaluation needs two eigensystems (omega1 and beta+ / alpha)
 // and prunes with their transition matrices mixed (p1, 1 - p1) per branch.
 #include <algorithm>
+#include <chrono>
 #include <array>
 #include <cmath>
 #include <new>
@@ -85,6 +86,48 @@ Task<Pt<D>> nelder_mead_nd(Site& s, Make make, Arr<D> init, Arr<D> lb, Arr<D> ub
         for (int d = 0; d < D; ++d) c[d] /= double(D);
         Arr<D> xr;
         for (int d = 0; d < D; ++d) xr[d] = c[d] + 1.0 * (c[d] - v[D].x[d]);
+        if (s.speculate) {
+            // The step evaluates the reflection r and then at most one of the expansion and the two
+            // contractions; all four points are known before r's value, so they are evaluated in one
+            // batch and the decisions below are the sequential ones.  Unused values are not counted.
+            const Arr<D> xrc = clampx(xr);
+            Arr<D> xe, xo, xi;
+            for (int d = 0; d < D; ++d) {
+                xe[d] = c[d] + 2.0 * (xrc[d] - c[d]);
+                xo[d] = c[d] + 0.5 * (xrc[d] - c[d]);
+                xi[d] = c[d] + 0.5 * (v[D].x[d] - c[d]);
+            }
+            xs = {xrc, clampx(xe), clampx(xo), clampx(xi)};
+            co_await eval_all();
+            const Pt<D> r{xs[0], -rq[0].lnl};
+            int used = 1;
+            bool shrink = false;
+            if (r.f < v[0].f) {
+                const Pt<D> e{xs[1], -rq[1].lnl};
+                v[D] = (e.f < r.f) ? e : r;
+                used = 2;
+            } else if (r.f < v[D - 1].f) {
+                v[D] = r;
+            } else {
+                const bool outside = r.f < v[D].f;
+                const Pt<D> cc = outside ? Pt<D>{xs[2], -rq[2].lnl} : Pt<D>{xs[3], -rq[3].lnl};
+                used = 2;
+                if (cc.f < (outside ? r.f : v[D].f)) v[D] = cc;
+                else shrink = true;
+            }
+            s.evaluations -= 4 - used;
+            if (shrink) {
+                xs.clear();
+                for (int i = 1; i <= D; ++i) {
+                    Arr<D> x;
+                    for (int d = 0; d < D; ++d) x[d] = v[0].x[d] + 0.5 * (v[i].x[d] - v[0].x[d]);
+                    xs.push_back(clampx(x));
+                }
+                co_await eval_all();
+                for (int i = 1; i <= D; ++i) v[i] = Pt<D>{xs[i - 1], -rq[i - 1].lnl};
+            }
+            continue;
+        }
         const auto [xrc, rr] = one(xr);
         const Pt<D> r{xrc, -(co_await Eval{s, rr})};
         if (r.f < v[0].f) {
@@ -232,6 +275,7 @@ using namespace h3g::sitefit;
 extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths, h3g_meme_result* out,
                                    double* branch_ebf) {
     if (!prob) return H3G_ERR_ARG;
+    const auto t_start = std::chrono::steady_clock::now();
     try {
         FelProblemView v;
         std::vector<int> variable;
@@ -258,6 +302,7 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
         LockstepOptions opt;
         opt.max_requests = std::max({64, N, std::min(8 * N, 16384)});
         opt.temp_slots = std::min(2 * opt.max_requests, 32768);
+        opt.spec_threshold = 32;            // four candidates per site still fit one wave of the pruning kernel
         std::string err;
         FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, opt.max_requests,
                                            slots_needed(N, opt.temp_slots), &err);
@@ -265,6 +310,7 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
         std::vector<Site> sites(N);
         std::vector<h3g_fel_result> fel(N, h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0});
         std::vector<MemeOut> mo(N);
+        LockstepState state;                // one slot map for both phases: sites keep their slots
         h3g_status st = H3G_OK;
         {
             std::vector<Fit> fits;
@@ -274,14 +320,14 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
                 fits.push_back(fel_search(sites[i], fel[i]));
             }
             opt.cache_tol = 1e-12;          // the FEL baseline keeps FEL's per-pattern cache (fel.hpp:368-376)
-            st = run_lockstep(dev, sites, fits, opt, &err);
+            st = run_lockstep(dev, sites, fits, opt, state, &err);
         }
         if (st == H3G_OK) {
             std::vector<Fit> fits;
             fits.reserve(N);
             for (int i = 0; i < N; ++i) fits.push_back(meme_search(sites[i], fel[i], mo[i]));
             opt.cache_tol = 0.0;            // MEME builds its models afresh for every evaluation
-            st = run_lockstep(dev, sites, fits, opt, &err);
+            st = run_lockstep(dev, sites, fits, opt, state, &err);
         }
         // empirical Bayes factors at the reported MLE, in chunks
         std::vector<int> todo;
@@ -298,19 +344,18 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
                 Site& s = sites[i];
                 const h3g_meme_result& r = mo[i].r;
                 const double om[2] = {mo[i].omega1, r.beta_plus / r.alpha};
+                int own[2];
                 for (int c = 0; c < 2; ++c) {
-                    const int own = kSharedSlots + 2 * i + c;
+                    own[c] = own_slot(i, 1 - s.buf[c], c);
                     eom.push_back(om[c]);
-                    eslot.push_back(own);
+                    eslot.push_back(own[c]);
                     eprev.push_back(s.slot[c]);
-                    s.slot[c] = own;
-                    s.cached[c] = om[c];
                 }
                 rpat.push_back(s.pattern);
                 ra.push_back(r.alpha);
                 rw.push_back(r.p1);
-                rs1.push_back(kSharedSlots + 2 * i);
-                rs2.push_back(kSharedSlots + 2 * i + 1);
+                rs1.push_back(own[0]);
+                rs2.push_back(own[1]);
             }
             ebf.assign((k1 - k0) * size_t(v.n), 1.0);
             if (!fel_device_ebf(dev, int(eom.size()), eom.data(), eslot.data(), eprev.data(), int(rpat.size()), rpat.data(),
@@ -332,10 +377,12 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
             }
         }
         size_t h2d = 0, d2h = 0;
-        fel_device_transfer(dev, &h2d, &d2h);
+        int launches = 0;
+        fel_device_transfer(dev, &h2d, &d2h, &launches);
         fel_device_destroy(dev);
         if (st != H3G_OK) { fel_set_error(prob, "h3g_meme_run: " + err); return st; }
-        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h);
+        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h, launches,
+                            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
         for (int i = 0; i < N; ++i) {
             h3g_meme_result& r = mo[i].r;
             // meme.hpp:599-619: length of the site's mixture model over the tested tree

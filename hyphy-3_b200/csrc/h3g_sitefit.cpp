@@ -15,9 +15,9 @@ uint64_t bits_of(double x) {
 }
 
 h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fit>& fits, const LockstepOptions& opt,
-                        std::string* err) {
+                        LockstepState& state, std::string* err) {
     const int N = int(sites.size());
-    const int own_base = kSharedSlots, temp_base = kSharedSlots + 2 * N;
+    const int temp_base = slots_needed(N, 0);
     for (int i = 0; i < N; ++i) {
         sites[i].resume = fits[i].h;
         sites[i].pending = nullptr;
@@ -29,13 +29,21 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
         h.resume();
         if (fits[i].h.promise().error) { *err = "optimiser failed"; return H3G_ERR_NUMERIC; }
     }
-    std::unordered_map<uint64_t, int> shared;          // omega bits -> shared slot (whole run)
+    auto& shared = state.shared;                        // omega bits -> shared slot (whole run)
     std::unordered_map<uint64_t, int> users;           // omega bits -> sites requesting it this batch
     std::unordered_map<uint64_t, int> temp;            // omega bits -> pool slot (this batch)
     std::vector<uint64_t> keys;
     std::vector<int> admitted, req_pat, req_slot, req_slot2, eig_slot, eig_prev;
     std::vector<double> req_a, req_w1, eig_om, lnl;
     std::vector<Req*> req_ptr;
+    const size_t n_slots = size_t(slots_needed(N, opt.temp_slots));
+    if (state.written.size() < n_slots) {
+        state.written.resize(n_slots, -1);
+        state.solved.resize(n_slots, 0);
+    }
+    auto& written = state.written;
+    auto& solved = state.solved;
+    int& batch = state.batch;
     for (;;) {
         users.clear();
         bool any = false;
@@ -73,6 +81,9 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
             const bool single = k == 1;
             if (!single && temp_used + 2 * k > opt.temp_slots) continue;    // next batch
             admitted.push_back(i);
+            int flip_slot[2] = {-1, -1};
+            double flip_om[2] = {0.0, 0.0};
+            bool first = true;
             for (Req& r : *s.pending) {
                 const int nc = r.om2 >= 0.0 ? 2 : 1;
                 int sl[2] = {-1, -1};
@@ -91,17 +102,24 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
                         if (auto t = temp.find(key); t != temp.end()) {
                             slot = t->second;
                         } else {
-                            slot = temp_base + temp_used++;
+                            if (first) {                    // into the site's other buffer, current afterwards
+                                slot = own_slot(i, 1 - s.buf[c], c);
+                                flip_slot[c] = slot;
+                                flip_om[c] = om;
+                            } else {
+                                slot = temp_base + temp_used++;
+                            }
                             temp.emplace(key, slot);
-                            solve(om, slot, s.slot[c]);     // warm start from the site's last eigensystem
+                            solve(om, slot, s.slot[c]);     // warm start from the site's current eigensystem
                         }
                     } else {
-                        slot = own_base + 2 * i + c;
-                        solve(om, slot, s.slot[c]);         // in place when the site's last one was its own
+                        slot = own_slot(i, s.buf[c], c);
+                        solve(om, slot, s.slot[c]);         // in place when the current one is the site's own
                     }
                     if (single) { s.slot[c] = slot; s.cached[c] = om; }
                     sl[c] = slot;
                 }
+                first = false;
                 req_pat.push_back(s.pattern);
                 req_a.push_back(r.a);
                 req_w1.push_back(nc == 2 ? r.w1 : 1.0);
@@ -110,17 +128,46 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
                 req_ptr.push_back(&r);
                 mixed = mixed || nc == 2;
             }
+            for (int c = 0; c < 2; ++c)
+                if (flip_slot[c] >= 0) {
+                    s.buf[c] ^= 1;
+                    s.slot[c] = flip_slot[c];
+                    s.cached[c] = flip_om[c];
+                }
         }
         if (admitted.empty()) { *err = "a pattern's requests exceed one device batch"; return H3G_ERR_STATE; }
+        // one launch solves every slot at most once, reads no slot it writes (an in-place warm
+        // start excepted), and every request reads slots solved in this or an earlier batch
+        for (size_t e = 0; e < eig_slot.size(); ++e) {
+            if (written[size_t(eig_slot[e])] == batch) { *err = "an eigensystem slot is solved twice in one batch"; return H3G_ERR_STATE; }
+            written[size_t(eig_slot[e])] = batch;
+        }
+        for (size_t e = 0; e < eig_prev.size(); ++e) {
+            const int pv = eig_prev[e];
+            if (pv < 0) continue;
+            if ((written[size_t(pv)] == batch && pv != eig_slot[e]) || !solved[size_t(pv)]) {
+                *err = "a warm start reads a slot solved in the same batch";
+                return H3G_ERR_STATE;
+            }
+        }
+        for (size_t e = 0; e < eig_slot.size(); ++e) solved[size_t(eig_slot[e])] = 1;
+        for (size_t r = 0; r < req_slot.size(); ++r)
+            if (!solved[size_t(req_slot[r])] || (req_slot2[r] >= 0 && !solved[size_t(req_slot2[r])])) {
+                *err = "a request reads an eigensystem that was never solved";
+                return H3G_ERR_STATE;
+            }
+        ++batch;
         lnl.assign(req_pat.size(), 0.0);
         if (!fel_device_eval(dev, int(eig_om.size()), eig_om.data(), eig_slot.data(), eig_prev.data(), int(req_pat.size()),
                              req_pat.data(), req_a.data(), req_slot.data(), mixed ? req_slot2.data() : nullptr,
                              mixed ? req_w1.data() : nullptr, lnl.data(), err))
             return H3G_ERR_CUDA;
         for (size_t r = 0; r < req_ptr.size(); ++r) req_ptr[r]->lnl = lnl[r];
+        const bool small = int(req_pat.size()) <= opt.spec_threshold;
         for (int i : admitted) {
             Site& s = sites[i];
             s.pending = nullptr;
+            s.speculate = small;
             std::coroutine_handle<> h = s.resume;
             s.resume = {};
             h.resume();

@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <exception>
 #include <string>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -40,7 +41,10 @@ struct Site {
     std::coroutine_handle<> resume;         // innermost coroutine waiting on them
     int slot[2] = {-1, -1};                 // eigensystem last used per component (cache, warm starts)
     double cached[2] = {-1.0, -1.0};
+    int buf[2] = {0, 0};                    // which of the site's two own slots per component is current
     int evaluations = 0;
+    bool speculate = false;                 // the last batch was small: a search may evaluate its next
+                                            // candidates together (results are unchanged)
 };
 
 // Top-level coroutine of one pattern; the driver owns and destroys it.
@@ -122,22 +126,38 @@ struct EvalMany {
 };
 
 // Eigensystem slot layout of a run: [0, kSharedSlots) omegas requested by
-// several patterns in one batch (kept for the run), then two slots per site
-// (its own components, warm-started in place), then a pool for the sites
-// that park several requests at once (reused every batch).
+// several patterns in one batch (kept for the run), then four slots per site
+// (two buffers per component: a single request is solved in place in the
+// current one, the first request of a multi-request batch into the other,
+// which then becomes current), then a pool for the remaining requests of
+// multi-request sites (reused every batch).  Every solve is warm-started from
+// the site's current eigensystem.
 constexpr int kSharedSlots = 64;
-inline int slots_needed(int n_sites, int temp_slots) { return kSharedSlots + 2 * n_sites + temp_slots; }
+inline int own_slot(int site, int buf, int c) { return kSharedSlots + 4 * site + 2 * buf + c; }
+inline int slots_needed(int n_sites, int temp_slots) { return kSharedSlots + 4 * n_sites + temp_slots; }
 
 struct LockstepOptions {
     double cache_tol = 0.0;     // a site reuses its eigensystem while |omega - cached| <= cache_tol
     int max_requests = 1;       // per device batch (the device was created with this many)
     int temp_slots = 0;         // pool size for multi-request sites
+    int spec_threshold = 0;     // batches of at most this many requests set Site::speculate
+};
+
+// What a run's slots hold across its lockstep phases (FEL then MEME on the
+// same device and sites): the shared omegas, and which slots were solved in
+// which batch.  Sites keep their cached slots from one phase to the next, so
+// a shared slot must keep its omega for the whole run.
+struct LockstepState {
+    std::unordered_map<uint64_t, int> shared;          // omega bits -> shared slot
+    std::vector<int> written;                          // batch that last solved each slot
+    std::vector<char> solved;
+    int batch = 0;
 };
 
 // Resume every fit until all have finished.  Returns H3G_OK, or H3G_ERR_CUDA /
 // H3G_ERR_NUMERIC / H3G_ERR_STATE with *err set.
 h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fit>& fits, const LockstepOptions& opt,
-                        std::string* err);
+                        LockstepState& state, std::string* err);
 
 uint64_t bits_of(double x);
 

@@ -212,7 +212,8 @@ typedef struct {
  * FEL time (input length x 3 / mean rate of the base model, fel.hpp:230-273);
  * out[n_patterns].  Blocks until done.  The problem's installed model (if
  * any) is left untouched; h3g_last_eval_transfer then reports the bytes the
- * whole run moved between host and device. */
+ * whole run moved between host and device, and h3g_last_eval_stats the run's
+ * host wall time and kernel launches. */
 h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths, h3g_fel_result* out);
 
 /* ---------------------------------------------------------------- MEME

@@ -100,6 +100,7 @@ def test_meme_cd2_ebf_matches_oracle(cd2):
     # device vs two re-prunings per branch in the oracle)
     close = (np.abs(dev["alpha"] - np.asarray(ref["alpha"])) <= 1e-6 * np.maximum(1.0, dev["alpha"])) & \
             (np.abs(dev["beta_plus"] - np.asarray(ref["beta_plus"])) <= 1e-6 * np.maximum(1.0, dev["beta_plus"])) & \
+            (np.abs(dev["beta1"] - np.asarray(ref["beta1"])) <= 1e-6 * np.maximum(1.0, dev["beta1"])) & \
             (np.abs(dev["p1"] - np.asarray(ref["p1"])) <= 1e-6) & (np.asarray(ref["evals"]) > 0)
     tested = close & (dev["lrt"] > 0)
     assert tested.sum() >= 5
