@@ -422,6 +422,11 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+MEME_METRIC = "MEME per-site fits/s (FEL baseline + MEME alternative, null and branch EBFs per codon site)"
+MEME_WORKLOAD = ("MEME per-site fits: 256-taxon random unrooted tree (509 branches), 2000 simulated codons, every "
+                 "branch tested; per site the FEL fit, the reference's 4-D Nelder-Mead of (alpha, omega1, p1, beta+) "
+                 "from its start grid, the 3-D null and warm refit where beta+ > alpha, LRT, p-value and the "
+                 "empirical Bayes factor of every branch")
 FEL_METRIC = "FEL per-site fits/s (alternative + null model per codon site)"
 FEL_WORKLOAD = ("FEL per-site fits: 256-taxon random unrooted tree (509 branches), 2000 simulated codons, "
                 "every branch tested; per site the reference's 12-point grid, bounded Nelder-Mead on (alpha, beta), "
@@ -442,7 +447,9 @@ def _fel_inputs(h, aln, p):
 
 
 def run_fel(args) -> None:
-    """FEL per-site fits of the 256-taxon / 2000-codon workload through h3g_fel_run (FP64)."""
+    """FEL (or, with --analysis meme, MEME) per-site fits of the 256-taxon / 2000-codon workload through
+    h3g_fel_run / h3g_meme_run (FP64)."""
+    meme = args.analysis == "meme"
     import torch
     import _hyphy3 as h
     from hyphy3 import _capi
@@ -465,24 +472,27 @@ def run_fel(args) -> None:
     pi, qs, qn = _fel_inputs(h, aln, p)
     bl = np.array(tree.get_branch_lengths()) * conv
     steps = max(3, min(args.steps, 5))
-    out = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)          # warm-up
+    fit = (lambda: pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)) if meme else \
+          (lambda: pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl))
+    out = fit()                                                          # warm-up
     torch.cuda.synchronize()
     sampler = ClockSampler(0)
     sampler.start()
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        out = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)
+        out = fit()
         times.append(time.perf_counter() - t0)
     clocks = sampler.stop()
     h2d, d2h = pr.last_transfer()
+    launches = pr.last_stats()[1]
     secs = statistics.median(times)
     sites = wl.n_sites
     evals = float(np.dot(out["evaluations"], weights))
     branches = n - 1
     value = sites / secs
     t0 = time.perf_counter()
-    res = fel.run()
+    res = h.MEMEAnalyzer(tree, aln, p).run() if meme else fel.run()
     e2e_secs = time.perf_counter() - t0
     cpu = None
     if not args.no_cpu:
@@ -492,27 +502,33 @@ def run_fel(args) -> None:
         cls = {"alpha": 1.0, "beta": p.beta, "theta": list(wl.theta)}
         threads = o.max_threads()
         o.set_threads(threads)
-        k = max(threads, 16)
+        # a MEME site costs the oracle ~100x a FEL site: one pattern per thread, a few threads
+        k = min(threads, 4) if meme else max(threads, 16)
+        run_cpu = o.meme_run if meme else o.fel_run
         o.fel_run(ot, oa, cls, 2)
         t0 = time.perf_counter()
-        r = o.fel_run(ot, oa, cls, k)
+        r = run_cpu(ot, oa, cls, k)
         cs = time.perf_counter() - t0
         fitted = int(np.sum(np.array(r["evals"]) > 0))
-        cpu = {"value": k / cs, "unit": "sites/s", "cores": threads, "kind": "port",
+        cpu = {"value": k / cs, "unit": "sites/s", "cores": min(threads, k) if meme else threads, "kind": "port",
                "sample": f"the first {k} patterns ({fitted} fitted, the rest invariant) of the same alignment, "
-                         f"{cs:.1f} s (oracle restatement of fel.hpp with the reference's optimisers)"}
+                         f"{cs:.1f} s (oracle restatement of {'meme.hpp' if meme else 'fel.hpp'} with the "
+                         f"reference's optimisers)"}
     line = {
-        "metric": FEL_METRIC, "value": value, "unit": "sites/s", "n_gpus": 1, "steps": steps, "warmup": 1,
+        "metric": MEME_METRIC if meme else FEL_METRIC, "value": value, "unit": "sites/s", "n_gpus": 1, "steps": steps,
+        "warmup": 1,
         "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": FEL_WORKLOAD, "sites": sites, "patterns": aln.num_patterns, "branches": branches},
+        "config": {"workload": MEME_WORKLOAD if meme else FEL_WORKLOAD, "sites": sites, "patterns": aln.num_patterns,
+                   "branches": branches},
         "site_branch_lnl_evals_per_s": evals * branches / secs,
         "evaluations_per_site": evals / sites,
         "e2e": {"value": sites / e2e_secs, "unit": "sites/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "api": "hyphy3.FELAnalyzer(tree, aln, params).run()"},
+                "api": f"hyphy3.{'MEMEAnalyzer' if meme else 'FELAnalyzer'}(tree, aln, params).run()"},
         "cpu_baseline": cpu,
         "significant_at_0.1": int(sum(1 for r in res if r.p_value <= 0.1)),
-        "clocks": clocks, "timing": "host wall clock around each blocking h3g_fel_run (median of steps)",
+        "clocks": clocks, "gpu_launches": int(launches),
+        "timing": f"host wall clock around each blocking {'h3g_meme_run' if meme else 'h3g_fel_run'} (median of steps)",
     }
     print(json.dumps(line), flush=True)
     pr.close()
@@ -610,6 +626,7 @@ def main() -> None:
     ap.add_argument("--config", type=int, choices=[1, 2, 3], default=1,
                     help="1: 64-taxon 3-omega mixture (headline); 2: FEL per-site fits, 256 taxa x 2000 codons; "
                          "3: 1024-taxon, 4 rate x 2 omega classes")
+    ap.add_argument("--analysis", choices=["fel", "meme"], default="fel", help="--config 2: which per-site analysis")
     args = ap.parse_args()
     if args.config == 2 and args.impl == "ours" and not args.profile:
         run_fel(args)

@@ -86,6 +86,8 @@ struct h3g_problem {
     double *m_cw = nullptr, *m_rt = nullptr, *m_rw = nullptr, *m_dQ = nullptr;
     uint8_t* m_it = nullptr;
     // captured evaluation graphs, keyed by (want, with host copies)
+    // the site-fit evaluator of the last h3g_fel_run / h3g_meme_run, kept for the next run
+    h3g::FelDevice* fel_dev = nullptr;
     struct GraphEntry { unsigned key; cudaGraphExec_t exec; int launches; };
     std::vector<GraphEntry> graphs;
     void drop_graphs() {
@@ -94,6 +96,7 @@ struct h3g_problem {
     }
     ~h3g_problem() {
         drop_graphs();
+        h3g::fel_device_free(fel_dev);
         if (h_pin) cudaFreeHost(h_pin);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -343,6 +346,8 @@ bool fel_problem_view(h3g_problem* pr, FelProblemView* v) {
 void fel_set_error(h3g_problem* pr, const std::string& msg) {
     if (pr && pr->ctx) pr->ctx->err = msg;
 }
+
+FelDevice*& problem_fel_device(h3g_problem* pr) { return pr->fel_dev; }
 
 void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h, int launches, double ms) {
     pr->last_h2d = h2d;

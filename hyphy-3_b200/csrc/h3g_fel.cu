@@ -80,8 +80,8 @@ __global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __res
     extern __shared__ __align__(16) double sm[];
     double* A = sm;
     double* E = sm + SP * LD;
-    __shared__ double rc[32], rsn[32], red[kFT / 32];
-    __shared__ int rp[32], rq[32], rot[32];
+    __shared__ double rc[32], rsn[32], rt[32], rapq[32], rapp[32], raqq[32], red[kFT / 32];
+    __shared__ int rp[32], rq[32];
     const int tid = threadIdx.x, S = f.S;
     const double om = omega[blockIdx.x];
     const int sl = slot[blockIdx.x];
@@ -162,45 +162,58 @@ __global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __res
         off = block_sum_or_max(off, red, false);
         tot = block_sum_or_max(tot, red, false);
         if (off <= 1e-30 * tot || off == 0.0) break;
+        // One round = 32 disjoint rotations (p_k, q_k), k < 32, covering all 64 indices.  Warp 0
+        // computes them (t from one square root and one divide, c = rsqrt(1 + t^2)); then every
+        // 2x2 block (I, J) of A is replaced by R_I^T A_IJ R_J in one pass, the diagonal blocks by
+        // their exact values a_pp - t a_pq, a_qq + t a_pq and 0 (Golub & Van Loan, Alg. 8.5.1),
+        // and the columns of E by E R.  Two barriers per round.
         for (int round = 0; round < SP - 1; ++round) {
             if (tid < 32) {
                 int p, q;
                 if (tid == 0) { p = SP - 1; q = round; }
                 else { p = (round + tid) % (SP - 1); q = (round - tid + (SP - 1)) % (SP - 1); }
                 if (p > q) { const int tmp = p; p = q; q = tmp; }
-                const double apq = A[p * LD + q];
-                double c = 1.0, s = 0.0;
-                const bool active = fabs(apq) >= 1e-300;
-                if (active) {
-                    const double tau = (A[q * LD + q] - A[p * LD + p]) / (2.0 * apq);
-                    const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + tt * tt);
-                    s = tt * c;
+                const double apq = A[p * LD + q], app = A[p * LD + p], aqq = A[q * LD + q];
+                double c = 1.0, s = 0.0, t = 0.0;
+                if (fabs(apq) >= 1e-300) {
+                    // t = tan(theta) of the smaller rotation, tau = (a_qq - a_pp) / (2 a_pq):
+                    // t = sign(tau) / (|tau| + sqrt(1 + tau^2)) = 2 a_pq sign(d) / (|d| + sqrt(d^2 + 4 a_pq^2)), d = a_qq - a_pp
+                    const double d = aqq - app;
+                    const double tt = 2.0 * apq / (fabs(d) + sqrt(d * d + 4.0 * apq * apq));
+                    t = d >= 0.0 ? tt : -tt;
+                    c = rsqrt(1.0 + t * t);
+                    s = t * c;
                 }
-                rp[tid] = p; rq[tid] = q; rc[tid] = c; rsn[tid] = s; rot[tid] = active;
+                rp[tid] = p; rq[tid] = q; rc[tid] = c; rsn[tid] = s;
+                rt[tid] = t; rapq[tid] = apq; rapp[tid] = app; raqq[tid] = aqq;
             }
             __syncthreads();
-            for (int e = tid; e < 32 * SP; e += kFT) {      // columns p, q of A and E
+            for (int e = tid; e < 32 * 32; e += kFT) {      // block (I, J) of A
+                const int I = e >> 5, J = e & 31;
+                const int pI = rp[I], qI = rq[I], pJ = rp[J], qJ = rq[J];
+                if (I == J) {
+                    A[pI * LD + pI] = rapp[I] - rt[I] * rapq[I];
+                    A[qI * LD + qI] = raqq[I] + rt[I] * rapq[I];
+                    A[pI * LD + qI] = 0.0;
+                    A[qI * LD + pI] = 0.0;
+                    continue;
+                }
+                const double cI = rc[I], sI = rsn[I], cJ = rc[J], sJ = rsn[J];
+                const double a = A[pI * LD + pJ], b = A[pI * LD + qJ], cc = A[qI * LD + pJ], dd = A[qI * LD + qJ];
+                const double m0 = cJ * a - sJ * b, m1 = sJ * a + cJ * b;      // [a b; c d] R_J
+                const double m2 = cJ * cc - sJ * dd, m3 = sJ * cc + cJ * dd;
+                A[pI * LD + pJ] = cI * m0 - sI * m2;                        // R_I^T (...)
+                A[pI * LD + qJ] = cI * m1 - sI * m3;
+                A[qI * LD + pJ] = sI * m0 + cI * m2;
+                A[qI * LD + qJ] = sI * m1 + cI * m3;
+            }
+            for (int e = tid; e < 32 * SP; e += kFT) {      // columns p, q of E
                 const int k = e >> 6, i = e & 63;
-                if (!rot[k]) continue;
                 const int p = rp[k], q = rq[k];
                 const double c = rc[k], s = rsn[k];
-                const double akp = A[i * LD + p], akq = A[i * LD + q];
-                A[i * LD + p] = c * akp - s * akq;
-                A[i * LD + q] = s * akp + c * akq;
                 const double ekp = E[i * LD + p], ekq = E[i * LD + q];
                 E[i * LD + p] = c * ekp - s * ekq;
                 E[i * LD + q] = s * ekp + c * ekq;
-            }
-            __syncthreads();
-            for (int e = tid; e < 32 * SP; e += kFT) {      // rows p, q of A
-                const int k = e >> 6, j = e & 63;
-                if (!rot[k]) continue;
-                const int p = rp[k], q = rq[k];
-                const double c = rc[k], s = rsn[k];
-                const double apk = A[p * LD + j], aqk = A[q * LD + j];
-                A[p * LD + j] = c * apk - s * aqk;
-                A[q * LD + j] = s * apk + c * aqk;
             }
             __syncthreads();
         }
@@ -715,19 +728,18 @@ struct FelDevice {
 
 constexpr int kEbfChunk = 256;
 
-FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
-                             const double* branch_lengths, int max_requests, int n_slots, std::string* err) {
-    FelProblemView v;
-    if (!fel_problem_view(pr, &v)) { *err = "invalid problem"; return nullptr; }
+namespace {
+
+// Buffers that depend on the problem (traversals, levels) and on the run's sizes
+// (requests per batch, eigensystem slots), not on the model.
+FelDevice* fel_device_alloc(h3g_problem* pr, const FelProblemView& v, int max_requests, int n_slots, std::string* err) {
     auto* d = new (std::nothrow) FelDevice;
     if (!d) { *err = "host allocation failed"; return nullptr; }
     d->pr = pr;
     d->s = problem_stream(pr);
-    d->S = S;
     d->n = v.n;
     d->max_req = std::max(1, max_requests);
     d->n_slots = std::max(1, n_slots);
-    d->t = problem_topo(pr, S);
     // depth-first events in the children CSR order
     std::vector<int> ev;
     ev.reserve(2 * size_t(v.n));
@@ -772,12 +784,6 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v.device);
-    std::vector<double> sq(SP, 0.0), isq(SP, 0.0), pp(SP, 0.0);
-    for (int i = 0; i < S; ++i) {
-        sq[i] = std::sqrt(std::max(pi[i], 1e-12));
-        isq[i] = 1.0 / sq[i];
-        pp[i] = pi[i];
-    }
     auto take = [&](auto** ptr, size_t count) -> bool {
         void* q = nullptr;
         if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**ptr)) != cudaSuccess) return false;
@@ -786,7 +792,7 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
         return true;
     };
     double *qs = nullptr, *qn = nullptr, *dsq = nullptr, *disq = nullptr, *dpi = nullptr;
-    bool ok = take(&qs, size_t(S) * S) && take(&qn, size_t(S) * S) && take(&dsq, SP) && take(&disq, SP) && take(&dpi, SP) &&
+    bool ok = take(&qs, SP2) && take(&qn, SP2) && take(&dsq, SP) && take(&disq, SP) && take(&dpi, SP) &&
               take(&d->f.lam, size_t(d->n_slots) * SP) && take(&d->f.U, size_t(d->n_slots) * SP2) &&
               take(&d->f.V, size_t(d->n_slots) * SP2) && take(&d->d_bl, v.n) && take(&d->d_ev, ev.size()) &&
               take(&d->d_stack, size_t(kEbfChunk) * d->depth * SP) && take(&d->d_out, d->max_req) &&
@@ -798,17 +804,10 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     ok = ok && cudaMallocHost(reinterpret_cast<void**>(&d->h_req), d->req_bytes()) == cudaSuccess &&
          cudaMallocHost(reinterpret_cast<void**>(&d->h_out), d->max_req * sizeof(double)) == cudaSuccess;
     if (!ok) { *err = "device allocation failed"; delete d; return nullptr; }
-    d->f.S = S; d->f.Qs = qs; d->f.Qn = qn; d->f.sq = dsq; d->f.isq = disq; d->f.pi = dpi;
-    cudaStream_t s = d->s;
-    ok = cudaMemcpyAsync(qs, Qs, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(qn, Qn, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(dsq, sq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(disq, isq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(dpi, pp.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(d->d_bl, branch_lengths, v.n * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(d->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaMemcpyAsync(d->d_lv, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess &&
-         cudaStreamSynchronize(s) == cudaSuccess;
+    d->f.Qs = qs; d->f.Qn = qn; d->f.sq = dsq; d->f.isq = disq; d->f.pi = dpi;
+    ok = cudaMemcpyAsync(d->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice, d->s) == cudaSuccess &&
+         cudaMemcpyAsync(d->d_lv, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice, d->s) == cudaSuccess &&
+         cudaStreamSynchronize(d->s) == cudaSuccess;
     static bool configured = false;
     if (ok && !configured) {
         ok = cudaFuncSetAttribute(k_fel_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEigSmem)) == cudaSuccess &&
@@ -823,6 +822,50 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
     if (!ok) { *err = std::string("FEL set-up: ") + cudaGetErrorString(cudaGetLastError()); delete d; return nullptr; }
     d->grid1 = std::max(1, std::min(per1, 2) * std::max(sms, 1));     // the workspace holds 2 x SMs CTAs
     d->grid2 = std::max(1, std::min(per2, 2) * std::max(sms, 1));
+    return d;
+}
+
+}  // namespace
+
+FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
+                             const double* branch_lengths, int max_requests, int n_slots, std::string* err) {
+    FelProblemView v;
+    if (!fel_problem_view(pr, &v) || S < 1 || S > SP) { *err = "invalid problem"; return nullptr; }
+    FelDevice*& cached = problem_fel_device(pr);
+    if (cached && (cached->max_req < max_requests || cached->n_slots < n_slots)) {
+        fel_device_free(cached);
+        cached = nullptr;
+    }
+    if (!cached) cached = fel_device_alloc(pr, v, max_requests, n_slots, err);
+    FelDevice* d = cached;
+    if (!d) return nullptr;
+    // the run's model: rates, frequencies, branch lengths
+    d->S = S;
+    d->f.S = S;
+    d->t = problem_topo(pr, S);
+    d->h2d = d->d2h = 0;
+    d->launches = 0;
+    std::vector<double> sq(SP, 0.0), isq(SP, 0.0), pp(SP, 0.0);
+    for (int i = 0; i < S; ++i) {
+        sq[i] = std::sqrt(std::max(pi[i], 1e-12));
+        isq[i] = 1.0 / sq[i];
+        pp[i] = pi[i];
+    }
+    cudaStream_t s = d->s;
+    const bool ok =
+        cudaMemcpyAsync(const_cast<double*>(d->f.Qs), Qs, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(const_cast<double*>(d->f.Qn), Qn, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(const_cast<double*>(d->f.sq), sq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(const_cast<double*>(d->f.isq), isq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(const_cast<double*>(d->f.pi), pp.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaMemcpyAsync(d->d_bl, branch_lengths, v.n * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+        cudaStreamSynchronize(s) == cudaSuccess;
+    if (!ok) {
+        *err = std::string("FEL set-up: ") + cudaGetErrorString(cudaGetLastError());
+        fel_device_free(d);
+        cached = nullptr;
+        return nullptr;
+    }
     return d;
 }
 
@@ -967,6 +1010,10 @@ void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h, int* laun
 }
 
 void fel_device_destroy(FelDevice* d) {
+    if (d && d->s) cudaStreamSynchronize(d->s);
+}
+
+void fel_device_free(FelDevice* d) {
     if (d && d->s) cudaStreamSynchronize(d->s);
     delete d;
 }

@@ -44,7 +44,12 @@ bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int*
                     const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
                     const double* req_w1, double* ebf_out, std::string* err);
 void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h, int* launches);   // bytes moved, kernels launched
+// ends a run: the evaluator stays with its problem (problem_fel_device) and a
+// later fel_device_create with the same problem and no larger sizes reuses its
+// device buffers instead of allocating them again
 void fel_device_destroy(FelDevice* d);
+void fel_device_free(FelDevice* d);                 // release (problem destruction)
+FelDevice*& problem_fel_device(h3g_problem* pr);    // h3g_capi.cu
 // record a whole run's transfers, kernel launches and host wall time where
 // h3g_last_eval_transfer / h3g_last_eval_stats report them (h3g_capi.cu)
 void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h, int launches, double ms);

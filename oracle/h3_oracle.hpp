@@ -572,7 +572,8 @@ inline void jacobi_eigen(Mat A, std::vector<double>& w, Mat& V) {
         for (int p = 0; p < n - 1; ++p) for (int q = p + 1; q < n; ++q) {
             double apq = A(p, q);
             if (std::fabs(apq) < 1e-300) continue;
-            double tau = (A(q, q) - A(p, p)) / (2.0 * apq);
+            const double app = A(p, p), aqq = A(q, q);
+            double tau = (aqq - app) / (2.0 * apq);
             double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
             double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c;
             for (int k = 0; k < n; ++k) {
@@ -587,6 +588,8 @@ inline void jacobi_eigen(Mat A, std::vector<double>& w, Mat& V) {
                 double vkp = V(k, p), vkq = V(k, q);
                 V(k, p) = c * vkp - s * vkq; V(k, q) = s * vkp + c * vkq;
             }
+            // the rotation annihilates a_pq; set the 2x2 block to its exact values (Alg. 8.5.1)
+            A(p, p) = app - t * apq; A(q, q) = aqq + t * apq; A(p, q) = 0.0; A(q, p) = 0.0;
         }
     }
     w.resize(n);
@@ -1271,6 +1274,56 @@ struct MemeRun {
     std::vector<MemeSite> patterns;
 };
 
+// meme.hpp:484-588: for every non-root branch b, the pattern's likelihood with b
+// alone in class 1 (P1) and alone in class + (Pp), every other branch mixed (Pm);
+// ebf[b] = exp(clamp(lnL_+ - lnL_1, -50, 50)), 1e6 when only lnL_1 is the zero
+// sentinel, 0 when lnL_+ is.
+inline void meme_branch_ebf(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, int p, const std::vector<Mat>& P1,
+                            const std::vector<Mat>& Pp, std::vector<Mat>& Pm, const std::vector<double>& pi,
+                            std::vector<double>& ebf) {
+    const int S = a.code.S, n = tr.n();
+    Pass w;
+    ebf.assign(n, 1.0);
+    for (int b = 0; b < n; ++b) {
+        if (b == tr.root) continue;
+        const Mat keep = Pm[b];
+        Pm[b] = P1[b];
+        inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
+        const double l1 = w.logL;
+        Pm[b] = Pp[b];
+        inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
+        const double lp = w.logL;
+        Pm[b] = keep;
+        double e = 1.0;
+        if (l1 > -1e10 && lp > -1e10) e = std::exp(std::clamp(lp - l1, -50.0, 50.0));
+        else if (l1 <= -1e10 && lp > -1e10) e = 1e6;
+        else e = 0.0;
+        ebf[b] = e;
+    }
+}
+
+// The branch EBFs of pattern p at given (alpha, omega1, p1, beta+) and FEL-time branch lengths.
+inline std::vector<double> meme_ebf_at(const Tree& tr, const Alignment& a, const Params& base, const std::vector<double>& bl,
+                                       int p, double alpha, double omega1, double p1, double beta_plus) {
+    const int S = a.code.S, n = tr.n();
+    Params q1 = base; q1.alpha = 1.0; q1.beta = omega1;
+    Params qp = base; qp.alpha = 1.0; qp.beta = beta_plus / std::max(alpha, 1e-12);
+    MG94 m1, mp;
+    m1.update(q1, a.pos_freq, a.pi, a.code);
+    mp.update(qp, a.pos_freq, a.pi, a.code);
+    std::vector<Mat> P1(n, Mat::eye(S)), Pp(n, Mat::eye(S)), Pm(n, Mat::eye(S));
+    const double ap = std::max(alpha, 1e-12);
+    for (int i = 0; i < n; ++i) {
+        if (i == tr.root) continue;
+        P1[i] = m1.P(ap * bl[i]);
+        Pp[i] = mp.P(ap * bl[i]);
+        for (size_t e = 0; e < Pm[i].a.size(); ++e) Pm[i].a[e] = p1 * P1[i].a[e] + (1.0 - p1) * Pp[i].a[e];
+    }
+    std::vector<double> ebf;
+    meme_branch_ebf(tr, a, leaf_map(tr, a), p, P1, Pp, Pm, a.pi, ebf);
+    return ebf;
+}
+
 // meme.hpp:166-632 with num_background == 0
 inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
                              const MemeRun& run, int p) {
@@ -1377,23 +1430,9 @@ inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vect
         }
         // empirical Bayes factors: every branch alone in class + vs class 1 (meme.hpp:484-588)
         build(res.alpha, omega1, res.p1, res.beta_plus);
-        for (int b = 0; b < n; ++b) {
-            if (b == tr.root) continue;
-            const Mat keep = Pm[b];
-            Pm[b] = P1[b];
-            inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
-            const double l1 = w.logL;
-            Pm[b] = Pp[b];
-            inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
-            const double lp = w.logL;
-            Pm[b] = keep;
-            double e = 1.0;
-            if (l1 > -1e10 && lp > -1e10) e = std::exp(std::clamp(lp - l1, -50.0, 50.0));
-            else if (l1 <= -1e10 && lp > -1e10) e = 1e6;
-            else e = 0.0;
-            res.ebf[b] = e;
-            if (e >= 100.0) ++res.bus;
-        }
+        meme_branch_ebf(tr, a, l2t, p, P1, Pp, Pm, pi, res.ebf);
+        for (int b = 0; b < n; ++b)
+            if (b != tr.root && res.ebf[b] >= 100.0) ++res.bus;
     } else {
         res.lrt = 0.0; res.p_value = 2.0 / 3.0;
     }

@@ -214,6 +214,11 @@ PYBIND11_MODULE(h3oracle, m) {
         d["mu_n"] = r.mu_n;
         return d;
     }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("max_patterns") = -1);
+    m.def("meme_ebf_at", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<double>& bl, int pattern,
+                            double alpha, double omega1, double p1, double beta_plus) {
+        return meme_ebf_at(t, a, params_from(p), bl, pattern, alpha, omega1, p1, beta_plus);
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths"), py::arg("pattern"), py::arg("alpha"),
+       py::arg("omega1"), py::arg("p1"), py::arg("beta_plus"));
     m.def("set_threads", [](int n) {
 #ifdef _OPENMP
         omp_set_num_threads(n);
