@@ -60,7 +60,7 @@ WORKLOADS = {
 MEASURED_TRAFFIC = {
     (1, "mixed"): {"inside": 19.5e6, "outside": 36.2e6, "accum_A": 49.4e6},
     (1, "fp64"): {"inside": 36.5e6, "outside": 68.7e6, "accum_A": 98.3e6},
-    (3, "mixed"): {"inside": 13.548e9, "outside": 22.313e9, "accum_A": 18.797e9},
+    (3, "mixed"): {"inside": 16.763e9, "outside": 27.682e9, "accum_A": 18.793e9},
     (3, "fp64"): {"inside": 29.259e9, "outside": 48.234e9, "accum_A": 34.723e9},
 }
 
@@ -475,6 +475,13 @@ def run_fel(args) -> None:
     fit = (lambda: pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)) if meme else \
           (lambda: pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl))
     out = fit()                                                          # warm-up
+    if args.profile:                                                     # one more run, nothing else (for ncu)
+        out = fit()
+        ms, launches = pr.last_stats()
+        print(json.dumps({"profile": args.analysis, "sites": wl.n_sites, "ms": ms, "gpu_launches": launches}), flush=True)
+        pr.close()
+        ctx.close()
+        return
     torch.cuda.synchronize()
     sampler = ClockSampler(0)
     sampler.start()
@@ -622,13 +629,13 @@ def main() -> None:
     ap.add_argument("--precision", choices=["auto", "fp64", "mixed"], default="auto")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true", help="device evaluations only (for ncu)")
-    ap.add_argument("--sites", type=int, default=None, help="--profile only: shrink the alignment to this many codons")
+    ap.add_argument("--sites", type=int, default=None, help="shrink the alignment to this many codons (--profile; --config 2)")
     ap.add_argument("--config", type=int, choices=[1, 2, 3], default=1,
                     help="1: 64-taxon 3-omega mixture (headline); 2: FEL per-site fits, 256 taxa x 2000 codons; "
                          "3: 1024-taxon, 4 rate x 2 omega classes")
     ap.add_argument("--analysis", choices=["fel", "meme"], default="fel", help="--config 2: which per-site analysis")
     args = ap.parse_args()
-    if args.config == 2 and args.impl == "ours" and not args.profile:
+    if args.config == 2 and args.impl == "ours":
         run_fel(args)
     elif args.profile:
         run_profile(args)
