@@ -81,43 +81,6 @@ __device__ __forceinline__ int renorm_row(float (&v)[kSG], float* smax, const La
     return sh;
 }
 
-// v *= (P_c * leaf_vector(c, p)) restricted to states 16g .. 16g+15, in FP32.
-__device__ __forceinline__ void mul_leaf(float (&v)[kSG], const Topo& t, const MixedWork& mw, int m, int c, int p, int g) {
-    const int tx = t.taxon[c];
-    const float* PTc = mw.PT32 + mat_off_f(m, c, t.n);
-    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * t.Pp + p]);
-    const float* src;
-    if (st >= 0) {
-        src = PTc + st * SP + kSG * g;
-    } else {
-        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * t.Pp + p];
-        if (mk == 0 || (mk & t.all_mask) == t.all_mask) {
-            src = mw.rs32 + (size_t(m) * t.n + c) * SP + kSG * g;
-        } else {
-            float acc[kSG];
-#pragma unroll
-            for (int i = 0; i < kSG; ++i) acc[i] = 0.f;
-            for (uint64_t b = mk; b; b &= b - 1) {
-                const float4* r4 = reinterpret_cast<const float4*>(PTc + (__ffsll((long long)b) - 1) * SP + kSG * g);
-#pragma unroll
-                for (int q4 = 0; q4 < kSG / 4; ++q4) {
-                    const float4 x = __ldg(r4 + q4);
-                    acc[4 * q4] += x.x; acc[4 * q4 + 1] += x.y; acc[4 * q4 + 2] += x.z; acc[4 * q4 + 3] += x.w;
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < kSG; ++i) v[i] *= acc[i];
-            return;
-        }
-    }
-    const float4* s4 = reinterpret_cast<const float4*>(src);
-#pragma unroll
-    for (int q4 = 0; q4 < kSG / 4; ++q4) {
-        const float4 x = __ldg(s4 + q4);
-        v[4 * q4] *= x.x; v[4 * q4 + 1] *= x.y; v[4 * q4 + 2] *= x.z; v[4 * q4 + 3] *= x.w;
-    }
-}
-
 // Where this thread's 16 states of a child's message live: a contiguous
 // row of PT32 / rs32 for a leaf (one-hot or fully ambiguous codon), a masked
 // sum of PT32 rows (partially ambiguous codon), or the child's stored message
@@ -183,10 +146,6 @@ __device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
 __device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
     for (int i = 0; i < kSG; ++i) v[i] = __ldcg(src + i * stride);
-}
-__device__ __forceinline__ void mul_part(float (&v)[kSG], const float* src, size_t stride) {
-#pragma unroll
-    for (int i = 0; i < kSG; ++i) v[i] *= src[i * stride];
 }
 __device__ __forceinline__ void store_part(const float (&v)[kSG], float* dst, size_t stride) {
 #pragma unroll
@@ -727,7 +686,6 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
         unsigned char* DS = VS + kVStage;
         const unsigned char* raw = ring + sl * kRawSlot;
         if (kt >= 2 && !tc::mbar_wait(&mma_bar[st], uint32_t(((kt - 2) >> 1) & 1)) && lane == 0) atomicOr(w.err, 4);
-        const int p0 = p_begin + kt * kAT;
         {
             const uint32_t rg = uint32_t(row >> 3) * 128 + uint32_t(row & 7) * 16;
             float x[8];
