@@ -70,7 +70,8 @@ def build(force: bool = False) -> dict[str, pathlib.Path]:
     mod_src = PYDIR / "_hyphy3_module.cpp"
     mod_deps = [mod_src, lib, ROOT / "include" / "hyphy" / "core" / "likelihood_gpu.hpp",
                 ROOT / "include" / "hyphy" / "analyses" / "fel_gpu.hpp",
-                ROOT / "include" / "hyphy" / "analyses" / "meme_gpu.hpp", ROOT / "include" / "hyphy" / "opt" / "optimizer_gpu.hpp",
+                ROOT / "include" / "hyphy" / "analyses" / "meme_gpu.hpp",
+                ROOT / "include" / "hyphy" / "analyses" / "busted_gpu.hpp", ROOT / "include" / "hyphy" / "opt" / "optimizer_gpu.hpp",
                 ROOT / "include" / "hyphy" / "core" / "h3_host.hpp", ROOT / "include" / "h3g.h"]
     if force or _stale(mod, mod_deps):
         import pybind11

@@ -1,10 +1,13 @@
 // _hyphy3 — Python module with the reference binding's names for the likelihood
 // core (src/python/bindings.cpp:50-119 core types, :725-732 the gradient call),
 // backed by the B200 LikelihoodEngine (include/hyphy/core/likelihood_gpu.hpp).
+#include <optional>
+
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include "hyphy/analyses/busted_gpu.hpp"
 #include "hyphy/analyses/fel_gpu.hpp"
 #include "hyphy/analyses/meme_gpu.hpp"
 #include "hyphy/opt/optimizer_gpu.hpp"
@@ -289,6 +292,47 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("conversion_factor", &FELAnalyzer::conversion_factor)
         .def_readonly("baseline_tree_length", &FELAnalyzer::baseline_tree_length)
         .def_readonly("site_results", &FELAnalyzer::site_results);
+
+    // BUSTED likelihood core: evaluate_log_l and the two EM expectation steps
+    using hyphy::analyses::BUSTEDAnalyzer;
+    using VecS = std::vector<Scalar>;
+    py::class_<BUSTEDAnalyzer>(m, "BUSTEDAnalyzer")
+        .def(py::init([](Tree tree, Alignment aln, const MG94Parameters& params) {
+                 return BUSTEDAnalyzer(std::move(tree), std::move(aln), params);
+             }),
+             "tree"_a, "alignment"_a, "params"_a = MG94Parameters{})
+        .def_readwrite("branch_tau", &BUSTEDAnalyzer::branch_tau)
+        .def_readwrite("is_test_branch", &BUSTEDAnalyzer::is_test_branch)
+        .def_readwrite("num_test_branches", &BUSTEDAnalyzer::num_test_branches)
+        .def_readwrite("mg94_omega", &BUSTEDAnalyzer::mg94_omega)
+        .def_readwrite("mg94_background_omega", &BUSTEDAnalyzer::mg94_background_omega)
+        .def_readonly("mg94_tree_length", &BUSTEDAnalyzer::mg94_tree_length)
+        .def("evaluate_log_l", [](const BUSTEDAnalyzer& b, Scalar s, const VecS& omegas, const VecS& weights, const VecS& syn_rates,
+                                  const VecS& syn_weights, std::optional<VecS> custom, Scalar delta, Scalar psi) {
+                 VecS pll;
+                 Scalar l;
+                 {
+                     py::gil_scoped_release rel;
+                     l = b.evaluate_log_l(s, omegas, weights, syn_rates, syn_weights, custom ? &*custom : nullptr, &pll, delta, psi);
+                 }
+                 return py::make_tuple(l, pll);
+             }, "s"_a, "omegas"_a, "weights"_a, "syn_rates"_a = VecS{1.0}, "syn_weights"_a = VecS{1.0},
+             "custom_branch_lengths"_a = std::nullopt, "delta"_a = 0.0, "psi"_a = 0.0)
+        .def("compute_expected_weights", [](const BUSTEDAnalyzer& b, Scalar s, const VecS& omegas, const VecS& weights,
+                                            const VecS& syn_rates, const VecS& syn_weights, std::optional<VecS> custom,
+                                            Scalar delta, Scalar psi) {
+                 py::gil_scoped_release rel;
+                 return b.compute_expected_weights(s, omegas, weights, syn_rates, syn_weights, custom ? &*custom : nullptr, delta, psi);
+             }, "s"_a, "omegas"_a, "weights"_a, "syn_rates"_a = VecS{1.0}, "syn_weights"_a = VecS{1.0},
+             "custom_branch_lengths"_a = std::nullopt, "delta"_a = 0.0, "psi"_a = 0.0)
+        .def("compute_expected_syn_weights", [](const BUSTEDAnalyzer& b, Scalar s, const VecS& omegas, const VecS& weights,
+                                                const VecS& syn_rates, const VecS& syn_weights, std::optional<VecS> custom,
+                                                Scalar delta, Scalar psi) {
+                 py::gil_scoped_release rel;
+                 return b.compute_expected_syn_weights(s, omegas, weights, syn_rates, syn_weights, custom ? &*custom : nullptr, delta,
+                                                       psi);
+             }, "s"_a, "omegas"_a, "weights"_a, "syn_rates"_a, "syn_weights"_a, "custom_branch_lengths"_a = std::nullopt,
+             "delta"_a = 0.0, "psi"_a = 0.0);
 
     // MEME (bindings.cpp of the reference: MEMESiteResult / MEMEAnalyzer)
     using hyphy::analyses::MEMEAnalyzer;

@@ -2,9 +2,10 @@
 
 Re-exports the core types and likelihood entry points of the reference
 package (python/hyphy3/__init__.py) from the device-backed _hyphy3 module.
-Of the analysis drivers, FELAnalyzer and MEMEAnalyzer (every branch tested)
-and MG94Fitter run on the device; the others (BUSTED EM, aBSREL, RELAX, ...)
-are not part of this package.
+Of the analysis drivers, FELAnalyzer and MEMEAnalyzer (every branch tested),
+MG94Fitter and the likelihood core of BUSTEDAnalyzer (evaluate_log_l and the
+EM expectation steps) run on the device; the others (BUSTED's fit driver,
+aBSREL, RELAX, ...) are not part of this package.
 """
 import os
 import sys
@@ -16,6 +17,7 @@ if _pydir not in sys.path:
 
 from _hyphy3 import (  # noqa: E402
     Alignment,
+    BUSTEDAnalyzer,
     FELAnalyzer,
     FELSettings,
     FELSiteResult,

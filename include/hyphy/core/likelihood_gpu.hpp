@@ -336,7 +336,9 @@ public:
         const std::vector<Scalar>& omegas, const std::vector<Scalar>& weights,
         const std::vector<Scalar>& syn_rates = {1.0}, const std::vector<Scalar>& syn_weights = {1.0},
         const std::vector<bool>* is_test_branch = nullptr, Scalar omega_bg = -1.0,
-        bool want_gradients = true, bool zero_likelihood_sentinel = false) {
+        bool want_gradients = true, bool zero_likelihood_sentinel = false, bool direction_gradients = true) {
+        // direction_gradients = false: branch, class-weight and rate-weight gradients only (no
+        // omega / theta directions, so no directional products are installed or evaluated)
         auto& eng = gpu_detail::Engine::get();
         const GeneticCode& code = aln.code ? *aln.code : *GeneticCode::universal();
         const int S = code.num_sense_codons, K = int(omegas.size()), M = int(syn_rates.size());
@@ -368,9 +370,11 @@ public:
         key = gpu_detail::fnv(key, syn_rates.data(), syn_rates.size() * 8);
         key = gpu_detail::fnv(key, syn_weights.data(), syn_weights.size() * 8);
         key = gpu_detail::fnv(key, it.data(), it.size());
-        const double flags[4] = {omega_bg, double(want_gradients), double(zero_likelihood_sentinel), double(get_precision())};
+        const bool dirs = want_gradients && direction_gradients;
+        const double flags[5] = {omega_bg, double(want_gradients), double(zero_likelihood_sentinel), double(get_precision()),
+                                 double(dirs)};
         key = gpu_detail::fnv(key, flags, sizeof(flags));
-        const int n_dirs_expected = want_gradients ? K + (has_bg ? 1 : 0) + 5 : 0;
+        const int n_dirs_expected = dirs ? K + (has_bg ? 1 : 0) + 5 : 0;
         if (eng.installed(pr) != key) {
         for (auto& p : ps) mp.add(eng.model(p, aln));
         auto add_dir = [&](int only_model, const std::vector<std::vector<double>>& per_model) {
@@ -380,7 +384,7 @@ public:
             }
             ++ndirs;
         };
-        if (want_gradients) {
+        if (dirs) {
             std::vector<std::vector<double>> db(nm);
             for (int k = 0; k < nm; ++k) db[size_t(k)] = gpu_detail::dq_beta(ps[size_t(k)], aln.pos_nuc_frequencies, code);
             for (int k = 0; k < K; ++k) add_dir(k, db);
@@ -420,7 +424,7 @@ public:
         if (want_gradients) want |= H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL;
         eng.check(h3g_eval(pr, bl.data(), want, &r));
         res.log_likelihood = r.lnl;
-        if (want_gradients) {
+        if (dirs) {
             res.grad_omegas.assign(gd.begin(), gd.begin() + K);
             size_t q = size_t(K);
             if (has_bg) res.grad_omega_bg = gd[q++];

@@ -1465,4 +1465,107 @@ inline MemeRun meme_run(const Tree& tr, const Alignment& a, const Params& base, 
     return run;
 }
 
+// ------------------------------------------------------------ BUSTED E-steps
+// busted.hpp:509-660 (evaluate_log_l), :662-975 (compute_expected_weights) and
+// :978-1134 (compute_expected_syn_weights) without the error sink (eps_sink = 0)
+// and without bridge resolutions.  Test branches mix the K omega classes at
+// the P level, other branches use the background model; synonymous-rate
+// classes are separate passes combined per site by log-sum-exp.  bl are the
+// branch lengths already multiplied by s (raw time, alpha_m * bl per class).
+struct BustedEStep {
+    double lnl = 0.0;
+    std::vector<double> weights, syn_weights, pattern_ll;
+};
+inline BustedEStep busted_estep(const Tree& tr, const Alignment& a, const Params& base, const std::vector<double>& bl,
+                                const std::vector<double>& omegas, const std::vector<double>& weights,
+                                const std::vector<double>& syn_rates, const std::vector<double>& syn_weights,
+                                const std::vector<char>& is_test, double omega_bg) {
+    const int S = a.code.S, n = tr.n(), P = a.P, K = int(omegas.size()), M = int(syn_rates.size());
+    const auto l2t = leaf_map(tr, a);
+    auto test = [&](int b) { return is_test.empty() ? b != tr.root : bool(is_test[b]); };
+    int n_test = 0;
+    for (int b = 0; b < n; ++b) if (b != tr.root && test(b)) ++n_test;
+    std::vector<MG94> mk(K);
+    for (int k = 0; k < K; ++k) { Params q = base; q.alpha = 1.0; q.beta = omegas[k]; mk[k].update(q, a.pos_freq, a.pi, a.code); }
+    MG94 mbg;
+    if (n_test + 1 < n) { Params q = base; q.alpha = 1.0; q.beta = omega_bg; mbg.update(q, a.pos_freq, a.pi, a.code); }
+    std::vector<std::vector<std::vector<Mat>>> Pc(M, std::vector<std::vector<Mat>>(K, std::vector<Mat>(n, Mat::eye(S))));
+    std::vector<std::vector<Mat>> Pmix(M, std::vector<Mat>(n, Mat::eye(S)));
+    for (int m = 0; m < M; ++m)
+        for (int b = 0; b < n; ++b) {
+            if (b == tr.root) continue;
+            const double t = syn_rates[m] * bl[b];
+            for (int k = 0; k < K; ++k) Pc[m][k][b] = mk[k].P(t);
+            if (test(b)) {
+                Pmix[m][b] = Mat(S, S);
+                for (int k = 0; k < K; ++k)
+                    for (size_t e = 0; e < Pmix[m][b].a.size(); ++e) Pmix[m][b].a[e] += weights[k] * Pc[m][k][b].a[e];
+            } else {
+                Pmix[m][b] = mbg.P(t);
+            }
+        }
+    BustedEStep r;
+    r.pattern_ll.assign(P, -1e20);
+    std::vector<std::vector<double>> wacc(K, std::vector<double>(P, 0.0)), sacc(M, std::vector<double>(P, 0.0));
+    std::vector<double> wt_w(P, 0.0), wt_s(P, 0.0);
+    #pragma omp parallel num_threads(n_threads_for(P))
+    {
+        std::vector<Pass> w(M);
+        std::vector<double> pd(S);
+        #pragma omp for schedule(static)
+        for (int p = 0; p < P; ++p) {
+            const double wt = a.weights[p];
+            std::vector<double> post(M, 0.0);
+            double mx = -1e300;
+            for (int m = 0; m < M; ++m) {
+                if (syn_weights[m] <= 1e-12 && M > 1) continue;
+                inside_outside(tr, a, p, l2t, Pmix[m], a.pi, S, w[m], true);
+                if (w[m].L > 0.0) mx = std::max(mx, (M > 1 ? std::log(syn_weights[m]) : 0.0) + w[m].logL);
+            }
+            if (!(mx > -1e19)) continue;
+            double se = 0.0;
+            for (int m = 0; m < M; ++m)
+                if ((M == 1 || syn_weights[m] > 1e-12) && w[m].L > 0.0) { post[m] = std::exp((M > 1 ? std::log(syn_weights[m]) : 0.0) + w[m].logL - mx); se += post[m]; }
+            if (!(se > 0.0)) continue;
+            r.pattern_ll[p] = M == 1 ? w[0].logL : mx + std::log(se);
+            for (int m = 0; m < M; ++m) { post[m] /= se; sacc[m][p] = wt * post[m]; }
+            wt_s[p] = wt;
+            // busted.hpp:822-860: per test branch and class, w_k * post_m * V . (P_k D) / L_m
+            for (int b = 0; b < n; ++b) {
+                if (b == tr.root || !test(b)) continue;
+                for (int k = 0; k < K; ++k)
+                    for (int m = 0; m < M; ++m) {
+                        if (post[m] <= 1e-12 || !(w[m].L > 0.0)) continue;
+                        matvec(Pc[m][k][b], w[m].D[b].data(), pd.data());
+                        double dot = 0.0;
+                        for (int i = 0; i < S; ++i) dot += w[m].V[b][i] * pd[i];
+                        wacc[k][p] += wt * weights[k] * post[m] * dot / w[m].L;
+                    }
+                wt_w[p] += wt;
+            }
+        }
+    }
+    Neumaier ll;
+    for (int p = 0; p < P; ++p) ll.add(a.weights[p] * r.pattern_ll[p]);
+    r.lnl = ll.value();
+    auto normalise = [](std::vector<double> acc, double total, const std::vector<double>& old) {
+        if (!(total > 0.0)) return old;
+        double sum = 0.0;
+        for (auto& x : acc) { x = std::clamp(x / total, 1e-6, 1.0 - 1e-6); sum += x; }
+        for (auto& x : acc) x /= sum;
+        return acc;
+    };
+    std::vector<double> wk(K, 0.0), sm(M, 0.0);
+    double tw = 0.0, ts = 0.0;
+    for (int p = 0; p < P; ++p) {
+        for (int k = 0; k < K; ++k) wk[k] += wacc[k][p];
+        for (int m = 0; m < M; ++m) sm[m] += sacc[m][p];
+        tw += wt_w[p];
+        ts += wt_s[p];
+    }
+    r.weights = K <= 1 ? std::vector<double>{1.0} : normalise(wk, tw, weights);
+    r.syn_weights = M <= 1 ? std::vector<double>{1.0} : normalise(sm, ts, syn_weights);
+    return r;
+}
+
 } // namespace h3o

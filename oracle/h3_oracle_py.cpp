@@ -219,6 +219,23 @@ PYBIND11_MODULE(h3oracle, m) {
         return meme_ebf_at(t, a, params_from(p), bl, pattern, alpha, omega1, p1, beta_plus);
     }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths"), py::arg("pattern"), py::arg("alpha"),
        py::arg("omega1"), py::arg("p1"), py::arg("beta_plus"));
+    m.def("busted_estep", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<double>& bl,
+                             const std::vector<double>& omegas, const std::vector<double>& weights,
+                             const std::vector<double>& syn_rates, const std::vector<double>& syn_weights,
+                             const std::vector<int>& is_test, double omega_bg) {
+        std::vector<char> it(is_test.begin(), is_test.end());
+        const Params base = params_from(p);        // reads Python objects: before the GIL is released
+        BustedEStep r;
+        { py::gil_scoped_release rel; r = busted_estep(t, a, base, bl, omegas, weights, syn_rates, syn_weights, it, omega_bg); }
+        py::dict d;
+        d["lnl"] = r.lnl;
+        d["weights"] = r.weights;
+        d["syn_weights"] = r.syn_weights;
+        d["pattern_ll"] = r.pattern_ll;
+        return d;
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths"), py::arg("omegas"), py::arg("weights"),
+       py::arg("syn_rates") = std::vector<double>{1.0}, py::arg("syn_weights") = std::vector<double>{1.0},
+       py::arg("is_test") = std::vector<int>{}, py::arg("omega_bg") = -1.0);
     m.def("set_threads", [](int n) {
 #ifdef _OPENMP
         omp_set_num_threads(n);
