@@ -2,7 +2,8 @@
 //
 // Per evaluation (one CUDA stream, level-synchronous over the tree):
 //   k_build_P      P_{m,b} = sum_k c_k clamp(U_k diag(e^{lam_k tau}) V_k), dP = d P / d t
-//                  (rate_matrix.hpp:251-257, likelihood.hpp:1118-1127, busted.hpp:1191-1216)
+//                  (rate_matrix.hpp:251-257, likelihood.hpp:1118-1127, busted.hpp:1191-1216),
+//                  FP64 tensor-core products
 //   k_inside       one launch per height level: D_u = prod_c P_c D_c with power-of-two
 //                  rescaling, then the message P_u D_u for the parent (likelihood.hpp:500-597)
 //   k_root         L = pi . D_root, log-sum-exp over rate classes, per-pattern scale
@@ -83,114 +84,132 @@ __device__ __forceinline__ void stage_matrix(double* __restrict__ s, const doubl
     for (int k = tid; k < SP2 / 2; k += nthr) s2[k] = __ldg(g2 + k);
 }
 
+// --------------------------------------------------- FP64 tensor-core products
+// 64x64x64 products on the FP64 tensor cores (mma.sync m8n8k4 .f64; tcgen05 has no FP64
+// kind) by the 8 warps of a 256-thread CTA: warp w owns rows 16(w/2) .. +16 and columns
+// 32(w%2) .. +32 as 2 x 4 tiles of 8x8, operands and results stay in registers between
+// the k steps.  Both operands are row-major in shared memory with a padded stride of 68
+// doubles: the fragment loads of a half-warp, (row + lane/4) * 68 + k + lane%4 and
+// (k + lane%4) * 68 + col + lane/4, fall in 16 different banks.
+constexpr int LDM = SP + 4;
+
+struct Frag64 {
+    double v[2][4][2];        // C[r0 + 8i + lane/4][c0 + 8j + 2(lane%4) + e]
+};
+
+__device__ __forceinline__ void frag_zero(Frag64& f) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) f.v[i][j][0] = f.v[i][j][1] = 0.0;
+}
+// position of f.v[i][j][e] in the 64x64 result
+__device__ __forceinline__ int frag_row(int i) { return 16 * (int(threadIdx.x) >> 6) + 8 * i + ((threadIdx.x & 31) >> 2); }
+__device__ __forceinline__ int frag_col(int j, int e) {
+    return 32 * ((int(threadIdx.x) >> 5) & 1) + 8 * j + 2 * (threadIdx.x & 3) + e;
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+// c = X Y, X and Y [64][LDM] in shared memory
+__device__ __forceinline__ void mm64(const double* __restrict__ X, const double* __restrict__ Y, Frag64& c) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int r0 = 16 * (wp >> 1), c0 = 32 * (wp & 1), g = lane >> 2, q = lane & 3;
+    frag_zero(c);
+#pragma unroll 4
+    for (int k = 0; k < SP; k += 4) {
+        double a[2], b[4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) a[i] = X[(r0 + 8 * i + g) * LDM + k + q];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Y[(k + q) * LDM + c0 + 8 * j + g];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dmma(c.v[i][j][0], c.v[i][j][1], a[i], b[j]);
+    }
+}
+
 // ------------------------------------------------------------------ build P
 // grid (n, M): one CTA per branch and rate class computes the whole 64x64
 // P_{m,b} = sum_k c_k clamp(U_k diag(e^{lam_k tau}) V_k) and
-// dP_{m,b} = sum_k c_k r_m conv_k Q_k clamp(P_k), model by model.  Thread t owns
-// the 4x4 block rows 4(t/16).., columns 4(t%16)..; operands are staged in
-// shared memory so every k step reads two contiguous 32-byte row pieces
-// (a broadcast of the two row blocks of the warp and 16 consecutive column blocks).
-// dynamic smem: UE (U^T scaled by e, then Q^T), V, clamp(P_k): 3 x 64 x 64 doubles.
+// dP_{m,b} = sum_k c_k r_m conv_k Q_k clamp(P_k), model by model, as two FP64
+// tensor-core products per model (mm64).
+// dynamic smem: 2 x 64 x LDM doubles (U e then Q; V then clamp(P_k)).
 __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    double* sUE = sm;             // sUE[l][r] = U[r][l] e_l, later Q^T: sUE[l][r] = Q[r][l]
-    double* sV = sm + SP2;        // sV[l][c] = V[l][c]
-    double* sPk = sm + 2 * SP2;   // sPk[l][c] = clamp(P_k)[l][c]
+    double* sX = sm;                 // U_k diag(e), then Q_k
+    double* sY = sm + SP * LDM;      // V_k, then clamp(P_k)
     __shared__ double se[SP];
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
     if (b == t.root) return;
-    const int r0 = 4 * (tid >> 4), c0 = 4 * (tid & 15);
     const bool test = md.is_test == nullptr || md.is_test[b] != 0;
     const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
-    double accP[4][4], accD[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) accP[a][c] = accD[a][c] = 0.0;
+    Frag64 accP, accD;
+    frag_zero(accP);
+    frag_zero(accD);
     for (int k = k0; k < k1; ++k) {
         const double cw = test ? md.class_w[k] : 1.0;
         const double cv = time_conv(md, k);
         const double rate = md.rates[m];
         const double tau = rate * w.bl[b] * cv;
-        __syncthreads();
+        __syncthreads();                          // the previous model's products are done
         if (tid < SP) se[tid] = exp(md.lam[size_t(k) * SP + tid] * tau);
-        stage_matrix(sV, md.V + size_t(k) * SP2, tid, 256);
         __syncthreads();
         {
-            const double2* g2 = reinterpret_cast<const double2*>(md.UT + size_t(k) * SP2);
-            double2* s2 = reinterpret_cast<double2*>(sUE);
-            for (int e = tid; e < SP2 / 2; e += 256) {
-                const double f = se[e >> 5];           // row l = (2e) / 64 of U^T
-                double2 x = __ldg(g2 + e);
-                x.x *= f; x.y *= f;
-                s2[e] = x;
+            const double* U = md.U + size_t(k) * SP2;
+            const double* V = md.V + size_t(k) * SP2;
+            for (int e = tid; e < SP2; e += 256) {
+                const int r = e >> 6, l = e & 63;
+                sX[r * LDM + l] = __ldg(U + e) * se[l];
+                sY[r * LDM + l] = __ldg(V + e);
             }
         }
         __syncthreads();
-        double pk[4][4];
+        Frag64 pk;
+        mm64(sX, sY, pk);                         // P_k = (U e) V
+        __syncthreads();                          // every warp is done with U e and V
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) pk[a][c] = 0.0;
-#pragma unroll 4
-        for (int l = 0; l < SP; ++l) {
-            const double2 u01 = *reinterpret_cast<const double2*>(sUE + l * SP + r0);
-            const double2 u23 = *reinterpret_cast<const double2*>(sUE + l * SP + r0 + 2);
-            const double2 v01 = *reinterpret_cast<const double2*>(sV + l * SP + c0);
-            const double2 v23 = *reinterpret_cast<const double2*>(sV + l * SP + c0 + 2);
-            const double uu[4] = {u01.x, u01.y, u23.x, u23.y}, vv[4] = {v01.x, v01.y, v23.x, v23.y};
+            for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) pk[a][c] = fma(uu[a], vv[c], pk[a][c]);
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                pk[a][c] = fmax(pk[a][c], 0.0);
-                accP[a][c] = fma(cw, pk[a][c], accP[a][c]);
-            }
-            *reinterpret_cast<double2*>(sPk + (r0 + a) * SP + c0) = make_double2(pk[a][0], pk[a][1]);
-            *reinterpret_cast<double2*>(sPk + (r0 + a) * SP + c0 + 2) = make_double2(pk[a][2], pk[a][3]);
+                for (int e = 0; e < 2; ++e) {
+                    const double x = fmax(pk.v[i][j][e], 0.0);
+                    accP.v[i][j][e] = fma(cw, x, accP.v[i][j][e]);
+                    sY[frag_row(i) * LDM + frag_col(j, e)] = x;
+                }
+        {
+            const double* Q = md.Q + size_t(k) * SP2;
+            for (int e = tid; e < SP2; e += 256) sX[(e >> 6) * LDM + (e & 63)] = __ldg(Q + e);
         }
         __syncthreads();
-        stage_matrix(sUE, md.QT + size_t(k) * SP2, tid, 256);
-        __syncthreads();
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) pk[a][c] = 0.0;
-#pragma unroll 4
-        for (int l = 0; l < SP; ++l) {            // (Q clamp(P_k))[r][c] = sum_l Q[r][l] P_k[l][c]
-            const double2 q01 = *reinterpret_cast<const double2*>(sUE + l * SP + r0);
-            const double2 q23 = *reinterpret_cast<const double2*>(sUE + l * SP + r0 + 2);
-            const double2 p01 = *reinterpret_cast<const double2*>(sPk + l * SP + c0);
-            const double2 p23 = *reinterpret_cast<const double2*>(sPk + l * SP + c0 + 2);
-            const double qq[4] = {q01.x, q01.y, q23.x, q23.y}, pp[4] = {p01.x, p01.y, p23.x, p23.y};
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) pk[a][c] = fma(qq[a], pp[c], pk[a][c]);
-        }
+        Frag64 qp;
+        mm64(sX, sY, qp);                         // Q clamp(P_k)
         const double sc = cw * rate * cv;
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) accD[a][c] = fma(sc, pk[a][c], accD[a][c]);
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) accD.v[i][j][e] = fma(sc, qp.v[i][j][e], accD.v[i][j][e]);
     }
     const size_t o = mat_off(m, b, t.n);
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int r = r0 + a;
-        *reinterpret_cast<double2*>(w.P + o + r * SP + c0) = make_double2(accP[a][0], accP[a][1]);
-        *reinterpret_cast<double2*>(w.P + o + r * SP + c0 + 2) = make_double2(accP[a][2], accP[a][3]);
-        *reinterpret_cast<double2*>(w.dP + o + r * SP + c0) = make_double2(accD[a][0], accD[a][1]);
-        *reinterpret_cast<double2*>(w.dP + o + r * SP + c0 + 2) = make_double2(accD[a][2], accD[a][3]);
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) w.PT[o + (c0 + c) * SP + r] = accP[a][c];
-    }
+        for (int j = 0; j < 4; ++j) {
+            const int r = frag_row(i), c = frag_col(j, 0);
+            *reinterpret_cast<double2*>(w.P + o + r * SP + c) = make_double2(accP.v[i][j][0], accP.v[i][j][1]);
+            *reinterpret_cast<double2*>(w.dP + o + r * SP + c) = make_double2(accD.v[i][j][0], accD.v[i][j][1]);
+            w.PT[o + c * SP + r] = accP.v[i][j][0];
+            w.PT[o + (c + 1) * SP + r] = accP.v[i][j][1];
+        }
 }
 
 // Row sums of P_{m,b} (the message of a leaf with missing data).  grid (n, M), block 64.
@@ -542,34 +561,27 @@ __global__ void __launch_bounds__(256) k_areduce(Topo t, Model md, Work w) {
 // ------------------------------------------------------------------ frechet
 // grid (G, M, nmod): CTA (g, m, k) walks the branches b = g, g+G, ... that use
 // model k (test branches for k < K, background branches for k = K), computes
-// the spectral transform At = U_k^T A_{m,b} V_k^T and accumulates
-// H += c_k At o E(lambda, tau_b) in registers (likelihood.hpp:1428-1471), plus
-// the diagonal sums for d/dc_k and the d mu term.  Thread t owns the 4x4 block
-// rows 4(t/16).., columns 4(t%16).. of every 64x64 product, so shared-memory
-// reads are consecutive (or broadcast) across a warp.
-// block 256, dynamic smem (64*64 (A, then T^T) + 64*64 (V^T) + 64*64 (U_k)) doubles.
+// the spectral transform At = U_k^T A_{m,b} V_k^T (two FP64 tensor-core products,
+// mm64) and accumulates H += c_k At o E(lambda, tau_b) in registers
+// (likelihood.hpp:1428-1471), plus the diagonal sums for d/dc_k and the d mu term.
+// block 256, dynamic smem 3 x 64 x LDM doubles (U_k^T, V_k^T, A then T).
 __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    double* sA = sm;                  // A_{m,b}, then (U^T A)^T : sTT[l][r] = T[r][l]
-    double* sTT = sA;
-    double* sVT = sm + SP2;           // V_k^T : sVT[l][c] = V[c][l]
-    double* sU = sm + 2 * SP2;        // U_k
+    double* sUT = sm;                     // U_k^T: sUT[r][l] = U[l][r]
+    double* sVT = sm + SP * LDM;          // V_k^T: sVT[l][c] = V[c][l]
+    double* sA = sm + 2 * SP * LDM;       // A_{m,b}, then T = U^T A
     __shared__ double se[SP];
     __shared__ double red[8];
     const int g = blockIdx.x, m = blockIdx.y, k = blockIdx.z, tid = threadIdx.x, n = t.n, M = md.M;
-    const int r0 = 4 * (tid >> 4), c0 = 4 * (tid & 15);
-    stage_matrix(sU, md.U + size_t(k) * SP2, tid, 256);
     for (int e = tid; e < SP2; e += 256) {
-        const int c = e >> 6, l = e & 63;                 // V[c][l], coalesced read
-        sVT[l * SP + c] = md.V[size_t(k) * SP2 + e];
+        const int x = e >> 6, y = e & 63;                 // coalesced reads of U[x][y], V[x][y]
+        sUT[y * LDM + x] = md.U[size_t(k) * SP2 + e];
+        sVT[y * LDM + x] = md.V[size_t(k) * SP2 + e];
     }
     const double* lam = md.lam + size_t(k) * SP;
-    double H[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) H[a][c] = 0.0;
+    Frag64 H;
+    frag_zero(H);
     double dg = 0.0, dq = 0.0;
     for (int b = g; b < n; b += G) {
         if (b == t.root) continue;
@@ -577,68 +589,49 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
         if ((k < md.K) != test) continue;
         const double cw = test ? md.class_w[k] : 1.0;
         const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
-        __syncthreads();
-        stage_matrix(sA, w.Afull + (size_t(b) * M + m) * SP2, tid, 256);
+        __syncthreads();                                  // the previous branch is done with sA
+        {
+            const double* A = w.Afull + (size_t(b) * M + m) * SP2;
+            for (int e = tid; e < SP2; e += 256) sA[(e >> 6) * LDM + (e & 63)] = __ldg(A + e);
+        }
         if (tid < SP) se[tid] = exp(lam[tid] * tau);
         __syncthreads();
-        double acc[4][4];
+        Frag64 T;
+        mm64(sUT, sA, T);                                 // T = U^T A
+        __syncthreads();                                  // every warp is done with A: T overwrites it
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
-#pragma unroll 4
-        for (int l = 0; l < SP; ++l) {          // T[r][c] = sum_l U[l][r] A[l][c]
-            const double2 u01 = *reinterpret_cast<const double2*>(sU + l * SP + r0);
-            const double2 u23 = *reinterpret_cast<const double2*>(sU + l * SP + r0 + 2);
-            const double2 a01 = *reinterpret_cast<const double2*>(sA + l * SP + c0);
-            const double2 a23 = *reinterpret_cast<const double2*>(sA + l * SP + c0 + 2);
-            const double uu[4] = {u01.x, u01.y, u23.x, u23.y}, aa[4] = {a01.x, a01.y, a23.x, a23.y};
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[a][c] = fma(uu[a], aa[c], acc[a][c]);
-        }
-        __syncthreads();                        // every thread is done with A: T^T overwrites it
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) sTT[(c0 + c) * SP + r0 + a] = acc[a][c];
+            for (int j = 0; j < 4; ++j)
+                *reinterpret_cast<double2*>(sA + frag_row(i) * LDM + frag_col(j, 0)) = make_double2(T.v[i][j][0], T.v[i][j][1]);
         __syncthreads();
+        Frag64 At;
+        mm64(sA, sVT, At);                                // At = T V^T
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < 2; ++i) {
+            const int r = frag_row(i);
+            const double li = lam[r], ei = se[r];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
-#pragma unroll 4
-        for (int l = 0; l < SP; ++l) {          // At[r][c] = sum_l T[r][l] V[c][l]
-            const double2 t01 = *reinterpret_cast<const double2*>(sTT + l * SP + r0);
-            const double2 t23 = *reinterpret_cast<const double2*>(sTT + l * SP + r0 + 2);
-            const double2 v01 = *reinterpret_cast<const double2*>(sVT + l * SP + c0);
-            const double2 v23 = *reinterpret_cast<const double2*>(sVT + l * SP + c0 + 2);
-            const double tt[4] = {t01.x, t01.y, t23.x, t23.y}, vv[4] = {v01.x, v01.y, v23.x, v23.y};
+            for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) acc[a][c] = fma(tt[a], vv[c], acc[a][c]);
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int i = r0 + a;
-            const double li = lam[i], ei = se[i];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int j = c0 + c;
-                const double d = li - lam[j], ej = se[j];
-                const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
-                H[a][c] = fma(cw * acc[a][c], E, H[a][c]);
-                if (i == j) { if (test) dg += ei * acc[a][c]; dq += cw * tau * li * ei * acc[a][c]; }
-            }
+                for (int e = 0; e < 2; ++e) {
+                    const int c = frag_col(j, e);
+                    const double d = li - lam[c], ej = se[c], a = At.v[i][j][e];
+                    const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
+                    H.v[i][j][e] = fma(cw * a, E, H.v[i][j][e]);
+                    if (r == c) {
+                        if (test) dg += ei * a;
+                        dq += cw * tau * li * ei * a;
+                    }
+                }
         }
     }
     double* Hp = w.Hpart + ((size_t(k) * M + m) * G + g) * SP2;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) Hp[(r0 + a) * SP + c0 + c] = H[a][c];
+        for (int j = 0; j < 4; ++j)
+            *reinterpret_cast<double2*>(Hp + frag_row(i) * SP + frag_col(j, 0)) = make_double2(H.v[i][j][0], H.v[i][j][1]);
     dg = block_sum_256(dg, red);
     dq = block_sum_256(dq, red);
     if (tid == 0) {
@@ -761,11 +754,10 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
 }
 
 // ------------------------------------------------------------------ launch
-static size_t smem_bytes(int mats) { return size_t(mats) * SP2 * sizeof(double); }
 static const size_t kPruneSmem = (SP2 + SP * kTileP + kGroups * kTileP) * sizeof(double);
 static const size_t kDirSmem = (2 * SP2 + 16 * SP) * sizeof(double);
-static const size_t kBuildSmem = (3 * SP2) * sizeof(double);
-static const size_t kFrechetSmem = (3 * SP2) * sizeof(double);
+static const size_t kBuildSmem = size_t(2) * SP * LDM * sizeof(double);
+static const size_t kFrechetSmem = size_t(3) * SP * LDM * sizeof(double);
 
 void fp64_configure() {
     cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
