@@ -56,6 +56,9 @@ struct h3g_problem {
     int2* d_kdesc = nullptr;
     int4* d_in_info = nullptr;
     int4* d_out_info = nullptr;
+    int* d_chains = nullptr;           // [in_next | in_heads | out_next | out_heads]
+    int n_in_heads = 0, n_out_heads = 0;
+    size_t off_in_heads = 0, off_out_next = 0, off_out_heads = 0;
     int8_t* d_states = nullptr;
     uint64_t* d_masks = nullptr;
     double* d_w = nullptr;
@@ -110,6 +113,8 @@ struct h3g_problem {
         t.ch_off = d_ch_off; t.ch = d_ch; t.parent = d_parent; t.iidx = d_iidx; t.leaf = d_leaf; t.taxon = d_taxon;
         t.states = d_states; t.masks = d_masks; t.w = d_w;
         t.kdesc = d_kdesc; t.in_info = d_in_info; t.out_info = d_out_info;
+        t.in_next = d_chains; t.in_heads = d_chains + off_in_heads;
+        t.out_next = d_chains + off_out_next; t.out_heads = d_chains + off_out_heads;
         t.all_mask = S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1);
         return t;
     }
@@ -284,6 +289,51 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
             out_info[2 * k] = make_int4(c, u, pr->iidx[u], is_leaf[c] ? -1 : pr->iidx[c]);
             out_info[2 * k + 1] = make_int4(pr->ch_off[u], pr->ch_off[u + 1], 0, 0);
         }
+        // chains (see Topo): inside, a node whose parent has no other internal child hands its
+        // message to the parent in the same CTA; outside, a node continues with its deepest
+        // internal child.  Heads keep the pass order, so every wait is on an earlier claim.
+        std::vector<int> in_pos(n, -1), out_pos(n, -1);
+        for (size_t k = 0; k < pr->in_nodes.size(); ++k) in_pos[pr->in_nodes[k]] = int(k);
+        for (size_t k = 0; k < pr->out_nodes.size(); ++k) out_pos[pr->out_nodes[k]] = int(k);
+        std::vector<int> n_int(n, 0);
+        for (int i = 0; i < n; ++i)
+            for (int c : kids[i]) n_int[i] += is_leaf[c] ? 0 : 1;
+        std::vector<int> in_next(pr->in_nodes.size(), -1), in_heads, out_next(pr->out_nodes.size(), -1), out_heads;
+        std::vector<char> fused_in(pr->in_nodes.size(), 0), fused_out(pr->out_nodes.size(), 0);
+        for (size_t k = 0; k < pr->in_nodes.size(); ++k) {
+            const int u = pr->in_nodes[k], par = parent[u];
+            if (par >= 0 && n_int[par] == 1) {
+                in_next[k] = in_pos[par];
+                fused_in[size_t(in_pos[par])] = 1;
+            }
+        }
+        for (size_t k = 0; k < pr->in_nodes.size(); ++k)
+            if (!fused_in[k]) in_heads.push_back(int(k));
+        for (size_t k = 0; k < pr->out_nodes.size(); ++k) {
+            const int c = pr->out_nodes[k];
+            if (is_leaf[c]) continue;
+            int best = -1;
+            for (int d : kids[c])
+                if (!is_leaf[d] && (best < 0 || height[d] > height[best])) best = d;
+            if (best >= 0) {
+                out_next[k] = out_pos[best];
+                fused_out[size_t(out_pos[best])] = 1;
+            }
+        }
+        for (size_t k = 0; k < pr->out_nodes.size(); ++k)
+            if (!fused_out[k]) out_heads.push_back(int(k));
+        pr->n_in_heads = int(in_heads.size());
+        pr->n_out_heads = int(out_heads.size());
+        std::vector<int> chains(in_next);
+        pr->off_in_heads = chains.size();
+        chains.insert(chains.end(), in_heads.begin(), in_heads.end());
+        pr->off_out_next = chains.size();
+        chains.insert(chains.end(), out_next.begin(), out_next.end());
+        pr->off_out_heads = chains.size();
+        chains.insert(chains.end(), out_heads.begin(), out_heads.end());
+        if (chains.empty()) chains.push_back(-1);
+        H3G_TRY_CUDA(ctx, A.alloc(&pr->d_chains, chains.size()));
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_chains, chains.data(), chains.size() * sizeof(int), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_kdesc, kdesc.size()));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_in_info, in_info.size()));
         H3G_TRY_CUDA(ctx, A.alloc(&pr->d_out_info, out_info.size()));
@@ -612,7 +662,7 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
     int l = 0;
     if (mixed) {
         // one persistent launch over every level, per-tile dependencies
-        l = launch_inside_mixed(t, md, w, pr->mw, pr->d_in_nodes, int(pr->in_nodes.size()), s);
+        l = launch_inside_mixed(t, md, w, pr->mw, pr->n_in_heads, s);
     } else {
         for (size_t lv = 0; lv + 1 < pr->in_off.size(); ++lv) {
             const int cnt = pr->in_off[lv + 1] - pr->in_off[lv];
@@ -625,7 +675,7 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
     if (grads) {
         l = 0;
         if (mixed) {
-            l = launch_outside_mixed(t, md, w, pr->mw, pr->d_out_nodes, int(pr->out_nodes.size()), s);
+            l = launch_outside_mixed(t, md, w, pr->mw, pr->n_out_heads, s);
         } else {
             for (size_t lv = 0; lv + 1 < pr->out_off.size(); ++lv) {
                 const int cnt = pr->out_off[lv + 1] - pr->out_off[lv];

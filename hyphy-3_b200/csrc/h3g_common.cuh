@@ -69,6 +69,12 @@ struct Topo {
     const int2* kdesc;       // [children CSR] {child, code}: code = taxon (>= 0) or -1 for a leaf, -(2 + iidx) for an internal child
     const int4* in_info;     // [internal nodes, inside order] {u, iidx[u], first child slot, end}
     const int4* out_info;    // [2 x children, outside order] {c, u, iidx[u], iidx[c] or -1}, {first sibling slot, end, 0, 0}
+    // chains of the persistent passes: the items are chain heads; a CTA carries a chain's
+    // message in registers from one node to the next
+    const int* in_next;      // [inside position] position of the parent when its only internal child is this node, else -1
+    const int* in_heads;     // [chains] inside position of each chain's first node, inside order
+    const int* out_next;     // [outside position] position of this node's deepest internal child, else -1
+    const int* out_heads;    // [chains] outside position of each chain's first node, outside order
 };
 
 struct Model {

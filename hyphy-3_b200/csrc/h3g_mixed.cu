@@ -247,16 +247,20 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
     if (!tc::mbar_wait(&s.bars[1], phase) && (tid & 31) == 0) atomicOr(err, 2);
     tc::tc_fence_after();
     const uint32_t row = tmem + (uint32_t(32 * l.q) << 16) + uint32_t(kSG * l.g);
-    float t16[kKSteps][16];
+    // read back in two halves of 8 columns (fewer live registers)
 #pragma unroll
-    for (int ks = 0; ks < kKSteps; ++ks) tc::tmem_ld16(row + uint32_t(ks * SP), t16[ks]);
-    tc::tmem_wait_ld();
+    for (int h = 0; h < 2; ++h) {
+        float t8[kKSteps][8];
 #pragma unroll
-    for (int i = 0; i < kSG; ++i) {
-        double acc = 0.0;
+        for (int ks = 0; ks < kKSteps; ++ks) tc::tmem_ld8(row + uint32_t(ks * SP + 8 * h), t8[ks]);
+        tc::tmem_wait_ld();
 #pragma unroll
-        for (int ks = 0; ks < kKSteps; ++ks) acc += double(t16[ks][i]);
-        o[i] = float(acc);
+        for (int i = 0; i < 8; ++i) {
+            double acc = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < kKSteps; ++ks) acc += double(t8[ks][i]);
+            o[8 * h + i] = float(acc);
+        }
     }
     tc::tc_fence_before();
     __syncthreads();
@@ -324,6 +328,14 @@ __device__ __forceinline__ void wait_item(const int* flag, int epoch, int* err) 
         __nanosleep(64);
     }
 }
+// all threads: the partials are stored; make them visible and raise the flag
+__device__ __forceinline__ void publish(int* flag, int epoch) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        st_release(flag, epoch);
+    }
+}
 // all threads: the item's partials are stored; make them visible, raise its flag, and
 // claim the CTA's next item in the same step (the item being published waits for nothing
 // more, so holding the next claim meanwhile cannot block anyone)
@@ -340,8 +352,9 @@ __device__ __forceinline__ int publish_and_claim(int* flag, int epoch, int* ctr,
 }
 
 // ------------------------------------------------------------------ inside
-// Persistent: grid min(items, 2 x SMs), block 512; items (node k, m, tile) in the
-// order of t.in_info (internal nodes by increasing height, the root last).
+// Persistent: grid min(items, 2 x SMs), block 512; items (chain, m, tile) in the order of
+// t.in_heads (chains by the height of their first node, the root's last).  A chain runs up
+// the tree while the parent's only internal child is the node just finished.
 __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
@@ -356,56 +369,79 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
     int item = claim(mw.sync + 1, &s_item);
     while (item < n_items) {
         const int tile = item % ntile, rest = item / ntile, m = rest % M;
-        const int4 info = t.in_info[rest / M];
-        const int u = info.x, iu = info.y, k0 = info.z, k1 = info.w;
         const int p = tile * MT + l.r;
         const size_t so = size_t(kSG * l.g) * Pp + p;     // this thread's first state of the pattern column
-        const bool root = u == t.root;
-        if (!root) tc_load_b(s, mw.Bp, mat_off_f(m, u, t.n));
-        if (threadIdx.x == 0)
-            for (int k = k0; k < k1; ++k) {
-                const int code = t.kdesc[k].y;
-                if (code <= -2) wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err);
-            }
-        __syncthreads();
-        // the first two children's messages load together (padding states are zero in every
-        // message), then one product and one renormalisation; further children one at a time
+        int pos = t.in_heads[rest / M];
+        int carried = -1;                                 // the chain's previous node, whose message v holds
         float v[kSG];
-        int E = 0;
-        {
-            const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k0], p, l.g, so);
-            E = s0.E;
-            if (k0 + 1 < k1) {
-                const MsgSrc s1 = msg_src(t, mw, m, M, t.kdesc[k0 + 1], p, l.g, so);
-                float b[kSG];
-                msg_load(s0, v);
-                msg_load(s1, b);
+        int E = 0, iu = 0;
+        for (;;) {
+            const int4 info = t.in_info[pos];
+            const int u = info.x, k0 = info.z, k1 = info.w;
+            iu = info.y;
+            const bool root = u == t.root;
+            if (!root) tc_load_b(s, mw.Bp, mat_off_f(m, u, t.n));
+            if (carried < 0) {
+                if (threadIdx.x == 0)
+                    for (int k = k0; k < k1; ++k) {
+                        const int code = t.kdesc[k].y;
+                        if (code <= -2) wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err);
+                    }
+                __syncthreads();
+                // the first two children's messages load together (padding states are zero in every
+                // message), then one product and one renormalisation; further children one at a time
+                const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k0], p, l.g, so);
+                E = s0.E;
+                if (k0 + 1 < k1) {
+                    const MsgSrc s1 = msg_src(t, mw, m, M, t.kdesc[k0 + 1], p, l.g, so);
+                    float b[kSG];
+                    msg_load(s0, v);
+                    msg_load(s1, b);
 #pragma unroll
-                for (int i = 0; i < kSG; ++i) v[i] *= b[i];
-                E += s1.E;
+                    for (int i = 0; i < kSG; ++i) v[i] *= b[i];
+                    E += s1.E;
+                } else {
+                    msg_load(s0, v);
+                }
+                E += renorm_row(v, s.smax, l);
+                for (int k = k0 + 2; k < k1; ++k) {
+                    const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
+                    float a[kSG];
+                    msg_load(sr, a);
+#pragma unroll
+                    for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+                    E += sr.E + renorm_row(v, s.smax, l);
+                }
             } else {
-                msg_load(s0, v);
-            }
-            E += renorm_row(v, s.smax, l);
-        }
-        for (int k = k0 + 2; k < k1; ++k) {
-            const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
-            float a[kSG];
-            msg_load(sr, a);
+                // a chain node: its only internal child is the previous node (message in v, exponent E);
+                // the other children are leaves
+                for (int k = k0; k < k1; ++k) {
+                    const int2 d = t.kdesc[k];
+                    if (d.x == carried) continue;
+                    const MsgSrc sr = msg_src(t, mw, m, M, d, p, l.g, so);
+                    float a[kSG];
+                    msg_load(sr, a);
 #pragma unroll
-            for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-            E += sr.E + renorm_row(v, s.smax, l);
-        }
-        store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
-        if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
-        if (!root) {
+                    for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+                    E += sr.E + renorm_row(v, s.smax, l);
+                }
+            }
+            store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
+            if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
+            if (root) break;
             tc_write_part(s, v, l);
-            float o[kSG];
-            tc_run(s, o, l, w.err, phase);
+            tc_run(s, v, l, w.err, phase);                // v: the message to the parent
             phase ^= 1u;
-            const int sh = renorm_row(o, s.smax, l);
-            store_part(o, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
-            if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E + sh;
+            const int sh = renorm_row(v, s.smax, l);
+            E += sh;
+            store_part(v, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
+            if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E;
+            const int nxt = t.in_next[pos];
+            if (nxt < 0) break;
+            // the parent has no other internal child: it is next, with this message in registers
+            // (its flag is never read, so none is raised)
+            carried = u;
+            pos = nxt;
         }
         item = publish_and_claim(mw.flag_in + (size_t(iu) * M + m) * ntile + tile, epoch, mw.sync + 1, &s_item);
     }
@@ -455,8 +491,9 @@ __global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
 }
 
 // ------------------------------------------------------------------ outside
-// Persistent like the inside pass; items (child k, m, tile) in the order of t.out_info
-// (children of the root first, then by increasing depth of the parent).
+// Persistent like the inside pass; items (chain, m, tile) in the order of t.out_heads (chains
+// by the depth of their first node's parent).  A chain runs down the tree through each
+// node's deepest internal child.
 __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
@@ -472,64 +509,64 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
     int item = claim(mw.sync + 2, &s_item);
     while (item < n_items) {
         const int tile = item % ntile, rest = item / ntile, m = rest % M;
-        const int4 oi = t.out_info[2 * (rest / M)], oj = t.out_info[2 * (rest / M) + 1];
-        const int c = oi.x, u = oi.y, iu = oi.z, ic = oi.w, k0 = oj.x, k1 = oj.y;
         const int p = tile * MT + l.r;
         const size_t so = size_t(kSG * l.g) * Pp + p;
-        const bool internal = ic >= 0;
-        if (internal) tc_load_b(s, mw.Bpt, mat_off_f(m, c, t.n));
-        if (threadIdx.x == 0 && u != t.root) wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err);
-        __syncthreads();
-        // the parent's outside vector (pi at the root) and the first sibling's message load together
+        int pos = t.out_heads[rest / M];
+        bool carried = false;                             // v holds the parent's outside vector (chain)
         float v[kSG];
-        int EV = 0;
-        int k = k0;
-        while (k < k1 && t.kdesc[k].x == c) ++k;
-        {
-            float a[kSG];
-            const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
-            if (u == t.root) {
+        int EV = 0, last = -1;
+        for (;;) {
+            const int4 oi = t.out_info[2 * pos], oj = t.out_info[2 * pos + 1];
+            const int c = oi.x, u = oi.y, iu = oi.z, ic = oi.w, k0 = oj.x, k1 = oj.y;
+            const bool internal = ic >= 0;
+            if (internal) tc_load_b(s, mw.Bpt, mat_off_f(m, c, t.n));
+            if (!carried) {
+                if (threadIdx.x == 0 && u != t.root) wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err);
+                __syncthreads();
+                if (u == t.root) {
 #pragma unroll
-                for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
-            } else {
-                load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
-                EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
+                    for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
+                    EV = 0;
+                } else {
+                    load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
+                    EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
+                }
             }
-            msg_load(s0, a);
+            // times every sibling's message, renormalised after each
+            for (int k = k0; k < k1; ++k) {
+                const int2 sb = t.kdesc[k];
+                if (sb.x == c) continue;
+                const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
+                float a[kSG];
+                msg_load(sr, a);
 #pragma unroll
-            for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-            EV += s0.E + renorm_row(v, s.smax, l);
-            ++k;
-        }
-        for (; k < k1; ++k) {
-            const int2 sb = t.kdesc[k];
-            if (sb.x == c) continue;
-            const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
-            float a[kSG];
-            msg_load(sr, a);
+                for (int i = 0; i < kSG; ++i) v[i] *= a[i];
+                EV += sr.E + renorm_row(v, s.smax, l);
+            }
+            // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
+            const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
+            const int EDc = internal ? mw.ED[col_off(ic, m, M, t.Pp) + p] : 0;
+            const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
+            float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
 #pragma unroll
-            for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-            EV += sr.E + renorm_row(v, s.smax, l);
+            for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
+            if (!internal) break;                          // a leaf: no outside vector below it
+            tc_write_part(s, v, l);
+            tc_run(s, v, l, w.err, phase);                // v: U_c, the outside vector at c
+            phase ^= 1u;
+            EV += renorm_row(v, s.smax, l);
+            store_part(v, mw.U + part_off(ic, m, M, t.Pp) + so, Pp);
+            if (l.g == 0) mw.EU[col_off(ic, m, M, t.Pp) + p] = EV;
+            const int nxt = t.out_next[pos];
+            if (nxt < 0) { last = ic; break; }
+            // c's other children read U_c: raise its flag, then go on with the deepest internal
+            // child, U_c kept in registers
+            publish(mw.flag_out + (size_t(ic) * M + m) * ntile + tile, epoch);
+            carried = true;
+            pos = nxt;
         }
-        // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
-        const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
-        const int EDc = internal ? mw.ED[col_off(ic, m, M, t.Pp) + p] : 0;
-        const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
-        float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
-#pragma unroll
-        for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
-        if (!internal) {
-            item = claim(mw.sync + 2, &s_item);
-            continue;
-        }
-        tc_write_part(s, v, l);
-        float o[kSG];
-        tc_run(s, o, l, w.err, phase);
-        phase ^= 1u;
-        const int sh = renorm_row(o, s.smax, l);
-        store_part(o, mw.U + part_off(ic, m, M, t.Pp) + so, Pp);
-        if (l.g == 0) mw.EU[col_off(ic, m, M, t.Pp) + p] = EV + sh;
-        item = publish_and_claim(mw.flag_out + (size_t(ic) * M + m) * ntile + tile, epoch, mw.sync + 2, &s_item);
+        item = last >= 0 ? publish_and_claim(mw.flag_out + (size_t(last) * M + m) * ntile + tile, epoch, mw.sync + 2, &s_item)
+                         : claim(mw.sync + 2, &s_item);
     }
     tc_teardown(s);
 }
@@ -816,9 +853,8 @@ static int persistent_ctas(int items) {
     }();
     return std::max(1, std::min(items, 2 * sms));
 }
-int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s) {
+int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s) {
     const int items = count * md.M * (t.Pp / MT);
-    (void)d_nodes;     // the item order is t.in_info's
     launch_k(k_inside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items);
     return 1;
 }
@@ -826,9 +862,8 @@ int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const Mixed
     launch_k(k_root_mx, (t.Pp + 127) / 128, 128, 0, s, t, md, w, mw);
     return 1;
 }
-int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s) {
+int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s) {
     const int items = count * md.M * (t.Pp / MT);
-    (void)d_kids;      // the item order is t.out_info's
     launch_k(k_outside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items);
     return 1;
 }

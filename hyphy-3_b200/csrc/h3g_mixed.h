@@ -37,9 +37,10 @@ bool mixed_available();
 void mixed_configure();
 h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, int M, int Pp);
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
-int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_nodes, int count, cudaStream_t s);
+// count: chains of the pass (Topo::in_heads / out_heads)
+int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s);
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
-int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_kids, int count, cudaStream_t s);
+int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s);
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 
 }  // namespace h3g
