@@ -50,6 +50,7 @@ struct FelModel {
     double* lam;          // [slots][64]
     double* U;            // [slots][64*64]
     double* V;            // [slots][64*64]
+    const uint8_t* bg;    // [n] 1 on a background branch (requests with a background eigensystem)
 };
 
 __device__ __forceinline__ double block_sum_or_max(double v, double* red, bool is_max) {
@@ -240,6 +241,7 @@ struct FelReqs {
     const int* slot;      // eigensystem of component 0
     const int* slot2;     // component 1 (NC = 2)
     const double* w1;     // weight of component 0 (NC = 2); component 1 gets 1 - w1
+    const int* slot_bg;   // eigensystem of the background branches (BG)
 };
 
 template <int NC>
@@ -409,7 +411,9 @@ __device__ void prune(const Spectral<NC>& sp, double* sL, const Topo& t, const d
 // l + 32.  A node's message sum_c w_c U_c (e_c o (V_c D)) goes to the CTA's
 // workspace row; its partial D is the product of its children's rows,
 // rescaled by 2^256 whenever its maximum falls below 2^-256 (exponents summed
-// over the tree).  Persistent: CTA b evaluates requests b, b + grid, ...
+// over the tree).  With BG, a branch flagged in f.bg uses the request's
+// background eigensystem alone (weight 1) instead of the NC tested ones.
+// Persistent: CTA b evaluates requests b, b + grid, ...
 struct LevelPlan {
     int H;                    // levels: 0 = leaves ... H - 1 = the root alone
     const int* off;           // [H + 1]
@@ -419,9 +423,11 @@ struct LevelPlan {
 constexpr int kLvT = 512;
 constexpr int kLvW = kLvT / 32;
 
-constexpr size_t lv_smem(int nc) {
-    return (size_t(nc) * (2 * SP * LD + SP) + size_t(kLvW) * (nc + 1) * SP) * sizeof(double);
+// nc tested components, plus the background's eigensystem when bg
+constexpr size_t lv_smem(int nc, bool bg) {
+    return (size_t(nc + (bg ? 1 : 0)) * (2 * SP * LD + SP) + size_t(kLvW) * (nc + 1) * SP) * sizeof(double);
 }
+static_assert(lv_smem(2, true) <= 227 * 1024, "three eigensystems must fit one CTA");
 
 __device__ __forceinline__ double warp_max(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -433,19 +439,20 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-template <int NC>
+template <int NC, bool BG>
 __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const double* __restrict__ bl, LevelPlan lp,
                                                    double* __restrict__ work, FelReqs q, int n_req, double* __restrict__ out) {
+    constexpr int NT = NC + (BG ? 1 : 0);                 // eigensystems per request; the last is the background's
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
     __shared__ int sE;
     __shared__ double sL;
-    double* U[NC];
-    double* V[NC];
-    double* lam[NC];
+    double* U[NT];
+    double* V[NT];
+    double* lam[NT];
     double* z = sm;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
+    for (int c = 0; c < NT; ++c) {
         U[c] = z; z += SP * LD;
         V[c] = z; z += SP * LD;
         lam[c] = z; z += SP;
@@ -456,7 +463,7 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
     double* msg = work + size_t(blockIdx.x) * t.n * SP;
     const int s0 = lane, s1 = lane + 32;
     for (int r = blockIdx.x; r < n_req; r += gridDim.x) {
-        int sl[NC];
+        int sl[NT];
         double w[NC];
         sl[0] = q.slot[r];
         if constexpr (NC == 2) {
@@ -466,11 +473,12 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
         } else {
             w[0] = 1.0;
         }
+        if constexpr (BG) sl[NT - 1] = q.slot_bg[r];
         const double a = q.a[r];
         const int p = q.pattern[r];
         __syncthreads();                                   // the previous request is done with shared memory
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
+        for (int c = 0; c < NT; ++c) {
             const double* gU = f.U + size_t(sl[c]) * SP2;
             const double* gV = f.V + size_t(sl[c]) * SP2;
             for (int e = tid; e < SP2; e += kLvT) {
@@ -486,6 +494,9 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
             const int b1 = lp.off[h + 1];
             for (int i = lp.off[h] + warp; i < b1; i += kLvW) {
                 const int u = lp.nodes[i];
+                // the branch above u: the tested components, or the background one alone
+                const bool bgn = BG && f.bg[u] != 0;
+                const int ncu = bgn ? 1 : NC;
                 double x[NC][2];
                 if (t.leaf[u]) {                           // x_c = V_c * leaf vector
                     const int tx = t.taxon[u];
@@ -498,13 +509,15 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
                     const bool all = mk == 0 || (mk & t.all_mask) == t.all_mask;
 #pragma unroll
                     for (int c = 0; c < NC; ++c) {
+                        if (c >= ncu) break;
+                        const double* Vc = bgn ? V[NT - 1] : V[c];
                         double a0 = 0.0, a1 = 0.0;
                         if (st >= 0) {
-                            a0 = V[c][s0 * LD + st];
-                            a1 = V[c][s1 * LD + st];
+                            a0 = Vc[s0 * LD + st];
+                            a1 = Vc[s1 * LD + st];
                         } else {
                             for (int j = 0; j < S; ++j)
-                                if (all || ((mk >> j) & 1)) { a0 += V[c][s0 * LD + j]; a1 += V[c][s1 * LD + j]; }
+                                if (all || ((mk >> j) & 1)) { a0 += Vc[s0 * LD + j]; a1 += Vc[s1 * LD + j]; }
                         }
                         x[c][0] = a0;
                         x[c][1] = a1;
@@ -535,9 +548,11 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
                     __syncwarp();
 #pragma unroll
                     for (int c = 0; c < NC; ++c) {
+                        if (c >= ncu) break;
+                        const double* Vc = bgn ? V[NT - 1] : V[c];
                         double a0 = 0.0, a1 = 0.0;
-                        const double* v0 = V[c] + s0 * LD;
-                        const double* v1 = V[c] + s1 * LD;
+                        const double* v0 = Vc + s0 * LD;
+                        const double* v1 = Vc + s1 * LD;
 #pragma unroll 16
                         for (int j = 0; j < SP; ++j) {
                             const double dj = dv[j];
@@ -551,16 +566,19 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
                 const double tb = bl[u];
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    xv[c * SP + s0] = x[c][0] * exp(lam[c][s0] * tb);
-                    xv[c * SP + s1] = x[c][1] * exp(lam[c][s1] * tb);
+                    if (c >= ncu) break;
+                    const double* lc = bgn ? lam[NT - 1] : lam[c];
+                    xv[c * SP + s0] = x[c][0] * exp(lc[s0] * tb);
+                    xv[c * SP + s1] = x[c][1] * exp(lc[s1] * tb);
                 }
                 __syncwarp();
                 double m0 = 0.0, m1 = 0.0;
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
+                    if (c >= ncu) break;
                     double a0 = 0.0, a1 = 0.0;
-                    const double* u0 = U[c] + s0 * LD;
-                    const double* u1 = U[c] + s1 * LD;
+                    const double* u0 = (bgn ? U[NT - 1] : U[c]) + s0 * LD;
+                    const double* u1 = (bgn ? U[NT - 1] : U[c]) + s1 * LD;
                     const double* xc = xv + c * SP;
 #pragma unroll 16
                     for (int j = 0; j < SP; ++j) {
@@ -568,8 +586,9 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
                         a0 = fma(u0[j], xj, a0);
                         a1 = fma(u1[j], xj, a1);
                     }
-                    m0 += w[c] * a0;
-                    m1 += w[c] * a1;
+                    const double wc = bgn ? 1.0 : w[c];
+                    m0 += wc * a0;
+                    m1 += wc * a1;
                 }
                 __syncwarp();                              // dv / xv are reused by this warp's next node
                 msg[size_t(u) * SP + s0] = s0 < S ? fmax(m0, 0.0) : 0.0;
@@ -699,13 +718,14 @@ struct FelDevice {
     Topo t{};
     FelModel f{};
     double* d_bl = nullptr;
+    uint8_t* d_bg = nullptr;              // [n] background flags of the run
     int* d_ev = nullptr;
     double* d_stack = nullptr;            // EBF pass: [kEbfChunk][depth][64] open partials
     int* d_lv = nullptr;                  // level plan: [H + 1] offsets, then [n] nodes
     int H = 0;
     double* d_work = nullptr;             // level-synchronous pruning: [grid][n][64] messages
-    int grid1 = 1, grid2 = 1;             // persistent CTAs for one / two components
-    unsigned char* d_req = nullptr;       // per batch: [om | a | w1 | eslot | eprev | pat | slot | slot2], packed to the batch's sizes
+    int grid[2][2] = {{1, 1}, {1, 1}};    // persistent CTAs per [tested components - 1][background]
+    unsigned char* d_req = nullptr;       // per batch: [om | a | w1 | eslot | eprev | pat | slot | slot2 | slot_bg], packed to the batch's sizes
     unsigned char* h_req = nullptr;       // pinned mirror
     double* d_out = nullptr;
     double* h_out = nullptr;
@@ -715,15 +735,16 @@ struct FelDevice {
     size_t h2d = 0, d2h = 0;              // bytes moved by the batches so far
     int launches = 0;                     // kernels launched so far
     std::vector<void*> owned;
-    std::vector<int> order;               // one-component requests first, then two-component ones
+    std::vector<uint8_t> bg_host;
+    std::vector<int> order;               // requests grouped by kernel: (1, -), (2, -), (1, bg), (2, bg)
     ~FelDevice() {
         for (void* p : owned) cudaFree(p);
         if (h_req) cudaFreeHost(h_req);
         if (h_out) cudaFreeHost(h_out);
         if (h_ebf) cudaFreeHost(h_ebf);
     }
-    // a batch holds up to max_req requests and two eigensolves per request
-    size_t req_bytes() const { return 4 * size_t(max_req) * sizeof(double) + 7 * size_t(max_req) * sizeof(int); }
+    // a batch holds up to max_req requests and three eigensolves per request
+    size_t req_bytes() const { return 5 * size_t(max_req) * sizeof(double) + 10 * size_t(max_req) * sizeof(int); }
 };
 
 constexpr int kEbfChunk = 256;
@@ -794,7 +815,8 @@ FelDevice* fel_device_alloc(h3g_problem* pr, const FelProblemView& v, int max_re
     double *qs = nullptr, *qn = nullptr, *dsq = nullptr, *disq = nullptr, *dpi = nullptr;
     bool ok = take(&qs, SP2) && take(&qn, SP2) && take(&dsq, SP) && take(&disq, SP) && take(&dpi, SP) &&
               take(&d->f.lam, size_t(d->n_slots) * SP) && take(&d->f.U, size_t(d->n_slots) * SP2) &&
-              take(&d->f.V, size_t(d->n_slots) * SP2) && take(&d->d_bl, v.n) && take(&d->d_ev, ev.size()) &&
+              take(&d->f.V, size_t(d->n_slots) * SP2) && take(&d->d_bl, v.n) && take(&d->d_bg, v.n) &&
+              take(&d->d_ev, ev.size()) &&
               take(&d->d_stack, size_t(kEbfChunk) * d->depth * SP) && take(&d->d_out, d->max_req) &&
               take(&d->d_lv, lv.size()) && take(&d->d_work, size_t(2) * std::max(sms, 1) * v.n * SP);
     void* rq = nullptr;
@@ -804,31 +826,37 @@ FelDevice* fel_device_alloc(h3g_problem* pr, const FelProblemView& v, int max_re
     ok = ok && cudaMallocHost(reinterpret_cast<void**>(&d->h_req), d->req_bytes()) == cudaSuccess &&
          cudaMallocHost(reinterpret_cast<void**>(&d->h_out), d->max_req * sizeof(double)) == cudaSuccess;
     if (!ok) { *err = "device allocation failed"; delete d; return nullptr; }
-    d->f.Qs = qs; d->f.Qn = qn; d->f.sq = dsq; d->f.isq = disq; d->f.pi = dpi;
+    d->f.Qs = qs; d->f.Qn = qn; d->f.sq = dsq; d->f.isq = disq; d->f.pi = dpi; d->f.bg = d->d_bg;
     ok = cudaMemcpyAsync(d->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice, d->s) == cudaSuccess &&
          cudaMemcpyAsync(d->d_lv, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice, d->s) == cudaSuccess &&
          cudaStreamSynchronize(d->s) == cudaSuccess;
     static bool configured = false;
     if (ok && !configured) {
         ok = cudaFuncSetAttribute(k_fel_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEigSmem)) == cudaSuccess &&
-             cudaFuncSetAttribute(k_site_lnl<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(1))) == cudaSuccess &&
-             cudaFuncSetAttribute(k_site_lnl<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(2))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_site_lnl<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(1, false))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_site_lnl<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(2, false))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_site_lnl<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(1, true))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_site_lnl<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(2, true))) == cudaSuccess &&
              cudaFuncSetAttribute(k_meme_ebf, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEbfSmem)) == cudaSuccess;
         configured = ok;
     }
-    int per1 = 0, per2 = 0;
-    ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, k_site_lnl<1>, kLvT, lv_smem(1)) == cudaSuccess &&
-         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_site_lnl<2>, kLvT, lv_smem(2)) == cudaSuccess;
+    int per[2][2] = {{0, 0}, {0, 0}};
+    ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0][0], k_site_lnl<1, false>, kLvT, lv_smem(1, false)) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1][0], k_site_lnl<2, false>, kLvT, lv_smem(2, false)) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0][1], k_site_lnl<1, true>, kLvT, lv_smem(1, true)) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1][1], k_site_lnl<2, true>, kLvT, lv_smem(2, true)) == cudaSuccess;
     if (!ok) { *err = std::string("FEL set-up: ") + cudaGetErrorString(cudaGetLastError()); delete d; return nullptr; }
-    d->grid1 = std::max(1, std::min(per1, 2) * std::max(sms, 1));     // the workspace holds 2 x SMs CTAs
-    d->grid2 = std::max(1, std::min(per2, 2) * std::max(sms, 1));
+    for (int c = 0; c < 2; ++c)
+        for (int b = 0; b < 2; ++b)       // the workspace holds 2 x SMs CTAs
+            d->grid[c][b] = std::max(1, std::min(per[c][b], 2) * std::max(sms, 1));
     return d;
 }
 
 }  // namespace
 
 FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
-                             const double* branch_lengths, int max_requests, int n_slots, std::string* err) {
+                             const double* branch_lengths, const uint8_t* background, int max_requests, int n_slots,
+                             std::string* err) {
     FelProblemView v;
     if (!fel_problem_view(pr, &v) || S < 1 || S > SP) { *err = "invalid problem"; return nullptr; }
     FelDevice*& cached = problem_fel_device(pr);
@@ -851,8 +879,12 @@ FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const dou
         isq[i] = 1.0 / sq[i];
         pp[i] = pi[i];
     }
+    d->bg_host.assign(size_t(v.n), 0);
+    if (background)
+        for (int i = 0; i < v.n; ++i) d->bg_host[size_t(i)] = i != v.root && background[i] ? 1 : 0;
     cudaStream_t s = d->s;
     const bool ok =
+        cudaMemcpyAsync(d->d_bg, d->bg_host.data(), size_t(v.n), cudaMemcpyHostToDevice, s) == cudaSuccess &&
         cudaMemcpyAsync(const_cast<double*>(d->f.Qs), Qs, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
         cudaMemcpyAsync(const_cast<double*>(d->f.Qn), Qn, size_t(S) * S * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
         cudaMemcpyAsync(const_cast<double*>(d->f.sq), sq.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
@@ -875,8 +907,8 @@ namespace {
 // the eigensolves.  Returns the request views (in packed order) through q.
 bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                  const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2, const double* req_w1,
-                 const std::vector<int>& order, FelReqs* q, std::string* err) {
-    if (n_eig > 2 * d->max_req || n_req > d->max_req || n_eig < 0 || n_req < 0) { *err = "FEL batch too large"; return false; }
+                 const int* req_slot_bg, const std::vector<int>& order, FelReqs* q, std::string* err) {
+    if (n_eig > 3 * d->max_req || n_req > d->max_req || n_eig < 0 || n_req < 0) { *err = "FEL batch too large"; return false; }
     for (int i = 0; i < n_eig; ++i)
         if (eig_slot[i] < 0 || eig_slot[i] >= d->n_slots || eig_prev[i] < -1 || eig_prev[i] >= d->n_slots) {
             *err = "FEL eigensystem slot out of range";
@@ -885,7 +917,8 @@ bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* ei
     for (int i = 0; i < n_req; ++i) {
         const bool mix = req_slot2 && req_slot2[i] >= 0;
         if (req_slot[i] < 0 || req_slot[i] >= d->n_slots || req_pattern[i] < 0 || req_pattern[i] >= d->t.P ||
-            (mix && req_slot2[i] >= d->n_slots) || !(req_a[i] > 0.0) || (req_w1 && !(req_w1[i] >= 0.0 && req_w1[i] <= 1.0))) {
+            (mix && req_slot2[i] >= d->n_slots) || (req_slot_bg && req_slot_bg[i] >= d->n_slots) || !(req_a[i] > 0.0) ||
+            (req_w1 && !(req_w1[i] >= 0.0 && req_w1[i] <= 1.0))) {
             *err = "FEL request out of range";
             return false;
         }
@@ -893,8 +926,8 @@ bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* ei
     const size_t o_a = size_t(n_eig) * sizeof(double), o_w = o_a + size_t(n_req) * sizeof(double);
     const size_t o_es = o_w + size_t(n_req) * sizeof(double), o_pv = o_es + size_t(n_eig) * sizeof(int);
     const size_t o_pat = o_pv + size_t(n_eig) * sizeof(int), o_sl = o_pat + size_t(n_req) * sizeof(int);
-    const size_t o_s2 = o_sl + size_t(n_req) * sizeof(int);
-    const size_t bytes = o_s2 + size_t(n_req) * sizeof(int);
+    const size_t o_s2 = o_sl + size_t(n_req) * sizeof(int), o_sb = o_s2 + size_t(n_req) * sizeof(int);
+    const size_t bytes = o_sb + size_t(n_req) * sizeof(int);
     unsigned char* h = d->h_req;
     std::copy(eig_omega, eig_omega + n_eig, reinterpret_cast<double*>(h));
     std::copy(eig_slot, eig_slot + n_eig, reinterpret_cast<int*>(h + o_es));
@@ -906,6 +939,7 @@ bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* ei
         reinterpret_cast<int*>(h + o_pat)[k] = req_pattern[i];
         reinterpret_cast<int*>(h + o_sl)[k] = req_slot[i];
         reinterpret_cast<int*>(h + o_s2)[k] = req_slot2 ? req_slot2[i] : -1;
+        reinterpret_cast<int*>(h + o_sb)[k] = req_slot_bg ? req_slot_bg[i] : -1;
     }
     cudaStream_t s = d->s;
     if (cudaMemcpyAsync(d->d_req, h, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
@@ -921,39 +955,51 @@ bool stage_batch(FelDevice* d, int n_eig, const double* eig_omega, const int* ei
     }
     *q = FelReqs{reinterpret_cast<const int*>(g + o_pat), reinterpret_cast<const double*>(g + o_a),
                  reinterpret_cast<const int*>(g + o_sl), reinterpret_cast<const int*>(g + o_s2),
-                 reinterpret_cast<const double*>(g + o_w)};
+                 reinterpret_cast<const double*>(g + o_w), reinterpret_cast<const int*>(g + o_sb)};
     return true;
 }
 
 FelReqs offset(const FelReqs& q, int k) {
-    return FelReqs{q.pattern + k, q.a + k, q.slot + k, q.slot2 + k, q.w1 + k};
+    return FelReqs{q.pattern + k, q.a + k, q.slot + k, q.slot2 + k, q.w1 + k, q.slot_bg + k};
 }
 
 }  // namespace
 
 bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                      const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
-                     const double* req_w1, double* lnl_out, std::string* err) {
+                     const double* req_w1, const int* req_slot_bg, double* lnl_out, std::string* err) {
     if (n_req == 0 && n_eig == 0) return true;
+    // group the requests by kernel: tested components (1 or 2) x background eigensystem (no / yes)
     auto& order = d->order;
     order.clear();
-    for (int i = 0; i < n_req; ++i)
-        if (!(req_slot2 && req_slot2[i] >= 0)) order.push_back(i);
-    const int n1 = int(order.size());
-    for (int i = 0; i < n_req; ++i)
-        if (req_slot2 && req_slot2[i] >= 0) order.push_back(i);
+    int start[5] = {0, 0, 0, 0, 0};
+    for (int g = 0; g < 4; ++g) {
+        const bool two = g & 1, bg = g >> 1;
+        for (int i = 0; i < n_req; ++i)
+            if ((req_slot2 && req_slot2[i] >= 0) == two && (req_slot_bg && req_slot_bg[i] >= 0) == bg) order.push_back(i);
+        start[g + 1] = int(order.size());
+    }
     FelReqs q{};
-    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, order, &q, err))
+    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1,
+                     req_slot_bg, order, &q, err))
         return false;
     cudaStream_t s = d->s;
     const LevelPlan lp{d->H, d->d_lv, d->d_lv + d->H + 1};
-    d->launches += (n1 > 0) + (n_req > n1);
-    if (n1 > 0)
-        launch_k(k_site_lnl<1>, std::min(n1, d->grid1), kLvT, lv_smem(1), s, d->f, d->t, static_cast<const double*>(d->d_bl),
-                 lp, d->d_work, q, n1, d->d_out);
-    if (n_req > n1)
-        launch_k(k_site_lnl<2>, std::min(n_req - n1, d->grid2), kLvT, lv_smem(2), s, d->f, d->t,
-                 static_cast<const double*>(d->d_bl), lp, d->d_work, offset(q, n1), n_req - n1, d->d_out + n1);
+    const double* bl = d->d_bl;
+    for (int g = 0; g < 4; ++g) {
+        const int k0 = start[g], cnt = start[g + 1] - start[g];
+        if (cnt == 0) continue;
+        const FelReqs qg = offset(q, k0);
+        double* o = d->d_out + k0;
+        const int grid = std::min(cnt, d->grid[g & 1][g >> 1]);
+        switch (g) {
+            case 0: launch_k(k_site_lnl<1, false>, grid, kLvT, lv_smem(1, false), s, d->f, d->t, bl, lp, d->d_work, qg, cnt, o); break;
+            case 1: launch_k(k_site_lnl<2, false>, grid, kLvT, lv_smem(2, false), s, d->f, d->t, bl, lp, d->d_work, qg, cnt, o); break;
+            case 2: launch_k(k_site_lnl<1, true>, grid, kLvT, lv_smem(1, true), s, d->f, d->t, bl, lp, d->d_work, qg, cnt, o); break;
+            default: launch_k(k_site_lnl<2, true>, grid, kLvT, lv_smem(2, true), s, d->f, d->t, bl, lp, d->d_work, qg, cnt, o); break;
+        }
+        ++d->launches;
+    }
     d->d2h += size_t(n_req) * sizeof(double);
     const bool ok = cudaGetLastError() == cudaSuccess &&
                     (n_req == 0 || cudaMemcpyAsync(d->h_out, d->d_out, n_req * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess) &&
@@ -984,7 +1030,8 @@ bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int*
     order.resize(n_req);
     for (int i = 0; i < n_req; ++i) order[i] = i;
     FelReqs q{};
-    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, order, &q, err))
+    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, nullptr,
+                     order, &q, err))
         return false;
     cudaStream_t s = d->s;
     const size_t bytes = size_t(n_req) * d->n * sizeof(double);

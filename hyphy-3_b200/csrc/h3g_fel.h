@@ -29,14 +29,19 @@ void fel_set_error(h3g_problem* pr, const std::string& msg);
 // Q(omega) = Qs + omega Qn.  A request evaluates one pattern's log-likelihood
 // at time scale a with the eigensystem in its slot, or, when slot2 >= 0, with
 // the two eigensystems mixed at the transition-matrix level with weights
-// (w1, 1 - w1).  req_slot2 / req_w1 may be null (every request one component).
+// (w1, 1 - w1).  When slot_bg >= 0 the branches flagged in the run's
+// background[] use that eigensystem alone.  req_slot2 / req_w1 / req_slot_bg
+// may be null (no request has that component).
 struct FelDevice;
+// background[n_nodes] (may be null: none) flags the branches a request's
+// background eigensystem applies to; the root's flag is ignored
 FelDevice* fel_device_create(h3g_problem* pr, int S, const double* pi, const double* Qs, const double* Qn,
-                             const double* branch_lengths, int max_requests, int n_slots, std::string* err);
+                             const double* branch_lengths, const uint8_t* background, int max_requests, int n_slots,
+                             std::string* err);
 // eig_prev[i] >= 0: slot whose eigenvectors start the solve (warm start), -1: from the identity
 bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                      const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
-                     const double* req_w1, double* lnl_out, std::string* err);
+                     const double* req_w1, const int* req_slot_bg, double* lnl_out, std::string* err);
 // MEME's empirical Bayes factors of every branch for two-component requests
 // (at most fel_device_max_ebf(d) per call): ebf_out[r * n_nodes + b]
 int fel_device_max_ebf(const FelDevice* d);

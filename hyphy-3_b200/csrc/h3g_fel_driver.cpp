@@ -1,5 +1,5 @@
-// h3g_fel_driver.cpp — h3g_fel_run: FEL per-site fits with every pattern's
-// optimiser advanced in lockstep.
+// h3g_fel_driver.cpp — h3g_fel_run / h3g_fel_run_tested: FEL per-site fits with
+// every pattern's optimiser advanced in lockstep.
 //
 // Each pattern runs the reference's search (analyses/fel.hpp:326-446 with
 // every branch tested; optimisers from opt/nelder_mead.hpp:24-229) written as
@@ -172,6 +172,74 @@ Fit fel_search(Site& s, h3g_fel_result& res) {
     res.evaluations = s.evaluations;
 }
 
+namespace {
+
+// (alpha, beta on the tested branches, beta_bg on the background) -> request: time scale alpha,
+// omega beta / alpha, and beta_bg / alpha on the background unless |beta - beta_bg| < 1e-9, when
+// every branch uses the tested model (fel.hpp:462-500)
+Req subset_req(double a, double bt, double bb) {
+    Req r{a, bt / a, -1.0, 1.0, 0.0};
+    if (std::fabs(bt - bb) >= 1e-9) r.om_bg = bb / a;
+    return r;
+}
+
+}  // namespace
+
+// The reference's branch-subset search of one pattern (fel.hpp:462-572).  The
+// start grids are evaluated together: each grid point is scored independently
+// and the best is picked in the reference's order, so the path is unchanged.
+Fit fel_search_subset(Site& s, h3g_fel_result& res) {
+    using A3 = Arr<3>;
+    using A2 = Arr<2>;
+    // 12-point start grid of the alternative model (fel.hpp:518-533)
+    static const double g3[12][3] = {{0.01, 0.1, 0.1}, {1.0, 0.1, 0.1}, {1.0, 0.5, 0.5},   {1.0, 1.0, 1.0},
+                                     {1.0, 5.0, 5.0},  {10.0, 0.1, 0.1}, {0.01, 0.5, 0.5}, {0.01, 5.0, 5.0},
+                                     {10.0, 0.5, 0.5}, {10.0, 1.0, 1.0}, {10.0, 50.0, 50.0}, {100.0, 1.0, 1.0}};
+    std::vector<Req> rq;
+    for (const auto& g : g3) rq.push_back(subset_req(g[0], g[1], g[2]));
+    co_await EvalMany{s, rq};
+    double best = -1e20;
+    A3 init = {1.0, 1.0, 1.0};
+    for (int i = 0; i < 12; ++i)
+        if (rq[size_t(i)].lnl > best) {
+            best = rq[size_t(i)].lnl;
+            init = {g3[i][0], g3[i][1], g3[i][2]};
+        }
+    // alternative model: bounded 3-D Nelder-Mead on (alpha, beta, beta_bg), tol 1e-4, 100 iterations
+    auto make3 = [](const A3& x) { return subset_req(x[0], x[1], x[2]); };
+    const Pt<3> alt = co_await nelder_mead_nd<3>(s, make3, init, A3{1e-4, 1e-4, 1e-4}, A3{1000.0, 1000.0, 1000.0}, 1e-4,
+                                                 100, {});
+    res.alpha = alt.x[0];
+    res.beta = alt.x[1];
+    res.beta_nuisance = alt.x[2];
+    res.log_l_alt = -alt.f;
+    // null model beta = alpha, beta_bg free: the initial point, then a 7 x 4 grid (fel.hpp:546-563)
+    const double ina = (std::min(res.alpha, 100.0) + 3.0 * std::min(res.beta, 100.0)) / 4.0, inb = res.beta_nuisance;
+    std::vector<A2> pts = {{ina, inb}};
+    for (double ca : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0})
+        for (double cb : {inb, 0.1, 1.0, 5.0}) pts.push_back({ca, cb});
+    rq.clear();
+    for (const auto& x : pts) rq.push_back(subset_req(x[0], x[0], x[1]));
+    co_await EvalMany{s, rq};
+    double best_null = rq[0].lnl;
+    A2 initn = pts[0];
+    for (size_t i = 1; i < pts.size(); ++i)
+        if (rq[i].lnl > best_null) {
+            best_null = rq[i].lnl;
+            initn = pts[i];
+        }
+    // bounded 2-D Nelder-Mead on (alpha, beta_bg), tol 1e-4, 80 iterations
+    auto make2 = [](const A2& x) { return subset_req(x[0], x[0], x[1]); };
+    const Pt<2> nul = co_await nelder_mead_nd<2>(s, make2, initn, A2{1e-4, 1e-4}, A2{1000.0, 1000.0}, 1e-4, 80, {});
+    res.alpha_null = nul.x[0];
+    res.log_l_null = -nul.f;
+    double lrt = 0.0;
+    if (res.log_l_alt > -1e10 && res.log_l_null > -1e10) lrt = std::max(0.0, 2.0 * (res.log_l_alt - res.log_l_null));
+    res.lrt = lrt;
+    res.p_value = std::erfc(std::sqrt(lrt / 2.0));
+    res.evaluations = s.evaluations;
+}
+
 h3g_status prepare_site_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths, const char* who,
                             FelProblemView* pv, std::vector<int>* variable) {
     const std::string w(who);
@@ -223,35 +291,53 @@ h3g_status prepare_site_run(h3g_problem* prob, const h3g_fel_model* m, const dou
 using namespace h3g;
 using namespace h3g::sitefit;
 
-extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths,
-                                  h3g_fel_result* out) {
+static h3g_status fel_run_impl(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths,
+                               const uint8_t* tested, h3g_fel_result* out, const char* who) {
     if (!prob) return H3G_ERR_ARG;
     const auto t_start = std::chrono::steady_clock::now();
+    const std::string w(who);
     try {
         FelProblemView v;
         std::vector<int> variable;
-        if (!out) { fel_set_error(prob, "h3g_fel_run: null argument"); return H3G_ERR_ARG; }
-        const h3g_status pst = prepare_site_run(prob, m, branch_lengths, "h3g_fel_run", &v, &variable);
+        if (!out) { fel_set_error(prob, w + ": null argument"); return H3G_ERR_ARG; }
+        const h3g_status pst = prepare_site_run(prob, m, branch_lengths, who, &v, &variable);
         if (pst != H3G_OK) return pst;
-        for (int p = 0; p < v.P; ++p) out[p] = h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0};
+        // fel.hpp:215-227: the branches outside the tested set form the background
+        std::vector<uint8_t> background(size_t(v.n), 0);
+        bool subset = false;
+        if (tested)
+            for (int b = 0; b < v.n; ++b)
+                if (b != v.root && !tested[b]) { background[size_t(b)] = 1; subset = true; }
+        const h3g_fel_result zero{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0, 0.0};
+        for (int p = 0; p < v.P; ++p) out[p] = zero;
         const int N = int(variable.size());
         if (N == 0) return H3G_OK;
         const int S = m->S;
         std::string err;
         LockstepOptions opt;
-        opt.cache_tol = 1e-12;              // fel.hpp:368-376
-        opt.max_requests = N;               // one request per pattern at a time
-        opt.temp_slots = 0;
-        FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, opt.max_requests,
-                                           slots_needed(N, opt.temp_slots), &err);
-        if (!dev) { fel_set_error(prob, "h3g_fel_run: " + err); return H3G_ERR_CUDA; }
+        if (!subset) {
+            opt.cache_tol = 1e-12;          // fel.hpp:368-376
+            opt.max_requests = N;           // one request per pattern at a time
+            opt.temp_slots = 0;
+        } else {
+            // the reference builds both models afresh for every evaluation; a start grid parks
+            // up to 29 requests at once, each with up to two eigensystems
+            opt.cache_tol = 0.0;
+            opt.components = 3;
+            opt.max_requests = std::max({64, N, std::min(8 * N, 16384)});
+            opt.temp_slots = std::min(2 * opt.max_requests, 32768);
+            opt.spec_threshold = 32;
+        }
+        FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, subset ? background.data() : nullptr,
+                                           opt.max_requests, slots_needed(N, opt.temp_slots, opt.components), &err);
+        if (!dev) { fel_set_error(prob, w + ": " + err); return H3G_ERR_CUDA; }
         std::vector<Site> sites(N);
-        std::vector<h3g_fel_result> res(N, h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0});
+        std::vector<h3g_fel_result> res(N, zero);
         std::vector<Fit> fits;
         fits.reserve(N);
         for (int i = 0; i < N; ++i) {
             sites[i].pattern = variable[i];
-            fits.push_back(fel_search(sites[i], res[i]));
+            fits.push_back(subset ? fel_search_subset(sites[i], res[i]) : fel_search(sites[i], res[i]));
         }
         LockstepState state;
         const h3g_status st = run_lockstep(dev, sites, fits, opt, state, &err);
@@ -259,17 +345,31 @@ extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, con
         int launches = 0;
         fel_device_transfer(dev, &h2d, &d2h, &launches);
         fel_device_destroy(dev);
-        if (st != H3G_OK) { fel_set_error(prob, "h3g_fel_run: " + err); return st; }
-        // the run's own inputs and outputs: model, branch lengths, per-pattern results
-        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double), d2h, launches,
+        if (st != H3G_OK) { fel_set_error(prob, w + ": " + err); return st; }
+        // the run's own inputs and outputs: model, branch lengths, background flags, per-pattern results
+        fel_record_transfer(prob, h2d + (2 * size_t(S) * S + S + v.n) * sizeof(double) + size_t(v.n), d2h, launches,
                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
         for (int i = 0; i < N; ++i) out[variable[i]] = res[i];
         return H3G_OK;
     } catch (const std::bad_alloc&) {
-        fel_set_error(prob, "h3g_fel_run: host allocation failed");
+        fel_set_error(prob, w + ": host allocation failed");
         return H3G_ERR_OOM;
     } catch (const std::exception& e) {
-        fel_set_error(prob, std::string("h3g_fel_run: ") + e.what());
+        fel_set_error(prob, w + ": " + e.what());
         return H3G_ERR_ARG;
     }
+}
+
+extern "C" h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths,
+                                  h3g_fel_result* out) {
+    return fel_run_impl(prob, m, branch_lengths, nullptr, out, "h3g_fel_run");
+}
+
+extern "C" h3g_status h3g_fel_run_tested(h3g_problem* prob, const h3g_fel_model* m, const double* branch_lengths,
+                                         const uint8_t* tested, h3g_fel_result* out) {
+    if (prob && !tested) {
+        fel_set_error(prob, "h3g_fel_run_tested: null argument");
+        return H3G_ERR_ARG;
+    }
+    return fel_run_impl(prob, m, branch_lengths, tested, out, "h3g_fel_run_tested");
 }

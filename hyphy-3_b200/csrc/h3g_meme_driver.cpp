@@ -23,145 +23,6 @@
 namespace h3g::sitefit {
 namespace {
 
-template <int D>
-using Arr = std::array<double, D>;
-
-template <int D>
-struct Pt {
-    Arr<D> x{};
-    double f = 0.0;
-};
-
-// opt/nelder_mead.hpp:209-357, minimising -lnL: the best of the start point and
-// the grid seeds a simplex of D perturbed vertices; reflection 1, expansion 2,
-// contraction 0.5, shrink 0.5; stops when the f-spread and the coordinate
-// spread between the best and worst vertex are both below tol.  Independent
-// evaluations (start + grid, the first simplex, a shrink) are parked together.
-template <int D, class Make>
-Task<Pt<D>> nelder_mead_nd(Site& s, Make make, Arr<D> init, Arr<D> lb, Arr<D> ub, double tol, int max_iter,
-                           std::vector<Arr<D>> grid) {
-    auto clampx = [&](const Arr<D>& v) {
-        Arr<D> c;
-        for (int d = 0; d < D; ++d) c[d] = std::clamp(v[d], lb[d], ub[d]);
-        return c;
-    };
-    std::vector<Arr<D>> xs;
-    std::vector<Req> rq;
-    auto eval_all = [&]() {
-        rq.clear();
-        for (const auto& x : xs) rq.push_back(make(x));
-        return EvalMany{s, rq};
-    };
-    xs.push_back(clampx(init));
-    for (const auto& g : grid) xs.push_back(clampx(g));
-    co_await eval_all();
-    Pt<D> best{xs[0], -rq[0].lnl};
-    for (size_t i = 1; i < xs.size(); ++i)
-        if (-rq[i].lnl < best.f) best = Pt<D>{xs[i], -rq[i].lnl};
-    std::array<Pt<D>, D + 1> v;
-    v[0] = best;
-    xs.clear();
-    for (int d = 0; d < D; ++d) {
-        Arr<D> x = best.x;
-        const double step = std::max(0.05, 0.2 * std::fabs(best.x[d]));
-        if (best.x[d] + step <= ub[d]) x[d] += step;
-        else x[d] -= step;
-        xs.push_back(clampx(x));
-    }
-    co_await eval_all();
-    for (int d = 0; d < D; ++d) v[d + 1] = Pt<D>{xs[d], -rq[d].lnl};
-    auto by_f = [](const Pt<D>& a, const Pt<D>& b) { return a.f < b.f; };
-    auto one = [&](const Arr<D>& x) {
-        const Arr<D> c = clampx(x);
-        return std::pair<Arr<D>, Req>{c, make(c)};
-    };
-    for (int iter = 0; iter < max_iter; ++iter) {
-        std::sort(v.begin(), v.end(), by_f);
-        double dx = 0.0;
-        for (int d = 0; d < D; ++d) dx = std::max(dx, std::fabs(v[D].x[d] - v[0].x[d]));
-        if (std::fabs(v[D].f - v[0].f) < tol && dx < tol) break;
-        Arr<D> c{};
-        for (int i = 0; i < D; ++i)
-            for (int d = 0; d < D; ++d) c[d] += v[i].x[d];
-        for (int d = 0; d < D; ++d) c[d] /= double(D);
-        Arr<D> xr;
-        for (int d = 0; d < D; ++d) xr[d] = c[d] + 1.0 * (c[d] - v[D].x[d]);
-        if (s.speculate) {
-            // The step evaluates the reflection r and then at most one of the expansion and the two
-            // contractions; all four points are known before r's value, so they are evaluated in one
-            // batch and the decisions below are the sequential ones.  Unused values are not counted.
-            const Arr<D> xrc = clampx(xr);
-            Arr<D> xe, xo, xi;
-            for (int d = 0; d < D; ++d) {
-                xe[d] = c[d] + 2.0 * (xrc[d] - c[d]);
-                xo[d] = c[d] + 0.5 * (xrc[d] - c[d]);
-                xi[d] = c[d] + 0.5 * (v[D].x[d] - c[d]);
-            }
-            xs = {xrc, clampx(xe), clampx(xo), clampx(xi)};
-            co_await eval_all();
-            const Pt<D> r{xs[0], -rq[0].lnl};
-            int used = 1;
-            bool shrink = false;
-            if (r.f < v[0].f) {
-                const Pt<D> e{xs[1], -rq[1].lnl};
-                v[D] = (e.f < r.f) ? e : r;
-                used = 2;
-            } else if (r.f < v[D - 1].f) {
-                v[D] = r;
-            } else {
-                const bool outside = r.f < v[D].f;
-                const Pt<D> cc = outside ? Pt<D>{xs[2], -rq[2].lnl} : Pt<D>{xs[3], -rq[3].lnl};
-                used = 2;
-                if (cc.f < (outside ? r.f : v[D].f)) v[D] = cc;
-                else shrink = true;
-            }
-            s.evaluations -= 4 - used;
-            if (shrink) {
-                xs.clear();
-                for (int i = 1; i <= D; ++i) {
-                    Arr<D> x;
-                    for (int d = 0; d < D; ++d) x[d] = v[0].x[d] + 0.5 * (v[i].x[d] - v[0].x[d]);
-                    xs.push_back(clampx(x));
-                }
-                co_await eval_all();
-                for (int i = 1; i <= D; ++i) v[i] = Pt<D>{xs[i - 1], -rq[i - 1].lnl};
-            }
-            continue;
-        }
-        const auto [xrc, rr] = one(xr);
-        const Pt<D> r{xrc, -(co_await Eval{s, rr})};
-        if (r.f < v[0].f) {
-            Arr<D> xe;
-            for (int d = 0; d < D; ++d) xe[d] = c[d] + 2.0 * (r.x[d] - c[d]);
-            const auto [xec, re] = one(xe);
-            const Pt<D> e{xec, -(co_await Eval{s, re})};
-            v[D] = (e.f < r.f) ? e : r;
-        } else if (r.f < v[D - 1].f) {
-            v[D] = r;
-        } else {
-            const bool outside = r.f < v[D].f;
-            Arr<D> xc;
-            for (int d = 0; d < D; ++d) xc[d] = c[d] + 0.5 * ((outside ? r.x[d] : v[D].x[d]) - c[d]);
-            const auto [xcc, rc] = one(xc);
-            const Pt<D> cc{xcc, -(co_await Eval{s, rc})};
-            if (cc.f < (outside ? r.f : v[D].f)) {
-                v[D] = cc;
-            } else {
-                xs.clear();
-                for (int i = 1; i <= D; ++i) {
-                    Arr<D> x;
-                    for (int d = 0; d < D; ++d) x[d] = v[0].x[d] + 0.5 * (v[i].x[d] - v[0].x[d]);
-                    xs.push_back(clampx(x));
-                }
-                co_await eval_all();
-                for (int i = 1; i <= D; ++i) v[i] = Pt<D>{xs[i - 1], -rq[i - 1].lnl};
-            }
-        }
-    }
-    std::sort(v.begin(), v.end(), by_f);
-    co_return v[0];
-}
-
 struct MemeOut {
     h3g_meme_result r{};
     double omega1 = 0.0;      // omega of component 1 at the reported MLE
@@ -304,8 +165,8 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
         opt.temp_slots = std::min(2 * opt.max_requests, 32768);
         opt.spec_threshold = 32;            // four candidates per site still fit one wave of the pruning kernel
         std::string err;
-        FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, opt.max_requests,
-                                           slots_needed(N, opt.temp_slots), &err);
+        FelDevice* dev = fel_device_create(prob, S, m->pi, m->Qs, m->Qn, branch_lengths, nullptr, opt.max_requests,
+                                           slots_needed(N, opt.temp_slots, opt.components), &err);
         if (!dev) { fel_set_error(prob, "h3g_meme_run: " + err); return H3G_ERR_CUDA; }
         std::vector<Site> sites(N);
         std::vector<h3g_fel_result> fel(N, h3g_fel_result{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0});
@@ -346,7 +207,7 @@ extern "C" h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* m, co
                 const double om[2] = {mo[i].omega1, r.beta_plus / r.alpha};
                 int own[2];
                 for (int c = 0; c < 2; ++c) {
-                    own[c] = own_slot(i, 1 - s.buf[c], c);
+                    own[c] = own_slot(i, 1 - s.buf[c], c, opt.components);
                     eom.push_back(om[c]);
                     eslot.push_back(own[c]);
                     eprev.push_back(s.slot[c]);

@@ -17,7 +17,9 @@ uint64_t bits_of(double x) {
 h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fit>& fits, const LockstepOptions& opt,
                         LockstepState& state, std::string* err) {
     const int N = int(sites.size());
-    const int temp_base = slots_needed(N, 0);
+    const int C = opt.components;
+    if (C < 2 || C > 3) { *err = "components must be 2 or 3"; return H3G_ERR_STATE; }
+    const int temp_base = slots_needed(N, 0, C);
     for (int i = 0; i < N; ++i) {
         sites[i].resume = fits[i].h;
         sites[i].pending = nullptr;
@@ -33,10 +35,10 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
     std::unordered_map<uint64_t, int> users;           // omega bits -> sites requesting it this batch
     std::unordered_map<uint64_t, int> temp;            // omega bits -> pool slot (this batch)
     std::vector<uint64_t> keys;
-    std::vector<int> admitted, req_pat, req_slot, req_slot2, eig_slot, eig_prev;
+    std::vector<int> admitted, req_pat, req_slot, req_slot2, req_slot3, eig_slot, eig_prev;
     std::vector<double> req_a, req_w1, eig_om, lnl;
     std::vector<Req*> req_ptr;
-    const size_t n_slots = size_t(slots_needed(N, opt.temp_slots));
+    const size_t n_slots = size_t(slots_needed(N, opt.temp_slots, C));
     if (state.written.size() < n_slots) {
         state.written.resize(n_slots, -1);
         state.solved.resize(n_slots, 0);
@@ -53,8 +55,10 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
             any = true;
             keys.clear();
             for (const Req& r : *s.pending)
-                for (int c = 0; c < (r.om2 >= 0.0 ? 2 : 1); ++c) {
-                    const double om = c ? r.om2 : r.om1;
+                for (int c = 0; c < 3; ++c) {
+                    if (!req_has(r, c)) continue;
+                    if (c >= C) { *err = "a request has more components than the run"; return H3G_ERR_STATE; }
+                    const double om = req_omega(r, c);
                     if (s.slot[c] >= 0 && std::fabs(om - s.cached[c]) <= opt.cache_tol) continue;
                     keys.push_back(bits_of(om));
                 }
@@ -64,10 +68,10 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
         }
         if (!any) break;
         temp.clear();
-        admitted.clear(); req_pat.clear(); req_slot.clear(); req_slot2.clear(); req_a.clear(); req_w1.clear();
+        admitted.clear(); req_pat.clear(); req_slot.clear(); req_slot2.clear(); req_slot3.clear(); req_a.clear(); req_w1.clear();
         eig_om.clear(); eig_slot.clear(); eig_prev.clear(); req_ptr.clear();
         int temp_used = 0;
-        bool mixed = false;
+        bool mixed = false, background = false;
         auto solve = [&](double om, int slot, int prev) {
             eig_om.push_back(om);
             eig_slot.push_back(slot);
@@ -79,16 +83,19 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
             const int k = int(s.pending->size());
             if (int(req_pat.size()) + k > opt.max_requests) continue;       // next batch
             const bool single = k == 1;
-            if (!single && temp_used + 2 * k > opt.temp_slots) continue;    // next batch
+            int need = 0;                                                    // eigensystems of the site's requests
+            for (const Req& r : *s.pending)
+                for (int c = 0; c < C; ++c) need += req_has(r, c) ? 1 : 0;
+            if (!single && temp_used + need > opt.temp_slots) continue;     // next batch
             admitted.push_back(i);
-            int flip_slot[2] = {-1, -1};
-            double flip_om[2] = {0.0, 0.0};
+            int flip_slot[3] = {-1, -1, -1};
+            double flip_om[3] = {0.0, 0.0, 0.0};
             bool first = true;
             for (Req& r : *s.pending) {
-                const int nc = r.om2 >= 0.0 ? 2 : 1;
-                int sl[2] = {-1, -1};
-                for (int c = 0; c < nc; ++c) {
-                    const double om = c ? r.om2 : r.om1;
+                int sl[3] = {-1, -1, -1};
+                for (int c = 0; c < C; ++c) {
+                    if (!req_has(r, c)) continue;
+                    const double om = req_omega(r, c);
                     if (s.slot[c] >= 0 && std::fabs(om - s.cached[c]) <= opt.cache_tol) { sl[c] = s.slot[c]; continue; }
                     const uint64_t key = bits_of(om);
                     int slot = -1;
@@ -103,7 +110,7 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
                             slot = t->second;
                         } else {
                             if (first) {                    // into the site's other buffer, current afterwards
-                                slot = own_slot(i, 1 - s.buf[c], c);
+                                slot = own_slot(i, 1 - s.buf[c], c, C);
                                 flip_slot[c] = slot;
                                 flip_om[c] = om;
                             } else {
@@ -113,7 +120,7 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
                             solve(om, slot, s.slot[c]);     // warm start from the site's current eigensystem
                         }
                     } else {
-                        slot = own_slot(i, s.buf[c], c);
+                        slot = own_slot(i, s.buf[c], c, C);
                         solve(om, slot, s.slot[c]);         // in place when the current one is the site's own
                     }
                     if (single) { s.slot[c] = slot; s.cached[c] = om; }
@@ -122,13 +129,15 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
                 first = false;
                 req_pat.push_back(s.pattern);
                 req_a.push_back(r.a);
-                req_w1.push_back(nc == 2 ? r.w1 : 1.0);
+                req_w1.push_back(sl[1] >= 0 ? r.w1 : 1.0);
                 req_slot.push_back(sl[0]);
                 req_slot2.push_back(sl[1]);
+                req_slot3.push_back(sl[2]);
                 req_ptr.push_back(&r);
-                mixed = mixed || nc == 2;
+                mixed = mixed || sl[1] >= 0;
+                background = background || sl[2] >= 0;
             }
-            for (int c = 0; c < 2; ++c)
+            for (int c = 0; c < C; ++c)
                 if (flip_slot[c] >= 0) {
                     s.buf[c] ^= 1;
                     s.slot[c] = flip_slot[c];
@@ -152,7 +161,8 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
         }
         for (size_t e = 0; e < eig_slot.size(); ++e) solved[size_t(eig_slot[e])] = 1;
         for (size_t r = 0; r < req_slot.size(); ++r)
-            if (!solved[size_t(req_slot[r])] || (req_slot2[r] >= 0 && !solved[size_t(req_slot2[r])])) {
+            if (!solved[size_t(req_slot[r])] || (req_slot2[r] >= 0 && !solved[size_t(req_slot2[r])]) ||
+                (req_slot3[r] >= 0 && !solved[size_t(req_slot3[r])])) {
                 *err = "a request reads an eigensystem that was never solved";
                 return H3G_ERR_STATE;
             }
@@ -160,7 +170,7 @@ h3g_status run_lockstep(FelDevice* dev, std::vector<Site>& sites, std::vector<Fi
         lnl.assign(req_pat.size(), 0.0);
         if (!fel_device_eval(dev, int(eig_om.size()), eig_om.data(), eig_slot.data(), eig_prev.data(), int(req_pat.size()),
                              req_pat.data(), req_a.data(), req_slot.data(), mixed ? req_slot2.data() : nullptr,
-                             mixed ? req_w1.data() : nullptr, lnl.data(), err))
+                             mixed ? req_w1.data() : nullptr, background ? req_slot3.data() : nullptr, lnl.data(), err))
             return H3G_ERR_CUDA;
         for (size_t r = 0; r < req_ptr.size(); ++r) req_ptr[r]->lnl = lnl[r];
         const bool small = int(req_pat.size()) <= opt.spec_threshold;

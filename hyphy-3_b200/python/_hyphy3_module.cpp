@@ -52,7 +52,8 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("parent_id", &TreeNode::parent_id)
         .def_readonly("children", &TreeNode::children)
         .def_readwrite("branch_length", &TreeNode::branch_length)
-        .def_readonly("is_leaf", &TreeNode::is_leaf);
+        .def_readonly("is_leaf", &TreeNode::is_leaf)
+        .def_readonly("model_tag", &TreeNode::model_tag);
 
     py::class_<Tree>(m, "Tree")
         .def(py::init<>())
@@ -61,6 +62,18 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_static("from_newick_file", &Tree::from_newick_file, "filepath"_a, "keep_rooted"_a = true)
         .def("num_nodes", &Tree::num_nodes)
         .def("num_leaves", &Tree::num_leaves)
+        .def("select_branches", [](const Tree& t, const std::string& spec, const std::string& regex,
+                                   const std::vector<std::string>& names, bool auto_detect, bool throw_on_empty) {
+                 const auto sel = t.select_branches(spec, regex, names, auto_detect, throw_on_empty);
+                 py::dict d;
+                 d["is_selected"] = sel.is_selected;
+                 d["selected_names"] = sel.selected_names;
+                 d["unselected_names"] = sel.unselected_names;
+                 d["num_selected"] = sel.num_selected;
+                 d["num_unselected"] = sel.num_unselected;
+                 return d;
+             }, "spec"_a = "All", "regex"_a = "", "explicit_names"_a = std::vector<std::string>{},
+             "auto_detect_test_tags_when_all"_a = false, "throw_on_empty"_a = true)
         .def_readonly("root_id", &Tree::root_id)
         .def_readonly("post_order", &Tree::post_order)
         .def_readonly("nodes", &Tree::nodes)
@@ -281,10 +294,18 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("log_l_null", &SiteResult::log_l_null)
         .def_readonly("evaluations", &SiteResult::evaluations);
     py::class_<FELAnalyzer>(m, "FELAnalyzer")
-        .def(py::init([](Tree tree, Alignment aln, const MG94Parameters& params, const FELSettings& settings) {
-                 return FELAnalyzer(std::move(tree), std::move(aln), params, settings);
+        .def(py::init([](Tree tree, Alignment aln, const MG94Parameters& params, const FELSettings& settings, Scalar bg_om) {
+                 return FELAnalyzer(std::move(tree), std::move(aln), params, settings, bg_om);
              }),
-             "tree"_a, "alignment"_a, "params"_a = MG94Parameters{}, "settings"_a = FELSettings{})
+             "tree"_a, "alignment"_a, "params"_a = MG94Parameters{}, "settings"_a = FELSettings{}, "background_omega"_a = -1.0)
+        .def_readonly("is_test_branch", &FELAnalyzer::is_test_branch)
+        .def_readonly("test_branch_names", &FELAnalyzer::test_branch_names)
+        .def_readonly("bg_branch_names", &FELAnalyzer::bg_branch_names)
+        .def_readonly("num_tested", &FELAnalyzer::num_tested)
+        .def_readonly("num_background", &FELAnalyzer::num_background)
+        .def_readonly("baseline_tested_tree_length", &FELAnalyzer::baseline_tested_tree_length)
+        .def_readonly("baseline_bg_tree_length", &FELAnalyzer::baseline_bg_tree_length)
+        .def_readonly("tree", &FELAnalyzer::tree)
         .def("run", [](FELAnalyzer& f, bool show_progress, bool force_progress) {
                  py::gil_scoped_release rel;
                  return f.run(show_progress, force_progress);

@@ -26,6 +26,7 @@ EXPORTED = [
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
+    "h3g_fel_run_tested",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -47,7 +48,8 @@ class FelModel(C.Structure):
 
 class FelResult(C.Structure):
     _fields_ = [("alpha", C.c_double), ("beta", C.c_double), ("alpha_null", C.c_double), ("log_l_alt", C.c_double),
-                ("log_l_null", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double), ("evaluations", C.c_int)]
+                ("log_l_null", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double), ("evaluations", C.c_int),
+                ("beta_nuisance", C.c_double)]
 
 
 class MemeResult(C.Structure):
@@ -96,6 +98,7 @@ def load() -> C.CDLL:
                                                 C.POINTER(C.c_int32), C.c_int, C.c_int, C.POINTER(C.c_int8),
                                                 C.POINTER(C.c_uint64), _dp, C.c_int, _dp, _dp, _dp, _dp]
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
+        lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         for name in EXPORTED:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
@@ -226,15 +229,23 @@ class Problem:
             self.h, int(pi.size), _ptr(pi), _ptr(Q), _ptr(lam), _ptr(U), _ptr(V), _ptr(bl), precision, C.byref(lnl), _ptr(g)))
         return lnl.value, g
 
-    def fel_run(self, *, pi, Qs, Qn, branch_lengths) -> dict:
-        """FEL per-pattern fits (h3g_fel_run); branch lengths in FEL time.  Returns arrays per pattern."""
+    def fel_run(self, *, pi, Qs, Qn, branch_lengths, tested=None) -> dict:
+        """FEL per-pattern fits (h3g_fel_run, or h3g_fel_run_tested when tested[n_nodes] is given);
+        branch lengths in FEL time.  Returns arrays per pattern."""
         pi, Qs, Qn, bl = _f64(pi), _f64(Qs), _f64(Qn), _f64(branch_lengths)
         S = int(pi.size)
         if Qs.shape != (S, S) or Qn.shape != (S, S) or bl.size != self.n:
             raise ValueError("Qs, Qn must be S x S and branch_lengths one per node")
         m = FelModel(S=S, pi=_ptr(pi), Qs=_ptr(Qs), Qn=_ptr(Qn))
         res = (FelResult * max(self.P, 1))()
-        self.ctx.check(self.ctx.lib.h3g_fel_run(self.h, C.byref(m), _ptr(bl), res))
+        if tested is None:
+            self.ctx.check(self.ctx.lib.h3g_fel_run(self.h, C.byref(m), _ptr(bl), res))
+        else:
+            tv = np.ascontiguousarray(np.asarray(tested, dtype=bool), dtype=np.uint8)
+            if tv.size != self.n:
+                raise ValueError("tested needs one entry per node")
+            self.ctx.check(self.ctx.lib.h3g_fel_run_tested(
+                self.h, C.byref(m), _ptr(bl), tv.ctypes.data_as(C.POINTER(C.c_uint8)), res))
         names = [f[0] for f in FelResult._fields_]
         return {k: np.array([getattr(res[i], k) for i in range(self.P)]) for k in names}
 

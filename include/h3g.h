@@ -206,6 +206,7 @@ typedef struct {
     double log_l_alt, log_l_null;
     double lrt, p_value;
     int evaluations;          /* likelihood evaluations used; 0 for an invariant pattern (not fitted) */
+    double beta_nuisance;     /* beta on the background branches (h3g_fel_run_tested with a background); else 0 */
 } h3g_fel_result;
 
 /* Fit every pattern of prob.  branch_lengths[n_nodes] are in the reference's
@@ -215,6 +216,20 @@ typedef struct {
  * whole run moved between host and device, and h3g_last_eval_stats the run's
  * host wall time and kernel launches. */
 h3g_status h3g_fel_run(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths, h3g_fel_result* out);
+
+/* As h3g_fel_run with the tested branches given: tested[n_nodes] != 0 marks a
+ * tested branch (the root's entry is ignored).  When every branch is tested
+ * this is h3g_fel_run.  Otherwise every pattern runs the reference's
+ * branch-subset search (FELAnalyzer::analyze_pattern, fel.hpp:462-572): the
+ * alternative model has alpha, beta on the tested branches and beta_nuisance
+ * on the others (12-point grid, bounded 3-D Nelder-Mead), the null model sets
+ * beta = alpha (the initial point and a 7 x 4 grid, bounded 2-D Nelder-Mead).
+ * A branch evolves under Q = alpha Qs + beta Qn of its set, i.e. the MG94
+ * model Qs + (beta / alpha) Qn with time scaled by alpha; when
+ * |beta - beta_nuisance| < 1e-9 both sets use the tested one.  Background
+ * branch lengths are converted by the caller (fel.hpp:230-266). */
+h3g_status h3g_fel_run_tested(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths,
+                              const uint8_t* tested, h3g_fel_result* out);
 
 /* ---------------------------------------------------------------- MEME
  * Mixed-effects model of episodic selection per site on the device, replacing

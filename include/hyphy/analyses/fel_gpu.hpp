@@ -4,10 +4,12 @@
 // Same constructor and run() as the reference class: the constructor converts
 // branch lengths to the FEL time scale (t x 3 / mean rate of the base MG94
 // model, fel.hpp:230-273); run() fits every site pattern (fel.hpp:326-446)
-// and maps patterns back to sites (fel.hpp:778-833).  Only the path where every
-// branch is tested (FELSettings::test_branches == "All", no regex, no names)
-// is on the device; any other selection throws std::runtime_error.  Ancestral
-// substitution summaries (SiteResult::subs in the reference) are not produced.
+// and maps patterns back to sites (fel.hpp:778-833).  The tested branches are
+// chosen as in the reference (Tree::select_branches with {T}-tag detection,
+// fel.hpp:215-227); with a background set every pattern runs the reference's
+// branch-subset search (fel.hpp:462-572) through h3g_fel_run_tested.
+// Ancestral substitution summaries (SiteResult::subs in the reference) and
+// bridge resolutions are not produced.
 #pragma once
 
 #include <stdexcept>
@@ -56,30 +58,61 @@ public:
     Scalar p_value_threshold = 0.1;
     Scalar baseline_tree_length = 0.0;
     Scalar baseline_tested_tree_length = 0.0;
+    Scalar baseline_bg_tree_length = 0.0;
     Scalar conversion_factor = 1.0;
     std::vector<SiteResult> site_results;
 
+    // branch partition (fel.hpp:215-227)
+    std::vector<bool> is_test_branch;
+    std::vector<std::string> test_branch_names;
+    std::vector<std::string> bg_branch_names;
+    size_t num_tested = 0;
+    size_t num_background = 0;
+    Scalar background_omega = -1.0;
+
     FELAnalyzer(Tree t, Alignment a, MG94Parameters params = MG94Parameters{}, FELSettings s = FELSettings{}, Scalar bg_om = -1.0)
-        : tree(std::move(t)), aln(std::move(a)), base_params(params), settings(std::move(s)) {
-        (void)bg_om;
-        if (settings.test_branches != "All" || !settings.test_branch_regex.empty() || !settings.test_branch_names.empty())
-            throw std::runtime_error("FELAnalyzer (device): only the all-branches-tested analysis is supported");
+        : tree(std::move(t)), aln(std::move(a)), base_params(params), settings(std::move(s)), background_omega(bg_om) {
         p_value_threshold = settings.p_value_threshold;
         prepare_branch_lengths();
     }
 
-    // fel.hpp:230-273 with every branch tested
+    void partition_branches() {
+        auto sel = tree.select_branches(settings.test_branches, settings.test_branch_regex, settings.test_branch_names, true);
+        is_test_branch = std::move(sel.is_selected);
+        test_branch_names = std::move(sel.selected_names);
+        bg_branch_names = std::move(sel.unselected_names);
+        num_tested = sel.num_selected;
+        num_background = sel.num_unselected;
+    }
+
+    // fel.hpp:230-273: tested branches t x 3 / mean rate of the base model; background ones
+    // by the mean rate at omega = background_omega when that is > 0
     void prepare_branch_lengths() {
+        partition_branches();
         const auto& code = aln.code ? *aln.code : *hyphy::core::GeneticCode::universal();
         MG94Matrix base;
         base.update(base_params, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
         conversion_factor = base.scale_factor > 1e-12 ? 3.0 / base.scale_factor : 1.0;
-        baseline_tree_length = baseline_tested_tree_length = 0.0;
+        Scalar bg_conv = conversion_factor;
+        if (num_background > 0 && background_omega > 0.0) {
+            MG94Parameters pbg = base_params;
+            pbg.alpha = 1.0;
+            pbg.beta = background_omega;
+            MG94Matrix mbg;
+            mbg.update(pbg, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+            if (mbg.scale_factor > 1e-12) bg_conv = 3.0 / mbg.scale_factor;
+        }
+        baseline_tree_length = baseline_tested_tree_length = baseline_bg_tree_length = 0.0;
         for (auto& node : tree.nodes) {
             if (node.id == tree.root_id) continue;
             baseline_tree_length += node.branch_length;
-            baseline_tested_tree_length += node.branch_length;
-            node.branch_length *= conversion_factor;
+            if (is_test_branch[size_t(node.id)]) {
+                baseline_tested_tree_length += node.branch_length;
+                node.branch_length *= conversion_factor;
+            } else {
+                baseline_bg_tree_length += node.branch_length;
+                node.branch_length *= bg_conv;
+            }
         }
     }
 
@@ -109,13 +142,16 @@ public:
             if (node.id != tree.root_id) bl[size_t(node.id)] = node.branch_length;
         h3g_fel_model m{S, pi.data(), qs.data(), qn.data()};
         std::vector<h3g_fel_result> res(aln.patterns.size());
-        eng.check(h3g_fel_run(pr, &m, bl.data(), res.data()));
+        std::vector<uint8_t> tested(tree.num_nodes(), 1);
+        for (const auto& node : tree.nodes)
+            if (node.id != tree.root_id) tested[size_t(node.id)] = is_test_branch[size_t(node.id)] ? 1 : 0;
+        eng.check(h3g_fel_run_tested(pr, &m, bl.data(), tested.data(), res.data()));
         site_results.assign(aln.num_codons, SiteResult{});
         for (size_t s = 0; s < aln.num_codons; ++s) {
             const auto& r = res[aln.site_to_pattern[s]];
             SiteResult& o = site_results[s];
             o.site_index = s;
-            o.alpha = r.alpha; o.beta = r.beta; o.alpha_null = r.alpha_null;
+            o.alpha = r.alpha; o.beta = r.beta; o.beta_nuisance = r.beta_nuisance; o.alpha_null = r.alpha_null;
             o.lrt = r.lrt; o.p_value = r.p_value;
             o.log_l_alt = r.log_l_alt; o.log_l_null = r.log_l_null;
             o.total_branch_length = r.alpha_null * baseline_tested_tree_length;

@@ -19,11 +19,13 @@
 #include <cstdint>
 #include <fstream>
 #include <memory>
+#include <regex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
 #include <string_view>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 namespace hyphy::core {
@@ -592,6 +594,26 @@ public:
         }
     }
 
+    struct BranchSelection {
+        std::vector<bool> is_selected;            // per node id; the root is never selected
+        std::vector<std::string> selected_names;  // in node-id order
+        std::vector<std::string> unselected_names;
+        size_t num_selected = 0;
+        size_t num_unselected = 0;
+    };
+
+    // tree.hpp:893-1075: which branches a site analysis tests.  Precedence: a regex (matched,
+    // case-insensitive, against the node name or its {tag}), then explicit names or tags, then
+    // spec: "All" (every branch; with auto_detect, only the branches tagged {T}/{test}/
+    // {foreground}/{fg} when any is), "all-branches", "Internal", "Leaves" / "terminal" /
+    // "tips", "Unlabeled" / "untagged", a comma-separated list of names, tags and those
+    // keywords, or one name or tag (a regex when nothing matches it exactly and it holds
+    // regex metacharacters).  Names, tags and keywords compare case-insensitively, with
+    // surrounding braces and blanks removed.
+    BranchSelection select_branches(const std::string& spec = "All", const std::string& regex_str = "",
+                                    const std::vector<std::string>& explicit_names = {},
+                                    bool auto_detect_test_tags_when_all = false, bool throw_on_empty = true) const;
+
 private:
     void apply_label(int32_t id, std::string tok) {
         TreeNode& nd = nodes[size_t(id)];
@@ -614,6 +636,118 @@ private:
         nd.name = nm;
     }
 };
+
+inline Tree::BranchSelection Tree::select_branches(const std::string& spec, const std::string& regex_str,
+                                                   const std::vector<std::string>& explicit_names,
+                                                   bool auto_detect_test_tags_when_all, bool throw_on_empty) const {
+    auto lower = [](std::string s) {
+        for (auto& ch : s) ch = char(std::tolower(static_cast<unsigned char>(ch)));
+        return s;
+    };
+    auto unbrace = [](const std::string& s) {
+        const auto blank = [](char ch) { return ch == ' ' || ch == '\t' || ch == '\r' || ch == '\n'; };
+        size_t b = 0, e = s.size();
+        while (b < e && blank(s[b])) ++b;
+        while (e > b && blank(s[e - 1])) --e;
+        if (e - b >= 2 && s[b] == '{' && s[e - 1] == '}') {
+            ++b; --e;
+            while (b < e && blank(s[b])) ++b;
+            while (e > b && blank(s[e - 1])) --e;
+        }
+        return s.substr(b, e - b);
+    };
+    auto fg = [](const std::string& t) { return t == "t" || t == "test" || t == "foreground" || t == "fg"; };
+    auto bg = [](const std::string& t) { return t == "r" || t == "ref" || t == "reference" || t == "background" || t == "bg"; };
+    auto regex_match = [&](const std::regex& re, const TreeNode& nd) {
+        return std::regex_search(nd.name, re) || (!nd.model_tag.empty() && std::regex_search(nd.model_tag, re));
+    };
+    BranchSelection sel;
+    sel.is_selected.assign(nodes.size(), false);
+    auto each = [&](auto&& pick) {
+        for (const auto& nd : nodes)
+            if (nd.id != root_id) sel.is_selected[size_t(nd.id)] = pick(nd);
+    };
+    if (!regex_str.empty()) {
+        const std::regex re(regex_str, std::regex::icase);
+        each([&](const TreeNode& nd) { return regex_match(re, nd); });
+    } else if (!explicit_names.empty()) {
+        std::unordered_set<std::string> want;
+        for (const auto& item : explicit_names) {
+            const std::string k = lower(unbrace(item));
+            if (!k.empty()) want.insert(k);
+        }
+        each([&](const TreeNode& nd) {
+            const std::string tag = lower(nd.model_tag);
+            return want.count(lower(nd.name)) > 0 || (!tag.empty() && want.count(tag) > 0);
+        });
+    } else {
+        const std::string mode = unbrace(spec), m = lower(mode);
+        if (m.empty() || m == "all") {
+            bool tagged = false;
+            if (auto_detect_test_tags_when_all)
+                for (const auto& nd : nodes)
+                    if (nd.id != root_id && fg(lower(nd.model_tag))) tagged = true;
+            each([&](const TreeNode& nd) { return tagged ? fg(lower(nd.model_tag)) : true; });
+        } else if (m == "all-branches" || m == "all_branches") {
+            each([](const TreeNode&) { return true; });
+        } else if (m == "internal") {
+            each([](const TreeNode& nd) { return !nd.is_leaf; });
+        } else if (m == "leaves" || m == "terminal" || m == "tips") {
+            each([](const TreeNode& nd) { return nd.is_leaf; });
+        } else if (m == "unlabeled" || m == "untagged") {
+            each([](const TreeNode& nd) { return nd.model_tag.empty(); });
+        } else if (mode.find(',') != std::string::npos) {
+            std::unordered_set<std::string> tok;
+            std::stringstream ss(mode);
+            for (std::string item; std::getline(ss, item, ',');) {
+                const std::string k = lower(unbrace(item));
+                if (!k.empty()) tok.insert(k);
+            }
+            auto any = [&](auto&& pred) {
+                for (const auto& k : tok)
+                    if (pred(k)) return true;
+                return false;
+            };
+            each([&](const TreeNode& nd) {
+                const std::string name = lower(nd.name), tag = lower(nd.model_tag);
+                if (tok.count(name) || (!tag.empty() && tok.count(tag))) return true;
+                if (tok.count("internal") && !nd.is_leaf) return true;
+                if ((tok.count("leaves") || tok.count("terminal")) && nd.is_leaf) return true;
+                if ((tok.count("unlabeled") || tok.count("untagged")) && nd.model_tag.empty()) return true;
+                if (fg(tag) && any(fg)) return true;
+                return bg(tag) && any(bg);
+            });
+        } else {
+            bool hit = false;
+            each([&](const TreeNode& nd) {
+                const std::string name = lower(nd.name), tag = lower(nd.model_tag);
+                const bool ok = (!tag.empty() && tag == m) || name == m || (fg(m) && fg(tag)) || (bg(m) && bg(tag));
+                hit = hit || ok;
+                return ok;
+            });
+            if (!hit && spec.find_first_of(".*+?^$[]()|\\") != std::string::npos) {
+                try {
+                    const std::regex re(spec, std::regex::icase);
+                    each([&](const TreeNode& nd) { return regex_match(re, nd); });
+                } catch (const std::regex_error&) {
+                }
+            }
+        }
+    }
+    for (const auto& nd : nodes) {
+        if (nd.id == root_id) continue;
+        if (sel.is_selected[size_t(nd.id)]) {
+            sel.selected_names.push_back(nd.name);
+            ++sel.num_selected;
+        } else {
+            sel.unselected_names.push_back(nd.name);
+            ++sel.num_unselected;
+        }
+    }
+    if (throw_on_empty && sel.num_selected == 0 && nodes.size() > 1)
+        throw std::runtime_error("No branches matched '--branches " + (regex_str.empty() ? spec : regex_str) + "'.");
+    return sel;
+}
 
 // ----------------------------------------------------------------- MG94xREV
 struct MG94Parameters {

@@ -1261,6 +1261,138 @@ inline NMPointN<D> nelder_mead_nd(F&& f, const std::array<double, D>& init, cons
     return s[0];
 }
 
+// ------------------------------------------------------------ FEL, branch subsets
+// fel.hpp:215-266 (partition_branches, prepare_branch_lengths) and :462-572
+// (analyze_pattern with num_background > 0), without bridge resolutions.
+
+struct FelSubsetSite {
+    double alpha = 0, beta = 0, beta_nuisance = 0, alpha_null = 0, lrt = 0, p_value = 1, total_bl = 0;
+    double lnl_alt = 0, lnl_null = 0;
+    int evals = 0;
+};
+struct FelSubsetRun {
+    double conversion = 1.0, bg_conversion = 1.0, tested_length = 0.0, bg_length = 0.0;
+    std::vector<double> bl;           // branch lengths in FEL time
+    std::vector<char> tested;         // per node; the root's entry is 0
+    std::vector<FelSubsetSite> patterns;
+};
+
+// tested branches t * 3 / mu(base); background ones t * 3 / mu(alpha 1, beta bg_omega) when
+// bg_omega > 0, else as the tested ones (fel.hpp:230-266)
+inline FelSubsetRun fel_prepare_tested(const Tree& tr, const Alignment& a, const Params& base, const std::vector<char>& tested,
+                                       double bg_omega = -1.0) {
+    FelSubsetRun r;
+    MG94 m0; m0.update(base, a.pos_freq, a.pi, a.code);
+    r.conversion = m0.mu > 1e-12 ? 3.0 / m0.mu : 1.0;
+    r.bg_conversion = r.conversion;
+    r.tested.assign(tr.n(), 0);
+    bool any_bg = false;
+    for (int i = 0; i < tr.n(); ++i)
+        if (i != tr.root) { r.tested[i] = tested[i] ? 1 : 0; any_bg = any_bg || !tested[i]; }
+    if (any_bg && bg_omega > 0.0) {
+        Params q = base; q.alpha = 1.0; q.beta = bg_omega;
+        MG94 mb; mb.update(q, a.pos_freq, a.pi, a.code);
+        if (mb.mu > 1e-12) r.bg_conversion = 3.0 / mb.mu;
+    }
+    r.bl.assign(tr.n(), 0.0);
+    for (int i = 0; i < tr.n(); ++i) {
+        if (i == tr.root) continue;
+        if (r.tested[i]) { r.tested_length += tr.bl[i]; r.bl[i] = tr.bl[i] * r.conversion; }
+        else { r.bg_length += tr.bl[i]; r.bl[i] = tr.bl[i] * r.bg_conversion; }
+    }
+    return r;
+}
+
+// fel.hpp:462-572: the likelihood builds MG94(alpha = a, beta = b_test) for the tested branches
+// and MG94(a, b_bg) for the others at the FEL-time lengths, one model for all when
+// |b_test - b_bg| < 1e-9; 3-D Nelder-Mead for the alternative, 2-D for the null (beta = alpha)
+inline FelSubsetSite fel_pattern_subset(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
+                                        const FelSubsetRun& run, int p) {
+    FelSubsetSite res;
+    int first = -1; bool invariant = true;
+    for (int t = 0; t < a.T; ++t) {
+        const int st = a.states[size_t(p) * a.T + t];
+        if (st >= 0) { if (first == -1) first = st; else if (st != first) { invariant = false; break; } }
+    }
+    if (invariant) return res;
+    const int S = a.code.S, n = tr.n();
+    std::vector<Mat> Pb(n, Mat::eye(S));
+    Pass w;
+    MG94 mt, mb;
+    auto lnl = [&](double aa, double bt, double bb) {
+        ++res.evals;
+        Params qt = base; qt.alpha = aa; qt.beta = bt;
+        mt.update(qt, a.pos_freq, a.pi, a.code);
+        const bool same = std::fabs(bt - bb) < 1e-9;
+        if (!same) { Params qb = base; qb.alpha = aa; qb.beta = bb; mb.update(qb, a.pos_freq, a.pi, a.code); }
+        for (int i = 0; i < n; ++i)
+            if (i != tr.root) Pb[i] = (same || run.tested[i]) ? mt.P(run.bl[i]) : mb.P(run.bl[i]);
+        inside_outside(tr, a, p, l2t, Pb, mt.pi, S, w, false);
+        return w.logL;
+    };
+    using A3 = std::array<double, 3>;
+    using A2 = std::array<double, 2>;
+    static const double g3[12][3] = {{0.01, 0.1, 0.1}, {1.0, 0.1, 0.1}, {1.0, 0.5, 0.5},   {1.0, 1.0, 1.0},
+                                     {1.0, 5.0, 5.0},  {10.0, 0.1, 0.1}, {0.01, 0.5, 0.5}, {0.01, 5.0, 5.0},
+                                     {10.0, 0.5, 0.5}, {10.0, 1.0, 1.0}, {10.0, 50.0, 50.0}, {100.0, 1.0, 1.0}};
+    double best = -1e20;
+    A3 init = {1.0, 1.0, 1.0};
+    for (const auto& g : g3) {
+        const double l = lnl(g[0], g[1], g[2]);
+        if (l > best) { best = l; init = {g[0], g[1], g[2]}; }
+    }
+    const auto alt = nelder_mead_nd<3>([&](const A3& x) { return -lnl(x[0], x[1], x[2]); }, init, A3{1e-4, 1e-4, 1e-4},
+                                       A3{1000.0, 1000.0, 1000.0}, 1e-4, 100, {});
+    res.alpha = alt.x[0]; res.beta = alt.x[1]; res.beta_nuisance = alt.x[2]; res.lnl_alt = -alt.f;
+    const double ina = (std::min(res.alpha, 100.0) + 3.0 * std::min(res.beta, 100.0)) / 4.0, inb = res.beta_nuisance;
+    double best_null = lnl(ina, ina, inb);
+    A2 initn = {ina, inb};
+    for (double ca : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0})
+        for (double cb : {inb, 0.1, 1.0, 5.0}) {
+            const double l = lnl(ca, ca, cb);
+            if (l > best_null) { best_null = l; initn = {ca, cb}; }
+        }
+    const auto nul = nelder_mead_nd<2>([&](const A2& x) { return -lnl(x[0], x[0], x[1]); }, initn, A2{1e-4, 1e-4},
+                                       A2{1000.0, 1000.0}, 1e-4, 80, {});
+    res.alpha_null = nul.x[0]; res.lnl_null = -nul.f;
+    double lrt = 0.0;
+    if (res.lnl_alt > -1e10 && res.lnl_null > -1e10) lrt = std::max(0.0, 2.0 * (res.lnl_alt - res.lnl_null));
+    res.lrt = lrt;
+    res.p_value = std::erfc(std::sqrt(lrt / 2.0));
+    res.total_bl = res.alpha_null * run.tested_length;
+    return res;
+}
+
+// one likelihood of the subset model (for checks of the device evaluator)
+inline double fel_subset_lnl(const Tree& tr, const Alignment& a, const Params& base, const FelSubsetRun& run, int p,
+                             double aa, double bt, double bb) {
+    const auto l2t = leaf_map(tr, a);
+    const int S = a.code.S, n = tr.n();
+    std::vector<Mat> Pb(n, Mat::eye(S));
+    Pass w;
+    MG94 mt, mb;
+    Params qt = base; qt.alpha = aa; qt.beta = bt;
+    mt.update(qt, a.pos_freq, a.pi, a.code);
+    const bool same = std::fabs(bt - bb) < 1e-9;
+    if (!same) { Params qb = base; qb.alpha = aa; qb.beta = bb; mb.update(qb, a.pos_freq, a.pi, a.code); }
+    for (int i = 0; i < n; ++i)
+        if (i != tr.root) Pb[i] = (same || run.tested[i]) ? mt.P(run.bl[i]) : mb.P(run.bl[i]);
+    inside_outside(tr, a, p, l2t, Pb, mt.pi, S, w, false);
+    return w.logL;
+}
+
+// fel.hpp:778-833 (run) with a background: every pattern, in parallel
+inline FelSubsetRun fel_run_tested(const Tree& tr, const Alignment& a, const Params& base, const std::vector<char>& tested,
+                                   double bg_omega = -1.0, int max_patterns = -1) {
+    FelSubsetRun run = fel_prepare_tested(tr, a, base, tested, bg_omega);
+    const auto l2t = leaf_map(tr, a);
+    const int P = max_patterns < 0 ? a.P : std::min(a.P, max_patterns);
+    run.patterns.assign(P, FelSubsetSite{});
+    #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(P))
+    for (int p = 0; p < P; ++p) run.patterns[p] = fel_pattern_subset(tr, a, l2t, base, run, p);
+    return run;
+}
+
 struct MemeSite {
     double alpha = 0, beta1 = 0, p1 = 1, beta_plus = 0, p_plus = 0, lrt = 0, p_value = 1;
     int bus = 0;                      // branches with EBF >= 100

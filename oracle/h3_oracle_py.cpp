@@ -181,6 +181,43 @@ PYBIND11_MODULE(h3oracle, m) {
         d["branch_lengths"] = r.bl;
         return d;
     }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("max_patterns") = -1);
+    m.def("fel_run_tested", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<bool>& tested,
+                               double bg_omega, int max_patterns) {
+        const Params pp = params_from(p);
+        if (int(tested.size()) != t.n()) throw std::runtime_error("tested needs one entry per node");
+        const std::vector<char> tv(tested.begin(), tested.end());
+        FelSubsetRun r;
+        { py::gil_scoped_release rel; r = fel_run_tested(t, a, pp, tv, bg_omega, max_patterns); }
+        const size_t P = r.patterns.size();
+        py::dict d;
+        auto col = [&](auto get) { py::array_t<double> x(P); for (size_t i = 0; i < P; ++i) x.mutable_data()[i] = get(r.patterns[i]); return x; };
+        d["alpha"] = col([](const FelSubsetSite& s) { return s.alpha; });
+        d["beta"] = col([](const FelSubsetSite& s) { return s.beta; });
+        d["beta_nuisance"] = col([](const FelSubsetSite& s) { return s.beta_nuisance; });
+        d["alpha_null"] = col([](const FelSubsetSite& s) { return s.alpha_null; });
+        d["lrt"] = col([](const FelSubsetSite& s) { return s.lrt; });
+        d["p_value"] = col([](const FelSubsetSite& s) { return s.p_value; });
+        d["total_branch_length"] = col([](const FelSubsetSite& s) { return s.total_bl; });
+        d["log_l_alt"] = col([](const FelSubsetSite& s) { return s.lnl_alt; });
+        d["log_l_null"] = col([](const FelSubsetSite& s) { return s.lnl_null; });
+        d["evals"] = col([](const FelSubsetSite& s) { return double(s.evals); });
+        d["conversion"] = r.conversion;
+        d["bg_conversion"] = r.bg_conversion;
+        d["tested_length"] = r.tested_length;
+        d["bg_length"] = r.bg_length;
+        d["branch_lengths"] = r.bl;
+        return d;
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("tested"), py::arg("bg_omega") = -1.0,
+       py::arg("max_patterns") = -1);
+    m.def("fel_subset_lnl", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<bool>& tested,
+                               double bg_omega, int pattern, double alpha, double beta, double beta_bg) {
+        const Params pp = params_from(p);
+        if (int(tested.size()) != t.n()) throw std::runtime_error("tested needs one entry per node");
+        const std::vector<char> tv(tested.begin(), tested.end());
+        const FelSubsetRun r = fel_prepare_tested(t, a, pp, tv, bg_omega);
+        return fel_subset_lnl(t, a, pp, r, pattern, alpha, beta, beta_bg);
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("tested"), py::arg("bg_omega"), py::arg("pattern"),
+       py::arg("alpha"), py::arg("beta"), py::arg("beta_bg"));
     m.def("meme_run", [](const Tree& t, const Alignment& a, const py::dict& p, int max_patterns) {
         const Params pp = params_from(p);
         MemeRun r;

@@ -26,6 +26,8 @@ FILES = {
     # FEL parity on CD2 with matched branch lengths: tests/test_fel_cd2_parity.cpp:66-118
     "cd2.fna": "benchmarks/data/cd2.fna",
     "cd2_fitted.nwk": "benchmarks/data/cd2_fitted.nwk",
+    # FEL branch-subset selection by {T} tags in the embedded tree: tests/test_fel.cpp:128-170
+    "Fig4E.nex": "tests/data/Fig4E.nex",
 }
 
 
@@ -84,7 +86,44 @@ def main(ref: str) -> None:
     # that fit's branch lengths, omega and the GTR exchangeabilities.  Thresholds: tests/test_meme.cpp:66-150.
     known["cd2_meme"] = meme_case(ref_root, "cd2_meme_rel.json", "tests/test_meme.cpp:66-104", 0.95, 0.95, 0.95, 0.95)
     known["adh_meme"] = meme_case(ref_root, "adh_meme_rel.json", "tests/test_meme.cpp:106-144", 0.95, 0.92, 0.95, 0.95)
+    known.update(fel_subset_cases(ref_root))
     (out / "known_answers.json").write_text(json.dumps(known, indent=1) + "\n")
+
+
+def fel_subset_cases(ref_root: pathlib.Path) -> dict:
+    """The branch-subset FEL cases of tests/test_fel.cpp: the cd2_reduced "Leaves" run (its fitted
+    tree, base parameters, tested / background counts and invariant sites) and the Fig4E {T}-tag
+    counts, read from the test source."""
+    src = (ref_root / "tests" / "test_fel.cpp").read_text()
+    lines = src.splitlines()
+
+    def case(title):
+        start = next(i for i, ln in enumerate(lines) if "TEST_CASE" in ln and title in ln)
+        end = next((i for i in range(start + 1, len(lines)) if "TEST_CASE" in lines[i]), len(lines))
+        return start, "\n".join(lines[start:end])
+
+    s0, leaves = case("Leaves mode")
+    nwk = re.search(r'nwk_fitted\s*=\s*"([^"]+)"', leaves).group(1)
+    val = {k: float(v) for k, v in re.findall(r"base_p\.(\w+)\s*=\s*([-0-9.eE]+);", leaves)}
+    theta = [val[k] for k in ("theta_AC", "theta_AT", "theta_CG", "theta_CT", "theta_GT")]
+    n_t = int(re.search(r"num_tested\s*==\s*(\d+)", leaves).group(1))
+    n_b = int(re.search(r"num_background\s*==\s*(\d+)", leaves).group(1))
+    inv = sorted({int(i) for i in re.findall(r"results\[(\d+)\]\.p_value\s*==\s*1\.0", leaves)})
+    s1, tags = case("Fig4E")
+    t_t = int(re.search(r"num_tested\s*==\s*(\d+)", tags).group(1))
+    t_b = int(re.search(r"num_background\s*==\s*(\d+)", tags).group(1))
+    return {
+        "cd2_reduced_fel_leaves": {
+            "source": f"tests/test_fel.cpp:{s0 + 1} (cd2_reduced.fna, test_branches = Leaves)",
+            "newick": nwk, "test_branches": "Leaves",
+            "params": {"alpha": val["alpha"], "beta": val["beta"], "theta": theta},
+            "num_tested": n_t, "num_background": n_b, "invariant_sites": inv,
+        },
+        "fig4e_tags": {
+            "source": f"tests/test_fel.cpp:{s1 + 1} (Fig4E.nex embedded tree, test_branches = All, {{T}} tags)",
+            "num_tested": t_t, "num_background": t_b,
+        },
+    }
 
 
 def labelled_newick(topology: str, lengths: dict) -> str:

@@ -1,5 +1,5 @@
-// Host-logic harness for the site-fit drivers (h3g_sitefit.cpp, h3g_fel_driver.cpp,
-// h3g_meme_driver.cpp): the device evaluator is replaced by a CPU function of the
+// Host-logic harness for the site-fit drivers (h3g_sitefit.cpp, h3g_fel_driver.cpp with and
+// without a background branch set, h3g_meme_driver.cpp): the device evaluator is replaced by a CPU function of the
 // solved omegas, so the lockstep loop's batching, eigensystem-slot assignment and
 // consistency checks run without a GPU.  The fake likelihood is rugged (a bowl plus
 // an oscillation) so the simplex searches take many steps, park several requests at
@@ -31,8 +31,8 @@ bool fel_problem_view(h3g_problem* pr, FelProblemView* v) {
 void fel_set_error(h3g_problem* pr, const std::string& msg) { pr->err = msg; }
 void fel_record_transfer(h3g_problem*, size_t, size_t, int, double) {}
 struct FelDevice { int n_slots, max_req, n; std::vector<double> om; std::vector<int> solved; int batches = 0; };
-FelDevice* fel_device_create(h3g_problem* pr, int, const double*, const double*, const double*, const double*, int max_requests,
-                             int n_slots, std::string*) {
+FelDevice* fel_device_create(h3g_problem* pr, int, const double*, const double*, const double*, const double*, const uint8_t*,
+                             int max_requests, int n_slots, std::string*) {
     auto* d = new FelDevice{n_slots, max_requests, pr->n, std::vector<double>(n_slots, -1.0), std::vector<int>(n_slots, 0)};
     return d;
 }
@@ -44,13 +44,15 @@ static double fake_lnl(int p, double a, double o1, double o2, double w1) {
     return l;
 }
 bool fel_device_eval(FelDevice* d, int n_eig, const double* eom, const int* es, const int* ep, int n_req, const int* pat,
-                     const double* a, const int* s1, const int* s2, const double* w1, double* out, std::string* err) {
+                     const double* a, const int* s1, const int* s2, const double* w1, const int* sb, double* out,
+                     std::string* err) {
     ++d->batches;
-    if (n_eig > 2 * d->max_req || n_req > d->max_req) { *err = "too large"; return false; }
+    if (n_eig > 3 * d->max_req || n_req > d->max_req) { *err = "too large"; return false; }
     for (int e = 0; e < n_eig; ++e) { d->om[es[e]] = eom[e]; d->solved[es[e]] = 1; (void)ep; }
     for (int r = 0; r < n_req; ++r) {
         const double o1 = d->om[s1[r]], o2 = (s2 && s2[r] >= 0) ? d->om[s2[r]] : -1.0;
         out[r] = fake_lnl(pat[r], a[r], o1, o2, w1 ? w1[r] : 1.0);
+        if (sb && sb[r] >= 0) out[r] -= 0.3 * std::pow(std::log(d->om[sb[r]] + 1e-3) + 0.2 * (pat[r] % 4), 2);
     }
     return true;
 }
@@ -79,6 +81,11 @@ static int run(int P) {
     std::vector<h3g_fel_result> fel(P);
     h3g_status st = h3g_fel_run(&pr, &m, bl.data(), fel.data());
     if (st != H3G_OK) { printf("fel status %d %s\n", int(st), pr.err.c_str()); return 1; }
+    // the branch-subset search: leaves 1 and 2 tested, 3 and 4 background
+    const uint8_t tested[5] = {0, 1, 1, 0, 0};
+    std::vector<h3g_fel_result> sub(P);
+    st = h3g_fel_run_tested(&pr, &m, bl.data(), tested, sub.data());
+    if (st != H3G_OK) { printf("fel subset status %d %s\n", int(st), pr.err.c_str()); return 1; }
     std::vector<h3g_meme_result> out(P);
     std::vector<double> ebf(size_t(P) * pr.n);
     st = h3g_meme_run(&pr, &m, bl.data(), out.data(), ebf.data());
@@ -87,7 +94,8 @@ static int run(int P) {
     long evals = 0;
     for (int p = 0; p < P; ++p) {
         sum += fel[p].log_l_alt + fel[p].log_l_null + out[p].log_l_meme + out[p].alpha + out[p].beta_plus + out[p].p1;
-        evals += fel[p].evaluations + out[p].evaluations;
+        sum += sub[p].log_l_alt + sub[p].log_l_null + sub[p].beta_nuisance;
+        evals += fel[p].evaluations + out[p].evaluations + sub[p].evaluations;
     }
     printf("P %d checksum %.17g evaluations %ld\n", P, sum, evals);
     return 0;

@@ -1,4 +1,4 @@
-"""FEL per-site fits on the device against the oracle's restatement of the reference (fel.hpp:326-446).
+"""FEL per-site fits on the device against the oracle's restatement of the reference (fel.hpp:326-572).
 
 Both run the reference's search (grid, bounded Nelder-Mead, Brent) pattern by
 pattern; the device evaluates every likelihood in FP64 by spectral pruning
@@ -116,7 +116,67 @@ def test_fel_analyzer_api_matches_reference_test(oracle, golden_dir):
     np.testing.assert_allclose(lrt, np.asarray(ref["lrt"])[sp], rtol=0, atol=2e-4)
     np.testing.assert_allclose([r.total_branch_length for r in res], np.asarray(ref["total_branch_length"])[sp],
                                rtol=1e-3, atol=1e-6)
-    with pytest.raises(RuntimeError):
-        s = h3.FELSettings()
-        s.test_branches = "Internal"
-        h3.FELAnalyzer(t, a, p, s)
+
+
+def _leaves(t):
+    return [bool(x) for x in t.is_leaf]
+
+
+def test_fel_subset_cd2_matches_oracle(ctx, oracle, golden_dir):
+    """Leaves tested, internal branches background (fel.hpp:462-572) on CD2, device vs oracle."""
+    k = json.loads((golden_dir / "known_answers.json").read_text())["cd2_fel"]
+    a = oracle.Alignment.load(str(golden_dir / "cd2.fna"))
+    t = oracle.Tree.parse((golden_dir / "cd2_fitted.nwk").read_text())
+    tested = _leaves(t)
+    ref = oracle.fel_run_tested(t, a, k["params"], tested)
+    pi, qs, qn = _fel_inputs(oracle, a, k["params"])
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    dev = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=ref["branch_lengths"], tested=tested)
+    _compare(dev, ref)
+    var = np.asarray(ref["evals"]) > 0
+    assert np.all(dev["beta_nuisance"][~var] == 0.0)
+    assert np.all((dev["beta_nuisance"][var] >= 1e-4) & (dev["beta_nuisance"][var] <= 1000.0))
+    # the split is a different model from the all-branches one
+    full = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=ref["branch_lengths"])
+    assert np.abs(full["log_l_alt"] - dev["log_l_alt"]).max() > 1e-3
+
+
+def test_fel_tested_all_is_the_all_branches_run(ctx, oracle, golden_dir):
+    a = oracle.Alignment.load(str(golden_dir / "cd2_reduced.fna"))
+    t = oracle.Tree.parse((golden_dir / "cd2_reduced.nwk").read_text())
+    params = {"alpha": 1.0, "beta": 0.5, "theta": [1, 1, 1, 2, 1]}
+    pi, qs, qn = _fel_inputs(oracle, a, params)
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    bl = np.array(t.branch_lengths)
+    one = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl)
+    two = pr.fel_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=bl, tested=[True] * t.num_nodes())
+    for key in ("alpha", "beta", "log_l_alt", "log_l_null", "lrt", "evaluations"):
+        np.testing.assert_array_equal(one[key], two[key])
+
+
+def test_fel_analyzer_leaves_reference_case(oracle, golden_dir, known):
+    """The reference's "Leaves" case (tests/test_fel.cpp:78-126) through hyphy3.FELAnalyzer."""
+    import _hyphy3 as h3
+    k = known["cd2_reduced_fel_leaves"]
+    a = h3.Alignment.load(str(golden_dir / "cd2_reduced.fna"))
+    t = h3.Tree.from_newick(k["newick"])
+    p = h3.MG94Parameters()
+    p.alpha, p.beta = k["params"]["alpha"], k["params"]["beta"]
+    p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = k["params"]["theta"]
+    s = h3.FELSettings()
+    s.test_branches = k["test_branches"]
+    f = h3.FELAnalyzer(t, a, p, s)
+    assert (f.num_tested, f.num_background) == (k["num_tested"], k["num_background"])
+    assert len(f.test_branch_names) == f.num_tested and len(f.bg_branch_names) == f.num_background
+    res = f.run()
+    assert len(res) == a.num_codons
+    for i in k["invariant_sites"]:
+        assert res[i].alpha == 0.0 and res[i].beta == 0.0 and res[i].p_value == 1.0
+    oa = oracle.Alignment.load(str(golden_dir / "cd2_reduced.fna"))
+    ot = oracle.Tree.parse(k["newick"])
+    ref = oracle.fel_run_tested(ot, oa, k["params"], _leaves(ot))
+    sp = np.array(oa.site_pattern)
+    np.testing.assert_allclose([r.lrt for r in res], np.asarray(ref["lrt"])[sp], rtol=0, atol=2e-4)
+    np.testing.assert_allclose([r.log_l_alt for r in res], np.asarray(ref["log_l_alt"])[sp], rtol=0, atol=1e-4)
+    np.testing.assert_allclose([r.total_branch_length for r in res], np.asarray(ref["total_branch_length"])[sp],
+                               rtol=1e-3, atol=1e-6)
