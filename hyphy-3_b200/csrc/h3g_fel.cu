@@ -255,21 +255,28 @@ struct Spectral {
 };
 
 constexpr size_t spectral_doubles(int nc) { return size_t(nc) * (2 * SP * LD + 6 * SP); }
-constexpr size_t kEbfSmem = (spectral_doubles(2) + 3 * SP) * sizeof(double);
+// EBF pass: two class eigensystems, plus the background's when NT = 3
+constexpr size_t ebf_smem(int nt) { return (spectral_doubles(nt) + 3 * SP) * sizeof(double); }
+static_assert(ebf_smem(3) + kMaxDepth * sizeof(int) + 16 * sizeof(double) <= 227 * 1024, "EBF pass must fit one CTA");
 
-// carve shared memory and stage request r's eigensystems; returns the first free double
+// carve shared memory and stage request r's eigensystems (NC = 3: the third is the
+// background's, weight 1); returns the first free double
 template <int NC>
 __device__ double* spectral_setup(Spectral<NC>& sp, double* sm, const FelModel& f, const FelReqs& q, int r) {
     const int tid = threadIdx.x;
     double* z = sm;
     int sl[NC];
     sl[0] = q.slot[r];
-    if constexpr (NC == 2) {
+    if constexpr (NC >= 2) {
         sl[1] = q.slot2[r];
         sp.w[0] = q.w1[r];
         sp.w[1] = 1.0 - q.w1[r];
     } else {
         sp.w[0] = 1.0;
+    }
+    if constexpr (NC == 3) {
+        sl[2] = q.slot_bg[r];
+        sp.w[2] = 1.0;
     }
     const double a = q.a[r];
 #pragma unroll
@@ -303,13 +310,16 @@ __device__ __forceinline__ double max64(double v, double* r2) {
 
 // Depth-first pruning of pattern p (ev: 2 node + 1 opens an internal node,
 // 2 node closes a node and sends its message to the parent's partial).  Open
-// partials live on stk with power-of-two exponents in sexp.  STORE: the
-// component messages of every non-root node are written to msg[node][c][64]
-// (the outside pass of k_meme_ebf reads them).  On return stk[0..63] holds the
-// root partial and sexp[0] its exponent.
+// partials live on stk with power-of-two exponents in sexp.  NC = 2: every
+// branch mixes the two class eigensystems; NC = 3: a branch flagged in bgf uses
+// the third (background) one alone.  STORE: the two class messages of every
+// non-root node are written to msg[node][c][64], the background message in
+// both slots of a background branch (the outside pass of k_meme_ebf reads
+// them).  On return stk[0..63] holds the root partial and sexp[0] its exponent.
 template <int NC, bool STORE>
 __device__ void prune(const Spectral<NC>& sp, double* sL, const Topo& t, const double* __restrict__ bl,
-                      const int* __restrict__ ev, int n_ev, double* stk, int* sexp, double* red, int p, double* msg) {
+                      const uint8_t* __restrict__ bgf, const int* __restrict__ ev, int n_ev, double* stk, int* sexp,
+                      double* red, int p, double* msg) {
     const int tid = threadIdx.x, S = t.S, row = tid & 63, qd = tid >> 6;
     int sp_ = -1;
     for (int k = 0; k < n_ev; ++k) {
@@ -378,13 +388,18 @@ __device__ void prune(const Spectral<NC>& sp, double* sL, const Topo& t, const d
         if (tid < SP) {
             // the two warps that own the partial multiply, take its maximum between
             // themselves (named barrier 1, 64 threads) and rescale; the other warps go on
+            const bool bgn = NC == 3 && bgf[node] != 0;
+            double mc[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                mc[c] = (sp.part[c][tid] + sp.part[c][SP + tid]) + (sp.part[c][2 * SP + tid] + sp.part[c][3 * SP + tid]);
             double m = 0.0;
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const double mc = (sp.part[c][tid] + sp.part[c][SP + tid]) + (sp.part[c][2 * SP + tid] + sp.part[c][3 * SP + tid]);
-                m += sp.w[c] * mc;
-                if constexpr (STORE) msg[(size_t(node) * 3 + c) * SP + tid] = tid < S ? fmax(mc, 0.0) : 0.0;
+            for (int c = 0; c < (NC == 3 ? 2 : NC); ++c) {
+                m += sp.w[c] * mc[c];
+                if constexpr (STORE) msg[(size_t(node) * 3 + c) * SP + tid] = tid < S ? fmax(bgn ? mc[NC - 1] : mc[c], 0.0) : 0.0;
             }
+            if (bgn) m = mc[NC - 1];
             m = tid < S ? fmax(m, 0.0) : 0.0;
             double v = stk[sp_ * SP + tid] * m;
             double w = v;
@@ -608,6 +623,9 @@ __global__ void __launch_bounds__(kLvT) k_site_lnl(FelModel f, Topo t, const dou
 // vector (pi at the root, P_mix^T top below).  Every vector may carry any
 // positive factor common to both classes, so the outside pass normalises by
 // the maximum instead of tracking exponents.  ebf[r][b] for every non-root b.
+// NT = 3: background branches (f.bg) use the request's background
+// eigensystem alone and get ebf 1 (meme.hpp:497-552).
+template <int NT>
 __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const double* __restrict__ bl, const int* __restrict__ ev,
                                                   int n_ev, int depth, double* __restrict__ stack, FelReqs q,
                                                   double* __restrict__ msg_all, double* __restrict__ ebf_all) {
@@ -616,15 +634,15 @@ __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const doub
     __shared__ int sexp[kMaxDepth];
     __shared__ double red[kFT / 32], r2[2], r4[4];
     const int tid = threadIdx.x, S = t.S, r = blockIdx.x, n = t.n, row = tid & 63, qd = tid >> 6;
-    Spectral<2> sp;
-    double* sL = spectral_setup<2>(sp, sm, f, q, r);
+    Spectral<NT> sp;
+    double* sL = spectral_setup<NT>(sp, sm, f, q, r);
     double* ou = sL + SP;                                  // outside vector of the open node
     double* top = ou + SP;
     double* stk = stack + size_t(r) * depth * SP;
     double* msg = msg_all + size_t(r) * n * 3 * SP;        // [node][M_1 | M_+ | O or prefix][64]
     double* ebf = ebf_all + size_t(r) * n;
     __syncthreads();
-    prune<2, true>(sp, sL, t, bl, ev, n_ev, stk, sexp, red, q.pattern[r], msg);
+    prune<NT, true>(sp, sL, t, bl, f.bg, ev, n_ev, stk, sexp, red, q.pattern[r], msg);
     const double w0 = sp.w[0], w1 = sp.w[1];
     if (tid == 0) ebf[t.root] = 1.0;
     for (int k = 0; k < n_ev; ++k) {                       // internal nodes in pre-order
@@ -648,6 +666,7 @@ __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const doub
         for (int i = c1 - 1; i >= c0; --i) {               // suffix products, children in reverse
             const int c = t.ch[i];
             const size_t b = size_t(c) * 3 * SP;
+            const bool bgc = NT == 3 && f.bg[c] != 0;
             if (tid < SP) {
                 double tv = msg[b + 2 * SP + tid] * suf;
                 const double mx = max64(tv, r2);
@@ -665,7 +684,7 @@ __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const doub
                     double e = 0.0;
                     if (L1 > 0.0 && Lp > 0.0) e = exp(fmin(fmax(log(Lp) - log(L1), -50.0), 50.0));
                     else if (!(L1 > 0.0) && Lp > 0.0) e = 1e6;
-                    ebf[c] = e;
+                    ebf[c] = bgc ? 1.0 : e;
                 }
                 suf *= w0 * msg[b + tid] + w1 * msg[b + SP + tid];
                 const double ms = max64(suf, r2);
@@ -674,7 +693,7 @@ __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const doub
             __syncthreads();
             if (!t.leaf[c]) {                              // O_c = sum_k w_k V_k^T (e_k o (U_k^T top))
 #pragma unroll
-                for (int m = 0; m < 2; ++m) {
+                for (int m = 0; m < NT; ++m) {
                     double s = 0.0;
 #pragma unroll
                     for (int j = 0; j < 16; ++j) s = fma(sp.U[m][(16 * qd + j) * LD + row], top[16 * qd + j], s);
@@ -683,13 +702,13 @@ __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const doub
                 __syncthreads();
                 if (tid < SP) {
 #pragma unroll
-                    for (int m = 0; m < 2; ++m)
+                    for (int m = 0; m < NT; ++m)
                         sp.x[m][tid] = ((sp.part[m][tid] + sp.part[m][SP + tid]) + (sp.part[m][2 * SP + tid] + sp.part[m][3 * SP + tid])) *
                                        exp(sp.lam[m][tid] * bl[c]);
                 }
                 __syncthreads();
 #pragma unroll
-                for (int m = 0; m < 2; ++m) {
+                for (int m = 0; m < NT; ++m) {
                     double s = 0.0;
 #pragma unroll
                     for (int j = 0; j < 16; ++j) s = fma(sp.V[m][(16 * qd + j) * LD + row], sp.x[m][16 * qd + j], s);
@@ -701,6 +720,10 @@ __global__ void __launch_bounds__(kFT) k_meme_ebf(FelModel f, Topo t, const doub
 #pragma unroll
                     for (int m = 0; m < 2; ++m)
                         o += sp.w[m] * ((sp.part[m][tid] + sp.part[m][SP + tid]) + (sp.part[m][2 * SP + tid] + sp.part[m][3 * SP + tid]));
+                    if (bgc) {
+                        const int m = NT - 1;
+                        o = (sp.part[m][tid] + sp.part[m][SP + tid]) + (sp.part[m][2 * SP + tid] + sp.part[m][3 * SP + tid]);
+                    }
                     msg[b + 2 * SP + tid] = tid < S ? fmax(o, 0.0) : 0.0;
                 }
                 __syncthreads();
@@ -837,7 +860,8 @@ FelDevice* fel_device_alloc(h3g_problem* pr, const FelProblemView& v, int max_re
              cudaFuncSetAttribute(k_site_lnl<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(2, false))) == cudaSuccess &&
              cudaFuncSetAttribute(k_site_lnl<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(1, true))) == cudaSuccess &&
              cudaFuncSetAttribute(k_site_lnl<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lv_smem(2, true))) == cudaSuccess &&
-             cudaFuncSetAttribute(k_meme_ebf, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEbfSmem)) == cudaSuccess;
+             cudaFuncSetAttribute(k_meme_ebf<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ebf_smem(2))) == cudaSuccess &&
+             cudaFuncSetAttribute(k_meme_ebf<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ebf_smem(3))) == cudaSuccess;
         configured = ok;
     }
     int per[2][2] = {{0, 0}, {0, 0}};
@@ -1011,10 +1035,13 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int
 
 bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                     const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
-                    const double* req_w1, double* ebf_out, std::string* err) {
+                    const double* req_w1, const int* req_slot_bg, double* ebf_out, std::string* err) {
     if (n_req > kEbfChunk) { *err = "EBF batch larger than 256 requests"; return false; }
     for (int i = 0; i < n_req; ++i)
-        if (req_slot2[i] < 0) { *err = "EBF request needs two components"; return false; }
+        if (req_slot2[i] < 0 || (req_slot_bg && req_slot_bg[i] < 0)) {
+            *err = "EBF request needs two components (and the background's when one is given)";
+            return false;
+        }
     if (!d->d_msg) {
         void *m = nullptr, *e = nullptr;
         bool ok = cudaMalloc(&m, size_t(kEbfChunk) * d->n * 3 * SP * sizeof(double)) == cudaSuccess;
@@ -1030,15 +1057,16 @@ bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int*
     order.resize(n_req);
     for (int i = 0; i < n_req; ++i) order[i] = i;
     FelReqs q{};
-    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1, nullptr,
-                     order, &q, err))
+    if (!stage_batch(d, n_eig, eig_omega, eig_slot, eig_prev, n_req, req_pattern, req_a, req_slot, req_slot2, req_w1,
+                     req_slot_bg, order, &q, err))
         return false;
     cudaStream_t s = d->s;
     const size_t bytes = size_t(n_req) * d->n * sizeof(double);
     d->launches += n_req > 0;
     if (n_req > 0)
-        launch_k(k_meme_ebf, n_req, kFT, kEbfSmem, s, d->f, d->t, static_cast<const double*>(d->d_bl),
-                 static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack, q, d->d_msg, d->d_ebf);
+        launch_k(req_slot_bg ? k_meme_ebf<3> : k_meme_ebf<2>, n_req, kFT, ebf_smem(req_slot_bg ? 3 : 2), s, d->f, d->t,
+                 static_cast<const double*>(d->d_bl), static_cast<const int*>(d->d_ev), d->n_ev, d->depth, d->d_stack, q,
+                 d->d_msg, d->d_ebf);
     d->d2h += bytes;
     const bool ok = cudaGetLastError() == cudaSuccess &&
                     (n_req == 0 || cudaMemcpyAsync(d->h_ebf, d->d_ebf, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess) &&

@@ -43,11 +43,13 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eig_omega, const int
                      const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
                      const double* req_w1, const int* req_slot_bg, double* lnl_out, std::string* err);
 // MEME's empirical Bayes factors of every branch for two-component requests
-// (at most fel_device_max_ebf(d) per call): ebf_out[r * n_nodes + b]
+// (at most fel_device_max_ebf(d) per call): ebf_out[r * n_nodes + b].  With
+// req_slot_bg (every entry >= 0) the background branches use that eigensystem
+// and get factor 1.
 int fel_device_max_ebf(const FelDevice* d);
 bool fel_device_ebf(FelDevice* d, int n_eig, const double* eig_omega, const int* eig_slot, const int* eig_prev, int n_req,
                     const int* req_pattern, const double* req_a, const int* req_slot, const int* req_slot2,
-                    const double* req_w1, double* ebf_out, std::string* err);
+                    const double* req_w1, const int* req_slot_bg, double* ebf_out, std::string* err);
 void fel_device_transfer(const FelDevice* d, size_t* h2d, size_t* d2h, int* launches);   // bytes moved, kernels launched
 // ends a run: the evaluator stays with its problem (problem_fel_device) and a
 // later fel_device_create with the same problem and no larger sizes reuses its

@@ -389,5 +389,10 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readwrite("p_value_threshold", &MEMEAnalyzer::p_value_threshold)
         .def_readonly("conversion_factor", &MEMEAnalyzer::conversion_factor)
         .def_readonly("baseline_tree_length", &MEMEAnalyzer::baseline_tree_length)
+        .def("select_test_branches", &MEMEAnalyzer::select_test_branches, "spec"_a)
+        .def_readonly("test_branches", &MEMEAnalyzer::test_branches)
+        .def_readonly("is_test_branch", &MEMEAnalyzer::is_test_branch)
+        .def_readonly("num_tested", &MEMEAnalyzer::num_tested)
+        .def_readonly("num_background", &MEMEAnalyzer::num_background)
         .def_readonly("site_results", &MEMEAnalyzer::site_results);
 }

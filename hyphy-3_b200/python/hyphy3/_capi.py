@@ -26,7 +26,7 @@ EXPORTED = [
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
-    "h3g_fel_run_tested",
+    "h3g_fel_run_tested", "h3g_meme_run_tested",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -57,7 +57,7 @@ class MemeResult(C.Structure):
                 ("p_plus", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double),
                 ("branches_under_selection", C.c_int), ("total_branch_length", C.c_double),
                 ("log_l_meme", C.c_double), ("log_l_fel", C.c_double), ("p_value_meme_vs_fel", C.c_double),
-                ("fel_alpha", C.c_double), ("fel_beta", C.c_double), ("evaluations", C.c_int)]
+                ("fel_alpha", C.c_double), ("fel_beta", C.c_double), ("evaluations", C.c_int), ("beta_bg", C.c_double)]
 
 
 class Result(C.Structure):
@@ -100,6 +100,8 @@ def load() -> C.CDLL:
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
+        lib.h3g_meme_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
+                                            C.POINTER(MemeResult), _dp]
         for name in EXPORTED:
             getattr(lib, name).restype = getattr(lib, name).restype or C.c_int
         lib.h3g_version.restype = C.c_char_p
@@ -249,9 +251,10 @@ class Problem:
         names = [f[0] for f in FelResult._fields_]
         return {k: np.array([getattr(res[i], k) for i in range(self.P)]) for k in names}
 
-    def meme_run(self, *, pi, Qs, Qn, branch_lengths, with_ebf: bool = True) -> dict:
-        """MEME per-pattern fits (h3g_meme_run); branch lengths in FEL time.  Returns arrays per pattern
-        and, with with_ebf, "branch_ebf" [n_patterns, n_nodes]."""
+    def meme_run(self, *, pi, Qs, Qn, branch_lengths, with_ebf: bool = True, tested=None, fel_tested=None) -> dict:
+        """MEME per-pattern fits (h3g_meme_run, or h3g_meme_run_tested when tested[n_nodes] is given;
+        fel_tested, the FEL baseline's set, defaults to tested); branch lengths in FEL time.  Returns
+        arrays per pattern and, with with_ebf, "branch_ebf" [n_patterns, n_nodes]."""
         pi, Qs, Qn, bl = _f64(pi), _f64(Qs), _f64(Qn), _f64(branch_lengths)
         S = int(pi.size)
         if Qs.shape != (S, S) or Qn.shape != (S, S) or bl.size != self.n:
@@ -259,7 +262,20 @@ class Problem:
         m = FelModel(S=S, pi=_ptr(pi), Qs=_ptr(Qs), Qn=_ptr(Qn))
         res = (MemeResult * max(self.P, 1))()
         ebf = np.zeros((max(self.P, 1), self.n)) if with_ebf else None
-        self.ctx.check(self.ctx.lib.h3g_meme_run(self.h, C.byref(m), _ptr(bl), res, _ptr(ebf) if with_ebf else None))
+        if tested is None:
+            self.ctx.check(self.ctx.lib.h3g_meme_run(self.h, C.byref(m), _ptr(bl), res, _ptr(ebf) if with_ebf else None))
+        else:
+            def mask(x):
+                v = np.ascontiguousarray(np.asarray(x, dtype=bool), dtype=np.uint8)
+                if v.size != self.n:
+                    raise ValueError("tested / fel_tested need one entry per node")
+                return v
+            tv = mask(tested)
+            fv = mask(fel_tested) if fel_tested is not None else None
+            u8 = C.POINTER(C.c_uint8)
+            self.ctx.check(self.ctx.lib.h3g_meme_run_tested(
+                self.h, C.byref(m), _ptr(bl), tv.ctypes.data_as(u8), fv.ctypes.data_as(u8) if fv is not None else None,
+                res, _ptr(ebf) if with_ebf else None))
         names = [f[0] for f in MemeResult._fields_]
         out = {k: np.array([getattr(res[i], k) for i in range(self.P)]) for k in names}
         if with_ebf:

@@ -234,7 +234,8 @@ h3g_status h3g_fel_run_tested(h3g_problem* prob, const h3g_fel_model* model, con
 /* ---------------------------------------------------------------- MEME
  * Mixed-effects model of episodic selection per site on the device, replacing
  * MEMEAnalyzer::analyze_pattern / run (include/hyphy/analyses/meme.hpp:166-632,
- * :634-676) for the case where every branch is tested.  Per pattern: the FEL
+ * :634-676) with every branch tested (h3g_meme_run_tested below for a
+ * tested / background split).  Per pattern: the FEL
  * fit above as the starting point; the alternative model (alpha, omega1, p1,
  * beta+) by the bounded 4-D Nelder-Mead from the reference's start grid; when
  * beta+ > alpha and p+ > 1e-6, the null model (beta+ = alpha) by a 3-D
@@ -252,6 +253,7 @@ typedef struct {
     double p_value_meme_vs_fel;                   /* exp(-LRT(MEME vs FEL) / 2), 1 when MEME is not better */
     double fel_alpha, fel_beta;
     int evaluations;          /* likelihood evaluations of the MEME search (FEL excluded); 0 for an invariant pattern */
+    double beta_bg;           /* beta on the background branches (h3g_meme_run_tested with a background); else 0 */
 } h3g_meme_result;
 
 /* Fit every pattern of prob; branch_lengths as for h3g_fel_run; out[n_patterns].
@@ -259,6 +261,19 @@ typedef struct {
  * factors (1 for the root, for invariant patterns and where no EBF is computed). */
 h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths, h3g_meme_result* out,
                         double* branch_ebf);
+
+/* As h3g_meme_run with the tested branches given (meme.hpp:84-92, :219-632):
+ * tested[n_nodes] != 0 marks a branch of the MEME test (the root's entry is
+ * ignored); fel_tested[n_nodes] likewise for the FEL baseline of each pattern,
+ * NULL when it is the same set (the reference partitions FEL's branches with
+ * {T}-tag detection and MEME's without, so the two differ only for "All" on a
+ * tagged tree).  With a background, the background branches evolve under
+ * Q = alpha Qs + beta_bg Qn: the alternative model adds beta_bg (5-D
+ * Nelder-Mead from the start grid with beta_bg = FEL's beta_nuisance), the null
+ * model beta+ = alpha keeps it free (4-D), background branches get EBF 1, and
+ * the site's tree length weighs them by their own rate. */
+h3g_status h3g_meme_run_tested(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths,
+                               const uint8_t* tested, const uint8_t* fel_tested, h3g_meme_result* out, double* branch_ebf);
 
 #ifdef __cplusplus
 }

@@ -6,10 +6,12 @@
 // model, meme.hpp:150-164); run() fits every site pattern (the FEL baseline,
 // the 4-D alternative and 3-D null Nelder-Mead searches, LRT, empirical Bayes
 // factors; meme.hpp:166-632) and maps patterns back to sites
-// (meme.hpp:634-676).  Only the analysis where every branch is tested
-// ("All") is on the device; any other branch selection throws
-// std::runtime_error.  create_and_fit (nucleotide GTR fit first) and the
-// ancestral substitution summaries (MEMESiteResult::subs) are not provided.
+// (meme.hpp:634-676).  The tested branches follow the reference
+// (meme.hpp:84-92): MEME's own set by Tree::select_branches without tag
+// detection, its FEL baseline's with detection; with a background set the
+// search frees beta_bg (h3g_meme_run_tested).  create_and_fit (nucleotide GTR
+// fit first), bridge resolutions and the ancestral substitution summaries
+// (MEMESiteResult::subs) are not provided.
 #pragma once
 
 #include <stdexcept>
@@ -56,13 +58,23 @@ public:
     size_t num_tested = 0;
     size_t num_background = 0;
 
+    std::vector<bool> is_test_branch;
+
     MEMEAnalyzer(Tree t, Alignment a, MG94Parameters params = MG94Parameters{}, std::string branches_spec = "All")
         : tree(t), aln(std::move(a)), base_params(params), fel_analyzer(t, aln, params), test_branches(std::move(branches_spec)) {
-        if (test_branches != "All")
-            throw std::runtime_error("MEMEAnalyzer (device): only the all-branches-tested analysis is supported");
         prepare_branch_lengths();
-        num_tested = tree.num_nodes() - 1;
-        num_background = 0;
+        select_test_branches(test_branches);
+    }
+
+    // meme.hpp:84-92
+    void select_test_branches(const std::string& spec) {
+        test_branches = spec;
+        auto sel = tree.select_branches(spec, "", {}, false);
+        is_test_branch = std::move(sel.is_selected);
+        num_tested = sel.num_selected;
+        num_background = sel.num_unselected;
+        fel_analyzer.settings.test_branches = spec;
+        fel_analyzer.partition_branches();
     }
 
     // meme.hpp:150-164
@@ -106,7 +118,13 @@ public:
         h3g_fel_model m{S, pi.data(), qs.data(), qn.data()};
         std::vector<h3g_meme_result> res(aln.patterns.size());
         std::vector<double> ebf(aln.patterns.size() * n, 1.0);
-        eng.check(h3g_meme_run(pr, &m, bl.data(), res.data(), ebf.data()));
+        std::vector<uint8_t> tested(n, 1), fel_tested(n, 1);
+        for (const auto& node : tree.nodes) {
+            if (node.id == tree.root_id) continue;
+            tested[size_t(node.id)] = is_test_branch[size_t(node.id)] ? 1 : 0;
+            fel_tested[size_t(node.id)] = fel_analyzer.is_test_branch[size_t(node.id)] ? 1 : 0;
+        }
+        eng.check(h3g_meme_run_tested(pr, &m, bl.data(), tested.data(), fel_tested.data(), res.data(), ebf.data()));
         site_results.assign(aln.num_codons, MEMESiteResult{});
         for (size_t s = 0; s < aln.num_codons; ++s) {
             const size_t p = aln.site_to_pattern[s];
@@ -117,7 +135,7 @@ public:
             o.lrt = r.lrt; o.p_value = r.p_value; o.branches_under_selection = r.branches_under_selection;
             o.total_branch_length = r.total_branch_length;
             o.log_l_meme = r.log_l_meme; o.log_l_fel = r.log_l_fel; o.p_value_meme_vs_fel = r.p_value_meme_vs_fel;
-            o.fel_alpha = r.fel_alpha; o.fel_beta = r.fel_beta;
+            o.fel_alpha = r.fel_alpha; o.fel_beta = r.fel_beta; o.beta_bg = r.beta_bg;
             o.branch_ebf.assign(ebf.begin() + std::ptrdiff_t(p * n), ebf.begin() + std::ptrdiff_t((p + 1) * n));
             o.evaluations = r.evaluations;
         }

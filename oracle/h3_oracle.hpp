@@ -1394,7 +1394,7 @@ inline FelSubsetRun fel_run_tested(const Tree& tr, const Alignment& a, const Par
 }
 
 struct MemeSite {
-    double alpha = 0, beta1 = 0, p1 = 1, beta_plus = 0, p_plus = 0, lrt = 0, p_value = 1;
+    double alpha = 0, beta1 = 0, p1 = 1, beta_plus = 0, p_plus = 0, lrt = 0, p_value = 1, beta_bg = 0;
     int bus = 0;                      // branches with EBF >= 100
     double total_bl = 0, lnl_meme = 0, lnl_fel = 0, p_vs_fel = 1, fel_alpha = 0, fel_beta = 0;
     int evals = 0;
@@ -1412,12 +1412,12 @@ struct MemeRun {
 // sentinel, 0 when lnL_+ is.
 inline void meme_branch_ebf(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, int p, const std::vector<Mat>& P1,
                             const std::vector<Mat>& Pp, std::vector<Mat>& Pm, const std::vector<double>& pi,
-                            std::vector<double>& ebf) {
+                            std::vector<double>& ebf, const std::vector<char>* tested = nullptr) {
     const int S = a.code.S, n = tr.n();
     Pass w;
     ebf.assign(n, 1.0);
     for (int b = 0; b < n; ++b) {
-        if (b == tr.root) continue;
+        if (b == tr.root || (tested && !(*tested)[b])) continue;       // background branches keep 1
         const Mat keep = Pm[b];
         Pm[b] = P1[b];
         inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
@@ -1434,35 +1434,72 @@ inline void meme_branch_ebf(const Tree& tr, const Alignment& a, const std::vecto
     }
 }
 
-// The branch EBFs of pattern p at given (alpha, omega1, p1, beta+) and FEL-time branch lengths.
+// The branch EBFs of pattern p at given (alpha, omega1, p1, beta+) and FEL-time branch lengths;
+// with tested (per node, non-empty) the other branches use omega beta_bg / alpha and keep EBF 1.
 inline std::vector<double> meme_ebf_at(const Tree& tr, const Alignment& a, const Params& base, const std::vector<double>& bl,
-                                       int p, double alpha, double omega1, double p1, double beta_plus) {
+                                       int p, double alpha, double omega1, double p1, double beta_plus,
+                                       const std::vector<char>& tested = {}, double beta_bg = 0.0) {
     const int S = a.code.S, n = tr.n();
+    const double ap = std::max(alpha, 1e-12);
     Params q1 = base; q1.alpha = 1.0; q1.beta = omega1;
-    Params qp = base; qp.alpha = 1.0; qp.beta = beta_plus / std::max(alpha, 1e-12);
-    MG94 m1, mp;
+    Params qp = base; qp.alpha = 1.0; qp.beta = beta_plus / ap;
+    Params qb = base; qb.alpha = 1.0; qb.beta = beta_bg / ap;
+    MG94 m1, mp, mb;
     m1.update(q1, a.pos_freq, a.pi, a.code);
     mp.update(qp, a.pos_freq, a.pi, a.code);
+    if (!tested.empty()) mb.update(qb, a.pos_freq, a.pi, a.code);
     std::vector<Mat> P1(n, Mat::eye(S)), Pp(n, Mat::eye(S)), Pm(n, Mat::eye(S));
-    const double ap = std::max(alpha, 1e-12);
     for (int i = 0; i < n; ++i) {
         if (i == tr.root) continue;
         P1[i] = m1.P(ap * bl[i]);
         Pp[i] = mp.P(ap * bl[i]);
+        if (!tested.empty() && !tested[i]) { Pm[i] = mb.P(ap * bl[i]); continue; }
         for (size_t e = 0; e < Pm[i].a.size(); ++e) Pm[i].a[e] = p1 * P1[i].a[e] + (1.0 - p1) * Pp[i].a[e];
     }
     std::vector<double> ebf;
-    meme_branch_ebf(tr, a, leaf_map(tr, a), p, P1, Pp, Pm, a.pi, ebf);
+    meme_branch_ebf(tr, a, leaf_map(tr, a), p, P1, Pp, Pm, a.pi, ebf, tested.empty() ? nullptr : &tested);
     return ebf;
 }
 
-// meme.hpp:166-632 with num_background == 0
-inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
-                             const MemeRun& run, int p) {
+// One MEME log-likelihood of pattern p (meme.hpp:219-272): tested branches mix omega1 and
+// beta+ / alpha with (p1, 1 - p1); with tested non-empty the others use beta_bg / alpha alone.
+inline double meme_lnl_at(const Tree& tr, const Alignment& a, const Params& base, const std::vector<double>& bl, int p,
+                          double alpha, double omega1, double p1, double beta_plus, const std::vector<char>& tested,
+                          double beta_bg) {
+    const int S = a.code.S, n = tr.n();
+    Params q1 = base; q1.alpha = alpha; q1.beta = alpha * omega1;
+    Params qp = base; qp.alpha = alpha; qp.beta = beta_plus;
+    Params qb = base; qb.alpha = alpha; qb.beta = beta_bg;
+    MG94 m1, mp, mb;
+    m1.update(q1, a.pos_freq, a.pi, a.code);
+    mp.update(qp, a.pos_freq, a.pi, a.code);
+    if (!tested.empty()) mb.update(qb, a.pos_freq, a.pi, a.code);
+    std::vector<Mat> Pm(n, Mat::eye(S));
+    for (int i = 0; i < n; ++i) {
+        if (i == tr.root) continue;
+        if (!tested.empty() && !tested[i]) { Pm[i] = mb.P(bl[i]); continue; }
+        const Mat A = m1.P(bl[i]), B = mp.P(bl[i]);
+        for (size_t e = 0; e < Pm[i].a.size(); ++e) Pm[i].a[e] = p1 * A.a[e] + (1.0 - p1) * B.a[e];
+    }
+    Pass w;
+    inside_outside(tr, a, p, leaf_map(tr, a), Pm, m1.pi, S, w, false);
+    return w.logL;
+}
+
+// The FEL fit a MEME search starts from (FelSite or FelSubsetSite).
+struct MemeFelStart { double alpha = 0, beta = 0, beta_nuisance = 0, alpha_null = 0, lnl_alt = 0; };
+
+// meme.hpp:166-632.  tested: per node, empty when every branch is tested; with a background the
+// background branches evolve under omega beta_bg / alpha alone, beta_bg free in both models
+// (5-D alternative from the grid with beta_bg = FEL's beta_nuisance, 4-D null), EBF 1 on them.
+inline MemeSite meme_pattern_tested(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
+                                    const std::vector<double>& bl, const std::vector<char>& tested, const MemeFelStart& fel,
+                                    double mu_s, double mu_n, int p) {
     MemeSite res;
     const int S = a.code.S, n = tr.n();
+    bool has_bg = false;
+    for (int i = 0; i < n; ++i) if (i != tr.root && !tested.empty() && !tested[i]) has_bg = true;
     res.ebf.assign(n, 1.0);
-    const FelSite& fel = run.fel.patterns[p];
     res.fel_alpha = fel.alpha; res.fel_beta = fel.beta; res.lnl_fel = fel.lnl_alt;
     int first = -1; bool invariant = true;
     for (int t = 0; t < a.T; ++t) {
@@ -1471,8 +1508,8 @@ inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vect
     }
     if (invariant) { res.lnl_fel = 0.0; return res; }
     // eigensystems of Q(omega) = Qs + omega Qn, reused when omega repeats exactly
-    // (least recently used at the front; a hit moves to the back, so the model
-    // returned by the previous call is never the one evicted)
+    // (least recently used at the front; a hit moves to the back, so the models
+    // returned by the current call are never the ones evicted)
     std::list<std::pair<double, MG94>> cache;
     auto model = [&](double om) -> const MG94& {
         for (auto it = cache.begin(); it != cache.end(); ++it)
@@ -1485,28 +1522,32 @@ inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vect
     };
     std::vector<Mat> P1(n, Mat::eye(S)), Pp(n, Mat::eye(S)), Pm(n, Mat::eye(S));
     Pass w;
-    auto build = [&](double al, double w1, double p1, double bp) {
+    auto build = [&](double al, double w1, double p1, double bp, double bbg) {
         const double ap = std::max(al, 1e-12);
         const MG94& m1 = model(w1);
         const MG94& mp = model(bp / ap);
+        const MG94& mb = has_bg ? model(bbg / ap) : m1;
         for (int i = 0; i < n; ++i) {
             if (i == tr.root) continue;
-            P1[i] = m1.P(ap * run.fel.bl[i]);
-            Pp[i] = mp.P(ap * run.fel.bl[i]);
+            P1[i] = m1.P(ap * bl[i]);
+            Pp[i] = mp.P(ap * bl[i]);
+            if (has_bg && !tested[i]) { Pm[i] = mb.P(ap * bl[i]); continue; }
             for (size_t e = 0; e < Pm[i].a.size(); ++e) Pm[i].a[e] = p1 * P1[i].a[e] + (1.0 - p1) * Pp[i].a[e];
         }
     };
     const std::vector<double>& pi = a.pi;
-    auto lnl = [&](double al, double w1, double p1, double bp) {
+    auto lnl = [&](double al, double w1, double p1, double bp, double bbg) {
         ++res.evals;
-        build(al, w1, p1, bp);
+        build(al, w1, p1, bp, bbg);
         inside_outside(tr, a, p, l2t, Pm, pi, S, w, false);
         return w.logL;
     };
+    using A5 = std::array<double, 5>;
     using A4 = std::array<double, 4>;
     using A3 = std::array<double, 3>;
     // start grid (meme.hpp:282-312)
     const double af = std::clamp(fel.alpha, 1e-4, 10000.0), bf = std::clamp(fel.beta, 1e-4, 100000.0);
+    const double bg0 = (has_bg && fel.beta_nuisance > 0.0) ? std::clamp(fel.beta_nuisance, 1e-4, 100000.0) : bf;
     const double w10 = std::clamp(bf / std::max(af, 1e-4), 0.0, 1.0);
     std::vector<A4> grid;
     if (af >= bf) {
@@ -1522,36 +1563,70 @@ inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vect
                 {af, 0.10, 0.90, bf * 15.0}, {af, 0.00, 0.95, bf * 30.0}, {af, 1.00, 0.01, std::max(bf, af * 1.5)}};
     }
     const A4 lb4 = {1e-4, 0.0, 1e-6, 1e-4}, ub4 = {10000.0, 1.0, 1.0 - 1e-6, 100000.0};
-    auto obj4 = [&](const A4& x) { return -lnl(x[0], x[1], x[2], x[3]); };
-    // alternative model (meme.hpp:340-354)
-    const auto alt = nelder_mead_nd<4>(obj4, grid[0], lb4, ub4, 1e-5, 800, grid);
-    double omega1 = alt.x[1];
-    res.alpha = alt.x[0]; res.p1 = alt.x[2]; res.beta_plus = alt.x[3];
-    res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1; res.lnl_meme = -alt.f;
+    const A5 lb5 = {1e-4, 0.0, 1e-6, 1e-4, 1e-4}, ub5 = {10000.0, 1.0, 1.0 - 1e-6, 100000.0, 100000.0};
+    auto obj4 = [&](const A4& x) { return -lnl(x[0], x[1], x[2], x[3], 0.0); };
+    auto obj5 = [&](const A5& x) { return -lnl(x[0], x[1], x[2], x[3], x[4]); };
+    double omega1 = w10;
+    if (has_bg) {
+        // meme.hpp:318-337
+        std::vector<A5> grid5;
+        for (const auto& g : grid) grid5.push_back({g[0], g[1], g[2], g[3], bg0});
+        const auto alt = nelder_mead_nd<5>(obj5, grid5[0], lb5, ub5, 1e-5, 800, grid5);
+        res.alpha = alt.x[0]; omega1 = alt.x[1]; res.p1 = alt.x[2]; res.beta_plus = alt.x[3]; res.beta_bg = alt.x[4];
+        res.lnl_meme = -alt.f;
+    } else {
+        // meme.hpp:338-354
+        const auto alt = nelder_mead_nd<4>(obj4, grid[0], lb4, ub4, 1e-5, 800, grid);
+        res.alpha = alt.x[0]; omega1 = alt.x[1]; res.p1 = alt.x[2]; res.beta_plus = alt.x[3]; res.beta_bg = 0.0;
+        res.lnl_meme = -alt.f;
+    }
+    res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1;
     if (res.beta_plus > res.alpha && res.p_plus > 1e-6) {
-        // null model beta+ = alpha (meme.hpp:404-452)
+        double lnl_null = -1e20, a_null = res.alpha, w_null = omega1, p_null = res.p1, bg_null = res.beta_bg;
         const double an = std::clamp(fel.alpha_null, 1e-4, 50.0);
-        std::vector<A3> ng = {{res.alpha, omega1, res.p1}, {an, 1.0, 0.5}, {an, omega1, res.p1},
-                              {std::clamp(res.alpha, 1e-4, 50.0), 1.0, 0.5}};
-        for (double c : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0, 20.0}) { ng.push_back({c, 0.5, 0.5}); ng.push_back({c, 0.0, 0.9}); }
-        const A3 lb3 = {1e-4, 0.0, 1e-6}, ub3 = {10000.0, 1.0, 1.0 - 1e-6};
-        const auto nul = nelder_mead_nd<3>([&](const A3& x) { return -lnl(x[0], x[1], x[2], x[0]); }, ng[0], lb3, ub3,
-                                           1e-5, 800, ng);
-        const double lnl_null = -nul.f, a_null = nul.x[0], w_null = nul.x[1], p_null = nul.x[2];
-        if (lnl_null > res.lnl_meme && std::isfinite(lnl_null)) {
-            // warm-started alternative (meme.hpp:436-452)
-            const std::vector<A4> wg = {{a_null, w_null, p_null, a_null}, {a_null, w_null, 0.99, a_null}};
-            const auto alt2 = nelder_mead_nd<4>(obj4, wg[0], lb4, ub4, 1e-5, 800, wg);
-            if (-alt2.f > res.lnl_meme) {
-                res.alpha = alt2.x[0]; omega1 = alt2.x[1]; res.p1 = alt2.x[2]; res.beta_plus = alt2.x[3];
-                res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1; res.lnl_meme = -alt2.f;
+        if (has_bg) {
+            // null model beta+ = alpha, beta_bg free (meme.hpp:364-405)
+            std::vector<A4> ng = {{res.alpha, omega1, res.p1, res.beta_bg}, {an, 1.0, 0.5, bg0}, {an, omega1, res.p1, bg0},
+                                  {std::clamp(res.alpha, 1e-4, 50.0), 1.0, 0.5, res.beta_bg}};
+            for (double c : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0, 20.0}) {
+                ng.push_back({c, 0.5, 0.5, res.beta_bg}); ng.push_back({c, 0.0, 0.9, res.beta_bg});
+            }
+            const auto nul = nelder_mead_nd<4>([&](const A4& x) { return -lnl(x[0], x[1], x[2], x[0], x[3]); }, ng[0], lb4, ub4,
+                                               1e-5, 800, ng);
+            lnl_null = -nul.f; a_null = nul.x[0]; w_null = nul.x[1]; p_null = nul.x[2]; bg_null = nul.x[3];
+            if (lnl_null > res.lnl_meme && std::isfinite(lnl_null)) {
+                const std::vector<A5> wg = {{a_null, w_null, p_null, a_null, bg_null}, {a_null, w_null, 0.99, a_null, bg_null}};
+                const auto alt2 = nelder_mead_nd<5>(obj5, wg[0], lb5, ub5, 1e-5, 800, wg);
+                if (-alt2.f > res.lnl_meme) {
+                    res.alpha = alt2.x[0]; omega1 = alt2.x[1]; res.p1 = alt2.x[2]; res.beta_plus = alt2.x[3];
+                    res.beta_bg = alt2.x[4];
+                    res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1; res.lnl_meme = -alt2.f;
+                }
+            }
+        } else {
+            // null model beta+ = alpha (meme.hpp:406-452)
+            std::vector<A3> ng = {{res.alpha, omega1, res.p1}, {an, 1.0, 0.5}, {an, omega1, res.p1},
+                                  {std::clamp(res.alpha, 1e-4, 50.0), 1.0, 0.5}};
+            for (double c : {0.01, 0.1, 0.5, 1.0, 2.0, 5.0, 10.0, 20.0}) { ng.push_back({c, 0.5, 0.5}); ng.push_back({c, 0.0, 0.9}); }
+            const A3 lb3 = {1e-4, 0.0, 1e-6}, ub3 = {10000.0, 1.0, 1.0 - 1e-6};
+            const auto nul = nelder_mead_nd<3>([&](const A3& x) { return -lnl(x[0], x[1], x[2], x[0], 0.0); }, ng[0], lb3, ub3,
+                                               1e-5, 800, ng);
+            lnl_null = -nul.f; a_null = nul.x[0]; w_null = nul.x[1]; p_null = nul.x[2];
+            if (lnl_null > res.lnl_meme && std::isfinite(lnl_null)) {
+                // warm-started alternative (meme.hpp:436-452)
+                const std::vector<A4> wg = {{a_null, w_null, p_null, a_null}, {a_null, w_null, 0.99, a_null}};
+                const auto alt2 = nelder_mead_nd<4>(obj4, wg[0], lb4, ub4, 1e-5, 800, wg);
+                if (-alt2.f > res.lnl_meme) {
+                    res.alpha = alt2.x[0]; omega1 = alt2.x[1]; res.p1 = alt2.x[2]; res.beta_plus = alt2.x[3];
+                    res.beta1 = res.alpha * omega1; res.p_plus = 1.0 - res.p1; res.lnl_meme = -alt2.f;
+                }
             }
         }
         // meme.hpp:456-482
         if (lnl_null <= -1e10 || res.lnl_meme <= -1e10 || !std::isfinite(lnl_null) || !std::isfinite(res.lnl_meme)) {
             res.lrt = 0.0; res.p_value = 1.0;
         } else if (lnl_null > res.lnl_meme) {
-            res.alpha = a_null; res.beta1 = a_null * w_null; res.p1 = p_null; res.beta_plus = a_null;
+            res.alpha = a_null; res.beta1 = a_null * w_null; res.p1 = p_null; res.beta_plus = a_null; res.beta_bg = bg_null;
             res.p_plus = 1.0 - p_null; res.lnl_meme = lnl_null; omega1 = w_null;
             res.lrt = 0.0; res.p_value = 2.0 / 3.0;
         } else if (std::fabs(res.lnl_meme - lnl_null) <= 1e-12) {
@@ -1560,23 +1635,33 @@ inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vect
             res.lrt = 2.0 * (res.lnl_meme - lnl_null);
             res.p_value = (2.0 / 3.0) * (0.45 * std::erfc(std::sqrt(res.lrt / 2.0)) + 0.55 * std::exp(-res.lrt / 2.0));
         }
-        // empirical Bayes factors: every branch alone in class + vs class 1 (meme.hpp:484-588)
-        build(res.alpha, omega1, res.p1, res.beta_plus);
-        meme_branch_ebf(tr, a, l2t, p, P1, Pp, Pm, pi, res.ebf);
+        // empirical Bayes factors of the tested branches (meme.hpp:484-588); the background model
+        // takes beta_bg, or beta1 when that is not positive
+        build(res.alpha, omega1, res.p1, res.beta_plus, res.beta_bg > 0.0 ? res.beta_bg : res.beta1);
+        meme_branch_ebf(tr, a, l2t, p, P1, Pp, Pm, pi, res.ebf, has_bg ? &tested : nullptr);
         for (int b = 0; b < n; ++b)
             if (b != tr.root && res.ebf[b] >= 100.0) ++res.bus;
     } else {
         res.lrt = 0.0; res.p_value = 2.0 / 3.0;
     }
-    // meme.hpp:590-619
+    // meme.hpp:607-634
     const double d_fel = 2.0 * (res.lnl_meme - res.lnl_fel);
     res.p_vs_fel = d_fel > 0.0 ? std::exp(-d_fel / 2.0) : 1.0;
-    const double rate = (res.p1 * (res.alpha * run.mu_s + res.beta1 * run.mu_n) +
-                         res.p_plus * (res.alpha * run.mu_s + res.beta_plus * run.mu_n)) / 3.0;
+    const double test_rate = (res.p1 * (res.alpha * mu_s + res.beta1 * mu_n) + res.p_plus * (res.alpha * mu_s + res.beta_plus * mu_n)) / 3.0;
+    const double bg_rate = has_bg ? (res.alpha * mu_s + (res.beta_bg > 0.0 ? res.beta_bg : res.beta1) * mu_n) / 3.0 : test_rate;
     double tbl = 0.0;
-    for (int b = 0; b < n; ++b) if (b != tr.root) tbl += run.fel.bl[b] * rate;
+    for (int b = 0; b < n; ++b)
+        if (b != tr.root) tbl += bl[b] * ((has_bg && !tested[b]) ? bg_rate : test_rate);
     res.total_bl = tbl;
     return res;
+}
+
+// meme.hpp:166-632 with num_background == 0
+inline MemeSite meme_pattern(const Tree& tr, const Alignment& a, const std::vector<int>& l2t, const Params& base,
+                             const MemeRun& run, int p) {
+    const FelSite& f = run.fel.patterns[p];
+    const MemeFelStart fs{f.alpha, f.beta, 0.0, f.alpha_null, f.lnl_alt};
+    return meme_pattern_tested(tr, a, l2t, base, run.fel.bl, {}, fs, run.mu_s, run.mu_n, p);
 }
 
 // meme.hpp:150-164, :620-660 (run): FEL baseline then MEME for every pattern, in parallel
@@ -1594,6 +1679,47 @@ inline MemeRun meme_run(const Tree& tr, const Alignment& a, const Params& base, 
     run.patterns.assign(P, MemeSite{});
     #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(P))
     for (int p = 0; p < P; ++p) run.patterns[p] = meme_pattern(tr, a, l2t, base, run, p);
+    return run;
+}
+
+// meme.hpp:84-92, :150-164, :620-660 with branch sets: tested (MEME) and fel_tested (its FEL baseline,
+// partitioned with {T}-tag detection in the reference); every length converted by the base model's rate
+struct MemeTestedRun {
+    std::vector<double> bl;
+    std::vector<MemeFelStart> fel;
+    double mu_s = 0, mu_n = 0;
+    std::vector<MemeSite> patterns;
+};
+inline MemeTestedRun meme_run_tested(const Tree& tr, const Alignment& a, const Params& base, const std::vector<char>& tested,
+                                     const std::vector<char>& fel_tested, int max_patterns = -1) {
+    MemeTestedRun run;
+    const FelRun fr = fel_prepare(tr, a, base);
+    run.bl = fr.bl;
+    bool fel_bg = false;
+    for (int i = 0; i < tr.n(); ++i) if (i != tr.root && !fel_tested[i]) fel_bg = true;
+    FelSubsetRun sr;
+    sr.bl = fr.bl; sr.tested = fel_tested; sr.conversion = sr.bg_conversion = fr.conversion;
+    Params ps = base; ps.alpha = 1.0; ps.beta = 0.0;
+    Params pn = base; pn.alpha = 0.0; pn.beta = 1.0;
+    MG94 ms, mn;
+    ms.update(ps, a.pos_freq, a.pi, a.code);
+    mn.update(pn, a.pos_freq, a.pi, a.code);
+    run.mu_s = ms.mu; run.mu_n = mn.mu;
+    const auto l2t = leaf_map(tr, a);
+    const int P = max_patterns < 0 ? a.P : std::min(a.P, max_patterns);
+    run.fel.assign(P, MemeFelStart{});
+    run.patterns.assign(P, MemeSite{});
+    #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(P))
+    for (int p = 0; p < P; ++p) {
+        if (fel_bg) {
+            const FelSubsetSite f = fel_pattern_subset(tr, a, l2t, base, sr, p);
+            run.fel[p] = MemeFelStart{f.alpha, f.beta, f.beta_nuisance, f.alpha_null, f.lnl_alt};
+        } else {
+            const FelSite f = fel_pattern(tr, a, l2t, base, fr, p);
+            run.fel[p] = MemeFelStart{f.alpha, f.beta, 0.0, f.alpha_null, f.lnl_alt};
+        }
+        run.patterns[p] = meme_pattern_tested(tr, a, l2t, base, run.bl, tested, run.fel[p], run.mu_s, run.mu_n, p);
+    }
     return run;
 }
 

@@ -239,6 +239,7 @@ PYBIND11_MODULE(h3oracle, m) {
         d["p_value_meme_vs_fel"] = col([](const MemeSite& s) { return s.p_vs_fel; });
         d["fel_alpha"] = col([](const MemeSite& s) { return s.fel_alpha; });
         d["fel_beta"] = col([](const MemeSite& s) { return s.fel_beta; });
+        d["beta_bg"] = col([](const MemeSite& s) { return s.beta_bg; });
         d["evals"] = col([](const MemeSite& s) { return double(s.evals); });
         const size_t n = size_t(t.n());
         py::array_t<double> ebf({P, n});
@@ -252,10 +253,60 @@ PYBIND11_MODULE(h3oracle, m) {
         return d;
     }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("max_patterns") = -1);
     m.def("meme_ebf_at", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<double>& bl, int pattern,
-                            double alpha, double omega1, double p1, double beta_plus) {
-        return meme_ebf_at(t, a, params_from(p), bl, pattern, alpha, omega1, p1, beta_plus);
+                            double alpha, double omega1, double p1, double beta_plus, const std::vector<bool>& tested,
+                            double beta_bg) {
+        const std::vector<char> tv(tested.begin(), tested.end());
+        return meme_ebf_at(t, a, params_from(p), bl, pattern, alpha, omega1, p1, beta_plus, tv, beta_bg);
     }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths"), py::arg("pattern"), py::arg("alpha"),
-       py::arg("omega1"), py::arg("p1"), py::arg("beta_plus"));
+       py::arg("omega1"), py::arg("p1"), py::arg("beta_plus"), py::arg("tested") = std::vector<bool>{},
+       py::arg("beta_bg") = 0.0);
+    m.def("meme_lnl_at", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<double>& bl, int pattern,
+                            double alpha, double omega1, double p1, double beta_plus, const std::vector<bool>& tested,
+                            double beta_bg) {
+        const std::vector<char> tv(tested.begin(), tested.end());
+        return meme_lnl_at(t, a, params_from(p), bl, pattern, alpha, omega1, p1, beta_plus, tv, beta_bg);
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("branch_lengths"), py::arg("pattern"), py::arg("alpha"),
+       py::arg("omega1"), py::arg("p1"), py::arg("beta_plus"), py::arg("tested") = std::vector<bool>{},
+       py::arg("beta_bg") = 0.0);
+    m.def("meme_run_tested", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<bool>& tested,
+                                const std::vector<bool>& fel_tested, int max_patterns) {
+        const Params pp = params_from(p);
+        if (int(tested.size()) != t.n() || (!fel_tested.empty() && int(fel_tested.size()) != t.n()))
+            throw std::runtime_error("tested / fel_tested need one entry per node");
+        const std::vector<char> tv(tested.begin(), tested.end());
+        const std::vector<char> fv = fel_tested.empty() ? tv : std::vector<char>(fel_tested.begin(), fel_tested.end());
+        MemeTestedRun r;
+        { py::gil_scoped_release rel; r = meme_run_tested(t, a, pp, tv, fv, max_patterns); }
+        const size_t P = r.patterns.size();
+        py::dict d;
+        auto col = [&](auto get) { py::array_t<double> x(P); for (size_t i = 0; i < P; ++i) x.mutable_data()[i] = get(r.patterns[i]); return x; };
+        d["alpha"] = col([](const MemeSite& s) { return s.alpha; });
+        d["beta1"] = col([](const MemeSite& s) { return s.beta1; });
+        d["p1"] = col([](const MemeSite& s) { return s.p1; });
+        d["beta_plus"] = col([](const MemeSite& s) { return s.beta_plus; });
+        d["p_plus"] = col([](const MemeSite& s) { return s.p_plus; });
+        d["beta_bg"] = col([](const MemeSite& s) { return s.beta_bg; });
+        d["lrt"] = col([](const MemeSite& s) { return s.lrt; });
+        d["p_value"] = col([](const MemeSite& s) { return s.p_value; });
+        d["branches_under_selection"] = col([](const MemeSite& s) { return double(s.bus); });
+        d["total_branch_length"] = col([](const MemeSite& s) { return s.total_bl; });
+        d["log_l_meme"] = col([](const MemeSite& s) { return s.lnl_meme; });
+        d["log_l_fel"] = col([](const MemeSite& s) { return s.lnl_fel; });
+        d["p_value_meme_vs_fel"] = col([](const MemeSite& s) { return s.p_vs_fel; });
+        d["fel_alpha"] = col([](const MemeSite& s) { return s.fel_alpha; });
+        d["fel_beta"] = col([](const MemeSite& s) { return s.fel_beta; });
+        d["evals"] = col([](const MemeSite& s) { return double(s.evals); });
+        const size_t n = size_t(t.n());
+        py::array_t<double> ebf({P, n});
+        for (size_t i = 0; i < P; ++i)
+            for (size_t b = 0; b < n; ++b) ebf.mutable_data()[i * n + b] = r.patterns[i].ebf[b];
+        d["branch_ebf"] = ebf;
+        d["branch_lengths"] = r.bl;
+        d["mu_s"] = r.mu_s;
+        d["mu_n"] = r.mu_n;
+        return d;
+    }, py::arg("tree"), py::arg("aln"), py::arg("params"), py::arg("tested"), py::arg("fel_tested") = std::vector<bool>{},
+       py::arg("max_patterns") = -1);
     m.def("busted_estep", [](const Tree& t, const Alignment& a, const py::dict& p, const std::vector<double>& bl,
                              const std::vector<double>& omegas, const std::vector<double>& weights,
                              const std::vector<double>& syn_rates, const std::vector<double>& syn_weights,

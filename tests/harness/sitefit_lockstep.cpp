@@ -1,5 +1,5 @@
 // Host-logic harness for the site-fit drivers (h3g_sitefit.cpp, h3g_fel_driver.cpp with and
-// without a background branch set, h3g_meme_driver.cpp): the device evaluator is replaced by a CPU function of the
+// without a background branch set, h3g_meme_driver.cpp likewise): the device evaluator is replaced by a CPU function of the
 // solved omegas, so the lockstep loop's batching, eigensystem-slot assignment and
 // consistency checks run without a GPU.  The fake likelihood is rugged (a bowl plus
 // an oscillation) so the simplex searches take many steps, park several requests at
@@ -58,7 +58,7 @@ bool fel_device_eval(FelDevice* d, int n_eig, const double* eom, const int* es, 
 }
 int fel_device_max_ebf(const FelDevice* d) { return std::min(256, d->max_req); }
 bool fel_device_ebf(FelDevice* d, int, const double*, const int*, const int*, int n_req, const int*, const double*, const int*,
-                    const int*, const double*, double* ebf, std::string*) {
+                    const int*, const double*, const int*, double* ebf, std::string*) {
     for (size_t i = 0; i < size_t(n_req) * d->n; ++i) ebf[i] = 1.0;
     return true;
 }
@@ -90,12 +90,16 @@ static int run(int P) {
     std::vector<double> ebf(size_t(P) * pr.n);
     st = h3g_meme_run(&pr, &m, bl.data(), out.data(), ebf.data());
     if (st != H3G_OK) { printf("meme status %d %s\n", int(st), pr.err.c_str()); return 1; }
+    std::vector<h3g_meme_result> msub(P);
+    st = h3g_meme_run_tested(&pr, &m, bl.data(), tested, nullptr, msub.data(), ebf.data());
+    if (st != H3G_OK) { printf("meme subset status %d %s\n", int(st), pr.err.c_str()); return 1; }
     double sum = 0.0;
     long evals = 0;
     for (int p = 0; p < P; ++p) {
         sum += fel[p].log_l_alt + fel[p].log_l_null + out[p].log_l_meme + out[p].alpha + out[p].beta_plus + out[p].p1;
         sum += sub[p].log_l_alt + sub[p].log_l_null + sub[p].beta_nuisance;
-        evals += fel[p].evaluations + out[p].evaluations + sub[p].evaluations;
+        sum += msub[p].log_l_meme + msub[p].beta_bg + msub[p].alpha;
+        evals += fel[p].evaluations + out[p].evaluations + sub[p].evaluations + msub[p].evaluations;
     }
     printf("P %d checksum %.17g evaluations %ld\n", P, sum, evals);
     return 0;

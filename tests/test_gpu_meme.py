@@ -1,4 +1,4 @@
-"""MEME per-site fits on the device against the oracle's restatement of the reference (meme.hpp:166-632).
+"""MEME per-site fits on the device against the oracle's restatement of the reference (meme.hpp:84-632).
 
 Both run the reference's searches (FEL baseline, 4-D and 3-D bounded
 Nelder-Mead from the same start grids) pattern by pattern.  The device
@@ -57,6 +57,19 @@ def _hyphy_acceptance(k, lrt, pv):
     assert np.corrcoef(_ranks(pv), _ranks(mle[:, 6]))[0, 1] >= k["min_spearman_p"]
 
 
+def _same_log_ebf(e_dev, e_ref):
+    """log EBF = log L+ - log L1 at one branch.  The smaller of the two class likelihoods carries an
+    absolute error of up to ~1e-11 of the larger one's in any FP64 evaluation, the reference's
+    included (at a large omega the spectral transition matrices reach their small entries by
+    cancelling terms of order one), so the tolerance grows as 1e-11 e^|log EBF|; beyond
+    |log EBF| = 20 both sides must only lie beyond the same bound."""
+    ld, lr = np.log(np.maximum(e_dev, 1e-300)), np.log(np.maximum(e_ref, 1e-300))
+    big = np.abs(lr) > 20.0
+    tol = 1e-5 + 1e-11 * np.exp(np.abs(lr[~big]))
+    assert np.all(np.abs(ld[~big] - lr[~big]) <= tol), (ld[~big] - lr[~big], tol)
+    assert np.all(np.sign(ld[big]) == np.sign(lr[big])) and np.all(np.abs(ld[big]) > 20.0)
+
+
 def _case(oracle, golden_dir, name, fasta):
     k = json.loads((golden_dir / "known_answers.json").read_text())[name]
     a = oracle.Alignment.load(str(golden_dir / fasta))
@@ -110,8 +123,7 @@ def test_meme_cd2_ebf_matches_oracle(oracle, cd2):
         al = dev["alpha"][i]
         e_r = np.asarray(oracle.meme_ebf_at(t, a, k["params"], bl, int(i), al, dev["beta1"][i] / al, dev["p1"][i],
                                             dev["beta_plus"][i]))
-        # log EBF is a difference of two log-likelihoods of ~ -300: FP64 rounding of each is ~1e-7
-        np.testing.assert_allclose(np.log(np.maximum(e_d[i], 1e-300)), np.log(np.maximum(e_r, 1e-300)), rtol=0, atol=1e-5)
+        _same_log_ebf(e_d[i], e_r)
     assert np.mean(dev["branches_under_selection"] == np.asarray(ref["branches_under_selection"])) > 0.9
 
 
@@ -167,5 +179,56 @@ def test_meme_analyzer_api(oracle, golden_dir):
     pv = np.array([r.p_value for r in res])
     _hyphy_acceptance(k, lrt, pv)
     assert all(len(r.branch_ebf) == t.num_nodes() for r in res)
-    with pytest.raises(RuntimeError):
-        h3.MEMEAnalyzer(t, a, p, "Internal")
+    m = h3.MEMEAnalyzer(t, a, p, "Internal")
+    internal = [nd.id for nd in t.nodes if nd.id != t.root_id and not nd.is_leaf]
+    assert m.num_tested == len(internal) and m.num_background == t.num_nodes() - 1 - len(internal)
+    res = m.run()
+    leaves = [nd.id for nd in t.nodes if nd.is_leaf]
+    assert all(all(r.branch_ebf[i] == 1.0 for i in leaves) for r in res)
+    assert any(r.beta_bg > 0.0 for r in res)
+
+
+@pytest.fixture(scope="module")
+def cd2_leaves(ctx, oracle, golden_dir):
+    """CD2 with the leaves tested and the internal branches as background."""
+    k, a, t = _case(oracle, golden_dir, "cd2_meme", "cd2.fna")
+    tested = [bool(x) for x in t.is_leaf]
+    ref = oracle.meme_run_tested(t, a, k["params"], tested)
+    pi, qs, qn = _inputs(oracle, a, k["params"])
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    dev = pr.meme_run(pi=pi, Qs=qs, Qn=qn, branch_lengths=ref["branch_lengths"], tested=tested)
+    return k, a, t, tested, ref, dev
+
+
+def test_meme_subset_cd2_matches_oracle(cd2_leaves):
+    _, _, t, tested, ref, dev = cd2_leaves
+    inv = np.asarray(ref["evals"]) == 0
+    assert np.array_equal(dev["evaluations"] == 0, inv)
+    # the FEL baseline runs the branch-subset search: same searches, same optima
+    np.testing.assert_allclose(dev["log_l_fel"], ref["log_l_fel"], rtol=0, atol=1e-4)
+    d = np.abs(dev["log_l_meme"] - np.asarray(ref["log_l_meme"]))
+    assert np.mean(d[~inv] <= 1e-3) > 0.9
+    same = (~inv) & (d <= 1e-4)
+    np.testing.assert_allclose(dev["lrt"][same], np.asarray(ref["lrt"])[same], rtol=0, atol=5e-3)
+    assert np.corrcoef(dev["lrt"][~inv], np.asarray(ref["lrt"])[~inv])[0, 1] > 0.99
+    assert np.all((dev["beta_bg"][~inv] >= 1e-4) & (dev["beta_bg"][~inv] <= 1e5))
+    np.testing.assert_allclose(dev["total_branch_length"][same], np.asarray(ref["total_branch_length"])[same], rtol=1e-3)
+    background = [i for i in range(t.num_nodes()) if i != t.root and not tested[i]]
+    assert np.all(dev["branch_ebf"][:, background] == 1.0)
+
+
+def test_meme_subset_cd2_ebf_matches_oracle(oracle, cd2_leaves):
+    """Device EBFs with a background (k_meme_ebf<3>) against the oracle's re-prunings at the device's MLE."""
+    k, a, t, tested, ref, dev = cd2_leaves
+    e_d = dev["branch_ebf"]
+    np.testing.assert_array_equal((e_d >= 100).sum(axis=1), dev["branches_under_selection"])
+    fitted = np.asarray(ref["evals"]) > 0
+    reach = np.flatnonzero(fitted & (dev["beta_plus"] > dev["alpha"]) & (dev["p_plus"] > 1e-6))
+    assert len(reach) >= 5
+    bl = ref["branch_lengths"]
+    for i in reach:
+        al = dev["alpha"][i]
+        bg = dev["beta_bg"][i] if dev["beta_bg"][i] > 0.0 else dev["beta1"][i]
+        e_r = np.asarray(oracle.meme_ebf_at(t, a, k["params"], bl, int(i), al, dev["beta1"][i] / al, dev["p1"][i],
+                                            dev["beta_plus"][i], tested, bg))
+        _same_log_ebf(e_d[i], e_r)
