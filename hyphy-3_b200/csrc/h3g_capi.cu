@@ -23,7 +23,12 @@ struct h3g_ctx {
     bool own_stream = false;
     int live_problems = 0;
     std::string err;
+    void* compress = nullptr;      // alignment-compression scratch (h3g_compress.cu), kept between calls
 };
+
+namespace h3g {
+void compress_scratch_free(void* p);     // h3g_compress.cu
+}
 
 namespace {
 
@@ -164,6 +169,7 @@ extern "C" h3g_status h3g_ctx_destroy(h3g_ctx* ctx) {
     if (!ctx) return H3G_ERR_ARG;
     if (ctx->live_problems > 0) return fail(ctx, H3G_ERR_STATE, "destroy every problem before its context");
     cudaSetDevice(ctx->device);
+    if (ctx->compress) h3g::compress_scratch_free(ctx->compress);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return H3G_OK;
@@ -373,6 +379,11 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
 }
 
 namespace h3g {
+
+cudaStream_t ctx_stream(h3g_ctx* ctx) { return ctx->stream; }
+int ctx_device(h3g_ctx* ctx) { return ctx->device; }
+h3g_status ctx_fail(h3g_ctx* ctx, h3g_status st, const std::string& msg) { return fail(ctx, st, msg); }
+void*& ctx_compress_scratch(h3g_ctx* ctx) { return ctx->compress; }
 
 Topo problem_topo(h3g_problem* pr, int S) {
     Topo t = pr->topo();

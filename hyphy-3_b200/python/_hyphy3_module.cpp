@@ -11,6 +11,7 @@
 #include "hyphy/analyses/fel_gpu.hpp"
 #include "hyphy/analyses/meme_gpu.hpp"
 #include "hyphy/opt/optimizer_gpu.hpp"
+#include "hyphy/core/alignment_gpu.hpp"
 #include "hyphy/core/likelihood_gpu.hpp"
 
 namespace py = pybind11;
@@ -96,17 +97,35 @@ PYBIND11_MODULE(_hyphy3, m) {
 
     py::class_<Alignment>(m, "Alignment")
         .def(py::init<>())
-        .def_static("load", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
+        .def_static("load", [](const std::string& f, bool device) {
+            if (!device) return Alignment::load(f);
+            Alignment a = Alignment::load_unfinalized(f);
+            hyphy::core::finalize_on_device(a);
+            return a;
+        }, "filepath"_a, "device"_a = false)
         .def_static("from_fasta", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
         .def_static("from_nexus", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
         .def_static("from_text", [](const std::string& s) { return Alignment::from_text(s); }, "text"_a)
-        .def_static("from_sequences", [](const std::vector<std::string>& names, const std::vector<std::string>& seqs, const std::string& code) {
+        .def_static("from_sequences", [](const std::vector<std::string>& names, const std::vector<std::string>& seqs, const std::string& code,
+                                         bool device) {
             if (names.size() != seqs.size()) throw std::runtime_error("names and seqs differ in length");
             Alignment a;
             for (size_t i = 0; i < names.size(); ++i) a.add_sequence(names[i], seqs[i]);
-            a.finalize(GeneticCode::from_name(code));
+            if (device) hyphy::core::finalize_on_device(a, GeneticCode::from_name(code));
+            else a.finalize(GeneticCode::from_name(code));
             return a;
-        }, "names"_a, "seqs"_a, "code"_a = "Universal")
+        }, "names"_a, "seqs"_a, "code"_a = "Universal", "device"_a = false)
+        .def_property_readonly("site_to_pattern", [](const Alignment& a) { return a.site_to_pattern; })
+        .def("pattern_weights", [](const Alignment& a) {
+            std::vector<size_t> w;
+            for (const auto& p : a.patterns) w.push_back(p.weight);
+            return w;
+        })
+        .def("pattern_sites", [](const Alignment& a) {
+            std::vector<std::vector<size_t>> s;
+            for (const auto& p : a.patterns) s.push_back(p.sites);
+            return s;
+        })
         .def_readonly("num_taxa", &Alignment::num_taxa)
         .def_property_readonly("num_sequences", [](const Alignment& a) { return a.num_taxa; })
         .def_readonly("num_codons", &Alignment::num_codons)

@@ -26,7 +26,7 @@ EXPORTED = [
     "h3g_problem_destroy", "h3g_model_set", "h3g_eval", "h3g_eval_from_P", "h3g_branch_length_gradients",
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
-    "h3g_fel_run_tested", "h3g_meme_run_tested",
+    "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -50,6 +50,14 @@ class FelResult(C.Structure):
     _fields_ = [("alpha", C.c_double), ("beta", C.c_double), ("alpha_null", C.c_double), ("log_l_alt", C.c_double),
                 ("log_l_null", C.c_double), ("lrt", C.c_double), ("p_value", C.c_double), ("evaluations", C.c_int),
                 ("beta_nuisance", C.c_double)]
+
+
+class GeneticCodeDesc(C.Structure):
+    _fields_ = [("S", C.c_int), ("codon_to_sense", C.POINTER(C.c_int8))]
+
+
+class CompressInfo(C.Structure):
+    _fields_ = [("n_patterns", C.c_int64), ("pos_counts", C.c_int64 * 12), ("rounds", C.c_int), ("hash_bits", C.c_int)]
 
 
 class MemeResult(C.Structure):
@@ -100,6 +108,11 @@ def load() -> C.CDLL:
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
+        _i32p = C.POINTER(C.c_int32)
+        lib.h3g_alignment_compress.argtypes = [vp, C.c_int, C.c_int64, C.c_void_p, C.c_size_t, C.POINTER(GeneticCodeDesc), _i32p,
+                                               _i32p, _i32p, C.POINTER(C.c_int8), C.POINTER(C.c_uint64), C.POINTER(CompressInfo)]
+        lib.h3g_alignment_compress_device.argtypes = [vp, C.c_int, C.c_int64, C.c_void_p, C.c_size_t, C.POINTER(GeneticCodeDesc),
+                                                      vp, vp, vp, vp, vp, C.POINTER(CompressInfo)]
         lib.h3g_meme_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
                                             C.POINTER(MemeResult), _dp]
         for name in EXPORTED:
@@ -134,6 +147,34 @@ class Context:
     def check(self, st: int) -> None:
         if st != H3G_OK:
             raise H3GError(f"status {st}: {self.lib.h3g_last_error(self.h).decode()}")
+
+    def alignment_compress(self, rows, codon_to_sense, hash_bits: int = 0) -> dict:
+        """Codon translation, nucleotide counts and site-pattern compression of an in-frame alignment
+        (h3g_alignment_compress).  rows: [n_taxa, n_nuc] uint8 array (or equal-length strings);
+        codon_to_sense: 64 sense indices (-1 for stops) in A, C, G, T order.  Returns the patterns in
+        first-site order: "site_to_pattern", "weight", "first_site", "states" [P, T], "masks" [P, T],
+        "pos_counts" [3, 4], "rounds"."""
+        if not isinstance(rows, np.ndarray):
+            rows = np.frombuffer(b"".join(r.encode("latin-1") for r in rows), dtype=np.uint8).reshape(len(rows), -1)
+        rows = np.ascontiguousarray(rows, dtype=np.uint8)
+        T, L = rows.shape
+        sense = np.ascontiguousarray(codon_to_sense, dtype=np.int8)
+        code = GeneticCodeDesc(S=int((sense >= 0).sum()), codon_to_sense=sense.ctypes.data_as(C.POINTER(C.c_int8)))
+        Cn = L // 3
+        s2p = np.zeros(max(Cn, 1), np.int32)
+        w = np.zeros(max(Cn, 1), np.int32)
+        first = np.zeros(max(Cn, 1), np.int32)
+        st = np.zeros((max(Cn, 1), T), np.int8)
+        mk = np.zeros((max(Cn, 1), T), np.uint64)
+        info = CompressInfo(hash_bits=hash_bits)
+        i32 = C.POINTER(C.c_int32)
+        self.check(self.lib.h3g_alignment_compress(
+            self.h, T, L, rows.ctypes.data_as(C.c_void_p), L, C.byref(code), s2p.ctypes.data_as(i32), w.ctypes.data_as(i32),
+            first.ctypes.data_as(i32), st.ctypes.data_as(C.POINTER(C.c_int8)), mk.ctypes.data_as(C.POINTER(C.c_uint64)),
+            C.byref(info)))
+        P = int(info.n_patterns)
+        return {"site_to_pattern": s2p[:Cn], "weight": w[:P], "first_site": first[:P], "states": st[:P], "masks": mk[:P],
+                "pos_counts": np.array(info.pos_counts[:], dtype=np.int64).reshape(3, 4), "rounds": int(info.rounds)}
 
     def close(self) -> None:
         """Destroy the context after every problem still alive on it."""

@@ -275,6 +275,51 @@ h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* model, const dou
 h3g_status h3g_meme_run_tested(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths,
                                const uint8_t* tested, const uint8_t* fel_tested, h3g_meme_result* out, double* branch_ebf);
 
+/* ---------------------------------------------------------------- alignments
+ * Alignment::finalize's codon translation, nucleotide counts and pattern
+ * compression (include/hyphy/core/alignment.hpp:665-722, :893-911, :1021-1078)
+ * on the device.  Each codon column of the in-frame alignment is translated
+ * per taxon to a sense-codon state (-1 when ambiguous, a gap or a stop) and a
+ * mask of the compatible sense codons (genetic_code.hpp:82-109: IUPAC
+ * ambiguity, '!' and all-ambiguous triplets and stops give every sense codon);
+ * identical columns (same states and masks) form one site pattern, patterns
+ * are numbered in the order of their first site, and the weight of a pattern
+ * is its number of sites.  Unambiguous A/C/G/T(U) characters are counted per
+ * codon position.  Identity is decided by comparing the translated columns in
+ * full, so the result does not depend on the column hash. */
+typedef struct {
+    int S;                          /* sense codons, 1..63 */
+    const int8_t* codon_to_sense;   /* [64] sense index of codon 16 n1 + 4 n2 + n3 (A, C, G, T = 0..3), -1 for a stop */
+} h3g_genetic_code;
+
+typedef struct {
+    int64_t n_patterns;             /* distinct columns */
+    int64_t pos_counts[12];         /* unambiguous nucleotides at codon position p, [p][A C G T] */
+    int rounds;                     /* hash rounds used (1 unless hashes of different columns collided) */
+    int hash_bits;                  /* in: 0 or 64 for the full column hash; 1..63 keeps only that many bits (tests) */
+} h3g_compress_info;
+
+/* seqs: n_taxa rows of n_nuc characters (n_nuc a positive multiple of 3), row i at
+ * seqs + i * row_stride, host memory.  n_codons = n_nuc / 3.  Outputs, host memory,
+ * sized for n_codons patterns (the first n_patterns rows are written):
+ * site_to_pattern[n_codons], pattern_weight[n_codons], pattern_first_site[n_codons]
+ * (may be NULL), pattern_states[n_codons * n_taxa] and pattern_masks[n_codons * n_taxa]
+ * (pattern-major, as SitePattern::states / ambiguous_masks).  info->hash_bits is read,
+ * the rest written.  The context's stream carries the copies and kernels; the call
+ * blocks until the results are on the host. */
+h3g_status h3g_alignment_compress(h3g_ctx* ctx, int n_taxa, int64_t n_nuc, const char* seqs, size_t row_stride,
+                                  const h3g_genetic_code* code, int32_t* site_to_pattern, int32_t* pattern_weight,
+                                  int32_t* pattern_first_site, int8_t* pattern_states, uint64_t* pattern_masks,
+                                  h3g_compress_info* info);
+
+/* The same with every array in device memory (d_seqs read, the outputs written
+ * on the context's stream).  info (host) receives n_patterns and the counts;
+ * the call returns once they are known, the outputs complete on the stream. */
+h3g_status h3g_alignment_compress_device(h3g_ctx* ctx, int n_taxa, int64_t n_nuc, const char* d_seqs, size_t row_stride,
+                                         const h3g_genetic_code* code, int32_t* d_site_to_pattern, int32_t* d_pattern_weight,
+                                         int32_t* d_pattern_first_site, int8_t* d_pattern_states, uint64_t* d_pattern_masks,
+                                         h3g_compress_info* info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -211,15 +211,23 @@ public:
     static Alignment from_fasta(const std::string& path) { return load(path); }
     static Alignment from_nexus(const std::string& path) { return load(path); }
 
-    static Alignment from_text(const std::string& text, std::shared_ptr<const GeneticCode> gc = nullptr) {
+    // finalize = false leaves the sequences as read (load_unfinalized, alignment.hpp:648-650)
+    static Alignment from_text(const std::string& text, std::shared_ptr<const GeneticCode> gc = nullptr, bool finalize = true) {
         Alignment a;
         size_t b = text.find_first_not_of(" \t\r\n");
         if (b != std::string::npos && (text.compare(b, 6, "#NEXUS") == 0 || text.compare(b, 6, "#nexus") == 0))
             a.read_nexus(text);
         else
             a.read_fasta(text);
-        a.finalize(gc);
+        if (finalize) a.finalize(gc);
+        else if (gc) a.code = gc;
         return a;
+    }
+    static Alignment load_unfinalized(const std::string& path) {
+        std::ifstream f(path, std::ios::binary);
+        if (!f) throw std::runtime_error("Could not open alignment file: " + path);
+        std::stringstream ss; ss << f.rdbuf();
+        return from_text(ss.str(), nullptr, false);
     }
 
     // alignment.hpp:665-723
@@ -348,12 +356,20 @@ private:
 
     // alignment.hpp:893-1019 — empirical nucleotide and positional frequencies, then CF3x4.
     void compute_frequencies() {
-        double nc[4] = {0, 0, 0, 0}, pc[3][4] = {};
+        double pc[3][4] = {};
         for (auto& s : sequences)
             for (size_t i = 0; i < 3 * num_codons; ++i) {
                 int n = char_to_nuc(s.raw_seq[i]);
-                if (n >= 0) { nc[n] += 1; pc[i % 3][n] += 1; }
+                if (n >= 0) pc[i % 3][n] += 1;
             }
+        frequencies_from_counts(pc);
+    }
+
+public:
+    // alignment.hpp:911-1019 from the counts of unambiguous nucleotides per codon position
+    void frequencies_from_counts(const double pc[3][4]) {
+        double nc[4];
+        for (int b = 0; b < 4; ++b) nc[b] = pc[0][b] + pc[1][b] + pc[2][b];
         auto floor_norm = [](double* f) {
             bool pad = false;
             for (int b = 0; b < 4; ++b) if (f[b] < 1e-8) { f[b] = 1e-8; pad = true; }
@@ -401,6 +417,7 @@ private:
         std::copy(&x[0][0], &x[0][0] + 12, &pos_nuc_frequencies[0][0]);
     }
 
+private:
     // alignment.hpp:1021-1078 — unique columns in first-occurrence order.
     void compress_patterns() {
         const size_t T = num_taxa;
