@@ -62,6 +62,10 @@ MEASURED_TRAFFIC = {
     (1, "fp64"): {"inside": 36.5e6, "outside": 68.7e6, "accum_A": 98.3e6},
     (3, "mixed"): {"inside": 16.763e9, "outside": 27.682e9, "accum_A": 18.793e9},
     (3, "fp64"): {"inside": 29.259e9, "outside": 48.234e9, "accum_A": 34.723e9},
+    # alignment compression, 1024 taxa x 100000 codons, captured at full size (one pass:
+    # dram__bytes_read.sum + dram__bytes_write.sum of the call's launch)
+    ("compress", "translate"): 479.30e6,
+    ("compress", "rounds"): 207.80e6,
 }
 
 
@@ -542,6 +546,158 @@ def run_fel(args) -> None:
     ctx.close()
 
 
+COMPRESS_METRIC = "alignment cells (taxon x codon) translated and compressed to site patterns per second"
+COMPRESS_WORKLOAD = ("Alignment::finalize on the device: 1024 taxa x 100000 codons, columns resampled with replacement "
+                     "from a simulated 1024-taxon Yule alignment of 5000 codons; codon translation, positional nucleotide "
+                     "counts, site patterns in first-occurrence order")
+
+
+def _compress_rows(n_codons: int):
+    """[1024, 3 n_codons] uint8 rows: columns of the 1024-taxon simulated alignment drawn with replacement."""
+    from hyphy3.simulate import make_workload
+    wl = make_workload(3)
+    T = len(wl.seqs)
+    base = np.frombuffer(b"".join(x.encode() for x in wl.seqs), np.uint8).reshape(T, -1, 3)
+    cols = np.random.default_rng(SEED_COMPRESS).integers(0, base.shape[1], n_codons)
+    return np.ascontiguousarray(base[:, cols, :].reshape(T, -1))
+
+
+SEED_COMPRESS = 20261204
+
+
+def run_compress(args) -> None:
+    """h3g_alignment_compress_device on device-resident rows (value) and h3g_alignment_compress from
+    pinned host rows (e2e); the oracle's finalize on the same rows as the CPU baseline."""
+    import ctypes as C
+    import torch
+    from hyphy3 import _capi
+    n_codons = args.sites or 100000
+    rows = _compress_rows(n_codons)
+    T, L = rows.shape
+    cells = T * n_codons
+    stream = torch.cuda.current_stream()
+    ctx = _capi.Context(0, stream=stream.cuda_stream)
+    lib = ctx.lib
+    sense = np.full(64, -1, np.int8)
+    from hyphy3.simulate import universal_code
+    codons, _ = universal_code()
+    for i, cod in enumerate(codons):
+        sense[16 * cod[0] + 4 * cod[1] + cod[2]] = i
+    code = _capi.GeneticCodeDesc(S=len(codons), codon_to_sense=sense.ctypes.data_as(C.POINTER(C.c_int8)))
+    d_rows = torch.from_numpy(rows).cuda()
+    d_s2p = torch.empty(n_codons, dtype=torch.int32, device="cuda")
+    d_w = torch.empty(n_codons, dtype=torch.int32, device="cuda")
+    d_first = torch.empty(n_codons, dtype=torch.int32, device="cuda")
+    d_st = torch.empty(n_codons * T, dtype=torch.int8, device="cuda")
+    d_mk = torch.empty(n_codons * T, dtype=torch.int64, device="cuda")
+    info = _capi.CompressInfo()
+    vp = C.c_void_p
+
+    def dev_call(profile=0):
+        info.profile = profile
+        ctx.check(lib.h3g_alignment_compress_device(ctx.h, T, L, vp(d_rows.data_ptr()), L, C.byref(code), vp(d_s2p.data_ptr()),
+                                                    vp(d_w.data_ptr()), vp(d_first.data_ptr()), vp(d_st.data_ptr()),
+                                                    vp(d_mk.data_ptr()), C.byref(info)))
+
+    warm = max(3, args.warmup)
+    for _ in range(warm):
+        dev_call()
+    torch.cuda.synchronize()
+    if args.profile:                                                     # one more call, nothing else (for ncu)
+        dev_call()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "compress", "codons": n_codons, "patterns": int(info.n_patterns),
+                          "gpu_launches": int(info.launches)}), flush=True)
+        ctx.close()
+        return
+    steps = max(3, min(args.steps, 50))
+    # stage times of the library's own events (one profiled call per step, outside the timed loop)
+    stage = np.zeros(4)
+    for _ in range(steps):
+        dev_call(profile=1)
+        stage += np.array(info.stage_ms[:])
+    stage /= steps
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        dev_call()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / steps
+    P = int(info.n_patterns)
+    launches = int(info.launches)
+    # e2e: the C ABI with host buffers (pinned), copies in the timed region
+    h_rows = torch.from_numpy(rows).pin_memory()
+    h_s2p = torch.empty(n_codons, dtype=torch.int32).pin_memory()
+    h_w = torch.empty(n_codons, dtype=torch.int32).pin_memory()
+    h_first = torch.empty(n_codons, dtype=torch.int32).pin_memory()
+    h_st = torch.empty(n_codons * T, dtype=torch.int8).pin_memory()
+    h_mk = torch.empty(n_codons * T, dtype=torch.int64).pin_memory()
+    i32 = C.POINTER(C.c_int32)
+
+    def host_call():
+        ctx.check(lib.h3g_alignment_compress(ctx.h, T, L, vp(h_rows.data_ptr()), L, C.byref(code), C.cast(h_s2p.data_ptr(), i32),
+                                             C.cast(h_w.data_ptr(), i32), C.cast(h_first.data_ptr(), i32),
+                                             C.cast(h_st.data_ptr(), C.POINTER(C.c_int8)),
+                                             C.cast(h_mk.data_ptr(), C.POINTER(C.c_uint64)), C.byref(info)))
+
+    host_call()
+    e2e = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        host_call()
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e)
+    assert np.array_equal(h_s2p.numpy(), d_s2p.cpu().numpy()) and int(info.n_patterns) == P
+    # roofline of the dominant stage: algorithmic bytes per call
+    dup_cells = T * (n_codons - P)
+    algo = {"translate": 5 * cells,                                      # 3 B read, 2 B key written per cell
+            "rounds": 4 * dup_cells + 24 * n_codons,                    # keys of a duplicate and of its first column; hash/table
+            "numbering": 16 * n_codons,
+            "output": 16 * n_codons + 11 * P * T}                       # site map, weights; 2 B read + 9 B written per pattern cell
+    names = ["translate", "rounds", "numbering", "output"]
+    k = int(np.argmax(stage))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo[names[k]] / (stage[k] * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        import h3oracle as o
+        seqs = [bytes(r).decode("latin-1") for r in rows]
+        t0 = time.perf_counter()
+        ref = o.Alignment.from_sequences([f"t{i}" for i in range(T)], seqs, "Universal")
+        cs = time.perf_counter() - t0
+        ok = ref.num_patterns == P and np.array_equal(np.asarray(ref.site_pattern), h_s2p.numpy())
+        cpu = {"value": cells / cs, "unit": "cells/s", "cores": 1, "kind": "port",
+               "sample": f"the whole workload ({cells} cells), {cs:.1f} s, one thread: the oracle's restatement of "
+                         f"alignment.hpp:665-722, 1021-1078 (std::map of translated columns); same patterns: {ok}"}
+    line = {
+        "metric": COMPRESS_METRIC, "value": cells / (ms * 1e-3), "unit": "cells/s", "n_gpus": 1, "steps": steps,
+        "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u64",
+        "data": "synthetic",
+        "config": {"workload": COMPRESS_WORKLOAD, "taxa": T, "codons": n_codons, "patterns": P,
+                   "l2": "inputs (307 MB) and keys (205 MB) larger than L2, no flush"},
+        "e2e": {"value": cells / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(rows.nbytes),
+                "d2h_bytes_per_step": int(4 * n_codons + 8 * P + 9 * P * T),
+                "api": "h3g_alignment_compress (C ABI, pinned host buffers)", "timing": "host wall clock, median"},
+        "gpu_launches": launches * steps,
+        "stage_ms": dict(zip(names, map(float, stage))),
+        "roofline": {"bound": "hbm", "kernel": names[k], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": MEASURED_TRAFFIC.get(("compress", names[k])),
+                     "traffic_unit": "bytes per call (the stage's launches), from ncu",
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "algorithmic_bytes": algo[names[k]]},
+        "cpu_baseline": cpu, "clocks": clocks,
+        "timing": "CUDA events on the launching stream around the timed calls (each call reads its round count back)",
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def _mixed_available() -> bool:
     return os.environ.get("H3G_BENCH_PRECISION", "mixed") == "mixed"
 
@@ -633,9 +789,12 @@ def main() -> None:
     ap.add_argument("--config", type=int, choices=[1, 2, 3], default=1,
                     help="1: 64-taxon 3-omega mixture (headline); 2: FEL per-site fits, 256 taxa x 2000 codons; "
                          "3: 1024-taxon, 4 rate x 2 omega classes")
-    ap.add_argument("--analysis", choices=["fel", "meme"], default="fel", help="--config 2: which per-site analysis")
+    ap.add_argument("--analysis", choices=["fel", "meme", "compress"], default="fel",
+                    help="--config 2: which per-site analysis; compress: alignment finalize on the device (any config)")
     args = ap.parse_args()
-    if args.config == 2 and args.impl == "ours":
+    if args.analysis == "compress" and args.impl == "ours":
+        run_compress(args)
+    elif args.config == 2 and args.impl == "ours":
         run_fel(args)
     elif args.profile:
         run_profile(args)

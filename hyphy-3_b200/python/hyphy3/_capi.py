@@ -57,7 +57,8 @@ class GeneticCodeDesc(C.Structure):
 
 
 class CompressInfo(C.Structure):
-    _fields_ = [("n_patterns", C.c_int64), ("pos_counts", C.c_int64 * 12), ("rounds", C.c_int), ("hash_bits", C.c_int)]
+    _fields_ = [("n_patterns", C.c_int64), ("pos_counts", C.c_int64 * 12), ("rounds", C.c_int), ("hash_bits", C.c_int),
+                ("profile", C.c_int), ("stage_ms", C.c_double * 4), ("launches", C.c_int)]
 
 
 class MemeResult(C.Structure):

@@ -297,6 +297,10 @@ typedef struct {
     int64_t pos_counts[12];         /* unambiguous nucleotides at codon position p, [p][A C G T] */
     int rounds;                     /* hash rounds used (1 unless hashes of different columns collided) */
     int hash_bits;                  /* in: 0 or 64 for the full column hash; 1..63 keeps only that many bits (tests) */
+    int profile;                    /* in: nonzero records device times of the stages into stage_ms */
+    double stage_ms[4];             /* translate (k_translate), rounds (hash / insert / verify), numbering (scan),
+                                       output (assign / gather); device event times, 0 unless profile */
+    int launches;                   /* kernels the call launched */
 } h3g_compress_info;
 
 /* seqs: n_taxa rows of n_nuc characters (n_nuc a positive multiple of 3), row i at
