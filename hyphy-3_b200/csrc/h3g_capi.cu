@@ -28,6 +28,7 @@ struct h3g_ctx {
 
 namespace h3g {
 void compress_scratch_free(void* p);     // h3g_compress.cu
+void nuc_state_free(void* p);            // h3g_nuc.cu
 }
 
 namespace {
@@ -96,6 +97,7 @@ struct h3g_problem {
     // captured evaluation graphs, keyed by (want, with host copies)
     // the site-fit evaluator of the last h3g_fel_run / h3g_meme_run, kept for the next run
     h3g::FelDevice* fel_dev = nullptr;
+    void* nuc = nullptr;               // nucleotide evaluator (h3g_nuc.cu), built on first use
     struct GraphEntry { unsigned key; cudaGraphExec_t exec; int launches; };
     std::vector<GraphEntry> graphs;
     void drop_graphs() {
@@ -105,6 +107,7 @@ struct h3g_problem {
     ~h3g_problem() {
         drop_graphs();
         h3g::fel_device_free(fel_dev);
+        if (nuc) h3g::nuc_state_free(nuc);
         if (h_pin) cudaFreeHost(h_pin);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -409,6 +412,8 @@ void fel_set_error(h3g_problem* pr, const std::string& msg) {
 }
 
 FelDevice*& problem_fel_device(h3g_problem* pr) { return pr->fel_dev; }
+void*& problem_nuc_state(h3g_problem* pr) { return pr->nuc; }
+int problem_max_state(h3g_problem* pr) { return pr->max_state; }
 
 void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h, int launches, double ms) {
     pr->last_h2d = h2d;

@@ -116,6 +116,7 @@ PYBIND11_MODULE(_hyphy3, m) {
             return a;
         }, "names"_a, "seqs"_a, "code"_a = "Universal", "device"_a = false)
         .def_property_readonly("site_to_pattern", [](const Alignment& a) { return a.site_to_pattern; })
+        .def("to_nucleotide_alignment", &Alignment::to_nucleotide_alignment)
         .def("pattern_weights", [](const Alignment& a) {
             std::vector<size_t> w;
             for (const auto& p : a.patterns) w.push_back(p.weight);
@@ -155,6 +156,39 @@ PYBIND11_MODULE(_hyphy3, m) {
             }
             return py::make_tuple(st, mk, w);
         }, "(states[P,T] int8, masks[P,T] uint64, weights[P]) of the compressed patterns");
+
+    py::class_<hyphy::core::GTRParameters>(m, "GTRParameters")
+        .def(py::init<>())
+        .def_readwrite("theta_AC", &hyphy::core::GTRParameters::theta_AC)
+        .def_readwrite("theta_AT", &hyphy::core::GTRParameters::theta_AT)
+        .def_readwrite("theta_CG", &hyphy::core::GTRParameters::theta_CG)
+        .def_readwrite("theta_CT", &hyphy::core::GTRParameters::theta_CT)
+        .def_readwrite("theta_GT", &hyphy::core::GTRParameters::theta_GT);
+    py::class_<hyphy::core::GTRMatrix>(m, "GTRMatrix")
+        .def(py::init<>())
+        .def("update", [](hyphy::core::GTRMatrix& g, const hyphy::core::GTRParameters& p, const std::vector<double>& f) {
+            if (f.size() != 4) throw std::runtime_error("frequencies need 4 entries");
+            g.update(p, f.data());
+        }, "params"_a, "frequencies"_a)
+        .def("transition_matrix", [](const hyphy::core::GTRMatrix& g, Scalar t) {
+            const auto P = g.transition_matrix(t);
+            py::array_t<double> r({4, 4});
+            std::copy(P.v.begin(), P.v.end(), r.mutable_data());
+            return r;
+        }, "t"_a)
+        .def_readonly("scale_factor", &hyphy::core::GTRMatrix::scale_factor)
+        .def_readonly("pi", &hyphy::core::GTRMatrix::pi)
+        .def_readonly("eigenvalues", &hyphy::core::GTRMatrix::eigenvalues);
+    m.def("compute_gtr_log_likelihood", [](const Tree& tree, const Alignment& aln, const hyphy::core::GTRMatrix& g) {
+        std::vector<Scalar> site;
+        Scalar l;
+        {
+            py::gil_scoped_release rel;
+            l = LikelihoodEngine::compute_gtr_log_likelihood(tree, aln, g, nullptr, &site);
+        }
+        return py::make_tuple(l, site);
+    }, "tree"_a, "alignment"_a, "gtr_model"_a,
+       "LikelihoodEngine::compute_gtr_log_likelihood on the device: (lnL, per-pattern lnL)");
 
     py::class_<MG94Parameters>(m, "MG94Parameters")
         .def(py::init<>())

@@ -27,6 +27,7 @@ EXPORTED = [
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
+    "h3g_nuc_eval_from_P",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -107,6 +108,7 @@ def load() -> C.CDLL:
                                                 C.POINTER(C.c_int32), C.c_int, C.c_int, C.POINTER(C.c_int8),
                                                 C.POINTER(C.c_uint64), _dp, C.c_int, _dp, _dp, _dp, _dp]
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
+        lib.h3g_nuc_eval_from_P.argtypes = [vp, _dp, _dp, _dp, _dp]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)

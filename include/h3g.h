@@ -275,6 +275,18 @@ h3g_status h3g_meme_run(h3g_problem* prob, const h3g_fel_model* model, const dou
 h3g_status h3g_meme_run_tested(h3g_problem* prob, const h3g_fel_model* model, const double* branch_lengths,
                                const uint8_t* tested, const uint8_t* fel_tested, h3g_meme_result* out, double* branch_ebf);
 
+/* ---------------------------------------------------------------- nucleotide GTR
+ * The nucleotide log-likelihood of LikelihoodEngine::compute_gtr_log_likelihood
+ * (include/hyphy/core/likelihood.hpp:181-254) on a problem whose patterns are
+ * nucleotide patterns (states 0..3 or -1, masks over A C G T as built by
+ * Alignment::to_nucleotide_alignment, alignment.hpp:832-890).  P[n_nodes][4][4]
+ * row-major transition matrices (the root's entry ignored), pi[4] the root
+ * frequencies.  *lnl = sum over patterns of weight x (log L, or -1e20 when
+ * L <= 0), a fixed-order Neumaier sum; site_lnl[n_patterns] (may be NULL) the
+ * per-pattern log-likelihoods.  One thread per pattern walks the tree depth-first
+ * (FP64, power-of-two rescaling).  Blocks until done. */
+h3g_status h3g_nuc_eval_from_P(h3g_problem* prob, const double* P, const double* pi, double* lnl, double* site_lnl);
+
 /* ---------------------------------------------------------------- alignments
  * Alignment::finalize's codon translation, nucleotide counts and pattern
  * compression (include/hyphy/core/alignment.hpp:665-722, :893-911, :1021-1078)

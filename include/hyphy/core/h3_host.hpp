@@ -366,6 +366,44 @@ private:
     }
 
 public:
+    // alignment.hpp:832-890: the nucleotide patterns of this alignment (num_codons = 0): per site
+    // the IUPAC set of every taxon is the key, state = the unambiguous nucleotide or -1, mask = the
+    // set; patterns in first-occurrence order; this alignment's nucleotide frequencies are kept.
+    Alignment to_nucleotide_alignment() const {
+        if (num_codons == 0 && !patterns.empty()) return *this;
+        Alignment r;
+        r.taxon_names = taxon_names;
+        r.sequences = sequences;
+        r.num_taxa = num_taxa;
+        r.num_nucleotides = num_nucleotides;
+        r.num_codons = 0;
+        r.code = code;
+        r.embedded_tree_newick = embedded_tree_newick;
+        std::copy(nuc_frequencies, nuc_frequencies + 4, r.nuc_frequencies);
+        std::unordered_map<std::string, size_t> seen;
+        r.site_to_pattern.assign(num_nucleotides, 0);
+        std::string key(num_taxa, 'N');
+        for (size_t site = 0; site < num_nucleotides; ++site) {
+            for (size_t t = 0; t < num_taxa; ++t) key[t] = char('A' + char_to_iupac_mask(sequences[t].raw_seq[site]));
+            auto [it, fresh] = seen.emplace(key, r.patterns.size());
+            if (fresh) {
+                SitePattern p;
+                p.states.resize(num_taxa);
+                p.ambiguous_masks.resize(num_taxa);
+                for (size_t t = 0; t < num_taxa; ++t) {
+                    const char ch = sequences[t].raw_seq[site];
+                    p.states[t] = char_to_nuc(ch);
+                    p.ambiguous_masks[t] = char_to_iupac_mask(ch);
+                }
+                r.patterns.push_back(std::move(p));
+            }
+            r.patterns[it->second].weight += 1;
+            r.patterns[it->second].sites.push_back(site);
+            r.site_to_pattern[site] = it->second;
+        }
+        return r;
+    }
+
     // alignment.hpp:911-1019 from the counts of unambiguous nucleotides per codon position
     void frequencies_from_counts(const double pc[3][4]) {
         double nc[4];
@@ -962,6 +1000,77 @@ public:
                 for (int j = 0; j < S; ++j) P(i, j) += u * V_pi(k, j);
             }
         for (auto& x : P.v) x = std::max(x, 0.0);
+        return P;
+    }
+};
+
+// ------------------------------------------------------------------- GTR
+// rate_matrix.hpp:14-21
+struct GTRParameters {
+    Scalar theta_AC = 1.0, theta_AT = 1.0, theta_CG = 1.0, theta_CT = 1.0, theta_GT = 1.0;   // theta_AG = 1
+};
+
+// rate_matrix.hpp:23-104: nucleotide GTR normalised to mean rate 1 (scale_factor), symmetric
+// eigensystem of diag(sqrt pi) Q diag(1 / sqrt pi) with pi floored at 1e-12, eigenvalues clamped
+// <= 0, P(t) = U_pi diag(e^{lambda t}) V_pi clamped at 0.
+class GTRMatrix {
+public:
+    Matrix Q{4, 4};
+    Vector pi = Vector(4, 0.0), sqrt_pi = Vector(4, 0.0), inv_sqrt_pi = Vector(4, 0.0), eigenvalues = Vector(4, 0.0);
+    Matrix U_pi{4, 4}, V_pi{4, 4};
+    Scalar scale_factor = 1.0;
+
+    void update(const GTRParameters& p, const double freq[4]) {
+        const double r[4][4] = {{0.0, p.theta_AC, 1.0, p.theta_AT},
+                                {p.theta_AC, 0.0, p.theta_CG, p.theta_CT},
+                                {1.0, p.theta_CG, 0.0, p.theta_GT},
+                                {p.theta_AT, p.theta_CT, p.theta_GT, 0.0}};
+        for (int i = 0; i < 4; ++i) {
+            pi[i] = freq[i];
+            sqrt_pi[i] = std::sqrt(std::max(pi[i], 1e-12));
+            inv_sqrt_pi[i] = 1.0 / sqrt_pi[i];
+        }
+        Q = Matrix(4, 4);
+        for (int i = 0; i < 4; ++i) {
+            double row = 0.0;
+            for (int j = 0; j < 4; ++j)
+                if (i != j) { Q(i, j) = r[i][j] * pi[j]; row += Q(i, j); }
+            Q(i, i) = -row;
+        }
+        double avg = 0.0;
+        for (int i = 0; i < 4; ++i) avg -= pi[i] * Q(i, i);
+        scale_factor = 1.0;
+        if (avg > 0.0) {
+            scale_factor = avg;
+            for (auto& x : Q.v) x /= avg;
+        }
+        std::vector<double> sym(16);
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) sym[size_t(i) * 4 + j] = sqrt_pi[i] * Q(i, j) * inv_sqrt_pi[j];
+        for (int i = 0; i < 4; ++i)
+            for (int j = i + 1; j < 4; ++j) {
+                const double m = 0.5 * (sym[size_t(i) * 4 + j] + sym[size_t(j) * 4 + i]);
+                sym[size_t(i) * 4 + j] = sym[size_t(j) * 4 + i] = m;
+            }
+        std::vector<double> Z;
+        symmetric_eigen(4, std::move(sym), eigenvalues, Z);
+        for (auto& l : eigenvalues) l = std::min(l, 0.0);
+        for (int i = 0; i < 4; ++i)
+            for (int k = 0; k < 4; ++k) {
+                U_pi(i, k) = inv_sqrt_pi[i] * Z[size_t(i) * 4 + k];
+                V_pi(k, i) = Z[size_t(i) * 4 + k] * sqrt_pi[i];
+            }
+    }
+    void update(const GTRParameters& p, const Vector& freq) { update(p, freq.data()); }
+
+    Matrix transition_matrix(Scalar t) const {
+        Matrix P(4, 4);
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) {
+                double x = 0.0;
+                for (int k = 0; k < 4; ++k) x += U_pi(i, k) * std::exp(eigenvalues[k] * t) * V_pi(k, j);
+                P(i, j) = std::max(x, 0.0);
+            }
         return P;
     }
 };

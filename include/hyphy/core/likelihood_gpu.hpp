@@ -4,6 +4,7 @@
 //   compute_branch_length_gradients   :1102-1211
 //   compute_joint_frechet_gradients   :1228-1594  (JointMG94Gradients :1213-1223)
 //   compute_tree_log_likelihood_from_P :766-806
+//   compute_gtr_log_likelihood         :181-254
 //   compute_mg94_log_likelihood        :257-292
 //   build_leaf_to_taxon_map            :162-178
 // and adds the BUSTED mixture gradient (include/hyphy/analyses/busted.hpp:1138-1429)
@@ -462,6 +463,32 @@ public:
         for (const auto& nd : tree.nodes)
             if (nd.id != tree.root_id) Pb[size_t(nd.id)] = mg94.transition_matrix(nd.branch_length * branch_scale);
         return compute_tree_log_likelihood_from_P(tree, aln, Pb, mg94.pi, S, custom_leaf_to_taxon);
+    }
+
+    // likelihood.hpp:181-254: the GTR log-likelihood of a nucleotide alignment (as from
+    // Alignment::to_nucleotide_alignment; a codon alignment is converted first)
+    static Scalar compute_gtr_log_likelihood(const Tree& tree, const Alignment& aln, const GTRMatrix& gtr_model,
+                                             const std::vector<size_t>* custom_leaf_to_taxon = nullptr,
+                                             std::vector<Scalar>* site_log_likelihoods = nullptr) {
+        if (aln.num_codons != 0) {
+            const Alignment nuc = aln.to_nucleotide_alignment();
+            return compute_gtr_log_likelihood(tree, nuc, gtr_model, custom_leaf_to_taxon, site_log_likelihoods);
+        }
+        auto& eng = gpu_detail::Engine::get();
+        std::vector<size_t> local;
+        const auto& l2t = custom_leaf_to_taxon ? *custom_leaf_to_taxon : (local = build_leaf_to_taxon_map(tree, aln));
+        h3g_problem* pr = eng.problem(tree, aln, l2t);
+        std::vector<double> P(tree.num_nodes() * 16, 0.0);
+        for (const auto& nd : tree.nodes) {
+            if (nd.id == tree.root_id) continue;
+            const Matrix m = gtr_model.transition_matrix(nd.branch_length);
+            std::copy(m.v.begin(), m.v.end(), P.begin() + ptrdiff_t(size_t(nd.id) * 16));
+        }
+        double lnl = 0.0;
+        if (site_log_likelihoods) site_log_likelihoods->assign(aln.patterns.size(), 0.0);
+        eng.check(h3g_nuc_eval_from_P(pr, P.data(), gtr_model.pi.data(), &lnl,
+                                      site_log_likelihoods ? site_log_likelihoods->data() : nullptr));
+        return lnl;
     }
 };
 

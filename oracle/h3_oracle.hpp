@@ -688,7 +688,7 @@ inline void leaf_vector(const Alignment& a, int p, int taxon, int S, double* out
     int st = a.states[size_t(p) * a.T + taxon];
     if (st >= 0 && st < S) { std::fill(out, out + S, 0.0); out[st] = 1.0; return; }
     uint64_t m = a.masks[size_t(p) * a.T + taxon];
-    uint64_t all = a.code.all_sense();
+    const uint64_t all = S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1);
     if (m == 0 || (m & all) == all) { std::fill(out, out + S, 1.0); return; }
     for (int s = 0; s < S; ++s) out[s] = (m >> s & 1) ? 1.0 : 0.0;
 }
@@ -785,6 +785,99 @@ inline double mg94_loglik(const Tree& tr, const Alignment& a, const MG94& m, dou
     std::vector<Mat> Pb(tr.n(), Mat::eye(a.code.S));
     for (int i = 0; i < tr.n(); ++i) if (i != tr.root) Pb[i] = m.P((bl ? (*bl)[i] : tr.bl[i]) * branch_scale);
     return loglik_from_P(tr, a, Pb, m.pi);
+}
+
+// ------------------------------------------------------------ nucleotide GTR
+// alignment.hpp:832-890 (to_nucleotide_alignment): per nucleotide site the IUPAC set of every taxon
+// is the pattern key; state = the unambiguous nucleotide (char_to_nuc) or -1, mask = the set; patterns
+// in first-occurrence order; the codon alignment's nucleotide frequencies are kept.
+inline Alignment nucleotide_patterns(const Alignment& a) {
+    Alignment r;
+    r.names = a.names; r.seqs = a.seqs; r.code = a.code; r.T = a.T; r.n_codons = 0;
+    std::copy(a.nuc_freq, a.nuc_freq + 4, r.nuc_freq);
+    const size_t L = a.seqs.empty() ? 0 : a.seqs[0].size();
+    std::map<std::string, int> seen;
+    std::string key(size_t(a.T), 'N');
+    for (size_t site = 0; site < L; ++site) {
+        for (int t = 0; t < a.T; ++t) key[size_t(t)] = char('A' + iupac_bits(a.seqs[size_t(t)][site]));
+        auto it = seen.find(key);
+        if (it == seen.end()) {
+            seen.emplace(key, r.P);
+            r.site_pattern.push_back(r.P++);
+            for (int t = 0; t < a.T; ++t) {
+                const char ch = a.seqs[size_t(t)][site];
+                r.states.push_back(int8_t(nuc_index(ch)));
+                r.masks.push_back(uint64_t(iupac_bits(ch)));
+            }
+            r.weights.push_back(1.0);
+        } else {
+            r.site_pattern.push_back(it->second);
+            r.weights[size_t(it->second)] += 1.0;
+        }
+    }
+    return r;
+}
+
+// rate_matrix.hpp:14-104: GTR with theta_AG = 1, Q normalised to mean rate 1, symmetric
+// eigensystem of diag(sqrt pi) Q diag(1 / sqrt pi) (pi floored at 1e-12), eigenvalues <= 0,
+// P(t) = U diag(e^{lambda t}) V clamped at 0
+struct GTR {
+    double pi[4] = {0.25, 0.25, 0.25, 0.25};
+    double scale = 1.0;
+    std::vector<double> lam;
+    Mat Q{4, 4}, U{4, 4}, V{4, 4};
+    void update(const double theta[5], const double freq[4]) {
+        const double AC = theta[0], AT = theta[1], CG = theta[2], CT = theta[3], GT = theta[4];
+        const double r[4][4] = {{0, AC, 1, AT}, {AC, 0, CG, CT}, {1, CG, 0, GT}, {AT, CT, GT, 0}};
+        double sq[4], isq[4];
+        for (int i = 0; i < 4; ++i) { pi[i] = freq[i]; sq[i] = std::sqrt(std::max(pi[i], 1e-12)); isq[i] = 1.0 / sq[i]; }
+        Q = Mat(4, 4);
+        for (int i = 0; i < 4; ++i) {
+            double row = 0;
+            for (int j = 0; j < 4; ++j) if (i != j) { Q(i, j) = r[i][j] * pi[j]; row += Q(i, j); }
+            Q(i, i) = -row;
+        }
+        double avg = 0;
+        for (int i = 0; i < 4; ++i) avg -= pi[i] * Q(i, i);
+        if (avg > 0) { scale = avg; for (auto& x : Q.a) x /= avg; }
+        Mat Sm(4, 4);
+        for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) Sm(i, j) = sq[i] * Q(i, j) * isq[j];
+        for (int i = 0; i < 4; ++i) for (int j = i + 1; j < 4; ++j) { const double m = 0.5 * (Sm(i, j) + Sm(j, i)); Sm(i, j) = m; Sm(j, i) = m; }
+        Mat E;
+        jacobi_eigen(Sm, lam, E);
+        for (auto& l : lam) l = std::min(l, 0.0);
+        for (int i = 0; i < 4; ++i) for (int k = 0; k < 4; ++k) { U(i, k) = isq[i] * E(i, k); V(k, i) = E(i, k) * sq[i]; }
+    }
+    Mat P(double t) const {
+        Mat out(4, 4);
+        for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) {
+            double x = 0;
+            for (int k = 0; k < 4; ++k) x += U(i, k) * std::exp(lam[k] * t) * V(k, j);
+            out(i, j) = std::max(x, 0.0);
+        }
+        return out;
+    }
+};
+
+// likelihood.hpp:181-254 (compute_gtr_log_likelihood): per pattern L = pi . D_root, weight x
+// (log L + scale) or weight x -1e20 when L <= 0, Neumaier sum over the patterns in order
+inline double gtr_loglik(const Tree& tr, const Alignment& nuc, const GTR& g, const std::vector<double>& bl,
+                         std::vector<double>* site = nullptr) {
+    std::vector<Mat> Pb(tr.n(), Mat::eye(4));
+    for (int i = 0; i < tr.n(); ++i) if (i != tr.root) Pb[i] = g.P(bl[i]);
+    const std::vector<double> pi(g.pi, g.pi + 4);
+    const auto l2t = leaf_map(tr, nuc);
+    std::vector<double> pl(size_t(nuc.P));
+    #pragma omp parallel num_threads(n_threads_for(nuc.P))
+    {
+        Pass w;
+        #pragma omp for schedule(static)
+        for (int p = 0; p < nuc.P; ++p) { inside_outside(tr, nuc, p, l2t, Pb, pi, 4, w, false); pl[size_t(p)] = w.logL; }
+    }
+    Neumaier acc;
+    for (int p = 0; p < nuc.P; ++p) acc.add(nuc.weights[size_t(p)] * pl[size_t(p)]);
+    if (site) *site = pl;
+    return acc.value();
 }
 
 // ------------------------------------------------ general mixture evaluation

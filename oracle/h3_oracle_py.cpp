@@ -160,6 +160,23 @@ PYBIND11_MODULE(h3oracle, m) {
        py::arg("is_test") = std::vector<bool>{}, py::arg("rates") = std::vector<double>{}, py::arg("rate_w") = std::vector<double>{},
        py::arg("branch_lengths") = std::vector<double>{}, py::arg("normalized_time") = false, py::arg("want_global") = false,
        py::arg("zero_l_sentinel") = false);
+    m.def("nucleotide_patterns", &nucleotide_patterns, py::arg("aln"));
+    m.def("gtr_matrix", [](const std::vector<double>& theta, const std::vector<double>& freq, double t) {
+        if (theta.size() != 5 || freq.size() != 4) throw std::runtime_error("theta needs 5 entries, freq 4");
+        GTR g; g.update(theta.data(), freq.data());
+        py::dict d; d["Q"] = mat_np(g.Q); d["P"] = mat_np(g.P(t)); d["lam"] = g.lam; d["scale"] = g.scale;
+        return d;
+    }, py::arg("theta"), py::arg("freq"), py::arg("t") = 0.0);
+    m.def("gtr_loglik", [](const Tree& t, const Alignment& nuc, const std::vector<double>& theta, const std::vector<double>& freq,
+                           std::vector<double> bl) {
+        if (theta.size() != 5 || freq.size() != 4) throw std::runtime_error("theta needs 5 entries, freq 4");
+        if (bl.empty()) bl = t.bl;
+        GTR g; g.update(theta.data(), freq.data());
+        std::vector<double> site;
+        double l;
+        { py::gil_scoped_release rel; l = gtr_loglik(t, nuc, g, bl, &site); }
+        return py::make_tuple(l, site);
+    }, py::arg("tree"), py::arg("nuc"), py::arg("theta"), py::arg("freq"), py::arg("branch_lengths") = std::vector<double>{});
     m.def("fel_run", [](const Tree& t, const Alignment& a, const py::dict& p, int max_patterns) {
         const Params pp = params_from(p);
         FelRun r;

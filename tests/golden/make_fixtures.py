@@ -87,6 +87,10 @@ def main(ref: str) -> None:
     known["cd2_meme"] = meme_case(ref_root, "cd2_meme_rel.json", "tests/test_meme.cpp:66-104", 0.95, 0.95, 0.95, 0.95)
     known["adh_meme"] = meme_case(ref_root, "adh_meme_rel.json", "tests/test_meme.cpp:106-144", 0.95, 0.92, 0.95, 0.95)
     known.update(fel_subset_cases(ref_root))
+    # HyPhy 2.5's nucleotide GTR fits (rates, frequencies, branch lengths, log-likelihood) recorded in the
+    # FEL ground truth of the reference's parity tests (tests/test_fel_multi_dataset.cpp:195-196)
+    known["cd2_gtr"] = gtr_case(ref_root, "cd2_fel.json", "cd2.fna")
+    known["adh_gtr"] = gtr_case(ref_root, "adh_fel.json", "adh.nex")
     (out / "known_answers.json").write_text(json.dumps(known, indent=1) + "\n")
 
 
@@ -129,6 +133,20 @@ def fel_subset_cases(ref_root: pathlib.Path) -> dict:
 def labelled_newick(topology: str, lengths: dict) -> str:
     """Attach ':length' to every named node of a HyPhy tree string (names only, no lengths)."""
     return re.sub(r"([A-Za-z_][A-Za-z0-9_]*)", lambda m: f"{m.group(1)}:{lengths[m.group(1)]!r}", topology) + ";"
+
+
+def gtr_case(ref_root: pathlib.Path, name: str, alignment: str) -> dict:
+    d = json.loads((ref_root / "benchmarks" / "ground_truth" / name).read_text())
+    g = d["fits"]["Nucleotide GTR"]
+    lengths = {k: v["Nucleotide GTR"] for k, v in d["branch attributes"]["0"].items()}
+    r = g["Rate Distributions"]
+    pairs = ["A to nucleotide C", "A to nucleotide T", "C to nucleotide G", "C to nucleotide T", "G to nucleotide T"]
+    return {
+        "source": f"benchmarks/ground_truth/{name} (HyPhy 2.5): fits / Nucleotide GTR and its branch lengths",
+        "alignment": alignment, "newick": labelled_newick(d["input"]["trees"]["0"], lengths),
+        "theta": [r[f"Substitution rate from nucleotide {x}"] for x in pairs],
+        "freqs": [x[0] for x in g["Equilibrium frequencies"]], "log_l": g["Log Likelihood"],
+    }
 
 
 def meme_case(ref_root: pathlib.Path, name: str, test_ref: str, r_lrt, rho_lrt, r_p, rho_p) -> dict:
