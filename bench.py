@@ -698,6 +698,117 @@ def run_compress(args) -> None:
     ctx.close()
 
 
+GTR_METRIC = "nucleotide GTR pattern x branch log-likelihood evaluations per second"
+GTR_WORKLOAD = ("LikelihoodEngine::compute_gtr_log_likelihood: the simulated 1024-taxon Yule alignment (5000 codons = "
+                "15000 nucleotide sites), its nucleotide patterns, GTR at the simulation's exchangeabilities")
+
+
+def run_gtr(args) -> None:
+    """h3g_nuc_eval_from_P on the nucleotide patterns of the 1024-taxon workload (value), the public
+    compute_gtr_log_likelihood from host objects (e2e), the oracle on the host's threads (CPU baseline)."""
+    import ctypes as C
+    import torch
+    import _hyphy3 as h
+    from hyphy3 import _capi
+    from hyphy3.simulate import make_workload
+    wl = make_workload(3)
+    aln = h.Alignment.from_sequences(wl.names, wl.seqs)
+    nuc = aln.to_nucleotide_alignment()
+    tree = h.Tree.from_newick(wl.newick)
+    gp = h.GTRParameters()
+    gp.theta_AC, gp.theta_AT, gp.theta_CG, gp.theta_CT, gp.theta_GT = wl.theta
+    g = h.GTRMatrix()
+    g.update(gp, list(nuc.nuc_frequencies))
+    stream = torch.cuda.current_stream()
+    ctx = _capi.Context(0, stream=stream.cuda_stream)
+    states, masks, weights = nuc.pattern_arrays()
+    l2t = h.build_leaf_to_taxon_map(tree, nuc)
+    n = tree.num_nodes()
+    is_leaf = np.array([nd.is_leaf for nd in tree.nodes], dtype=np.uint8)
+    pr = _capi.Problem(ctx, np.array(tree.parents, dtype=np.int32), is_leaf,
+                       np.array([l2t[i] if is_leaf[i] else -1 for i in range(n)], dtype=np.int32), states, masks, weights)
+    bl = tree.get_branch_lengths()
+    P = np.zeros((n, 4, 4))
+    for i in range(n):
+        if i != tree.root_id:
+            P[i] = g.transition_matrix(bl[i])
+    pi = np.ascontiguousarray(g.pi, dtype=np.float64)
+    lnl = C.c_double()
+    dp = C.POINTER(C.c_double)
+
+    def call():
+        ctx.check(ctx.lib.h3g_nuc_eval_from_P(pr.h, P.ctypes.data_as(dp), pi.ctypes.data_as(dp), C.byref(lnl), None))
+
+    warm = max(3, args.warmup)
+    for _ in range(warm):
+        call()
+    if args.profile:
+        call()
+        print(json.dumps({"profile": "gtr", "patterns": int(nuc.num_patterns), "lnl": lnl.value}), flush=True)
+        pr.close()
+        ctx.close()
+        return
+    steps = max(3, min(args.steps, 200))
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        call()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / steps
+    Pn, T, branches = int(nuc.num_patterns), int(nuc.num_taxa), n - 1
+    units = Pn * branches
+    # e2e: the public API from host objects (transition matrices built on the host, cached device problem)
+    e2e = []
+    for _ in range(min(steps, 10)):
+        t0 = time.perf_counter()
+        l_api, _site = h.compute_gtr_log_likelihood(tree, nuc, g)
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(e2e)
+    internal = sum(1 for nd in tree.nodes if not nd.is_leaf)
+    algo = Pn * (T * 1 + 2 * 36 * (internal - 1) + 8)                   # leaf states; partials parked and restored; site
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo / (ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        import h3oracle as o
+        threads = o.max_threads()
+        o.set_threads(threads)
+        onuc = o.nucleotide_patterns(o.Alignment.from_sequences(wl.names, wl.seqs))
+        ot = o.Tree.parse(wl.newick)
+        t0 = time.perf_counter()
+        l_ref, _ = o.gtr_loglik(ot, onuc, list(wl.theta), list(nuc.nuc_frequencies))
+        cs = time.perf_counter() - t0
+        cpu = {"value": units / cs, "unit": "pattern*branch/s", "cores": threads, "kind": "port",
+               "sample": f"the whole workload, {cs:.2f} s on {threads} threads (oracle restatement of likelihood.hpp:181-254); "
+                         f"lnL {l_ref:.6f} vs device {lnl.value:.6f}"}
+    line = {
+        "metric": GTR_METRIC, "value": units / (ms * 1e-3), "unit": "pattern*branch/s", "n_gpus": 1, "steps": steps,
+        "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": GTR_WORKLOAD, "taxa": T, "nucleotide_sites": int(nuc.num_nucleotides), "patterns": Pn,
+                   "branches": branches, "l2": "partial stack L2-resident; no flush"},
+        "e2e": {"value": units / e2e_s, "unit": "pattern*branch/s", "h2d_bytes_per_step": int(P.nbytes + 32),
+                "d2h_bytes_per_step": int(8 + 8 * Pn), "api": "_hyphy3.compute_gtr_log_likelihood(tree, nuc_aln, gtr)",
+                "timing": "host wall clock, median"},
+        "gpu_launches": 2 * steps, "lnl": lnl.value, "api_lnl": l_api,
+        "roofline": {"bound": "hbm", "kernel": "k_nuc_lnl", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get(("gtr", "k_nuc_lnl")),
+                     "traffic_unit": "bytes per launch, from ncu", "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "algorithmic_bytes": algo, "note": "the call (P upload, two kernels, lnL read back) timed as a whole"},
+        "cpu_baseline": cpu, "clocks": clocks,
+        "timing": "CUDA events on the launching stream around the timed calls",
+    }
+    print(json.dumps(line), flush=True)
+    pr.close()
+    ctx.close()
+
+
 def _mixed_available() -> bool:
     return os.environ.get("H3G_BENCH_PRECISION", "mixed") == "mixed"
 
@@ -789,11 +900,14 @@ def main() -> None:
     ap.add_argument("--config", type=int, choices=[1, 2, 3], default=1,
                     help="1: 64-taxon 3-omega mixture (headline); 2: FEL per-site fits, 256 taxa x 2000 codons; "
                          "3: 1024-taxon, 4 rate x 2 omega classes")
-    ap.add_argument("--analysis", choices=["fel", "meme", "compress"], default="fel",
-                    help="--config 2: which per-site analysis; compress: alignment finalize on the device (any config)")
+    ap.add_argument("--analysis", choices=["fel", "meme", "compress", "gtr"], default="fel",
+                    help="--config 2: which per-site analysis; compress: alignment finalize on the device; "
+                         "gtr: nucleotide GTR likelihood (both any config)")
     args = ap.parse_args()
     if args.analysis == "compress" and args.impl == "ours":
         run_compress(args)
+    elif args.analysis == "gtr" and args.impl == "ours":
+        run_gtr(args)
     elif args.config == 2 and args.impl == "ours":
         run_fel(args)
     elif args.profile:

@@ -11,6 +11,10 @@
 // rescaled by 2^256 when their maximum falls below 2^-256; L = pi . D_root, the site
 // log-likelihood log L - E ln 2, or the reference's -1e20 when L <= 0; the weighted sum
 // over patterns is a fixed-order Neumaier sum.  FP64 throughout.
+//
+// With fewer patterns than it takes to fill the GPU (kLevelBelow), the tree is walked
+// level by level instead: one launch per height, one thread per (internal node of the
+// level, pattern), partials stored per internal node.
 #include <algorithm>
 #include <cmath>
 #include <new>
@@ -31,7 +35,9 @@ int problem_max_state(h3g_problem* pr);
 namespace {
 
 constexpr int kNucT = 128;                                 // threads per block (patterns)
+constexpr int kLvlT = 256;
 constexpr int kSumT = 1024;
+constexpr int kLevelBelow = 131072;                        // patterns: below, the level-by-level walk
 
 struct NucState {
     int n_ev = 0, depth = 1, P = 0;
@@ -42,6 +48,11 @@ struct NucState {
     double* d_site = nullptr;                              // [P]
     double4* d_stk = nullptr;                              // [depth][Pp]
     int* d_exp = nullptr;                                  // [depth][Pp]
+    bool levels = false;                                   // level-by-level walk
+    std::vector<int> lv_off;                               // [H + 1] internal nodes by height
+    int* d_lv = nullptr;                                   // [NI]
+    double4* d_part = nullptr;                             // [NI][Pp]
+    int* d_pexp = nullptr;                                 // [NI][Pp]
     double* d_lnl = nullptr;
     double* h_pin = nullptr;                               // lnl read back
     std::vector<void*> owned;
@@ -121,6 +132,65 @@ __global__ void __launch_bounds__(kNucT) k_nuc_lnl(Topo t, const int* __restrict
     site[p] = L > 0.0 ? log(L) - double(E) * 0.69314718055994530942 : -1e20;
 }
 
+// leaf vector of taxon tx at pattern p (likelihood.hpp:54-87)
+__device__ __forceinline__ void nuc_leaf(const Topo& t, int tx, int p, double (&x)[4]) {
+    int st = -1;
+    uint64_t mk = 0xF;
+    if (tx >= 0) {
+        st = t.states[size_t(tx) * size_t(t.Pp) + p];
+        if (!(st >= 0 && st < 4)) mk = t.masks[size_t(tx) * size_t(t.Pp) + p];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        x[i] = (st >= 0 && st < 4) ? (i == st ? 1.0 : 0.0) : ((mk == 0 || (mk & 0xF) == 0xF || ((mk >> i) & 1)) ? 1.0 : 0.0);
+}
+
+// one thread per (internal node of this level, pattern): the product of the children's messages
+__global__ void __launch_bounds__(kLvlT) k_nuc_level(Topo t, const int* __restrict__ nodes, int cnt, const double* __restrict__ P,
+                                                      const double* __restrict__ pi, double4* __restrict__ part,
+                                                      int* __restrict__ pexp, double* __restrict__ site) {
+    pdl_enter();                                           // the lower levels' partials are complete
+    const int i = int(blockIdx.x) * kLvlT + int(threadIdx.x);
+    if (i >= cnt * t.P) return;
+    const int u = nodes[i / t.P], p = i - (i / t.P) * t.P;
+    const size_t Pp = size_t(t.Pp);
+    double d[4] = {1.0, 1.0, 1.0, 1.0};
+    int E = 0;
+    for (int e = t.ch_off[u]; e < t.ch_off[u + 1]; ++e) {
+        const int c = t.ch[e];
+        double x[4];
+        if (t.leaf[c]) {
+            nuc_leaf(t, t.taxon[c], p, x);
+        } else {
+            const size_t o = size_t(t.iidx[c]) * Pp + p;
+            const double4 v = part[o];
+            x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+            E += pexp[o];
+        }
+        const double* Pn = P + size_t(c) * 16;
+        double mx = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            d[k] *= __ldg(Pn + 4 * k) * x[0] + __ldg(Pn + 4 * k + 1) * x[1] + __ldg(Pn + 4 * k + 2) * x[2] +
+                    __ldg(Pn + 4 * k + 3) * x[3];
+            mx = fmax(mx, d[k]);
+        }
+        if (mx > 0.0 && mx < 0x1p-256) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) d[k] *= 0x1p256;
+            E += 256;
+        }
+    }
+    if (u == t.root) {
+        const double L = pi[0] * d[0] + pi[1] * d[1] + pi[2] * d[2] + pi[3] * d[3];
+        site[p] = L > 0.0 ? log(L) - double(E) * 0.69314718055994530942 : -1e20;
+    } else {
+        const size_t o = size_t(t.iidx[u]) * Pp + p;
+        part[o] = make_double4(d[0], d[1], d[2], d[3]);
+        pexp[o] = E;
+    }
+}
+
 // one block: weights x site log-likelihoods, Neumaier over contiguous chunks, then the chunk sums in order
 __global__ void __launch_bounds__(kSumT) k_nuc_sum(const double* __restrict__ site, const double* __restrict__ w, int P,
                                                    double* __restrict__ out) {
@@ -190,6 +260,26 @@ NucState* nuc_state(h3g_problem* pr, const FelProblemView& v, std::string* err) 
     s->depth = deepest;
     s->P = t.P;
     s->Pp = size_t(t.Pp);
+    s->levels = t.P < kLevelBelow;
+    std::vector<int> lv;
+    if (s->levels) {                                       // internal nodes by height, children first
+        std::vector<int> h(size_t(v.n), 0);
+        for (int e : ev)
+            if (!(e & 1)) {                                // a node closes after its descendants
+                const int u = e >> 1;
+                for (int c = v.ch_off[u]; c < v.ch_off[u + 1]; ++c) h[size_t(u)] = std::max(h[size_t(u)], h[size_t(v.ch[c])] + 1);
+            }
+        for (int c = v.ch_off[v.root]; c < v.ch_off[v.root + 1]; ++c) h[size_t(v.root)] = std::max(h[size_t(v.root)], h[size_t(v.ch[c])] + 1);
+        const int H = h[size_t(v.root)];
+        s->lv_off.assign(size_t(H) + 1, 0);
+        for (int u = 0; u < v.n; ++u)
+            if (!v.leaf[u]) ++s->lv_off[size_t(h[size_t(u)])];
+        for (int k = 1; k <= H; ++k) s->lv_off[size_t(k)] += s->lv_off[size_t(k) - 1];
+        lv.resize(size_t(s->lv_off[size_t(H)]));
+        std::vector<int> fill(s->lv_off.begin(), s->lv_off.end() - 1);
+        for (int u = 0; u < v.n; ++u)
+            if (!v.leaf[u]) lv[size_t(fill[size_t(h[size_t(u)]) - 1]++)] = u;
+    }
     auto take = [&](auto** p, size_t count) {
         void* q = nullptr;
         if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(**p)) != cudaSuccess) return false;
@@ -197,11 +287,15 @@ NucState* nuc_state(h3g_problem* pr, const FelProblemView& v, std::string* err) 
         *p = static_cast<std::remove_reference_t<decltype(*p)>>(q);
         return true;
     };
-    const bool ok = take(&s->d_ev, ev.size()) && take(&s->d_P, size_t(v.n) * 16) && take(&s->d_pi, 4) &&
-                    take(&s->d_site, size_t(std::max(t.P, 1))) && take(&s->d_stk, size_t(deepest) * s->Pp) &&
-                    take(&s->d_exp, size_t(deepest) * s->Pp) && take(&s->d_lnl, 1) &&
-                    cudaMallocHost(reinterpret_cast<void**>(&s->h_pin), sizeof(double)) == cudaSuccess &&
-                    cudaMemcpy(s->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+    bool ok = take(&s->d_ev, ev.size()) && take(&s->d_P, size_t(v.n) * 16) && take(&s->d_pi, 4) &&
+              take(&s->d_site, size_t(std::max(t.P, 1))) && take(&s->d_lnl, 1) &&
+              cudaMallocHost(reinterpret_cast<void**>(&s->h_pin), sizeof(double)) == cudaSuccess &&
+              cudaMemcpy(s->d_ev, ev.data(), ev.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok && s->levels)
+        ok = take(&s->d_lv, lv.size()) && take(&s->d_part, size_t(t.NI) * s->Pp) && take(&s->d_pexp, size_t(t.NI) * s->Pp) &&
+             cudaMemcpy(s->d_lv, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+    else if (ok)
+        ok = take(&s->d_stk, size_t(deepest) * s->Pp) && take(&s->d_exp, size_t(deepest) * s->Pp);
     if (!ok) {
         *err = "device allocation failed";
         delete s;
@@ -240,8 +334,18 @@ extern "C" h3g_status h3g_nuc_eval_from_P(h3g_problem* pr, const double* P, cons
     bool ok = cudaMemcpyAsync(s->d_P, P, size_t(v.n) * 16 * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess &&
               cudaMemcpyAsync(s->d_pi, pi, 4 * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess;
     if (ok && s->P > 0) {
-        launch_k(k_nuc_lnl, (s->P + kNucT - 1) / kNucT, kNucT, 0, st, t, static_cast<const int*>(s->d_ev), s->n_ev,
-                 static_cast<const double*>(s->d_P), static_cast<const double*>(s->d_pi), s->d_stk, s->d_exp, s->d_site);
+        if (s->levels) {
+            for (size_t k = 0; k + 1 < s->lv_off.size(); ++k) {
+                const int cnt = s->lv_off[k + 1] - s->lv_off[k];
+                if (cnt == 0) continue;
+                launch_k(k_nuc_level, int((size_t(cnt) * size_t(s->P) + kLvlT - 1) / kLvlT), kLvlT, 0, st, t,
+                         static_cast<const int*>(s->d_lv + s->lv_off[k]), cnt, static_cast<const double*>(s->d_P),
+                         static_cast<const double*>(s->d_pi), s->d_part, s->d_pexp, s->d_site);
+            }
+        } else {
+            launch_k(k_nuc_lnl, (s->P + kNucT - 1) / kNucT, kNucT, 0, st, t, static_cast<const int*>(s->d_ev), s->n_ev,
+                     static_cast<const double*>(s->d_P), static_cast<const double*>(s->d_pi), s->d_stk, s->d_exp, s->d_site);
+        }
         launch_k(k_nuc_sum, 1, kSumT, 0, st, static_cast<const double*>(s->d_site), t.w, s->P, s->d_lnl);
     }
     ok = ok && cudaGetLastError() == cudaSuccess &&

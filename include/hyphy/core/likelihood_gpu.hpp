@@ -16,7 +16,9 @@
 #pragma once
 
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
+#include <unordered_map>
 #include <list>
 #include <memory>
 #include <stdexcept>
@@ -149,11 +151,18 @@ public:
                 const auto& sp = aln.patterns[size_t(p)];
                 uint64_t& l = lane[p & 3];
                 l = fnv(l, sp.states.data(), sp.states.size());
-                for (size_t t = 0; t < sp.states.size(); ++t)
-                    if (sp.states[t] < 0) {
-                        const uint64_t m = t < sp.ambiguous_masks.size() ? sp.ambiguous_masks[t] : 0;
-                        l = fnv(l, &m, 8);
-                    }
+                const size_t nt = sp.states.size();
+                for (size_t t0 = 0; t0 < nt; t0 += 8) {     // eight states at a time: any unresolved (sign bit)?
+                    uint64_t w = 0;
+                    const size_t k = std::min<size_t>(8, nt - t0);
+                    std::memcpy(&w, sp.states.data() + t0, k);
+                    if (!(w & 0x8080808080808080ull)) continue;
+                    for (size_t t = t0; t < t0 + k; ++t)
+                        if (sp.states[t] < 0) {
+                            const uint64_t m = t < sp.ambiguous_masks.size() ? sp.ambiguous_masks[t] : 0;
+                            l = fnv(l, &m, 8);
+                        }
+                }
                 const double wt = double(sp.weight);
                 l = fnv(l, &wt, 8);
             }
@@ -242,10 +251,18 @@ public:
     static std::vector<size_t> build_leaf_to_taxon_map(const Tree& tree, const Alignment& aln) {
         std::vector<size_t> m(tree.num_nodes(), size_t(-1));
         size_t leaves = 0, hit = 0;
+        // exact names through a hash map (the first taxon of each name, as the linear search finds);
+        // the case-insensitive and prefix rules of Alignment::taxon_index for the rest
+        std::unordered_map<std::string, size_t> exact;
+        exact.reserve(aln.taxon_names.size());
+        for (size_t i = 0; i < aln.taxon_names.size(); ++i) exact.emplace(aln.taxon_names[i], i);
         for (const auto& nd : tree.nodes) {
             if (!nd.is_leaf) continue;
             ++leaves;
-            m[size_t(nd.id)] = aln.taxon_index(nd.name);
+            std::string nm = nd.name;
+            if (nm.size() >= 2 && (nm.front() == '\'' || nm.front() == '"') && nm.back() == nm.front()) nm = nm.substr(1, nm.size() - 2);
+            const auto it = exact.find(nm);
+            m[size_t(nd.id)] = it != exact.end() ? it->second : aln.taxon_index(nd.name);
             if (m[size_t(nd.id)] != size_t(-1)) ++hit;
         }
         if (leaves > 0 && hit == 0)

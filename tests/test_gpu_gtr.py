@@ -88,3 +88,16 @@ def test_gtr_rejects_codon_problem():
         pr.close()
     finally:
         c.close()
+
+
+def test_gtr_many_patterns_depth_first_path(oracle):
+    """More patterns than the level-by-level walk takes (131072): the depth-first, thread-per-pattern kernel."""
+    rng = np.random.default_rng(9)
+    n = 16
+    names = [f"t{i}" for i in range(n)]
+    newick = "(" + ",".join(f"({names[2 * i]}:0.1,{names[2 * i + 1]}:0.2):0.05" for i in range(n // 2)) + ");"
+    cols = 141000                                                   # a multiple of 3; almost every column distinct
+    seqs = ["".join(rng.choice(np.array(list("ACGTRN-")), cols, p=[0.24, 0.24, 0.24, 0.24, 0.02, 0.01, 0.01]))
+            for _ in range(n)]
+    a = _check_synthetic(oracle, names, seqs, newick, [0.9, 0.4, 0.6, 2.5, 0.8], [0.3, 0.2, 0.2, 0.3])
+    assert a.num_patterns >= 131072
