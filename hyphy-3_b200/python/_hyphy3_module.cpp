@@ -179,6 +179,31 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("scale_factor", &hyphy::core::GTRMatrix::scale_factor)
         .def_readonly("pi", &hyphy::core::GTRMatrix::pi)
         .def_readonly("eigenvalues", &hyphy::core::GTRMatrix::eigenvalues);
+    py::class_<hyphy::opt::GTRFitResult>(m, "GTRFitResult")
+        .def_readonly("log_likelihood", &hyphy::opt::GTRFitResult::log_likelihood)
+        .def_readonly("aicc", &hyphy::opt::GTRFitResult::aicc)
+        .def_readonly("params", &hyphy::opt::GTRFitResult::params)
+        .def_readonly("tree", &hyphy::opt::GTRFitResult::tree)
+        .def_readonly("iterations", &hyphy::opt::GTRFitResult::iterations)
+        .def_readonly("converged", &hyphy::opt::GTRFitResult::converged);
+    py::class_<hyphy::opt::GTRFitter>(m, "GTRFitter")
+        .def(py::init([](Tree t, const Alignment& a) { return hyphy::opt::GTRFitter(std::move(t), a); }), "tree"_a, "alignment"_a)
+        .def("fit", [](hyphy::opt::GTRFitter& f, int max_iters, Scalar tol) {
+                 py::gil_scoped_release rel;
+                 return f.fit(max_iters, tol);
+             }, "max_iters"_a = 500, "tolerance"_a = 1e-5)
+        .def_readonly("nuc_aln", &hyphy::opt::GTRFitter::nuc_aln);
+    m.def("compute_gtr_gradients", [](const Tree& tree, const Alignment& aln, const hyphy::core::GTRParameters& p,
+                                      const std::vector<Scalar>& bl) {
+        hyphy::core::LikelihoodEngine::GTRGradients r;
+        {
+            py::gil_scoped_release rel;
+            r = LikelihoodEngine::compute_gtr_gradients(tree, aln, p, bl);
+        }
+        return py::make_tuple(r.log_likelihood, r.grad_branches,
+                              std::vector<Scalar>(r.grad_theta.begin(), r.grad_theta.end()));
+    }, "tree"_a, "alignment"_a, "params"_a, "branch_lengths"_a = std::vector<Scalar>{},
+       "GTR lnL, d lnL / d t per node and d lnL / d theta (AC AT CG CT GT) on the device");
     m.def("compute_gtr_log_likelihood", [](const Tree& tree, const Alignment& aln, const hyphy::core::GTRMatrix& g) {
         std::vector<Scalar> site;
         Scalar l;

@@ -17,6 +17,7 @@
 
 #include <cstdlib>
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <unordered_map>
 #include <list>
@@ -480,6 +481,74 @@ public:
         for (const auto& nd : tree.nodes)
             if (nd.id != tree.root_id) Pb[size_t(nd.id)] = mg94.transition_matrix(nd.branch_length * branch_scale);
         return compute_tree_log_likelihood_from_P(tree, aln, Pb, mg94.pi, S, custom_leaf_to_taxon);
+    }
+
+    // The GTR log-likelihood with its gradient in every branch length and the five exchangeabilities
+    // (theta_AG = 1), for fitting: the device's joint-gradient engine on the 4-state problem, FP64.
+    // P = exp(Q_norm t) with Q_norm = Q / mu (rate_matrix.hpp:70-78) is the engine's normalised time
+    // exp(Q (t / 3) 3 / mu), so the raw generator, its eigensystem and mu are installed with lengths
+    // t / 3; directions dQ / d theta carry the d mu term.  branch_lengths per node (the root's ignored).
+    struct GTRGradients {
+        Scalar log_likelihood = 0.0;
+        std::vector<Scalar> grad_branches;          // d lnL / d t, per node
+        std::array<Scalar, 5> grad_theta{};         // AC AT CG CT GT
+    };
+    static GTRGradients compute_gtr_gradients(const Tree& tree, const Alignment& aln, const GTRParameters& params,
+                                              const std::vector<Scalar>& branch_lengths,
+                                              const std::vector<size_t>* custom_leaf_to_taxon = nullptr) {
+        if (aln.num_codons != 0) {
+            const Alignment nuc = aln.to_nucleotide_alignment();
+            return compute_gtr_gradients(tree, nuc, params, branch_lengths, custom_leaf_to_taxon);
+        }
+        auto& eng = gpu_detail::Engine::get();
+        std::vector<size_t> local;
+        const auto& l2t = custom_leaf_to_taxon ? *custom_leaf_to_taxon : (local = build_leaf_to_taxon_map(tree, aln));
+        h3g_problem* pr = eng.problem(tree, aln, l2t);
+        const size_t n = tree.num_nodes();
+        GTRMatrix g;
+        g.update(params, aln.nuc_frequencies);
+        const double mu = g.scale_factor;
+        std::vector<double> Q(16), lam(4), U(16), V(16), dQ(5 * 16, 0.0);
+        for (int i = 0; i < 4; ++i) {
+            lam[size_t(i)] = g.eigenvalues[size_t(i)] * mu;
+            for (int j = 0; j < 4; ++j) {
+                Q[size_t(i) * 4 + j] = g.Q(i, j) * mu;
+                U[size_t(i) * 4 + j] = g.U_pi(i, j);
+                V[size_t(i) * 4 + j] = g.V_pi(i, j);
+            }
+        }
+        static const int pairs[5][2] = {{0, 1}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+        for (int x = 0; x < 5; ++x) {
+            const int a = pairs[x][0], b = pairs[x][1];
+            double* d = dQ.data() + size_t(x) * 16;
+            d[a * 4 + b] = aln.nuc_frequencies[b];
+            d[b * 4 + a] = aln.nuc_frequencies[a];
+            d[a * 4 + a] = -aln.nuc_frequencies[b];
+            d[b * 4 + b] = -aln.nuc_frequencies[a];
+        }
+        const double one = 1.0;
+        h3g_model_desc d{};
+        d.S = 4; d.pi = aln.nuc_frequencies; d.n_models = 1;
+        d.Q = Q.data(); d.lam = lam.data(); d.U = U.data(); d.V = V.data(); d.mu = &mu;
+        d.K = 1; d.class_w = &one; d.has_bg = 0; d.is_test = nullptr;
+        d.M = 1; d.rates = &one; d.rate_w = &one; d.time_mode = H3G_TIME_NORMALIZED;
+        d.n_dirs = 5; d.dQ = dQ.data(); d.precision = H3G_PREC_FP64; d.zero_l_sentinel = 1;
+        eng.set_installed(pr, 0);
+        eng.check(h3g_model_set(pr, &d));
+        std::vector<double> bl(n, 0.0);
+        for (const auto& nd : tree.nodes)
+            if (nd.id != tree.root_id) bl[size_t(nd.id)] = (branch_lengths.empty() ? nd.branch_length : branch_lengths[size_t(nd.id)]) / 3.0;
+        GTRGradients res;
+        res.grad_branches.assign(n, 0.0);
+        std::vector<double> gd(5, 0.0);
+        h3g_result r{};
+        r.grad_t = res.grad_branches.data();
+        r.grad_dir = gd.data();
+        eng.check(h3g_eval(pr, bl.data(), H3G_WANT_LNL | H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL, &r));
+        res.log_likelihood = r.lnl;
+        for (auto& x : res.grad_branches) x /= 3.0;
+        for (int x = 0; x < 5; ++x) res.grad_theta[size_t(x)] = gd[size_t(x)];
+        return res;
     }
 
     // likelihood.hpp:181-254: the GTR log-likelihood of a nucleotide alignment (as from

@@ -309,4 +309,151 @@ public:
     }
 };
 
+// opt/nelder_mead.hpp:15-108 (Brent1D::minimize): Brent's parabolic interpolation with golden-section
+// steps on [a, c] from x = b, minimising f; returns (x, f(x))
+template <class F>
+inline std::pair<Scalar, Scalar> brent_minimize(F&& f, Scalar a, Scalar b, Scalar c, Scalar tol, int max_iter) {
+    const Scalar CGOLD = 0.3819660, ZEPS = 1e-10;
+    Scalar x = b, w = b, v = b, e = 0.0, d = 0.0;
+    Scalar fx = f(x), fw = fx, fv = fx;
+    Scalar lo = std::min(a, c), hi = std::max(a, c);
+    for (int iter = 0; iter < max_iter; ++iter) {
+        const Scalar xm = 0.5 * (lo + hi), tol1 = tol * std::fabs(x) + ZEPS, tol2 = 2.0 * tol1;
+        if (std::fabs(x - xm) <= tol2 - 0.5 * (hi - lo)) break;
+        if (std::fabs(e) > tol1) {
+            Scalar r = (x - w) * (fx - fv), q = (x - v) * (fx - fw), pp = (x - v) * q - (x - w) * r;
+            q = 2.0 * (q - r);
+            if (q > 0.0) pp = -pp;
+            q = std::fabs(q);
+            const Scalar etemp = e;
+            e = d;
+            if (std::fabs(pp) >= std::fabs(0.5 * q * etemp) || pp <= q * (lo - x) || pp >= q * (hi - x)) {
+                e = x >= xm ? lo - x : hi - x;
+                d = CGOLD * e;
+            } else {
+                d = pp / q;
+                const Scalar u = x + d;
+                if (u - lo < tol2 || hi - u < tol2) d = xm - x >= 0.0 ? std::fabs(tol1) : -std::fabs(tol1);
+            }
+        } else {
+            e = x >= xm ? lo - x : hi - x;
+            d = CGOLD * e;
+        }
+        const Scalar u = std::fabs(d) >= tol1 ? x + d : x + (d >= 0.0 ? std::fabs(tol1) : -std::fabs(tol1));
+        const Scalar fu = f(u);
+        if (fu <= fx) {
+            if (u >= x) lo = x; else hi = x;
+            v = w; fv = fw; w = x; fw = fx; x = u; fx = fu;
+        } else {
+            if (u < x) lo = u; else hi = u;
+            if (fu <= fw || w == x) { v = w; fv = fw; w = u; fw = fu; }
+            else if (fu <= fv || v == x || v == w) { v = u; fv = fu; }
+        }
+    }
+    return {x, fx};
+}
+
+struct GTRFitResult {
+    Scalar log_likelihood = 0.0;
+    Scalar aicc = 0.0;
+    hyphy::core::GTRParameters params;
+    Tree tree;
+    int iterations = 0;
+    bool converged = false;
+};
+
+// GTRFitter (optimizer.hpp:33-200): the nucleotide GTR model (five exchangeabilities, every branch
+// length) on the alignment's nucleotide patterns.  Same start as the reference: rates (0.5, 0.3, 0.5,
+// 1.0, 0.3), branches shorter than 1e-4 set to 0.05, then the global tree scale by Brent on
+// [0.01, 50] (tol 1e-2, 12 iterations).  The reference then alternates coordinate-wise Brent
+// searches of the rates with a branch sweep over cavity vectors; here the rates and the branch lengths
+// are fitted jointly by the bounded L-BFGS of this header on their log scale, with the objective and
+// gradient from the device (compute_gtr_gradients).  Same maximum, different path.  AICc with
+// K = 5 + branches and N = nucleotide sites (stats.hpp:114-121).
+class GTRFitter {
+public:
+    Tree tree;
+    Alignment aln;
+    Alignment nuc_aln;
+
+    GTRFitter(Tree t, const Alignment& a) : tree(std::move(t)), aln(a), nuc_aln(a.to_nucleotide_alignment()) {}
+
+    GTRFitResult fit(int max_iters = 500, Scalar tolerance = 1e-5) {
+        std::vector<int32_t> br;
+        for (const auto& nd : tree.nodes)
+            if (nd.id != tree.root_id && nd.parent_id != hyphy::core::INVALID_INDEX) br.push_back(nd.id);
+        const size_t B = br.size(), n = tree.num_nodes();
+        hyphy::core::GTRParameters p;
+        p.theta_AC = 0.5; p.theta_AT = 0.3; p.theta_CG = 0.5; p.theta_CT = 1.0; p.theta_GT = 0.3;
+        Tree cur = tree;
+        for (int32_t id : br)
+            if (cur.nodes[size_t(id)].branch_length < 1e-4) cur.nodes[size_t(id)].branch_length = 0.05;
+        const auto l2t = LikelihoodEngine::build_leaf_to_taxon_map(cur, nuc_aln);
+        auto lengths = [&](Scalar scale) {
+            std::vector<Scalar> bl(n, 0.0);
+            for (int32_t id : br) bl[size_t(id)] = cur.nodes[size_t(id)].branch_length * scale;
+            return bl;
+        };
+        hyphy::core::GTRMatrix g;
+        auto lnl_at = [&](const std::vector<Scalar>& bl, const hyphy::core::GTRParameters& q) {
+            g.update(q, nuc_aln.nuc_frequencies);
+            Tree t = cur;
+            for (int32_t id : br) t.nodes[size_t(id)].branch_length = bl[size_t(id)];
+            return LikelihoodEngine::compute_gtr_log_likelihood(t, nuc_aln, g, &l2t);
+        };
+        // stage 1: global tree scale (optimizer.hpp:85-100)
+        const auto sc = brent_minimize([&](Scalar s) { return -lnl_at(lengths(s), p); }, 0.01, 1.0, 50.0, 1e-2, 12);
+        for (int32_t id : br) cur.nodes[size_t(id)].branch_length *= sc.first;
+        // stage 2: rates and branch lengths jointly, log scale, the reference's bounds
+        const size_t dim = B + 5;
+        std::vector<Scalar> x(dim), lb(dim), ub(dim);
+        for (size_t i = 0; i < B; ++i) {
+            x[i] = std::log(std::clamp(cur.nodes[size_t(br[i])].branch_length, 1e-6, 50.0));
+            lb[i] = std::log(1e-6);
+            ub[i] = std::log(50.0);
+        }
+        const std::array<Scalar, 5> th0 = {p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT};
+        for (size_t k = 0; k < 5; ++k) {
+            x[B + k] = std::log(th0[k]);
+            lb[B + k] = std::log(1e-4);
+            ub[B + k] = std::log(100.0);
+        }
+        auto params_of = [&](const std::vector<Scalar>& y) {
+            hyphy::core::GTRParameters q;
+            q.theta_AC = std::exp(y[B]); q.theta_AT = std::exp(y[B + 1]); q.theta_CG = std::exp(y[B + 2]);
+            q.theta_CT = std::exp(y[B + 3]); q.theta_GT = std::exp(y[B + 4]);
+            return q;
+        };
+        Scalar best_f = std::numeric_limits<Scalar>::infinity();
+        std::vector<Scalar> best_x = x;
+        auto fg = [&](const std::vector<Scalar>& y, std::vector<Scalar>& gr) -> Scalar {
+            std::vector<Scalar> bl(n, 0.0);
+            for (size_t i = 0; i < B; ++i) bl[size_t(br[i])] = std::exp(y[i]);
+            const auto q = params_of(y);
+            const auto r = LikelihoodEngine::compute_gtr_gradients(cur, nuc_aln, q, bl, &l2t);
+            gr.assign(y.size(), 0.0);
+            for (size_t i = 0; i < B; ++i) gr[i] = -bl[size_t(br[i])] * r.grad_branches[size_t(br[i])];
+            const std::array<Scalar, 5> th = {q.theta_AC, q.theta_AT, q.theta_CG, q.theta_CT, q.theta_GT};
+            for (size_t k = 0; k < 5; ++k) gr[B + k] = -th[k] * r.grad_theta[k];
+            const Scalar fx = -r.log_likelihood;
+            if (std::isfinite(fx) && fx < best_f) { best_f = fx; best_x = y; }
+            return fx;
+        };
+        BoxLBFGSResult sol = box_lbfgs(fg, x, lb, ub, tolerance, std::max<int>(max_iters, int(5 * B + 60)));
+        Scalar fx = sol.f;
+        x = sol.x;
+        if (std::isfinite(best_f) && (!std::isfinite(fx) || best_f < fx)) { x = best_x; fx = best_f; }
+        for (size_t i = 0; i < B; ++i) cur.nodes[size_t(br[i])].branch_length = std::exp(x[i]);
+        GTRFitResult res;
+        res.params = params_of(x);
+        res.tree = cur;
+        res.log_likelihood = lnl_at(lengths(1.0), res.params);
+        res.iterations = sol.iterations;
+        res.converged = sol.converged || sol.pg_inf <= std::max<Scalar>(tolerance, 1e-3);
+        const Scalar K = Scalar(5 + B), N = Scalar(nuc_aln.num_nucleotides);
+        res.aicc = N > K + 1.0 ? -2.0 * res.log_likelihood + 2.0 * K * N / (N - K - 1.0) : -2.0 * res.log_likelihood + 2.0 * K;
+        return res;
+    }
+};
+
 }  // namespace hyphy::opt
