@@ -97,12 +97,13 @@ PYBIND11_MODULE(_hyphy3, m) {
 
     py::class_<Alignment>(m, "Alignment")
         .def(py::init<>())
-        .def_static("load", [](const std::string& f, bool device) {
-            if (!device) return Alignment::load(f);
+        .def_static("load", [](const std::string& f, bool device, std::optional<std::string> code) {
+            const auto gc = code ? GeneticCode::from_name(*code) : nullptr;
+            if (!device) return Alignment::load(f, gc);
             Alignment a = Alignment::load_unfinalized(f);
-            hyphy::core::finalize_on_device(a);
+            hyphy::core::finalize_on_device(a, gc);
             return a;
-        }, "filepath"_a, "device"_a = false)
+        }, "filepath"_a, "device"_a = false, "genetic_code"_a = std::nullopt)
         .def_static("from_fasta", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
         .def_static("from_nexus", [](const std::string& f) { return Alignment::load(f); }, "filepath"_a)
         .def_static("from_text", [](const std::string& s) { return Alignment::from_text(s); }, "text"_a)
@@ -376,6 +377,26 @@ PYBIND11_MODULE(_hyphy3, m) {
                  return FELAnalyzer(std::move(tree), std::move(aln), params, settings, bg_om);
              }),
              "tree"_a, "alignment"_a, "params"_a = MG94Parameters{}, "settings"_a = FELSettings{}, "background_omega"_a = -1.0)
+        .def_static("create_and_fit", [](Tree tree, Alignment aln, const FELSettings& settings) {
+                        py::gil_scoped_release rel;
+                        return FELAnalyzer::create_and_fit(std::move(tree), std::move(aln), settings);
+                    }, "tree"_a, "alignment"_a, "settings"_a = FELSettings{})
+        .def_static("create_and_fit", [](Tree tree, Alignment aln, Scalar pvalue_threshold, bool full_model) {
+                        py::gil_scoped_release rel;
+                        return FELAnalyzer::create_and_fit(std::move(tree), std::move(aln), pvalue_threshold, nullptr, full_model);
+                    }, "tree"_a, "alignment"_a, "pvalue_threshold"_a = 0.1, "full_model"_a = true)
+        .def_readonly("base_params", &FELAnalyzer::base_params)
+        .def_readonly("settings", &FELAnalyzer::settings)
+        .def_readonly("p_value_threshold", &FELAnalyzer::p_value_threshold)
+        .def_readonly("background_omega", &FELAnalyzer::background_omega)
+        .def_readonly("global_log_l", &FELAnalyzer::global_log_l)
+        .def_readonly("global_aicc", &FELAnalyzer::global_aicc)
+        .def_readonly("has_gtr_fit", &FELAnalyzer::has_gtr_fit)
+        .def_readonly("gtr_log_l", &FELAnalyzer::gtr_log_l)
+        .def_readonly("gtr_aicc", &FELAnalyzer::gtr_aicc)
+        .def_readonly("gtr_rates", &FELAnalyzer::gtr_rates)
+        .def_readonly("gtr_branch_lengths", &FELAnalyzer::gtr_branch_lengths)
+        .def_readonly("full_model", &FELAnalyzer::full_model)
         .def_readonly("is_test_branch", &FELAnalyzer::is_test_branch)
         .def_readonly("test_branch_names", &FELAnalyzer::test_branch_names)
         .def_readonly("bg_branch_names", &FELAnalyzer::bg_branch_names)
@@ -460,6 +481,20 @@ PYBIND11_MODULE(_hyphy3, m) {
                  return MEMEAnalyzer(std::move(tree), std::move(aln), params, std::move(branches));
              }),
              "tree"_a, "alignment"_a, "params"_a = MG94Parameters{}, "branches"_a = "All")
+        .def_static("create_and_fit", [](Tree tree, Alignment aln, Scalar pvalue_threshold, bool full_model, std::string branches) {
+                        py::gil_scoped_release rel;
+                        return MEMEAnalyzer::create_and_fit(std::move(tree), std::move(aln), pvalue_threshold, nullptr, full_model,
+                                                            std::move(branches));
+                    }, "tree"_a, "alignment"_a, "pvalue_threshold"_a = 0.1, "full_model"_a = true, "branches"_a = "All")
+        .def_readonly("base_params", &MEMEAnalyzer::base_params)
+        .def_readonly("tree", &MEMEAnalyzer::tree)
+        .def_readonly("global_log_l", &MEMEAnalyzer::global_log_l)
+        .def_readonly("global_aicc", &MEMEAnalyzer::global_aicc)
+        .def_readonly("has_gtr_fit", &MEMEAnalyzer::has_gtr_fit)
+        .def_readonly("gtr_log_l", &MEMEAnalyzer::gtr_log_l)
+        .def_readonly("gtr_aicc", &MEMEAnalyzer::gtr_aicc)
+        .def_readonly("gtr_rates", &MEMEAnalyzer::gtr_rates)
+        .def_readonly("gtr_branch_lengths", &MEMEAnalyzer::gtr_branch_lengths)
         .def("run", [](MEMEAnalyzer& f, bool show_progress, bool force_progress) {
                  py::gil_scoped_release rel;
                  return f.run(show_progress, force_progress);

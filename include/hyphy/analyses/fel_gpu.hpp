@@ -8,15 +8,20 @@
 // chosen as in the reference (Tree::select_branches with {T}-tag detection,
 // fel.hpp:215-227); with a background set every pattern runs the reference's
 // branch-subset search (fel.hpp:462-572) through h3g_fel_run_tested.
+// create_and_fit (fel.hpp:145-214) fits the nucleotide GTR model, then the
+// global MG94 model from its rates, both on the device, before FEL.
 // Ancestral substitution summaries (SiteResult::subs in the reference) and
 // bridge resolutions are not produced.
 #pragma once
 
+#include <functional>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../core/likelihood_gpu.hpp"
+#include "../opt/optimizer_gpu.hpp"
 
 namespace hyphy::analyses {
 
@@ -60,7 +65,17 @@ public:
     Scalar baseline_tested_tree_length = 0.0;
     Scalar baseline_bg_tree_length = 0.0;
     Scalar conversion_factor = 1.0;
+    Scalar global_log_l = 0.0;
+    Scalar global_aicc = 0.0;
     std::vector<SiteResult> site_results;
+
+    // the nucleotide GTR fit create_and_fit starts from
+    bool has_gtr_fit = false;
+    Scalar gtr_log_l = 0.0;
+    Scalar gtr_aicc = 0.0;
+    hyphy::core::GTRParameters gtr_rates;
+    std::unordered_map<std::string, Scalar> gtr_branch_lengths;
+    bool full_model = true;
 
     // branch partition (fel.hpp:215-227)
     std::vector<bool> is_test_branch;
@@ -73,7 +88,58 @@ public:
     FELAnalyzer(Tree t, Alignment a, MG94Parameters params = MG94Parameters{}, FELSettings s = FELSettings{}, Scalar bg_om = -1.0)
         : tree(std::move(t)), aln(std::move(a)), base_params(params), settings(std::move(s)), background_omega(bg_om) {
         p_value_threshold = settings.p_value_threshold;
+        full_model = settings.full_model;
         prepare_branch_lengths();
+    }
+
+    // fel.hpp:145-201: GTR fit, then the global MG94 fit from its rates (every branch, omega and, with a
+    // tested / background split, the background omega; or omega and a tree scale when !full_model), then
+    // the analyzer on that tree.  AICc of the MG94 fit: K = 5 + (2 omegas with a split, else 1) + branches,
+    // N = codons.
+    static FELAnalyzer create_and_fit(Tree input_tree, Alignment aln, FELSettings settings = FELSettings{},
+                                      std::function<void(const std::string&, double)> progress_cb = nullptr) {
+        if (progress_cb) progress_cb("Phase 1: Fitting Nucleotide GTR Model", 0.1);
+        hyphy::opt::GTRFitter gtr_fitter(input_tree, aln);
+        const auto gtr = gtr_fitter.fit();
+        if (progress_cb) progress_cb("Phase 2: Refining under Global MG94 Model", 0.3);
+        MG94Parameters p;
+        p.theta_AC = gtr.params.theta_AC; p.theta_AT = gtr.params.theta_AT; p.theta_CG = gtr.params.theta_CG;
+        p.theta_CT = gtr.params.theta_CT; p.theta_GT = gtr.params.theta_GT;
+        const auto sel = gtr.tree.select_branches(settings.test_branches, settings.test_branch_regex, settings.test_branch_names, true);
+        const bool split = sel.num_selected > 0 && sel.num_unselected > 0;
+        hyphy::opt::MG94Fitter mg(gtr.tree, aln);
+        hyphy::opt::FitResult fit;
+        Scalar bg_om = -1.0;
+        if (settings.full_model) {
+            fit = mg.fit_full_model(1.0, p, progress_cb, 250, 1e-5, split ? &sel.is_selected : nullptr, split ? &bg_om : nullptr);
+            p = fit.params;
+        } else {
+            fit = mg.fit_omega_and_scale(1.0, p);
+            p.alpha = 1.0;
+            p.beta = fit.x_opt[0];
+            bg_om = p.beta;
+        }
+        FELAnalyzer out(fit.tree, std::move(aln), p, settings, bg_om);
+        out.global_log_l = fit.log_likelihood;
+        out.global_aicc = hyphy::opt::compute_aicc(fit.log_likelihood, 5 + (split ? 2 : 1) + (fit.tree.num_nodes() - 1),
+                                                   out.aln.num_codons);
+        out.has_gtr_fit = true;
+        out.gtr_log_l = gtr.log_likelihood;
+        out.gtr_aicc = gtr.aicc;
+        out.gtr_rates = gtr.params;
+        for (const auto& nd : gtr.tree.nodes)
+            if (nd.id != gtr.tree.root_id) out.gtr_branch_lengths[nd.name] = nd.branch_length;
+        return out;
+    }
+
+    // fel.hpp:203-214
+    static FELAnalyzer create_and_fit(Tree input_tree, Alignment aln, Scalar pvalue_threshold,
+                                      std::function<void(const std::string&, double)> progress_cb = nullptr,
+                                      bool full_model = true) {
+        FELSettings s;
+        s.p_value_threshold = pvalue_threshold;
+        s.full_model = full_model;
+        return create_and_fit(std::move(input_tree), std::move(aln), s, std::move(progress_cb));
     }
 
     void partition_branches() {

@@ -9,13 +9,16 @@
 // (meme.hpp:634-676).  The tested branches follow the reference
 // (meme.hpp:84-92): MEME's own set by Tree::select_branches without tag
 // detection, its FEL baseline's with detection; with a background set the
-// search frees beta_bg (h3g_meme_run_tested).  create_and_fit (nucleotide GTR
-// fit first), bridge resolutions and the ancestral substitution summaries
+// search frees beta_bg (h3g_meme_run_tested).  create_and_fit (meme.hpp:95-148)
+// fits the nucleotide GTR model, then the global MG94 model, on the device.
+// Bridge resolutions and the ancestral substitution summaries
 // (MEMESiteResult::subs) are not provided.
 #pragma once
 
+#include <functional>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "fel_gpu.hpp"
@@ -53,7 +56,13 @@ public:
     Scalar baseline_tree_length = 0.0;
     Scalar conversion_factor = 1.0;
     Scalar global_log_l = 0.0;
+    Scalar global_aicc = 0.0;
     std::vector<MEMESiteResult> site_results;
+    bool has_gtr_fit = false;
+    Scalar gtr_log_l = 0.0;
+    Scalar gtr_aicc = 0.0;
+    hyphy::core::GTRParameters gtr_rates;
+    std::unordered_map<std::string, Scalar> gtr_branch_lengths;
     std::string test_branches = "All";
     size_t num_tested = 0;
     size_t num_background = 0;
@@ -64,6 +73,46 @@ public:
         : tree(t), aln(std::move(a)), base_params(params), fel_analyzer(t, aln, params), test_branches(std::move(branches_spec)) {
         prepare_branch_lengths();
         select_test_branches(test_branches);
+    }
+
+    // meme.hpp:95-148: the branch set is checked before any fit; GTR fit, then the global MG94 fit from its
+    // rates (every branch and omega, with a separate background omega for a split; or omega and a tree scale
+    // when !full_model), then the analyzer on that tree
+    static MEMEAnalyzer create_and_fit(Tree input_tree, Alignment aln, Scalar pvalue_threshold = 0.1,
+                                       std::function<void(const std::string&, double)> progress_cb = nullptr,
+                                       bool full_model = true, std::string branches_spec = "All") {
+        input_tree.select_branches(branches_spec, "", {}, false);
+        if (progress_cb) progress_cb("Phase 1: Fitting Nucleotide GTR Model", 0.1);
+        hyphy::opt::GTRFitter gtr_fitter(input_tree, aln);
+        const auto gtr = gtr_fitter.fit();
+        if (progress_cb) progress_cb("Phase 2: Refining under Global MG94 Model", 0.3);
+        MG94Parameters p;
+        p.theta_AC = gtr.params.theta_AC; p.theta_AT = gtr.params.theta_AT; p.theta_CG = gtr.params.theta_CG;
+        p.theta_CT = gtr.params.theta_CT; p.theta_GT = gtr.params.theta_GT;
+        const auto sel = gtr.tree.select_branches(branches_spec, "", {}, true);
+        const bool split = sel.num_selected > 0 && sel.num_unselected > 0;
+        hyphy::opt::MG94Fitter mg(gtr.tree, aln);
+        hyphy::opt::FitResult fit;
+        if (full_model) {
+            fit = mg.fit_full_model(1.0, p, progress_cb, 250, 1e-5, split ? &sel.is_selected : nullptr);
+            p = fit.params;
+        } else {
+            fit = mg.fit_omega_and_scale(1.0, p);
+            p.alpha = 1.0;
+            p.beta = fit.x_opt[0];
+        }
+        MEMEAnalyzer out(fit.tree, std::move(aln), p, std::move(branches_spec));
+        out.p_value_threshold = pvalue_threshold;
+        out.global_log_l = fit.log_likelihood;
+        out.global_aicc = hyphy::opt::compute_aicc(fit.log_likelihood, 5 + (split ? 2 : 1) + (fit.tree.num_nodes() - 1),
+                                                   out.aln.num_codons);
+        out.has_gtr_fit = true;
+        out.gtr_log_l = gtr.log_likelihood;
+        out.gtr_aicc = gtr.aicc;
+        out.gtr_rates = gtr.params;
+        for (const auto& nd : gtr.tree.nodes)
+            if (nd.id != gtr.tree.root_id) out.gtr_branch_lengths[nd.name] = nd.branch_length;
+        return out;
     }
 
     // meme.hpp:84-92

@@ -353,6 +353,12 @@ inline std::pair<Scalar, Scalar> brent_minimize(F&& f, Scalar a, Scalar b, Scala
     return {x, fx};
 }
 
+// stats.hpp:114-121: AICc, falling back to AIC when n <= k + 1
+inline Scalar compute_aicc(Scalar log_l, size_t k_params, size_t n_obs) {
+    const Scalar k = Scalar(k_params), n = Scalar(n_obs);
+    return n > k + 1.0 ? -2.0 * log_l + 2.0 * k * n / (n - k - 1.0) : -2.0 * log_l + 2.0 * k;
+}
+
 struct GTRFitResult {
     Scalar log_likelihood = 0.0;
     Scalar aicc = 0.0;
@@ -450,8 +456,7 @@ public:
         res.log_likelihood = lnl_at(lengths(1.0), res.params);
         res.iterations = sol.iterations;
         res.converged = sol.converged || sol.pg_inf <= std::max<Scalar>(tolerance, 1e-3);
-        const Scalar K = Scalar(5 + B), N = Scalar(nuc_aln.num_nucleotides);
-        res.aicc = N > K + 1.0 ? -2.0 * res.log_likelihood + 2.0 * K * N / (N - K - 1.0) : -2.0 * res.log_likelihood + 2.0 * K;
+        res.aicc = compute_aicc(res.log_likelihood, 5 + B, nuc_aln.num_nucleotides);
         return res;
     }
 };

@@ -26,6 +26,12 @@ FILES = {
     # FEL parity on CD2 with matched branch lengths: tests/test_fel_cd2_parity.cpp:66-118
     "cd2.fna": "benchmarks/data/cd2.fna",
     "cd2_fitted.nwk": "benchmarks/data/cd2_fitted.nwk",
+    # BGLOBIN and COXI (Vertebrate-mtDNA code) with embedded trees: tests/test_fel_multi_dataset.cpp:123-197
+    "bglobin.nex": "benchmarks/data/bglobin.nex",
+    "COXI.nex": "benchmarks/data/COXI.nex",
+    # CD2 topology without lengths ({Group} tags) that FEL/MEME create_and_fit start from:
+    # tests/test_fel_multi_dataset.cpp:66-69, tests/test_meme.cpp:66-69
+    "cd2.nwk": "benchmarks/data/cd2.nwk",
     # FEL branch-subset selection by {T} tags in the embedded tree: tests/test_fel.cpp:128-170
     "Fig4E.nex": "tests/data/Fig4E.nex",
 }
@@ -91,7 +97,45 @@ def main(ref: str) -> None:
     # FEL ground truth of the reference's parity tests (tests/test_fel_multi_dataset.cpp:195-196)
     known["cd2_gtr"] = gtr_case(ref_root, "cd2_fel.json", "cd2.fna")
     known["adh_gtr"] = gtr_case(ref_root, "adh_fel.json", "adh.nex")
+    # FEL from an alignment and a tree alone (GTR fit, global MG94 fit, FEL) against HyPhy 2.5:
+    # tests/test_fel_multi_dataset.cpp:66-121
+    known["fel_e2e_cd2"] = fel_e2e_case(ref_root, "cd2_fel.json", "tests/test_fel_multi_dataset.cpp:66-92",
+                                        "cd2.fna", "cd2.nwk", True, 0.998, 0.995)
+    known["fel_e2e_adh"] = fel_e2e_case(ref_root, "adh_fel_rel.json", "tests/test_fel_multi_dataset.cpp:94-121",
+                                        "adh.nex", None, False, 0.998, 0.998)
+    known["fel_e2e_bglobin"] = fel_e2e_case(ref_root, "bglobin_fel_rel.json", "tests/test_fel_multi_dataset.cpp:123-150",
+                                            "bglobin.nex", None, False, 0.998, 0.998)
+    # p-value correlations, the GTR log-likelihood (relative 1e-4) and omega (0.005): :152-197
+    known["fel_e2e_coxi"] = fel_e2e_case(ref_root, "coxi_fel_rel.json", "tests/test_fel_multi_dataset.cpp:152-197",
+                                         "COXI.nex", None, False, 0.995, 0.995, code="Vertebrate-mtDNA",
+                                         min_p=(0.995, 0.995), omega_tol=0.005)
+    # MEME create_and_fit with the full MG94 fit on ADH: tests/test_meme.cpp:145-160 (HyPhy 2.5: -4686.18, 0.0941)
+    known["meme_full_fit_adh"] = {
+        "source": "tests/test_meme.cpp:145-160 (global_log_l >= -4687.5, |omega - 0.0941| < 0.01)",
+        "min_log_l": -4687.5, "omega": 0.0941, "omega_tol": 0.01,
+    }
     (out / "known_answers.json").write_text(json.dumps(known, indent=1) + "\n")
+
+
+def fel_e2e_case(ref_root: pathlib.Path, name: str, test_ref: str, alignment: str, tree, full_model: bool,
+                 r_lrt: float, rho_lrt: float, code=None, min_p=None, omega_tol=None) -> dict:
+    """HyPhy's per-site LRT / p-value columns, its nucleotide GTR and global MG94xREV fits for a create_and_fit
+    run; tree None means the alignment's embedded tree.  min_p / omega_tol: the p-value correlations and the
+    omega tolerance where the reference test checks them."""
+    g = json.loads((ref_root / "benchmarks/ground_truth" / name).read_text())
+    fit = g["fits"]["Global MG94xREV"]
+    mle = g["MLE"]["content"]["0"]
+    return {
+        "source": f"benchmarks/ground_truth/{name} (HyPhy 2.5); compared in {test_ref}",
+        "alignment": alignment, "tree": tree, "full_model": full_model, "genetic_code": code,
+        "lrt": [row[3] for row in mle], "p_value": [row[4] for row in mle],
+        "mg94_omega": fit["Rate Distributions"]["non-synonymous/synonymous rate ratio for *test*"][0][0],
+        "mg94_log_l": fit["Log Likelihood"],
+        "gtr_log_l": g["fits"]["Nucleotide GTR"]["Log Likelihood"],
+        "min_pearson_lrt": r_lrt, "min_spearman_lrt": rho_lrt,
+        "min_pearson_p": min_p[0] if min_p else None, "min_spearman_p": min_p[1] if min_p else None,
+        "omega_tol": omega_tol,
+    }
 
 
 def fel_subset_cases(ref_root: pathlib.Path) -> dict:

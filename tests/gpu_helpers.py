@@ -61,3 +61,17 @@ def dq_theta(aln, x, p):
 def rel(a, b):
     a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
     return float(np.max(np.abs(a - b)) / max(1.0, float(np.max(np.abs(b)))))
+
+
+def ranks(v):
+    """Average ranks with ties closer than 1e-12 (tests/test_fel_multi_dataset.cpp:22-44)."""
+    order = np.argsort(v, kind="stable")
+    r = np.empty(len(v))
+    i = 0
+    while i < len(v):
+        j = i + 1
+        while j < len(v) and abs(v[order[j]] - v[order[i]]) < 1e-12:
+            j += 1
+        r[order[i:j]] = 0.5 * (i + j - 1) + 1.0
+        i = j
+    return r

@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 from gpu_helpers import problem_from_oracle
+from gpu_helpers import ranks as _ranks
 
 pytestmark = pytest.mark.gpu
 
@@ -34,19 +35,6 @@ def _inputs(oracle, aln, params):
     np.fill_diagonal(qs, 0.0)
     np.fill_diagonal(qn, 0.0)
     return np.asarray(aln.pi), qs, qn
-
-
-def _ranks(v):
-    order = np.argsort(v, kind="stable")
-    r = np.empty(len(v))
-    i = 0
-    while i < len(v):
-        j = i + 1
-        while j < len(v) and abs(v[order[j]] - v[order[i]]) < 1e-12:
-            j += 1
-        r[order[i:j]] = 0.5 * (i + j - 1) + 1.0
-        i = j
-    return r
 
 
 def _hyphy_acceptance(k, lrt, pv):
