@@ -443,8 +443,16 @@ static size_t n_out_of(const h3g_problem* pr) { return 2 + size_t(pr->n) + pr->K
 // Allocate the evaluation workspace for (M, K, nmod, ndirs); reuses it when unchanged.
 static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int ndirs) {
     h3g_ctx* ctx = pr->ctx;
-    const size_t key[4] = {size_t(M), size_t(K), size_t(nmod), size_t(ndirs)};
-    if (pr->w.P && std::equal(key, key + 4, pr->work_key)) return H3G_OK;
+    // grow-only: a workspace sized for larger (M, K, models, directions) serves every smaller model (strides and
+    // offsets come from the installed model), so optimisers that alternate gradient and value-only evaluations
+    // (different direction counts) do not reallocate
+    size_t key[4] = {size_t(M), size_t(K), size_t(nmod), size_t(ndirs)};
+    if (pr->w.P && key[0] <= pr->work_key[0] && key[1] <= pr->work_key[1] && key[2] <= pr->work_key[2] &&
+        key[3] <= pr->work_key[3])
+        return H3G_OK;
+    if (pr->w.P)
+        for (int i = 0; i < 4; ++i) key[i] = std::max(key[i], pr->work_key[i]);
+    M = int(key[0]); K = int(key[1]); nmod = int(key[2]); ndirs = int(key[3]);
     cudaStreamSynchronize(ctx->stream);
     pr->drop_graphs();
     pr->work_mem.release();
@@ -586,23 +594,29 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             for (int k = 0; k < nm; ++k) pad_matrix(d->dQ + (size_t(x) * nm + k) * S * S, S, &dQ[(size_t(x) * nm + k) * SP2]);
         std::vector<uint8_t> it(pr->n, 1);
         if (d->is_test) std::copy(d->is_test, d->is_test + pr->n, it.begin());
-        const size_t mkey[5] = {size_t(nm), size_t(d->K), size_t(d->M), size_t(std::max(d->n_dirs, 1)), size_t(pr->n)};
-        if (!pr->m_pi || !std::equal(mkey, mkey + 5, pr->model_key)) {
+        // grow-only, like the workspace
+        size_t mkey[5] = {size_t(nm), size_t(d->K), size_t(d->M), size_t(std::max(d->n_dirs, 1)), size_t(pr->n)};
+        bool fits = pr->m_pi != nullptr;
+        for (int i = 0; i < 5 && fits; ++i) fits = mkey[i] <= pr->model_key[i];
+        if (!fits && pr->m_pi)
+            for (int i = 0; i < 5; ++i) mkey[i] = std::max(mkey[i], pr->model_key[i]);
+        if (!fits) {
             pr->drop_graphs();
             auto& A = pr->model_mem;
             A.release();
+            const size_t cnm = mkey[0], cK = mkey[1], cM = mkey[2], cdirs = mkey[3];
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_pi, SP));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_Q, Q.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_lam, lam.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_U, U.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_UT, UT.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_QT, QT.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_V, V.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_mu, mu.size()));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_cw, d->K));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rt, d->M));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rw, d->M));
-            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_dQ, dQ.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_Q, cnm * SP2));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_lam, cnm * SP));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_U, cnm * SP2));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_UT, cnm * SP2));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_QT, cnm * SP2));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_V, cnm * SP2));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_mu, cnm));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_cw, cK));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rt, cM));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rw, cM));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_dQ, cdirs * cnm * SP2));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_it, it.size()));
             std::copy(mkey, mkey + 5, pr->model_key);
         }

@@ -416,11 +416,90 @@ PYBIND11_MODULE(_hyphy3, m) {
     // BUSTED likelihood core: evaluate_log_l and the two EM expectation steps
     using hyphy::analyses::BUSTEDAnalyzer;
     using VecS = std::vector<Scalar>;
+    using hyphy::analyses::BUSTEDFit;
+    using hyphy::analyses::BUSTEDRateDistribution;
+    using hyphy::analyses::BUSTEDResult;
+    using hyphy::analyses::BUSTEDSettings;
+    py::class_<BUSTEDSettings>(m, "BUSTEDSettings")
+        .def(py::init<>())
+        .def_readwrite("full_auto", &BUSTEDSettings::full_auto)
+        .def_readwrite("num_rate_classes", &BUSTEDSettings::num_rate_classes)
+        .def_readwrite("srv", &BUSTEDSettings::srv)
+        .def_readwrite("num_syn_rate_classes", &BUSTEDSettings::num_syn_rate_classes)
+        .def_readwrite("auto_select_k", &BUSTEDSettings::auto_select_k)
+        .def_readwrite("max_k", &BUSTEDSettings::max_k)
+        .def_readwrite("refine_branch_lengths", &BUSTEDSettings::refine_branch_lengths)
+        .def_readwrite("multiple_hits", &BUSTEDSettings::multiple_hits)
+        .def_readwrite("error_sink", &BUSTEDSettings::error_sink)
+        .def_readwrite("error_sink_max_weight", &BUSTEDSettings::error_sink_max_weight)
+        .def_readwrite("error_sink_bf_threshold", &BUSTEDSettings::error_sink_bf_threshold)
+        .def_readwrite("test_branches", &BUSTEDSettings::test_branches)
+        .def_readwrite("phenotype_mode", &BUSTEDSettings::phenotype_mode)
+        .def_readwrite("relax_mode", &BUSTEDSettings::relax_mode)
+        .def_readwrite("p_value_threshold", &BUSTEDSettings::p_value_threshold);
+    py::class_<BUSTEDRateDistribution>(m, "BUSTEDRateDistribution")
+        .def_readonly("omegas", &BUSTEDRateDistribution::omegas)
+        .def_readonly("weights", &BUSTEDRateDistribution::weights)
+        .def_readonly("syn_rates", &BUSTEDRateDistribution::syn_rates)
+        .def_readonly("syn_weights", &BUSTEDRateDistribution::syn_weights)
+        .def_readonly("error_sink_weight", &BUSTEDRateDistribution::error_sink_weight)
+        .def_readonly("annotations", &BUSTEDRateDistribution::annotations);
+    py::class_<BUSTEDFit>(m, "BUSTEDFit")
+        .def_readonly("log_likelihood", &BUSTEDFit::log_likelihood)
+        .def_readonly("aicc", &BUSTEDFit::aicc)
+        .def_readonly("tree_scale", &BUSTEDFit::tree_scale)
+        .def_readonly("num_rate_classes", &BUSTEDFit::num_rate_classes)
+        .def_readonly("test_distribution", &BUSTEDFit::test_distribution)
+        .def_readonly("has_background_distribution", &BUSTEDFit::has_background_distribution)
+        .def_readonly("background_distribution", &BUSTEDFit::background_distribution)
+        .def_readonly("branch_lengths", &BUSTEDFit::branch_lengths)
+        .def_readonly("site_log_likelihoods", &BUSTEDFit::site_log_likelihoods)
+        .def_readonly("delta", &BUSTEDFit::delta)
+        .def_readonly("psi", &BUSTEDFit::psi)
+        .def_readonly("error_sink_weight", &BUSTEDFit::error_sink_weight)
+        .def_readonly("has_gtr_params", &BUSTEDFit::has_gtr_params)
+        .def_readonly("gtr_params", &BUSTEDFit::gtr_params)
+        .def_readonly("iterations", &BUSTEDFit::iterations);
+    py::class_<BUSTEDResult>(m, "BUSTEDResult")
+        .def_readonly("settings", &BUSTEDResult::settings)
+        .def_readonly("optimal_k", &BUSTEDResult::optimal_k)
+        .def_readonly("lrt", &BUSTEDResult::lrt)
+        .def_readonly("p_value", &BUSTEDResult::p_value)
+        .def_readonly("unconstrained", &BUSTEDResult::unconstrained)
+        .def_readonly("constrained", &BUSTEDResult::constrained)
+        .def_readonly("evidence_ratios", &BUSTEDResult::evidence_ratios)
+        .def_readonly("constrained_evidence_ratios", &BUSTEDResult::constrained_evidence_ratios)
+        .def_readonly("is_failed", &BUSTEDResult::is_failed)
+        .def_readonly("error_message", &BUSTEDResult::error_message)
+        .def_readonly("runtime_seconds", &BUSTEDResult::runtime_seconds);
     py::class_<BUSTEDAnalyzer>(m, "BUSTEDAnalyzer")
         .def(py::init([](Tree tree, Alignment aln, const MG94Parameters& params) {
                  return BUSTEDAnalyzer(std::move(tree), std::move(aln), params);
              }),
              "tree"_a, "alignment"_a, "params"_a = MG94Parameters{})
+        .def_static("create_and_fit", [](Tree tree, Alignment aln) {
+                        py::gil_scoped_release rel;
+                        return BUSTEDAnalyzer::create_and_fit(std::move(tree), std::move(aln));
+                    }, "tree"_a, "alignment"_a)
+        .def("run", [](const BUSTEDAnalyzer& b, const BUSTEDSettings& settings, bool show_progress, bool force_progress) {
+                 py::gil_scoped_release rel;
+                 return b.run(settings, show_progress, force_progress);
+             }, "settings"_a = BUSTEDSettings{}, "show_progress"_a = false, "force_progress"_a = false)
+        .def("fit_model", [](const BUSTEDAnalyzer& b, bool is_constrained, size_t K, bool refine, bool srv, size_t M,
+                             std::optional<BUSTEDFit> warm) {
+                 py::gil_scoped_release rel;
+                 return b.fit_model(is_constrained, K, refine, srv, M, "None", warm ? &*warm : nullptr);
+             }, "is_constrained"_a, "K"_a = 3, "refine_branches"_a = true, "srv"_a = false, "num_syn_rates"_a = 3,
+             "warm_start_fit"_a = std::nullopt)
+        .def_readonly("tree", &BUSTEDAnalyzer::tree)
+        .def_readonly("base_params", &BUSTEDAnalyzer::base_params)
+        .def_readonly("mg94_log_l", &BUSTEDAnalyzer::mg94_log_l)
+        .def_readonly("has_gtr_fit", &BUSTEDAnalyzer::has_gtr_fit)
+        .def_readonly("gtr_log_l", &BUSTEDAnalyzer::gtr_log_l)
+        .def_readonly("gtr_aicc", &BUSTEDAnalyzer::gtr_aicc)
+        .def_readonly("gtr_rates", &BUSTEDAnalyzer::gtr_rates)
+        .def_readonly("gtr_branch_lengths", &BUSTEDAnalyzer::gtr_branch_lengths)
+        .def_readonly("num_background_branches", &BUSTEDAnalyzer::num_background_branches)
         .def_readwrite("branch_tau", &BUSTEDAnalyzer::branch_tau)
         .def_readwrite("is_test_branch", &BUSTEDAnalyzer::is_test_branch)
         .def_readwrite("num_test_branches", &BUSTEDAnalyzer::num_test_branches)

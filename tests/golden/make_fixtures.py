@@ -109,6 +109,18 @@ def main(ref: str) -> None:
     known["fel_e2e_coxi"] = fel_e2e_case(ref_root, "coxi_fel_rel.json", "tests/test_fel_multi_dataset.cpp:152-197",
                                          "COXI.nex", None, False, 0.995, 0.995, code="Vertebrate-mtDNA",
                                          min_p=(0.995, 0.995), omega_tol=0.005)
+    # BUSTED on CD2 from cd2.nwk against HyPhy 2.5 (srv on): tests/test_busted.cpp:17-86
+    b = json.loads((ref_root / "benchmarks/ground_truth/cd2_busted.json").read_text())
+    known["cd2_busted"] = {
+        "source": "benchmarks/ground_truth/cd2_busted.json (HyPhy 2.5, srv on); compared in tests/test_busted.cpp:17-86",
+        "gtr_log_l": b["fits"]["Nucleotide GTR"]["Log Likelihood"],
+        "mg94_log_l": b["fits"]["MG94xREV with separate rates for branch sets"]["Log Likelihood"],
+        "unconstrained_log_l": b["fits"]["Unconstrained model"]["Log Likelihood"],
+        "constrained_log_l": b["fits"]["Constrained model"]["Log Likelihood"],
+        "lrt": b["test results"]["LRT"], "p_value": b["test results"]["p-value"],
+        # tolerances of the reference test
+        "tol_gtr": 1.0, "tol_mg94": 0.05, "tol_fit": 2.5, "tol_lrt": 1.5, "max_p": 0.01,
+    }
     # MEME create_and_fit with the full MG94 fit on ADH: tests/test_meme.cpp:145-160 (HyPhy 2.5: -4686.18, 0.0941)
     known["meme_full_fit_adh"] = {
         "source": "tests/test_meme.cpp:145-160 (global_log_l >= -4687.5, |omega - 0.0941| < 0.01)",
