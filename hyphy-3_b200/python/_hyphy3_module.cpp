@@ -469,6 +469,7 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("constrained", &BUSTEDResult::constrained)
         .def_readonly("evidence_ratios", &BUSTEDResult::evidence_ratios)
         .def_readonly("constrained_evidence_ratios", &BUSTEDResult::constrained_evidence_ratios)
+        .def_readonly("k_null_fits", &BUSTEDResult::k_null_fits)
         .def_readonly("is_failed", &BUSTEDResult::is_failed)
         .def_readonly("error_message", &BUSTEDResult::error_message)
         .def_readonly("runtime_seconds", &BUSTEDResult::runtime_seconds);

@@ -24,7 +24,7 @@
 // one device mixture evaluation; the synonymous-rate coordinates use central differences of
 // the device likelihood.  Not provided: the error sink (eps_sink must be 0), multiple hits,
 // bridge resolutions, a separate background distribution (background branches keep the
-// global MG94 background omega), automatic K selection, BUSTED-PH / RELAX modes and the
+// global MG94 background omega), the full automatic selector, BUSTED-PH / RELAX modes and the
 // branch-site diagnostics.
 #pragma once
 
@@ -104,6 +104,7 @@ struct BUSTEDResult {
     BUSTEDFit constrained;
     std::vector<Scalar> evidence_ratios;              // per site: exp(lnL_alt - lnL_null)
     std::vector<Scalar> constrained_evidence_ratios;  // per site: exp(lnL_alt - lnL_alt with omega_K := min(1, omega_K))
+    std::vector<BUSTEDFit> k_null_fits;               // auto_select_k: the null fits for K = 1 .. max_k
     bool is_failed = false;
     std::string error_message;
     Scalar runtime_seconds = 0.0;
@@ -472,14 +473,27 @@ public:
         return fit;
     }
 
+    // busted.hpp:3115-3142: the null model for K = 1 .. max_k; K grows while AICc drops by more than 2
+    std::pair<size_t, std::vector<BUSTEDFit>> select_optimal_k(size_t max_k = 3, bool refine_branches = true, bool srv = false,
+                                                              size_t num_syn_rates = 3,
+                                                              const std::string& multiple_hits = "None") const {
+        std::vector<BUSTEDFit> nulls;
+        for (size_t k = 1; k <= std::max<size_t>(1, max_k); ++k)
+            nulls.push_back(fit_model(true, k, refine_branches, srv, num_syn_rates, multiple_hits));
+        size_t best = 1;
+        for (size_t k = 2; k <= nulls.size(); ++k)
+            if (nulls[k - 1].aicc < nulls[best - 1].aicc - 2.0) best = k;
+        return {best, std::move(nulls)};
+    }
+
     // busted.hpp:5969-6682, standard all-branch BUSTED: the unconstrained fit, the constrained fit warm-started from
     // it, the unconstrained refit from the constrained one while that is higher; LRT with the 0.5 chi2_0 +
     // 0.5 chi2_2 null (K >= 2; K = 1: one-sided chi2_1 with omega <= 1 under the null); per-site evidence ratios
     BUSTEDResult run(BUSTEDSettings settings = {}, bool show_progress = false, bool force_progress = false) const {
         (void)show_progress; (void)force_progress;
         const auto t0 = std::chrono::steady_clock::now();
-        if (settings.full_auto || settings.auto_select_k || settings.error_sink || settings.phenotype_mode || settings.relax_mode)
-            throw std::runtime_error("BUSTEDAnalyzer (device): automatic model selection, the error sink, BUSTED-PH and RELAX modes are not supported");
+        if (settings.full_auto || settings.error_sink || settings.phenotype_mode || settings.relax_mode)
+            throw std::runtime_error("BUSTEDAnalyzer (device): full automatic selection, the error sink, BUSTED-PH and RELAX modes are not supported");
         const auto sel = tree.select_branches(settings.test_branches, "", {}, false);
         is_test_branch = sel.is_selected;
         num_test_branches = sel.num_selected;
@@ -492,13 +506,28 @@ public:
         res.optimal_k = K;
         const bool refine = settings.refine_branch_lengths, srv = settings.srv;
         const size_t M = settings.num_syn_rate_classes;
-        res.unconstrained = fit_model(false, K, refine, srv, M, settings.multiple_hits);
-        res.constrained = fit_model(true, K, refine, srv, M, settings.multiple_hits, &res.unconstrained);
+        if (settings.auto_select_k) {
+            // busted.hpp:6339-6412 with select_optimal_k (:3115-3142): null fits for K = 1 .. max_k, a class added
+            // only when it lowers AICc by more than 2; the alternative from the chosen null, the null again from it
+            auto [opt_k, nulls] = select_optimal_k(settings.max_k, refine, srv, M, settings.multiple_hits);
+            res.optimal_k = opt_k;
+            res.k_null_fits = std::move(nulls);
+            res.constrained = res.k_null_fits[opt_k - 1];
+            res.unconstrained = fit_model(false, opt_k, refine, srv, M, settings.multiple_hits, &res.constrained);
+            if (opt_k >= 2) {
+                BUSTEDFit null2 = fit_model(true, opt_k, refine, srv, M, settings.multiple_hits, &res.unconstrained);
+                if (null2.log_likelihood > res.constrained.log_likelihood) res.constrained = std::move(null2);
+            }
+        } else {
+            res.unconstrained = fit_model(false, K, refine, srv, M, settings.multiple_hits);
+            res.constrained = fit_model(true, K, refine, srv, M, settings.multiple_hits, &res.unconstrained);
+        }
+        const size_t Kf = res.optimal_k;
         // the alternative contains the null: refit it from the null with the last omega moved above 1
-        for (int retry = 0; retry < 2; ++retry) {
+        for (int retry = 0; retry < 2 && Kf >= 2; ++retry) {
             BUSTEDFit from_null = res.constrained;
-            if (K >= 2) from_null.test_distribution.omegas.back() = 1.5;
-            BUSTEDFit alt = fit_model(false, K, refine, srv, M, settings.multiple_hits, &from_null);
+            from_null.test_distribution.omegas.back() = 1.5;
+            BUSTEDFit alt = fit_model(false, Kf, refine, srv, M, settings.multiple_hits, &from_null);
             const bool better = alt.log_likelihood > res.unconstrained.log_likelihood + 1e-6;
             if (better) res.unconstrained = std::move(alt);
             if (!better || res.constrained.log_likelihood <= res.unconstrained.log_likelihood + 1e-5) break;
@@ -509,7 +538,7 @@ public:
             res.error_message = "Optimization failed: model log-likelihood collapsed to the zero-likelihood sentinel.";
             res.lrt = 0.0;
             res.p_value = 1.0;
-        } else if (K == 1) {
+        } else if (Kf == 1) {
             if (res.unconstrained.test_distribution.omegas[0] <= 1.0 ||
                 res.unconstrained.log_likelihood <= res.constrained.log_likelihood) {
                 res.constrained = res.unconstrained;

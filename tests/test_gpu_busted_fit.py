@@ -78,6 +78,24 @@ def test_busted_adh_structure(golden_dir):
     assert len(res.unconstrained.branch_lengths) == b.tree.num_nodes()
 
 
+def test_busted_auto_k_adh(golden_dir):
+    """tests/test_busted.cpp:137-164: on ADH the AICc step-up over the null fits picks K = 2 and still detects
+    positive selection."""
+    import _hyphy3 as h3
+    aln = h3.Alignment.load(str(golden_dir / "adh.nex"))
+    b = h3.BUSTEDAnalyzer.create_and_fit(h3.Tree.from_newick(aln.embedded_tree_newick), aln)
+    s = h3.BUSTEDSettings()
+    s.auto_select_k = True
+    s.max_k = 3
+    s.refine_branch_lengths = True
+    res = b.run(s)
+    aicc = [f.aicc for f in res.k_null_fits]
+    assert res.optimal_k == 2, aicc
+    assert len(res.unconstrained.test_distribution.omegas) == 2 and len(res.constrained.test_distribution.omegas) == 2
+    assert res.unconstrained.test_distribution.omegas[1] >= 1.0 and res.constrained.test_distribution.omegas[1] == 1.0
+    assert res.lrt >= 0.0 and res.p_value <= 0.05, (res.lrt, res.p_value)
+
+
 def test_busted_rejects_unsupported_modes(cd2_busted):
     import _hyphy3 as h3
     s = h3.BUSTEDSettings()
