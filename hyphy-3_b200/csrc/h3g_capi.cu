@@ -92,7 +92,8 @@ struct h3g_problem {
     uint64_t model_hash = 0;
     double *m_pi = nullptr, *m_Q = nullptr, *m_lam = nullptr, *m_U = nullptr, *m_V = nullptr, *m_mu = nullptr;
     double *m_UT = nullptr, *m_QT = nullptr;
-    double *m_cw = nullptr, *m_rt = nullptr, *m_rw = nullptr, *m_dQ = nullptr;
+    double *m_cw = nullptr, *m_bw = nullptr, *m_rt = nullptr, *m_rw = nullptr, *m_dQ = nullptr;
+    std::vector<double> h_bw;   // background weights as uploaded (ones when the caller gives none)
     uint8_t* m_it = nullptr;
     // captured evaluation graphs, keyed by (want, with host copies)
     // the site-fit evaluator of the last h3g_fel_run / h3g_meme_run, kept for the next run
@@ -438,7 +439,7 @@ static void pad_matrix(const double* src, int S, double* dst) {
     for (int i = 0; i < S; ++i) std::copy(src + size_t(i) * S, src + size_t(i) * S + S, dst + size_t(i) * SP);
 }
 
-static size_t n_out_of(const h3g_problem* pr) { return 2 + size_t(pr->n) + pr->K + pr->nmod + pr->M; }
+static size_t n_out_of(const h3g_problem* pr) { return 2 + size_t(pr->n) + 2 * size_t(pr->nmod) + pr->M; }
 
 // Allocate the evaluation workspace for (M, K, nmod, ndirs); reuses it when unchanged.
 static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int ndirs) {
@@ -489,12 +490,12 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     w.ngroups = int(std::max<size_t>(1, std::min<size_t>(n, (296 + size_t(M) * nmod - 1) / (size_t(M) * nmod))));
     const size_t G = size_t(w.ngroups);
     H3G_TRY_CUDA(ctx, A.alloc(&w.Hpart, size_t(nmod) * M * G * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(std::max(K, 1)) * M * G));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(nmod) * M * G));
     H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * G));
     H3G_TRY_CUDA(ctx, A.alloc(&w.H, size_t(nmod) * SP2));
     H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 17));
     H3G_TRY_CUDA(ctx, A.alloc(&w.G, size_t(std::max(ndirs, 1)) * nmod * SP2));
-    const size_t n_out = 2 + n + K + nmod + M;
+    const size_t n_out = 2 + n + 2 * size_t(nmod) + M;
     H3G_TRY_CUDA(ctx, A.alloc(&w.out, n_out));
     H3G_TRY_CUDA(ctx, A.alloc(&w.err, 1));
     cudaMemsetAsync(w.err, 0, sizeof(int), ctx->stream);
@@ -507,7 +508,7 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
         h3g_status st = mixed_alloc(pr->mw, A.ptrs, pr->n, pr->NI, M, pr->Pp);
         if (st != H3G_OK) return fail(ctx, st, "mixed-precision workspace allocation failed");
     }
-    cudaMemsetAsync(w.gc, 0, size_t(std::max(K, 1)) * M * G * sizeof(double), ctx->stream);
+    cudaMemsetAsync(w.gc, 0, size_t(nmod) * M * G * sizeof(double), ctx->stream);
     cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * G * sizeof(double), ctx->stream);
     pr->off_out = n;
     pr->off_dir = pr->off_out + n_out;
@@ -535,7 +536,8 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     h3g_ctx* ctx = pr->ctx;
     if (d->S < 1 || d->S > SP) return fail(ctx, H3G_ERR_ARG, "S must be in [1, 64]");
     if (d->K < 1 || d->M < 1 || d->M > kMaxRateClasses) return fail(ctx, H3G_ERR_ARG, "need K >= 1 and 1 <= M <= 16");
-    if (d->n_models != d->K + (d->has_bg ? 1 : 0)) return fail(ctx, H3G_ERR_ARG, "n_models must equal K + has_bg");
+    if (d->has_bg < 0 || d->n_models != d->K + d->has_bg) return fail(ctx, H3G_ERR_ARG, "n_models must equal K + has_bg");
+    if (d->has_bg > 1 && !d->bg_w) return fail(ctx, H3G_ERR_ARG, "several background classes need bg_w");
     if (!d->pi || !d->Q || !d->lam || !d->U || !d->V || !d->class_w || !d->rates || !d->rate_w)
         return fail(ctx, H3G_ERR_ARG, "model arrays missing");
     if (d->time_mode == H3G_TIME_NORMALIZED && !d->mu) return fail(ctx, H3G_ERR_ARG, "normalized time needs mu");
@@ -545,6 +547,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     const int S = d->S, nm = d->n_models;
     if (pr->max_state >= S) return fail(ctx, H3G_ERR_ARG, "a pattern state index is >= S");
     auto finite = [](const double* a, size_t k) { for (size_t i = 0; i < k; ++i) if (!std::isfinite(a[i])) return false; return true; };
+    if (d->bg_w && !finite(d->bg_w, size_t(d->has_bg))) return fail(ctx, H3G_ERR_NUMERIC, "non-finite background weights");
     if (!finite(d->pi, S) || !finite(d->Q, size_t(nm) * S * S) || !finite(d->lam, size_t(nm) * S) || !finite(d->U, size_t(nm) * S * S) ||
         !finite(d->V, size_t(nm) * S * S) || !finite(d->class_w, d->K) || !finite(d->rates, d->M) || !finite(d->rate_w, d->M))
         return fail(ctx, H3G_ERR_NUMERIC, "non-finite model parameters");
@@ -561,6 +564,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         h = hash_bytes(h, d->V, size_t(nm) * S * S * sizeof(double));
         if (d->mu) h = hash_bytes(h, d->mu, nm * sizeof(double));
         h = hash_bytes(h, d->class_w, d->K * sizeof(double));
+        if (d->bg_w) h = hash_bytes(h, d->bg_w, size_t(d->has_bg) * sizeof(double));
         h = hash_bytes(h, d->rates, d->M * sizeof(double));
         h = hash_bytes(h, d->rate_w, d->M * sizeof(double));
         if (d->is_test) h = hash_bytes(h, d->is_test, size_t(pr->n));
@@ -614,6 +618,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_V, cnm * SP2));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_mu, cnm));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_cw, cK));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_bw, cnm));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rt, cM));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rw, cM));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_dQ, cdirs * cnm * SP2));
@@ -630,6 +635,11 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_V, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_mu, mu.data(), mu.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_cw, d->class_w, d->K * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (d->has_bg > 0) {
+            pr->h_bw.assign(size_t(d->has_bg), 1.0);
+            if (d->bg_w) std::copy(d->bg_w, d->bg_w + d->has_bg, pr->h_bw.begin());
+            H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_bw, pr->h_bw.data(), pr->h_bw.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_rt, d->rates, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_rw, d->rate_w, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_dQ, dQ.data(), dQ.size() * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -639,7 +649,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         md.sentinel = d->zero_l_sentinel;
         md.pi = pr->m_pi; md.Q = pr->m_Q; md.lam = pr->m_lam; md.U = pr->m_U; md.V = pr->m_V; md.mu = pr->m_mu;
         md.UT = pr->m_UT; md.QT = pr->m_QT;
-        md.class_w = pr->m_cw; md.rates = pr->m_rt; md.rate_w = pr->m_rw; md.is_test = d->is_test ? pr->m_it : nullptr;
+        md.class_w = pr->m_cw; md.bg_w = pr->m_bw; md.rates = pr->m_rt; md.rate_w = pr->m_rw; md.is_test = d->is_test ? pr->m_it : nullptr;
         md.dQ = pr->m_dQ;
         if (std::memcmp(&md, &pr->md, sizeof(Model)) != 0) pr->drop_graphs();
         pr->md = md;
@@ -805,7 +815,9 @@ static void unpack_result(h3g_problem* pr, unsigned want, h3g_result* out) {
         out->grad_t[pr->root] = 0.0;
     }
     if (out->grad_class_w) for (int k = 0; k < pr->K; ++k) out->grad_class_w[k] = global ? hout[2 + n + k] : 0.0;
-    if (out->grad_rate_w) for (int m = 0; m < pr->M; ++m) out->grad_rate_w[m] = grads ? hout[2 + n + pr->K + pr->nmod + m] : 0.0;
+    if (out->grad_bg_w)
+        for (int j = 0; j < pr->nmod - pr->K; ++j) out->grad_bg_w[j] = global ? hout[2 + n + pr->K + j] : 0.0;
+    if (out->grad_rate_w) for (int m = 0; m < pr->M; ++m) out->grad_rate_w[m] = grads ? hout[2 + n + 2 * pr->nmod + m] : 0.0;
     if (out->grad_dir) {
         // sum_k sum (V dQ U) o H_k, minus (normalised time) sum_k dmu_k / mu_k * sum_b tau_b dL/dtau_b
         const double* dir = pr->h_pin + pr->off_dir;
@@ -817,7 +829,7 @@ static void unpack_result(h3g_problem* pr, unsigned want, h3g_result* out) {
                     double v = 0.0;
                     for (int b = 0; b < 16; ++b) v += d[b];
                     if (pr->time_mode == H3G_TIME_NORMALIZED)
-                        v -= d[16] / std::max(pr->h_mu[size_t(k)], 1e-12) * hout[2 + n + pr->K + k];
+                        v -= d[16] / std::max(pr->h_mu[size_t(k)], 1e-12) * hout[2 + n + pr->nmod + k];
                     g += v;
                 }
             out->grad_dir[x] = g;

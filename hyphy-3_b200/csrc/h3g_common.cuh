@@ -88,6 +88,7 @@ struct Model {
     const double* V;         // [nmod][64*64]
     const double* mu;        // [nmod]
     const double* class_w;   // [K]
+    const double* bg_w;      // [nmod - K] background mixing weights
     const double* rates;     // [M]
     const double* rate_w;    // [M]
     const uint8_t* is_test;  // [n] or null
@@ -121,7 +122,7 @@ struct Work {
     double* H;               // [nmod][64*64]
     double* dirpart;         // [ndirs][nmod][17]: 16 partials of sum (V dQ U) o H, then d mu = -sum pi_i dQ_ii
     double* G;               // [ndirs][nmod][64*64] V_k dQ_x U_k (depends on the model only)
-    double* out;             // [2 + n + K + nmod + M] lnl | error flag | grad_t | gc | stg | grad_rate_w
+    double* out;             // [2 + n + 2 nmod + M] lnl | error flag | grad_t | gc (per model) | stg | grad_rate_w
     int* err;                // sticky device error flags (bounded waits that expired)
 };
 

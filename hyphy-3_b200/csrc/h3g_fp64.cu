@@ -149,12 +149,12 @@ __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
     if (b == t.root) return;
     const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-    const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.K + 1;
+    const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.nmod;
     Frag64 accP, accD;
     frag_zero(accP);
     frag_zero(accD);
     for (int k = k0; k < k1; ++k) {
-        const double cw = test ? md.class_w[k] : 1.0;
+        const double cw = test ? md.class_w[k] : md.bg_w[k - md.K];
         const double cv = time_conv(md, k);
         const double rate = md.rates[m];
         const double tau = rate * w.bl[b] * cv;
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
         if (b == t.root) continue;
         const bool test = md.is_test == nullptr || md.is_test[b] != 0;
         if ((k < md.K) != test) continue;
-        const double cw = test ? md.class_w[k] : 1.0;
+        const double cw = test ? md.class_w[k] : md.bg_w[k - md.K];
         const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
         __syncthreads();                                  // the previous branch is done with sA
         {
@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
                     const double E = fabs(d) < 1e-9 ? tau * ei : (ei - ej) / d;
                     H.v[i][j][e] = fma(cw * a, E, H.v[i][j][e]);
                     if (r == c) {
-                        if (test) dg += ei * a;
+                        dg += ei * a;
                         dq += cw * tau * li * ei * a;
                     }
                 }
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
     dq = block_sum_256(dq, red);
     if (tid == 0) {
         const size_t o = (size_t(k) * M + m) * G + g;
-        if (k < md.K) w.gc[o] = dg;
+        w.gc[o] = dg;
         w.stg[o] = dq;
     }
 }
@@ -735,21 +735,21 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
     for (int k = 0; k < md.nmod; ++k) {
         double a = 0.0, z = 0.0;
         for (int idx = tid; idx < M * w.ngroups; idx += 256) {
-            if (k < md.K) a += w.gc[size_t(k) * M * w.ngroups + idx];
+            a += w.gc[size_t(k) * M * w.ngroups + idx];
             z += w.stg[size_t(k) * M * w.ngroups + idx];
         }
         a = block_sum_256(a, red);
         z = block_sum_256(z, red);
         if (tid == 0) {
-            if (k < md.K) w.out[2 + n + k] = a;
-            w.out[2 + n + md.K + k] = z;
+            w.out[2 + n + k] = a;                 // d lnL / d (class or background weight of model k)
+            w.out[2 + n + md.nmod + k] = z;
         }
     }
     for (int m = 0; m < M; ++m) {
         double a = 0.0;
         for (int p = tid; p < t.Pp; p += 256) a += w.rw[size_t(m) * t.Pp + p];
         a = block_sum_256(a, red);
-        if (tid == 0) w.out[2 + n + md.K + md.nmod + m] = a;
+        if (tid == 0) w.out[2 + n + 2 * md.nmod + m] = a;
     }
 }
 

@@ -27,6 +27,8 @@ static py::dict mixture_dict(const MixtureGradients& g) {
     d["grad_weights"] = g.grad_weights;
     d["grad_theta"] = std::vector<double>(g.grad_theta, g.grad_theta + 5);
     d["grad_syn_weights"] = g.grad_syn_weights;
+    d["grad_bg_omegas"] = g.grad_bg_omegas;
+    d["grad_bg_weights"] = g.grad_bg_weights;
     d["site_log_likelihoods"] = g.site_log_likelihoods;
     return d;
 }
@@ -269,19 +271,21 @@ PYBIND11_MODULE(_hyphy3, m) {
     m.def("compute_mixture_gradients", [](const Tree& t, const Alignment& a, const MG94Parameters& base, const std::vector<Scalar>& bl,
                                           const std::vector<Scalar>& omegas, const std::vector<Scalar>& weights,
                                           const std::vector<Scalar>& syn_rates, const std::vector<Scalar>& syn_weights,
-                                          py::object is_test, Scalar omega_bg, bool want_gradients, bool sentinel) {
+                                          py::object is_test, Scalar omega_bg, bool want_gradients, bool sentinel,
+                                          const std::vector<Scalar>& bg_omegas, const std::vector<Scalar>& bg_weights) {
         std::vector<bool> store;
         const std::vector<bool>* mask = opt_mask(is_test, store);
         MixtureGradients g;
         {
             py::gil_scoped_release rel;
             g = LikelihoodEngine::compute_mixture_gradients(t, a, base, bl, omegas, weights, syn_rates, syn_weights, mask, omega_bg,
-                                                            want_gradients, sentinel);
+                                                            want_gradients, sentinel, true, bg_omegas, bg_weights);
         }
         return mixture_dict(g);
     }, "tree"_a, "aln"_a, "base_params"_a, "branch_lengths"_a, "omegas"_a, "weights"_a,
        "syn_rates"_a = std::vector<Scalar>{1.0}, "syn_weights"_a = std::vector<Scalar>{1.0}, "is_test_branch"_a = py::none(),
-       "omega_bg"_a = -1.0, "want_gradients"_a = true, "zero_likelihood_sentinel"_a = false);
+       "omega_bg"_a = -1.0, "want_gradients"_a = true, "zero_likelihood_sentinel"_a = false,
+       "bg_omegas"_a = std::vector<Scalar>{}, "bg_weights"_a = std::vector<Scalar>{});
 
     m.def("compute_tree_log_likelihood_from_P", [](const Tree& t, const Alignment& a,
                                                    const std::vector<py::array_t<double, py::array::c_style | py::array::forcecast>>& Ps,

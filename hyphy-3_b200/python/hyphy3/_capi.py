@@ -39,7 +39,7 @@ class ModelDesc(C.Structure):
         ("S", C.c_int), ("pi", _dp), ("n_models", C.c_int), ("Q", _dp), ("lam", _dp), ("U", _dp), ("V", _dp),
         ("mu", _dp), ("K", C.c_int), ("class_w", _dp), ("has_bg", C.c_int), ("is_test", C.POINTER(C.c_uint8)),
         ("M", C.c_int), ("rates", _dp), ("rate_w", _dp), ("time_mode", C.c_int), ("n_dirs", C.c_int),
-        ("dQ", _dp), ("precision", C.c_int), ("zero_l_sentinel", C.c_int),
+        ("dQ", _dp), ("precision", C.c_int), ("zero_l_sentinel", C.c_int), ("bg_w", _dp),
     ]
 
 
@@ -72,7 +72,7 @@ class MemeResult(C.Structure):
 
 class Result(C.Structure):
     _fields_ = [("lnl", C.c_double), ("site_lnl", _dp), ("grad_t", _dp), ("grad_dir", _dp),
-                ("grad_class_w", _dp), ("grad_rate_w", _dp)]
+                ("grad_class_w", _dp), ("grad_rate_w", _dp), ("grad_bg_w", _dp)]
 
 
 _lib = None
@@ -227,8 +227,10 @@ class Problem:
             pass
 
     def set_model(self, *, pi, Q, lam, U, V, mu=None, class_w=(1.0,), has_bg=False, is_test=None, rates=(1.0,),
-                  rate_w=(1.0,), time_mode=TIME_RAW, dQ=None, precision=PREC_FP64, zero_l_sentinel=False) -> None:
-        """Q, U, V: [n_models, S, S]; lam: [n_models, S]; dQ: [n_dirs, n_models, S, S]."""
+                  rate_w=(1.0,), time_mode=TIME_RAW, dQ=None, precision=PREC_FP64, zero_l_sentinel=False,
+                  bg_w=None) -> None:
+        """Q, U, V: [n_models, S, S]; lam: [n_models, S]; dQ: [n_dirs, n_models, S, S].  bg_w: weights of
+        len(bg_w) background classes (models K ..), or None with has_bg for one background model."""
         Q = _f64(Q); U = _f64(U); V = _f64(V); lam = _f64(lam)
         if Q.ndim == 2:
             Q, U, V, lam = Q[None], U[None], V[None], lam[None]
@@ -239,10 +241,15 @@ class Problem:
         it = None if is_test is None else np.ascontiguousarray(is_test, dtype=np.uint8)
         dq = None if dQ is None else _f64(dQ)
         nd = 0 if dq is None else int(dq.shape[0])
+        bw = None if bg_w is None else _f64(bg_w)
+        if bw is not None:
+            nbg = int(bw.size)
+        else:
+            nbg = int(has_bg) if isinstance(has_bg, int) and not isinstance(has_bg, bool) else int(bool(has_bg))
         d = ModelDesc(S=S, pi=_ptr(pi), n_models=nm, Q=_ptr(Q), lam=_ptr(lam), U=_ptr(U), V=_ptr(V), mu=_ptr(mu_a),
-                      K=len(cw), class_w=_ptr(cw), has_bg=int(bool(has_bg)), is_test=_ptr(it, C.c_uint8), M=len(rt),
+                      K=len(cw), class_w=_ptr(cw), has_bg=nbg, is_test=_ptr(it, C.c_uint8), M=len(rt),
                       rates=_ptr(rt), rate_w=_ptr(rw), time_mode=time_mode, n_dirs=nd, dQ=_ptr(dq),
-                      precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)))
+                      precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)), bg_w=_ptr(bw))
         self.ctx.check(self.ctx.lib.h3g_model_set(self.h, C.byref(d)))
         self.K, self.M, self.ndirs, self.nmod = len(cw), len(rt), nd, nm
 
@@ -252,9 +259,11 @@ class Problem:
             raise ValueError("branch lengths must have one entry per node")
         if out is None:
             out = {"site_lnl": np.zeros(self.P), "grad_t": np.zeros(self.n), "grad_dir": np.zeros(max(self.ndirs, 1)),
-                   "grad_class_w": np.zeros(self.K), "grad_rate_w": np.zeros(self.M)}
+                   "grad_class_w": np.zeros(self.K), "grad_rate_w": np.zeros(self.M),
+                   "grad_bg_w": np.zeros(max(self.nmod - self.K, 1))}
         r = Result(site_lnl=_ptr(out["site_lnl"]), grad_t=_ptr(out["grad_t"]), grad_dir=_ptr(out["grad_dir"]),
-                   grad_class_w=_ptr(out["grad_class_w"]), grad_rate_w=_ptr(out["grad_rate_w"]))
+                   grad_class_w=_ptr(out["grad_class_w"]), grad_rate_w=_ptr(out["grad_rate_w"]),
+                   grad_bg_w=_ptr(out.get("grad_bg_w")))
         self.ctx.check(self.ctx.lib.h3g_eval(self.h, _ptr(bl), want, C.byref(r)))
         out["lnl"] = r.lnl
         return out

@@ -67,12 +67,13 @@ typedef struct h3g_problem h3g_problem;
 
 /* Reversible substitution models as eigensystems, P(tau) = U diag(exp(lam*tau)) V,
  * clamped at 0 (rate_matrix.hpp:251-257).  Models [0, K) are mixed at the P
- * level with weights class_w on test branches; when has_bg != 0 model K is
- * used alone on branches whose is_test entry is 0. */
+ * level with weights class_w on test branches; models [K, K + has_bg) are mixed
+ * with weights bg_w on branches whose is_test entry is 0 (has_bg = 1 with
+ * bg_w = NULL: one background model, weight 1). */
 typedef struct {
     int S;                    /* states (<= 64; 61 for the universal code) */
     const double* pi;         /* S equilibrium frequencies (root prior) */
-    int n_models;             /* K + (has_bg ? 1 : 0) */
+    int n_models;             /* K + has_bg */
     const double* Q;          /* n_models * S * S generators */
     const double* lam;        /* n_models * S eigenvalues (clamped <= 0) */
     const double* U;          /* n_models * S * S, U_pi */
@@ -80,7 +81,7 @@ typedef struct {
     const double* mu;         /* n_models mean rates (used by H3G_TIME_NORMALIZED) */
     int K;                    /* test-branch classes */
     const double* class_w;    /* K mixing weights */
-    int has_bg;
+    int has_bg;               /* background classes (0: every branch is a test branch) */
     const uint8_t* is_test;   /* n_nodes flags, NULL = every branch is a test branch */
     int M;                    /* synonymous-rate classes (separate pruning passes) */
     const double* rates;      /* M rate multipliers r_m */
@@ -91,6 +92,7 @@ typedef struct {
     int precision;            /* h3g_precision */
     int zero_l_sentinel;      /* 1: a pattern with L <= 0 adds weight * -1e20 to lnL (evaluate_log_l);
                                  0: it adds 0 (the gradient entry points) */
+    const double* bg_w;       /* has_bg background mixing weights; NULL allowed only when has_bg <= 1 */
 } h3g_model_desc;
 
 typedef struct {
@@ -100,6 +102,7 @@ typedef struct {
     double* grad_dir;         /* n_dirs, or NULL */
     double* grad_class_w;     /* K partials d lnL / d class_w[k], or NULL */
     double* grad_rate_w;      /* M partials d lnL / d rate_w[m], or NULL */
+    double* grad_bg_w;        /* has_bg partials d lnL / d bg_w[j], or NULL */
 } h3g_result;
 
 /* Context: one device, one stream (NULL = a private non-blocking stream).

@@ -47,6 +47,8 @@ struct MixtureGradients {
     std::vector<Scalar> grad_weights;    // d lnL / d w_k (unconstrained partials)
     Scalar grad_theta[5] = {0, 0, 0, 0, 0};   // AC AT CG CT GT
     std::vector<Scalar> grad_syn_weights;     // d lnL / d rho_m (unconstrained partials)
+    std::vector<Scalar> grad_bg_omegas;       // background classes: d lnL / d omega_bg_j
+    std::vector<Scalar> grad_bg_weights;      // background classes: d lnL / d w_bg_j (unconstrained partials)
     std::vector<Scalar> site_log_likelihoods;
 };
 
@@ -355,9 +357,12 @@ public:
         const std::vector<Scalar>& omegas, const std::vector<Scalar>& weights,
         const std::vector<Scalar>& syn_rates = {1.0}, const std::vector<Scalar>& syn_weights = {1.0},
         const std::vector<bool>* is_test_branch = nullptr, Scalar omega_bg = -1.0,
-        bool want_gradients = true, bool zero_likelihood_sentinel = false, bool direction_gradients = true) {
+        bool want_gradients = true, bool zero_likelihood_sentinel = false, bool direction_gradients = true,
+        const std::vector<Scalar>& bg_omegas = {}, const std::vector<Scalar>& bg_weights = {}) {
         // direction_gradients = false: branch, class-weight and rate-weight gradients only (no
-        // omega / theta directions, so no directional products are installed or evaluated)
+        // omega / theta directions, so no directional products are installed or evaluated).
+        // bg_omegas / bg_weights (non-empty): background branches mix these classes at the P level (the
+        // RELAX and two-set BUSTED models) instead of using the one omega_bg
         auto& eng = gpu_detail::Engine::get();
         const GeneticCode& code = aln.code ? *aln.code : *GeneticCode::universal();
         const int S = code.num_sense_codons, K = int(omegas.size()), M = int(syn_rates.size());
@@ -374,11 +379,19 @@ public:
                 if (!it[i] && int(i) != tree.root_id) has_bg = true;
             }
         }
-        if (has_bg && omega_bg < 0) throw std::runtime_error("mixture: background branches need omega_bg >= 0");
+        const int Kb = has_bg ? (bg_omegas.empty() ? 1 : int(bg_omegas.size())) : 0;
+        if (!bg_omegas.empty() && bg_weights.size() != bg_omegas.size())
+            throw std::runtime_error("mixture: bg_omegas and bg_weights sizes differ");
+        if (has_bg && bg_omegas.empty() && omega_bg < 0) throw std::runtime_error("mixture: background branches need omega_bg >= 0");
         gpu_detail::ModelPack mp;
         std::vector<MG94Parameters> ps;
         for (int k = 0; k < K; ++k) { MG94Parameters p = base; p.alpha = 1.0; p.beta = omegas[size_t(k)]; ps.push_back(p); }
-        if (has_bg) { MG94Parameters p = base; p.alpha = 1.0; p.beta = omega_bg; ps.push_back(p); }
+        for (int j = 0; j < Kb; ++j) {
+            MG94Parameters p = base;
+            p.alpha = 1.0;
+            p.beta = bg_omegas.empty() ? omega_bg : bg_omegas[size_t(j)];
+            ps.push_back(p);
+        }
         const int nm = int(ps.size());
         const size_t SS = size_t(S) * S;
         int ndirs = 0;
@@ -389,11 +402,15 @@ public:
         key = gpu_detail::fnv(key, syn_rates.data(), syn_rates.size() * 8);
         key = gpu_detail::fnv(key, syn_weights.data(), syn_weights.size() * 8);
         key = gpu_detail::fnv(key, it.data(), it.size());
+        if (!bg_omegas.empty()) {
+            key = gpu_detail::fnv(key, bg_omegas.data(), bg_omegas.size() * 8);
+            key = gpu_detail::fnv(key, bg_weights.data(), bg_weights.size() * 8);
+        }
         const bool dirs = want_gradients && direction_gradients;
         const double flags[5] = {omega_bg, double(want_gradients), double(zero_likelihood_sentinel), double(get_precision()),
                                  double(dirs)};
         key = gpu_detail::fnv(key, flags, sizeof(flags));
-        const int n_dirs_expected = dirs ? K + (has_bg ? 1 : 0) + 5 : 0;
+        const int n_dirs_expected = dirs ? K + Kb + 5 : 0;
         if (eng.installed(pr) != key) {
         for (auto& p : ps) mp.add(eng.model(p, aln));
         auto add_dir = [&](int only_model, const std::vector<std::vector<double>>& per_model) {
@@ -407,7 +424,7 @@ public:
             std::vector<std::vector<double>> db(nm);
             for (int k = 0; k < nm; ++k) db[size_t(k)] = gpu_detail::dq_beta(ps[size_t(k)], aln.pos_nuc_frequencies, code);
             for (int k = 0; k < K; ++k) add_dir(k, db);
-            if (has_bg) add_dir(K, db);
+            for (int j = 0; j < Kb; ++j) add_dir(K + j, db);
             for (auto& pr2 : gpu_detail::kThetaPairs) {
                 std::vector<std::vector<double>> dt(nm);
                 for (int k = 0; k < nm; ++k)
@@ -418,7 +435,8 @@ public:
         h3g_model_desc d{};
         d.S = S; d.pi = aln.codon_frequencies_f3x4.data(); d.n_models = nm;
         d.Q = mp.Q.data(); d.lam = mp.lam.data(); d.U = mp.U.data(); d.V = mp.V.data(); d.mu = mp.mu.data();
-        d.K = K; d.class_w = weights.data(); d.has_bg = has_bg ? 1 : 0; d.is_test = it.data();
+        d.K = K; d.class_w = weights.data(); d.has_bg = Kb; d.is_test = it.data();
+        d.bg_w = bg_omegas.empty() ? nullptr : bg_weights.data();
         d.M = M; d.rates = syn_rates.data(); d.rate_w = syn_weights.data(); d.time_mode = H3G_TIME_RAW;
         d.n_dirs = ndirs; d.dQ = ndirs ? mp.dQ.data() : nullptr; d.precision = int(get_precision());
         d.zero_l_sentinel = zero_likelihood_sentinel ? 1 : 0;
@@ -431,6 +449,7 @@ public:
         res.grad_branches.assign(n, 0.0);
         res.grad_weights.assign(size_t(K), 0.0);
         res.grad_syn_weights.assign(size_t(M), 0.0);
+        res.grad_bg_weights.assign(size_t(Kb), 0.0);
         res.site_log_likelihoods.assign(aln.patterns.size(), 0.0);
         std::vector<double> gd(size_t(std::max(ndirs, 1)), 0.0);
         h3g_result r{};
@@ -439,6 +458,7 @@ public:
         r.grad_dir = gd.data();
         r.grad_class_w = res.grad_weights.data();
         r.grad_rate_w = res.grad_syn_weights.data();
+        r.grad_bg_w = Kb ? res.grad_bg_weights.data() : nullptr;
         unsigned want = H3G_WANT_LNL | H3G_WANT_SITE_LNL;
         if (want_gradients) want |= H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL;
         eng.check(h3g_eval(pr, bl.data(), want, &r));
@@ -446,7 +466,8 @@ public:
         if (dirs) {
             res.grad_omegas.assign(gd.begin(), gd.begin() + K);
             size_t q = size_t(K);
-            if (has_bg) res.grad_omega_bg = gd[q++];
+            for (int j = 0; j < Kb; ++j) res.grad_bg_omegas.push_back(gd[q++]);
+            if (Kb) res.grad_omega_bg = res.grad_bg_omegas[0];
             for (int x = 0; x < 5; ++x) res.grad_theta[x] = gd[q++];
         }
         return res;
