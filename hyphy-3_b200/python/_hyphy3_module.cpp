@@ -10,6 +10,7 @@
 #include "hyphy/analyses/busted_gpu.hpp"
 #include "hyphy/analyses/fel_gpu.hpp"
 #include "hyphy/analyses/meme_gpu.hpp"
+#include "hyphy/analyses/relax_gpu.hpp"
 #include "hyphy/opt/optimizer_gpu.hpp"
 #include "hyphy/core/alignment_gpu.hpp"
 #include "hyphy/core/likelihood_gpu.hpp"
@@ -592,4 +593,67 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("num_tested", &MEMEAnalyzer::num_tested)
         .def_readonly("num_background", &MEMEAnalyzer::num_background)
         .def_readonly("site_results", &MEMEAnalyzer::site_results);
+
+    // RELAX (relax.hpp of the reference): settings, fits, result, analyzer
+    using hyphy::analyses::RELAXAnalyzer;
+    using hyphy::analyses::RELAXModelFit;
+    using hyphy::analyses::RELAXRateDistribution;
+    using hyphy::analyses::RELAXResult;
+    using hyphy::analyses::RELAXSettings;
+    py::class_<RELAXSettings>(m, "RELAXSettings")
+        .def(py::init<>())
+        .def_readwrite("p_value_threshold", &RELAXSettings::p_value_threshold)
+        .def_readwrite("refine_branch_lengths", &RELAXSettings::refine_branch_lengths)
+        .def_readwrite("max_iterations", &RELAXSettings::max_iterations)
+        .def_readwrite("tolerance", &RELAXSettings::tolerance);
+    py::class_<RELAXRateDistribution>(m, "RELAXRateDistribution")
+        .def_readonly("omegas", &RELAXRateDistribution::omegas)
+        .def_readonly("weights", &RELAXRateDistribution::weights);
+    py::class_<RELAXModelFit>(m, "RELAXModelFit")
+        .def_readonly("log_likelihood", &RELAXModelFit::log_likelihood)
+        .def_readonly("aicc", &RELAXModelFit::aicc)
+        .def_readonly("parameters", &RELAXModelFit::parameters)
+        .def_readonly("tree_scale", &RELAXModelFit::tree_scale)
+        .def_readonly("k", &RELAXModelFit::k)
+        .def_readonly("realized_cycles", &RELAXModelFit::realized_cycles)
+        .def_readonly("converged", &RELAXModelFit::converged)
+        .def_readonly("reference_distribution", &RELAXModelFit::reference_distribution)
+        .def_readonly("test_distribution", &RELAXModelFit::test_distribution)
+        .def_readonly("branch_lengths", &RELAXModelFit::branch_lengths)
+        .def_readonly("site_log_likelihoods", &RELAXModelFit::site_log_likelihoods);
+    py::class_<RELAXResult>(m, "RELAXResult")
+        .def_readonly("gtr_log_likelihood", &RELAXResult::gtr_log_likelihood)
+        .def_readonly("gtr_aicc", &RELAXResult::gtr_aicc)
+        .def_readonly("gtr_rates", &RELAXResult::gtr_rates)
+        .def_readonly("gtr_branch_lengths", &RELAXResult::gtr_branch_lengths)
+        .def_readonly("mg94_log_likelihood", &RELAXResult::mg94_log_likelihood)
+        .def_readonly("mg94_aicc", &RELAXResult::mg94_aicc)
+        .def_readonly("mg94_omega_R", &RELAXResult::mg94_omega_R)
+        .def_readonly("mg94_omega_T", &RELAXResult::mg94_omega_T)
+        .def_readonly("mg94_branch_lengths", &RELAXResult::mg94_branch_lengths)
+        .def_readonly("alternative_fit", &RELAXResult::alternative_fit)
+        .def_readonly("null_fit", &RELAXResult::null_fit)
+        .def_readonly("lrt", &RELAXResult::lrt)
+        .def_readonly("p_value", &RELAXResult::p_value)
+        .def_readonly("k", &RELAXResult::k)
+        .def_readonly("is_relaxed", &RELAXResult::is_relaxed)
+        .def_readonly("is_intensified", &RELAXResult::is_intensified)
+        .def_readonly("is_significant", &RELAXResult::is_significant)
+        .def_readonly("is_failed", &RELAXResult::is_failed)
+        .def_readonly("error_message", &RELAXResult::error_message)
+        .def_readonly("test_branches", &RELAXResult::test_branches)
+        .def_readonly("reference_branches", &RELAXResult::reference_branches)
+        .def_readonly("runtime_seconds", &RELAXResult::runtime_seconds);
+    py::class_<RELAXAnalyzer>(m, "RELAXAnalyzer")
+        .def(py::init([](Tree t, Alignment a, const RELAXSettings& s) { return RELAXAnalyzer(std::move(t), std::move(a), s); }),
+             "tree"_a, "alignment"_a, "settings"_a = RELAXSettings{})
+        .def_static("create", [](Tree t, Alignment a, const RELAXSettings& s) { return RELAXAnalyzer::create(std::move(t), std::move(a), s); },
+                    "tree"_a, "alignment"_a, "settings"_a = RELAXSettings{})
+        .def("run", [](const RELAXAnalyzer& r) {
+                 py::gil_scoped_release rel;
+                 return r.run();
+             })
+        .def_readonly("test_branch_names", &RELAXAnalyzer::test_branch_names)
+        .def_readonly("ref_branch_names", &RELAXAnalyzer::ref_branch_names)
+        .def_readonly("is_test_branch", &RELAXAnalyzer::is_test_branch);
 }

@@ -121,6 +121,16 @@ def main(ref: str) -> None:
         # tolerances of the reference test
         "tol_gtr": 1.0, "tol_mg94": 0.05, "tol_fit": 2.5, "tol_lrt": 1.5, "max_p": 0.01,
     }
+    # RELAX on Fig4E (tagged test / reference sets) against HyPhy 2.5.101: tests/test_relax.cpp:17-100
+    known["fig4e_relax"] = {
+        "source": "tests/test_relax.cpp:17-100 (Fig4E.nex, embedded tree, {T}/{R} tags; HyPhy 2.5.101 relax, 3 rates)",
+        "num_test": 17, "num_reference": 47,
+        "gtr_log_l": -5317.276, "tol_gtr": 0.5,
+        "max_omega_R": 0.25, "min_omega_T": 0.40,
+        "alt_minus_mg94": 2.18, "tol_alt_minus_mg94": 1.5, "min_alt": -4983.5,
+        "min_null": -5045.16, "max_null": -5000.0,
+        "max_k": 0.01, "lrt": 123.27, "tol_lrt": 8.0, "max_p": 1e-15,
+    }
     # MEME create_and_fit with the full MG94 fit on ADH: tests/test_meme.cpp:145-160 (HyPhy 2.5: -4686.18, 0.0941)
     known["meme_full_fit_adh"] = {
         "source": "tests/test_meme.cpp:145-160 (global_log_l >= -4687.5, |omega - 0.0941| < 0.01)",
