@@ -23,9 +23,9 @@
 // with the likelihood and the gradients in the branch lengths, omegas and class weights from
 // one device mixture evaluation; the synonymous-rate coordinates use central differences of
 // the device likelihood.  Not provided: the error sink (eps_sink must be 0), multiple hits,
-// bridge resolutions, a separate background distribution (background branches keep the
-// global MG94 background omega), the full automatic selector, BUSTED-PH / RELAX modes and the
-// branch-site diagnostics.
+// bridge resolutions, the full automatic selector, BUSTED-PH / RELAX modes and the branch-site
+// diagnostics.  A test set that leaves background branches fits the two-set model (a separate
+// K-class background distribution, busted.hpp:4344-5087).
 #pragma once
 
 #include <algorithm>
@@ -243,19 +243,23 @@ public:
         test.resize(n, true);
         if (tree.root_id >= 0) test[size_t(tree.root_id)] = false;
         std::vector<int32_t> br;
+        bool has_bg = false;
         for (const auto& nd : tree.nodes) {
             if (nd.id == tree.root_id) continue;
-            if (!test[size_t(nd.id)])
-                throw std::runtime_error("BUSTEDAnalyzer (device): background branches (a separate background distribution) are not supported");
+            if (!test[size_t(nd.id)]) has_bg = true;
             br.push_back(nd.id);
         }
         const size_t nb = br.size();
+        // two-set model (busted.hpp:4344-5087): background branches get their own K-class distribution, free in
+        // both the unconstrained and the constrained fit; its coordinates follow the exchangeabilities
+        const size_t n_bom = has_bg ? K : 0, n_bw = has_bg ? K - 1 : 0;
         // coordinates: lengths (log), omegas, class-weight sticks, log rate ratios, rate-weight sticks
         const size_t n_len = refine_branches ? nb : 1;
         const bool last_free = !is_constrained && K >= 2;
         const size_t n_om = K == 1 ? 1 : (K - 1) + (last_free ? 1 : 0);
         const size_t i_om = n_len, i_w = i_om + n_om, i_r = i_w + (K - 1), i_q = i_r + (M - 1), i_th = i_q + (M - 1),
-                     dim = i_th + 5;
+                     i_bom = i_th + 5, i_bw = i_bom + n_bom, dim = i_bw + n_bw;
+        auto bom_is_log = [&](size_t j) { return j == K - 1; };   // K = 1: one free omega on a log scale
         std::vector<Scalar> lb(dim), ub(dim);
         for (size_t i = 0; i < n_len; ++i) {
             lb[i] = std::log(refine_branches ? 1e-8 : 1e-4);
@@ -271,11 +275,16 @@ public:
         for (size_t j = i_w; j < i_r; ++j) { lb[j] = 0.0; ub[j] = 1.0; }
         for (size_t j = i_r; j < i_q; ++j) { lb[j] = std::log(1e-4); ub[j] = std::log(1e4); }
         for (size_t j = i_q; j < i_th; ++j) { lb[j] = 0.0; ub[j] = 1.0; }
-        for (size_t j = i_th; j < dim; ++j) { lb[j] = std::log(1e-4); ub[j] = std::log(1e4); }
+        for (size_t j = i_th; j < i_bom; ++j) { lb[j] = std::log(1e-4); ub[j] = std::log(1e4); }
+        for (size_t j = 0; j < n_bom; ++j) {
+            if (bom_is_log(j)) { lb[i_bom + j] = std::log(K == 1 ? 1e-5 : 1.0); ub[i_bom + j] = std::log(1e4); }
+            else { lb[i_bom + j] = 0.0; ub[i_bom + j] = 1.0; }
+        }
+        for (size_t j = i_bw; j < dim; ++j) { lb[j] = 0.0; ub[j] = 1.0; }
 
         std::vector<Scalar> base_len(n, 0.0);   // the tree-scale mode scales these
         for (int32_t id : br) base_len[size_t(id)] = branch_tau[size_t(id)];
-        struct Point { std::vector<Scalar> bl, om, w, r, q; Scalar scale = 1.0; MG94Parameters base; };
+        struct Point { std::vector<Scalar> bl, om, w, r, q, bom, bw; Scalar scale = 1.0; MG94Parameters base; };
         auto sticks = [](const std::vector<Scalar>& x, size_t off, size_t cnt) {
             std::vector<Scalar> w(cnt + 1);
             Scalar rem = 1.0;
@@ -307,10 +316,16 @@ public:
             pt.base = base_params;
             pt.base.theta_AC = std::exp(x[i_th]); pt.base.theta_AT = std::exp(x[i_th + 1]); pt.base.theta_CG = std::exp(x[i_th + 2]);
             pt.base.theta_CT = std::exp(x[i_th + 3]); pt.base.theta_GT = std::exp(x[i_th + 4]);
+            if (has_bg) {
+                pt.bom.resize(K);
+                for (size_t j = 0; j < K; ++j) pt.bom[j] = bom_is_log(j) ? std::exp(x[i_bom + j]) : x[i_bom + j];
+                pt.bw = sticks(x, i_bw, K - 1);
+            }
             return pt;
         };
         auto encode = [&](const std::vector<Scalar>& bl, Scalar scale, const std::vector<Scalar>& om, const std::vector<Scalar>& w,
-                          const std::vector<Scalar>& r, const std::vector<Scalar>& q, const MG94Parameters& th) {
+                          const std::vector<Scalar>& r, const std::vector<Scalar>& q, const MG94Parameters& th,
+                          const std::vector<Scalar>& bom = {}, const std::vector<Scalar>& bw = {}) {
             std::vector<Scalar> x(dim, 0.0);
             if (refine_branches) for (size_t i = 0; i < nb; ++i) x[i] = std::log(std::max<Scalar>(bl[size_t(br[i])], 1e-8));
             else x[0] = std::log(scale);
@@ -320,13 +335,20 @@ public:
             to_sticks(q, x, i_q);
             const Scalar t5[5] = {th.theta_AC, th.theta_AT, th.theta_CG, th.theta_CT, th.theta_GT};
             for (size_t j = 0; j < 5; ++j) x[i_th + j] = std::log(std::max<Scalar>(t5[j], 1e-300));
+            if (has_bg) {
+                for (size_t j = 0; j < K; ++j) {
+                    const Scalar v = j < bom.size() ? bom[j] : 1.0;
+                    x[i_bom + j] = bom_is_log(j) ? std::log(std::max<Scalar>(v, 1e-300)) : v;
+                }
+                if (bw.size() == K) to_sticks(bw, x, i_bw);
+            }
             for (size_t j = 0; j < dim; ++j) x[j] = std::clamp(x[j], lb[j], ub[j]);
             return x;
         };
         auto evaluate = [&](const Point& pt, bool grads) {
             return hyphy::core::LikelihoodEngine::compute_mixture_gradients(
                 tree, aln, pt.base, pt.bl, pt.om, pt.w, pt.r, pt.q, &test, -1.0, grads,
-                /*zero_likelihood_sentinel=*/true, /*direction_gradients=*/grads);
+                /*zero_likelihood_sentinel=*/true, /*direction_gradients=*/grads, pt.bom, pt.bw);
         };
         // objective -lnL and its gradient in the coordinates above
         auto fg = [&](const std::vector<Scalar>& x, std::vector<Scalar>& g) -> Scalar {
@@ -342,15 +364,22 @@ public:
             }
             for (size_t j = 0; j < n_om; ++j) g[i_om + j] = -(om_is_log(j) ? pt.om[j] : 1.0) * r.grad_omegas[j];
             // w_k = R_k p_k (k < K-1), w_{K-1} = R_{K-1}, R_k = prod_{i<k} (1 - p_i)
-            for (size_t j = 0; j + 1 < K; ++j) {
-                Scalar d = 0.0;
-                for (size_t k = j; k < K; ++k) {
-                    Scalar dw = 1.0;
-                    for (size_t i = 0; i < k; ++i) dw *= (i == j) ? -1.0 : (1.0 - x[i_w + i]);
-                    if (k + 1 < K && k != j) dw *= x[i_w + k];
-                    d += r.grad_weights[k] * dw;
+            auto stick_grad = [&](size_t off, const std::vector<Scalar>& gw) {
+                for (size_t j = 0; j + 1 < K; ++j) {
+                    Scalar d = 0.0;
+                    for (size_t k = j; k < K; ++k) {
+                        Scalar dw = 1.0;
+                        for (size_t i = 0; i < k; ++i) dw *= (i == j) ? -1.0 : (1.0 - x[off + i]);
+                        if (k + 1 < K && k != j) dw *= x[off + k];
+                        d += gw[k] * dw;
+                    }
+                    g[off + j] = -d;
                 }
-                g[i_w + j] = -d;
+            };
+            stick_grad(i_w, r.grad_weights);
+            if (has_bg) {
+                for (size_t j = 0; j < K; ++j) g[i_bom + j] = -(bom_is_log(j) ? pt.bom[j] : 1.0) * r.grad_bg_omegas[j];
+                stick_grad(i_bw, r.grad_bg_weights);
             }
             // rate-weight sticks, exactly: r_m = r~_m / sum_k rho_k r~_k, and sum_m r_m dlnL/dr_m (at fixed rho) equals
             // sum_b t_b dlnL/dt_b (every rate scales every branch), so
@@ -392,10 +421,23 @@ public:
         else if (M == 3) { r0 = {0.3, 1.0, 3.1}; q0 = {0.3, 0.6, 0.1}; }
         else if (M >= 4) for (size_t m = 0; m < M; ++m) r0[m] = 0.15 * std::pow(25.0, Scalar(m) / Scalar(M - 1));
         const Scalar om_mg = std::clamp(mg94_omega, 0.05, 0.9);
+        std::vector<Scalar> bom0, bw0;
+        if (has_bg) {
+            const Scalar obg = std::clamp(mg94_background_omega >= 0.0 ? mg94_background_omega : mg94_omega, 0.01, 0.9);
+            if (K == 1) { bom0 = {obg}; bw0 = {1.0}; }
+            else {
+                for (size_t k = 0; k + 1 < K; ++k) {
+                    bom0.push_back(K == 2 ? obg : 0.05 + (obg - 0.05) * Scalar(k) / Scalar(K - 2));
+                    bw0.push_back(0.95 / Scalar(K - 1));
+                }
+                bom0.push_back(1.5);
+                bw0.push_back(0.05);
+            }
+        }
         std::vector<std::vector<Scalar>> starts;
         if (K == 1) {
             starts.push_back(encode(base_len, 1.0, {is_constrained ? std::min<Scalar>(1.0, mg94_omega) : std::max<Scalar>(mg94_omega, 1e-5)},
-                                    {1.0}, r0, q0, base_params));
+                                    {1.0}, r0, q0, base_params, bom0, bw0));
         } else {
             const Scalar lo[5] = {0.1, 0.01, 0.0, 0.05, 0.0}, hi[5] = {0.5, om_mg, 0.3, 0.8, 0.1},
                          top[5] = {2.0, 3.0, 1.5, 10.0, 2.0}, wtop[5] = {0.1, 0.1, 0.2, 0.05, 0.5};
@@ -407,7 +449,7 @@ public:
                 }
                 om[K - 1] = is_constrained ? 1.0 : top[j];
                 w[K - 1] = wtop[j];
-                starts.push_back(encode(base_len, 1.0, om, w, r0, q0, base_params));
+                starts.push_back(encode(base_len, 1.0, om, w, r0, q0, base_params, bom0, bw0));
             }
         }
         if (warm_start_fit && warm_start_fit->test_distribution.omegas.size() == K) {
@@ -420,7 +462,9 @@ public:
             const auto& bl = warm_start_fit->branch_lengths.size() == n ? warm_start_fit->branch_lengths : base_len;
             starts.push_back(encode(bl, warm_start_fit->tree_scale, om, d.weights, rates_fit ? d.syn_rates : r0,
                                     rates_fit ? d.syn_weights : q0,
-                                    warm_start_fit->has_gtr_params ? warm_start_fit->gtr_params : base_params));
+                                    warm_start_fit->has_gtr_params ? warm_start_fit->gtr_params : base_params,
+                                    warm_start_fit->background_distribution.omegas.size() == K ? warm_start_fit->background_distribution.omegas : bom0,
+                                    warm_start_fit->background_distribution.weights.size() == K ? warm_start_fit->background_distribution.weights : bw0));
         }
         hyphy::opt::BoxLBFGSResult best;
         best.f = std::numeric_limits<Scalar>::infinity();
@@ -452,6 +496,16 @@ public:
         for (size_t k = 0; k < K; ++k) idx[k] = k;
         if (K > 2) std::sort(idx.begin(), idx.end() - 1, [&](size_t a, size_t b) { return pt.om[a] < pt.om[b]; });
         for (size_t k : idx) { fit.test_distribution.omegas.push_back(pt.om[k]); fit.test_distribution.weights.push_back(pt.w[k]); }
+        if (has_bg) {
+            std::vector<size_t> ib(K);
+            for (size_t k = 0; k < K; ++k) ib[k] = k;
+            if (K > 2) std::sort(ib.begin(), ib.end() - 1, [&](size_t a, size_t b) { return pt.bom[a] < pt.bom[b]; });
+            fit.has_background_distribution = true;
+            for (size_t k : ib) {
+                fit.background_distribution.omegas.push_back(pt.bom[k]);
+                fit.background_distribution.weights.push_back(pt.bw[k]);
+            }
+        }
         if (srv) {
             std::vector<size_t> im(M);
             for (size_t m = 0; m < M; ++m) im[m] = m;
@@ -467,7 +521,7 @@ public:
                 ann[k] = "Rate classes " + std::to_string(k) + " and " + std::to_string(k + 1) + " collapsed into identical omega";
         // busted.hpp:2598-2605: 5 exchangeabilities + 9 frequency parameters, lengths (or a scale), mixture and
         // synonymous-rate parameters; N = codons x taxa
-        const size_t n_mix = (2 * K - 1) - (is_constrained && K >= 2 ? 1 : 0);
+        const size_t n_mix = (2 * K - 1) - (is_constrained && K >= 2 ? 1 : 0) + (has_bg ? 2 * K - 1 : 0);
         const size_t k_params = 14 + (refine_branches ? nb : 1) + n_mix + (srv ? 2 * (M - 1) : 0);
         fit.aicc = hyphy::opt::compute_aicc(fit.log_likelihood, k_params, aln.num_codons * aln.num_taxa);
         return fit;
@@ -498,8 +552,6 @@ public:
         is_test_branch = sel.is_selected;
         num_test_branches = sel.num_selected;
         num_background_branches = sel.num_unselected;
-        if (num_background_branches > 0)
-            throw std::runtime_error("BUSTEDAnalyzer (device): a test set with background branches (two-set BUSTED) is not supported");
         BUSTEDResult res;
         res.settings = settings;
         const size_t K = std::max<size_t>(1, settings.num_rate_classes);
@@ -565,11 +617,16 @@ public:
             const auto& u = res.unconstrained.test_distribution;
             std::vector<Scalar> om = u.omegas;
             om.back() = std::min<Scalar>(1.0, om.back());
-            std::vector<Scalar> clamped;
-            evaluate_log_l(1.0, om, u.weights, u.syn_rates.empty() ? std::vector<Scalar>{1.0} : u.syn_rates,
-                           u.syn_weights.empty() ? std::vector<Scalar>{1.0} : u.syn_weights, &res.unconstrained.branch_lengths,
-                           &clamped, 0.0, 0.0, 0.0,
-                           res.unconstrained.has_gtr_params ? &res.unconstrained.gtr_params : nullptr);
+            const auto& uf = res.unconstrained;
+            std::vector<bool> test(is_test_branch);
+            test.resize(tree.num_nodes(), true);
+            if (tree.root_id >= 0) test[size_t(tree.root_id)] = false;
+            const auto cl = hyphy::core::LikelihoodEngine::compute_mixture_gradients(
+                tree, aln, uf.has_gtr_params ? uf.gtr_params : base_params, uf.branch_lengths, om, u.weights,
+                u.syn_rates.empty() ? std::vector<Scalar>{1.0} : u.syn_rates,
+                u.syn_weights.empty() ? std::vector<Scalar>{1.0} : u.syn_weights, &test, -1.0, false,
+                /*zero_likelihood_sentinel=*/true, false, uf.background_distribution.omegas, uf.background_distribution.weights);
+            const std::vector<Scalar>& clamped = cl.site_log_likelihoods;
             for (size_t st = 0; st < n_sites; ++st) {
                 const size_t p = size_t(aln.site_to_pattern[st]);
                 const Scalar alt = res.unconstrained.site_log_likelihoods[p];

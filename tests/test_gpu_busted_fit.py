@@ -103,6 +103,28 @@ def test_busted_rejects_unsupported_modes(cd2_busted):
     with pytest.raises(Exception):
         cd2_busted.run(s)
     s = h3.BUSTEDSettings()
-    s.test_branches = "Internal"
+    s.relax_mode = True
     with pytest.raises(Exception):
         cd2_busted.run(s)
+
+
+def test_busted_two_set_cd2(cd2_busted, golden_dir):
+    """A test set that leaves background branches (busted.hpp:6413-6460): both fits carry a free 3-class
+    background distribution; only the test set's last omega is held at 1 under the null."""
+    import _hyphy3 as h3
+    s = h3.BUSTEDSettings()
+    s.test_branches = "Human,Chimp,Baboon,RhMonkey,Node3,Node2"
+    res = cd2_busted.run(s)
+    assert cd2_busted.num_background_branches > 0
+    _check_fit_structure(res, 187)
+    for fit in (res.unconstrained, res.constrained):
+        b = fit.background_distribution
+        assert fit.has_background_distribution and len(b.omegas) == 3
+        assert all(0.0 <= o <= 1.0 for o in b.omegas[:2]) and b.omegas[2] >= 1.0
+        assert sum(b.weights) == pytest.approx(1.0, abs=1e-12)
+        w = np.asarray(h3.Alignment.load(str(golden_dir / "cd2.fna")).pattern_arrays()[2], dtype=float)
+        assert float(np.dot(w, fit.site_log_likelihoods)) == pytest.approx(fit.log_likelihood, rel=1e-12)
+    # the two-set alternative is at least as good as the one-set alternative restricted to the test branches'
+    # classes on every branch (the background distribution can take the test distribution's values)
+    one = cd2_busted.run()
+    assert res.unconstrained.log_likelihood >= one.unconstrained.log_likelihood - 0.5
