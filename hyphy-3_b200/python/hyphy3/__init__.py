@@ -1,11 +1,10 @@
 """HyPhy 3 likelihood core on NVIDIA B200.
 
-Re-exports the core types and likelihood entry points of the reference
-package (python/hyphy3/__init__.py) from the device-backed _hyphy3 module.
-Of the analysis drivers, FELAnalyzer and MEMEAnalyzer (every branch tested),
-MG94Fitter and the likelihood core of BUSTEDAnalyzer (evaluate_log_l and the
-EM expectation steps) run on the device; the others (BUSTED's fit driver,
-aBSREL, RELAX, ...) are not part of this package.
+Re-exports the core types, the likelihood entry points and the analysis drivers of the
+reference package (python/hyphy3/__init__.py) that run on the device from the _hyphy3 module:
+FELAnalyzer, MEMEAnalyzer, BUSTEDAnalyzer (fits, two-set model, auto K), RELAXAnalyzer,
+MG94Fitter, GTRFitter and the GTR likelihood.  aBSREL, FUBAR and the other drivers are not
+part of this package.
 """
 import os
 import sys
@@ -18,6 +17,21 @@ if _pydir not in sys.path:
 from _hyphy3 import (  # noqa: E402
     Alignment,
     BUSTEDAnalyzer,
+    BUSTEDFit,
+    BUSTEDRateDistribution,
+    BUSTEDResult,
+    BUSTEDSettings,
+    GTRFitResult,
+    GTRFitter,
+    GTRMatrix,
+    GTRParameters,
+    RELAXAnalyzer,
+    RELAXModelFit,
+    RELAXRateDistribution,
+    RELAXResult,
+    RELAXSettings,
+    compute_gtr_gradients,
+    compute_gtr_log_likelihood,
     FELAnalyzer,
     FELSettings,
     FELSiteResult,
@@ -48,5 +62,8 @@ __all__ = [
     "Alignment", "FELAnalyzer", "FELSettings", "FELSiteResult", "FitResult", "MG94Fitter", "GeneticCode", "MG94Parameters", "Tree", "TreeNode", "build_leaf_to_taxon_map",
     "compute_branch_length_gradients", "compute_joint_frechet_gradients", "compute_mg94_log_likelihood",
     "compute_mixture_gradients", "compute_tree_log_likelihood_from_P", "get_precision", "library_version",
-    "mg94_eigensystem", "set_precision", "autograd",
+    "mg94_eigensystem", "set_precision", "autograd", "MEMEAnalyzer", "MEMESiteResult", "BUSTEDAnalyzer", "BUSTEDFit",
+    "BUSTEDRateDistribution", "BUSTEDResult", "BUSTEDSettings", "GTRFitResult", "GTRFitter", "GTRMatrix", "GTRParameters",
+    "RELAXAnalyzer", "RELAXModelFit", "RELAXRateDistribution", "RELAXResult", "RELAXSettings", "compute_gtr_gradients",
+    "compute_gtr_log_likelihood",
 ]

@@ -100,3 +100,14 @@ def test_gpu_entry_points_fail_loudly_without_device(h3, golden_dir):
     t = h3.Tree.from_newick((golden_dir / "cd2_reduced.nwk").read_text())
     with pytest.raises(RuntimeError, match="libh3g"):
         h3.compute_branch_length_gradients(t, a, h3.MG94Parameters())
+
+
+def test_package_exports_the_device_drivers():
+    """hyphy3 re-exports the reference package's names for everything that runs on the device
+    (python/hyphy3/__init__.py of the reference), and every name in __all__ resolves."""
+    import hyphy3
+    for name in hyphy3.__all__:
+        assert hasattr(hyphy3, name), name
+    for name in ("FELAnalyzer", "MEMEAnalyzer", "BUSTEDAnalyzer", "BUSTEDSettings", "BUSTEDResult", "RELAXAnalyzer",
+                 "RELAXSettings", "GTRFitter", "MG94Fitter", "compute_gtr_log_likelihood"):
+        assert name in hyphy3.__all__, name
