@@ -506,6 +506,12 @@ PYBIND11_MODULE(_hyphy3, m) {
         .def_readonly("gtr_rates", &BUSTEDAnalyzer::gtr_rates)
         .def_readonly("gtr_branch_lengths", &BUSTEDAnalyzer::gtr_branch_lengths)
         .def_readonly("num_background_branches", &BUSTEDAnalyzer::num_background_branches)
+        .def("select_test_branches", [](const BUSTEDAnalyzer& b, const std::string& spec) {
+                 auto sel = b.tree.select_branches(spec, "", {}, false);
+                 b.is_test_branch = sel.is_selected;
+                 b.num_test_branches = sel.num_selected;
+                 b.num_background_branches = sel.num_unselected;
+             }, "spec"_a)
         .def_readwrite("branch_tau", &BUSTEDAnalyzer::branch_tau)
         .def_readwrite("is_test_branch", &BUSTEDAnalyzer::is_test_branch)
         .def_readwrite("num_test_branches", &BUSTEDAnalyzer::num_test_branches)
@@ -523,6 +529,21 @@ PYBIND11_MODULE(_hyphy3, m) {
                  return py::make_tuple(l, pll);
              }, "s"_a, "omegas"_a, "weights"_a, "syn_rates"_a = VecS{1.0}, "syn_weights"_a = VecS{1.0},
              "custom_branch_lengths"_a = std::nullopt, "delta"_a = 0.0, "psi"_a = 0.0)
+        .def("evaluate_two_set_log_l", [](const BUSTEDAnalyzer& b, Scalar s, const VecS& omegas_test, const VecS& weights_test,
+                                          const VecS& omegas_bg, const VecS& weights_bg, const VecS& syn_rates,
+                                          const VecS& syn_weights, std::optional<VecS> custom,
+                                          std::optional<MG94Parameters> custom_base) {
+                 VecS pll;
+                 Scalar l;
+                 {
+                     py::gil_scoped_release rel;
+                     l = b.evaluate_two_set_log_l(s, omegas_test, weights_test, omegas_bg, weights_bg, syn_rates, syn_weights,
+                                                  custom ? &*custom : nullptr, &pll, 0.0, 0.0, 0.0, 0.0, nullptr, nullptr,
+                                                  custom_base ? &*custom_base : nullptr);
+                 }
+                 return py::make_tuple(l, pll);
+             }, "s"_a, "omegas_test"_a, "weights_test"_a, "omegas_bg"_a, "weights_bg"_a, "syn_rates"_a = VecS{1.0},
+             "syn_weights"_a = VecS{1.0}, "custom_branch_lengths"_a = std::nullopt, "custom_base_params"_a = std::nullopt)
         .def("compute_expected_weights", [](const BUSTEDAnalyzer& b, Scalar s, const VecS& omegas, const VecS& weights,
                                             const VecS& syn_rates, const VecS& syn_weights, std::optional<VecS> custom,
                                             Scalar delta, Scalar psi) {

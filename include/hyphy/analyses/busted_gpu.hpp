@@ -166,6 +166,37 @@ public:
         return r.log_likelihood;
     }
 
+    // busted.hpp:3146-3378 (no error sinks, no unclassified set): test branches mix (omegas_test, weights_test),
+    // every other branch (omegas_bg, weights_bg); lengths s x branch_tau or s x custom_branch_lengths (raw time)
+    Scalar evaluate_two_set_log_l(Scalar s, const std::vector<Scalar>& omegas_test, const std::vector<Scalar>& weights_test,
+                                  const std::vector<Scalar>& omegas_bg, const std::vector<Scalar>& weights_bg,
+                                  const std::vector<Scalar>& syn_rates = {1.0}, const std::vector<Scalar>& syn_weights = {1.0},
+                                  const std::vector<Scalar>* custom_branch_lengths = nullptr,
+                                  std::vector<Scalar>* out_pattern_ll = nullptr, Scalar delta = 0.0, Scalar psi = 0.0,
+                                  Scalar eps_sink_test = 0.0, Scalar eps_sink_bg = 0.0,
+                                  const std::vector<Scalar>* omegas_unclass = nullptr,
+                                  const std::vector<Scalar>* weights_unclass = nullptr,
+                                  const MG94Parameters* custom_base_params = nullptr) const {
+        if (eps_sink_test != 0.0 || eps_sink_bg != 0.0 || omegas_unclass || weights_unclass)
+            throw std::runtime_error("BUSTEDAnalyzer (device): error sinks and an unclassified set are not supported");
+        MG94Parameters base = custom_base_params ? *custom_base_params : base_params;
+        base.delta = delta;
+        base.psi = psi;
+        const size_t n = tree.num_nodes();
+        std::vector<Scalar> bl(n, 0.0);
+        for (const auto& node : tree.nodes)
+            if (node.id != tree.root_id)
+                bl[size_t(node.id)] = s * (custom_branch_lengths ? (*custom_branch_lengths)[size_t(node.id)] : branch_tau[size_t(node.id)]);
+        std::vector<bool> test(is_test_branch);
+        test.resize(n, true);
+        if (tree.root_id >= 0) test[size_t(tree.root_id)] = false;
+        const auto r = hyphy::core::LikelihoodEngine::compute_mixture_gradients(
+            tree, aln, base, bl, omegas_test, weights_test, syn_rates, syn_weights, &test, -1.0, false,
+            /*zero_likelihood_sentinel=*/true, false, omegas_bg, weights_bg);
+        if (out_pattern_ll) *out_pattern_ll = r.site_log_likelihoods;
+        return r.log_likelihood;
+    }
+
     // busted.hpp:662-975 (eps_sink = 0): the E-step for the omega-class weights
     std::vector<Scalar> compute_expected_weights(Scalar s, const std::vector<Scalar>& omegas, const std::vector<Scalar>& weights,
                                                  const std::vector<Scalar>& syn_rates = {1.0},

@@ -124,6 +124,14 @@ def test_busted_two_set_cd2(cd2_busted, golden_dir):
         assert sum(b.weights) == pytest.approx(1.0, abs=1e-12)
         w = np.asarray(h3.Alignment.load(str(golden_dir / "cd2.fna")).pattern_arrays()[2], dtype=float)
         assert float(np.dot(w, fit.site_log_likelihoods)) == pytest.approx(fit.log_likelihood, rel=1e-12)
+    # busted.hpp:3146: the two-set likelihood at the fitted parameters reproduces the fit (lnL and per pattern)
+    u = res.unconstrained
+    cd2_busted.select_test_branches("Human,Chimp,Baboon,RhMonkey,Node3,Node2")
+    lnl, pll = cd2_busted.evaluate_two_set_log_l(
+        1.0, list(u.test_distribution.omegas), list(u.test_distribution.weights), list(u.background_distribution.omegas),
+        list(u.background_distribution.weights), custom_branch_lengths=list(u.branch_lengths), custom_base_params=u.gtr_params)
+    assert lnl == pytest.approx(u.log_likelihood, rel=1e-12)
+    np.testing.assert_allclose(pll, u.site_log_likelihoods, rtol=1e-12, atol=1e-12)
     # the two-set alternative is at least as good as the one-set alternative restricted to the test branches'
     # classes on every branch (the background distribution can take the test distribution's values)
     one = cd2_busted.run()
