@@ -103,9 +103,15 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
+            # nvidia-smi takes a moment to start: wait (bounded) for its first sample, then drop it,
+            # so the samples kept are the ones taken while the timed region runs
+            t_end = time.time() + 3.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except OSError:
             self.proc = None
 
@@ -195,60 +201,93 @@ def stage_work(aln_P: int, tree, M: int, elem_bytes: int = 8) -> dict:
             "accum_A": (acc_b * cols, acc_f * cols)}
 
 
-def cpu_baseline(wl, reps: int = 3, max_sites: int | None = None) -> dict:
-    """The CPU restatement of the reference engine on the host cores (all threads)."""
-    import h3oracle as o
-    nsite = wl.n_sites if max_sites is None else min(max_sites, wl.n_sites)
-    seqs = [sq[:3 * nsite] for sq in wl.seqs]
-    a = o.Alignment.from_sequences(wl.names, seqs)
-    t = o.Tree.parse(wl.newick)
-    cls = [{"alpha": 1.0, "beta": om, "theta": wl.theta} for om in wl.omegas]
-    rates, rw = (list(wl.rates), list(wl.rate_w)) if len(wl.rates) > 1 else ([], [])
-    threads = o.max_threads()
-    o.set_threads(threads)
-    bl = list(t.branch_lengths)
-    o.mixture_eval(t, a, cls, wl.omega_w, None, [], rates, rw, bl, False, True, False)
+def load_simulate():
+    """hyphy3/simulate.py loaded by file path: the workload generator is plain numpy, and loading it
+    this way keeps the hyphy3 package (and with it the CUDA library) out of the CPU-only legs."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("h3_simulate", ROOT / "hyphy-3_b200" / "python" / "hyphy3" / "simulate.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["h3_simulate"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# patterns per CPU step: the whole 64-taxon alignment; a 384-pattern slice of the 1024-taxon one
+# (about 3 s per evaluation on 16 host threads)
+CPU_SAMPLE_PATTERNS = {1: None, 3: 384}
+
+
+class CpuEngine:
+    """The CPU restatement of the reference engine (oracle/, FP64, OpenMP on every host thread) in the
+    reference's batched shape: 64-pattern tiles, S x 64 products per branch (likelihood.hpp:1151-1197),
+    on the workload's tree and classes and a bounded slice of its site patterns."""
+
+    def __init__(self, wl, max_patterns: int | None):
+        import h3oracle as o
+        self.o = o
+        a = o.Alignment.from_sequences(wl.names, wl.seqs)
+        self.full_patterns = a.num_patterns
+        if max_patterns is not None and max_patterns < self.full_patterns:
+            a = a.subset_patterns(0, max_patterns)
+        self.a = a
+        self.t = o.Tree.parse(wl.newick)
+        self.cls = [{"alpha": 1.0, "beta": om, "theta": list(wl.theta)} for om in wl.omegas]
+        self.w = list(wl.omega_w)
+        self.rates, self.rw = (list(wl.rates), list(wl.rate_w)) if len(wl.rates) > 1 else ([], [])
+        self.threads = o.max_threads()
+        o.set_threads(self.threads)
+        self.bl = list(self.t.branch_lengths)
+        self.sites = float(np.sum(a.weights))
+        self.branches = self.t.num_nodes() - 1
+        self.patterns = len(a.weights)
+
+    def step(self) -> float:
+        return self.o.mixture_eval(self.t, self.a, self.cls, self.w, None, [], self.rates, self.rw, self.bl,
+                                   False, True, False, True)["lnl"]
+
+    def sample_text(self, n_steps: int, what: str) -> str:
+        return (f"{n_steps} {what}: lnL + gradients w.r.t. every branch length, omega, class weight, theta and rate "
+                f"weight over {self.patterns} of {self.full_patterns} site patterns ({self.sites:.0f} sites) x "
+                f"{self.branches} branches, oracle/ CPU restatement in 64-pattern tiles (the reference itself needs "
+                f"Eigen 3.4, absent from this image)")
+
+
+def cpu_baseline(wl, config: int, reps: int = 3) -> dict:
+    """The CPU restatement on the host cores (all threads), a bounded sample of the workload."""
+    eng = CpuEngine(wl, CPU_SAMPLE_PATTERNS.get(config))
+    eng.step()
     times = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        o.mixture_eval(t, a, cls, wl.omega_w, None, [], rates, rw, bl, False, True, False)
+        eng.step()
         times.append(time.perf_counter() - t0)
-    units = nsite * (t.num_nodes() - 1)
     med = statistics.median(times)
-    what = "full evaluations" if nsite == wl.n_sites else f"evaluations of the first {nsite} of {wl.n_sites} sites"
-    return {"value": units / med, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{reps} {what} (lnL + all gradients, x {t.num_nodes() - 1} branches) after 1 warm-up, "
-                      f"median {med:.3f} s"}
+    return {"value": eng.sites * eng.branches / med, "unit": UNIT, "cores": eng.threads, "kind": "port",
+            "sample": eng.sample_text(reps, f"evaluations after 1 warm-up, median {med:.3f} s")}
 
 
 def run_reference(args) -> None:
+    """The reference arm: the CPU restatement of the reference engine on every host thread (rank 0 only),
+    exactly --warmup untimed and --steps timed evaluations of the configured workload's sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    _, wl, _, _ = build_inputs()
-    import h3oracle as o
-    a = o.Alignment.from_sequences(wl.names, wl.seqs)
-    t = o.Tree.parse(wl.newick)
-    cls = [{"alpha": 1.0, "beta": om, "theta": wl.theta} for om in wl.omegas]
-    threads = o.max_threads()
-    o.set_threads(threads)
-    bl = list(t.branch_lengths)
-    for _ in range(max(1, min(args.warmup, 2))):
-        o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
-    steps = max(1, min(args.steps, 5))
+    sim = load_simulate()
+    wl = sim.make_workload(args.config)
+    eng = CpuEngine(wl, CPU_SAMPLE_PATTERNS.get(args.config))
+    for _ in range(args.warmup):
+        eng.step()
     t0 = time.perf_counter()
-    for _ in range(steps):
-        o.mixture_eval(t, a, cls, wl.omega_w, None, [], [], [], bl, False, True, False)
-    dt = (time.perf_counter() - t0) / steps
-    units = wl.n_sites * (t.num_nodes() - 1)
-    v = units / dt
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+    for _ in range(args.steps):
+        eng.step()
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    v = eng.sites * eng.branches / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sites": wl.n_sites, "branches": t.num_nodes() - 1},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{steps} full evaluations after warm-up (reference engine restated in C++/OpenMP: "
-                                       "the reference itself needs Eigen 3.4, absent from this image)"},
+            "config": {"workload": WORKLOADS[args.config], "sites": wl.n_sites, "branches": eng.branches},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": eng.threads, "kind": "port",
+                             "sample": eng.sample_text(args.steps, "timed evaluations")},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -307,10 +346,12 @@ def run_ours(args) -> None:
 
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
-    def device_timed(steps, warmup):
+    def device_timed(steps, warmup, sampler=None):
         for _ in range(warmup):
             pr.eval_resident(want)
         torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         if dist:
             dist.barrier()
@@ -330,9 +371,7 @@ def run_ours(args) -> None:
     for prec_name, code in ([("fp64", _capi.PREC_FP64)] + ([("mixed", _capi.PREC_MIXED)] if precision == "mixed" else [])):
         install(code)
         sampler = ClockSampler(local) if prec_name == precision else None
-        if sampler:
-            sampler.start()
-        secs = device_timed(args.steps, max(args.warmup, 3))
+        secs = device_timed(args.steps, max(args.warmup, 3), sampler)
         clocks = sampler.stop() if sampler else None
         t = torch.tensor([secs], dtype=torch.float64, device="cuda")
         if dist:
@@ -397,8 +436,7 @@ def run_ours(args) -> None:
             fl = work64[k][1] / (f_st[k][0] * 1e-3) / 1e12
             fp64_pipe[k] = {"tflops": fl, "frac_of_dgemm": fl / fp64_peak if fp64_peak else None, "ms": f_st[k][0]}
 
-    cpu = (cpu_baseline(wl, max_sites=None if args.config == 1 else 24)
-           if (rank == 0 and world == 1 and not args.no_cpu) else None)
+    cpu = cpu_baseline(wl, args.config) if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -890,16 +928,16 @@ def run_profile(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["auto", "fp64", "mixed"], default="auto")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true", help="device evaluations only (for ncu)")
     ap.add_argument("--sites", type=int, default=None, help="shrink the alignment to this many codons (--profile; --config 2)")
-    ap.add_argument("--config", type=int, choices=[1, 2, 3], default=1,
-                    help="1: 64-taxon 3-omega mixture (headline); 2: FEL per-site fits, 256 taxa x 2000 codons; "
-                         "3: 1024-taxon, 4 rate x 2 omega classes")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3], default=3,
+                    help="1: 64-taxon 3-omega mixture; 2: FEL per-site fits, 256 taxa x 2000 codons; "
+                         "3: 1024-taxon, 4 rate x 2 omega classes (headline: the largest single-GPU workload)")
     ap.add_argument("--analysis", choices=["fel", "meme", "compress", "gtr"], default="fel",
                     help="--config 2: which per-site analysis; compress: alignment finalize on the device; "
                          "gtr: nucleotide GTR likelihood (both any config)")

@@ -68,11 +68,8 @@ def build(force: bool = False) -> dict[str, pathlib.Path]:
     ext = sysconfig.get_config_var("EXT_SUFFIX")
     mod = PYDIR / f"_hyphy3{ext}"
     mod_src = PYDIR / "_hyphy3_module.cpp"
-    mod_deps = [mod_src, lib, ROOT / "include" / "hyphy" / "core" / "likelihood_gpu.hpp",
-                ROOT / "include" / "hyphy" / "analyses" / "fel_gpu.hpp",
-                ROOT / "include" / "hyphy" / "analyses" / "meme_gpu.hpp",
-                ROOT / "include" / "hyphy" / "analyses" / "busted_gpu.hpp", ROOT / "include" / "hyphy" / "opt" / "optimizer_gpu.hpp",
-                ROOT / "include" / "hyphy" / "core" / "h3_host.hpp", ROOT / "include" / "h3g.h"]
+    # every host header the module compiles against (shims, analyses, optimisers)
+    mod_deps = [mod_src, lib, ROOT / "include" / "h3g.h"] + sorted((ROOT / "include" / "hyphy").rglob("*.hpp"))
     if force or _stale(mod, mod_deps):
         import pybind11
         _run([HOSTCXX, "-O2", "-std=c++20", "-fPIC", "-shared", "-Wall", "-Wno-unused-parameter",

@@ -64,6 +64,7 @@ struct h3g_problem {
     int4* d_out_info = nullptr;
     int* d_chains = nullptr;           // [in_next | in_heads | out_next | out_heads]
     int n_in_heads = 0, n_out_heads = 0;
+    WaitCfg wait;                     // flag-wait limit of the persistent mixed passes
     size_t off_in_heads = 0, off_out_next = 0, off_out_heads = 0;
     int8_t* d_states = nullptr;
     uint64_t* d_masks = nullptr;
@@ -702,7 +703,7 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
     int l = 0;
     if (mixed) {
         // one persistent launch over every level, per-tile dependencies
-        l = launch_inside_mixed(t, md, w, pr->mw, pr->n_in_heads, s);
+        l = launch_inside_mixed(t, md, w, pr->mw, pr->n_in_heads, pr->wait, s);
     } else {
         for (size_t lv = 0; lv + 1 < pr->in_off.size(); ++lv) {
             const int cnt = pr->in_off[lv + 1] - pr->in_off[lv];
@@ -715,7 +716,7 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
     if (grads) {
         l = 0;
         if (mixed) {
-            l = launch_outside_mixed(t, md, w, pr->mw, pr->n_out_heads, s);
+            l = launch_outside_mixed(t, md, w, pr->mw, pr->n_out_heads, pr->wait, s);
         } else {
             for (size_t lv = 0; lv + 1 < pr->out_off.size(); ++lv) {
                 const int cnt = pr->out_off[lv + 1] - pr->out_off[lv];
@@ -845,6 +846,17 @@ static h3g_status check_bl(h3g_problem* pr, const double* bl) {
     return H3G_OK;
 }
 
+// A bounded device wait expired during the evaluation just read back: clear the device's sticky
+// error word (so the next evaluation on this problem starts clean) and report H3G_ERR_TIMEOUT.
+static h3g_status timed_out(h3g_problem* pr) {
+    h3g_ctx* ctx = pr->ctx;
+    if (pr->w.err) {
+        cudaMemsetAsync(pr->w.err, 0, sizeof(int), ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    return fail(ctx, H3G_ERR_TIMEOUT, "a bounded device wait expired (results of this evaluation are invalid)");
+}
+
 extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want, h3g_result* out) {
     if (!pr || !bl || !out) return H3G_ERR_ARG;
     h3g_ctx* ctx = pr->ctx;
@@ -857,8 +869,16 @@ extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want,
     H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     cudaEventElapsedTime(&pr->last_ms, pr->ev0, pr->ev1);
     unpack_result(pr, norm_want(want), out);
-    if (pr->h_pin[pr->off_out + 1] != 0.0) return fail(ctx, H3G_ERR_TIMEOUT, "a bounded tensor-core wait expired on the device");
+    if (pr->h_pin[pr->off_out + 1] != 0.0) return timed_out(pr);
     if (!std::isfinite(out->lnl)) return fail(ctx, H3G_ERR_NUMERIC, "non-finite log-likelihood");
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_problem_set_wait_limit(h3g_problem* pr, uint32_t polls, int unmatched) {
+    if (!pr) return H3G_ERR_ARG;
+    pr->wait.polls = polls ? polls : WaitCfg{}.polls;
+    pr->wait.skew = unmatched ? 1 : 0;
+    pr->drop_graphs();               // the limit is a launch parameter of the captured passes
     return H3G_OK;
 }
 
@@ -890,6 +910,7 @@ extern "C" h3g_status h3g_read_result(h3g_problem* pr, unsigned want, h3g_result
     enqueue_readback(pr, norm_want(want));
     H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     unpack_result(pr, norm_want(want), out);
+    if (pr->h_pin[pr->off_out + 1] != 0.0) return timed_out(pr);
     return H3G_OK;
 }
 

@@ -321,10 +321,12 @@ __device__ __forceinline__ int claim(int* ctr, int* s_item) {
     __syncthreads();
     return *s_item;
 }
-// thread 0: bounded wait until an item's flag holds this evaluation's epoch
-__device__ __forceinline__ void wait_item(const int* flag, int epoch, int* err) {
-    for (uint32_t it = 0; ld_acquire(flag) != epoch; ++it) {
-        if (it > (1u << 22)) { atomicOr(err, 32); return; }
+// thread 0: bounded wait (wc.polls polls) until an item's flag holds this evaluation's epoch
+// (plus wc.skew: a nonzero skew waits for a value no item publishes, the test of this path)
+__device__ __forceinline__ void wait_item(const int* flag, int epoch, int* err, const WaitCfg& wc) {
+    const int want = epoch + wc.skew;
+    for (uint32_t it = 0; ld_acquire(flag) != want; ++it) {
+        if (it >= wc.polls) { atomicOr(err, 32); return; }
         __nanosleep(64);
     }
 }
@@ -355,7 +357,7 @@ __device__ __forceinline__ int publish_and_claim(int* flag, int epoch, int* ctr,
 // Persistent: grid min(items, 2 x SMs), block 512; items (chain, m, tile) in the order of
 // t.in_heads (chains by the height of their first node, the root's last).  A chain runs up
 // the tree while the parent's only internal child is the node just finished.
-__global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items) {
+__global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items, WaitCfg wc) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
     __shared__ int s_item;
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 if (threadIdx.x == 0)
                     for (int k = k0; k < k1; ++k) {
                         const int code = t.kdesc[k].y;
-                        if (code <= -2) wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err);
+                        if (code <= -2) wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err, wc);
                     }
                 __syncthreads();
                 // the first two children's messages load together (padding states are zero in every
@@ -494,7 +496,7 @@ __global__ void k_root_mx(Topo t, Model md, Work w, MixedWork mw) {
 // Persistent like the inside pass; items (chain, m, tile) in the order of t.out_heads (chains
 // by the depth of their first node's parent).  A chain runs down the tree through each
 // node's deepest internal child.
-__global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items) {
+__global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Work w, MixedWork mw, int n_items, WaitCfg wc) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
     __shared__ int s_item;
@@ -521,7 +523,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
             const bool internal = ic >= 0;
             if (internal) tc_load_b(s, mw.Bpt, mat_off_f(m, c, t.n));
             if (!carried) {
-                if (threadIdx.x == 0 && u != t.root) wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err);
+                if (threadIdx.x == 0 && u != t.root) wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err, wc);
                 __syncthreads();
                 if (u == t.root) {
 #pragma unroll
@@ -853,18 +855,20 @@ static int persistent_ctas(int items) {
     }();
     return std::max(1, std::min(items, 2 * sms));
 }
-int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s) {
+int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
+                        cudaStream_t s) {
     const int items = count * md.M * (t.Pp / MT);
-    launch_k(k_inside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items);
+    launch_k(k_inside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
     return 1;
 }
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
     launch_k(k_root_mx, (t.Pp + 127) / 128, 128, 0, s, t, md, w, mw);
     return 1;
 }
-int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s) {
+int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
+                         cudaStream_t s) {
     const int items = count * md.M * (t.Pp / MT);
-    launch_k(k_outside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items);
+    launch_k(k_outside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
     return 1;
 }
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {

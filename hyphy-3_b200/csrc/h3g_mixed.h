@@ -33,14 +33,24 @@ struct MixedWork {
     int* sync = nullptr;     // [4]              epoch, inside and outside item counters
 };
 
+// Limit of the persistent passes' waits on another item's flag: polls before the wait gives up
+// (the kernel then records H3G_ERR_TIMEOUT's flag and carries on), and a skew added to the
+// awaited epoch (nonzero only to test that path: no item publishes that value).
+struct WaitCfg {
+    uint32_t polls = 1u << 22;
+    int skew = 0;
+};
+
 bool mixed_available();
 void mixed_configure();
 h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, int M, int Pp);
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 // count: chains of the pass (Topo::in_heads / out_heads)
-int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s);
+int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
+                        cudaStream_t s);
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
-int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, cudaStream_t s);
+int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
+                         cudaStream_t s);
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 
 }  // namespace h3g

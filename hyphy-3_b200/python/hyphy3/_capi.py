@@ -27,7 +27,7 @@ EXPORTED = [
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
-    "h3g_nuc_eval_from_P",
+    "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -109,6 +109,7 @@ def load() -> C.CDLL:
                                                 C.POINTER(C.c_uint64), _dp, C.c_int, _dp, _dp, _dp, _dp]
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
         lib.h3g_nuc_eval_from_P.argtypes = [vp, _dp, _dp, _dp, _dp]
+        lib.h3g_problem_set_wait_limit.argtypes = [vp, C.c_uint32, C.c_int]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)
@@ -135,7 +136,11 @@ def _ptr(a: np.ndarray | None, ct=C.c_double):
 
 
 class H3GError(RuntimeError):
-    pass
+    """A C ABI call failed; .status is its h3g_status."""
+
+    def __init__(self, msg: str, status: int = -1):
+        super().__init__(msg)
+        self.status = status
 
 
 class Context:
@@ -149,7 +154,7 @@ class Context:
 
     def check(self, st: int) -> None:
         if st != H3G_OK:
-            raise H3GError(f"status {st}: {self.lib.h3g_last_error(self.h).decode()}")
+            raise H3GError(f"status {st}: {self.lib.h3g_last_error(self.h).decode()}", st)
 
     def alignment_compress(self, rows, codon_to_sense, hash_bits: int = 0) -> dict:
         """Codon translation, nucleotide counts and site-pattern compression of an in-frame alignment
@@ -342,6 +347,11 @@ class Problem:
     def empty_result(self) -> dict:
         return {"site_lnl": np.zeros(self.P), "grad_t": np.zeros(self.n), "grad_dir": np.zeros(max(self.ndirs, 1)),
                 "grad_class_w": np.zeros(self.K), "grad_rate_w": np.zeros(self.M)}
+
+    def set_wait_limit(self, polls: int = 0, unmatched: bool = False) -> None:
+        """Polls before a persistent-pass flag wait gives up (0 = default); unmatched makes every such
+        wait look for a value no item publishes (tests the H3G_ERR_TIMEOUT path)."""
+        self.ctx.check(self.ctx.lib.h3g_problem_set_wait_limit(self.h, C.c_uint32(polls), C.c_int(int(unmatched))))
 
     def stage_branch_lengths(self, bl) -> None:
         bl = _f64(bl)

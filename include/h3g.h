@@ -160,6 +160,16 @@ h3g_status h3g_stage_branch_lengths(h3g_problem* prob, const double* bl);
 h3g_status h3g_eval_resident(h3g_problem* prob, unsigned want);
 h3g_status h3g_read_result(h3g_problem* prob, unsigned want, h3g_result* out);
 
+/* Limit of the waits the mixed-precision persistent passes make on one another's
+ * items: polls before a wait gives up (0 = the default, about 2^22 polls of 64 ns).
+ * An expired wait lets the kernel finish, and the evaluation returns
+ * H3G_ERR_TIMEOUT (its results are invalid); the next evaluation on the problem
+ * starts clean.  unmatched != 0 makes every such wait look for a flag value that
+ * no item publishes, so that each one expires: it exists to test this path
+ * without a fault or a hang.  No counterpart in the reference (a CPU engine has
+ * no device waits). */
+h3g_status h3g_problem_set_wait_limit(h3g_problem* prob, uint32_t polls, int unmatched);
+
 /* Per-stage device time of one evaluation (mean over reps runs, events between
  * stages, no graph): stage_ms[H3G_N_STAGES], stage_launches[H3G_N_STAGES] (may
  * be NULL).  Stage order: H3G_STAGE_NAMES. */

@@ -752,6 +752,173 @@ inline void inside_outside(const Tree& tr, const Alignment& a, int p, const std:
     }
 }
 
+// ------------------------------------------------- 64-pattern tile inside-outside
+// The reference's batched form (likelihood.hpp:295-340 workspaces, :479-762
+// compute_inside_outside_batch_in_place): every node holds S x B matrices for a
+// tile of B <= 64 patterns (element (s, b) at s * B + b), the child messages and
+// the outside vectors are S x S by S x B products, and the 1e150 rescaling runs
+// per column exactly as in the per-pattern form above, so both forms give the
+// same numbers (the products sum over k in the same order as matvec / matvec_t).
+constexpr int kTile = 64;   // likelihood.hpp:1155 tile_size
+
+struct TilePass {
+    int B = 0;
+    std::vector<std::vector<double>> D, PD, U, V;   // [node][S * B]
+    std::vector<std::vector<int>> boost;            // [node][B]
+    std::vector<std::vector<double>> lscale;        // [node][B]
+    std::vector<std::vector<double>> pref, suff;    // [child slot][S * B]
+    std::vector<std::vector<int>> pb, sb;           // [child slot][B]
+    std::vector<double> L, logL;                    // [B]
+};
+
+// C = op(A) X with op(A) = A (Trans = false) or A^T, A S x S, X and C S x B: 4 x 4
+// register blocks, every entry summed over k = 0, 1, ... from 0.0 (the order of matvec)
+template <bool Trans>
+inline void gemm_tile_blocked(const Mat& A, const double* X, double* C, int S, int B) {
+    auto a_at = [&](int i, int k) { return Trans ? A.a[size_t(k) * A.c + i] : A.a[size_t(i) * A.c + k]; };
+    for (int i0 = 0; i0 < S; i0 += 4) {
+        const int ni = std::min(4, S - i0);
+        for (int b0 = 0; b0 < B; b0 += 4) {
+            const int nb = std::min(4, B - b0);
+            double acc[4][4] = {{0.0}};
+            if (ni == 4 && nb == 4) {
+                for (int k = 0; k < S; ++k) {
+                    const double* x = X + size_t(k) * B + b0;
+                    const double a0 = a_at(i0, k), a1 = a_at(i0 + 1, k), a2 = a_at(i0 + 2, k), a3 = a_at(i0 + 3, k);
+                    for (int q = 0; q < 4; ++q) {
+                        acc[0][q] += a0 * x[q]; acc[1][q] += a1 * x[q];
+                        acc[2][q] += a2 * x[q]; acc[3][q] += a3 * x[q];
+                    }
+                }
+            } else {
+                for (int k = 0; k < S; ++k)
+                    for (int r = 0; r < ni; ++r) {
+                        const double a = a_at(i0 + r, k);
+                        for (int q = 0; q < nb; ++q) acc[r][q] += a * X[size_t(k) * B + b0 + q];
+                    }
+            }
+            for (int r = 0; r < ni; ++r)
+                for (int q = 0; q < nb; ++q) C[size_t(i0 + r) * B + b0 + q] = acc[r][q];
+        }
+    }
+}
+// C = A X  (A S x S, X and C S x B)
+inline void gemm_tile(const Mat& A, const double* X, double* C, int S, int B) { gemm_tile_blocked<false>(A, X, C, S, B); }
+// C = A^T X
+inline void gemm_tile_t(const Mat& A, const double* X, double* C, int S, int B) { gemm_tile_blocked<true>(A, X, C, S, B); }
+// A += Y Z^T over the tile (Y, Z S x B): 4 x 4 register blocks summed over b
+inline void gemm_tile_acc_nt(const double* Y, const double* Z, Mat& A, int S, int B) {
+    for (int i0 = 0; i0 < S; i0 += 4) {
+        const int ni = std::min(4, S - i0);
+        for (int j0 = 0; j0 < S; j0 += 4) {
+            const int nj = std::min(4, S - j0);
+            double acc[4][4] = {{0.0}};
+            for (int b = 0; b < B; ++b) {
+                double y[4], z[4];
+                for (int r = 0; r < 4; ++r) y[r] = r < ni ? Y[size_t(i0 + r) * B + b] : 0.0;
+                for (int q = 0; q < 4; ++q) z[q] = q < nj ? Z[size_t(j0 + q) * B + b] : 0.0;
+                for (int r = 0; r < 4; ++r)
+                    for (int q = 0; q < 4; ++q) acc[r][q] += y[r] * z[q];
+            }
+            for (int r = 0; r < ni; ++r)
+                for (int q = 0; q < nj; ++q) A.a[size_t(i0 + r) * A.c + j0 + q] += acc[r][q];
+        }
+    }
+}
+// per column: multiply by 1e150 while the column maximum is in (0, 1e-150), counting steps
+inline void rescale_cols(double* X, int S, int B, int* count) {
+    for (int b = 0; b < B; ++b) {
+        double mx = 0.0;
+        for (int s = 0; s < S; ++s) mx = std::max(mx, X[size_t(s) * B + b]);
+        while (mx < kThresh && mx > 0.0) {
+            for (int s = 0; s < S; ++s) X[size_t(s) * B + b] *= kUp;
+            mx *= kUp;
+            ++count[b];
+        }
+    }
+}
+
+inline void inside_outside_tile(const Tree& tr, const Alignment& a, int p0, int B, const std::vector<int>& l2t,
+                                const std::vector<Mat>& Pb, const std::vector<double>& pi, int S, TilePass& w, bool outside) {
+    const int n = tr.n();
+    const size_t SB = size_t(S) * B;
+    if (w.B != B || int(w.D.size()) != n || (w.D.empty() ? 0 : w.D[0].size()) != SB) {
+        w.B = B;
+        w.D.assign(n, std::vector<double>(SB)); w.PD.assign(n, std::vector<double>(SB));
+        w.U.assign(n, std::vector<double>(SB)); w.V.assign(n, std::vector<double>(SB));
+        w.boost.assign(n, std::vector<int>(B)); w.lscale.assign(n, std::vector<double>(B));
+        w.L.assign(B, 0.0); w.logL.assign(B, 0.0);
+    }
+    std::vector<double> col(S);
+    for (int u : tr.post) {
+        auto& D = w.D[u];
+        std::fill(w.boost[u].begin(), w.boost[u].end(), 0);
+        std::fill(w.lscale[u].begin(), w.lscale[u].end(), 0.0);
+        if (tr.leaf[u]) {                                             // likelihood.hpp:505-512
+            for (int b = 0; b < B; ++b) {
+                leaf_vector(a, p0 + b, l2t[u], S, col.data());
+                for (int s = 0; s < S; ++s) D[size_t(s) * B + b] = col[s];
+            }
+            continue;
+        }
+        std::fill(D.begin(), D.end(), 1.0);                           // likelihood.hpp:568-595
+        for (int c : tr.children[u]) {
+            gemm_tile(Pb[c], w.D[c].data(), w.PD[c].data(), S, B);
+            const auto& M = w.PD[c];
+            for (size_t e = 0; e < SB; ++e) D[e] *= M[e];
+            for (int b = 0; b < B; ++b) w.lscale[u][b] += w.lscale[c][b];
+            rescale_cols(D.data(), S, B, w.boost[u].data());
+        }
+        rescale_cols(D.data(), S, B, w.boost[u].data());
+        for (int b = 0; b < B; ++b) w.lscale[u][b] -= w.boost[u][b] * kLogScaler;
+    }
+    for (int b = 0; b < B; ++b) {                                     // likelihood.hpp:599-608
+        double L = 0;
+        for (int s = 0; s < S; ++s) L += w.D[tr.root][size_t(s) * B + b] * pi[s];
+        w.L[b] = L;
+        w.logL[b] = L > 0 ? std::log(L) + w.lscale[tr.root][b] : -1e20;
+    }
+    if (!outside) return;
+    for (int s = 0; s < S; ++s) for (int b = 0; b < B; ++b) w.U[tr.root][size_t(s) * B + b] = pi[s];   // :611
+    for (auto it = tr.post.rbegin(); it != tr.post.rend(); ++it) {
+        const int u = *it;
+        if (tr.leaf[u]) continue;
+        const auto& ch = tr.children[u];
+        const size_t k = ch.size();
+        if (!k) continue;
+        if (w.pref.size() < k) {
+            w.pref.resize(k); w.suff.resize(k); w.pb.resize(k); w.sb.resize(k);
+        }
+        for (size_t i = 0; i < k; ++i) {
+            w.pref[i].assign(SB, 1.0); w.suff[i].assign(SB, 1.0);
+            w.pb[i].assign(B, 0); w.sb[i].assign(B, 0);
+        }
+        for (size_t i = 1; i < k; ++i) {                              // :707-722 prefix products
+            const auto& M = w.PD[ch[i - 1]];
+            for (size_t e = 0; e < SB; ++e) w.pref[i][e] = w.pref[i - 1][e] * M[e];
+            w.pb[i] = w.pb[i - 1];
+            rescale_cols(w.pref[i].data(), S, B, w.pb[i].data());
+        }
+        for (size_t i = k - 1; i > 0; --i) {                          // :724-739 suffix products
+            const auto& M = w.PD[ch[i]];
+            for (size_t e = 0; e < SB; ++e) w.suff[i - 1][e] = w.suff[i][e] * M[e];
+            w.sb[i - 1] = w.sb[i];
+            rescale_cols(w.suff[i - 1].data(), S, B, w.sb[i - 1].data());
+        }
+        for (size_t i = 0; i < k; ++i) {                              // :741-759
+            const int c = ch[i];
+            auto& Vc = w.V[c];
+            for (size_t e = 0; e < SB; ++e) Vc[e] = w.U[u][e] * w.pref[i][e] * w.suff[i][e];
+            for (int b = 0; b < B; ++b) {
+                int net = w.boost[u][b] - w.pb[i][b] - w.sb[i][b];
+                for (; net > 0; --net) for (int s = 0; s < S; ++s) Vc[size_t(s) * B + b] *= kUp;
+                for (; net < 0; ++net) for (int s = 0; s < S; ++s) Vc[size_t(s) * B + b] *= kDown;
+            }
+            gemm_tile_t(Pb[c], Vc.data(), w.U[c].data(), S, B);
+        }
+    }
+}
+
 inline int n_threads_for(int items) {
 #ifdef _OPENMP
     return std::max(1, std::min(omp_get_max_threads(), items));
@@ -899,6 +1066,7 @@ struct MixSpec {
     bool normalized_time = false;      // tau = t * 3 / mu (per model)
     bool want_global = false;
     bool zero_l_sentinel = false;      // true: L<=0 contributes w * -1e20 to lnL
+    bool tiled = false;                // true: 64-pattern tiles with S x B GEMMs (the reference's batched shape)
 };
 struct MixResult {
     double lnl = 0;
@@ -922,7 +1090,10 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
     // per (m, b): P, dP/dt, and the per-class (class, tau) used
     std::vector<std::vector<Mat>> Pm(M, std::vector<Mat>(n, Mat::eye(S))), dPm(M, std::vector<Mat>(n, Mat(S, S)));
     std::vector<std::vector<std::vector<Mat>>> Pk(M, std::vector<std::vector<Mat>>(n));
-    for (int m = 0; m < M; ++m) for (int b = 0; b < n; ++b) {
+    // every (m, b) is independent: built in parallel, same values as a serial loop
+    #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(M * n))
+    for (int mb = 0; mb < M * n; ++mb) {
+        const int m = mb / n, b = mb % n;
         if (b == tr.root) continue;
         double r = sp.rates[m];
         if (test(b)) {
@@ -954,8 +1125,105 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
     std::vector<std::vector<double>> pat_rw(M, std::vector<double>(P, 0.0));
     // A_{m,b} = sum_p f_{m,p} V D^T, accumulated per thread then reduced in thread order
     const bool G = sp.want_global;
+    // per pattern: combine the rate passes (root log-sum-exp, busted.hpp:1342-1375); post[m] = posterior
+    // of rate class m; false when the pattern has zero likelihood (no gradient terms)
+    auto combine = [&](int p, const double* Lm, const double* logLm, double* post) {
+        const double wt = a.weights[p];
+        for (int m = 0; m < M; ++m) post[m] = 0.0;
+        bool ok = false;
+        if (M == 1) {
+            if (Lm[0] > 0) { pat_ll[p] = wt * logLm[0]; post[0] = 1.0; ok = true; }
+            else if (sp.zero_l_sentinel) pat_ll[p] = wt * -1e20;
+            res.site_lnl[p] = Lm[0] > 0 ? logLm[0] : -1e20;
+        } else {
+            double mx = -std::numeric_limits<double>::infinity();
+            for (int m = 0; m < M; ++m)
+                if (sp.rate_w[m] > 1e-12 && Lm[m] > 0) mx = std::max(mx, std::log(sp.rate_w[m]) + logLm[m]);
+            res.site_lnl[p] = -1e20;
+            if (mx > -1e19) {
+                double se = 0;
+                for (int m = 0; m < M; ++m)
+                    if (sp.rate_w[m] > 1e-12 && Lm[m] > 0) { post[m] = std::exp(std::log(sp.rate_w[m]) + logLm[m] - mx); se += post[m]; }
+                if (se > 0) {
+                    pat_ll[p] = wt * (mx + std::log(se));
+                    res.site_lnl[p] = mx + std::log(se);
+                    for (int m = 0; m < M; ++m) post[m] /= se;
+                    ok = true;
+                }
+            }
+            if (!ok && sp.zero_l_sentinel) pat_ll[p] = wt * -1e20;
+        }
+        return ok;
+    };
+    std::vector<std::vector<Mat>> Athr;
+    if (sp.tiled) {
+        // likelihood.hpp:1151-1197: OpenMP over 64-pattern tiles, per branch the S x B product dP * D
+        // and (w / L) V . (dP D) per pattern; the A_b accumulation is (f V) D^T over the tile
+        if (M > 64) throw std::runtime_error("tiled mixture_eval: at most 64 rate classes");
+        const int ntile = (P + kTile - 1) / kTile;
+        const int nt = n_threads_for(ntile);
+        Athr.resize(G ? nt : 0);
+        #pragma omp parallel num_threads(nt)
+        {
+            int tid = 0;
+#ifdef _OPENMP
+            tid = omp_get_thread_num();
+#endif
+            if (G) Athr[tid].assign(size_t(M) * n, Mat(S, S));
+            std::vector<TilePass> w(M);
+            std::vector<double> dPD(size_t(S) * kTile), fv(size_t(S) * kTile);
+            std::vector<double> Lm(M), logLm(M), post(size_t(M) * kTile), f(size_t(M) * kTile);
+            std::vector<char> ok(kTile);
+            #pragma omp for schedule(static)
+            for (int t = 0; t < ntile; ++t) {
+                const int p0 = t * kTile, B = std::min(kTile, P - p0);
+                for (int m = 0; m < M; ++m)
+                    if (M == 1 || sp.rate_w[m] > 1e-12) inside_outside_tile(tr, a, p0, B, l2t, Pm[m], a.pi, S, w[m], true);
+                for (int b = 0; b < B; ++b) {
+                    for (int m = 0; m < M; ++m) {
+                        const bool on = M == 1 || sp.rate_w[m] > 1e-12;
+                        Lm[m] = on ? w[m].L[b] : 0.0;
+                        logLm[m] = on ? w[m].logL[b] : -1e20;
+                    }
+                    double pm[64];
+                    ok[b] = combine(p0 + b, Lm.data(), logLm.data(), pm);
+                    for (int m = 0; m < M; ++m) {
+                        post[size_t(m) * kTile + b] = pm[m];
+                        const bool use = ok[b] && !(pm[m] <= 1e-12 && M > 1);
+                        f[size_t(m) * kTile + b] = use ? a.weights[p0 + b] * pm[m] / w[m].L[b] : 0.0;
+                        if (use && M > 1) pat_rw[m][p0 + b] = a.weights[p0 + b] * pm[m] / sp.rate_w[m];
+                    }
+                }
+                for (int m = 0; m < M; ++m) {
+                    bool any = false;
+                    for (int b = 0; b < B; ++b) any = any || f[size_t(m) * kTile + b] != 0.0;
+                    if (!any) continue;
+                    const double* fm = &f[size_t(m) * kTile];
+                    for (int br = 0; br < n; ++br) {
+                        if (br == tr.root) continue;
+                        const auto& Vb = w[m].V[br];
+                        const auto& Db = w[m].D[br];
+                        gemm_tile(dPm[m][br], Db.data(), dPD.data(), S, B);
+                        for (int b = 0; b < B; ++b) {
+                            if (fm[b] == 0.0) continue;
+                            double g = 0;
+                            for (int s = 0; s < S; ++s) g += Vb[size_t(s) * B + b] * dPD[size_t(s) * B + b];
+                            pat_g[br][p0 + b] += fm[b] * g;
+                        }
+                        if (G) {
+                            // A += (f V) D^T : S x B by B x S
+                            Mat& A = Athr[tid][size_t(m) * n + br];
+                            for (int s = 0; s < S; ++s)
+                                for (int b = 0; b < B; ++b) fv[size_t(s) * B + b] = fm[b] * Vb[size_t(s) * B + b];
+                            gemm_tile_acc_nt(fv.data(), Db.data(), A, S, B);
+                        }
+                    }
+                }
+            }
+        }
+    } else {
     int nt = n_threads_for(P);
-    std::vector<std::vector<Mat>> Athr(G ? nt : 0);
+    Athr.resize(G ? nt : 0);
     #pragma omp parallel num_threads(nt)
     {
         int tid = 0;
@@ -1013,6 +1281,7 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
             }
         }
     }
+    }
     Neumaier acc; for (int p = 0; p < P; ++p) acc.add(pat_ll[p]);
     res.lnl = acc.value();
     std::vector<double> dL_dtau(n, 0.0);
@@ -1037,7 +1306,17 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
     std::vector<Mat> Hk(K, Mat(S, S)); Mat Hbg(S, S);
     std::vector<double> sum_tau_g(K, 0.0); double sum_tau_g_bg = 0.0;
     res.grad_class_w.assign(K, 0.0);
-    for (int m = 0; m < M; ++m) for (int b = 0; b < n; ++b) {
+    // (m, b) in fixed chunks summed in order inside each chunk, the chunks in order afterwards:
+    // deterministic whatever the thread count
+    const int nmb = M * n, kChunk = 32, nch = (nmb + kChunk - 1) / kChunk;
+    std::vector<std::vector<Mat>> Hk_c(nch, std::vector<Mat>(K, Mat(S, S)));
+    std::vector<Mat> Hbg_c(nch, Mat(S, S));
+    std::vector<std::vector<double>> stg_c(nch, std::vector<double>(K, 0.0)), gcw_c(nch, std::vector<double>(K, 0.0));
+    std::vector<double> stgbg_c(nch, 0.0);
+    #pragma omp parallel for schedule(dynamic) num_threads(n_threads_for(nch))
+    for (int ch = 0; ch < nch; ++ch)
+    for (int mb = ch * kChunk; mb < std::min(nmb, (ch + 1) * kChunk); ++mb) {
+        const int m = mb / n, b = mb % n;
         if (b == tr.root) continue;
         const Mat& Ab = A[size_t(m) * n + b];
         double r = sp.rates[m];
@@ -1046,24 +1325,33 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
                 double tau = r * bl[b] * conv(mk[k]);
                 // d/dc_k : <A, P_k>
                 double s = 0; for (size_t e = 0; e < Ab.a.size(); ++e) s += Ab.a[e] * Pk[m][b][k].a[e];
-                res.grad_class_w[k] += s;
+                gcw_c[ch][k] += s;
                 Mat At = matmul(matmul(transpose(mk[k].U), Ab), transpose(mk[k].Vp));
                 Mat E; frechetE(mk[k], tau, E);
-                for (size_t e = 0; e < At.a.size(); ++e) Hk[k].a[e] += sp.class_w[k] * At.a[e] * E.a[e];
+                for (size_t e = 0; e < At.a.size(); ++e) Hk_c[ch][k].a[e] += sp.class_w[k] * At.a[e] * E.a[e];
                 // tau * dlnL/dtau through this class, for the d mu term
                 Mat QP = matmul(mk[k].Q, Pk[m][b][k]);
                 double g = 0; for (size_t e = 0; e < Ab.a.size(); ++e) g += Ab.a[e] * QP.a[e];
-                sum_tau_g[k] += sp.class_w[k] * tau * g;
+                stg_c[ch][k] += sp.class_w[k] * tau * g;
             }
         } else {
             double tau = r * bl[b] * conv(mbg);
             Mat At = matmul(matmul(transpose(mbg.U), Ab), transpose(mbg.Vp));
             Mat E; frechetE(mbg, tau, E);
-            for (size_t e = 0; e < At.a.size(); ++e) Hbg.a[e] += At.a[e] * E.a[e];
+            for (size_t e = 0; e < At.a.size(); ++e) Hbg_c[ch].a[e] += At.a[e] * E.a[e];
             Mat QP = matmul(mbg.Q, Pm[m][b]);
             double g = 0; for (size_t e = 0; e < Ab.a.size(); ++e) g += Ab.a[e] * QP.a[e];
-            sum_tau_g_bg += tau * g;
+            stgbg_c[ch] += tau * g;
         }
+    }
+    for (int ch = 0; ch < nch; ++ch) {
+        for (int k = 0; k < K; ++k) {
+            for (size_t e = 0; e < Hk[k].a.size(); ++e) Hk[k].a[e] += Hk_c[ch][k].a[e];
+            res.grad_class_w[k] += gcw_c[ch][k];
+            sum_tau_g[k] += stg_c[ch][k];
+        }
+        for (size_t e = 0; e < Hbg.a.size(); ++e) Hbg.a[e] += Hbg_c[ch].a[e];
+        sum_tau_g_bg += stgbg_c[ch];
     }
     auto part = [&](const MG94& mm, const Mat& H, double sum_tg, const Mat& dQ) {
         Mat Mx = matmul(matmul(mm.Vp, dQ), mm.U);

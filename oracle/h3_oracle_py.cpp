@@ -65,6 +65,20 @@ PYBIND11_MODULE(h3oracle, m) {
             b.weights.assign(a.weights.begin() + begin, a.weights.begin() + end);
             return b;
         }, py::arg("begin"), py::arg("end"))
+        .def("select_patterns", [](const Alignment& a, const std::vector<int>& idx) {
+            // the listed patterns, in the order given, with the full alignment's frequencies
+            // (parity checks on a seeded subset of a large alignment)
+            Alignment b = a;
+            b.P = int(idx.size());
+            b.states.clear(); b.masks.clear(); b.weights.clear();
+            for (int i : idx) {
+                if (i < 0 || i >= a.P) throw std::out_of_range("pattern index");
+                b.states.insert(b.states.end(), a.states.begin() + size_t(i) * a.T, a.states.begin() + size_t(i + 1) * a.T);
+                b.masks.insert(b.masks.end(), a.masks.begin() + size_t(i) * a.T, a.masks.begin() + size_t(i + 1) * a.T);
+                b.weights.push_back(a.weights[size_t(i)]);
+            }
+            return b;
+        }, py::arg("indices"))
         .def_readonly("names", &Alignment::names)
         .def_readonly("embedded_tree", &Alignment::embedded_tree)
         .def_readonly("num_taxa", &Alignment::T)
@@ -144,7 +158,7 @@ PYBIND11_MODULE(h3oracle, m) {
        py::arg("is_test") = std::vector<bool>{}, py::arg("omega_bg") = -1.0);
     m.def("mixture_eval", [](const Tree& t, const Alignment& a, const std::vector<py::dict>& classes, const std::vector<double>& class_w,
                              py::object bg, std::vector<bool> is_test, std::vector<double> rates, std::vector<double> rate_w,
-                             std::vector<double> bl, bool normalized_time, bool want_global, bool zero_l_sentinel) {
+                             std::vector<double> bl, bool normalized_time, bool want_global, bool zero_l_sentinel, bool tiled) {
         MixSpec sp;
         for (auto& c : classes) sp.classes.push_back(params_from(c));
         sp.class_w = class_w;
@@ -152,6 +166,7 @@ PYBIND11_MODULE(h3oracle, m) {
         sp.is_test.assign(is_test.begin(), is_test.end());
         if (!rates.empty()) { sp.rates = rates; sp.rate_w = rate_w; }
         sp.normalized_time = normalized_time; sp.want_global = want_global; sp.zero_l_sentinel = zero_l_sentinel;
+        sp.tiled = tiled;
         if (bl.empty()) bl = t.bl;
         MixResult r;
         { py::gil_scoped_release rel; r = mixture_eval(t, a, sp, bl); }
@@ -159,7 +174,7 @@ PYBIND11_MODULE(h3oracle, m) {
     }, py::arg("tree"), py::arg("aln"), py::arg("classes"), py::arg("class_w"), py::arg("bg") = py::none(),
        py::arg("is_test") = std::vector<bool>{}, py::arg("rates") = std::vector<double>{}, py::arg("rate_w") = std::vector<double>{},
        py::arg("branch_lengths") = std::vector<double>{}, py::arg("normalized_time") = false, py::arg("want_global") = false,
-       py::arg("zero_l_sentinel") = false);
+       py::arg("zero_l_sentinel") = false, py::arg("tiled") = false);
     m.def("nucleotide_patterns", &nucleotide_patterns, py::arg("aln"));
     m.def("gtr_matrix", [](const std::vector<double>& theta, const std::vector<double>& freq, double t) {
         if (theta.size() != 5 || freq.size() != 4) throw std::runtime_error("theta needs 5 entries, freq 4");

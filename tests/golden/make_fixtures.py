@@ -7,6 +7,7 @@ answers its tests assert are recorded in known_answers.json with their source.
 
 Run from the repository root with the reference checked out read-only:
     python tests/golden/make_fixtures.py /path/to/reference
+(or set HYPHY3_REFERENCE to that path); there is no default location.
 """
 import json
 import pathlib
@@ -234,4 +235,8 @@ def meme_case(ref_root: pathlib.Path, name: str, test_ref: str, r_lrt, rho_lrt, 
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HYPHY3_REFERENCE")
+    if not src:
+        sys.exit("usage: python tests/golden/make_fixtures.py <reference checkout>  (or set HYPHY3_REFERENCE)")
+    main(src)

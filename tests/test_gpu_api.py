@@ -1,9 +1,10 @@
 """The reference-facing API (_hyphy3, hyphy3.autograd) on the device.
 
-These go through the library's own host data model and eigensolver, so the
-comparison with the oracle (a different eigensolver) is at 1e-9: with
-codon frequencies down to ~1e-10 the symmetrised eigenproblem itself only
-determines P(t) to ~1e-12 absolute.
+These go through the library's own host data model and its Householder + QL
+eigensolver, while the oracle uses cyclic Jacobi; the two eigensystems give
+transition matrices within 1e-11 and log-likelihoods within 1e-12 of each
+other (pinned on the CPU by tests/test_eigen_floor.py), so the API meets the
+same 1e-10 bound as the C ABI fed with the oracle's eigensystems.
 """
 import math
 
@@ -13,7 +14,7 @@ import pytest
 from gpu_helpers import rel
 
 pytestmark = pytest.mark.gpu
-TOL_API = 1e-9
+TOL_API = 1e-10
 
 
 @pytest.fixture(scope="module")
@@ -32,7 +33,7 @@ def test_point_loglik_matches_hyphy25(h3, known, golden_dir):
     lnl = h3.compute_mg94_log_likelihood(t, a, p)
     assert abs(lnl - k["point_mg94_logl"]) / abs(k["point_mg94_logl"]) < 1e-9
     ll2, g = h3.compute_branch_length_gradients(t, a, p)
-    assert abs(ll2 - lnl) < 1e-9 * abs(lnl)
+    assert abs(ll2 - lnl) < 1e-12 * abs(lnl)
 
 
 def test_branch_gradients_api_vs_oracle(h3, oracle, golden_dir):
@@ -61,15 +62,15 @@ def test_joint_frechet_api_vs_oracle(h3, oracle, golden_dir, known):
     r = h3.compute_joint_frechet_gradients(t, a, p, bl)
     ref = oracle.joint_frechet_gradients(u, b, {"alpha": 1.0, "beta": 0.45, "theta": [0.8, 1.2, 0.6, 1.8, 0.9]}, bl)
     assert abs(r["log_likelihood"] - ref["lnl"]) / abs(ref["lnl"]) < TOL_API
-    assert rel(r["grad_branches"], ref["grad_t"]) < 1e-7
-    assert abs(r["grad_omega"] - ref["grad_beta"][0]) / (1 + abs(ref["grad_beta"][0])) < 1e-7
-    assert rel(r["grad_theta"], ref["grad_theta"]) < 1e-7
+    assert rel(r["grad_branches"], ref["grad_t"]) < TOL_API
+    assert abs(r["grad_omega"] - ref["grad_beta"][0]) / (1 + abs(ref["grad_beta"][0])) < TOL_API
+    assert rel(r["grad_theta"], ref["grad_theta"]) < TOL_API
     # partitioned: every third branch in the background with omega_bg = 0.9
     mask = [i % 3 != 2 for i in range(t.num_nodes())]
     r2 = h3.compute_joint_frechet_gradients(t, a, p, bl, mask, 0.9)
     ref2 = oracle.joint_frechet_gradients(u, b, {"alpha": 1.0, "beta": 0.45, "theta": [0.8, 1.2, 0.6, 1.8, 0.9]}, bl, mask, 0.9)
     assert abs(r2["log_likelihood"] - ref2["lnl"]) / abs(ref2["lnl"]) < TOL_API
-    assert abs(r2["grad_omega_bg"] - ref2["grad_beta_bg"]) / (1 + abs(ref2["grad_beta_bg"])) < 1e-7
+    assert abs(r2["grad_omega_bg"] - ref2["grad_beta_bg"]) / (1 + abs(ref2["grad_beta_bg"])) < TOL_API
 
 
 def test_mixture_api_vs_oracle(h3, oracle):
@@ -86,11 +87,11 @@ def test_mixture_api_vs_oracle(h3, oracle):
     cls = [{"alpha": 1.0, "beta": o, "theta": wl.theta} for o in wl.omegas]
     ref = oracle.mixture_eval(u, b, cls, wl.omega_w, None, [], [0.4, 1.6], [0.5, 0.5], bl, False, True, False)
     assert abs(r["log_likelihood"] - ref["lnl"]) / abs(ref["lnl"]) < TOL_API
-    assert rel(r["grad_branches"], ref["grad_t"]) < 1e-8
-    assert rel(r["grad_omegas"], ref["grad_beta"]) < 1e-8
-    assert rel(r["grad_weights"], ref["grad_class_w"]) < 1e-8
-    assert rel(r["grad_theta"], ref["grad_theta"]) < 1e-8
-    assert rel(r["grad_syn_weights"], ref["grad_rate_w"]) < 1e-8
+    assert rel(r["grad_branches"], ref["grad_t"]) < TOL_API
+    assert rel(r["grad_omegas"], ref["grad_beta"]) < TOL_API
+    assert rel(r["grad_weights"], ref["grad_class_w"]) < TOL_API
+    assert rel(r["grad_theta"], ref["grad_theta"]) < TOL_API
+    assert rel(r["grad_syn_weights"], ref["grad_rate_w"]) < TOL_API
     # second call with the same model reuses the installed model and gives identical results
     r2 = h3.compute_mixture_gradients(t, a, base, bl, wl.omegas, wl.omega_w, [0.4, 1.6], [0.5, 0.5])
     assert r2["log_likelihood"] == r["log_likelihood"] and r2["grad_branches"] == r["grad_branches"]
