@@ -51,6 +51,7 @@ struct DevArena {
 
 struct h3g_problem {
     h3g_ctx* ctx = nullptr;
+    h3g_batch* batch = nullptr;        // the batch this problem evaluates in (its workspace lives there)
     int n = 0, root = -1, T = 0, P = 0, Pp = 0, NI = 0, max_state = -1;
     std::vector<int> ch_off, ch, iidx, taxon, in_off, out_off, in_nodes, out_nodes, parent_h;
     std::vector<uint8_t> leaf;
@@ -428,6 +429,7 @@ void fel_record_transfer(h3g_problem* pr, size_t h2d, size_t d2h, int launches, 
 
 extern "C" h3g_status h3g_problem_destroy(h3g_problem* prob) {
     if (!prob) return H3G_ERR_ARG;
+    if (prob->batch) return fail(prob->ctx, H3G_ERR_STATE, "destroy the problem's batch first");
     cudaSetDevice(prob->ctx->device);
     cudaStreamSynchronize(prob->ctx->stream);
     prob->ctx->live_problems--;
@@ -442,9 +444,124 @@ static void pad_matrix(const double* src, int S, double* dst) {
 
 static size_t n_out_of(const h3g_problem* pr) { return 2 + size_t(pr->n) + 2 * size_t(pr->nmod) + pr->M; }
 
+// Element counts of every device buffer of one evaluation workspace, for a problem of n nodes, NI
+// internal nodes, Pp padded patterns and a model of (M, K, nmod, ndirs); plus the A-accumulation
+// chunking and the Frechet branch groups those dimensions get.  A batch slot serves several problems
+// with one workspace: its counts are the element-wise maximum over them (offsets inside a buffer come
+// from the evaluated problem's own dimensions, so a larger buffer serves a smaller problem).
+struct WsLayout {
+    size_t n = 0, mats = 0, rsz = 0, pcols = 0, ecols = 0, gt = 0, apart = 0, afull = 0, hpart = 0, gsz = 0, hsz = 0,
+           dirpart = 0, gdir = 0, out = 0, part = 0, vf = 0;
+    int nchunk = 1, chunk = TP, ngroups = 1;
+    void max_with(const WsLayout& o) {
+        size_t* a[] = {&n, &mats, &rsz, &pcols, &ecols, &gt, &apart, &afull, &hpart, &gsz, &hsz, &dirpart, &gdir, &out, &part, &vf};
+        const size_t* b[] = {&o.n, &o.mats, &o.rsz, &o.pcols, &o.ecols, &o.gt, &o.apart, &o.afull, &o.hpart, &o.gsz, &o.hsz,
+                             &o.dirpart, &o.gdir, &o.out, &o.part, &o.vf};
+        for (size_t i = 0; i < sizeof(a) / sizeof(a[0]); ++i) *a[i] = std::max(*a[i], *b[i]);
+    }
+};
+
+static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod, int ndirs) {
+    (void)K;
+    WsLayout L;
+    L.n = n;
+    L.mats = size_t(M) * n * SP2;
+    L.rsz = size_t(M) * n * SP;
+    L.pcols = size_t(M) * Pp;
+    L.ecols = NI * M * Pp;
+    L.gt = size_t(M) * n;
+    // enough A chunks for ~600 CTAs, never below 256 patterns per chunk
+    const int want_chunks = std::max<int>(1, int((600 + n * M - 1) / (n * M)));
+    const int max_chunks = std::max<int>(1, int(Pp / 256));
+    L.nchunk = std::min(want_chunks, max_chunks);
+    L.chunk = int((Pp / TP + L.nchunk - 1) / L.nchunk) * TP;
+    L.nchunk = int((Pp + L.chunk - 1) / L.chunk);
+    L.apart = n * M * size_t(L.nchunk) * SP2;
+    L.afull = n * M * SP2;
+    // Frechet branch groups: about two CTAs per SM over (group, rate class, model)
+    L.ngroups = int(std::max<size_t>(1, std::min<size_t>(n, (296 + size_t(M) * nmod - 1) / (size_t(M) * nmod))));
+    const size_t G = size_t(L.ngroups);
+    L.hpart = size_t(nmod) * M * G * SP2;
+    L.gsz = size_t(nmod) * M * G;
+    L.hsz = size_t(nmod) * SP2;
+    L.dirpart = size_t(std::max(ndirs, 1)) * nmod * 17;
+    L.gdir = size_t(std::max(ndirs, 1)) * nmod * SP2;
+    L.out = 2 + n + 2 * size_t(nmod) + M;
+    L.part = NI * M * SP * Pp;
+    L.vf = n * M * SP * Pp;
+    return L;
+}
+
+// Allocate a workspace of layout L (FP64 or mixed partials) into A; w.bl is left to the caller.
+static h3g_status ws_alloc(h3g_ctx* ctx, const WsLayout& L, int precision, DevArena& A, Work& w, MixedWork& mw) {
+    w = Work{};
+    mw = MixedWork{};
+    w.nchunk = L.nchunk;
+    w.chunk = L.chunk;
+    w.ngroups = L.ngroups;
+    H3G_TRY_CUDA(ctx, A.alloc(&w.P, L.mats));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.PT, L.mats));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.dP, L.mats));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.rs, L.rsz));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.f, L.pcols));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.rw, L.pcols));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.contrib, L.pcols));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.site, L.pcols));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Ecum, L.ecols));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Eown, L.ecols));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.gt, L.gt));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Apart, L.apart));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Afull, L.afull));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.Hpart, L.hpart));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, L.gsz));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.stg, L.gsz));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.H, L.hsz));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, L.dirpart));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.G, L.gdir));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.out, L.out));
+    H3G_TRY_CUDA(ctx, A.alloc(&w.err, 1));
+    cudaMemsetAsync(w.err, 0, sizeof(int), ctx->stream);
+    if (precision == H3G_PREC_FP64) {
+        H3G_TRY_CUDA(ctx, A.alloc(&w.D, L.part));
+        H3G_TRY_CUDA(ctx, A.alloc(&w.Ms, L.part));
+        H3G_TRY_CUDA(ctx, A.alloc(&w.U, L.part));
+        H3G_TRY_CUDA(ctx, A.alloc(&w.Vf, L.vf));
+    } else {
+        MixedSizes z;
+        z.part = L.part; z.vf = L.vf; z.cols = L.ecols; z.mats = L.mats; z.rs = L.rsz; z.flags = L.ecols / TP;
+        h3g_status st = mixed_alloc(mw, A.ptrs, z);
+        if (st != H3G_OK) return fail(ctx, st, "mixed-precision workspace allocation failed");
+    }
+    cudaMemsetAsync(w.gc, 0, L.gsz * sizeof(double), ctx->stream);
+    cudaMemsetAsync(w.stg, 0, L.gsz * sizeof(double), ctx->stream);
+    return H3G_OK;
+}
+
+// Pinned host buffer of a problem: bl[n] | out | directional partials | per-pattern lnL.
+static h3g_status ensure_host_buffer(h3g_problem* pr, int M, int nmod, int ndirs) {
+    const size_t n_out = 2 + size_t(pr->n) + 2 * size_t(nmod) + M;
+    const size_t off_out = size_t(pr->n), off_dir = off_out + n_out;
+    const size_t off_site = off_dir + size_t(std::max(ndirs, 1)) * nmod * 17;
+    const size_t count = off_site + size_t(std::max(pr->P, 1));
+    if (pr->h_pin && count <= pr->h_pin_count) {
+        pr->off_out = off_out; pr->off_dir = off_dir; pr->off_site = off_site;
+        return H3G_OK;
+    }
+    cudaStreamSynchronize(pr->ctx->stream);
+    pr->drop_graphs();
+    if (pr->h_pin) { cudaFreeHost(pr->h_pin); pr->h_pin = nullptr; }
+    pr->off_out = off_out; pr->off_dir = off_dir; pr->off_site = off_site;
+    pr->h_pin_count = count;
+    H3G_TRY_CUDA(pr->ctx, cudaMallocHost(reinterpret_cast<void**>(&pr->h_pin), count * sizeof(double)));
+    return H3G_OK;
+}
+
 // Allocate the evaluation workspace for (M, K, nmod, ndirs); reuses it when unchanged.
 static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int ndirs) {
     h3g_ctx* ctx = pr->ctx;
+    if (!pr->d_bl) H3G_TRY_CUDA(ctx, pr->topo_mem.alloc(&pr->d_bl, size_t(pr->n)));
+    if (h3g_status st = ensure_host_buffer(pr, M, nmod, ndirs); st != H3G_OK) return st;
+    if (pr->batch) return H3G_OK;       // a batch member evaluates in its batch's slot workspaces
     // grow-only: a workspace sized for larger (M, K, models, directions) serves every smaller model (strides and
     // offsets come from the installed model), so optimisers that alternate gradient and value-only evaluations
     // (different direction counts) do not reallocate
@@ -458,65 +575,12 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     cudaStreamSynchronize(ctx->stream);
     pr->drop_graphs();
     pr->work_mem.release();
-    if (pr->h_pin) { cudaFreeHost(pr->h_pin); pr->h_pin = nullptr; }
     std::copy(key, key + 4, pr->work_key);
-    const size_t n = pr->n, NI = pr->NI, Pp = pr->Pp;
-    Work& w = pr->w;
-    w = Work{};
-    pr->mw = MixedWork{};
-    auto& A = pr->work_mem;
-    const size_t mats = size_t(M) * n * SP2;
-    // enough A chunks for ~600 CTAs, never below 256 patterns per chunk
-    const int want_chunks = std::max<int>(1, int((600 + n * M - 1) / (n * M)));
-    const int max_chunks = std::max<int>(1, int(Pp / 256));
-    w.nchunk = std::min(want_chunks, max_chunks);
-    w.chunk = int((Pp / TP + w.nchunk - 1) / w.nchunk) * TP;
-    w.nchunk = int((Pp + w.chunk - 1) / w.chunk);
-    H3G_TRY_CUDA(ctx, A.alloc(&pr->d_bl, n));
-    w.bl = pr->d_bl;
-    H3G_TRY_CUDA(ctx, A.alloc(&w.P, mats));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.PT, mats));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.dP, mats));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.rs, size_t(M) * n * SP));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.f, size_t(M) * Pp));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.rw, size_t(M) * Pp));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.contrib, Pp));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.site, Pp));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.Ecum, NI * M * Pp));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.Eown, NI * M * Pp));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.gt, size_t(M) * n));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.Apart, n * M * size_t(w.nchunk) * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.Afull, n * M * SP2));
-    // Frechet branch groups: about two CTAs per SM over (group, rate class, model)
-    w.ngroups = int(std::max<size_t>(1, std::min<size_t>(n, (296 + size_t(M) * nmod - 1) / (size_t(M) * nmod))));
-    const size_t G = size_t(w.ngroups);
-    H3G_TRY_CUDA(ctx, A.alloc(&w.Hpart, size_t(nmod) * M * G * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.gc, size_t(nmod) * M * G));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.stg, size_t(nmod) * M * G));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.H, size_t(nmod) * SP2));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.dirpart, size_t(std::max(ndirs, 1)) * nmod * 17));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.G, size_t(std::max(ndirs, 1)) * nmod * SP2));
-    const size_t n_out = 2 + n + 2 * size_t(nmod) + M;
-    H3G_TRY_CUDA(ctx, A.alloc(&w.out, n_out));
-    H3G_TRY_CUDA(ctx, A.alloc(&w.err, 1));
-    cudaMemsetAsync(w.err, 0, sizeof(int), ctx->stream);
-    if (pr->precision == H3G_PREC_FP64) {
-        H3G_TRY_CUDA(ctx, A.alloc(&w.D, NI * M * SP * Pp));
-        H3G_TRY_CUDA(ctx, A.alloc(&w.Ms, NI * M * SP * Pp));
-        H3G_TRY_CUDA(ctx, A.alloc(&w.U, NI * M * SP * Pp));
-        H3G_TRY_CUDA(ctx, A.alloc(&w.Vf, n * M * SP * Pp));
-    } else {
-        h3g_status st = mixed_alloc(pr->mw, A.ptrs, pr->n, pr->NI, M, pr->Pp);
-        if (st != H3G_OK) return fail(ctx, st, "mixed-precision workspace allocation failed");
-    }
-    cudaMemsetAsync(w.gc, 0, size_t(nmod) * M * G * sizeof(double), ctx->stream);
-    cudaMemsetAsync(w.stg, 0, size_t(nmod) * M * G * sizeof(double), ctx->stream);
-    pr->off_out = n;
-    pr->off_dir = pr->off_out + n_out;
-    pr->off_site = pr->off_dir + size_t(std::max(ndirs, 1)) * nmod * 17;
-    pr->h_pin_count = pr->off_site + size_t(std::max(pr->P, 1));
-    H3G_TRY_CUDA(ctx, cudaMallocHost(reinterpret_cast<void**>(&pr->h_pin), pr->h_pin_count * sizeof(double)));
-    return H3G_OK;
+    const WsLayout L = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), M, K, nmod, ndirs);
+    h3g_status st = ws_alloc(ctx, L, pr->precision, pr->work_mem, pr->w, pr->mw);
+    pr->w.bl = pr->d_bl;
+    if (st != H3G_OK) { pr->work_mem.release(); pr->w = Work{}; pr->mw = MixedWork{}; }
+    return st;
 }
 
 static uint64_t hash_bytes(uint64_t h, const void* p, size_t n) {
@@ -675,12 +739,12 @@ struct StageMarks {
     int launches[ST_COUNT];
 };
 
-// Enqueue the pruning pipeline (inside, root and optionally outside + gradients).
-static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, StageMarks* mk = nullptr) {
+// Enqueue the pruning pipeline (inside, root and optionally outside + gradients) on stream s (the
+// context stream, or a batch slot's), in workspace w / mw.
+static int enqueue_eval_on(h3g_problem* pr, unsigned want, bool from_given_P, cudaStream_t s, const Work& w,
+                           const MixedWork& mwk, StageMarks* mk = nullptr) {
     const Topo t = pr->topo();
     const Model& md = pr->md;
-    const Work& w = pr->w;
-    cudaStream_t s = pr->ctx->stream;
     const bool mixed = pr->precision == H3G_PREC_MIXED;
     const bool grads = (want & (H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL)) != 0;
     const bool global = (want & H3G_WANT_GRAD_GLOBAL) != 0;
@@ -699,11 +763,11 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
         cudaEventRecord(pr->ev_join, pr->s2);
     }
     mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
-    if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, pr->mw, s));
+    if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, mwk, s));
     int l = 0;
     if (mixed) {
         // one persistent launch over every level, per-tile dependencies
-        l = launch_inside_mixed(t, md, w, pr->mw, pr->n_in_heads, pr->wait, s);
+        l = launch_inside_mixed(t, md, w, mwk, pr->n_in_heads, pr->wait, s);
     } else {
         for (size_t lv = 0; lv + 1 < pr->in_off.size(); ++lv) {
             const int cnt = pr->in_off[lv + 1] - pr->in_off[lv];
@@ -712,11 +776,11 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
         }
     }
     mark(ST_INSIDE, l);
-    mark(ST_ROOT, mixed ? launch_root_mixed(t, md, w, pr->mw, s) : launch_root(t, md, w, s));
+    mark(ST_ROOT, mixed ? launch_root_mixed(t, md, w, mwk, s) : launch_root(t, md, w, s));
     if (grads) {
         l = 0;
         if (mixed) {
-            l = launch_outside_mixed(t, md, w, pr->mw, pr->n_out_heads, pr->wait, s);
+            l = launch_outside_mixed(t, md, w, mwk, pr->n_out_heads, pr->wait, s);
         } else {
             for (size_t lv = 0; lv + 1 < pr->out_off.size(); ++lv) {
                 const int cnt = pr->out_off[lv + 1] - pr->out_off[lv];
@@ -725,7 +789,7 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
             }
         }
         mark(ST_OUTSIDE, l);
-        mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, pr->mw, s) : launch_accumA_fp64(t, md, w, s));
+        mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, mwk, s) : launch_accumA_fp64(t, md, w, s));
         mark(ST_FRECHET, launch_frechet(t, md, w, global ? 1 : 0, s));
         if (side) cudaStreamWaitEvent(s, pr->ev_join, 0);
         if (global) mark(ST_HSUM, launch_global(t, md, w, s));
@@ -735,6 +799,10 @@ static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, Stage
     return L;
 }
 
+static int enqueue_eval(h3g_problem* pr, unsigned want, bool from_given_P, StageMarks* mk = nullptr) {
+    return enqueue_eval_on(pr, want, from_given_P, pr->ctx->stream, pr->w, pr->mw, mk);
+}
+
 static unsigned norm_want(unsigned want) {
     unsigned w = want & (H3G_WANT_SITE_LNL | H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL);
     return w | H3G_WANT_LNL;
@@ -742,21 +810,23 @@ static unsigned norm_want(unsigned want) {
 
 // Results the host reads back after an evaluation: the small output vector,
 // the directional partials and (optionally) the per-pattern lnL.
-static size_t enqueue_readback(h3g_problem* pr, unsigned want) {
-    cudaStream_t s = pr->ctx->stream;
+static size_t enqueue_readback_on(h3g_problem* pr, unsigned want, cudaStream_t s, const Work& w) {
     size_t bytes = n_out_of(pr) * sizeof(double);
-    cudaMemcpyAsync(pr->h_pin + pr->off_out, pr->w.out, bytes, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(pr->h_pin + pr->off_out, w.out, bytes, cudaMemcpyDeviceToHost, s);
     if ((want & H3G_WANT_GRAD_GLOBAL) && pr->ndirs > 0) {
         const size_t b = size_t(pr->ndirs) * pr->nmod * 17 * sizeof(double);
-        cudaMemcpyAsync(pr->h_pin + pr->off_dir, pr->w.dirpart, b, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(pr->h_pin + pr->off_dir, w.dirpart, b, cudaMemcpyDeviceToHost, s);
         bytes += b;
     }
     if ((want & H3G_WANT_SITE_LNL) && pr->P > 0) {
         const size_t b = size_t(pr->P) * sizeof(double);
-        cudaMemcpyAsync(pr->h_pin + pr->off_site, pr->w.site, b, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(pr->h_pin + pr->off_site, w.site, b, cudaMemcpyDeviceToHost, s);
         bytes += b;
     }
     return bytes;
+}
+static size_t enqueue_readback(h3g_problem* pr, unsigned want) {
+    return enqueue_readback_on(pr, want, pr->ctx->stream, pr->w);
 }
 
 static bool graphs_enabled() {
@@ -860,6 +930,7 @@ static h3g_status timed_out(h3g_problem* pr) {
 extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want, h3g_result* out) {
     if (!pr || !bl || !out) return H3G_ERR_ARG;
     h3g_ctx* ctx = pr->ctx;
+    if (pr->batch) return fail(ctx, H3G_ERR_STATE, "the problem belongs to a batch: use h3g_batch_eval");
     if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "h3g_eval before h3g_model_set");
     if (h3g_status st = check_bl(pr, bl); st != H3G_OK) return st;
     cudaSetDevice(ctx->device);
@@ -897,6 +968,7 @@ extern "C" h3g_status h3g_stage_branch_lengths(h3g_problem* pr, const double* bl
 
 extern "C" h3g_status h3g_eval_resident(h3g_problem* pr, unsigned want) {
     if (!pr) return H3G_ERR_ARG;
+    if (pr->batch) return fail(pr->ctx, H3G_ERR_STATE, "the problem belongs to a batch: use h3g_batch_eval");
     if (!pr->has_model) return fail(pr->ctx, H3G_ERR_STATE, "h3g_eval_resident before h3g_model_set");
     cudaSetDevice(pr->ctx->device);
     return run_eval(pr, want, false);
@@ -916,6 +988,7 @@ extern "C" h3g_status h3g_read_result(h3g_problem* pr, unsigned want, h3g_result
 
 extern "C" h3g_status h3g_profile_stages(h3g_problem* pr, unsigned want, int reps, double* stage_ms, int* stage_launches) {
     if (!pr || !stage_ms || reps < 1) return H3G_ERR_ARG;
+    if (pr->batch) return fail(pr->ctx, H3G_ERR_STATE, "the problem belongs to a batch");
     h3g_ctx* ctx = pr->ctx;
     if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "profile before h3g_model_set");
     cudaSetDevice(ctx->device);
@@ -946,6 +1019,7 @@ extern "C" h3g_status h3g_profile_stages(h3g_problem* pr, unsigned want, int rep
 extern "C" h3g_status h3g_eval_from_P(h3g_problem* pr, int S, const double* P, const double* pi, double* lnl, double* site_lnl) {
     if (!pr || !P || !pi || !lnl) return H3G_ERR_ARG;
     h3g_ctx* ctx = pr->ctx;
+    if (pr->batch) return fail(ctx, H3G_ERR_STATE, "the problem belongs to a batch");
     if (S < 1 || S > SP) return fail(ctx, H3G_ERR_ARG, "S must be in [1, 64]");
     // a single-class FP64 model whose transition matrices are given directly
     std::vector<double> zeroSS(size_t(S) * S, 0.0), lam(S, 0.0), one{1.0};
@@ -992,6 +1066,252 @@ extern "C" h3g_status h3g_branch_length_gradients(h3g_problem* pr, int S, const 
     st = h3g_eval(pr, bl, H3G_WANT_LNL | H3G_WANT_GRAD_T, &r);
     *lnl = r.lnl;
     return st;
+}
+
+
+// ------------------------------------------------------------------ batches
+// Many independent problems (genes) evaluated by one graph launch.  The genes are spread over
+// n_slots CUDA streams by longest-processing-time assignment on n x Pp x M; each slot owns one
+// workspace sized for the largest gene it serves, so device memory is n_slots workspaces rather
+// than one per gene.  A slot runs its genes one after another (H2D branch lengths, the evaluation's
+// kernels, D2H results); the slots run concurrently.  The whole batch is captured once per `want`
+// into one CUDA graph and replayed.
+struct h3g_batch {
+    h3g_ctx* ctx = nullptr;
+    std::vector<h3g_problem*> probs;
+    struct Slot {
+        cudaStream_t s = nullptr;
+        cudaEvent_t done = nullptr;
+        DevArena mem;
+        Work w{};
+        MixedWork mw{};
+        WsLayout L{};
+        std::vector<int> genes;
+    };
+    std::vector<std::unique_ptr<Slot>> slots;
+    int precision = -1;
+    std::vector<WsLayout> gene_layout;                // per gene, for its chunking and branch groups
+    std::vector<Model> captured_md;                   // models the graphs were captured with
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    struct GraphEntry { unsigned key; cudaGraphExec_t exec; int launches; };
+    std::vector<GraphEntry> graphs;
+    float last_ms = 0.f;
+    int last_launches = 0;
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+    ~h3g_batch() {
+        drop_graphs();
+        for (auto& sl : slots) {
+            if (sl->done) cudaEventDestroy(sl->done);
+            if (sl->s) cudaStreamDestroy(sl->s);
+        }
+        if (fork) cudaEventDestroy(fork);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+extern "C" h3g_status h3g_batch_create(h3g_ctx* ctx, int n_problems, h3g_problem* const* problems, int n_slots,
+                                       h3g_batch** out) {
+    if (!ctx || !out || n_problems < 1 || !problems) return H3G_ERR_ARG;
+    *out = nullptr;
+    if (n_slots < 1 || n_slots > 64) return fail(ctx, H3G_ERR_ARG, "n_slots must be in [1, 64]");
+    for (int i = 0; i < n_problems; ++i) {
+        if (!problems[i] || problems[i]->ctx != ctx) return fail(ctx, H3G_ERR_ARG, "every problem must live on this context");
+        if (problems[i]->batch) return fail(ctx, H3G_ERR_STATE, "a problem already belongs to a batch");
+        for (int j = 0; j < i; ++j)
+            if (problems[j] == problems[i]) return fail(ctx, H3G_ERR_ARG, "a problem is listed twice");
+    }
+    try {
+        cudaSetDevice(ctx->device);
+        auto b = std::make_unique<h3g_batch>();
+        b->ctx = ctx;
+        b->probs.assign(problems, problems + n_problems);
+        H3G_TRY_CUDA(ctx, cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        H3G_TRY_CUDA(ctx, cudaEventCreate(&b->ev0));
+        H3G_TRY_CUDA(ctx, cudaEventCreate(&b->ev1));
+        for (int k = 0; k < std::min(n_slots, n_problems); ++k) {
+            auto sl = std::make_unique<h3g_batch::Slot>();
+            H3G_TRY_CUDA(ctx, cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
+            H3G_TRY_CUDA(ctx, cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
+            b->slots.push_back(std::move(sl));
+        }
+        cudaStreamSynchronize(ctx->stream);
+        for (h3g_problem* pr : b->probs) {
+            // the problem's own workspace is no longer needed: it evaluates in the batch's slots
+            pr->drop_graphs();
+            pr->work_mem.release();
+            pr->w = Work{};
+            pr->mw = MixedWork{};
+            std::fill(pr->work_key, pr->work_key + 4, size_t(0));
+            pr->batch = b.get();
+        }
+        *out = b.release();
+        return H3G_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, H3G_ERR_OOM, "host allocation failed");
+    }
+}
+
+extern "C" h3g_status h3g_batch_destroy(h3g_batch* b) {
+    if (!b) return H3G_ERR_ARG;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    for (auto& sl : b->slots) cudaStreamSynchronize(sl->s);
+    for (h3g_problem* pr : b->probs) {
+        pr->batch = nullptr;
+        pr->has_model = false;        // its workspace went with the batch: install a model again to use it alone
+        pr->model_hash = 0;
+    }
+    delete b;
+    return H3G_OK;
+}
+
+// Slot assignment and slot workspaces for the installed models (grow-only, like a problem's).
+static h3g_status batch_prepare(h3g_batch* b) {
+    h3g_ctx* ctx = b->ctx;
+    const int G = int(b->probs.size());
+    int prec = -1;
+    for (h3g_problem* pr : b->probs) {
+        if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "every problem of a batch needs a model (h3g_model_set)");
+        if (prec >= 0 && pr->precision != prec) return fail(ctx, H3G_ERR_ARG, "the problems of a batch must share one precision");
+        prec = pr->precision;
+    }
+    std::vector<WsLayout> lay(G);
+    for (int g = 0; g < G; ++g) {
+        const h3g_problem* pr = b->probs[g];
+        lay[g] = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), pr->M, pr->K, pr->nmod, pr->ndirs);
+    }
+    const bool first = b->slots[0]->genes.empty() && b->slots[0]->w.P == nullptr;
+    if (first || prec != b->precision) {
+        // longest processing time first: genes by decreasing n x Pp x M, each to the least loaded slot
+        std::vector<int> order(G);
+        for (int g = 0; g < G; ++g) order[g] = g;
+        auto cost = [&](int g) { return double(b->probs[g]->n) * double(b->probs[g]->Pp) * double(b->probs[g]->M); };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+        std::vector<double> load(b->slots.size(), 0.0);
+        for (auto& sl : b->slots) sl->genes.clear();
+        for (int g : order) {
+            const size_t k = size_t(std::min_element(load.begin(), load.end()) - load.begin());
+            b->slots[k]->genes.push_back(g);
+            load[k] += cost(g);
+        }
+        for (auto& sl : b->slots) std::sort(sl->genes.begin(), sl->genes.end());
+    }
+    for (auto& sl : b->slots) {
+        WsLayout need;
+        for (int g : sl->genes) need.max_with(lay[g]);
+        WsLayout have = sl->L;
+        have.max_with(need);
+        const bool fits = sl->w.P && prec == b->precision && std::memcmp(&have, &sl->L, sizeof(WsLayout)) == 0;
+        if (fits) continue;
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& t : b->slots) cudaStreamSynchronize(t->s);
+        b->drop_graphs();
+        sl->mem.release();
+        sl->L = have;
+        if (h3g_status st = ws_alloc(ctx, have, prec, sl->mem, sl->w, sl->mw); st != H3G_OK) {
+            sl->mem.release();
+            sl->w = Work{};
+            sl->L = WsLayout{};
+            return st;
+        }
+    }
+    b->precision = prec;
+    b->gene_layout = lay;
+    return H3G_OK;
+}
+
+// The workspace view gene g evaluates in: its slot's buffers, its own branch lengths, chunking and groups.
+static Work batch_view(const h3g_batch* b, const h3g_batch::Slot& sl, int g) {
+    Work w = sl.w;
+    w.bl = b->probs[g]->d_bl;
+    w.nchunk = b->gene_layout[g].nchunk;
+    w.chunk = b->gene_layout[g].chunk;
+    w.ngroups = b->gene_layout[g].ngroups;
+    return w;
+}
+
+extern "C" h3g_status h3g_batch_eval(h3g_batch* b, const double* const* bl, unsigned want, h3g_result* results) {
+    if (!b || !bl || !results) return H3G_ERR_ARG;
+    h3g_ctx* ctx = b->ctx;
+    const int G = int(b->probs.size());
+    for (int g = 0; g < G; ++g) {
+        if (!bl[g]) return fail(ctx, H3G_ERR_ARG, "branch lengths missing for a problem");
+        if (h3g_status st = check_bl(b->probs[g], bl[g]); st != H3G_OK) return st;
+    }
+    cudaSetDevice(ctx->device);
+    if (h3g_status st = batch_prepare(b); st != H3G_OK) return st;
+    // models reinstalled with different device buffers invalidate the captured graphs
+    bool same = int(b->captured_md.size()) == G;
+    for (int g = 0; g < G && same; ++g) same = std::memcmp(&b->captured_md[g], &b->probs[g]->md, sizeof(Model)) == 0;
+    if (!same) {
+        b->drop_graphs();
+        b->captured_md.resize(G);
+        for (int g = 0; g < G; ++g) b->captured_md[g] = b->probs[g]->md;
+    }
+    for (int g = 0; g < G; ++g) {
+        h3g_problem* pr = b->probs[g];
+        std::copy(bl[g], bl[g] + pr->n, pr->h_pin);
+        pr->h_pin[pr->root] = 0.0;
+    }
+    const unsigned key = norm_want(want);
+    cudaStream_t s = ctx->stream;
+    cudaGraphExec_t exec = nullptr;
+    for (auto& e : b->graphs) if (e.key == key) { exec = e.exec; b->last_launches = e.launches; }
+    if (!exec) {
+        cudaGraph_t graph = nullptr;
+        int launches = 0;
+        H3G_TRY_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaEventRecord(b->fork, s);
+        for (auto& sl : b->slots) {
+            cudaStreamWaitEvent(sl->s, b->fork, 0);
+            for (int g : sl->genes) {
+                h3g_problem* pr = b->probs[g];
+                const Work w = batch_view(b, *sl, g);
+                cudaMemcpyAsync(pr->d_bl, pr->h_pin, size_t(pr->n) * sizeof(double), cudaMemcpyHostToDevice, sl->s);
+                launches += enqueue_eval_on(pr, key, false, sl->s, w, sl->mw);
+                enqueue_readback_on(pr, key, sl->s, w);
+            }
+            cudaEventRecord(sl->done, sl->s);
+            cudaStreamWaitEvent(s, sl->done, 0);
+        }
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess) { ctx->err = std::string("batch graph capture: ") + cudaGetErrorString(e); return H3G_ERR_CUDA; }
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { ctx->err = std::string("batch graph instantiate: ") + cudaGetErrorString(e); return H3G_ERR_CUDA; }
+        b->graphs.push_back({key, exec, launches});
+        b->last_launches = launches;
+    }
+    H3G_TRY_CUDA(ctx, cudaEventRecord(b->ev0, s));
+    H3G_TRY_CUDA(ctx, cudaGraphLaunch(exec, s));
+    H3G_TRY_CUDA(ctx, cudaEventRecord(b->ev1, s));
+    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+    bool expired = false;
+    for (int g = 0; g < G; ++g) {
+        h3g_problem* pr = b->probs[g];
+        unpack_result(pr, key, &results[g]);
+        expired = expired || pr->h_pin[pr->off_out + 1] != 0.0;
+    }
+    if (expired) {
+        for (auto& sl : b->slots) if (sl->w.err) cudaMemsetAsync(sl->w.err, 0, sizeof(int), s);
+        cudaStreamSynchronize(s);
+        return fail(ctx, H3G_ERR_TIMEOUT, "a bounded device wait expired in the batch (results are invalid)");
+    }
+    for (int g = 0; g < G; ++g)
+        if (!std::isfinite(results[g].lnl)) return fail(ctx, H3G_ERR_NUMERIC, "non-finite log-likelihood in the batch");
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_batch_last_stats(const h3g_batch* b, double* device_ms, int* n_launches) {
+    if (!b) return H3G_ERR_ARG;
+    if (device_ms) *device_ms = b->last_ms;
+    if (n_launches) *n_launches = b->last_launches;
+    return H3G_OK;
 }
 
 extern "C" h3g_status h3g_last_eval_stats(const h3g_problem* pr, double* device_ms, int* n_launches) {

@@ -60,24 +60,6 @@ __device__ __forceinline__ void mul_leaf_msg(double (&v)[SP], const Topo& t, con
     }
 }
 
-// out[i] = sum_j S[j*64 + i] * v[j] for a 64x64 matrix staged in shared memory,
-// written with a stride to global memory (one thread = one pattern).
-__device__ __forceinline__ void smem_matvec_store(const double* __restrict__ sM, const double (&v)[SP], double* dst, size_t stride) {
-    for (int i8 = 0; i8 < SP; i8 += 8) {
-        double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
-#pragma unroll
-        for (int j = 0; j < SP; ++j) {
-            const double2* r = reinterpret_cast<const double2*>(sM + j * SP + i8);
-            const double2 a = r[0], b = r[1], c = r[2], d = r[3];
-            const double x = v[j];
-            s0 = fma(a.x, x, s0); s1 = fma(a.y, x, s1); s2 = fma(b.x, x, s2); s3 = fma(b.y, x, s3);
-            s4 = fma(c.x, x, s4); s5 = fma(c.y, x, s5); s6 = fma(d.x, x, s6); s7 = fma(d.y, x, s7);
-        }
-        dst[(i8 + 0) * stride] = s0; dst[(i8 + 1) * stride] = s1; dst[(i8 + 2) * stride] = s2; dst[(i8 + 3) * stride] = s3;
-        dst[(i8 + 4) * stride] = s4; dst[(i8 + 5) * stride] = s5; dst[(i8 + 6) * stride] = s6; dst[(i8 + 7) * stride] = s7;
-    }
-}
-
 __device__ __forceinline__ void stage_matrix(double* __restrict__ s, const double* __restrict__ g, int tid, int nthr) {
     const double2* g2 = reinterpret_cast<const double2*>(g);
     double2* s2 = reinterpret_cast<double2*>(s);
@@ -292,34 +274,57 @@ __device__ __forceinline__ int renorm_cols(double (&v)[8], double* smax, int g, 
     return 0;
 }
 
-// out[q] = sum_j sM[j*64 + 8g + q] * sX[j*32 + lane]   (sM a 64x64 matrix, sX a 64x32 tile)
-__device__ __forceinline__ void tile_matvec8(const double* __restrict__ sM, const double* __restrict__ sX, int g, int lane, double (&o)[8]) {
-#pragma unroll
-    for (int q = 0; q < 8; ++q) o[q] = 0.0;
-#pragma unroll 16
-    for (int j = 0; j < SP; ++j) {
-        const double2* r = reinterpret_cast<const double2*>(sM + j * SP + 8 * g);
-        const double2 a = r[0], b = r[1], c = r[2], d = r[3];
-        const double x = sX[j * kTileP + lane];
-        o[0] = fma(a.x, x, o[0]); o[1] = fma(a.y, x, o[1]); o[2] = fma(b.x, x, o[2]); o[3] = fma(b.y, x, o[3]);
-        o[4] = fma(c.x, x, o[4]); o[5] = fma(c.y, x, o[5]); o[6] = fma(d.x, x, o[6]); o[7] = fma(d.y, x, o[7]);
+// Partial tiles of the FP64 pruning CTAs in shared memory: [64 states][32 patterns] with a row
+// stride of kDL = 36 doubles, so the B-fragment loads (k + lane%4) * 36 + col + lane/4 of a half-warp
+// fall in 16 different banks.
+constexpr int kDL = kTileP + 4;
+
+// Stage a 64x64 matrix row-major with the padded stride LDM (k_build_P's operand layout).
+__device__ __forceinline__ void stage_matrix_pad(double* __restrict__ s, const double* __restrict__ g, int tid, int nthr) {
+    const double2* g2 = reinterpret_cast<const double2*>(g);
+    for (int e = tid; e < SP2 / 2; e += nthr) {
+        const int r = e / (SP / 2), c2 = e % (SP / 2);
+        *reinterpret_cast<double2*>(s + r * LDM + 2 * c2) = __ldg(g2 + e);
     }
 }
 
-// grid (Pp/32, nodes in level, M), block 256, dynamic smem (64*64 + 64*32 + 8*32) doubles.
+// dst[i][p] = sum_k sM[i][k] sX[k][p] for the CTA's 64 x 32 tile on the FP64 tensor cores
+// (mma.sync m8n8k4): warp w owns output rows 8w .. 8w+7, all 32 columns as four 8x8 tiles,
+// 16 k steps of 4.  sM [64][LDM] row-major, sX [64][kDL]; dst has row stride `stride`
+// (state-major partials), each thread storing two adjacent patterns as one 16-byte write.
+__device__ __forceinline__ void tile_mm_store(const double* __restrict__ sM, const double* __restrict__ sX,
+                                              double* __restrict__ dst, size_t stride) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+    double c[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) c[j][0] = c[j][1] = 0.0;
+    const double* arow = sM + (8 * wp + g) * LDM + q;
+#pragma unroll 4
+    for (int k = 0; k < SP; k += 4) {
+        const double a = arow[k];
+        const double* brow = sX + (k + q) * kDL + g;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(c[j][0], c[j][1], a, brow[8 * j]);
+    }
+    double* d = dst + size_t(8 * wp + g) * stride + 2 * q;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) *reinterpret_cast<double2*>(d + 8 * j) = make_double2(c[j][0], c[j][1]);
+}
+
+// grid (Pp/32, nodes in level, M), block 256, dynamic smem (64*LDM + 64*kDL + 8*32) doubles.
 __global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const int* __restrict__ nodes) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    double* sPT = sm;                    // PT_u
-    double* sD = sm + SP2;               // D_u tile [64][32]
-    double* smax = sD + SP * kTileP;     // [8][32]
+    double* sP = sm;                     // P_u row-major [64][LDM]
+    double* sD = sm + SP * LDM;          // D_u tile [64][kDL]
+    double* smax = sD + SP * kDL;        // [8][32]
     const int u = nodes[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
     const int g = tid >> 5, lane = tid & 31;
     const int p = blockIdx.x * kTileP + lane;
     const int iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
     const bool root = (u == t.root);
-    if (!root) stage_matrix(sPT, w.PT + mat_off(m, u, t.n), tid, 256);
+    if (!root) stage_matrix_pad(sP, w.P + mat_off(m, u, t.n), tid, 256);
     double v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = (8 * g + q) < t.S ? 1.0 : 0.0;
@@ -346,14 +351,10 @@ __global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const 
     }
     if (root) return;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) sD[(8 * g + q) * kTileP + lane] = v[q];
+    for (int q = 0; q < 8; ++q) sD[(8 * g + q) * kDL + lane] = v[q];
     __syncthreads();
-    // message to the parent: (P_u D_u)_i = sum_j PT[j][i] D_j
-    double o[8];
-    tile_matvec8(sPT, sD, g, lane, o);
-    double* md_ = w.Ms + part_off(iu, m, M, t.Pp) + size_t(8 * g) * Pp + p;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) md_[q * Pp] = o[q];
+    // message to the parent: (P_u D_u)_i = sum_j P[i][j] D_j
+    tile_mm_store(sP, sD, w.Ms + part_off(iu, m, M, t.Pp) + size_t(blockIdx.x) * kTileP, Pp);
 }
 
 // --------------------------------------------------------------------- root
@@ -409,16 +410,16 @@ __global__ void k_root(Topo t, Model md, Work w) {
 __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const int* __restrict__ kids, int want_v) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
-    double* sP = sm;                     // P_c row-major
-    double* sV = sm + SP2;               // V_c tile [64][32]
-    double* smax = sV + SP * kTileP;
+    double* sPT = sm;                    // P_c^T row-major [64][LDM]
+    double* sV = sm + SP * LDM;          // V_c tile [64][kDL]
+    double* smax = sV + SP * kDL;
     const int c = kids[blockIdx.y], m = blockIdx.z, tid = threadIdx.x;
     const int g = tid >> 5, lane = tid & 31;
     const int p = blockIdx.x * kTileP + lane;
     const int u = t.parent[c], iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
     const bool internal = !t.leaf[c];
-    if (internal) stage_matrix(sP, w.P + mat_off(m, c, t.n), tid, 256);
+    if (internal) stage_matrix_pad(sPT, w.PT + mat_off(m, c, t.n), tid, 256);
     double v[8];
     if (u == t.root) {
 #pragma unroll
@@ -453,77 +454,102 @@ __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const
     }
     if (!internal) return;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) sV[(8 * g + q) * kTileP + lane] = v[q];
+    for (int q = 0; q < 8; ++q) sV[(8 * g + q) * kDL + lane] = v[q];
     __syncthreads();
-    // U_c = P_c^T V_c : (U_c)_i = sum_j P[j][i] V_j
-    double o[8];
-    tile_matvec8(sP, sV, g, lane, o);
-    double* dst = w.U + part_off(t.iidx[c], m, M, t.Pp) + size_t(8 * g) * Pp + p;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) dst[q * Pp] = o[q];
+    // U_c = P_c^T V_c : (U_c)_i = sum_j PT[i][j] V_j
+    tile_mm_store(sPT, sV, w.U + part_off(t.iidx[c], m, M, t.Pp) + size_t(blockIdx.x) * kTileP, Pp);
 }
 
 // ------------------------------------------------------------------ accum A
-// A_{m,b,chunk} = sum_{p in chunk} Vf_b[:, p] D_b[:, p]^T.  grid (n, M, nchunk), block 256.
+// A_{m,b,chunk} = sum_{p in chunk} Vf_b[:, p] D_b[:, p]^T on the FP64 tensor cores: C = X Y^T with
+// X = Vf (64 states x patterns), Y = D, K = the pattern axis.  8 warps as mm64 (warp w: rows
+// 16(w/2) .. +16, columns 32(w%2) .. +32, 2 x 4 tiles of 8x8), 32 patterns per stage, stages
+// double-buffered by 16-byte cp.async (a leaf's 0/1 vectors are written from its states and
+// masks instead).  grid (n, M, nchunk), block 256.
+constexpr int kAccP = 32;                                      // patterns per stage
+constexpr int kAL = kAccP + 4;                                 // row stride of a staged tile (doubles)
+constexpr size_t kAccStage = size_t(2) * SP * kAL;             // V and D tiles of one stage
+static const size_t kAccSmemF = 2 * kAccStage * sizeof(double);
+
+__device__ __forceinline__ void cp_async16_f64(double* dst, const double* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                 ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(src) : "memory");
+}
+
 __global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w) {
     pdl_enter();
-    __shared__ __align__(16) double sV[32][SP + 2];
-    __shared__ __align__(16) double sD[32][SP + 2];
+    extern __shared__ __align__(16) double smA[];
     const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
     const int M = md.M;
     const size_t Pp = size_t(t.Pp);
-    const int ti = tid & 15, tj = tid >> 4;
     const int p_begin = ck * w.chunk, p_end = min(t.Pp, p_begin + w.chunk);
+    const int nst = (p_end - p_begin) / kAccP;
     const bool lf = t.leaf[b];
     const int tx = lf ? t.taxon[b] : -1;
     const double* Vb = w.Vf + part_off(b, m, M, t.Pp);
     const double* Db = lf ? nullptr : w.D + part_off(t.iidx[b], m, M, t.Pp);
-    double acc[4][4];
+
+    // stage `st` of the chunk into buffer st & 1: 64 state rows x 32 patterns of Vf (and D)
+    auto stage = [&](int st) {
+        double* sV = smA + size_t(st & 1) * kAccStage;
+        double* sD = sV + SP * kAL;
+        const size_t p0 = size_t(p_begin) + size_t(st) * kAccP;
+        for (int c = tid; c < SP * (kAccP / 2); c += 256) {
+            const int r = c / (kAccP / 2), q2 = c % (kAccP / 2);
+            cp_async16_f64(sV + r * kAL + 2 * q2, Vb + size_t(r) * Pp + p0 + 2 * q2);
+            if (!lf) cp_async16_f64(sD + r * kAL + 2 * q2, Db + size_t(r) * Pp + p0 + 2 * q2);
+        }
+        if (lf) {
+            // pattern p0 + (tid % 32), states 8 (tid / 32) .. +8 of the leaf's 0/1 vector
+            const int pp = tid & 31, j0 = 8 * (tid >> 5);
+            const size_t p = p0 + pp;
+            const int sv = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
+            const uint64_t mk = (tx < 0 || sv >= 0) ? 0 : t.masks[size_t(tx) * Pp + p];
+            const bool all = tx < 0 || (sv < 0 && (mk == 0 || (mk & t.all_mask) == t.all_mask));
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
-    for (int p0 = p_begin; p0 < p_end; p0 += 32) {
-        for (int e = tid; e < 32 * SP; e += 256) {
-            const int pp = e & 31, i = e >> 5, p = p0 + pp;
-            const bool in = p < p_end;
-            sV[pp][i] = in ? Vb[i * Pp + p] : 0.0;
-            double d = 0.0;
-            if (in) {
-                if (!lf) {
-                    d = Db[i * Pp + p];
-                } else if (i < t.S) {
-                    const int st = tx < 0 ? -1 : int(t.states[size_t(tx) * Pp + p]);
-                    if (st >= 0) d = (st == i) ? 1.0 : 0.0;
-                    else {
-                        const uint64_t mk = tx < 0 ? t.all_mask : t.masks[size_t(tx) * Pp + p];
-                        d = (mk == 0 || (mk & t.all_mask) == t.all_mask || ((mk >> i) & 1)) ? 1.0 : 0.0;
-                    }
-                }
+            for (int q = 0; q < 8; ++q) {
+                const int j = j0 + q;
+                double d = 0.0;
+                if (j < t.S) d = all ? 1.0 : (sv >= 0 ? (sv == j ? 1.0 : 0.0) : (((mk >> j) & 1) ? 1.0 : 0.0));
+                sD[j * kAL + pp] = d;
             }
-            sD[pp][i] = d;
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
+    const int lane = tid & 31, wp = tid >> 5, g = lane >> 2, q = lane & 3;
+    const int r0 = 16 * (wp >> 1), c0 = 32 * (wp & 1);
+    Frag64 acc;
+    frag_zero(acc);
+    if (nst > 0) stage(0);
+    for (int st = 0; st < nst; ++st) {
+        if (st + 1 < nst) stage(st + 1);
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
         __syncthreads();
-#pragma unroll 8
-        for (int pp = 0; pp < 32; ++pp) {
-            const double2 a01 = *reinterpret_cast<const double2*>(&sV[pp][4 * ti]);
-            const double2 a23 = *reinterpret_cast<const double2*>(&sV[pp][4 * ti + 2]);
-            const double2 b01 = *reinterpret_cast<const double2*>(&sD[pp][4 * tj]);
-            const double2 b23 = *reinterpret_cast<const double2*>(&sD[pp][4 * tj + 2]);
-            const double av[4] = {a01.x, a01.y, a23.x, a23.y}, bv[4] = {b01.x, b01.y, b23.x, b23.y};
+        const double* sV = smA + size_t(st & 1) * kAccStage;
+        const double* sD = sV + SP * kAL;
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
+        for (int k = 0; k < kAccP; k += 4) {
+            double a[2], bb[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+            for (int i = 0; i < 2; ++i) a[i] = sV[(r0 + 8 * i + g) * kAL + k + q];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bb[j] = sD[(c0 + 8 * j + g) * kAL + k + q];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc.v[i][j][0], acc.v[i][j][1], a[i], bb[j]);
         }
-        __syncthreads();
+        __syncthreads();                         // the buffer is refilled by the next iteration's stage
     }
     double* dst = w.Apart + ((size_t(b) * M + m) * w.nchunk + ck) * SP2;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) dst[(4 * ti + a) * SP + 4 * tj + c] = acc[a][c];
+        for (int j = 0; j < 4; ++j)
+            *reinterpret_cast<double2*>(dst + frag_row(i) * SP + frag_col(j, 0)) = make_double2(acc.v[i][j][0], acc.v[i][j][1]);
 }
 
 __device__ __forceinline__ double block_sum_256(double x, double* red) {
@@ -754,7 +780,7 @@ __global__ void __launch_bounds__(256) k_small(Topo t, Model md, Work w, int gra
 }
 
 // ------------------------------------------------------------------ launch
-static const size_t kPruneSmem = (SP2 + SP * kTileP + kGroups * kTileP) * sizeof(double);
+static const size_t kPruneSmem = (SP * LDM + SP * kDL + kGroups * kTileP) * sizeof(double);
 static const size_t kDirSmem = (2 * SP2 + 16 * SP) * sizeof(double);
 static const size_t kBuildSmem = size_t(2) * SP * LDM * sizeof(double);
 static const size_t kFrechetSmem = size_t(3) * SP * LDM * sizeof(double);
@@ -765,6 +791,7 @@ void fp64_configure() {
     cudaFuncSetAttribute(k_outside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
     cudaFuncSetAttribute(k_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFrechetSmem));
     cudaFuncSetAttribute(k_dir, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kDirSmem));
+    cudaFuncSetAttribute(k_accumA, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kAccSmemF));
 }
 
 int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
@@ -789,7 +816,7 @@ int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int
     return 1;
 }
 int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    launch_k(k_accumA, dim3(t.n, md.M, w.nchunk), 256, 0, s, t, md, w);
+    launch_k(k_accumA, dim3(t.n, md.M, w.nchunk), 256, kAccSmemF, s, t, md, w);
     return 1;
 }
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {

@@ -118,10 +118,12 @@ __device__ __forceinline__ MsgSrc msg_src(const Topo& t, const MixedWork& mw, in
     }
     return r;
 }
-__device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
+// nv: how many of this thread's 16 states are real (S - 16 g, clamped to [0, 16]); the padding
+// states of stored partials are never written (zero since allocation) and never read.
+__device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG], int nv) {
     if (r.stride != 1) {                // a message written by another CTA of this launch: read through L2
 #pragma unroll
-        for (int i = 0; i < kSG; ++i) a[i] = __ldcg(r.src + i * r.stride);
+        for (int i = 0; i < kSG; ++i) a[i] = i < nv ? __ldcg(r.src + i * r.stride) : 0.f;
     } else if (r.mk == 0) {
         const float4* s4 = reinterpret_cast<const float4*>(r.src);
 #pragma unroll
@@ -143,13 +145,14 @@ __device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
     }
 }
 
-__device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride) {
+__device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride, int nv) {
 #pragma unroll
-    for (int i = 0; i < kSG; ++i) v[i] = __ldcg(src + i * stride);
+    for (int i = 0; i < kSG; ++i) v[i] = i < nv ? __ldcg(src + i * stride) : 0.f;
 }
-__device__ __forceinline__ void store_part(const float (&v)[kSG], float* dst, size_t stride) {
+__device__ __forceinline__ void store_part(const float (&v)[kSG], float* dst, size_t stride, int nv) {
 #pragma unroll
-    for (int i = 0; i < kSG; ++i) dst[i * stride] = v[i];
+    for (int i = 0; i < kSG; ++i)
+        if (i < nv) dst[i * stride] = v[i];
 }
 
 // Shared-memory block of one tensor-core contraction.
@@ -363,6 +366,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
     __shared__ int s_item;
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
+    const int nv = min(kSG, max(0, t.S - kSG * l.g));     // real states among this thread's 16
     const int M = md.M, ntile = t.Pp / MT;
     const size_t Pp = size_t(t.Pp);
     const int epoch = __ldcg(mw.sync);
@@ -397,19 +401,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 if (k0 + 1 < k1) {
                     const MsgSrc s1 = msg_src(t, mw, m, M, t.kdesc[k0 + 1], p, l.g, so);
                     float b[kSG];
-                    msg_load(s0, v);
-                    msg_load(s1, b);
+                    msg_load(s0, v, nv);
+                    msg_load(s1, b, nv);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= b[i];
                     E += s1.E;
                 } else {
-                    msg_load(s0, v);
+                    msg_load(s0, v, nv);
                 }
                 E += renorm_row(v, s.smax, l);
                 for (int k = k0 + 2; k < k1; ++k) {
                     const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
                     float a[kSG];
-                    msg_load(sr, a);
+                    msg_load(sr, a, nv);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
                     E += sr.E + renorm_row(v, s.smax, l);
@@ -422,13 +426,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                     if (d.x == carried) continue;
                     const MsgSrc sr = msg_src(t, mw, m, M, d, p, l.g, so);
                     float a[kSG];
-                    msg_load(sr, a);
+                    msg_load(sr, a, nv);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
                     E += sr.E + renorm_row(v, s.smax, l);
                 }
             }
-            store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
+            store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp, nv);
             if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
             if (root) break;
             tc_write_part(s, v, l);
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
             phase ^= 1u;
             const int sh = renorm_row(v, s.smax, l);
             E += sh;
-            store_part(v, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
+            store_part(v, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp, nv);
             if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E;
             const int nxt = t.in_next[pos];
             if (nxt < 0) break;
@@ -502,6 +506,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
     __shared__ int s_item;
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
+    const int nv = min(kSG, max(0, t.S - kSG * l.g));     // real states among this thread's 16
     const int M = md.M, ntile = t.Pp / MT;
     const size_t Pp = size_t(t.Pp);
     const int epoch = __ldcg(mw.sync);
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                     for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
                     EV = 0;
                 } else {
-                    load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
+                    load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp, nv);
                     EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
                 }
             }
@@ -540,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                 if (sb.x == c) continue;
                 const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
                 float a[kSG];
-                msg_load(sr, a);
+                msg_load(sr, a, nv);
 #pragma unroll
                 for (int i = 0; i < kSG; ++i) v[i] *= a[i];
                 EV += sr.E + renorm_row(v, s.smax, l);
@@ -551,13 +556,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
             const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
             float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
 #pragma unroll
-            for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
+            for (int i = 0; i < kSG; ++i)
+                if (i < nv) vf[i * Pp] = float(double(v[i]) * scale);
             if (!internal) break;                          // a leaf: no outside vector below it
             tc_write_part(s, v, l);
             tc_run(s, v, l, w.err, phase);                // v: U_c, the outside vector at c
             phase ^= 1u;
             EV += renorm_row(v, s.smax, l);
-            store_part(v, mw.U + part_off(ic, m, M, t.Pp) + so, Pp);
+            store_part(v, mw.U + part_off(ic, m, M, t.Pp) + so, Pp, nv);
             if (l.g == 0) mw.EU[col_off(ic, m, M, t.Pp) + p] = EV;
             const int nxt = t.out_next[pos];
             if (nxt < 0) { last = ic; break; }
@@ -680,6 +686,12 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
         tc::mbar_fence_init();
     }
     if (warp == 0) tc::tmem_alloc(slot, 256);
+    // the padding state rows of every ring slot are never copied: zero them once
+    for (int e = tid; e < kRing * 2 * (SP - t.S) * int(kRawRow / 4); e += kAccThreads) {
+        const int per_op = (SP - t.S) * int(kRawRow / 4), sl = e / (2 * per_op), rem = e % (2 * per_op);
+        const int op = rem / per_op, w4 = rem % per_op;
+        reinterpret_cast<uint32_t*>(ring + sl * kRawSlot + op * kRawOp + t.S * kRawRow)[w4] = 0u;
+    }
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
@@ -694,6 +706,7 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int c = tid + kAccThreads * q, r = c >> 4, c16 = c & 15;
+                if (r >= t.S) continue;            // padding state rows: zero in every slot (below)
                 cp_async16(dst + r * kRawRow + c16 * 16, Vb + size_t(r) * Pp + p0 + 4 * c16);
                 if (!lf) cp_async16(dst + kRawOp + r * kRawRow + c16 * 16, Db + size_t(r) * Pp + p0 + 4 * c16);
             }
@@ -822,7 +835,7 @@ void mixed_configure() {
     cudaFuncSetAttribute(k_outside_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMxSmem));
 }
 
-h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, int M, int Pp) {
+h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z) {
     auto take = [&](auto** ptr, size_t count) -> bool {
         void* p = nullptr;
         if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(**ptr)) != cudaSuccess) return false;
@@ -830,12 +843,16 @@ h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, 
         *ptr = static_cast<std::remove_reference_t<decltype(*ptr)>>(p);
         return true;
     };
-    const size_t part = size_t(NI) * M * SP * Pp, cols = size_t(NI) * M * Pp, mats = size_t(M) * n * SP2;
-    bool ok = take(&mw.D, part) && take(&mw.Ms, part) && take(&mw.U, part) && take(&mw.Vf, size_t(n) * M * SP * Pp) &&
+    const size_t part = z.part, cols = z.cols, mats = z.mats;
+    bool ok = take(&mw.D, part) && take(&mw.Ms, part) && take(&mw.U, part) && take(&mw.Vf, z.vf) &&
               take(&mw.ED, cols) && take(&mw.EM, cols) && take(&mw.EU, cols) && take(&mw.PT32, mats) &&
-              take(&mw.rs32, size_t(M) * n * SP);
+              take(&mw.rs32, z.rs);
+    // the padding states (S .. 63) of stored partials are never written: they stay zero from here
+    ok = ok && cudaMemset(mw.D, 0, part * sizeof(float)) == cudaSuccess && cudaMemset(mw.Ms, 0, part * sizeof(float)) == cudaSuccess &&
+         cudaMemset(mw.U, 0, part * sizeof(float)) == cudaSuccess &&
+         cudaMemset(mw.Vf, 0, z.vf * sizeof(float)) == cudaSuccess;
     for (int q = 0; q < 3 && ok; ++q) ok = take(&mw.Bp[q], mats) && take(&mw.Bpt[q], mats);
-    const size_t flags = size_t(NI) * M * (Pp / MT);
+    const size_t flags = z.flags;
     ok = ok && take(&mw.flag_in, flags) && take(&mw.flag_out, flags) && take(&mw.sync, 4);
     ok = ok && cudaMemset(mw.flag_in, 0, flags * sizeof(int)) == cudaSuccess &&
          cudaMemset(mw.flag_out, 0, flags * sizeof(int)) == cudaSuccess && cudaMemset(mw.sync, 0, 4 * sizeof(int)) == cudaSuccess;

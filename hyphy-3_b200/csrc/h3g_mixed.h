@@ -43,7 +43,12 @@ struct WaitCfg {
 
 bool mixed_available();
 void mixed_configure();
-h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, int n, int NI, int M, int Pp);
+// Element counts of the mixed path's buffers: part = NI M 64 Pp, vf = n M 64 Pp, cols = NI M Pp,
+// mats = M n 64 64, rs = M n 64, flags = NI M Pp / 128 (or the maxima over the problems a workspace serves).
+struct MixedSizes {
+    size_t part = 0, vf = 0, cols = 0, mats = 0, rs = 0, flags = 0;
+};
+h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z);
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 // count: chains of the pass (Topo::in_heads / out_heads)
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,

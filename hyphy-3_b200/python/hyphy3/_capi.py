@@ -27,7 +27,8 @@ EXPORTED = [
     "h3g_last_eval_stats", "h3g_last_eval_transfer", "h3g_stage_branch_lengths", "h3g_eval_resident",
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
-    "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit",
+    "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit", "h3g_batch_create", "h3g_batch_destroy", "h3g_batch_eval",
+    "h3g_batch_last_stats",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -110,6 +111,10 @@ def load() -> C.CDLL:
         lib.h3g_fel_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(FelResult)]
         lib.h3g_nuc_eval_from_P.argtypes = [vp, _dp, _dp, _dp, _dp]
         lib.h3g_problem_set_wait_limit.argtypes = [vp, C.c_uint32, C.c_int]
+        lib.h3g_batch_create.argtypes = [vp, C.c_int, C.POINTER(vp), C.c_int, C.POINTER(vp)]
+        lib.h3g_batch_destroy.argtypes = [vp]
+        lib.h3g_batch_eval.argtypes = [vp, C.POINTER(_dp), C.c_uint, C.POINTER(Result)]
+        lib.h3g_batch_last_stats.argtypes = [vp, _dp, C.POINTER(C.c_int)]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)
@@ -185,7 +190,9 @@ class Context:
                 "pos_counts": np.array(info.pos_counts[:], dtype=np.int64).reshape(3, 4), "rounds": int(info.rounds)}
 
     def close(self) -> None:
-        """Destroy the context after every problem still alive on it."""
+        """Destroy the context after every batch and problem still alive on it."""
+        for b in list(getattr(self, "_batches", ())):
+            b.close()
         for p in list(self._problems):
             p.close()
         if self.h:
@@ -384,6 +391,60 @@ class Problem:
         nl = C.c_int()
         self.ctx.check(self.ctx.lib.h3g_last_eval_stats(self.h, C.byref(ms), C.byref(nl)))
         return ms.value, nl.value
+
+
+class Batch:
+    """Independent problems (genes) evaluated by one graph launch per call (h3g_batch_*).
+
+    The problems keep their topology, patterns and models; their workspaces are the batch's
+    n_slots slot workspaces.  Install models with Problem.set_model (one precision for all) before
+    the first eval; after close() every problem needs set_model again to be used alone."""
+
+    def __init__(self, ctx: Context, problems, n_slots: int = 8):
+        self.ctx = ctx
+        self.problems = list(problems)
+        arr = (C.c_void_p * len(self.problems))(*[p.h.value for p in self.problems])
+        self.h = C.c_void_p()
+        ctx.check(ctx.lib.h3g_batch_create(ctx.h, len(self.problems), arr, n_slots, C.byref(self.h)))
+        if not hasattr(ctx, "_batches"):
+            ctx._batches = weakref.WeakSet()
+        ctx._batches.add(self)
+
+    def eval(self, branch_lengths, want=WANT_LNL | WANT_GRAD_T) -> list[dict]:
+        G = len(self.problems)
+        bls = [_f64(b) for b in branch_lengths]
+        if len(bls) != G or any(b.size != p.n for b, p in zip(bls, self.problems)):
+            raise ValueError("one branch-length vector (one entry per node) per problem")
+        outs = []
+        res = (Result * G)()
+        for g, p in enumerate(self.problems):
+            o = {"site_lnl": np.zeros(p.P), "grad_t": np.zeros(p.n), "grad_dir": np.zeros(max(p.ndirs, 1)),
+                 "grad_class_w": np.zeros(p.K), "grad_rate_w": np.zeros(p.M), "grad_bg_w": np.zeros(max(p.nmod - p.K, 1))}
+            outs.append(o)
+            res[g] = Result(site_lnl=_ptr(o["site_lnl"]), grad_t=_ptr(o["grad_t"]), grad_dir=_ptr(o["grad_dir"]),
+                            grad_class_w=_ptr(o["grad_class_w"]), grad_rate_w=_ptr(o["grad_rate_w"]),
+                            grad_bg_w=_ptr(o["grad_bg_w"]))
+        blp = (_dp * G)(*[_ptr(b) for b in bls])
+        self.ctx.check(self.ctx.lib.h3g_batch_eval(self.h, blp, want, res))
+        for g in range(G):
+            outs[g]["lnl"] = res[g].lnl
+        return outs
+
+    def last_stats(self) -> tuple[float, int]:
+        ms, nl = C.c_double(), C.c_int()
+        self.ctx.check(self.ctx.lib.h3g_batch_last_stats(self.h, C.byref(ms), C.byref(nl)))
+        return ms.value, nl.value
+
+    def close(self) -> None:
+        if self.h and self.ctx.h:
+            self.ctx.lib.h3g_batch_destroy(self.h)
+        self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def eval_from_P_noalloc(parent, is_leaf, leaf_taxon, states, masks, weights, P, pi, device: int = 0,

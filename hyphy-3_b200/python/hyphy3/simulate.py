@@ -188,6 +188,19 @@ def simulate_alignment(tree: TreeSpec, n_sites: int, rng: np.random.Generator, *
                 rows = cum[states[par, sel]]
                 states[u, sel] = np.minimum((rows < u_rand[sel, None]).sum(1), len(pi) - 1)
     names, seqs = [], []
+    if ambig_frac == 0.0:
+        # vectorised text: one uniform draw per (leaf, site) in the same order as the loop below,
+        # so the sequences are identical to it
+        table = np.array([NUC[a] + NUC[b] + NUC[c] for a, b, c in codons] + ["---"], dtype="S3")
+        for u in range(n):
+            if kids[u]:
+                continue
+            idx = states[u].copy()
+            x = rng.random(n_sites)
+            idx[x < gap_frac] = len(codons)
+            names.append(tree.names[u])
+            seqs.append(table[idx].tobytes().decode("ascii"))
+        return names, seqs
     iupac_one = {0: "MRW", 1: "MSY", 2: "RSK", 3: "WYK"}  # codes containing the true base
     for u in range(n):
         if kids[u]:

@@ -64,6 +64,7 @@ enum {
 
 typedef struct h3g_ctx h3g_ctx;
 typedef struct h3g_problem h3g_problem;
+typedef struct h3g_batch h3g_batch;
 
 /* Reversible substitution models as eigensystems, P(tau) = U diag(exp(lam*tau)) V,
  * clamped at 0 (rate_matrix.hpp:251-257).  Models [0, K) are mixed at the P
@@ -159,6 +160,34 @@ h3g_status h3g_last_eval_transfer(const h3g_problem* prob, size_t* h2d_bytes, si
 h3g_status h3g_stage_branch_lengths(h3g_problem* prob, const double* bl);
 h3g_status h3g_eval_resident(h3g_problem* prob, unsigned want);
 h3g_status h3g_read_result(h3g_problem* prob, unsigned want, h3g_result* out);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent problems -- genes of uneven taxon count and length, each with
+ * its own tree and model -- evaluated together.  The reference evaluates such
+ * genes one call at a time (LikelihoodEngine::compute_* per gene,
+ * likelihood.hpp:1102-1211, :1228-1594, OpenMP over each gene's 64-pattern
+ * tiles, :785-803); here one batch evaluation is one CUDA-graph launch that runs
+ * every gene: the genes are spread over n_slots streams by longest-processing-
+ * time assignment on nodes x patterns x rate classes, each slot owning one
+ * workspace sized for its largest gene (device memory grows with n_slots, not
+ * with the number of genes), the slots running concurrently.
+ *   h3g_batch_create   takes problems created with h3g_problem_create; their own
+ *                      workspaces are released.  Install each one's model with
+ *                      h3g_model_set (before or after), all with one precision.
+ *                      While in a batch a problem is evaluated only through it
+ *                      (its single-problem entry points return H3G_ERR_STATE).
+ *   h3g_batch_eval     bl[i] = branch lengths of problem i (n_nodes each);
+ *                      results[i] as for h3g_eval.  Blocks until all results
+ *                      are on the host.
+ *   h3g_batch_destroy  the problems stay valid but need h3g_model_set again.
+ * Replaces: a loop of compute_joint_frechet_gradients / compute_branch_length_
+ * gradients calls over genes. */
+h3g_status h3g_batch_create(h3g_ctx* ctx, int n_problems, h3g_problem* const* problems, int n_slots, h3g_batch** out);
+h3g_status h3g_batch_destroy(h3g_batch* batch);
+h3g_status h3g_batch_eval(h3g_batch* batch, const double* const* bl, unsigned want, h3g_result* results);
+/* Device time of the last batch evaluation in ms (CUDA events around the graph
+ * launch, host copies included) and the number of kernel launches in it. */
+h3g_status h3g_batch_last_stats(const h3g_batch* batch, double* device_ms, int* n_launches);
 
 /* Limit of the waits the mixed-precision persistent passes make on one another's
  * items: polls before a wait gives up (0 = the default, about 2^22 polls of 64 ns).

@@ -23,6 +23,7 @@
 #include <limits>
 #include <list>
 #include <map>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -547,10 +548,18 @@ inline std::vector<int> leaf_map(const Tree& tr, const Alignment& a) {
 }
 
 // ----------------------------------------------------------------- MG94xREV
+// An eigensystem handed to the oracle instead of its own (U_pi, V_pi, lambda): lets a test
+// compare another engine that diagonalises Q with a different solver like with like, the
+// eigensolver's own floor being pinned separately.
+struct GivenEigen {
+    std::vector<double> U, V, lam;     // S x S, S x S (row-major), S
+};
+
 struct Params {
     double alpha = 1.0, beta = 1.0;
     double theta[5] = {1, 1, 1, 1, 1}; // AC AT CG CT GT (AG == 1)
     double delta = 0.0, psi = 0.0;
+    std::shared_ptr<const GivenEigen> eig;   // null: the oracle's own Jacobi eigensystem
 };
 
 inline void nuc_rates(const Params& p, double r[4][4]) {
@@ -629,6 +638,13 @@ struct MG94 {
         for (auto& l : lam) l = std::min(l, 0.0);
         U = Mat(S, S); Vp = Mat(S, S);
         for (int i = 0; i < S; ++i) for (int j = 0; j < S; ++j) { U(i, j) = isq[i] * E(i, j); Vp(j, i) = E(i, j) * sq[i]; }
+        if (p.eig) {
+            if (p.eig->U.size() != size_t(S) * S || p.eig->V.size() != size_t(S) * S || p.eig->lam.size() != size_t(S))
+                throw std::runtime_error("given eigensystem has the wrong size");
+            std::copy(p.eig->U.begin(), p.eig->U.end(), U.a.begin());
+            std::copy(p.eig->V.begin(), p.eig->V.end(), Vp.a.begin());
+            lam = p.eig->lam;
+        }
     }
     // rate_matrix.hpp:251-257
     Mat P(double t) const {

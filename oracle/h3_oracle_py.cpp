@@ -19,6 +19,17 @@ static Params params_from(const py::dict& d) {
     }
     if (d.contains("delta")) p.delta = d["delta"].cast<double>();
     if (d.contains("psi")) p.psi = d["psi"].cast<double>();
+    if (d.contains("eig") && !d["eig"].is_none()) {
+        // {"U": S x S, "V": S x S, "lam": S} replacing the oracle's own eigensystem
+        auto e = d["eig"].cast<py::dict>();
+        auto flat = [&](const char* k) {
+            auto a = e[k].cast<py::array_t<double, py::array::c_style | py::array::forcecast>>();
+            return std::vector<double>(a.data(), a.data() + a.size());
+        };
+        auto g = std::make_shared<GivenEigen>();
+        g->U = flat("U"); g->V = flat("V"); g->lam = flat("lam");
+        p.eig = g;
+    }
     return p;
 }
 

@@ -51,3 +51,42 @@ def test_host_and_oracle_eigensystems_agree_on_P_and_lnL(oracle, golden_dir, kno
         lh = oracle.loglik_from_P(t, ao, Ph, pi)[0]
         lo = oracle.loglik_from_P(t, ao, Po, pi)[0]
         assert abs(lh - lo) / abs(lo) < 1e-11, (name, lh, lo)
+
+
+def _eig(h, aln, beta, theta):
+    p = h.MG94Parameters()
+    p.beta = beta
+    p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = theta
+    e = h.mg94_eigensystem(aln, p)
+    return {"U": np.asarray(e["U"]), "V": np.asarray(e["V"]), "lam": np.asarray(e["lam"])}
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(1.0, float(np.max(np.abs(b)))))
+
+
+def test_gradient_floor_between_eigensolvers(oracle, golden_dir, known):
+    """The oracle with the host's eigensystem against the oracle with its own: branch, omega and
+    exchangeability gradients agree within 5e-10 of max(1, |g|max) (the bound the API tests use
+    against the oracle's own eigensystem)."""
+    import _hyphy3 as h
+    ah = h.Alignment.load(str(golden_dir / "adh.nex"))
+    ao = oracle.Alignment.load(str(golden_dir / "adh.nex"))
+    t = oracle.Tree.parse(ao.embedded_tree)
+    bl = [0.0 if i == t.root else 0.05 for i in range(t.num_nodes())]
+    own = oracle.branch_length_gradients(t, ao, {"alpha": 1.0, "beta": 0.4}, bl)
+    given = oracle.branch_length_gradients(t, ao, {"alpha": 1.0, "beta": 0.4, "eig": _eig(h, ah, 0.4, [1] * 5)}, bl)
+    assert abs(own[0] - given[0]) / abs(own[0]) < 1e-11
+    assert _rel(given[1], own[1]) < 5e-10
+    k = known["cd2_reduced"]
+    ah = h.Alignment.load(str(golden_dir / "cd2_reduced.fna"))
+    ao = oracle.Alignment.load(str(golden_dir / "cd2_reduced.fna"))
+    t = oracle.Tree.parse(k["newick"])
+    th = [0.8, 1.2, 0.6, 1.8, 0.9]
+    bl = [0.0 if i == t.root else max(1e-4, x) for i, x in enumerate(t.branch_lengths)]
+    own = oracle.joint_frechet_gradients(t, ao, {"alpha": 1.0, "beta": 0.45, "theta": th}, bl)
+    given = oracle.joint_frechet_gradients(t, ao, {"alpha": 1.0, "beta": 0.45, "theta": th, "eig": _eig(h, ah, 0.45, th)}, bl)
+    assert abs(own["lnl"] - given["lnl"]) / abs(own["lnl"]) < 1e-11
+    for key in ("grad_t", "grad_beta", "grad_theta"):
+        assert _rel(given[key], own[key]) < 5e-10, key
