@@ -1,12 +1,14 @@
 """Benchmark: codon site-branch lnL+gradient evaluations per second on one B200.
 
-Workload (one step = one lnL + full-gradient evaluation):
-  BUSTED-style MG94xREV omega mixture on a 64-taxon random unrooted binary tree
-  (125 branches), 1000 simulated codons with 3 % gaps and 1 % ambiguous codons,
-  omega classes {0.1, 1, 5} with weights {0.6, 0.3, 0.1} mixed at the P level;
-  lnL plus the gradient w.r.t. all 125 branch lengths, the 3 omegas, the 3
-  mixture weights and the 5 nucleotide exchangeabilities.  Unit: alignment
-  sites x branches per completed evaluation (1000 x 125 per step).
+Workload (one step = one lnL + full-gradient evaluation), default --config 3, the largest
+single-GPU configuration:
+  1024-taxon Yule tree (2045 branches), 5000 simulated codons, MG94xREV with omegas
+  {0.2, 2} (weights {0.8, 0.2}) mixed at the P level and 4 discrete-gamma synonymous-rate
+  classes as separate pruning passes combined by a root log-sum-exp; lnL plus the gradient
+  w.r.t. every branch length, both omegas, both class weights, the 5 exchangeabilities and the
+  4 rate weights.  Unit: alignment sites x branches per completed evaluation (5000 x 2045).
+  --config 1: the 64-taxon, 1000-codon, 3-omega mixture; 2: FEL per-site fits; 4: 500 uneven
+  genes in one batch.
 
 value  device-resident throughput: branch lengths already on the device, each
        step timed with CUDA events on the library's stream, L2 flushed (256 MiB
@@ -16,9 +18,11 @@ e2e    the same evaluation through the public API (_hyphy3.compute_mixture_gradi
        synchronous calls.
 --impl reference  times the CPU restatement of the reference engine (the
        reference itself needs Eigen, which this image lacks) on the host cores.
-Multi-GPU (torchrun): one process per GPU, each evaluating its own replica
-gene (independent workloads, no collective); value = all ranks' units / max
-time over ranks.
+Multi-GPU (torchrun): one process per GPU.  Default (--mode sharded): the
+workload's site patterns split over the ranks, one NCCL all-reduce of the
+device-assembled result vector per step (strong scaling); --mode replicas: each
+rank evaluates its own replica gene with no collective (weak scaling).  value =
+all ranks' units / max time over ranks.
 """
 from __future__ import annotations
 
@@ -273,6 +277,9 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     sim = load_simulate()
+    if args.config == 4:
+        run_reference_genes(args, sim)
+        return
     wl = sim.make_workload(args.config)
     eng = CpuEngine(wl, CPU_SAMPLE_PATTERNS.get(args.config))
     for _ in range(args.warmup):
@@ -292,9 +299,124 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_reference_genes(args, sim) -> None:
+    """Reference arm of the multi-gene workload: each step evaluates a fixed sample of 4 of its genes
+    (lnL + branch gradients) with the CPU restatement on every host thread."""
+    import h3oracle as o
+    G = args.genes or 500
+    genes = sim.make_gene_batch(G)
+    sample = sorted(np.random.default_rng(1).choice(G, size=4, replace=False).tolist())
+    threads = o.max_threads()
+    o.set_threads(threads)
+    work = []
+    for gi in sample:
+        g = genes[gi]
+        oa = o.Alignment.from_sequences(g.names, g.seqs)
+        ot = o.Tree.parse(g.newick)
+        work.append((ot, oa, [{"alpha": 1.0, "beta": g.omega, "theta": list(g.theta)}]))
+    units = sum(oa.num_codons * (ot.num_nodes() - 1) for ot, oa, _ in work)
+
+    def step():
+        for ot, oa, cls in work:
+            o.mixture_eval(ot, oa, cls, [1.0], None, [], [], [], list(ot.branch_lengths), False, False, False, True)
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    v = units / dt
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": BATCH_WORKLOAD.format(G=G, S=args.slots), "genes": G},
+                      "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                       "sample": f"genes {sample} per step, lnL + branch gradients, oracle/ CPU restatement"},
+                      "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def run_sharded(args) -> None:
+    """N GPUs, one process each: the workload's site patterns split into N contiguous ranges
+    (hyphy3.distributed.ShardedProblem); per step every rank evaluates its range on its device, the
+    result vectors are assembled on the devices and summed by one NCCL all-reduce in device memory,
+    and the full-alignment result is copied to the host.  Strong scaling (one alignment, fixed)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from hyphy3 import _capi
+    from hyphy3.distributed import ShardedProblem
+    world = int(os.environ["WORLD_SIZE"])
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    h, wl, aln, tree = build_inputs(config=args.config)
+    stream = torch.cuda.current_stream()
+    ctx = _capi.Context(local, stream=stream.cuda_stream)
+    states, masks, weights = aln.pattern_arrays()
+    l2t = h.build_leaf_to_taxon_map(tree, aln)
+    n = tree.num_nodes()
+    is_leaf = np.array([nd.is_leaf for nd in tree.nodes], dtype=np.uint8)
+    sp = ShardedProblem(ctx, np.array(tree.parents, dtype=np.int32), is_leaf,
+                        np.array([l2t[i] if is_leaf[i] else -1 for i in range(n)], dtype=np.int32), states, masks, weights)
+    es = []
+    for om in wl.omegas:
+        p = h.MG94Parameters()
+        p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = wl.theta
+        p.beta = om
+        es.append(h.mg94_eigensystem(aln, p))
+    sp.set_model(pi=aln.codon_frequencies, Q=np.stack([e["Q"] for e in es]), lam=np.stack([e["lam"] for e in es]),
+                 U=np.stack([e["U"] for e in es]), V=np.stack([e["V"] for e in es]), mu=np.array([e["mu"] for e in es]),
+                 class_w=wl.omega_w, rates=list(wl.rates), rate_w=list(wl.rate_w), dQ=_directions(aln, wl, es),
+                 precision=_capi.PREC_MIXED)
+    want = _capi.WANT_LNL | _capi.WANT_GRAD_T | _capi.WANT_GRAD_GLOBAL
+    bl = np.array(tree.get_branch_lengths())
+    units = wl.n_sites * (n - 1)
+    for _ in range(max(args.warmup, 3)):
+        sp.eval(bl, want)
+    dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0 = time.perf_counter()
+    for e0, e1 in evs:
+        e0.record()
+        out = sp.eval(bl, want)
+        e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop() if sampler else None
+    dist.barrier()
+    t = torch.tensor([sum(a.elapsed_time(b) for a, b in evs) / 1e3, wall], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    secs, wall_max = float(t[0].item()), float(t[1].item())
+    if rank == 0:
+        line = {"metric": METRIC, "value": units * args.steps / secs, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "bf16x3/f32", "data": "synthetic",
+                "config": {"workload": WORKLOADS[args.config], "sites": wl.n_sites, "branches": n - 1,
+                           "patterns": aln.num_patterns, "precision": "mixed",
+                           "l2": "inputs far larger than L2 (partials stream through HBM every step)",
+                           "parallelism": f"pattern-shards{world} (one NCCL all-reduce of the result vector per step)"},
+                "e2e": {"value": units * args.steps / wall_max, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                        "d2h_bytes_per_step": 8 * (2 + n + sp.ndirs + sp.K + sp.M),
+                        "api": "hyphy3.distributed.ShardedProblem.eval", "timing": "host wall clock, max over ranks"},
+                "gpu_launches": None, "clocks": clocks, "lnl": out["lnl"]}
+        print(json.dumps(line), flush=True)
+    sp.close()
+    ctx.close()
+    dist.destroy_process_group()
+
+
 def run_ours(args) -> None:
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and args.mode == "sharded":
+        run_sharded(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -462,6 +584,135 @@ def run_ours(args) -> None:
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+BATCH_WORKLOAD = ("uneven multi-gene batch: {G} simulated genes, taxa ~ U{{8..512}}, codons ~ U{{100..3000}}, each with "
+                  "its own random unrooted tree and MG94xREV parameters (one omega); per step lnL + the gradient w.r.t. "
+                  "every branch length of every gene, all genes in one CUDA-graph launch over {S} slot workspaces")
+
+
+def _gene_problems(h, _capi, ctx, genes, precision):
+    """One device problem per gene with its MG94 model installed; the genes' host objects."""
+    probs, hosts = [], []
+    for g in genes:
+        aln = h.Alignment.from_sequences(g.names, g.seqs)
+        tree = h.Tree.from_newick(g.newick)
+        states, masks, weights = aln.pattern_arrays()
+        l2t = h.build_leaf_to_taxon_map(tree, aln)
+        n = tree.num_nodes()
+        is_leaf = np.array([nd.is_leaf for nd in tree.nodes], dtype=np.uint8)
+        pr = _capi.Problem(ctx, np.array(tree.parents, dtype=np.int32), is_leaf,
+                           np.array([l2t[i] if is_leaf[i] else -1 for i in range(n)], dtype=np.int32), states, masks, weights)
+        p = h.MG94Parameters()
+        p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = g.theta
+        p.beta = g.omega
+        e = h.mg94_eigensystem(aln, p)
+        pr.set_model(pi=aln.codon_frequencies, Q=e["Q"], lam=e["lam"], U=e["U"], V=e["V"], mu=[e["mu"]],
+                     precision=precision)
+        probs.append(pr)
+        hosts.append((aln, tree, p))
+    return probs, hosts
+
+
+def run_batch(args) -> None:
+    """The uneven multi-gene workload through h3g_batch_* (one graph launch per step), FP64 and mixed,
+    a short joint branch-length fit, and the CPU restatement on a sample of the genes."""
+    import torch
+    import _hyphy3 as h
+    from hyphy3 import _capi
+    from hyphy3.batch import fit_branch_lengths
+    from hyphy3.simulate import make_gene_batch
+    G = args.genes or 500
+    genes = make_gene_batch(G)
+    ctx = _capi.Context(0)
+    want = _capi.WANT_LNL | _capi.WANT_GRAD_T
+    results, units, batch = {}, 0, None
+    steps, warm = args.steps, max(args.warmup, 3)
+    for prec_name, prec in (("fp64", _capi.PREC_FP64), ("mixed", _capi.PREC_MIXED)):
+        if batch is None:
+            probs, hosts = _gene_problems(h, _capi, ctx, genes, prec)
+            batch = _capi.Batch(ctx, probs, n_slots=args.slots)
+            bls = [np.array(tr.get_branch_lengths()) for _, tr, _ in hosts]
+            units = sum(aln.num_sites * (tr.num_nodes() - 1) for aln, tr, _ in hosts)
+        else:
+            for pr, (aln, tree, p) in zip(probs, hosts):
+                e = h.mg94_eigensystem(aln, p)
+                pr.set_model(pi=aln.codon_frequencies, Q=e["Q"], lam=e["lam"], U=e["U"], V=e["V"], mu=[e["mu"]],
+                             precision=prec)
+        for _ in range(warm):
+            batch.eval(bls, want)
+        sampler = ClockSampler(0) if prec_name == "mixed" else None
+        if sampler:
+            sampler.start()
+        dev, t0 = [], time.perf_counter()
+        for _ in range(steps):
+            out = batch.eval(bls, want)
+            dev.append(batch.last_stats()[0])
+        wall = time.perf_counter() - t0
+        clocks = sampler.stop() if sampler else None
+        results[prec_name] = {"dev_s": sum(dev) / 1e3, "wall_s": wall, "launches": batch.last_stats()[1], "clocks": clocks,
+                              "lnl": [o["lnl"] for o in out], "grad": np.concatenate([o["grad_t"] for o in out])}
+    m, f = results["mixed"], results["fp64"]
+    acc = {"rel_dlnl": abs(sum(m["lnl"]) - sum(f["lnl"])) / abs(sum(f["lnl"])),
+           "max_gene_rel_dlnl": max(abs(a - b) / abs(b) for a, b in zip(m["lnl"], f["lnl"])),
+           "grad_rel_err": float(np.linalg.norm(m["grad"] - f["grad"]) / np.linalg.norm(f["grad"]))}
+    # joint fit of every gene's branch lengths (mixed): objective = one batch evaluation
+    t0 = time.perf_counter()
+    fit = fit_branch_lengths(batch, bls, max_iter=args.fit_iters)
+    fit_s = time.perf_counter() - t0
+    # algorithmic bytes of the three pruning stages summed over the genes (FP32 partials)
+    alg = 0.0
+    for aln, tree, _ in hosts:
+        w = stage_work(aln.num_patterns, tree, 1, 4)
+        alg += sum(w[k][0] for k in ("inside", "outside", "accum_A"))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    per_step = m["dev_s"] / steps
+    cpu = None
+    if not args.no_cpu:
+        import h3oracle as o
+        rng = np.random.default_rng(1)
+        sample = sorted(rng.choice(G, size=4, replace=False).tolist())
+        threads = o.max_threads()
+        o.set_threads(threads)
+        cu, ct = 0, 0.0
+        for gi in sample:
+            g = genes[gi]
+            oa = o.Alignment.from_sequences(g.names, g.seqs)
+            ot = o.Tree.parse(g.newick)
+            cls = [{"alpha": 1.0, "beta": g.omega, "theta": list(g.theta)}]
+            t1 = time.perf_counter()
+            o.mixture_eval(ot, oa, cls, [1.0], None, [], [], [], list(ot.branch_lengths), False, False, False, True)
+            ct += time.perf_counter() - t1
+            cu += oa.num_codons * (ot.num_nodes() - 1)
+        cpu = {"value": cu / ct, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"genes {sample}: one lnL + branch-gradient evaluation each, oracle/ CPU restatement in 64-pattern tiles"}
+    line = {
+        "metric": METRIC, "value": units * steps / m["dev_s"], "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warm,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16x3/f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD.format(G=G, S=args.slots), "genes": G,
+                   "sites": int(sum(aln.num_sites for aln, _, _ in hosts)), "branches": int(sum(t.num_nodes() - 1 for _, t, _ in hosts)),
+                   "site_branch_units": int(units), "precision": "mixed", "slots": args.slots,
+                   "l2": "inputs far larger than L2 (every gene's partials stream through HBM)", "parallelism": "single"},
+        "e2e": {"value": units * steps / m["wall_s"], "unit": UNIT, "h2d_bytes_per_step": int(sum(8 * t.num_nodes() for _, t, _ in hosts)),
+                "d2h_bytes_per_step": int(sum(8 * (4 + 2 * t.num_nodes()) for _, t, _ in hosts)),
+                "api": "hyphy3._capi.Batch.eval (h3g_batch_eval)", "timing": "host wall clock around synchronous calls"},
+        "gpu_launches": m["launches"] * steps,
+        "roofline": {"bound": "hbm", "kernel": "batch graph (inside + outside + accum_A of every gene)",
+                     "achieved": alg / per_step / 1e9, "peak": hbm, "unit": "GB/s", "frac": alg / per_step / 1e9 / hbm,
+                     "traffic": None, "peak_source": "measured" if peaks else "fallback",
+                     "algorithmic_bytes_per_eval": alg, "note": "whole graph time, H2D/D2H copies included"},
+        "clocks": m["clocks"], "cpu_baseline": cpu,
+        "fp64_value": units * steps / f["dev_s"], "accuracy_vs_fp64": acc,
+        "joint_fit": {"iterations": fit["iterations"], "evaluations": fit["evaluations"], "seconds": fit_s,
+                      "lnl_start": float(sum(m["lnl"])), "lnl_end": fit["log_likelihood"]},
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for pr in probs:
+        pr.close()
+    ctx.close()
 
 
 MEME_METRIC = "MEME per-site fits/s (FEL baseline + MEME alternative, null and branch EBFs per codon site)"
@@ -935,9 +1186,16 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true", help="device evaluations only (for ncu)")
     ap.add_argument("--sites", type=int, default=None, help="shrink the alignment to this many codons (--profile; --config 2)")
-    ap.add_argument("--config", type=int, choices=[1, 2, 3], default=3,
+    ap.add_argument("--mode", choices=["sharded", "replicas"], default="sharded",
+                    help="N > 1 GPUs: split one alignment's patterns over the ranks (NCCL all-reduce per step), or "
+                         "run an independent replica per rank (no collective)")
+    ap.add_argument("--genes", type=int, default=None, help="--config 4: number of genes (default 500)")
+    ap.add_argument("--slots", type=int, default=8, help="--config 4: batch slot workspaces (concurrent streams)")
+    ap.add_argument("--fit-iters", type=int, default=20, help="--config 4: L-BFGS iterations of the joint fit")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4], default=3,
                     help="1: 64-taxon 3-omega mixture; 2: FEL per-site fits, 256 taxa x 2000 codons; "
-                         "3: 1024-taxon, 4 rate x 2 omega classes (headline: the largest single-GPU workload)")
+                         "3: 1024-taxon, 4 rate x 2 omega classes (headline: the largest single-GPU workload); "
+                         "4: 500 uneven genes in one batch")
     ap.add_argument("--analysis", choices=["fel", "meme", "compress", "gtr"], default="fel",
                     help="--config 2: which per-site analysis; compress: alignment finalize on the device; "
                          "gtr: nucleotide GTR likelihood (both any config)")
@@ -948,6 +1206,8 @@ def main() -> None:
         run_gtr(args)
     elif args.config == 2 and args.impl == "ours":
         run_fel(args)
+    elif args.config == 4 and args.impl == "ours":
+        run_batch(args)
     elif args.profile:
         run_profile(args)
     elif args.impl == "reference":

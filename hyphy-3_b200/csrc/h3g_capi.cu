@@ -945,6 +945,24 @@ extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want,
     return H3G_OK;
 }
 
+extern "C" h3g_status h3g_pack_result_device(h3g_problem* pr, unsigned want, double* d_vec) {
+    if (!pr || !d_vec) return H3G_ERR_ARG;
+    if (!pr->has_model) return fail(pr->ctx, H3G_ERR_STATE, "h3g_pack_result_device before h3g_model_set");
+    if (pr->batch || !pr->w.out) return fail(pr->ctx, H3G_ERR_STATE, "no evaluation workspace on this problem");
+    cudaSetDevice(pr->ctx->device);
+    const unsigned key = norm_want(want);
+    const int grads = (key & (H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL)) != 0, global = (key & H3G_WANT_GRAD_GLOBAL) != 0;
+    launch_pack_result(pr->topo(), pr->md, pr->w, grads, global, d_vec, pr->ctx->stream);
+    H3G_TRY_CUDA(pr->ctx, cudaGetLastError());
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_ctx_stream(const h3g_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return H3G_ERR_ARG;
+    *stream = ctx->stream;
+    return H3G_OK;
+}
+
 extern "C" h3g_status h3g_problem_set_wait_limit(h3g_problem* pr, uint32_t polls, int unmatched) {
     if (!pr) return H3G_ERR_ARG;
     pr->wait.polls = polls ? polls : WaitCfg{}.polls;

@@ -834,6 +834,41 @@ int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
     launch_k(k_dir, dim3(md.ndirs, md.nmod, 4), 256, kDirSmem, s, t, md, w);
     return 1;
 }
+// The evaluation's results as one FP64 vector on the device, in the order
+// [lnl, grad_t (n, root 0), grad_dir (ndirs), grad_class_w (K), grad_rate_w (M), failed]:
+// every entry is a sum over site patterns (grad_dir's d mu term multiplies one such sum by a
+// model constant), so vectors of pattern shards add up to the whole alignment's.  The directional
+// gradient is assembled here from the 16 Frechet partials per (direction, model) exactly as the
+// host does for h3g_eval.  One block.
+__global__ void k_pack_result(Topo t, Model md, Work w, int grads, int global, double* dst) {
+    const int tid = threadIdx.x, n = t.n, K = md.K, M = md.M, nmod = md.nmod, ndirs = md.ndirs;
+    const double* out = w.out;
+    if (tid == 0) {
+        dst[0] = out[0];
+        dst[1 + n + ndirs + K + M] = out[1] != 0.0 ? 1.0 : 0.0;
+    }
+    for (int b = tid; b < n; b += blockDim.x) dst[1 + b] = (grads && b != t.root) ? out[2 + b] : 0.0;
+    for (int x = tid; x < ndirs; x += blockDim.x) {
+        double g = 0.0;
+        if (global)
+            for (int k = 0; k < nmod; ++k) {
+                const double* d = w.dirpart + (size_t(x) * nmod + k) * 17;
+                double v = 0.0;
+                for (int q = 0; q < 16; ++q) v += d[q];
+                if (md.time_mode == 1) v -= d[16] / fmax(md.mu[k], 1e-12) * out[2 + n + nmod + k];
+                g += v;
+            }
+        dst[1 + n + x] = g;
+    }
+    for (int k = tid; k < K; k += blockDim.x) dst[1 + n + ndirs + k] = global ? out[2 + n + k] : 0.0;
+    for (int m = tid; m < M; m += blockDim.x) dst[1 + n + ndirs + K + m] = grads ? out[2 + n + 2 * nmod + m] : 0.0;
+}
+
+int launch_pack_result(const Topo& t, const Model& md, const Work& w, int grads, int global, double* dst, cudaStream_t s) {
+    launch_k(k_pack_result, 1, 256, 0, s, t, md, w, grads, global, dst);
+    return 1;
+}
+
 int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s) {
     launch_k(k_small, 1, 256, 0, s, t, md, w, grads);
     return 1;

@@ -16,5 +16,6 @@ int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_globa
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
 int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
 int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s);
+int launch_pack_result(const Topo& t, const Model& md, const Work& w, int grads, int global, double* dst, cudaStream_t s);
 
 }  // namespace h3g

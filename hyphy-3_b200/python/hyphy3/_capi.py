@@ -28,7 +28,7 @@ EXPORTED = [
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
     "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit", "h3g_batch_create", "h3g_batch_destroy", "h3g_batch_eval",
-    "h3g_batch_last_stats",
+    "h3g_batch_last_stats", "h3g_pack_result_device", "h3g_ctx_stream",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -115,6 +115,8 @@ def load() -> C.CDLL:
         lib.h3g_batch_destroy.argtypes = [vp]
         lib.h3g_batch_eval.argtypes = [vp, C.POINTER(_dp), C.c_uint, C.POINTER(Result)]
         lib.h3g_batch_last_stats.argtypes = [vp, _dp, C.POINTER(C.c_int)]
+        lib.h3g_pack_result_device.argtypes = [vp, C.c_uint, vp]
+        lib.h3g_ctx_stream.argtypes = [vp, C.POINTER(vp)]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)
@@ -160,6 +162,13 @@ class Context:
     def check(self, st: int) -> None:
         if st != H3G_OK:
             raise H3GError(f"status {st}: {self.lib.h3g_last_error(self.h).decode()}", st)
+
+    @property
+    def stream_handle(self) -> int:
+        """The cudaStream_t this context enqueues on (h3g_ctx_stream), as an integer handle."""
+        sp = C.c_void_p()
+        self.check(self.lib.h3g_ctx_stream(self.h, C.byref(sp)))
+        return int(sp.value or 0)
 
     def alignment_compress(self, rows, codon_to_sense, hash_bits: int = 0) -> dict:
         """Codon translation, nucleotide counts and site-pattern compression of an in-frame alignment
@@ -359,6 +368,11 @@ class Problem:
         """Polls before a persistent-pass flag wait gives up (0 = default); unmatched makes every such
         wait look for a value no item publishes (tests the H3G_ERR_TIMEOUT path)."""
         self.ctx.check(self.ctx.lib.h3g_problem_set_wait_limit(self.h, C.c_uint32(polls), C.c_int(int(unmatched))))
+
+    def pack_device(self, want, d_ptr: int) -> None:
+        """Enqueue the assembly of the last resident evaluation's results into the device vector at d_ptr
+        (1 + n + ndirs + K + M + 1 doubles, h3g_pack_result_device)."""
+        self.ctx.check(self.ctx.lib.h3g_pack_result_device(self.h, want, C.c_void_p(d_ptr)))
 
     def stage_branch_lengths(self, bl) -> None:
         bl = _f64(bl)

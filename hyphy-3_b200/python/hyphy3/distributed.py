@@ -16,6 +16,11 @@ Two partitions, both exact:
 Errors do not desynchronise the ranks: a rank whose local evaluation fails
 still joins the all-reduce with a failure flag set, and every rank then raises.
 
+Data plane: with the NCCL backend and the library's problems, each rank's result
+vector is assembled on its device (h3g_pack_result_device) and all-reduced in
+device memory; with gloo (CPU tests) or substitute problems the vector is packed
+on the host.
+
 The evaluator on each rank is a `hyphy3._capi.Problem` (one device per
 process); `problem_factory(parent, is_leaf, leaf_taxon, states, masks, weights,
 pattern_range=(begin, end))` lets a caller substitute any object with the same
@@ -133,6 +138,44 @@ class ShardedProblem:
         self.K, self.M, self.ndirs = int(self.local.K), int(self.local.M), int(self.local.ndirs)
 
     def eval(self, bl, want=_capi.WANT_LNL | _capi.WANT_GRAD_T) -> dict:
+        import torch.distributed as dist
+        if dist.get_backend(self.group) == "nccl" and hasattr(self.local, "pack_device"):
+            return self._eval_device(bl, want)
+        return self._eval_host(bl, want)
+
+    def _eval_device(self, bl, want) -> dict:
+        """NCCL data plane: the local evaluation stays on the device, its result vector is assembled
+        there (h3g_pack_result_device), summed across ranks by one NCCL all-reduce on device memory,
+        and copied to the host once."""
+        import torch
+        import torch.distributed as dist
+        width = 1 + self.n + self.ndirs + self.K + self.M + 1
+        vec = torch.zeros(width, dtype=torch.float64, device="cuda")
+        err = None
+        try:
+            if self.end > self.begin:
+                self.local.stage_branch_lengths(bl)
+                self.local.eval_resident(want)
+                self.local.pack_device(want, vec.data_ptr())
+                # the all-reduce (torch's current stream) runs after the library's stream has packed
+                torch.cuda.current_stream().wait_stream(torch.cuda.ExternalStream(self.local.ctx.stream_handle))
+        except Exception as ex:  # joined below so that no rank is left waiting in the collective
+            err = ex
+            vec.zero_()
+            vec[-1] = 1.0
+        dist.all_reduce(vec, op=dist.ReduceOp.SUM, group=self.group)
+        host = vec.cpu().numpy()
+        if host[-1] != 0.0:
+            if err is not None:
+                raise err
+            raise RuntimeError(f"sharded evaluation failed on {int(host[-1])} rank(s)")
+        out = unpack_result(host, self.n, self.ndirs, self.K, self.M)
+        if want & _capi.WANT_SITE_LNL:
+            local = self.local.read_result(want)["site_lnl"] if self.end > self.begin else np.zeros(0)
+            out["site_lnl"] = self._gather_sites(np.asarray(local, dtype=np.float64)[: self.end - self.begin])
+        return out
+
+    def _eval_host(self, bl, want) -> dict:
         failed, err = False, None
         res = None
         try:

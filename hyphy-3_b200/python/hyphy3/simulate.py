@@ -254,6 +254,82 @@ class Workload:
 SEED_BASE = 20261203
 
 
+def simulate_gene(tree: TreeSpec, n_sites: int, rng: np.random.Generator, *, theta, pos_freq, omega) -> tuple[list[str], list[str]]:
+    """One-class MG94xREV codon sequences for the leaves of `tree`, sampled fast.
+
+    Same model as simulate_alignment with one omega class and no gaps or ambiguity codes, but
+    every node's states are drawn with one inverse-CDF search: the transition rows are laid end
+    to end, row s shifted by s, so the child state of a site whose parent is in state s is found by
+    searching s + u in the flattened cumulative table."""
+    codons, _ = universal_code()
+    n = len(tree.parent)
+    kids = [[] for _ in range(n)]
+    root = -1
+    for i, p in enumerate(tree.parent):
+        if p < 0:
+            root = i
+        else:
+            kids[p].append(i)
+    order = [root]
+    for u in order:
+        order.extend(kids[u])
+    Q, pi = mg94_generator(theta, omega, pos_freq)
+    expm = ReversibleExp(Q, pi)
+    S = len(pi)
+    shift = np.arange(S, dtype=float)[:, None]
+    states = np.zeros((n, n_sites), dtype=np.int64)
+    states[root] = rng.choice(S, size=n_sites, p=pi)
+    for u in order[1:]:
+        cum = np.cumsum(expm(tree.length[u]), axis=1)
+        cum /= cum[:, -1:]
+        flat = (cum + shift).ravel()
+        par = states[tree.parent[u]]
+        idx = np.searchsorted(flat, par + rng.random(n_sites), side="left")
+        states[u] = np.clip(idx - par * S, 0, S - 1)
+    table = np.array([NUC[a] + NUC[b] + NUC[c] for a, b, c in codons], dtype="S3")
+    names, seqs = [], []
+    for u in range(n):
+        if not kids[u]:
+            names.append(tree.names[u])
+            seqs.append(table[states[u]].tobytes().decode("ascii"))
+    return names, seqs
+
+
+@dataclasses.dataclass
+class Gene:
+    tree: TreeSpec
+    names: list[str]
+    seqs: list[str]
+    theta: list[float]
+    omega: float
+
+    @property
+    def newick(self) -> str:
+        return self.tree.newick()
+
+    @property
+    def n_sites(self) -> int:
+        return len(self.seqs[0]) // 3
+
+
+def make_gene_batch(n_genes: int = 500, *, taxa=(8, 512), sites=(100, 3000), seed: int | None = None) -> list[Gene]:
+    """The uneven multi-gene workload: n_genes alignments with taxa ~ U{taxa}, codons ~ U{sites},
+    each with its own random unrooted tree (branch lengths ~ Exp(mean 0.1)), GTR exchangeabilities
+    ~ U(0.5, 2), F3x4 generator frequencies ~ Dirichlet(1) per position and omega ~ U(0.1, 1)."""
+    rng = np.random.default_rng(SEED_BASE + 4 if seed is None else seed)
+    out = []
+    for _ in range(n_genes):
+        nt = int(rng.integers(taxa[0], taxa[1] + 1))
+        ns = int(rng.integers(sites[0], sites[1] + 1))
+        theta = list(rng.uniform(0.5, 2.0, size=5))
+        pos_freq = rng.dirichlet(np.ones(4), size=3)
+        omega = float(rng.uniform(0.1, 1.0))
+        tree = random_unrooted_tree(nt, rng, 0.1)
+        names, seqs = simulate_gene(tree, ns, rng, theta=theta, pos_freq=pos_freq, omega=omega)
+        out.append(Gene(tree, names, seqs, theta, omega))
+    return out
+
+
 def make_workload(config: int, *, n_sites: int | None = None, n_taxa: int | None = None) -> Workload:
     """Synthetic stand-ins for the five benchmark configurations (index 0..4); sizes may be shrunk for tests."""
     rng = np.random.default_rng(SEED_BASE + config)

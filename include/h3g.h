@@ -189,6 +189,20 @@ h3g_status h3g_batch_eval(h3g_batch* batch, const double* const* bl, unsigned wa
  * launch, host copies included) and the number of kernel launches in it. */
 h3g_status h3g_batch_last_stats(const h3g_batch* batch, double* device_ms, int* n_launches);
 
+/* The CUDA stream a context enqueues its work on (the one given to
+ * h3g_ctx_create, or its private stream). */
+h3g_status h3g_ctx_stream(const h3g_ctx* ctx, void** stream);
+
+/* For pattern-sharded evaluation across GPUs: after h3g_eval_resident, enqueue on
+ * the context stream the assembly of that evaluation's results into the caller's
+ * DEVICE vector d_vec of 1 + n_nodes + n_dirs + K + M + 1 doubles:
+ * [lnl, grad_t, grad_dir, grad_class_w, grad_rate_w, failed] (failed = 1 when a
+ * bounded device wait expired).  Every entry is a sum over site patterns, so the
+ * vectors of the ranks holding disjoint pattern ranges add up (one all-reduce) to
+ * the whole alignment's result, as the reference's per-tile pattern sums do
+ * (likelihood.hpp:794-806).  Returns without waiting. */
+h3g_status h3g_pack_result_device(h3g_problem* prob, unsigned want, double* d_vec);
+
 /* Limit of the waits the mixed-precision persistent passes make on one another's
  * items: polls before a wait gives up (0 = the default, about 2^22 polls of 64 ns).
  * An expired wait lets the kernel finish, and the evaluation returns
