@@ -4,7 +4,9 @@
 #include <cmath>
 #include <cstring>
 #include <exception>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -65,7 +67,9 @@ struct h3g_problem {
     int4* d_out_info = nullptr;
     int* d_chains = nullptr;           // [in_next | in_heads | out_next | out_heads]
     int n_in_heads = 0, n_out_heads = 0;
-    WaitCfg wait;                     // flag-wait limit of the persistent mixed passes
+    WaitCfg wait;                     // flag-wait limit and grid of the persistent mixed passes
+    h3g_tuning tuning{};              // launch shapes asked for (0 fields: the recorded tuning or the heuristic)
+    h3g_tuning applied{};             // launch shapes of the current workspace
     size_t off_in_heads = 0, off_out_next = 0, off_out_heads = 0;
     int8_t* d_states = nullptr;
     uint64_t* d_masks = nullptr;
@@ -444,6 +448,37 @@ static void pad_matrix(const double* src, int S, double* dst) {
 
 static size_t n_out_of(const h3g_problem* pr) { return 2 + size_t(pr->n) + 2 * size_t(pr->nmod) + pr->M; }
 
+// Tunings recorded by h3g_autotune, per problem shape (process-wide).
+struct TuneKey {
+    int device, n, NI, Pp, M, K, nmod, ndirs, precision;
+    bool operator<(const TuneKey& o) const {
+        const int a[] = {device, n, NI, Pp, M, K, nmod, ndirs, precision};
+        const int b[] = {o.device, o.n, o.NI, o.Pp, o.M, o.K, o.nmod, o.ndirs, o.precision};
+        return std::lexicographical_compare(a, a + 9, b, b + 9);
+    }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, h3g_tuning> g_tunings;
+
+static TuneKey tune_key(const h3g_problem* pr, int M, int K, int nmod, int ndirs) {
+    return {pr->ctx->device, pr->n, pr->NI, pr->Pp, M, K, nmod, ndirs, pr->precision};
+}
+
+// The launch shapes a problem runs with: the fields it set, else the tuning recorded for its shape,
+// else 0 (the heuristics).
+static h3g_tuning effective_tuning(const h3g_problem* pr, int M, int K, int nmod, int ndirs) {
+    h3g_tuning tu = pr->tuning;
+    if (tu.a_chunk > 0 && tu.ctas_per_sm > 0 && tu.frechet_groups > 0) return tu;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tunings.find(tune_key(pr, M, K, nmod, ndirs));
+    if (it != g_tunings.end()) {
+        if (tu.a_chunk <= 0) tu.a_chunk = it->second.a_chunk;
+        if (tu.ctas_per_sm <= 0) tu.ctas_per_sm = it->second.ctas_per_sm;
+        if (tu.frechet_groups <= 0) tu.frechet_groups = it->second.frechet_groups;
+    }
+    return tu;
+}
+
 // Element counts of every device buffer of one evaluation workspace, for a problem of n nodes, NI
 // internal nodes, Pp padded patterns and a model of (M, K, nmod, ndirs); plus the A-accumulation
 // chunking and the Frechet branch groups those dimensions get.  A batch slot serves several problems
@@ -461,7 +496,7 @@ struct WsLayout {
     }
 };
 
-static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod, int ndirs) {
+static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod, int ndirs, const h3g_tuning& tu) {
     (void)K;
     WsLayout L;
     L.n = n;
@@ -475,11 +510,13 @@ static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod
     const int max_chunks = std::max<int>(1, int(Pp / 256));
     L.nchunk = std::min(want_chunks, max_chunks);
     L.chunk = int((Pp / TP + L.nchunk - 1) / L.nchunk) * TP;
+    if (tu.a_chunk > 0) L.chunk = int(std::min<size_t>(Pp, size_t(std::max(2 * TP, tu.a_chunk / TP * TP))));
     L.nchunk = int((Pp + L.chunk - 1) / L.chunk);
     L.apart = n * M * size_t(L.nchunk) * SP2;
     L.afull = n * M * SP2;
     // Frechet branch groups: about two CTAs per SM over (group, rate class, model)
     L.ngroups = int(std::max<size_t>(1, std::min<size_t>(n, (296 + size_t(M) * nmod - 1) / (size_t(M) * nmod))));
+    if (tu.frechet_groups > 0) L.ngroups = int(std::min<size_t>(n, size_t(tu.frechet_groups)));
     const size_t G = size_t(L.ngroups);
     L.hpart = size_t(nmod) * M * G * SP2;
     L.gsz = size_t(nmod) * M * G;
@@ -566,7 +603,10 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     // offsets come from the installed model), so optimisers that alternate gradient and value-only evaluations
     // (different direction counts) do not reallocate
     size_t key[4] = {size_t(M), size_t(K), size_t(nmod), size_t(ndirs)};
-    if (pr->w.P && key[0] <= pr->work_key[0] && key[1] <= pr->work_key[1] && key[2] <= pr->work_key[2] &&
+    const h3g_tuning tu = effective_tuning(pr, M, K, nmod, ndirs);
+    pr->wait.ctas_per_sm = tu.ctas_per_sm > 0 ? tu.ctas_per_sm : 2;
+    const bool same_tuning = tu.a_chunk == pr->applied.a_chunk && tu.frechet_groups == pr->applied.frechet_groups;
+    if (pr->w.P && same_tuning && key[0] <= pr->work_key[0] && key[1] <= pr->work_key[1] && key[2] <= pr->work_key[2] &&
         key[3] <= pr->work_key[3])
         return H3G_OK;
     if (pr->w.P)
@@ -576,7 +616,8 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     pr->drop_graphs();
     pr->work_mem.release();
     std::copy(key, key + 4, pr->work_key);
-    const WsLayout L = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), M, K, nmod, ndirs);
+    const WsLayout L = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), M, K, nmod, ndirs, tu);
+    pr->applied = tu;
     h3g_status st = ws_alloc(ctx, L, pr->precision, pr->work_mem, pr->w, pr->mw);
     pr->w.bl = pr->d_bl;
     if (st != H3G_OK) { pr->work_mem.release(); pr->w = Work{}; pr->mw = MixedWork{}; }
@@ -945,6 +986,89 @@ extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want,
     return H3G_OK;
 }
 
+extern "C" h3g_status h3g_problem_set_tuning(h3g_problem* pr, const h3g_tuning* tu) {
+    if (!pr || !tu) return H3G_ERR_ARG;
+    if (tu->a_chunk < 0 || (tu->a_chunk > 0 && (tu->a_chunk % TP != 0 || tu->a_chunk < 2 * TP)))
+        return fail(pr->ctx, H3G_ERR_ARG, "a_chunk must be 0 or a multiple of 128 that is at least 256");
+    if (tu->ctas_per_sm < 0 || tu->ctas_per_sm > 2) return fail(pr->ctx, H3G_ERR_ARG, "ctas_per_sm must be 0, 1 or 2");
+    if (tu->frechet_groups < 0) return fail(pr->ctx, H3G_ERR_ARG, "frechet_groups must be >= 0");
+    pr->tuning = *tu;
+    pr->drop_graphs();               // launch shapes are captured in the graphs
+    if (pr->has_model) return ensure_workspace(pr, pr->M, pr->K, pr->nmod, pr->ndirs);
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_problem_get_tuning(const h3g_problem* pr, h3g_tuning* tu) {
+    if (!pr || !tu) return H3G_ERR_ARG;
+    const WsLayout L = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), std::max(pr->M, 1), pr->K,
+                                 std::max(pr->nmod, 1), pr->ndirs, effective_tuning(pr, pr->M, pr->K, pr->nmod, pr->ndirs));
+    tu->a_chunk = L.chunk;
+    tu->ctas_per_sm = pr->wait.ctas_per_sm;
+    tu->frechet_groups = L.ngroups;
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_autotune(h3g_problem* pr, const double* bl, unsigned want, int reps, h3g_tuning* best,
+                                   double* best_ms) {
+    if (!pr || !bl || reps < 1) return H3G_ERR_ARG;
+    h3g_ctx* ctx = pr->ctx;
+    if (pr->batch) return fail(ctx, H3G_ERR_STATE, "the problem belongs to a batch");
+    if (!pr->has_model) return fail(ctx, H3G_ERR_STATE, "h3g_autotune before h3g_model_set");
+    if (h3g_status st = check_bl(pr, bl); st != H3G_OK) return st;
+    cudaSetDevice(ctx->device);
+    const unsigned key = norm_want(want);
+    auto measure = [&](const h3g_tuning& tu, double* ms) -> h3g_status {
+        if (h3g_status st = h3g_problem_set_tuning(pr, &tu); st != H3G_OK) return st;
+        std::copy(bl, bl + pr->n, pr->h_pin);
+        pr->h_pin[pr->root] = 0.0;
+        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_bl, pr->h_pin, pr->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if (h3g_status st = run_eval(pr, key, false); st != H3G_OK) return st;      // warm-up (and graph capture)
+        H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        double tot = 0.0;
+        for (int r = 0; r < reps; ++r) {
+            if (h3g_status st = run_eval(pr, key, false); st != H3G_OK) return st;
+            H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            float m = 0.f;
+            cudaEventElapsedTime(&m, pr->ev0, pr->ev1);
+            tot += m;
+        }
+        *ms = tot / reps;
+        return H3G_OK;
+    };
+    const WsLayout L0 = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), pr->M, pr->K, pr->nmod, pr->ndirs, h3g_tuning{});
+    h3g_tuning cur{L0.chunk, 2, L0.ngroups};
+    double cur_ms = 0.0;
+    if (h3g_status st = measure(cur, &cur_ms); st != H3G_OK) return st;
+    auto uniq = [](std::vector<int> v) { std::sort(v.begin(), v.end()); v.erase(std::unique(v.begin(), v.end()), v.end()); return v; };
+    const int Pp = pr->Pp;
+    auto chunk_of = [&](int c) { return std::max(2 * TP, std::min(Pp, c / TP * TP)); };
+    std::vector<int> chunks = uniq({chunk_of(L0.chunk), chunk_of(Pp), chunk_of(Pp / 2), chunk_of(Pp / 4), chunk_of(Pp / 8),
+                                    chunk_of(1024), chunk_of(512), chunk_of(256)});
+    std::vector<int> groups = uniq({L0.ngroups, std::max(1, L0.ngroups / 2), std::min(pr->n, 2 * L0.ngroups),
+                                    std::min(pr->n, 4 * L0.ngroups)});
+    std::vector<int> ctas = pr->precision == H3G_PREC_MIXED ? std::vector<int>{2, 1} : std::vector<int>{2};
+    for (int field = 0; field < 3; ++field) {
+        const std::vector<int>& cand = field == 0 ? chunks : (field == 1 ? ctas : groups);
+        for (int v : cand) {
+            h3g_tuning tu = cur;
+            (field == 0 ? tu.a_chunk : (field == 1 ? tu.ctas_per_sm : tu.frechet_groups)) = v;
+            if (tu.a_chunk == cur.a_chunk && tu.ctas_per_sm == cur.ctas_per_sm && tu.frechet_groups == cur.frechet_groups)
+                continue;
+            double ms = 0.0;
+            if (h3g_status st = measure(tu, &ms); st != H3G_OK) return st;
+            if (ms < cur_ms) { cur = tu; cur_ms = ms; }
+        }
+    }
+    if (h3g_status st = h3g_problem_set_tuning(pr, &cur); st != H3G_OK) return st;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tunings[tune_key(pr, pr->M, pr->K, pr->nmod, pr->ndirs)] = cur;
+    }
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return H3G_OK;
+}
+
 extern "C" h3g_status h3g_pack_result_device(h3g_problem* pr, unsigned want, double* d_vec) {
     if (!pr || !d_vec) return H3G_ERR_ARG;
     if (!pr->has_model) return fail(pr->ctx, H3G_ERR_STATE, "h3g_pack_result_device before h3g_model_set");
@@ -1200,7 +1324,8 @@ static h3g_status batch_prepare(h3g_batch* b) {
     std::vector<WsLayout> lay(G);
     for (int g = 0; g < G; ++g) {
         const h3g_problem* pr = b->probs[g];
-        lay[g] = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), pr->M, pr->K, pr->nmod, pr->ndirs);
+        lay[g] = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), pr->M, pr->K, pr->nmod, pr->ndirs,
+                           effective_tuning(pr, pr->M, pr->K, pr->nmod, pr->ndirs));
     }
     const bool first = b->slots[0]->genes.empty() && b->slots[0]->w.P == nullptr;
     if (first || prec != b->precision) {

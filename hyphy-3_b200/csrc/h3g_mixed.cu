@@ -118,12 +118,10 @@ __device__ __forceinline__ MsgSrc msg_src(const Topo& t, const MixedWork& mw, in
     }
     return r;
 }
-// nv: how many of this thread's 16 states are real (S - 16 g, clamped to [0, 16]); the padding
-// states of stored partials are never written (zero since allocation) and never read.
-__device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG], int nv) {
+__device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG]) {
     if (r.stride != 1) {                // a message written by another CTA of this launch: read through L2
 #pragma unroll
-        for (int i = 0; i < kSG; ++i) a[i] = i < nv ? __ldcg(r.src + i * r.stride) : 0.f;
+        for (int i = 0; i < kSG; ++i) a[i] = __ldcg(r.src + i * r.stride);
     } else if (r.mk == 0) {
         const float4* s4 = reinterpret_cast<const float4*>(r.src);
 #pragma unroll
@@ -145,14 +143,13 @@ __device__ __forceinline__ void msg_load(const MsgSrc& r, float (&a)[kSG], int n
     }
 }
 
-__device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride, int nv) {
+__device__ __forceinline__ void load_part(float (&v)[kSG], const float* src, size_t stride) {
 #pragma unroll
-    for (int i = 0; i < kSG; ++i) v[i] = i < nv ? __ldcg(src + i * stride) : 0.f;
+    for (int i = 0; i < kSG; ++i) v[i] = __ldcg(src + i * stride);
 }
-__device__ __forceinline__ void store_part(const float (&v)[kSG], float* dst, size_t stride, int nv) {
+__device__ __forceinline__ void store_part(const float (&v)[kSG], float* dst, size_t stride) {
 #pragma unroll
-    for (int i = 0; i < kSG; ++i)
-        if (i < nv) dst[i * stride] = v[i];
+    for (int i = 0; i < kSG; ++i) dst[i * stride] = v[i];
 }
 
 // Shared-memory block of one tensor-core contraction.
@@ -366,7 +363,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
     __shared__ int s_item;
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
-    const int nv = min(kSG, max(0, t.S - kSG * l.g));     // real states among this thread's 16
     const int M = md.M, ntile = t.Pp / MT;
     const size_t Pp = size_t(t.Pp);
     const int epoch = __ldcg(mw.sync);
@@ -401,19 +397,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 if (k0 + 1 < k1) {
                     const MsgSrc s1 = msg_src(t, mw, m, M, t.kdesc[k0 + 1], p, l.g, so);
                     float b[kSG];
-                    msg_load(s0, v, nv);
-                    msg_load(s1, b, nv);
+                    msg_load(s0, v);
+                    msg_load(s1, b);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= b[i];
                     E += s1.E;
                 } else {
-                    msg_load(s0, v, nv);
+                    msg_load(s0, v);
                 }
                 E += renorm_row(v, s.smax, l);
                 for (int k = k0 + 2; k < k1; ++k) {
                     const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
                     float a[kSG];
-                    msg_load(sr, a, nv);
+                    msg_load(sr, a);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
                     E += sr.E + renorm_row(v, s.smax, l);
@@ -426,13 +422,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                     if (d.x == carried) continue;
                     const MsgSrc sr = msg_src(t, mw, m, M, d, p, l.g, so);
                     float a[kSG];
-                    msg_load(sr, a, nv);
+                    msg_load(sr, a);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
                     E += sr.E + renorm_row(v, s.smax, l);
                 }
             }
-            store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp, nv);
+            store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
             if (l.g == 0) mw.ED[col_off(iu, m, M, t.Pp) + p] = E;
             if (root) break;
             tc_write_part(s, v, l);
@@ -440,7 +436,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
             phase ^= 1u;
             const int sh = renorm_row(v, s.smax, l);
             E += sh;
-            store_part(v, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp, nv);
+            store_part(v, mw.Ms + part_off(iu, m, M, t.Pp) + so, Pp);
             if (l.g == 0) mw.EM[col_off(iu, m, M, t.Pp) + p] = E;
             const int nxt = t.in_next[pos];
             if (nxt < 0) break;
@@ -506,7 +502,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
     __shared__ int s_item;
     const TcTile s = carve(smraw);
     const Lane l = lane_of(threadIdx.x);
-    const int nv = min(kSG, max(0, t.S - kSG * l.g));     // real states among this thread's 16
     const int M = md.M, ntile = t.Pp / MT;
     const size_t Pp = size_t(t.Pp);
     const int epoch = __ldcg(mw.sync);
@@ -535,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                     for (int i = 0; i < kSG; ++i) v[i] = float(md.pi[kSG * l.g + i]);
                     EV = 0;
                 } else {
-                    load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp, nv);
+                    load_part(v, mw.U + part_off(iu, m, M, t.Pp) + so, Pp);
                     EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
                 }
             }
@@ -545,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                 if (sb.x == c) continue;
                 const MsgSrc sr = msg_src(t, mw, m, M, sb, p, l.g, so);
                 float a[kSG];
-                msg_load(sr, a, nv);
+                msg_load(sr, a);
 #pragma unroll
                 for (int i = 0; i < kSG; ++i) v[i] *= a[i];
                 EV += sr.E + renorm_row(v, s.smax, l);
@@ -556,14 +551,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
             const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
             float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
 #pragma unroll
-            for (int i = 0; i < kSG; ++i)
-                if (i < nv) vf[i * Pp] = float(double(v[i]) * scale);
+            for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
             if (!internal) break;                          // a leaf: no outside vector below it
             tc_write_part(s, v, l);
             tc_run(s, v, l, w.err, phase);                // v: U_c, the outside vector at c
             phase ^= 1u;
             EV += renorm_row(v, s.smax, l);
-            store_part(v, mw.U + part_off(ic, m, M, t.Pp) + so, Pp, nv);
+            store_part(v, mw.U + part_off(ic, m, M, t.Pp) + so, Pp);
             if (l.g == 0) mw.EU[col_off(ic, m, M, t.Pp) + p] = EV;
             const int nxt = t.out_next[pos];
             if (nxt < 0) { last = ic; break; }
@@ -614,6 +608,9 @@ constexpr uint32_t kRawRow = kAT * 4 + 16;                // padded FP32 row: co
 constexpr size_t kRawOp = size_t(SP) * kRawRow;           // 17 KB per operand
 constexpr size_t kRawSlot = 2 * kRawOp;                   // V and D
 constexpr size_t kAccSmem = 2 * kStage + kRing * kRawSlot + 8 * 2 + 16;
+// Two TMEM accumulator sets of 4 x 64 columns (all 512 columns: the shared memory above admits one
+// CTA per SM), so one group's drain overlaps the next group's products.
+constexpr uint32_t kAccSet = 256;
 
 struct Split8 { uint4 hi, mid, lo; };
 __device__ __forceinline__ Split8 split8(const float (&x)[8]) {
@@ -685,13 +682,7 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
         for (int q = 0; q < 2; ++q) tc::mbar_init(&mma_bar[q], 1);
         tc::mbar_fence_init();
     }
-    if (warp == 0) tc::tmem_alloc(slot, 256);
-    // the padding state rows of every ring slot are never copied: zero them once
-    for (int e = tid; e < kRing * 2 * (SP - t.S) * int(kRawRow / 4); e += kAccThreads) {
-        const int per_op = (SP - t.S) * int(kRawRow / 4), sl = e / (2 * per_op), rem = e % (2 * per_op);
-        const int op = rem / per_op, w4 = rem % per_op;
-        reinterpret_cast<uint32_t*>(ring + sl * kRawSlot + op * kRawOp + t.S * kRawRow)[w4] = 0u;
-    }
+    if (warp == 0) tc::tmem_alloc(slot, 2 * kAccSet);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
@@ -706,7 +697,6 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int c = tid + kAccThreads * q, r = c >> 4, c16 = c & 15;
-                if (r >= t.S) continue;            // padding state rows: zero in every slot (below)
                 cp_async16(dst + r * kRawRow + c16 * 16, Vb + size_t(r) * Pp + p0 + 4 * c16);
                 if (!lf) cp_async16(dst + kRawOp + r * kRawRow + c16 * 16, Db + size_t(r) * Pp + p0 + 4 * c16);
             }
@@ -728,6 +718,30 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
 #pragma unroll
     for (int x = 0; x < 16; ++x) dacc[x] = 0.0;
 
+    // Accumulator group G (tiles kADrain G .. kADrain G + kADrain - 1) runs on TMEM set G & 1; draining it
+    // waits for the commit of its last tile and adds the set into the FP64 registers.
+    auto drain = [&](int G) {
+        const int kl = min(ntile, (G + 1) * kADrain) - 1;
+        if (kl < 0) return;
+        if (!tc::mbar_wait(&mma_bar[kl & 1], uint32_t((kl >> 1) & 1)) && lane == 0) atomicOr(w.err, 8);
+        tc::tc_fence_after();
+        const uint32_t rowaddr = tmem + kAccSet * uint32_t(G & 1) + (uint32_t(32 * lq) << 16) + uint32_t(16 * cq);
+        // acc0, acc1 (internal branches) and acc2 (top rows) / acc3 (bottom rows, internal branches)
+        const uint32_t cols[3] = {0u, 64u, top ? 128u : 192u};
+        const bool use[3] = {true, !lf, top || !lf};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (!use[a]) continue;
+            float v16[16];
+            tc::tmem_ld16(rowaddr + cols[a], v16);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int x = 0; x < 16; ++x) dacc[x] += double(v16[x]);
+        }
+        tc::tc_fence_before();
+        __syncthreads();
+        tc::tc_fence_after();
+    };
     for (int q = 0; q < kRing - 1; ++q) produce(q);
     for (int kt = 0; kt < ntile; ++kt) {
         const int st = kt & 1, sl = kt % kRing;
@@ -767,44 +781,28 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
         if (tid == 0) {
             const uint32_t vs = tc::smem_u32(VS), ds = tc::smem_u32(DS);
             const bool first = (kt % kADrain) == 0;
+            const uint32_t set = tmem + kAccSet * uint32_t((kt / kADrain) & 1);     // this group's accumulators
 #pragma unroll
             for (int ks = 0; ks < kAT / 16; ++ks) {
                 const uint32_t acc = (first && ks == 0) ? 0u : 1u;
                 const uint64_t a1 = tc::smem_desc(vs + 1024 + 2 * ks * kVLbo, kVLbo, 128);   // [hi; mid]
                 const uint64_t a2 = tc::smem_desc(vs + 2 * ks * kVLbo, kVLbo, 128);          // [lo; hi]
                 const uint64_t bh = tc::smem_desc(ds + 2 * ks * kDLbo, kDLbo, 128);
-                tc::mma_bf16(tmem + 0, a1, bh, kIdesc, acc);
-                tc::mma_bf16(tmem + 128, a2, bh, kIdesc, acc);
+                tc::mma_bf16(set + 0, a1, bh, kIdesc, acc);
+                tc::mma_bf16(set + 128, a2, bh, kIdesc, acc);
                 if (!lf) {
                     const uint64_t bm = tc::smem_desc(ds + uint32_t(kDTerm) + 2 * ks * kDLbo, kDLbo, 128);
                     const uint64_t bl = tc::smem_desc(ds + uint32_t(2 * kDTerm) + 2 * ks * kDLbo, kDLbo, 128);
-                    tc::mma_bf16(tmem + 64, a1, bm, kIdesc, acc);
-                    tc::mma_bf16(tmem + 192, a2, bl, kIdesc, acc);
+                    tc::mma_bf16(set + 64, a1, bm, kIdesc, acc);
+                    tc::mma_bf16(set + 192, a2, bl, kIdesc, acc);
                 }
             }
             tc::mma_commit(&mma_bar[st]);
         }
-        if ((kt % kADrain) == kADrain - 1 || kt == ntile - 1) {
-            if (!tc::mbar_wait(&mma_bar[st], uint32_t((kt >> 1) & 1)) && lane == 0) atomicOr(w.err, 8);
-            tc::tc_fence_after();
-            const uint32_t rowaddr = tmem + (uint32_t(32 * lq) << 16) + uint32_t(16 * cq);
-            // acc0, acc1 (internal branches) and acc2 (top rows) / acc3 (bottom rows, internal branches)
-            const uint32_t cols[3] = {0u, 64u, top ? 128u : 192u};
-            const bool use[3] = {true, !lf, top || !lf};
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (!use[a]) continue;
-                float v16[16];
-                tc::tmem_ld16(rowaddr + cols[a], v16);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int x = 0; x < 16; ++x) dacc[x] += double(v16[x]);
-            }
-            tc::tc_fence_before();
-            __syncthreads();
-            tc::tc_fence_after();
-        }
+        // the previous group's accumulators drain while this tile's products run on the other set
+        if ((kt % kADrain) == 0 && kt > 0) drain(kt / kADrain - 1);
     }
+    drain((ntile - 1) / kADrain);
     // combine the two halves of each state row in shared memory (stages are idle now), write coalesced
     double* sA = reinterpret_cast<double*>(smraw);              // [64][65]
     const int i = 32 * lq + lane - (top ? 0 : 64);
@@ -822,7 +820,7 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
     for (int e = tid; e < SP2; e += kAccThreads) dst[e] = sA[(e >> 6) * 65 + (e & 63)];
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 256);
+    if (warp == 0) tc::tmem_dealloc(tmem, 2 * kAccSet);
 }
 
 }  // namespace
@@ -847,7 +845,7 @@ h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSize
     bool ok = take(&mw.D, part) && take(&mw.Ms, part) && take(&mw.U, part) && take(&mw.Vf, z.vf) &&
               take(&mw.ED, cols) && take(&mw.EM, cols) && take(&mw.EU, cols) && take(&mw.PT32, mats) &&
               take(&mw.rs32, z.rs);
-    // the padding states (S .. 63) of stored partials are never written: they stay zero from here
+    // partials start at zero (their padding states 61 .. 63 are then zero before any evaluation)
     ok = ok && cudaMemset(mw.D, 0, part * sizeof(float)) == cudaSuccess && cudaMemset(mw.Ms, 0, part * sizeof(float)) == cudaSuccess &&
          cudaMemset(mw.U, 0, part * sizeof(float)) == cudaSuccess &&
          cudaMemset(mw.Vf, 0, z.vf * sizeof(float)) == cudaSuccess;
@@ -863,19 +861,19 @@ int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork
     launch_k(k_prep_mx, dim3(t.n, md.M), 256, 0, s, t, md, w, mw);
     return 1;
 }
-static int persistent_ctas(int items) {
+static int persistent_ctas(int items, int per_sm) {
     static int sms = [] {
         int dev = 0, v = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
         return v;
     }();
-    return std::max(1, std::min(items, 2 * sms));
+    return std::max(1, std::min(items, std::max(1, std::min(per_sm, 2)) * sms));
 }
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
                         cudaStream_t s) {
     const int items = count * md.M * (t.Pp / MT);
-    launch_k(k_inside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
+    launch_k(k_inside_mx, persistent_ctas(items, wc.ctas_per_sm), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
     return 1;
 }
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
@@ -885,7 +883,7 @@ int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const Mixed
 int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
                          cudaStream_t s) {
     const int items = count * md.M * (t.Pp / MT);
-    launch_k(k_outside_mx, persistent_ctas(items), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
+    launch_k(k_outside_mx, persistent_ctas(items, wc.ctas_per_sm), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
     return 1;
 }
 int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {

@@ -39,6 +39,7 @@ struct MixedWork {
 struct WaitCfg {
     uint32_t polls = 1u << 22;
     int skew = 0;
+    int ctas_per_sm = 2;      // persistent grid: resident CTAs per SM (1 or 2; the kernels' resources admit 2)
 };
 
 bool mixed_available();

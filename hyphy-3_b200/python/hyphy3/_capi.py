@@ -28,11 +28,16 @@ EXPORTED = [
     "h3g_read_result", "h3g_profile_stages", "h3g_eval_from_P_noalloc", "h3g_fel_run", "h3g_meme_run",
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
     "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit", "h3g_batch_create", "h3g_batch_destroy", "h3g_batch_eval",
-    "h3g_batch_last_stats", "h3g_pack_result_device", "h3g_ctx_stream",
+    "h3g_batch_last_stats", "h3g_pack_result_device", "h3g_ctx_stream", "h3g_problem_set_tuning",
+    "h3g_problem_get_tuning", "h3g_autotune",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
 _dp = C.POINTER(C.c_double)
+
+
+class Tuning(C.Structure):
+    _fields_ = [("a_chunk", C.c_int), ("ctas_per_sm", C.c_int), ("frechet_groups", C.c_int)]
 
 
 class ModelDesc(C.Structure):
@@ -117,6 +122,9 @@ def load() -> C.CDLL:
         lib.h3g_batch_last_stats.argtypes = [vp, _dp, C.POINTER(C.c_int)]
         lib.h3g_pack_result_device.argtypes = [vp, C.c_uint, vp]
         lib.h3g_ctx_stream.argtypes = [vp, C.POINTER(vp)]
+        lib.h3g_problem_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        lib.h3g_problem_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        lib.h3g_autotune.argtypes = [vp, _dp, C.c_uint, C.c_int, C.POINTER(Tuning), _dp]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)
@@ -368,6 +376,22 @@ class Problem:
         """Polls before a persistent-pass flag wait gives up (0 = default); unmatched makes every such
         wait look for a value no item publishes (tests the H3G_ERR_TIMEOUT path)."""
         self.ctx.check(self.ctx.lib.h3g_problem_set_wait_limit(self.h, C.c_uint32(polls), C.c_int(int(unmatched))))
+
+    def set_tuning(self, a_chunk: int = 0, ctas_per_sm: int = 0, frechet_groups: int = 0) -> None:
+        """Launch shapes (h3g_problem_set_tuning); 0 = the recorded tuning or the heuristic."""
+        self.ctx.check(self.ctx.lib.h3g_problem_set_tuning(self.h, C.byref(Tuning(a_chunk, ctas_per_sm, frechet_groups))))
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        self.ctx.check(self.ctx.lib.h3g_problem_get_tuning(self.h, C.byref(t)))
+        return {"a_chunk": t.a_chunk, "ctas_per_sm": t.ctas_per_sm, "frechet_groups": t.frechet_groups}
+
+    def autotune(self, bl, want=WANT_LNL | WANT_GRAD_T, reps: int = 3) -> tuple[dict, float]:
+        """Time the launch-shape candidates (h3g_autotune), keep and record the fastest; (tuning, ms)."""
+        bl = _f64(bl)
+        t, ms = Tuning(), C.c_double()
+        self.ctx.check(self.ctx.lib.h3g_autotune(self.h, _ptr(bl), want, reps, C.byref(t), C.byref(ms)))
+        return {"a_chunk": t.a_chunk, "ctas_per_sm": t.ctas_per_sm, "frechet_groups": t.frechet_groups}, ms.value
 
     def pack_device(self, want, d_ptr: int) -> None:
         """Enqueue the assembly of the last resident evaluation's results into the device vector at d_ptr

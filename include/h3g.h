@@ -189,6 +189,29 @@ h3g_status h3g_batch_eval(h3g_batch* batch, const double* const* bl, unsigned wa
  * launch, host copies included) and the number of kernel launches in it. */
 h3g_status h3g_batch_last_stats(const h3g_batch* batch, double* device_ms, int* n_launches);
 
+/* ---------------------------------------------------------------- tuning
+ * Launch shapes that do not change results beyond rounding: the pattern chunk
+ * of the A accumulation (more chunks = more CTAs, more partial sums to reduce),
+ * the resident CTAs per SM of the mixed path's persistent passes, and the branch
+ * groups of the Frechet kernel.  0 in a field = the built-in heuristic.  The
+ * reference's counterpart is its fixed tile schedule (busted.hpp:385-401
+ * compute_tile_schedule, likelihood.hpp:91-104 optimal_omp_threads).
+ * h3g_autotune times the candidates of each field in turn (coordinate descent;
+ * reps evaluations each after one warm-up, CUDA events on the context stream),
+ * installs the fastest on the problem and records it for the problem's shape
+ * (nodes, internal nodes, padded patterns, M, K, models, directions, precision,
+ * device): later problems of that shape start from it.  Results are
+ * deterministic for a given tuning; tunings differ only in summation order. */
+typedef struct {
+    int a_chunk;          /* patterns per A-accumulation chunk: a multiple of 128, >= 256 */
+    int ctas_per_sm;      /* mixed persistent passes: 1 or 2 resident CTAs per SM */
+    int frechet_groups;   /* branch groups of the Frechet kernel: >= 1 */
+} h3g_tuning;
+h3g_status h3g_problem_set_tuning(h3g_problem* prob, const h3g_tuning* tuning);
+h3g_status h3g_problem_get_tuning(const h3g_problem* prob, h3g_tuning* tuning);
+/* Times evaluations at branch lengths bl[n_nodes]; best and best_ms may be NULL. */
+h3g_status h3g_autotune(h3g_problem* prob, const double* bl, unsigned want, int reps, h3g_tuning* best, double* best_ms);
+
 /* The CUDA stream a context enqueues its work on (the one given to
  * h3g_ctx_create, or its private stream). */
 h3g_status h3g_ctx_stream(const h3g_ctx* ctx, void** stream);
