@@ -591,8 +591,9 @@ BATCH_WORKLOAD = ("uneven multi-gene batch: {G} simulated genes, taxa ~ U{{8..51
                   "every branch length of every gene, all genes in one CUDA-graph launch over {S} slot workspaces")
 
 
-def _gene_problems(h, _capi, ctx, genes, precision):
-    """One device problem per gene with its MG94 model installed; the genes' host objects."""
+def _gene_problems(h, _capi, ctx, genes):
+    """One device problem per gene (no model yet: models go in once the problems belong to a batch,
+    whose slot workspaces they use); the genes' host objects."""
     probs, hosts = [], []
     for g in genes:
         aln = h.Alignment.from_sequences(g.names, g.seqs)
@@ -606,12 +607,16 @@ def _gene_problems(h, _capi, ctx, genes, precision):
         p = h.MG94Parameters()
         p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = g.theta
         p.beta = g.omega
-        e = h.mg94_eigensystem(aln, p)
-        pr.set_model(pi=aln.codon_frequencies, Q=e["Q"], lam=e["lam"], U=e["U"], V=e["V"], mu=[e["mu"]],
-                     precision=precision)
         probs.append(pr)
         hosts.append((aln, tree, p))
     return probs, hosts
+
+
+def _install_gene_models(h, probs, hosts, precision):
+    """Each gene's MG94 generator, diagonalised on the device."""
+    for pr, (aln, tree, p) in zip(probs, hosts):
+        e = h.mg94_eigensystem(aln, p)
+        pr.set_model(pi=aln.codon_frequencies, Q=e["Q"], mu=[e["mu"]], precision=precision)
 
 
 def run_batch(args) -> None:
@@ -630,15 +635,11 @@ def run_batch(args) -> None:
     steps, warm = args.steps, max(args.warmup, 3)
     for prec_name, prec in (("fp64", _capi.PREC_FP64), ("mixed", _capi.PREC_MIXED)):
         if batch is None:
-            probs, hosts = _gene_problems(h, _capi, ctx, genes, prec)
+            probs, hosts = _gene_problems(h, _capi, ctx, genes)
             batch = _capi.Batch(ctx, probs, n_slots=args.slots)
             bls = [np.array(tr.get_branch_lengths()) for _, tr, _ in hosts]
             units = sum(aln.num_sites * (tr.num_nodes() - 1) for aln, tr, _ in hosts)
-        else:
-            for pr, (aln, tree, p) in zip(probs, hosts):
-                e = h.mg94_eigensystem(aln, p)
-                pr.set_model(pi=aln.codon_frequencies, Q=e["Q"], lam=e["lam"], U=e["U"], V=e["V"], mu=[e["mu"]],
-                             precision=prec)
+        _install_gene_models(h, probs, hosts, prec)
         for _ in range(warm):
             batch.eval(bls, want)
         sampler = ClockSampler(0) if prec_name == "mixed" else None

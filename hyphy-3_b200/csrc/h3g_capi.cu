@@ -170,6 +170,7 @@ extern "C" h3g_status h3g_ctx_create(int device, void* cuda_stream, h3g_ctx** ou
         c->own_stream = true;
     }
     fp64_configure();
+    eigen_configure();
     mixed_configure();
     *out = c;
     return H3G_OK;
@@ -644,9 +645,11 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     if (d->K < 1 || d->M < 1 || d->M > kMaxRateClasses) return fail(ctx, H3G_ERR_ARG, "need K >= 1 and 1 <= M <= 16");
     if (d->has_bg < 0 || d->n_models != d->K + d->has_bg) return fail(ctx, H3G_ERR_ARG, "n_models must equal K + has_bg");
     if (d->has_bg > 1 && !d->bg_w) return fail(ctx, H3G_ERR_ARG, "several background classes need bg_w");
-    if (!d->pi || !d->Q || !d->lam || !d->U || !d->V || !d->class_w || !d->rates || !d->rate_w)
+    // U, V and lam all NULL: the device diagonalises every Q_k (h3g_eigen.cu)
+    const bool dev_eig = !d->U && !d->V && !d->lam;
+    if (!d->pi || !d->Q || (!dev_eig && (!d->lam || !d->U || !d->V)) || !d->class_w || !d->rates || !d->rate_w)
         return fail(ctx, H3G_ERR_ARG, "model arrays missing");
-    if (d->time_mode == H3G_TIME_NORMALIZED && !d->mu) return fail(ctx, H3G_ERR_ARG, "normalized time needs mu");
+    if (d->time_mode == H3G_TIME_NORMALIZED && !d->mu && !dev_eig) return fail(ctx, H3G_ERR_ARG, "normalized time needs mu");
     if (d->n_dirs < 0 || (d->n_dirs > 0 && !d->dQ)) return fail(ctx, H3G_ERR_ARG, "dQ directions missing");
     if (d->precision != H3G_PREC_FP64 && d->precision != H3G_PREC_MIXED) return fail(ctx, H3G_ERR_ARG, "unknown precision");
     if (d->precision == H3G_PREC_MIXED && !mixed_available()) return fail(ctx, H3G_ERR_CUDA, "mixed-precision path not built");
@@ -654,8 +657,9 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     if (pr->max_state >= S) return fail(ctx, H3G_ERR_ARG, "a pattern state index is >= S");
     auto finite = [](const double* a, size_t k) { for (size_t i = 0; i < k; ++i) if (!std::isfinite(a[i])) return false; return true; };
     if (d->bg_w && !finite(d->bg_w, size_t(d->has_bg))) return fail(ctx, H3G_ERR_NUMERIC, "non-finite background weights");
-    if (!finite(d->pi, S) || !finite(d->Q, size_t(nm) * S * S) || !finite(d->lam, size_t(nm) * S) || !finite(d->U, size_t(nm) * S * S) ||
-        !finite(d->V, size_t(nm) * S * S) || !finite(d->class_w, d->K) || !finite(d->rates, d->M) || !finite(d->rate_w, d->M))
+    if (!finite(d->pi, S) || !finite(d->Q, size_t(nm) * S * S) ||
+        (!dev_eig && (!finite(d->lam, size_t(nm) * S) || !finite(d->U, size_t(nm) * S * S) || !finite(d->V, size_t(nm) * S * S))) ||
+        !finite(d->class_w, d->K) || !finite(d->rates, d->M) || !finite(d->rate_w, d->M))
         return fail(ctx, H3G_ERR_NUMERIC, "non-finite model parameters");
     try {
         cudaSetDevice(ctx->device);
@@ -665,9 +669,12 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         h = hash_bytes(h, scal, sizeof(scal));
         h = hash_bytes(h, d->pi, S * sizeof(double));
         h = hash_bytes(h, d->Q, size_t(nm) * S * S * sizeof(double));
-        h = hash_bytes(h, d->lam, size_t(nm) * S * sizeof(double));
-        h = hash_bytes(h, d->U, size_t(nm) * S * S * sizeof(double));
-        h = hash_bytes(h, d->V, size_t(nm) * S * S * sizeof(double));
+        h = hash_bytes(h, &dev_eig, sizeof(dev_eig));
+        if (!dev_eig) {
+            h = hash_bytes(h, d->lam, size_t(nm) * S * sizeof(double));
+            h = hash_bytes(h, d->U, size_t(nm) * S * S * sizeof(double));
+            h = hash_bytes(h, d->V, size_t(nm) * S * S * sizeof(double));
+        }
         if (d->mu) h = hash_bytes(h, d->mu, nm * sizeof(double));
         h = hash_bytes(h, d->class_w, d->K * sizeof(double));
         if (d->bg_w) h = hash_bytes(h, d->bg_w, size_t(d->has_bg) * sizeof(double));
@@ -687,9 +694,11 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         std::copy(d->pi, d->pi + S, pi.begin());
         for (int k = 0; k < nm; ++k) {
             pad_matrix(d->Q + size_t(k) * S * S, S, &Q[size_t(k) * SP2]);
-            pad_matrix(d->U + size_t(k) * S * S, S, &U[size_t(k) * SP2]);
-            pad_matrix(d->V + size_t(k) * S * S, S, &V[size_t(k) * SP2]);
-            std::copy(d->lam + size_t(k) * S, d->lam + size_t(k) * S + S, &lam[size_t(k) * SP]);
+            if (!dev_eig) {
+                pad_matrix(d->U + size_t(k) * S * S, S, &U[size_t(k) * SP2]);
+                pad_matrix(d->V + size_t(k) * S * S, S, &V[size_t(k) * SP2]);
+                std::copy(d->lam + size_t(k) * S, d->lam + size_t(k) * S + S, &lam[size_t(k) * SP]);
+            }
             for (int i = 0; i < SP; ++i)
                 for (int j = 0; j < SP; ++j) {
                     UT[size_t(k) * SP2 + size_t(j) * SP + i] = U[size_t(k) * SP2 + size_t(i) * SP + j];
@@ -697,7 +706,16 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
                 }
         }
         std::vector<double> mu(nm, 1.0);
-        if (d->mu) std::copy(d->mu, d->mu + nm, mu.begin());
+        if (d->mu) {
+            std::copy(d->mu, d->mu + nm, mu.begin());
+        } else if (dev_eig) {
+            // the reference's scale_factor, stored but not applied (rate_matrix.hpp:228-233)
+            for (int k = 0; k < nm; ++k) {
+                double m = 0.0;
+                for (int i = 0; i < S; ++i) m -= d->pi[i] * d->Q[size_t(k) * S * S + size_t(i) * S + i];
+                mu[k] = m;
+            }
+        }
         pr->h_mu = mu;
         std::vector<double> dQ(size_t(std::max(d->n_dirs, 1)) * nm * SP2, 0.0);
         for (int x = 0; x < d->n_dirs; ++x)
@@ -734,11 +752,16 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         cudaStream_t s = ctx->stream;
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_pi, pi.data(), SP * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_Q, Q.data(), Q.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_lam, lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_U, U.data(), U.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_UT, UT.data(), UT.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_QT, QT.data(), QT.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_V, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (dev_eig) {
+            launch_model_eig(pr->m_Q, pr->m_pi, S, nm, pr->m_lam, pr->m_U, pr->m_UT, pr->m_V, s);
+            H3G_TRY_CUDA(ctx, cudaGetLastError());
+        } else {
+            H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_lam, lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_U, U.data(), U.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_UT, UT.data(), UT.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_V, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_mu, mu.data(), mu.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_cw, d->class_w, d->K * sizeof(double), cudaMemcpyHostToDevice, s));
         if (d->has_bg > 0) {
@@ -983,6 +1006,28 @@ extern "C" h3g_status h3g_eval(h3g_problem* pr, const double* bl, unsigned want,
     unpack_result(pr, norm_want(want), out);
     if (pr->h_pin[pr->off_out + 1] != 0.0) return timed_out(pr);
     if (!std::isfinite(out->lnl)) return fail(ctx, H3G_ERR_NUMERIC, "non-finite log-likelihood");
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_model_get_eigensystem(h3g_problem* pr, int k, double* lam, double* U, double* V) {
+    if (!pr || !lam || !U || !V) return H3G_ERR_ARG;
+    if (!pr->has_model) return fail(pr->ctx, H3G_ERR_STATE, "no model installed");
+    if (k < 0 || k >= pr->nmod) return fail(pr->ctx, H3G_ERR_ARG, "model index out of range");
+    cudaSetDevice(pr->ctx->device);
+    std::vector<double> l(SP), u(SP2), v(SP2);
+    cudaStream_t s = pr->ctx->stream;
+    H3G_TRY_CUDA(pr->ctx, cudaMemcpyAsync(l.data(), pr->m_lam + size_t(k) * SP, SP * sizeof(double), cudaMemcpyDeviceToHost, s));
+    H3G_TRY_CUDA(pr->ctx, cudaMemcpyAsync(u.data(), pr->m_U + size_t(k) * SP2, SP2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    H3G_TRY_CUDA(pr->ctx, cudaMemcpyAsync(v.data(), pr->m_V + size_t(k) * SP2, SP2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    H3G_TRY_CUDA(pr->ctx, cudaStreamSynchronize(s));
+    const int S = pr->S;
+    for (int i = 0; i < S; ++i) {
+        lam[i] = l[i];
+        for (int j = 0; j < S; ++j) {
+            U[size_t(i) * S + j] = u[size_t(i) * SP + j];
+            V[size_t(i) * S + j] = v[size_t(i) * SP + j];
+        }
+    }
     return H3G_OK;
 }
 

@@ -26,6 +26,7 @@
 
 #include "h3g_common.cuh"
 #include "h3g_fel.h"
+#include "h3g_jacobi.cuh"
 
 namespace h3g {
 
@@ -35,7 +36,7 @@ cudaStream_t problem_stream(h3g_problem* pr);      // h3g_capi.cu
 namespace {
 
 constexpr int kFT = 256;                  // threads per CTA
-constexpr int LD = SP + 1;                // padded row stride: column walks hit 32 distinct banks
+constexpr int LD = jac::LD;               // padded row stride: column walks hit 32 distinct banks
 constexpr int kMaxSweeps = 30;
 constexpr int kMaxDepth = 1024;           // open internal nodes on the traversal stack
 constexpr size_t kEigSmem = size_t(2) * SP * LD * sizeof(double);
@@ -53,20 +54,6 @@ struct FelModel {
     const uint8_t* bg;    // [n] 1 on a background branch (requests with a background eigensystem)
 };
 
-__device__ __forceinline__ double block_sum_or_max(double v, double* red, bool is_max) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const double w = __shfl_xor_sync(0xffffffffu, v, o);
-        v = is_max ? fmax(v, w) : v + w;
-    }
-    const int warp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) red[warp] = v;
-    __syncthreads();
-    double r = red[0];
-    for (int k = 1; k < kFT / 32; ++k) r = is_max ? fmax(r, red[k]) : r + red[k];
-    __syncthreads();
-    return r;
-}
-
 // ----------------------------------------------------------------- eigensystems
 // grid n_eig, block 256.  Jacobi rotations as in Golub & Van Loan (Alg. 8.5.3);
 // one sweep = 63 rounds of 32 disjoint pairs (circle schedule), each round
@@ -81,8 +68,7 @@ __global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __res
     extern __shared__ __align__(16) double sm[];
     double* A = sm;
     double* E = sm + SP * LD;
-    __shared__ double rc[32], rsn[32], rt[32], rapq[32], rapp[32], raqq[32], red[kFT / 32];
-    __shared__ int rp[32], rq[32];
+    __shared__ jac::Scratch js;
     const int tid = threadIdx.x, S = f.S;
     const double om = omega[blockIdx.x];
     const int sl = slot[blockIdx.x];
@@ -152,73 +138,7 @@ __global__ void __launch_bounds__(kFT) k_fel_eig(FelModel f, const double* __res
         }
         __syncthreads();
     }
-    for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
-        double off = 0.0, tot = 0.0;
-        for (int e = tid; e < SP2; e += kFT) {
-            const int i = e >> 6, j = e & 63;
-            const double x = A[i * LD + j] * A[i * LD + j];
-            tot += x;
-            if (i != j) off += x;
-        }
-        off = block_sum_or_max(off, red, false);
-        tot = block_sum_or_max(tot, red, false);
-        if (off <= 1e-30 * tot || off == 0.0) break;
-        // One round = 32 disjoint rotations (p_k, q_k), k < 32, covering all 64 indices.  Warp 0
-        // computes them (t from one square root and one divide, c = rsqrt(1 + t^2)); then every
-        // 2x2 block (I, J) of A is replaced by R_I^T A_IJ R_J in one pass, the diagonal blocks by
-        // their exact values a_pp - t a_pq, a_qq + t a_pq and 0 (Golub & Van Loan, Alg. 8.5.1),
-        // and the columns of E by E R.  Two barriers per round.
-        for (int round = 0; round < SP - 1; ++round) {
-            if (tid < 32) {
-                int p, q;
-                if (tid == 0) { p = SP - 1; q = round; }
-                else { p = (round + tid) % (SP - 1); q = (round - tid + (SP - 1)) % (SP - 1); }
-                if (p > q) { const int tmp = p; p = q; q = tmp; }
-                const double apq = A[p * LD + q], app = A[p * LD + p], aqq = A[q * LD + q];
-                double c = 1.0, s = 0.0, t = 0.0;
-                if (fabs(apq) >= 1e-300) {
-                    // t = tan(theta) of the smaller rotation, tau = (a_qq - a_pp) / (2 a_pq):
-                    // t = sign(tau) / (|tau| + sqrt(1 + tau^2)) = 2 a_pq sign(d) / (|d| + sqrt(d^2 + 4 a_pq^2)), d = a_qq - a_pp
-                    const double d = aqq - app;
-                    const double tt = 2.0 * apq / (fabs(d) + sqrt(d * d + 4.0 * apq * apq));
-                    t = d >= 0.0 ? tt : -tt;
-                    c = rsqrt(1.0 + t * t);
-                    s = t * c;
-                }
-                rp[tid] = p; rq[tid] = q; rc[tid] = c; rsn[tid] = s;
-                rt[tid] = t; rapq[tid] = apq; rapp[tid] = app; raqq[tid] = aqq;
-            }
-            __syncthreads();
-            for (int e = tid; e < 32 * 32; e += kFT) {      // block (I, J) of A
-                const int I = e >> 5, J = e & 31;
-                const int pI = rp[I], qI = rq[I], pJ = rp[J], qJ = rq[J];
-                if (I == J) {
-                    A[pI * LD + pI] = rapp[I] - rt[I] * rapq[I];
-                    A[qI * LD + qI] = raqq[I] + rt[I] * rapq[I];
-                    A[pI * LD + qI] = 0.0;
-                    A[qI * LD + pI] = 0.0;
-                    continue;
-                }
-                const double cI = rc[I], sI = rsn[I], cJ = rc[J], sJ = rsn[J];
-                const double a = A[pI * LD + pJ], b = A[pI * LD + qJ], cc = A[qI * LD + pJ], dd = A[qI * LD + qJ];
-                const double m0 = cJ * a - sJ * b, m1 = sJ * a + cJ * b;      // [a b; c d] R_J
-                const double m2 = cJ * cc - sJ * dd, m3 = sJ * cc + cJ * dd;
-                A[pI * LD + pJ] = cI * m0 - sI * m2;                        // R_I^T (...)
-                A[pI * LD + qJ] = cI * m1 - sI * m3;
-                A[qI * LD + pJ] = sI * m0 + cI * m2;
-                A[qI * LD + qJ] = sI * m1 + cI * m3;
-            }
-            for (int e = tid; e < 32 * SP; e += kFT) {      // columns p, q of E
-                const int k = e >> 6, i = e & 63;
-                const int p = rp[k], q = rq[k];
-                const double c = rc[k], s = rsn[k];
-                const double ekp = E[i * LD + p], ekq = E[i * LD + q];
-                E[i * LD + p] = c * ekp - s * ekq;
-                E[i * LD + q] = s * ekp + c * ekq;
-            }
-            __syncthreads();
-        }
-    }
+    jac::sweeps<kFT>(A, E, js, kMaxSweeps);
     double* lam = f.lam + size_t(sl) * SP;
     double* U = f.U + size_t(sl) * SP2;
     double* V = f.V + size_t(sl) * SP2;

@@ -16,6 +16,10 @@ int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_globa
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
 int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
 int launch_small(const Topo& t, const Model& md, const Work& w, int grads, cudaStream_t s);
+void eigen_configure();
+// Model eigensystems on the device (h3g_eigen.cu): Q [nmod][64*64] padded, pi [64] -> lam, U, U^T, V.
+int launch_model_eig(const double* Q, const double* pi, int S, int nmod, double* lam, double* U, double* UT, double* V,
+                     cudaStream_t s);
 int launch_pack_result(const Topo& t, const Model& md, const Work& w, int grads, int global, double* dst, cudaStream_t s);
 
 }  // namespace h3g

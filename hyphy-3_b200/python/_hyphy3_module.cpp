@@ -328,6 +328,12 @@ PYBIND11_MODULE(_hyphy3, m) {
         else throw std::runtime_error("precision must be 'fp64' or 'mixed'");
     }, "precision"_a);
     m.def("get_precision", []() { return LikelihoodEngine::get_precision() == H3G_PREC_MIXED ? "mixed" : "fp64"; });
+    m.def("set_eigensolver", [](const std::string& w) {
+        if (w == "device") LikelihoodEngine::set_device_eigensolver(true);
+        else if (w == "host") LikelihoodEngine::set_device_eigensolver(false);
+        else throw std::invalid_argument("eigensolver must be 'device' or 'host'");
+    }, py::arg("where"));
+    m.def("get_eigensolver", []() { return LikelihoodEngine::device_eigensolver() ? "device" : "host"; });
     m.def("library_version", []() { return std::string(h3g_version()); });
 
     // MG94 global fits (optimizer.hpp:741-1135)

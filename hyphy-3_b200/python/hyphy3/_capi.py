@@ -29,7 +29,7 @@ EXPORTED = [
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
     "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit", "h3g_batch_create", "h3g_batch_destroy", "h3g_batch_eval",
     "h3g_batch_last_stats", "h3g_pack_result_device", "h3g_ctx_stream", "h3g_problem_set_tuning",
-    "h3g_problem_get_tuning", "h3g_autotune",
+    "h3g_problem_get_tuning", "h3g_autotune", "h3g_model_get_eigensystem",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -125,6 +125,7 @@ def load() -> C.CDLL:
         lib.h3g_problem_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         lib.h3g_problem_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         lib.h3g_autotune.argtypes = [vp, _dp, C.c_uint, C.c_int, C.POINTER(Tuning), _dp]
+        lib.h3g_model_get_eigensystem.argtypes = [vp, C.c_int, _dp, _dp, _dp]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)
@@ -255,17 +256,23 @@ class Problem:
         except Exception:
             pass
 
-    def set_model(self, *, pi, Q, lam, U, V, mu=None, class_w=(1.0,), has_bg=False, is_test=None, rates=(1.0,),
+    def set_model(self, *, pi, Q, lam=None, U=None, V=None, mu=None, class_w=(1.0,), has_bg=False, is_test=None, rates=(1.0,),
                   rate_w=(1.0,), time_mode=TIME_RAW, dQ=None, precision=PREC_FP64, zero_l_sentinel=False,
                   bg_w=None) -> None:
         """Q, U, V: [n_models, S, S]; lam: [n_models, S]; dQ: [n_dirs, n_models, S, S].  bg_w: weights of
-        len(bg_w) background classes (models K ..), or None with has_bg for one background model."""
-        Q = _f64(Q); U = _f64(U); V = _f64(V); lam = _f64(lam)
+        len(bg_w) background classes (models K ..), or None with has_bg for one background model.
+        lam, U and V all None: the device diagonalises each Q (and mu defaults to -sum pi_i Q_ii)."""
+        Q = _f64(Q)
         if Q.ndim == 2:
-            Q, U, V, lam = Q[None], U[None], V[None], lam[None]
+            Q = Q[None]
+        dev_eig = U is None and V is None and lam is None       # the device diagonalises every Q_k
+        if not dev_eig:
+            U = _f64(U); V = _f64(V); lam = _f64(lam)
+            if U.ndim == 2:
+                U, V, lam = U[None], V[None], lam[None]
         nm, S = Q.shape[0], Q.shape[1]
         pi = _f64(pi)
-        mu_a = _f64(mu if mu is not None else np.ones(nm))
+        mu_a = None if (mu is None and dev_eig) else _f64(mu if mu is not None else np.ones(nm))
         cw = _f64(class_w); rt = _f64(rates); rw = _f64(rate_w)
         it = None if is_test is None else np.ascontiguousarray(is_test, dtype=np.uint8)
         dq = None if dQ is None else _f64(dQ)
@@ -280,7 +287,7 @@ class Problem:
                       rates=_ptr(rt), rate_w=_ptr(rw), time_mode=time_mode, n_dirs=nd, dQ=_ptr(dq),
                       precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)), bg_w=_ptr(bw))
         self.ctx.check(self.ctx.lib.h3g_model_set(self.h, C.byref(d)))
-        self.K, self.M, self.ndirs, self.nmod = len(cw), len(rt), nd, nm
+        self.K, self.M, self.ndirs, self.nmod, self.S = len(cw), len(rt), nd, nm, S
 
     def eval(self, bl, want=WANT_LNL | WANT_GRAD_T, out=None) -> dict:
         bl = _f64(bl)
@@ -305,8 +312,10 @@ class Problem:
         self.ctx.check(self.ctx.lib.h3g_eval_from_P(self.h, S, _ptr(P), _ptr(pi), C.byref(lnl), _ptr(site)))
         return lnl.value, site
 
-    def branch_length_gradients(self, *, pi, Q, lam, U, V, bl, precision=PREC_FP64) -> tuple[float, np.ndarray]:
-        pi, Q, lam, U, V, bl = (_f64(x) for x in (pi, Q, lam, U, V, bl))
+    def branch_length_gradients(self, *, pi, Q, lam=None, U=None, V=None, bl, precision=PREC_FP64) -> tuple[float, np.ndarray]:
+        """h3g_branch_length_gradients; lam, U, V all None: the device diagonalises Q."""
+        pi, Q, bl = (_f64(x) for x in (pi, Q, bl))
+        lam, U, V = (None if x is None else _f64(x) for x in (lam, U, V))
         lnl = C.c_double()
         g = np.zeros(self.n)
         self.ctx.check(self.ctx.lib.h3g_branch_length_gradients(
@@ -376,6 +385,13 @@ class Problem:
         """Polls before a persistent-pass flag wait gives up (0 = default); unmatched makes every such
         wait look for a value no item publishes (tests the H3G_ERR_TIMEOUT path)."""
         self.ctx.check(self.ctx.lib.h3g_problem_set_wait_limit(self.h, C.c_uint32(polls), C.c_int(int(unmatched))))
+
+    def get_eigensystem(self, k: int = 0) -> dict:
+        """The installed eigensystem of model k (given, or solved on the device): {"lam", "U", "V"}."""
+        S = self.S
+        lam, U, V = np.zeros(S), np.zeros((S, S)), np.zeros((S, S))
+        self.ctx.check(self.ctx.lib.h3g_model_get_eigensystem(self.h, k, _ptr(lam), _ptr(U), _ptr(V)))
+        return {"lam": lam, "U": U, "V": V}
 
     def set_tuning(self, a_chunk: int = 0, ctas_per_sm: int = 0, frechet_groups: int = 0) -> None:
         """Launch shapes (h3g_problem_set_tuning); 0 = the recorded tuning or the heuristic."""

@@ -79,7 +79,11 @@ typedef struct {
     const double* lam;        /* n_models * S eigenvalues (clamped <= 0) */
     const double* U;          /* n_models * S * S, U_pi */
     const double* V;          /* n_models * S * S, V_pi = U_pi^-1 */
-    const double* mu;         /* n_models mean rates (used by H3G_TIME_NORMALIZED) */
+                              /* lam, U and V all NULL: the device diagonalises every Q_k itself
+                                 (symmetrised with pi as rate_matrix.hpp:229-249 does, parallel
+                                 cyclic Jacobi in FP64); h3g_model_get_eigensystem reads the result */
+    const double* mu;         /* n_models mean rates (used by H3G_TIME_NORMALIZED); NULL with a
+                                 device eigensolve: -sum_i pi_i Q_k,ii */
     int K;                    /* test-branch classes */
     const double* class_w;    /* K mixing weights */
     int has_bg;               /* background classes (0: every branch is a test branch) */
@@ -188,6 +192,10 @@ h3g_status h3g_batch_eval(h3g_batch* batch, const double* const* bl, unsigned wa
 /* Device time of the last batch evaluation in ms (CUDA events around the graph
  * launch, host copies included) and the number of kernel launches in it. */
 h3g_status h3g_batch_last_stats(const h3g_batch* batch, double* device_ms, int* n_launches);
+
+/* The eigensystem of model k as installed (given, or solved on the device):
+ * lam[S], U[S*S], V[S*S] row-major. */
+h3g_status h3g_model_get_eigensystem(h3g_problem* prob, int k, double* lam, double* U, double* V);
 
 /* ---------------------------------------------------------------- tuning
  * Launch shapes that do not change results beyond rounding: the pattern chunk

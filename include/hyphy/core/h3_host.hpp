@@ -943,8 +943,10 @@ public:
     // rate_matrix.hpp:165-249: single-nucleotide changes weighted by
     // (alpha | beta) * theta * target positional frequency; double/triple hits
     // only with delta/psi > 0; the mean rate is stored but not applied.
+    // with_eigen = false builds the generator only (the device diagonalises it):
+    // eigenvalues, U_pi and V_pi stay empty.
     void update(const MG94Parameters& p, const double pos[3][4], const Vector& codon_freqs,
-                const GeneticCode& code = *GeneticCode::universal()) {
+                const GeneticCode& code = *GeneticCode::universal(), bool with_eigen = true) {
         S = code.num_sense_codons;
         pi = codon_freqs;
         double r[4][4];
@@ -968,6 +970,10 @@ public:
         }
         scale_factor = 0.0;
         for (int i = 0; i < S; ++i) scale_factor -= pi[size_t(i)] * Q(i, i);
+        if (!with_eigen) {
+            eigenvalues.clear(); U_pi = Matrix(); V_pi = Matrix();
+            return;
+        }
         sqrt_pi.resize(S); inv_sqrt_pi.resize(S);
         for (int i = 0; i < S; ++i) { sqrt_pi[i] = std::sqrt(std::max(pi[i], 1e-12)); inv_sqrt_pi[i] = 1.0 / sqrt_pi[i]; }
         std::vector<double> sym(size_t(S) * S);

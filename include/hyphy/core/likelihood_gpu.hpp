@@ -193,17 +193,23 @@ public:
         if (problems_.size() > 4) { h3g_problem_destroy(problems_.back().prob); problems_.pop_back(); }
         return pr;
     }
+    // true (default): models are installed as generators and diagonalised on the device
+    // (h3g_model_desc with NULL eigensystems); false: by the host's Householder + QL solver
+    static bool& device_eigen() { static bool on = true; return on; }
+
     const MG94Matrix& model(const MG94Parameters& p, const Alignment& aln) {
         const GeneticCode& code = aln.code ? *aln.code : *GeneticCode::universal();
+        const bool dev = device_eigen();
         uint64_t h = 1469598103934665603ull;
         h = fnv(h, &p, sizeof(p));
+        h = fnv(h, &dev, sizeof(dev));
         h = fnv(h, aln.pos_nuc_frequencies, sizeof(aln.pos_nuc_frequencies));
         h = fnv(h, aln.codon_frequencies_f3x4.data(), aln.codon_frequencies_f3x4.size() * 8);
         h = fnv(h, code.name.data(), code.name.size());
         for (auto it = models_.begin(); it != models_.end(); ++it)
             if (it->first == h) { models_.splice(models_.begin(), models_, it); return models_.front().second; }
         MG94Matrix m;
-        m.update(p, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code);
+        m.update(p, aln.pos_nuc_frequencies, aln.codon_frequencies_f3x4, code, !dev);
         models_.emplace_front(h, std::move(m));
         if (models_.size() > 32) models_.pop_back();
         return models_.front().second;
@@ -226,6 +232,7 @@ private:
 };
 
 // Packs eigensystems for h3g_model_desc.
+// (models built without an eigensystem leave lam, U, V empty: the device diagonalises Q).
 struct ModelPack {
     std::vector<double> Q, lam, U, V, mu, dQ;
     void add(const MG94Matrix& m) {
@@ -235,7 +242,11 @@ struct ModelPack {
         V.insert(V.end(), m.V_pi.v.begin(), m.V_pi.v.end());
         mu.push_back(m.scale_factor);
     }
+    const double* lam_p() const { return lam.empty() ? nullptr : lam.data(); }
+    const double* U_p() const { return U.empty() ? nullptr : U.data(); }
+    const double* V_p() const { return V.empty() ? nullptr : V.data(); }
 };
+inline const double* eig_ptr(const std::vector<double>& v) { return v.empty() ? nullptr : v.data(); }
 
 inline std::vector<double> node_lengths(const Tree& tree, const std::vector<Scalar>& bl) {
     std::vector<double> out(tree.num_nodes(), 0.0);
@@ -249,6 +260,10 @@ inline std::vector<double> node_lengths(const Tree& tree, const std::vector<Scal
 class LikelihoodEngine {
 public:
     static void set_precision(h3g_precision p) { gpu_detail::Engine::precision() = p; }
+    // Where MG94 eigensystems are solved: on the device (default: generators are installed and
+    // diagonalised there, h3g_model_desc with NULL eigensystems) or by the host's Householder + QL.
+    static void set_device_eigensolver(bool on) { gpu_detail::Engine::device_eigen() = on; }
+    static bool device_eigensolver() { return gpu_detail::Engine::device_eigen(); }
     static h3g_precision get_precision() { return gpu_detail::Engine::precision(); }
 
     static std::vector<size_t> build_leaf_to_taxon_map(const Tree& tree, const Alignment& aln) {
@@ -285,8 +300,9 @@ public:
         std::vector<Scalar> grad(tree.num_nodes(), 0.0);
         double lnl = 0.0;
         eng.set_installed(pr, 0);
-        eng.check(h3g_branch_length_gradients(pr, mg.S, aln.codon_frequencies_f3x4.data(), mg.Q.data(), mg.eigenvalues.data(),
-                                              mg.U_pi.data(), mg.V_pi.data(), bl.data(), int(get_precision()), &lnl, grad.data()));
+        eng.check(h3g_branch_length_gradients(pr, mg.S, aln.codon_frequencies_f3x4.data(), mg.Q.data(),
+                                              gpu_detail::eig_ptr(mg.eigenvalues), gpu_detail::eig_ptr(mg.U_pi.v),
+                                              gpu_detail::eig_ptr(mg.V_pi.v), bl.data(), int(get_precision()), &lnl, grad.data()));
         return {lnl, grad};
     }
 
@@ -326,7 +342,7 @@ public:
         const double one = 1.0;
         h3g_model_desc d{};
         d.S = S; d.pi = aln.codon_frequencies_f3x4.data(); d.n_models = nm;
-        d.Q = mp.Q.data(); d.lam = mp.lam.data(); d.U = mp.U.data(); d.V = mp.V.data(); d.mu = mp.mu.data();
+        d.Q = mp.Q.data(); d.lam = mp.lam_p(); d.U = mp.U_p(); d.V = mp.V_p(); d.mu = mp.mu.data();
         d.K = 1; d.class_w = &one; d.has_bg = part ? 1 : 0; d.is_test = part ? it.data() : nullptr;
         d.M = 1; d.rates = &one; d.rate_w = &one; d.time_mode = H3G_TIME_NORMALIZED;
         d.n_dirs = int(dirs.size()); d.dQ = mp.dQ.data(); d.precision = int(get_precision()); d.zero_l_sentinel = 0;
@@ -434,7 +450,7 @@ public:
         }
         h3g_model_desc d{};
         d.S = S; d.pi = aln.codon_frequencies_f3x4.data(); d.n_models = nm;
-        d.Q = mp.Q.data(); d.lam = mp.lam.data(); d.U = mp.U.data(); d.V = mp.V.data(); d.mu = mp.mu.data();
+        d.Q = mp.Q.data(); d.lam = mp.lam_p(); d.U = mp.U_p(); d.V = mp.V_p(); d.mu = mp.mu.data();
         d.K = K; d.class_w = weights.data(); d.has_bg = Kb; d.is_test = it.data();
         d.bg_w = bg_omegas.empty() ? nullptr : bg_weights.data();
         d.M = M; d.rates = syn_rates.data(); d.rate_w = syn_weights.data(); d.time_mode = H3G_TIME_RAW;

@@ -1,11 +1,12 @@
 """The reference-facing API (_hyphy3, hyphy3.autograd) on the device.
 
-The API diagonalises Q with the library's host eigensolver (Householder + QL); the
-oracle is handed that same eigensystem ("eig" in its parameters), so lnL and every
-gradient are compared like with like at the FP64 bound, 1e-10.  Against the oracle's
-own cyclic-Jacobi eigensystem the comparison is at the floor two correct FP64
-eigensolvers leave (tests/test_eigen_floor.py pins it on the CPU: lnL within 1e-11,
-gradients within 5e-10).
+The API installs MG94 generators and the device diagonalises them (parallel cyclic
+Jacobi, h3g_eigen.cu).  The oracle is handed that same eigensystem ("eig" in its
+parameters; read back through h3g_model_get_eigensystem from the same generator), so
+lnL and every gradient are compared like with like at the FP64 bound, 1e-10.  Against
+the oracle's own Jacobi eigensystem the comparison is at the floor two correct FP64
+eigensolvers leave (tests/test_eigen_floor.py pins it on the CPU for the host solver,
+tests/test_gpu_eigen.py for the device one: gradients within 5e-10).
 """
 import math
 
@@ -19,13 +20,29 @@ TOL_API = 1e-10
 TOL_EIG_FLOOR = 5e-10
 
 
+_EIG_CTX = []
+
+
 def host_eig(h3, aln, beta, theta=(1, 1, 1, 1, 1)):
-    """The library's own eigensystem of MG94(beta, theta) on aln, in the oracle's "eig" form."""
+    """The eigensystem the API installs for MG94(beta, theta) on aln, in the oracle's "eig" form: the
+    device's (the default eigensolver: the same generator diagonalised by the same kernel through the
+    C ABI) or, with set_eigensolver("host"), the host solver's."""
+    from hyphy3 import _capi
     p = h3.MG94Parameters()
     p.beta = beta
     p.theta_AC, p.theta_AT, p.theta_CG, p.theta_CT, p.theta_GT = theta
     e = h3.mg94_eigensystem(aln, p)
-    return {"U": np.asarray(e["U"]), "V": np.asarray(e["V"]), "lam": np.asarray(e["lam"])}
+    if h3.get_eigensolver() == "host":
+        return {"U": np.asarray(e["U"]), "V": np.asarray(e["V"]), "lam": np.asarray(e["lam"])}
+    if not _EIG_CTX:
+        _EIG_CTX.append(_capi.Context(0))
+    pr = _capi.Problem(_EIG_CTX[0], np.array([-1, 0, 0, 0], dtype=np.int32), np.array([0, 1, 1, 1], dtype=np.uint8),
+                       np.array([-1, 0, 1, 2], dtype=np.int32), np.zeros((1, 3), dtype=np.int8),
+                       np.zeros((1, 3), dtype=np.uint64), np.ones(1))
+    pr.set_model(pi=np.asarray(aln.codon_frequencies), Q=np.asarray(e["Q"]))
+    out = pr.get_eigensystem(0)
+    pr.close()
+    return out
 
 
 @pytest.fixture(scope="module")

@@ -36,10 +36,12 @@ def test_autotune_keeps_results_and_records_the_choice(oracle, precision_name):
     assert ms > 0 and best["a_chunk"] % 128 == 0 and best["ctas_per_sm"] in (1, 2) and best["frechet_groups"] >= 1
     assert pr.get_tuning() == best
     tuned = pr.eval(bl, want)
-    tol = 1e-12 if precision_name == "fp64" else 1e-9
-    assert abs(tuned["lnl"] - base["lnl"]) <= tol * abs(base["lnl"])
-    assert rel(tuned["grad_t"], base["grad_t"]) < tol * 10
-    assert rel(tuned["grad_dir"], base["grad_dir"]) < tol * 10
+    # lnL does not depend on the launch shapes; the gradients' A sums are regrouped: rounding of FP64
+    # partial sums (FP64 path), FP32 accumulator groups (mixed path, well inside its 1e-5 bound)
+    assert abs(tuned["lnl"] - base["lnl"]) <= 1e-13 * abs(base["lnl"])
+    gtol = 1e-11 if precision_name == "fp64" else 1e-6
+    assert rel(tuned["grad_t"], base["grad_t"]) < gtol
+    assert rel(tuned["grad_dir"], base["grad_dir"]) < gtol
     if precision_name == "fp64":
         ref = oracle.mixture_eval(t, a, models, list(wl.omega_w), None, [], [], [], list(bl), False, True, False)
         assert abs(tuned["lnl"] - ref["lnl"]) / abs(ref["lnl"]) < 1e-10
@@ -48,7 +50,8 @@ def test_autotune_keeps_results_and_records_the_choice(oracle, precision_name):
     pr.set_tuning(a_chunk=256, ctas_per_sm=1, frechet_groups=3)
     assert pr.get_tuning() == {"a_chunk": 256, "ctas_per_sm": 1, "frechet_groups": 3}
     alt = pr.eval(bl, want)
-    assert abs(alt["lnl"] - base["lnl"]) <= tol * abs(base["lnl"])
+    assert abs(alt["lnl"] - base["lnl"]) <= 1e-13 * abs(base["lnl"])
+    assert rel(alt["grad_t"], base["grad_t"]) < gtol
     with pytest.raises(_capi.H3GError):
         pr.set_tuning(a_chunk=200)
     # a new problem of the same shape starts from the recorded tuning
