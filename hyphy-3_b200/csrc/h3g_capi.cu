@@ -101,6 +101,7 @@ struct h3g_problem {
     double *m_cw = nullptr, *m_bw = nullptr, *m_rt = nullptr, *m_rw = nullptr, *m_dQ = nullptr;
     std::vector<double> h_bw;   // background weights as uploaded (ones when the caller gives none)
     uint8_t* m_it = nullptr;
+    int* m_br = nullptr;               // per-branch class offsets (branch_classes)
     // captured evaluation graphs, keyed by (want, with host copies)
     // the site-fit evaluator of the last h3g_fel_run / h3g_meme_run, kept for the next run
     h3g::FelDevice* fel_dev = nullptr;
@@ -645,6 +646,14 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
     if (d->K < 1 || d->M < 1 || d->M > kMaxRateClasses) return fail(ctx, H3G_ERR_ARG, "need K >= 1 and 1 <= M <= 16");
     if (d->has_bg < 0 || d->n_models != d->K + d->has_bg) return fail(ctx, H3G_ERR_ARG, "n_models must equal K + has_bg");
     if (d->has_bg > 1 && !d->bg_w) return fail(ctx, H3G_ERR_ARG, "several background classes need bg_w");
+    if (d->branch_classes) {
+        if (d->has_bg != 0 || d->is_test) return fail(ctx, H3G_ERR_ARG, "per-branch classes exclude has_bg and is_test");
+        const int32_t* o = d->branch_classes;
+        for (int b = 0; b < pr->n; ++b) {
+            if (o[b] < 0 || o[b + 1] > d->K || o[b + 1] < o[b]) return fail(ctx, H3G_ERR_ARG, "branch_classes must be non-decreasing in [0, K]");
+            if (b != pr->root && o[b + 1] == o[b]) return fail(ctx, H3G_ERR_ARG, "every branch needs at least one class");
+        }
+    }
     // U, V and lam all NULL: the device diagonalises every Q_k (h3g_eigen.cu)
     const bool dev_eig = !d->U && !d->V && !d->lam;
     if (!d->pi || !d->Q || (!dev_eig && (!d->lam || !d->U || !d->V)) || !d->class_w || !d->rates || !d->rate_w)
@@ -681,6 +690,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         h = hash_bytes(h, d->rates, d->M * sizeof(double));
         h = hash_bytes(h, d->rate_w, d->M * sizeof(double));
         if (d->is_test) h = hash_bytes(h, d->is_test, size_t(pr->n));
+        if (d->branch_classes) h = hash_bytes(h, d->branch_classes, size_t(pr->n + 1) * sizeof(int32_t));
         if (d->n_dirs > 0) h = hash_bytes(h, d->dQ, size_t(d->n_dirs) * nm * S * S * sizeof(double));
         if (pr->has_model && h == pr->model_hash) return H3G_OK;
         cudaStreamSynchronize(ctx->stream);
@@ -747,6 +757,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_rw, cM));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_dQ, cdirs * cnm * SP2));
             H3G_TRY_CUDA(ctx, A.alloc(&pr->m_it, it.size()));
+            H3G_TRY_CUDA(ctx, A.alloc(&pr->m_br, size_t(pr->n) + 1));
             std::copy(mkey, mkey + 5, pr->model_key);
         }
         cudaStream_t s = ctx->stream;
@@ -773,12 +784,16 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_rw, d->rate_w, d->M * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_dQ, dQ.data(), dQ.size() * sizeof(double), cudaMemcpyHostToDevice, s));
         H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_it, it.data(), it.size(), cudaMemcpyHostToDevice, s));
+        if (d->branch_classes)
+            H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_br, d->branch_classes, size_t(pr->n + 1) * sizeof(int32_t),
+                                              cudaMemcpyHostToDevice, s));
         Model md{};
         md.M = d->M; md.K = d->K; md.has_bg = d->has_bg; md.nmod = nm; md.time_mode = d->time_mode; md.ndirs = d->n_dirs;
         md.sentinel = d->zero_l_sentinel;
         md.pi = pr->m_pi; md.Q = pr->m_Q; md.lam = pr->m_lam; md.U = pr->m_U; md.V = pr->m_V; md.mu = pr->m_mu;
         md.UT = pr->m_UT; md.QT = pr->m_QT;
         md.class_w = pr->m_cw; md.bg_w = pr->m_bw; md.rates = pr->m_rt; md.rate_w = pr->m_rw; md.is_test = d->is_test ? pr->m_it : nullptr;
+        md.br_off = d->branch_classes ? pr->m_br : nullptr;
         md.dQ = pr->m_dQ;
         if (std::memcmp(&md, &pr->md, sizeof(Model)) != 0) pr->drop_graphs();
         pr->md = md;

@@ -92,6 +92,7 @@ struct Model {
     const double* rates;     // [M]
     const double* rate_w;    // [M]
     const uint8_t* is_test;  // [n] or null
+    const int* br_off;       // [n + 1] or null: branch b mixes classes [br_off[b], br_off[b + 1]) with class_w
     const double* dQ;        // [ndirs][nmod][64*64]
 };
 
@@ -129,6 +130,21 @@ struct Work {
 __device__ __forceinline__ size_t mat_off(int m, int b, int n) { return (size_t(m) * n + b) * SP2; }
 __device__ __forceinline__ size_t part_off(int ii, int m, int M, int Pp) { return (size_t(ii) * M + m) * SP * size_t(Pp); }
 __device__ __forceinline__ size_t col_off(int ii, int m, int M, int Pp) { return (size_t(ii) * M + m) * size_t(Pp); }
+
+// The classes a branch mixes and the weight of class k on it: a per-branch range of the class
+// table (br_off), else the K test classes on test branches and the background classes elsewhere.
+struct BranchModels {
+    int k0, k1;
+    bool test;
+};
+__device__ __forceinline__ BranchModels branch_models(const Model& md, int b) {
+    if (md.br_off) return {md.br_off[b], md.br_off[b + 1], true};
+    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
+    return {test ? 0 : md.K, test ? md.K : md.nmod, test};
+}
+__device__ __forceinline__ double class_weight(const Model& md, const BranchModels& bm, int k) {
+    return bm.test ? md.class_w[k] : md.bg_w[k - md.K];
+}
 
 __device__ __forceinline__ double time_conv(const Model& md, int k) {
     return md.time_mode == 1 ? 3.0 / fmax(md.mu[k], 1e-12) : 1.0;

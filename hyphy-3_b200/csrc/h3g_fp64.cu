@@ -130,13 +130,12 @@ __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
     __shared__ double se[SP];
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
     if (b == t.root) return;
-    const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-    const int k0 = test ? 0 : md.K, k1 = test ? md.K : md.nmod;
+    const BranchModels bm = branch_models(md, b);
     Frag64 accP, accD;
     frag_zero(accP);
     frag_zero(accD);
-    for (int k = k0; k < k1; ++k) {
-        const double cw = test ? md.class_w[k] : md.bg_w[k - md.K];
+    for (int k = bm.k0; k < bm.k1; ++k) {
+        const double cw = class_weight(md, bm, k);
         const double cv = time_conv(md, k);
         const double rate = md.rates[m];
         const double tau = rate * w.bl[b] * cv;
@@ -611,9 +610,9 @@ __global__ void __launch_bounds__(256) k_frechet(Topo t, Model md, Work w, int G
     double dg = 0.0, dq = 0.0;
     for (int b = g; b < n; b += G) {
         if (b == t.root) continue;
-        const bool test = md.is_test == nullptr || md.is_test[b] != 0;
-        if ((k < md.K) != test) continue;
-        const double cw = test ? md.class_w[k] : md.bg_w[k - md.K];
+        const BranchModels bm = branch_models(md, b);
+        if (k < bm.k0 || k >= bm.k1) continue;
+        const double cw = class_weight(md, bm, k);
         const double tau = md.rates[m] * w.bl[b] * time_conv(md, k);
         __syncthreads();                                  // the previous branch is done with sA
         {

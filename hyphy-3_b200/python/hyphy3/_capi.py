@@ -46,6 +46,7 @@ class ModelDesc(C.Structure):
         ("mu", _dp), ("K", C.c_int), ("class_w", _dp), ("has_bg", C.c_int), ("is_test", C.POINTER(C.c_uint8)),
         ("M", C.c_int), ("rates", _dp), ("rate_w", _dp), ("time_mode", C.c_int), ("n_dirs", C.c_int),
         ("dQ", _dp), ("precision", C.c_int), ("zero_l_sentinel", C.c_int), ("bg_w", _dp),
+        ("branch_classes", C.POINTER(C.c_int32)),
     ]
 
 
@@ -258,7 +259,7 @@ class Problem:
 
     def set_model(self, *, pi, Q, lam=None, U=None, V=None, mu=None, class_w=(1.0,), has_bg=False, is_test=None, rates=(1.0,),
                   rate_w=(1.0,), time_mode=TIME_RAW, dQ=None, precision=PREC_FP64, zero_l_sentinel=False,
-                  bg_w=None) -> None:
+                  bg_w=None, branch_classes=None) -> None:
         """Q, U, V: [n_models, S, S]; lam: [n_models, S]; dQ: [n_dirs, n_models, S, S].  bg_w: weights of
         len(bg_w) background classes (models K ..), or None with has_bg for one background model.
         lam, U and V all None: the device diagonalises each Q (and mu defaults to -sum pi_i Q_ii)."""
@@ -278,6 +279,8 @@ class Problem:
         dq = None if dQ is None else _f64(dQ)
         nd = 0 if dq is None else int(dq.shape[0])
         bw = None if bg_w is None else _f64(bg_w)
+        bc = None if branch_classes is None else np.ascontiguousarray(branch_classes, dtype=np.int32)
+        self._bc = bc                                    # kept alive while the model is installed
         if bw is not None:
             nbg = int(bw.size)
         else:
@@ -285,7 +288,8 @@ class Problem:
         d = ModelDesc(S=S, pi=_ptr(pi), n_models=nm, Q=_ptr(Q), lam=_ptr(lam), U=_ptr(U), V=_ptr(V), mu=_ptr(mu_a),
                       K=len(cw), class_w=_ptr(cw), has_bg=nbg, is_test=_ptr(it, C.c_uint8), M=len(rt),
                       rates=_ptr(rt), rate_w=_ptr(rw), time_mode=time_mode, n_dirs=nd, dQ=_ptr(dq),
-                      precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)), bg_w=_ptr(bw))
+                      precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)), bg_w=_ptr(bw),
+                      branch_classes=_ptr(bc, C.c_int32))
         self.ctx.check(self.ctx.lib.h3g_model_set(self.h, C.byref(d)))
         self.K, self.M, self.ndirs, self.nmod, self.S = len(cw), len(rt), nd, nm, S
 

@@ -98,6 +98,13 @@ typedef struct {
     int zero_l_sentinel;      /* 1: a pattern with L <= 0 adds weight * -1e20 to lnL (evaluate_log_l);
                                  0: it adds 0 (the gradient entry points) */
     const double* bg_w;       /* has_bg background mixing weights; NULL allowed only when has_bg <= 1 */
+    const int32_t* branch_classes;
+                              /* NULL, or n_nodes + 1 offsets into the K classes: branch b mixes classes
+                                 [branch_classes[b], branch_classes[b + 1]) with weights class_w (a
+                                 distribution of its own per branch, as aBSREL's branch-site models,
+                                 absrel.hpp:262-310); needs has_bg = 0 and is_test = NULL; the root's
+                                 range is ignored.  grad_class_w then holds every class's weight
+                                 partial. */
 } h3g_model_desc;
 
 typedef struct {

@@ -1083,6 +1083,8 @@ struct MixSpec {
     bool want_global = false;
     bool zero_l_sentinel = false;      // true: L<=0 contributes w * -1e20 to lnL
     bool tiled = false;                // true: 64-pattern tiles with S x B GEMMs (the reference's batched shape)
+    std::vector<int> branch_classes;   // empty, or n + 1 offsets: branch b mixes classes [bc[b], bc[b+1]) (aBSREL,
+                                       // absrel.hpp:262-276: P_b = sum_k w_bk P(omega_bk, t_b))
 };
 struct MixResult {
     double lnl = 0;
@@ -1100,6 +1102,9 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
     const int K = int(sp.classes.size()), M = int(sp.rates.size());
     auto l2t = leaf_map(tr, a);
     auto test = [&](int b) { return sp.is_test.empty() ? true : bool(sp.is_test[b]); };
+    // the test classes branch b mixes: all K, or its own range of them
+    auto kb0 = [&](int b) { return sp.branch_classes.empty() ? 0 : sp.branch_classes[size_t(b)]; };
+    auto kb1 = [&](int b) { return sp.branch_classes.empty() ? K : sp.branch_classes[size_t(b) + 1]; };
     std::vector<MG94> mk(K); for (int k = 0; k < K; ++k) mk[k].update(sp.classes[k], a.pos_freq, a.pi, a.code);
     MG94 mbg; if (sp.has_bg) mbg.update(sp.bg, a.pos_freq, a.pi, a.code);
     auto conv = [&](const MG94& m) { return sp.normalized_time ? 3.0 / std::max(m.mu, 1e-12) : 1.0; };
@@ -1115,7 +1120,7 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
         if (test(b)) {
             Pm[m][b] = Mat(S, S);
             Pk[m][b].resize(K);
-            for (int k = 0; k < K; ++k) {
+            for (int k = kb0(b); k < kb1(b); ++k) {
                 double cv = conv(mk[k]);
                 Mat Pkb = mk[k].P(r * bl[b] * cv);
                 Mat QP = matmul(mk[k].Q, Pkb);
@@ -1337,7 +1342,7 @@ inline MixResult mixture_eval(const Tree& tr, const Alignment& a, const MixSpec&
         const Mat& Ab = A[size_t(m) * n + b];
         double r = sp.rates[m];
         if (test(b)) {
-            for (int k = 0; k < K; ++k) {
+            for (int k = kb0(b); k < kb1(b); ++k) {
                 double tau = r * bl[b] * conv(mk[k]);
                 // d/dc_k : <A, P_k>
                 double s = 0; for (size_t e = 0; e < Ab.a.size(); ++e) s += Ab.a[e] * Pk[m][b][k].a[e];

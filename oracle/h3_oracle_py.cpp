@@ -169,7 +169,8 @@ PYBIND11_MODULE(h3oracle, m) {
        py::arg("is_test") = std::vector<bool>{}, py::arg("omega_bg") = -1.0);
     m.def("mixture_eval", [](const Tree& t, const Alignment& a, const std::vector<py::dict>& classes, const std::vector<double>& class_w,
                              py::object bg, std::vector<bool> is_test, std::vector<double> rates, std::vector<double> rate_w,
-                             std::vector<double> bl, bool normalized_time, bool want_global, bool zero_l_sentinel, bool tiled) {
+                             std::vector<double> bl, bool normalized_time, bool want_global, bool zero_l_sentinel, bool tiled,
+                             std::vector<int> branch_classes) {
         MixSpec sp;
         for (auto& c : classes) sp.classes.push_back(params_from(c));
         sp.class_w = class_w;
@@ -178,6 +179,10 @@ PYBIND11_MODULE(h3oracle, m) {
         if (!rates.empty()) { sp.rates = rates; sp.rate_w = rate_w; }
         sp.normalized_time = normalized_time; sp.want_global = want_global; sp.zero_l_sentinel = zero_l_sentinel;
         sp.tiled = tiled;
+        if (!branch_classes.empty()) {
+            if (int(branch_classes.size()) != t.n() + 1) throw std::runtime_error("branch_classes needs n_nodes + 1 offsets");
+            sp.branch_classes = branch_classes;
+        }
         if (bl.empty()) bl = t.bl;
         MixResult r;
         { py::gil_scoped_release rel; r = mixture_eval(t, a, sp, bl); }
@@ -185,7 +190,7 @@ PYBIND11_MODULE(h3oracle, m) {
     }, py::arg("tree"), py::arg("aln"), py::arg("classes"), py::arg("class_w"), py::arg("bg") = py::none(),
        py::arg("is_test") = std::vector<bool>{}, py::arg("rates") = std::vector<double>{}, py::arg("rate_w") = std::vector<double>{},
        py::arg("branch_lengths") = std::vector<double>{}, py::arg("normalized_time") = false, py::arg("want_global") = false,
-       py::arg("zero_l_sentinel") = false, py::arg("tiled") = false);
+       py::arg("zero_l_sentinel") = false, py::arg("tiled") = false, py::arg("branch_classes") = std::vector<int>{});
     m.def("nucleotide_patterns", &nucleotide_patterns, py::arg("aln"));
     m.def("gtr_matrix", [](const std::vector<double>& theta, const std::vector<double>& freq, double t) {
         if (theta.size() != 5 || freq.size() != 4) throw std::runtime_error("theta needs 5 entries, freq 4");
