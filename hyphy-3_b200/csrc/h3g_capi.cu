@@ -660,6 +660,8 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         return fail(ctx, H3G_ERR_ARG, "model arrays missing");
     if (d->time_mode == H3G_TIME_NORMALIZED && !d->mu && !dev_eig) return fail(ctx, H3G_ERR_ARG, "normalized time needs mu");
     if (d->n_dirs < 0 || (d->n_dirs > 0 && !d->dQ)) return fail(ctx, H3G_ERR_ARG, "dQ directions missing");
+    const int n_model_dirs = d->dQ_model ? d->n_models : 0;     // one extra direction per model
+    const int n_dirs_all = d->n_dirs + n_model_dirs;
     if (d->precision != H3G_PREC_FP64 && d->precision != H3G_PREC_MIXED) return fail(ctx, H3G_ERR_ARG, "unknown precision");
     if (d->precision == H3G_PREC_MIXED && !mixed_available()) return fail(ctx, H3G_ERR_CUDA, "mixed-precision path not built");
     const int S = d->S, nm = d->n_models;
@@ -674,7 +676,8 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         cudaSetDevice(ctx->device);
         // identical model already installed: nothing to upload
         uint64_t h = 1469598103934665603ull;
-        const int scal[9] = {S, nm, d->K, d->has_bg, d->M, d->time_mode, d->n_dirs, d->precision, d->zero_l_sentinel};
+        const int scal[10] = {S, nm, d->K, d->has_bg, d->M, d->time_mode, d->n_dirs, d->precision, d->zero_l_sentinel,
+                              n_model_dirs};
         h = hash_bytes(h, scal, sizeof(scal));
         h = hash_bytes(h, d->pi, S * sizeof(double));
         h = hash_bytes(h, d->Q, size_t(nm) * S * S * sizeof(double));
@@ -691,11 +694,12 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         h = hash_bytes(h, d->rate_w, d->M * sizeof(double));
         if (d->is_test) h = hash_bytes(h, d->is_test, size_t(pr->n));
         if (d->branch_classes) h = hash_bytes(h, d->branch_classes, size_t(pr->n + 1) * sizeof(int32_t));
+        if (d->dQ_model) h = hash_bytes(h, d->dQ_model, size_t(nm) * S * S * sizeof(double));
         if (d->n_dirs > 0) h = hash_bytes(h, d->dQ, size_t(d->n_dirs) * nm * S * S * sizeof(double));
         if (pr->has_model && h == pr->model_hash) return H3G_OK;
         cudaStreamSynchronize(ctx->stream);
         pr->has_model = false;
-        pr->S = S; pr->M = d->M; pr->K = d->K; pr->nmod = nm; pr->ndirs = d->n_dirs; pr->has_bg = d->has_bg;
+        pr->S = S; pr->M = d->M; pr->K = d->K; pr->nmod = nm; pr->ndirs = n_dirs_all; pr->has_bg = d->has_bg;
         pr->time_mode = d->time_mode; pr->sentinel = d->zero_l_sentinel;
         if (pr->precision != d->precision) { pr->drop_graphs(); pr->work_mem.release(); pr->w = Work{}; }
         pr->precision = d->precision;
@@ -727,13 +731,17 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             }
         }
         pr->h_mu = mu;
-        std::vector<double> dQ(size_t(std::max(d->n_dirs, 1)) * nm * SP2, 0.0);
+        // dense directions [n_dirs][nm], then the per-model ones [nm]
+        std::vector<double> dQ((size_t(std::max(d->n_dirs, 1)) * nm + size_t(n_model_dirs)) * SP2, 0.0);
         for (int x = 0; x < d->n_dirs; ++x)
             for (int k = 0; k < nm; ++k) pad_matrix(d->dQ + (size_t(x) * nm + k) * S * S, S, &dQ[(size_t(x) * nm + k) * SP2]);
+        for (int k = 0; k < n_model_dirs; ++k)
+            pad_matrix(d->dQ_model + size_t(k) * S * S, S, &dQ[(size_t(d->n_dirs) * nm + k) * SP2]);
         std::vector<uint8_t> it(pr->n, 1);
         if (d->is_test) std::copy(d->is_test, d->is_test + pr->n, it.begin());
         // grow-only, like the workspace
-        size_t mkey[5] = {size_t(nm), size_t(d->K), size_t(d->M), size_t(std::max(d->n_dirs, 1)), size_t(pr->n)};
+        size_t mkey[5] = {size_t(nm), size_t(d->K), size_t(d->M), size_t(std::max(d->n_dirs, 1) + (n_model_dirs ? 1 : 0)),
+                          size_t(pr->n)};
         bool fits = pr->m_pi != nullptr;
         for (int i = 0; i < 5 && fits; ++i) fits = mkey[i] <= pr->model_key[i];
         if (!fits && pr->m_pi)
@@ -788,7 +796,8 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
             H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->m_br, d->branch_classes, size_t(pr->n + 1) * sizeof(int32_t),
                                               cudaMemcpyHostToDevice, s));
         Model md{};
-        md.M = d->M; md.K = d->K; md.has_bg = d->has_bg; md.nmod = nm; md.time_mode = d->time_mode; md.ndirs = d->n_dirs;
+        md.M = d->M; md.K = d->K; md.has_bg = d->has_bg; md.nmod = nm; md.time_mode = d->time_mode; md.ndirs = n_dirs_all;
+        md.ndirs_dense = d->n_dirs;
         md.sentinel = d->zero_l_sentinel;
         md.pi = pr->m_pi; md.Q = pr->m_Q; md.lam = pr->m_lam; md.U = pr->m_U; md.V = pr->m_V; md.mu = pr->m_mu;
         md.UT = pr->m_UT; md.QT = pr->m_QT;
@@ -797,7 +806,7 @@ extern "C" h3g_status h3g_model_set(h3g_problem* pr, const h3g_model_desc* d) {
         md.dQ = pr->m_dQ;
         if (std::memcmp(&md, &pr->md, sizeof(Model)) != 0) pr->drop_graphs();
         pr->md = md;
-        h3g_status st = ensure_workspace(pr, d->M, d->K, nm, d->n_dirs);
+        h3g_status st = ensure_workspace(pr, d->M, d->K, nm, n_dirs_all);
         if (st != H3G_OK) return st;
         H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
         pr->model_hash = h;

@@ -79,6 +79,8 @@ struct Topo {
 
 struct Model {
     int M, K, has_bg, nmod, time_mode, ndirs, sentinel;
+    int ndirs_dense;         // the first ndirs_dense directions act on every model; direction ndirs_dense + k acts
+                             // on model k alone (one matrix each, stored after the dense ones)
     const double* pi;        // [64]
     const double* Q;         // [nmod][64*64]
     const double* QT;        // [nmod][64*64] transpose of Q
@@ -93,7 +95,7 @@ struct Model {
     const double* rate_w;    // [M]
     const uint8_t* is_test;  // [n] or null
     const int* br_off;       // [n + 1] or null: branch b mixes classes [br_off[b], br_off[b + 1]) with class_w
-    const double* dQ;        // [ndirs][nmod][64*64]
+    const double* dQ;        // [ndirs_dense][nmod][64*64], then [nmod][64*64] for the per-model directions
 };
 
 struct Work {

@@ -704,7 +704,14 @@ __global__ void __launch_bounds__(256) k_dir(Topo t, Model md, Work w) {
     double* sVr = sY + 16 * SP;      // V_k rows of the block
     __shared__ double red[8];
     const int x = blockIdx.x, k = blockIdx.y, rb = blockIdx.z, tid = threadIdx.x;
-    const double* dQ = md.dQ + (size_t(x) * md.nmod + k) * SP2;
+    const bool own = x >= md.ndirs_dense;                 // a per-model direction: model x - ndirs_dense only
+    if (own && k != x - md.ndirs_dense) {
+        double* Gz = w.G + (size_t(x) * md.nmod + k) * SP2 + size_t(16 * rb) * SP;
+        for (int e = tid; e < 16 * SP; e += 256) Gz[e] = 0.0;
+        if (rb == 0 && tid == 0) w.dirpart[(size_t(x) * md.nmod + k) * 17 + 16] = 0.0;
+        return;
+    }
+    const double* dQ = own ? md.dQ + (size_t(md.ndirs_dense) * md.nmod + k) * SP2 : md.dQ + (size_t(x) * md.nmod + k) * SP2;
     stage_matrix(sX, dQ, tid, 256);
     for (int e = tid; e < 16 * SP; e += 256) sVr[e] = md.V[size_t(k) * SP2 + size_t(16 * rb) * SP + e];
     __syncthreads();

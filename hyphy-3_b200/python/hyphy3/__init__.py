@@ -3,8 +3,8 @@
 Re-exports the core types, the likelihood entry points and the analysis drivers of the
 reference package (python/hyphy3/__init__.py) that run on the device from the _hyphy3 module:
 FELAnalyzer, MEMEAnalyzer, BUSTEDAnalyzer (fits, two-set model, auto K), RELAXAnalyzer,
-MG94Fitter, GTRFitter and the GTR likelihood.  aBSREL, FUBAR and the other drivers are not
-part of this package.
+MG94Fitter, GTRFitter and the GTR likelihood; ABSRELAnalyzer (hyphy3.absrel) and joint fits over
+batches of genes (hyphy3.batch).  FUBAR and the other drivers are not part of this package.
 """
 import os
 import sys
@@ -52,10 +52,14 @@ from _hyphy3 import (  # noqa: E402
     get_precision,
     library_version,
     mg94_eigensystem,
+    set_eigensolver,
+    get_eigensolver,
     set_precision,
 )
 
 from . import autograd  # noqa: E402
+from .absrel import ABSRELAnalyzer  # noqa: E402
+from .batch import fit_branch_lengths  # noqa: E402
 
 __version__ = "3.0.0"
 __all__ = [
@@ -65,5 +69,5 @@ __all__ = [
     "mg94_eigensystem", "set_precision", "autograd", "MEMEAnalyzer", "MEMESiteResult", "BUSTEDAnalyzer", "BUSTEDFit",
     "BUSTEDRateDistribution", "BUSTEDResult", "BUSTEDSettings", "GTRFitResult", "GTRFitter", "GTRMatrix", "GTRParameters",
     "RELAXAnalyzer", "RELAXModelFit", "RELAXRateDistribution", "RELAXResult", "RELAXSettings", "compute_gtr_gradients",
-    "compute_gtr_log_likelihood",
+    "compute_gtr_log_likelihood", "ABSRELAnalyzer", "fit_branch_lengths", "set_eigensolver", "get_eigensolver",
 ]

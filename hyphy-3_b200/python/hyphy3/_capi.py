@@ -46,7 +46,7 @@ class ModelDesc(C.Structure):
         ("mu", _dp), ("K", C.c_int), ("class_w", _dp), ("has_bg", C.c_int), ("is_test", C.POINTER(C.c_uint8)),
         ("M", C.c_int), ("rates", _dp), ("rate_w", _dp), ("time_mode", C.c_int), ("n_dirs", C.c_int),
         ("dQ", _dp), ("precision", C.c_int), ("zero_l_sentinel", C.c_int), ("bg_w", _dp),
-        ("branch_classes", C.POINTER(C.c_int32)),
+        ("branch_classes", C.POINTER(C.c_int32)), ("dQ_model", _dp),
     ]
 
 
@@ -259,7 +259,7 @@ class Problem:
 
     def set_model(self, *, pi, Q, lam=None, U=None, V=None, mu=None, class_w=(1.0,), has_bg=False, is_test=None, rates=(1.0,),
                   rate_w=(1.0,), time_mode=TIME_RAW, dQ=None, precision=PREC_FP64, zero_l_sentinel=False,
-                  bg_w=None, branch_classes=None) -> None:
+                  bg_w=None, branch_classes=None, dQ_model=None) -> None:
         """Q, U, V: [n_models, S, S]; lam: [n_models, S]; dQ: [n_dirs, n_models, S, S].  bg_w: weights of
         len(bg_w) background classes (models K ..), or None with has_bg for one background model.
         lam, U and V all None: the device diagonalises each Q (and mu defaults to -sum pi_i Q_ii)."""
@@ -280,6 +280,7 @@ class Problem:
         nd = 0 if dq is None else int(dq.shape[0])
         bw = None if bg_w is None else _f64(bg_w)
         bc = None if branch_classes is None else np.ascontiguousarray(branch_classes, dtype=np.int32)
+        dqm = None if dQ_model is None else _f64(dQ_model)          # [n_models, S, S], one direction per model
         self._bc = bc                                    # kept alive while the model is installed
         if bw is not None:
             nbg = int(bw.size)
@@ -289,9 +290,9 @@ class Problem:
                       K=len(cw), class_w=_ptr(cw), has_bg=nbg, is_test=_ptr(it, C.c_uint8), M=len(rt),
                       rates=_ptr(rt), rate_w=_ptr(rw), time_mode=time_mode, n_dirs=nd, dQ=_ptr(dq),
                       precision=precision, zero_l_sentinel=int(bool(zero_l_sentinel)), bg_w=_ptr(bw),
-                      branch_classes=_ptr(bc, C.c_int32))
+                      branch_classes=_ptr(bc, C.c_int32), dQ_model=_ptr(dqm))
         self.ctx.check(self.ctx.lib.h3g_model_set(self.h, C.byref(d)))
-        self.K, self.M, self.ndirs, self.nmod, self.S = len(cw), len(rt), nd, nm, S
+        self.K, self.M, self.ndirs, self.nmod, self.S = len(cw), len(rt), nd + (nm if dqm is not None else 0), nm, S
 
     def eval(self, bl, want=WANT_LNL | WANT_GRAD_T, out=None) -> dict:
         bl = _f64(bl)

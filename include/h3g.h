@@ -105,6 +105,10 @@ typedef struct {
                                  absrel.hpp:262-310); needs has_bg = 0 and is_test = NULL; the root's
                                  range is ignored.  grad_class_w then holds every class's weight
                                  partial. */
+    const double* dQ_model;   /* NULL, or n_models * S * S: one more direction per model k, dQ_model[k]
+                                 acting on model k alone (e.g. d/d omega of each branch class); their
+                                 gradients follow the n_dirs dense ones in grad_dir (n_dirs + n_models
+                                 entries) */
 } h3g_model_desc;
 
 typedef struct {

@@ -303,6 +303,18 @@ public:
         if (!std::isfinite(best.f)) throw std::runtime_error("RELAX: every start has a zero likelihood");
         auto fin_run = hyphy::opt::box_lbfgs(fg, best.x, lb, ub, settings.tolerance, settings.max_iterations);
         if (std::isfinite(fin_run.f) && fin_run.f <= best.f) best = std::move(fin_run);
+        // The model sets omega_T,0 = 0 once omega_R,0 <= 1e-12 (relax.hpp:589-597): the likelihood jumps at
+        // omega_R,0 -> 0 and a line search can stall just short of it.  Polish once from the optimum with
+        // omega_R,0 = 0 exactly and once with fresh curvature memory; keep the best.
+        for (int variant = 0; variant < 2; ++variant) {
+            std::vector<Scalar> x1 = best.x;
+            if (variant == 0) {
+                if (x1[i_om] <= lb[i_om]) continue;
+                x1[i_om] = lb[i_om];
+            }
+            auto r = hyphy::opt::box_lbfgs(fg, x1, lb, ub, settings.tolerance, settings.max_iterations);
+            if (std::isfinite(r.f) && r.f < best.f) best = std::move(r);
+        }
 
         const Point pt = decode(best.x);
         const Eval e = evaluate(pt, false);

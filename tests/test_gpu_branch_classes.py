@@ -51,6 +51,14 @@ def test_branch_classes_against_oracle(oracle, precision_name):
     assert rel(out["grad_class_w"], ref["grad_class_w"]) < tg
     assert rel(out["grad_dir"][:K], ref["grad_beta"]) < tg
     assert rel(out["grad_dir"][K:K + 2], [ref["grad_theta"][0], ref["grad_theta"][3]]) < tg
+    # the same omega gradients from one per-model direction each (dQ_model) instead of K dense ones
+    dense = np.copy(out["grad_dir"])
+    pr.set_model(pi=a.pi, Q=Q, lam=lam, U=U, V=V, mu=mu, class_w=w, dQ=np.stack(dirs[K:]), precision=prec,
+                 branch_classes=bc, dQ_model=np.stack([dq_beta(a, m) for m in models]))
+    out2 = pr.eval(bl, _capi.WANT_LNL | _capi.WANT_GRAD_T | _capi.WANT_GRAD_GLOBAL)
+    assert out2["lnl"] == out["lnl"]
+    assert np.array_equal(out2["grad_dir"][2:2 + K], dense[:K])
+    assert np.array_equal(out2["grad_dir"][:2], dense[K:K + 2])
     # malformed ranges are rejected
     bad = bc.copy()
     bad[2] = bad[1]
