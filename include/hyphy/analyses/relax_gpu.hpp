@@ -291,18 +291,27 @@ public:
         const Scalar sw[3][3] = {{0.6, 0.3, 0.1}, {0.5, 0.4, 0.1}, {0.7, 0.25, 0.05}};
         for (int j = 0; j < 3; ++j)
             starts.push_back(encode(len0, 1.0, {so[j][0], so[j][1], so[j][2]}, {sw[j][0], sw[j][1], sw[j][2]}, 1.0));
-        if (warm && warm->branch_lengths.size() == n)
+        if (warm && warm->branch_lengths.size() == n) {
             starts.push_back(encode(warm->branch_lengths, warm->tree_scale, warm->reference_distribution.omegas,
                                     warm->reference_distribution.weights, has_k ? warm->k : 1.0));
-        hyphy::opt::BoxLBFGSResult best;
-        best.f = std::numeric_limits<Scalar>::infinity();
+            if (has_k)   // the warm start with the relaxation moved both ways
+                for (Scalar kk : {0.5, 2.0})
+                    starts.push_back(encode(warm->branch_lengths, warm->tree_scale, warm->reference_distribution.omegas,
+                                            warm->reference_distribution.weights, kk));
+        }
+        // screen every start for 40 iterations, then run the two best to convergence
+        std::vector<hyphy::opt::BoxLBFGSResult> screened;
         for (const auto& x0 : starts) {
             auto r = hyphy::opt::box_lbfgs(fg, x0, lb, ub, settings.tolerance, 40);
-            if (std::isfinite(r.f) && r.f < best.f) best = std::move(r);
+            if (std::isfinite(r.f)) screened.push_back(std::move(r));
         }
-        if (!std::isfinite(best.f)) throw std::runtime_error("RELAX: every start has a zero likelihood");
-        auto fin_run = hyphy::opt::box_lbfgs(fg, best.x, lb, ub, settings.tolerance, settings.max_iterations);
-        if (std::isfinite(fin_run.f) && fin_run.f <= best.f) best = std::move(fin_run);
+        if (screened.empty()) throw std::runtime_error("RELAX: every start has a zero likelihood");
+        std::stable_sort(screened.begin(), screened.end(), [](const auto& a, const auto& b) { return a.f < b.f; });
+        hyphy::opt::BoxLBFGSResult best = screened.front();
+        for (size_t i = 0; i < std::min<size_t>(2, screened.size()); ++i) {
+            auto fin_run = hyphy::opt::box_lbfgs(fg, screened[i].x, lb, ub, settings.tolerance, settings.max_iterations);
+            if (std::isfinite(fin_run.f) && fin_run.f < best.f) best = std::move(fin_run);
+        }
         // The model sets omega_T,0 = 0 once omega_R,0 <= 1e-12 (relax.hpp:589-597): the likelihood jumps at
         // omega_R,0 -> 0 and a line search can stall just short of it.  Polish once from the optimum with
         // omega_R,0 = 0 exactly and once with fresh curvature memory; keep the best.
