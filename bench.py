@@ -464,6 +464,9 @@ def run_ours(args) -> None:
                      U=np.stack([e["U"] for e in es]), V=np.stack([e["V"] for e in es]),
                      mu=np.array([e["mu"] for e in es]), class_w=wl.omega_w, rates=list(wl.rates),
                      rate_w=list(wl.rate_w), dQ=dirs, precision=prec)
+        if args.memory_budget:
+            # subtree checkpointing: the workspace is held under the budget, partials recomputed per block
+            pr.set_memory_budget(int(args.memory_budget * 1e9))
         pr.stage_branch_lengths(bl)
 
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -505,7 +508,8 @@ def run_ours(args) -> None:
         res = pr.read_result(want)
         stages = pr.profile_stages(want, reps=3)
         results[prec_name] = {"secs": float(t.item()), "lnl": res["lnl"], "grad_t": res["grad_t"].copy(),
-                              "grad_dir": res["grad_dir"].copy(), "clocks": clocks, "stages": stages, "tuning": tuning}
+                              "grad_dir": res["grad_dir"].copy(), "clocks": clocks, "stages": stages, "tuning": tuning,
+                              "checkpoint": pr.checkpoint_info()}
     head = results[precision]
     ms_per_step = head["secs"] / args.steps * 1e3
     value = units * world * args.steps / head["secs"]
@@ -514,6 +518,8 @@ def run_ours(args) -> None:
 
     # end to end through the public API, host buffers in and out
     h.set_precision(precision)
+    if args.memory_budget:
+        h.set_memory_budget(int(args.memory_budget * 1e9))
     bl_list = list(bl)
     api_args = (tree, aln, base, bl_list, wl.omegas, wl.omega_w, list(wl.rates), list(wl.rate_w))
     for _ in range(max(args.warmup, 3)):
@@ -570,7 +576,9 @@ def run_ours(args) -> None:
             "dtype": "f64" if precision == "fp64" else "bf16x3/f32", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.config], "sites": wl.n_sites, "branches": n - 1, "patterns": aln.num_patterns,
                        "precision": precision, "l2": "flushed (256 MiB write) before every timed step",
-                       "parallelism": f"replicas{world}" if world > 1 else "single", "tuning": head["tuning"]},
+                       "parallelism": f"replicas{world}" if world > 1 else "single", "tuning": head["tuning"],
+                       "workspace_gb": head["checkpoint"]["workspace_bytes"] / 1e9,
+                       **({"checkpoint": head["checkpoint"]} if head["checkpoint"]["active"] else {})},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "_hyphy3.compute_mixture_gradients", "timing": "host wall clock around synchronous calls"},
             "gpu_launches": launches_per_eval * args.steps,
@@ -1192,6 +1200,8 @@ def main() -> None:
     ap.add_argument("--profile", action="store_true", help="device evaluations only (for ncu)")
     ap.add_argument("--sites", type=int, default=None, help="shrink the alignment to this many codons (--profile; --config 2)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic launch shapes)")
+    ap.add_argument("--memory-budget", type=float, default=0.0,
+                    help="GB one evaluation workspace may take (subtree checkpointing below the full size)")
     ap.add_argument("--mode", choices=["sharded", "replicas"], default="sharded",
                     help="N > 1 GPUs: split one alignment's patterns over the ranks (NCCL all-reduce per step), or "
                          "run an independent replica per rank (no collective)")

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/h3g.h"
+#include "h3g_checkpoint.h"
 #include "h3g_common.cuh"
 #include "h3g_fel.h"
 #include "h3g_kernels.h"
@@ -57,6 +58,7 @@ struct h3g_problem {
     int n = 0, root = -1, T = 0, P = 0, Pp = 0, NI = 0, max_state = -1;
     std::vector<int> ch_off, ch, iidx, taxon, in_off, out_off, in_nodes, out_nodes, parent_h;
     std::vector<uint8_t> leaf;
+    std::vector<int> bfs_order, depth_h, height_h;   // BFS order from the root, node depths and heights
     std::vector<int8_t> states_pm;     // [P][T] as uploaded (per-pattern checks on the host)
     DevArena topo_mem, model_mem, work_mem;
     int *d_ch_off = nullptr, *d_ch = nullptr, *d_iidx = nullptr, *d_taxon = nullptr, *d_in_nodes = nullptr, *d_out_nodes = nullptr;
@@ -123,8 +125,21 @@ struct h3g_problem {
         if (ev_join) cudaEventDestroy(ev_join);
         if (s2) cudaStreamDestroy(s2);
     }
+    // subtree checkpointing (h3g_checkpoint.h): budget and forced target asked for, the plan of the
+    // installed workspace and its device lists
+    uint64_t mem_budget = 0;
+    int ck_target_req = 0;
+    bool ck = false;
+    h3g::CkPlan ck_plan;
+    DevArena ck_mem;
+    int *d_ck_iidx = nullptr, *d_ck_vidx = nullptr, *d_ck_lists = nullptr;
+    int2* d_ck_kdesc = nullptr;
+    int4* d_ck_info = nullptr;
+    struct CkOffsets { int in, out, acc, in_info, out_info, in_next, in_heads, n_in_heads, out_next, out_heads, n_out_heads; };
+    std::vector<CkOffsets> ck_off;
+    uint64_t ws_bytes = 0, full_bytes = 0;
     Topo topo() const {
-        Topo t;
+        Topo t{};
         t.n = n; t.root = root; t.NI = NI; t.T = T; t.P = P; t.Pp = Pp; t.S = S;
         t.ch_off = d_ch_off; t.ch = d_ch; t.parent = d_parent; t.iidx = d_iidx; t.leaf = d_leaf; t.taxon = d_taxon;
         t.states = d_states; t.masks = d_masks; t.w = d_w;
@@ -132,6 +147,16 @@ struct h3g_problem {
         t.in_next = d_chains; t.in_heads = d_chains + off_in_heads;
         t.out_next = d_chains + off_out_next; t.out_heads = d_chains + off_out_heads;
         t.all_mask = S >= 64 ? ~uint64_t(0) : ((uint64_t(1) << S) - 1);
+        t.vidx = nullptr;
+        t.ncp = 0;
+        return t;
+    }
+    // the topology an evaluation of this problem's own workspace runs on: checkpoint slots when planned
+    Topo topo_eval() const {
+        Topo t = topo();
+        if (ck && !batch) {
+            t.iidx = d_ck_iidx; t.vidx = d_ck_vidx; t.kdesc = d_ck_kdesc; t.ncp = ck_plan.ncp;
+        }
         return t;
     }
 };
@@ -248,6 +273,9 @@ extern "C" h3g_status h3g_problem_create(h3g_ctx* ctx, int n_nodes, const int32_
             pr->ch_off[i + 1] = pr->ch_off[i] + int(kids[i].size());
             for (int c : kids[i]) pr->ch.push_back(c);
         }
+        pr->bfs_order = order;
+        pr->depth_h = depth;
+        pr->height_h = height;
         int H = 0, Dp = 0;
         for (int i = 0; i < n; ++i) if (!is_leaf[i]) { H = std::max(H, height[i]); Dp = std::max(Dp, depth[i]); }
         pr->in_off.assign(1, 0);
@@ -498,14 +526,19 @@ struct WsLayout {
     }
 };
 
-static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod, int ndirs, const h3g_tuning& tu) {
+// part_nodes / vf_nodes: partial slots of internal nodes and gradient-operand slots (NI and n, or
+// fewer under a checkpoint plan).
+static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod, int ndirs, const h3g_tuning& tu,
+                          size_t part_nodes = 0, size_t vf_nodes = 0) {
     (void)K;
+    if (!part_nodes) part_nodes = NI;
+    if (!vf_nodes) vf_nodes = n;
     WsLayout L;
     L.n = n;
     L.mats = size_t(M) * n * SP2;
     L.rsz = size_t(M) * n * SP;
     L.pcols = size_t(M) * Pp;
-    L.ecols = NI * M * Pp;
+    L.ecols = part_nodes * M * Pp;
     L.gt = size_t(M) * n;
     // enough A chunks for ~600 CTAs, never below 256 patterns per chunk
     const int want_chunks = std::max<int>(1, int((600 + n * M - 1) / (n * M)));
@@ -526,9 +559,22 @@ static WsLayout ws_layout(size_t n, size_t NI, size_t Pp, int M, int K, int nmod
     L.dirpart = size_t(std::max(ndirs, 1)) * nmod * 17;
     L.gdir = size_t(std::max(ndirs, 1)) * nmod * SP2;
     L.out = 2 + n + 2 * size_t(nmod) + M;
-    L.part = NI * M * SP * Pp;
-    L.vf = n * M * SP * Pp;
+    L.part = part_nodes * M * SP * Pp;
+    L.vf = vf_nodes * M * SP * Pp;
     return L;
+}
+
+// Device bytes ws_alloc takes for layout L.
+static uint64_t ws_bytes(const WsLayout& L, int precision) {
+    const uint64_t f64 = 3 * L.mats + L.rsz + 4 * L.pcols + L.gt + L.apart + L.afull + L.hpart + 2 * L.gsz + L.hsz +
+                         L.dirpart + L.gdir + L.out;
+    uint64_t b = f64 * 8 + 2 * uint64_t(L.ecols) * 4 + 4;
+    if (precision == H3G_PREC_FP64)
+        b += (3 * uint64_t(L.part) + L.vf) * 8;
+    else   // FP32 partials, three exponent planes, FP32 P^T and row sums, six BF16 split planes, two flag planes
+        b += (3 * uint64_t(L.part) + L.vf) * 4 + 3 * uint64_t(L.ecols) * 4 + L.mats * 4 + L.rsz * 4 + 6 * uint64_t(L.mats) * 2 +
+             2 * uint64_t(L.ecols / TP) * 4 + 16;
+    return b;
 }
 
 // Allocate a workspace of layout L (FP64 or mixed partials) into A; w.bl is left to the caller.
@@ -595,6 +641,161 @@ static h3g_status ensure_host_buffer(h3g_problem* pr, int M, int nmod, int ndirs
     return H3G_OK;
 }
 
+static std::vector<std::vector<int>> children_of(const h3g_problem* pr) {
+    std::vector<std::vector<int>> kids(pr->n);
+    for (int u = 0; u < pr->n; ++u) kids[u].assign(pr->ch.begin() + pr->ch_off[u], pr->ch.begin() + pr->ch_off[u + 1]);
+    return kids;
+}
+
+// Upload a checkpoint plan's slots and per-block lists: node lists of the FP64 level launches, and
+// the item descriptors and chains of the mixed path's persistent passes restricted to each block
+// (a chain never enters a block root, so a block's recompute list is its full list without the
+// root, which comes last).
+static h3g_status upload_checkpoints(h3g_problem* pr) {
+    h3g_ctx* ctx = pr->ctx;
+    const h3g::CkPlan& pl = pr->ck_plan;
+    const int n = pr->n;
+    const auto kids = children_of(pr);
+    std::vector<int> n_int(n, 0);
+    for (int u = 0; u < n; ++u)
+        for (int c : kids[u]) n_int[u] += pr->leaf[c] ? 0 : 1;
+    std::vector<int2> kdesc(std::max<size_t>(pr->ch.size(), 1));
+    for (size_t j = 0; j < pr->ch.size(); ++j) {
+        const int c = pr->ch[j];
+        kdesc[j] = make_int2(c, pr->leaf[c] ? pr->taxon[c] : -(2 + pl.iidx[c]));
+    }
+    std::vector<int> lists;
+    std::vector<int4> info;
+    std::vector<int> pos(n, -1);
+    pr->ck_off.clear();
+    for (const h3g::CkBlock& B : pl.blocks) {
+        h3g_problem::CkOffsets o{};
+        o.in = int(lists.size());
+        lists.insert(lists.end(), B.in_nodes.begin(), B.in_nodes.end());
+        o.out = int(lists.size());
+        lists.insert(lists.end(), B.out_kids.begin(), B.out_kids.end());
+        o.acc = int(lists.size());
+        lists.insert(lists.end(), B.acc.begin(), B.acc.end());
+        // inside items
+        o.in_info = int(info.size());
+        for (size_t k = 0; k < B.in_nodes.size(); ++k) {
+            const int u = B.in_nodes[k];
+            pos[u] = int(k);
+            info.push_back(make_int4(u, pl.iidx[u], pr->ch_off[u], pr->ch_off[u + 1]));
+        }
+        std::vector<int> nxt(B.in_nodes.size(), -1), heads;
+        std::vector<char> fused(B.in_nodes.size(), 0);
+        for (size_t k = 0; k < B.in_nodes.size(); ++k) {
+            const int u = B.in_nodes[k], par = pr->parent_h[u];
+            if (u != B.root && par != B.root && n_int[par] == 1) {
+                nxt[k] = pos[par];
+                fused[size_t(pos[par])] = 1;
+            }
+        }
+        for (size_t k = 0; k < B.in_nodes.size(); ++k)
+            if (!fused[k]) heads.push_back(int(k));
+        o.in_next = int(lists.size());
+        lists.insert(lists.end(), nxt.begin(), nxt.end());
+        o.in_heads = int(lists.size());
+        o.n_in_heads = int(heads.size());
+        lists.insert(lists.end(), heads.begin(), heads.end());
+        for (int u : B.in_nodes) pos[u] = -1;
+        // outside items
+        o.out_info = int(info.size());
+        for (size_t k = 0; k < B.out_kids.size(); ++k) {
+            const int c = B.out_kids[k], u = pr->parent_h[c];
+            pos[c] = int(k);
+            info.push_back(make_int4(c, u, pl.iidx[u], pr->leaf[c] ? -1 : pl.iidx[c]));
+            info.push_back(make_int4(pr->ch_off[u], pr->ch_off[u + 1], 0, 0));
+        }
+        std::vector<int> onxt(B.out_kids.size(), -1), oheads;
+        std::vector<char> ofused(B.out_kids.size(), 0);
+        for (size_t k = 0; k < B.out_kids.size(); ++k) {
+            const int c = B.out_kids[k];
+            if (pr->leaf[c] || pl.is_ckpt[c]) continue;
+            int best = -1;
+            for (int d : kids[c])
+                if (!pr->leaf[d] && (best < 0 || pr->height_h[d] > pr->height_h[best])) best = d;
+            if (best >= 0) {
+                onxt[k] = pos[best];
+                ofused[size_t(pos[best])] = 1;
+            }
+        }
+        for (size_t k = 0; k < B.out_kids.size(); ++k)
+            if (!ofused[k]) oheads.push_back(int(k));
+        o.out_next = int(lists.size());
+        lists.insert(lists.end(), onxt.begin(), onxt.end());
+        o.out_heads = int(lists.size());
+        o.n_out_heads = int(oheads.size());
+        lists.insert(lists.end(), oheads.begin(), oheads.end());
+        for (int c : B.out_kids) pos[c] = -1;
+        pr->ck_off.push_back(o);
+    }
+    if (lists.empty()) lists.push_back(-1);
+    if (info.empty()) info.push_back(make_int4(0, 0, 0, 0));
+    auto& A = pr->ck_mem;
+    A.release();
+    cudaStream_t s = ctx->stream;
+    H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ck_iidx, size_t(n)));
+    H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ck_vidx, size_t(n)));
+    H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ck_kdesc, kdesc.size()));
+    H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ck_lists, lists.size()));
+    H3G_TRY_CUDA(ctx, A.alloc(&pr->d_ck_info, info.size()));
+    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ck_iidx, pl.iidx.data(), size_t(n) * sizeof(int), cudaMemcpyHostToDevice, s));
+    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ck_vidx, pl.vidx.data(), size_t(n) * sizeof(int), cudaMemcpyHostToDevice, s));
+    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ck_kdesc, kdesc.data(), kdesc.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ck_lists, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    H3G_TRY_CUDA(ctx, cudaMemcpyAsync(pr->d_ck_info, info.data(), info.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    return H3G_OK;
+}
+
+// The workspace layout of (M, K, nmod, ndirs) and whether it is checkpointed: the full layout when it fits
+// the budget (the problem's, else the device's free memory plus the `held` bytes about to be released) and
+// no block size is forced; else the plan with the largest block size whose layout fits.
+static h3g_status choose_layout(h3g_problem* pr, int M, int K, int nmod, int ndirs, const h3g_tuning& tu, uint64_t held,
+                                WsLayout& L) {
+    const WsLayout full = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), M, K, nmod, ndirs, tu);
+    pr->full_bytes = ws_bytes(full, pr->precision);
+    uint64_t budget = pr->mem_budget;
+    if (!budget) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+        budget = uint64_t(double(fr + held) * 0.92);
+    }
+    pr->ck = false;
+    if (pr->ck_target_req <= 0 && (pr->full_bytes <= budget || (pr->mem_budget == 0 && budget == 0))) {
+        L = full;
+        return H3G_OK;
+    }
+    const auto kids = children_of(pr);
+    auto make = [&](int target) {
+        return h3g::plan_checkpoints(pr->n, pr->root, kids, pr->leaf.data(), pr->bfs_order, pr->depth_h, pr->height_h, target);
+    };
+    auto layout_of = [&](const h3g::CkPlan& p) {
+        return ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), M, K, nmod, ndirs, tu, size_t(p.ncp + p.scratch_int),
+                         size_t(p.ncp + p.scratch_all));
+    };
+    if (pr->ck_target_req > 0) {
+        pr->ck_plan = make(pr->ck_target_req);
+        L = layout_of(pr->ck_plan);
+        pr->ck = true;
+        return H3G_OK;
+    }
+    for (int target = pr->n;; target = std::max(2, target * 4 / 5)) {
+        h3g::CkPlan p = make(target);
+        const WsLayout Lc = layout_of(p);
+        if (ws_bytes(Lc, pr->precision) <= budget) {
+            pr->ck_plan = std::move(p);
+            L = Lc;
+            pr->ck = true;
+            return H3G_OK;
+        }
+        if (target == 2) break;
+    }
+    return fail(pr->ctx, H3G_ERR_OOM, "the evaluation workspace does not fit the memory budget even with subtree checkpoints");
+}
+
 // Allocate the evaluation workspace for (M, K, nmod, ndirs); reuses it when unchanged.
 static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int ndirs) {
     h3g_ctx* ctx = pr->ctx;
@@ -616,13 +817,21 @@ static h3g_status ensure_workspace(h3g_problem* pr, int M, int K, int nmod, int 
     M = int(key[0]); K = int(key[1]); nmod = int(key[2]); ndirs = int(key[3]);
     cudaStreamSynchronize(ctx->stream);
     pr->drop_graphs();
+    const uint64_t held = pr->w.P ? pr->ws_bytes : 0;
     pr->work_mem.release();
+    pr->w = Work{};
+    pr->mw = MixedWork{};
+    pr->ws_bytes = 0;
+    WsLayout L;
+    h3g_status st = choose_layout(pr, M, K, nmod, ndirs, tu, held, L);
+    if (st == H3G_OK && pr->ck) st = upload_checkpoints(pr);
+    if (st != H3G_OK) { pr->ck = false; return st; }
     std::copy(key, key + 4, pr->work_key);
-    const WsLayout L = ws_layout(size_t(pr->n), size_t(pr->NI), size_t(pr->Pp), M, K, nmod, ndirs, tu);
     pr->applied = tu;
-    h3g_status st = ws_alloc(ctx, L, pr->precision, pr->work_mem, pr->w, pr->mw);
+    st = ws_alloc(ctx, L, pr->precision, pr->work_mem, pr->w, pr->mw);
     pr->w.bl = pr->d_bl;
-    if (st != H3G_OK) { pr->work_mem.release(); pr->w = Work{}; pr->mw = MixedWork{}; }
+    if (st != H3G_OK) { pr->work_mem.release(); pr->w = Work{}; pr->mw = MixedWork{}; pr->ck = false; return st; }
+    pr->ws_bytes = ws_bytes(L, pr->precision);
     return st;
 }
 
@@ -829,8 +1038,12 @@ struct StageMarks {
 
 // Enqueue the pruning pipeline (inside, root and optionally outside + gradients) on stream s (the
 // context stream, or a batch slot's), in workspace w / mw.
+static int enqueue_eval_ck(h3g_problem* pr, unsigned want, bool from_given_P, cudaStream_t s, const Work& w,
+                           const MixedWork& mwk, StageMarks* mk);
+
 static int enqueue_eval_on(h3g_problem* pr, unsigned want, bool from_given_P, cudaStream_t s, const Work& w,
                            const MixedWork& mwk, StageMarks* mk = nullptr) {
+    if (pr->ck && !pr->batch) return enqueue_eval_ck(pr, want, from_given_P, s, w, mwk, mk);
     const Topo t = pr->topo();
     const Model& md = pr->md;
     const bool mixed = pr->precision == H3G_PREC_MIXED;
@@ -877,7 +1090,90 @@ static int enqueue_eval_on(h3g_problem* pr, unsigned want, bool from_given_P, cu
             }
         }
         mark(ST_OUTSIDE, l);
-        mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, mwk, s) : launch_accumA_fp64(t, md, w, s));
+        mark(ST_ACCUM_A, mixed ? launch_accumA_mixed(t, md, w, mwk, nullptr, 0, s) : launch_accumA_fp64(t, md, w, nullptr, 0, s));
+        mark(ST_FRECHET, launch_frechet(t, md, w, global ? 1 : 0, s));
+        if (side) cudaStreamWaitEvent(s, pr->ev_join, 0);
+        if (global) mark(ST_HSUM, launch_global(t, md, w, s));
+    }
+    if (side && !grads) cudaStreamWaitEvent(s, pr->ev_join, 0);
+    mark(ST_SMALL, launch_small(t, md, w, grads ? 1 : 0, s));
+    return L;
+}
+
+// The same pipeline over a checkpoint plan (h3g_checkpoint.h): inside block by block in post-order,
+// then per block in reverse post-order the recompute of its inside partials below its root, its
+// outside walk and its gradient-operand accumulation.  Stage marks: the recompute and the
+// accumulation of the blocks count under "outside".
+static int enqueue_eval_ck(h3g_problem* pr, unsigned want, bool from_given_P, cudaStream_t s, const Work& w,
+                           const MixedWork& mwk, StageMarks* mk) {
+    const Topo t = pr->topo_eval();
+    const Model& md = pr->md;
+    const h3g::CkPlan& pl = pr->ck_plan;
+    const bool mixed = pr->precision == H3G_PREC_MIXED;
+    const bool grads = (want & (H3G_WANT_GRAD_T | H3G_WANT_GRAD_GLOBAL)) != 0;
+    const bool global = (want & H3G_WANT_GRAD_GLOBAL) != 0;
+    const int* lists = pr->d_ck_lists;
+    const int4* info = pr->d_ck_info;
+    int L = 0;
+    auto mark = [&](Stage st, int launched) {
+        L += launched;
+        if (mk && launched) { cudaEventRecord(mk->ev[st + 1], s); mk->seen[st] = true; mk->launches[st] += launched; }
+    };
+    if (mk) cudaEventRecord(mk->ev[0], s);
+    const bool side = global && md.ndirs > 0;
+    if (side) {
+        cudaEventRecord(pr->ev_fork, s);
+        cudaStreamWaitEvent(pr->s2, pr->ev_fork, 0);
+        L += launch_dir(t, md, w, pr->s2);
+        cudaEventRecord(pr->ev_join, pr->s2);
+    }
+    mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
+    if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, mwk, s));
+    // inside partials of block bi: every level, or every level below the block root
+    auto inside = [&](size_t bi, bool with_root) {
+        const h3g::CkBlock& B = pl.blocks[bi];
+        const h3g_problem::CkOffsets& o = pr->ck_off[bi];
+        const int levels = int(B.in_lv.size()) - 1 - (with_root ? 0 : 1);
+        int l = 0;
+        if (levels <= 0) return 0;
+        if (mixed) {
+            Topo tb = t;
+            tb.in_info = info + o.in_info;
+            tb.in_next = lists + o.in_next;
+            tb.in_heads = lists + o.in_heads;
+            l += mixed_new_epoch(mwk, s);
+            l += launch_inside_mixed(tb, md, w, mwk, o.n_in_heads - (with_root ? 0 : 1), pr->wait, s);
+        } else {
+            for (int lv = 0; lv < levels; ++lv)
+                l += launch_inside_fp64(t, md, w, lists + o.in + B.in_lv[lv], B.in_lv[lv + 1] - B.in_lv[lv], s);
+        }
+        return l;
+    };
+    int l = 0;
+    for (size_t bi = 0; bi < pl.blocks.size(); ++bi) l += inside(bi, true);
+    mark(ST_INSIDE, l);
+    mark(ST_ROOT, mixed ? launch_root_mixed(t, md, w, mwk, s) : launch_root(t, md, w, s));
+    if (grads) {
+        l = 0;
+        for (size_t r = pl.blocks.size(); r-- > 0;) {
+            const h3g::CkBlock& B = pl.blocks[r];
+            const h3g_problem::CkOffsets& o = pr->ck_off[r];
+            if (r + 1 != pl.blocks.size()) l += inside(r, false);      // the root's block is still in scratch
+            if (mixed) {
+                Topo tb = t;
+                tb.out_info = info + o.out_info;
+                tb.out_next = lists + o.out_next;
+                tb.out_heads = lists + o.out_heads;
+                l += mixed_new_epoch(mwk, s);
+                l += launch_outside_mixed(tb, md, w, mwk, o.n_out_heads, pr->wait, s);
+                if (!B.acc.empty()) l += launch_accumA_mixed(t, md, w, mwk, lists + o.acc, int(B.acc.size()), s);
+            } else {
+                for (size_t lv = 0; lv + 1 < B.out_lv.size(); ++lv)
+                    l += launch_outside_fp64(t, md, w, lists + o.out + B.out_lv[lv], B.out_lv[lv + 1] - B.out_lv[lv], 1, s);
+                if (!B.acc.empty()) l += launch_accumA_fp64(t, md, w, lists + o.acc, int(B.acc.size()), s);
+            }
+        }
+        mark(ST_OUTSIDE, l);
         mark(ST_FRECHET, launch_frechet(t, md, w, global ? 1 : 0, s));
         if (side) cudaStreamWaitEvent(s, pr->ev_join, 0);
         if (global) mark(ST_HSUM, launch_global(t, md, w, s));
@@ -1162,6 +1458,92 @@ extern "C" h3g_status h3g_problem_set_wait_limit(h3g_problem* pr, uint32_t polls
     pr->wait.skew = unmatched ? 1 : 0;
     pr->drop_graphs();               // the limit is a launch parameter of the captured passes
     return H3G_OK;
+}
+
+extern "C" h3g_status h3g_problem_set_memory_budget(h3g_problem* pr, uint64_t bytes, int target) {
+    if (!pr) return H3G_ERR_ARG;
+    if (target < 0) return fail(pr->ctx, H3G_ERR_ARG, "target must be >= 0");
+    if (pr->batch) return fail(pr->ctx, H3G_ERR_STATE, "the problem belongs to a batch (its workspace lives there)");
+    cudaSetDevice(pr->ctx->device);
+    cudaStreamSynchronize(pr->ctx->stream);
+    pr->mem_budget = bytes;
+    pr->ck_target_req = target;
+    pr->drop_graphs();
+    pr->work_mem.release();
+    pr->w = Work{};
+    pr->mw = MixedWork{};
+    pr->ws_bytes = 0;
+    pr->ck = false;
+    if (pr->has_model) return ensure_workspace(pr, pr->M, pr->K, pr->nmod, pr->ndirs);
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_problem_checkpoint_info(const h3g_problem* pr, h3g_checkpoint_info* info) {
+    if (!pr || !info) return H3G_ERR_ARG;
+    *info = h3g_checkpoint_info{};
+    info->active = pr->ck ? 1 : 0;
+    info->workspace_bytes = pr->ws_bytes;
+    info->full_bytes = pr->full_bytes;
+    if (pr->ck) {
+        const h3g::CkPlan& pl = pr->ck_plan;
+        info->n_blocks = int32_t(pl.blocks.size());
+        info->target = pl.target;
+        info->n_persistent = pl.ncp;
+        info->scratch_internal = pl.scratch_int;
+        info->scratch_nodes = pl.scratch_all;
+    }
+    return H3G_OK;
+}
+
+extern "C" h3g_status h3g_checkpoint_plan(int n, const int32_t* parent, const uint8_t* is_leaf, int target,
+                                          int32_t* is_checkpoint, int32_t* block, int32_t* slot_internal,
+                                          int32_t* slot_vf, int32_t* counts) {
+    if (n < 2 || !parent || !is_leaf || target < 1) return H3G_ERR_ARG;
+    try {
+        std::vector<std::vector<int>> kids(n);
+        int root = -1;
+        for (int i = 0; i < n; ++i) {
+            const int p = parent[i];
+            if (p < 0) {
+                if (root >= 0) return H3G_ERR_ARG;
+                root = i;
+            } else {
+                if (p >= n || p == i || is_leaf[p]) return H3G_ERR_ARG;
+                kids[p].push_back(i);
+            }
+        }
+        if (root < 0 || is_leaf[root]) return H3G_ERR_ARG;
+        std::vector<int> order(1, root), depth(n, -1), height(n, 0);
+        depth[root] = 0;
+        for (size_t q = 0; q < order.size(); ++q)
+            for (int c : kids[order[q]]) {
+                if (depth[c] >= 0) return H3G_ERR_ARG;
+                depth[c] = depth[order[q]] + 1;
+                order.push_back(c);
+            }
+        if (int(order.size()) != n) return H3G_ERR_ARG;
+        for (int q = n - 1; q >= 0; --q) {
+            const int u = order[q];
+            for (int c : kids[u]) height[u] = std::max(height[u], height[c] + 1);
+            if (!is_leaf[u] && kids[u].empty()) height[u] = 1;
+        }
+        const h3g::CkPlan pl = h3g::plan_checkpoints(n, root, kids, is_leaf, order, depth, height, target);
+        for (int i = 0; i < n; ++i) {
+            if (is_checkpoint) is_checkpoint[i] = pl.is_ckpt[i];
+            if (block) block[i] = pl.block_of[i];
+            if (slot_internal) slot_internal[i] = pl.iidx[i];
+            if (slot_vf) slot_vf[i] = pl.vidx[i];
+        }
+        if (counts) {
+            counts[0] = int32_t(pl.blocks.size());
+            counts[1] = pl.ncp;
+            counts[2] = pl.scratch_int;
+            counts[3] = pl.scratch_all;
+        }
+        return H3G_OK;
+    } catch (const std::bad_alloc&) {
+        return H3G_ERR_OOM;
+    }
 }
 
 extern "C" h3g_status h3g_stage_branch_lengths(h3g_problem* pr, const double* bl) {

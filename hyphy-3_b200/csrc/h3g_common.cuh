@@ -75,7 +75,14 @@ struct Topo {
     const int* in_heads;     // [chains] inside position of each chain's first node, inside order
     const int* out_next;     // [outside position] position of this node's deepest internal child, else -1
     const int* out_heads;    // [chains] outside position of each chain's first node, outside order
+    // subtree checkpointing: Vf slot of each node (NULL: the node id).  With checkpoints, iidx and vidx
+    // map checkpoint nodes to persistent slots [0, ncp) and every other node to a scratch slot that
+    // the nodes of other blocks reuse
+    const int* vidx;
+    int ncp;
 };
+
+__device__ __forceinline__ int vslot(const Topo& t, int b) { return t.vidx ? t.vidx[b] : b; }
 
 struct Model {
     int M, K, has_bg, nmod, time_mode, ndirs, sentinel;

@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const
     }
     if (want_v) {
         const double fp = w.f[size_t(m) * Pp + p];
-        double* dst = w.Vf + part_off(c, m, M, t.Pp) + size_t(8 * g) * Pp + p;
+        double* dst = w.Vf + part_off(vslot(t, c), m, M, t.Pp) + size_t(8 * g) * Pp + p;
 #pragma unroll
         for (int q = 0; q < 8; ++q) dst[q * Pp] = fp * v[q];
     }
@@ -464,7 +464,8 @@ __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const
 // X = Vf (64 states x patterns), Y = D, K = the pattern axis.  8 warps as mm64 (warp w: rows
 // 16(w/2) .. +16, columns 32(w%2) .. +32, 2 x 4 tiles of 8x8), 32 patterns per stage, stages
 // double-buffered by 16-byte cp.async (a leaf's 0/1 vectors are written from its states and
-// masks instead).  grid (n, M, nchunk), block 256.
+// masks instead).  grid (branches, M, nchunk), block 256; `branches` lists the branches (NULL: every
+// node id, the root skipped).
 constexpr int kAccP = 32;                                      // patterns per stage
 constexpr int kAL = kAccP + 4;                                 // row stride of a staged tile (doubles)
 constexpr size_t kAccStage = size_t(2) * SP * kAL;             // V and D tiles of one stage
@@ -475,10 +476,10 @@ __device__ __forceinline__ void cp_async16_f64(double* dst, const double* src) {
                  ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(src) : "memory");
 }
 
-__global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w) {
+__global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w, const int* __restrict__ branches) {
     pdl_enter();
     extern __shared__ __align__(16) double smA[];
-    const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
+    const int b = branches ? branches[blockIdx.x] : int(blockIdx.x), m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
     const int M = md.M;
     const size_t Pp = size_t(t.Pp);
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w) {
     const int nst = (p_end - p_begin) / kAccP;
     const bool lf = t.leaf[b];
     const int tx = lf ? t.taxon[b] : -1;
-    const double* Vb = w.Vf + part_off(b, m, M, t.Pp);
+    const double* Vb = w.Vf + part_off(vslot(t, b), m, M, t.Pp);
     const double* Db = lf ? nullptr : w.D + part_off(t.iidx[b], m, M, t.Pp);
 
     // stage `st` of the chunk into buffer st & 1: 64 state rows x 32 patterns of Vf (and D)
@@ -821,8 +822,10 @@ int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int
     launch_k(k_outside, dim3(t.Pp / kTileP, count, md.M), 256, kPruneSmem, s, t, md, w, d_kids, want_v);
     return 1;
 }
-int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    launch_k(k_accumA, dim3(t.n, md.M, w.nchunk), 256, kAccSmemF, s, t, md, w);
+int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, const int* d_branches, int count, cudaStream_t s) {
+    const int* none = nullptr;
+    launch_k(k_accumA, dim3(d_branches ? count : t.n, md.M, w.nchunk), 256, kAccSmemF, s, t, md, w,
+             d_branches ? d_branches : none);
     return 1;
 }
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s) {

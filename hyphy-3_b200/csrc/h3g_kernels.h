@@ -11,7 +11,8 @@ int launch_prep_given_P(const Topo& t, const Work& w, cudaStream_t s);
 int launch_inside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, cudaStream_t s);
 int launch_root(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
 int launch_outside_fp64(const Topo& t, const Model& md, const Work& w, const int* d_nodes, int count, int want_v, cudaStream_t s);
-int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
+// d_branches NULL: every branch (grid over all node ids)
+int launch_accumA_fp64(const Topo& t, const Model& md, const Work& w, const int* d_branches, int count, cudaStream_t s);
 int launch_frechet(const Topo& t, const Model& md, const Work& w, int want_global, cudaStream_t s);
 int launch_global(const Topo& t, const Model& md, const Work& w, cudaStream_t s);
 int launch_dir(const Topo& t, const Model& md, const Work& w, cudaStream_t s);

@@ -387,7 +387,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 if (threadIdx.x == 0)
                     for (int k = k0; k < k1; ++k) {
                         const int code = t.kdesc[k].y;
-                        if (code <= -2) wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err, wc);
+                        // a checkpoint slot (below t.ncp) was written by an earlier launch: no wait
+                        if (code <= -2 && -(code + 2) >= t.ncp)
+                            wait_item(mw.flag_in + (size_t(-(code + 2)) * M + m) * ntile + tile, epoch, w.err, wc);
                     }
                 __syncthreads();
                 // the first two children's messages load together (padding states are zero in every
@@ -523,7 +525,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
             const bool internal = ic >= 0;
             if (internal) tc_load_b(s, mw.Bpt, mat_off_f(m, c, t.n));
             if (!carried) {
-                if (threadIdx.x == 0 && u != t.root) wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err, wc);
+                if (threadIdx.x == 0 && u != t.root && iu >= t.ncp)
+                    wait_item(mw.flag_out + (size_t(iu) * M + m) * ntile + tile, epoch, w.err, wc);
                 __syncthreads();
                 if (u == t.root) {
 #pragma unroll
@@ -549,7 +552,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
             const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
             const int EDc = internal ? mw.ED[col_off(ic, m, M, t.Pp) + p] : 0;
             const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
-            float* vf = mw.Vf + part_off(c, m, M, t.Pp) + so;
+            float* vf = mw.Vf + part_off(vslot(t, c), m, M, t.Pp) + so;
 #pragma unroll
             for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
             if (!internal) break;                          // a leaf: no outside vector below it
@@ -662,10 +665,11 @@ __device__ __forceinline__ void ld_row8(const unsigned char* raw, int row, int k
     x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
 }
 
-__global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw) {
+__global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, Work w, MixedWork mw,
+                                                              const int* __restrict__ branches) {
     pdl_enter();
     extern __shared__ __align__(1024) unsigned char smraw[];
-    const int b = blockIdx.x, m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
+    const int b = branches ? branches[blockIdx.x] : int(blockIdx.x), m = blockIdx.y, ck = blockIdx.z, tid = threadIdx.x;
     if (b == t.root) return;
     const int M = md.M, warp = tid >> 5, lane = tid & 31;
     const size_t Pp = size_t(t.Pp);
@@ -673,7 +677,7 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
     const int ntile = (p_end - p_begin) / kAT;
     const bool lf = t.leaf[b];
     const int tx = lf ? t.taxon[b] : -1;
-    const float* Vb = mw.Vf + part_off(b, m, M, t.Pp);
+    const float* Vb = mw.Vf + part_off(vslot(t, b), m, M, t.Pp);
     const float* Db = lf ? nullptr : mw.D + part_off(t.iidx[b], m, M, t.Pp);
     unsigned char* ring = smraw + 2 * kStage;
     uint64_t* mma_bar = reinterpret_cast<uint64_t*>(ring + kRing * kRawSlot);   // [2]
@@ -886,8 +890,27 @@ int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const Mi
     launch_k(k_outside_mx, persistent_ctas(items, wc.ctas_per_sm), kThreads, kMxSmem, s, t, md, w, mw, items, wc);
     return 1;
 }
-int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
-    launch_k(k_accumA_mx, dim3(t.n, md.M, w.nchunk), kAccThreads, kAccSmem, s, t, md, w, mw);
+int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_branches,
+                        int count, cudaStream_t s) {
+    const int* none = nullptr;
+    launch_k(k_accumA_mx, dim3(d_branches ? count : t.n, md.M, w.nchunk), kAccThreads, kAccSmem, s, t, md, w, mw,
+             d_branches ? d_branches : none);
+    return 1;
+}
+
+// A new epoch and fresh item counters between two persistent launches of one evaluation (the blocks of
+// a checkpoint plan reuse scratch slots, whose flags then hold an older epoch).
+__global__ void k_new_epoch_mx(MixedWork mw) {
+    pdl_enter();
+    if (threadIdx.x == 0) {
+        mw.sync[0] += 1;
+        mw.sync[1] = 0;
+        mw.sync[2] = 0;
+    }
+}
+
+int mixed_new_epoch(const MixedWork& mw, cudaStream_t s) {
+    launch_k(k_new_epoch_mx, 1, 32, 0, s, mw);
     return 1;
 }
 

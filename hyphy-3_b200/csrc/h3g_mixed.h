@@ -57,6 +57,10 @@ int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const Mix
 int launch_root_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 int launch_outside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
                          cudaStream_t s);
-int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
+// d_branches NULL: every branch (grid over all node ids)
+int launch_accumA_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, const int* d_branches,
+                        int count, cudaStream_t s);
+// new epoch and item counters for the next persistent launch of the same evaluation
+int mixed_new_epoch(const MixedWork& mw, cudaStream_t s);
 
 }  // namespace h3g

@@ -334,6 +334,9 @@ PYBIND11_MODULE(_hyphy3, m) {
         else throw std::invalid_argument("eigensolver must be 'device' or 'host'");
     }, py::arg("where"));
     m.def("get_eigensolver", []() { return LikelihoodEngine::device_eigensolver() ? "device" : "host"; });
+    m.def("set_memory_budget", [](uint64_t bytes) { LikelihoodEngine::set_memory_budget(bytes); }, py::arg("bytes"),
+          "Device bytes one evaluation workspace may take (0 = none); above it partials are checkpointed per subtree");
+    m.def("get_memory_budget", []() { return LikelihoodEngine::memory_budget(); });
     m.def("library_version", []() { return std::string(h3g_version()); });
 
     // MG94 global fits (optimizer.hpp:741-1135)

@@ -54,6 +54,8 @@ from _hyphy3 import (  # noqa: E402
     mg94_eigensystem,
     set_eigensolver,
     get_eigensolver,
+    set_memory_budget,
+    get_memory_budget,
     set_precision,
 )
 
@@ -70,4 +72,5 @@ __all__ = [
     "BUSTEDRateDistribution", "BUSTEDResult", "BUSTEDSettings", "GTRFitResult", "GTRFitter", "GTRMatrix", "GTRParameters",
     "RELAXAnalyzer", "RELAXModelFit", "RELAXRateDistribution", "RELAXResult", "RELAXSettings", "compute_gtr_gradients",
     "compute_gtr_log_likelihood", "ABSRELAnalyzer", "fit_branch_lengths", "set_eigensolver", "get_eigensolver",
+    "set_memory_budget", "get_memory_budget",
 ]

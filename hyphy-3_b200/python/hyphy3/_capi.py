@@ -29,7 +29,8 @@ EXPORTED = [
     "h3g_fel_run_tested", "h3g_meme_run_tested", "h3g_alignment_compress", "h3g_alignment_compress_device",
     "h3g_nuc_eval_from_P", "h3g_problem_set_wait_limit", "h3g_batch_create", "h3g_batch_destroy", "h3g_batch_eval",
     "h3g_batch_last_stats", "h3g_pack_result_device", "h3g_ctx_stream", "h3g_problem_set_tuning",
-    "h3g_problem_get_tuning", "h3g_autotune", "h3g_model_get_eigensystem",
+    "h3g_problem_get_tuning", "h3g_autotune", "h3g_model_get_eigensystem", "h3g_problem_set_memory_budget",
+    "h3g_problem_checkpoint_info", "h3g_checkpoint_plan",
 ]
 STAGE_NAMES = "build_P,prep_mixed,inside,root,outside,accum_A,frechet,hsum,small,dir".split(",")
 
@@ -38,6 +39,12 @@ _dp = C.POINTER(C.c_double)
 
 class Tuning(C.Structure):
     _fields_ = [("a_chunk", C.c_int), ("ctas_per_sm", C.c_int), ("frechet_groups", C.c_int)]
+
+
+class CheckpointInfo(C.Structure):
+    _fields_ = [("active", C.c_int32), ("n_blocks", C.c_int32), ("target", C.c_int32), ("n_persistent", C.c_int32),
+                ("scratch_internal", C.c_int32), ("scratch_nodes", C.c_int32), ("workspace_bytes", C.c_uint64),
+                ("full_bytes", C.c_uint64)]
 
 
 class ModelDesc(C.Structure):
@@ -127,6 +134,10 @@ def load() -> C.CDLL:
         lib.h3g_problem_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         lib.h3g_autotune.argtypes = [vp, _dp, C.c_uint, C.c_int, C.POINTER(Tuning), _dp]
         lib.h3g_model_get_eigensystem.argtypes = [vp, C.c_int, _dp, _dp, _dp]
+        lib.h3g_problem_set_memory_budget.argtypes = [vp, C.c_uint64, C.c_int]
+        lib.h3g_problem_checkpoint_info.argtypes = [vp, C.POINTER(CheckpointInfo)]
+        _i32 = C.POINTER(C.c_int32)
+        lib.h3g_checkpoint_plan.argtypes = [C.c_int, _i32, C.POINTER(C.c_uint8), C.c_int, _i32, _i32, _i32, _i32, _i32]
         lib.h3g_fel_run_tested.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(C.c_uint8), C.POINTER(FelResult)]
         lib.h3g_meme_run.argtypes = [vp, C.POINTER(FelModel), _dp, C.POINTER(MemeResult), _dp]
         _i32p = C.POINTER(C.c_int32)
@@ -142,6 +153,26 @@ def load() -> C.CDLL:
         lib.h3g_last_error.restype = C.c_char_p
         _lib = lib
     return _lib
+
+
+def checkpoint_plan(parent, is_leaf, target: int) -> dict:
+    """The subtree-checkpoint plan of a tree (host only, no device): per node is_checkpoint, block,
+    slot_internal and slot_vf, and the counts {blocks, persistent, scratch_internal, scratch_nodes}."""
+    lib = load()
+    par = np.ascontiguousarray(parent, dtype=np.int32)
+    lf = np.ascontiguousarray(is_leaf, dtype=np.uint8)
+    n = len(par)
+    out = {k: np.zeros(n, dtype=np.int32) for k in ("is_checkpoint", "block", "slot_internal", "slot_vf")}
+    counts = np.zeros(4, dtype=np.int32)
+    i32 = C.POINTER(C.c_int32)
+    st = lib.h3g_checkpoint_plan(n, par.ctypes.data_as(i32), lf.ctypes.data_as(C.POINTER(C.c_uint8)), int(target),
+                                 *(out[k].ctypes.data_as(i32) for k in ("is_checkpoint", "block", "slot_internal", "slot_vf")),
+                                 counts.ctypes.data_as(i32))
+    if st != 0:
+        raise H3GError(f"h3g_checkpoint_plan failed with status {st}", st)
+    out.update(blocks=int(counts[0]), persistent=int(counts[1]), scratch_internal=int(counts[2]),
+               scratch_nodes=int(counts[3]))
+    return out
 
 
 def _f64(a) -> np.ndarray:
@@ -390,6 +421,17 @@ class Problem:
         """Polls before a persistent-pass flag wait gives up (0 = default); unmatched makes every such
         wait look for a value no item publishes (tests the H3G_ERR_TIMEOUT path)."""
         self.ctx.check(self.ctx.lib.h3g_problem_set_wait_limit(self.h, C.c_uint32(polls), C.c_int(int(unmatched))))
+
+    def set_memory_budget(self, nbytes: int = 0, target: int = 0) -> None:
+        """Device bytes the evaluation workspace may take (0 = no budget; a workspace larger than free
+        device memory still checkpoints by itself); target > 0 forces the checkpoint block size."""
+        self.ctx.check(self.ctx.lib.h3g_problem_set_memory_budget(self.h, C.c_uint64(int(nbytes)), C.c_int(int(target))))
+
+    def checkpoint_info(self) -> dict:
+        """The installed workspace's checkpoint plan: active, blocks, target, slots and bytes."""
+        ci = CheckpointInfo()
+        self.ctx.check(self.ctx.lib.h3g_problem_checkpoint_info(self.h, C.byref(ci)))
+        return {f: int(getattr(ci, f)) for f, _ in CheckpointInfo._fields_}
 
     def get_eigensystem(self, k: int = 0) -> dict:
         """The installed eigensystem of model k (given, or solved on the device): {"lam", "U", "V"}."""

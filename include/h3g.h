@@ -255,6 +255,40 @@ h3g_status h3g_pack_result_device(h3g_problem* prob, unsigned want, double* d_ve
  * no device waits). */
 h3g_status h3g_problem_set_wait_limit(h3g_problem* prob, uint32_t polls, int unmatched);
 
+/* ------------------------------------------------------ subtree checkpointing
+ * The reference keeps every node's inside, outside and message partials for all
+ * patterns in host memory (likelihood.hpp:314-340).  Here, when the evaluation
+ * workspace of a problem exceeds its memory budget, the tree is cut into blocks
+ * (subtrees rooted at checkpoint nodes, each at most about `target` nodes): the
+ * inside pass keeps only the checkpoint nodes' partials, and the outside pass
+ * recomputes each block's inside partials from its checkpointed children before
+ * walking it.  Results are bit-identical to the unbudgeted evaluation (same
+ * kernels, same summation order).  Budget 0 = none, but a workspace larger than
+ * the device's free memory checkpoints by itself.  target > 0 forces that block
+ * size (0 = the largest that fits the budget).  FP64 and mixed precision; not for
+ * batch members (their workspaces are the batch's slots). */
+typedef struct {
+    int32_t active;          /* 1 when the installed workspace is checkpointed */
+    int32_t n_blocks;        /* blocks (= checkpoint nodes, the root included) */
+    int32_t target;          /* block size target of the plan */
+    int32_t n_persistent;    /* partial slots kept through the evaluation */
+    int32_t scratch_internal;/* internal-node slots shared by the blocks */
+    int32_t scratch_nodes;   /* gradient-operand slots shared by the blocks */
+    uint64_t workspace_bytes;/* device bytes of the installed workspace */
+    uint64_t full_bytes;     /* device bytes the workspace takes without checkpoints */
+} h3g_checkpoint_info;
+h3g_status h3g_problem_set_memory_budget(h3g_problem* prob, uint64_t bytes, int target);
+h3g_status h3g_problem_checkpoint_info(const h3g_problem* prob, h3g_checkpoint_info* info);
+/* The plan alone, on the host (no device needed): for a tree of n_nodes
+ * (parent[i] = -1 at the root) and a block size target, fills the per-node arrays
+ * that are not NULL: is_checkpoint, block (index of the block that computes the
+ * node, blocks in post-order, the root's last), slot_internal (partial slot of an
+ * internal node, -1 for leaves) and slot_vf (gradient-operand slot), and
+ * counts[4] = {blocks, persistent slots, scratch internal slots, scratch node slots}. */
+h3g_status h3g_checkpoint_plan(int n_nodes, const int32_t* parent, const uint8_t* is_leaf, int target,
+                               int32_t* is_checkpoint, int32_t* block, int32_t* slot_internal, int32_t* slot_vf,
+                               int32_t* counts);
+
 /* Per-stage device time of one evaluation (mean over reps runs, events between
  * stages, no graph): stage_ms[H3G_N_STAGES], stage_launches[H3G_N_STAGES] (may
  * be NULL).  Stage order: H3G_STAGE_NAMES. */

@@ -189,9 +189,16 @@ public:
         }
         h3g_problem* pr = nullptr;
         check(h3g_problem_create(ctx(), n, parent.data(), leaf.data(), taxon.data(), T, P, st.data(), mk.data(), w.data(), &pr));
+        if (memory_budget()) check(h3g_problem_set_memory_budget(pr, memory_budget(), 0));
         problems_.push_front({h, n, P, pr, 0});
         if (problems_.size() > 4) { h3g_problem_destroy(problems_.back().prob); problems_.pop_back(); }
         return pr;
+    }
+    // device bytes each problem's evaluation workspace may take (0: none; subtree checkpointing
+    // then starts only when a workspace exceeds the device's free memory)
+    static uint64_t& memory_budget() { static uint64_t b = 0; return b; }
+    void apply_memory_budget() {
+        for (auto& e : problems_) check(h3g_problem_set_memory_budget(e.prob, memory_budget(), 0));
     }
     // true (default): models are installed as generators and diagonalised on the device
     // (h3g_model_desc with NULL eigensystems); false: by the host's Householder + QL solver
@@ -265,6 +272,13 @@ public:
     static void set_device_eigensolver(bool on) { gpu_detail::Engine::device_eigen() = on; }
     static bool device_eigensolver() { return gpu_detail::Engine::device_eigen(); }
     static h3g_precision get_precision() { return gpu_detail::Engine::precision(); }
+    // Device bytes one evaluation workspace may take; above it the tree's partials are checkpointed per
+    // subtree and recomputed in the outside pass (bit-identical results).  0 = no budget.
+    static void set_memory_budget(uint64_t bytes) {
+        gpu_detail::Engine::memory_budget() = bytes;
+        gpu_detail::Engine::get().apply_memory_budget();
+    }
+    static uint64_t memory_budget() { return gpu_detail::Engine::memory_budget(); }
 
     static std::vector<size_t> build_leaf_to_taxon_map(const Tree& tree, const Alignment& aln) {
         std::vector<size_t> m(tree.num_nodes(), size_t(-1));
