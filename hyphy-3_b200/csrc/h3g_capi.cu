@@ -1063,8 +1063,9 @@ static int enqueue_eval_on(h3g_problem* pr, unsigned want, bool from_given_P, cu
         L += launch_dir(t, md, w, pr->s2);
         cudaEventRecord(pr->ev_join, pr->s2);
     }
-    mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
-    if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, mwk, s));
+    mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s)
+                                  : (mixed ? launch_build_P_mixed(t, md, w, mwk, s) : launch_build_P(t, md, w, s)));
+    if (mixed && from_given_P) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, mwk, s));
     int l = 0;
     if (mixed) {
         // one persistent launch over every level, per-tile dependencies
@@ -1127,8 +1128,9 @@ static int enqueue_eval_ck(h3g_problem* pr, unsigned want, bool from_given_P, cu
         L += launch_dir(t, md, w, pr->s2);
         cudaEventRecord(pr->ev_join, pr->s2);
     }
-    mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s) : launch_build_P(t, md, w, s));
-    if (mixed) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, mwk, s));
+    mark(ST_BUILD_P, from_given_P ? launch_prep_given_P(t, w, s)
+                                  : (mixed ? launch_build_P_mixed(t, md, w, mwk, s) : launch_build_P(t, md, w, s)));
+    if (mixed && from_given_P) mark(ST_PREP_MIXED, mixed_prepare(t, md, w, mwk, s));
     // inside partials of block bi: every level, or every level below the block root
     auto inside = [&](size_t bi, bool with_root) {
         const h3g::CkBlock& B = pl.blocks[bi];

@@ -18,6 +18,8 @@
 #include <cstdlib>
 #include "h3g_common.cuh"
 #include "h3g_kernels.h"
+#include "h3g_mixed.h"
+#include "h3g_tc.cuh"
 
 namespace h3g {
 
@@ -122,13 +124,23 @@ __device__ __forceinline__ void mm64(const double* __restrict__ X, const double*
 // dP_{m,b} = sum_k c_k r_m conv_k Q_k clamp(P_k), model by model, as two FP64
 // tensor-core products per model (mm64).
 // dynamic smem: 2 x 64 x LDM doubles (U e then Q; V then clamp(P_k)).
-__global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
+// kMixed: the split-precision path's operands instead of the FP64 P and P^T, from P staged in
+// shared memory: the BF16 hi/mid/lo tiles of P and P^T in the tcgen05 K-major layout (16-byte
+// stores of 8 consecutive K), FP32 P^T and the row sums (FP64 and FP32); thread 0 of CTA (0, 0)
+// starts the evaluation's epoch of the persistent passes.
+template <bool kMixed>
+__global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w, MixedWork mw) {
     pdl_enter();
     extern __shared__ __align__(16) double sm[];
     double* sX = sm;                 // U_k diag(e), then Q_k
     double* sY = sm + SP * LDM;      // V_k, then clamp(P_k)
     __shared__ double se[SP];
     const int b = blockIdx.x, m = blockIdx.y, tid = threadIdx.x;
+    if (kMixed && b == 0 && m == 0 && tid == 0) {        // a new evaluation: new epoch, fresh item counters
+        mw.sync[0] += 1;
+        mw.sync[1] = 0;
+        mw.sync[2] = 0;
+    }
     if (b == t.root) return;
     const BranchModels bm = branch_models(md, b);
     Frag64 accP, accD;
@@ -181,16 +193,62 @@ __global__ void __launch_bounds__(256) k_build_P(Topo t, Model md, Work w) {
                 for (int e = 0; e < 2; ++e) accD.v[i][j][e] = fma(sc, qp.v[i][j][e], accD.v[i][j][e]);
     }
     const size_t o = mat_off(m, b, t.n);
+    if constexpr (!kMixed) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int r = frag_row(i), c = frag_col(j, 0);
-            *reinterpret_cast<double2*>(w.P + o + r * SP + c) = make_double2(accP.v[i][j][0], accP.v[i][j][1]);
-            *reinterpret_cast<double2*>(w.dP + o + r * SP + c) = make_double2(accD.v[i][j][0], accD.v[i][j][1]);
-            w.PT[o + c * SP + r] = accP.v[i][j][0];
-            w.PT[o + (c + 1) * SP + r] = accP.v[i][j][1];
+            for (int j = 0; j < 4; ++j) {
+                const int r = frag_row(i), c = frag_col(j, 0);
+                *reinterpret_cast<double2*>(w.P + o + r * SP + c) = make_double2(accP.v[i][j][0], accP.v[i][j][1]);
+                *reinterpret_cast<double2*>(w.dP + o + r * SP + c) = make_double2(accD.v[i][j][0], accD.v[i][j][1]);
+                w.PT[o + c * SP + r] = accP.v[i][j][0];
+                w.PT[o + (c + 1) * SP + r] = accP.v[i][j][1];
+            }
+    } else {
+        __syncthreads();                          // every warp is done reading sX (Q) and sY
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int r = frag_row(i), c = frag_col(j, 0);
+                *reinterpret_cast<double2*>(w.dP + o + r * SP + c) = make_double2(accD.v[i][j][0], accD.v[i][j][1]);
+                sX[r * LDM + c] = accP.v[i][j][0];
+                sX[r * LDM + c + 1] = accP.v[i][j][1];
+            }
+        __syncthreads();
+        // chunk c: row c / 8 of the tile, K = 8 (c % 8) .. +8
+        for (int c = tid; c < SP * (SP / 8); c += 256) {
+            const int r = c >> 3, k0 = (c & 7) * 8;
+            const uint32_t off = tc::kmajor_off16(SP, r, k0) / 2;
+            float x[8];
+            uint32_t hw[3][4];
+            // P tile: row r = output state i, K = input state j
+#pragma unroll
+            for (int e = 0; e < 8; ++e) x[e] = float(sX[r * LDM + k0 + e]);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) tc::split3x2(x[2 * e], x[2 * e + 1], hw[0][e], hw[1][e], hw[2][e]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                *reinterpret_cast<uint4*>(mw.Bp[q] + o + off) = make_uint4(hw[q][0], hw[q][1], hw[q][2], hw[q][3]);
+            // P^T tile: row r = input state j, K = output state i; FP32 P^T row r
+#pragma unroll
+            for (int e = 0; e < 8; ++e) x[e] = float(sX[(k0 + e) * LDM + r]);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) tc::split3x2(x[2 * e], x[2 * e + 1], hw[0][e], hw[1][e], hw[2][e]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                *reinterpret_cast<uint4*>(mw.Bpt[q] + o + off) = make_uint4(hw[q][0], hw[q][1], hw[q][2], hw[q][3]);
+            float4* pt = reinterpret_cast<float4*>(mw.PT32 + o + size_t(r) * SP + k0);
+            pt[0] = make_float4(x[0], x[1], x[2], x[3]);
+            pt[1] = make_float4(x[4], x[5], x[6], x[7]);
         }
+        if (tid < SP) {
+            double rs = 0.0;
+            for (int j = 0; j < SP; ++j) rs += sX[tid * LDM + j];
+            w.rs[(size_t(m) * t.n + b) * SP + tid] = rs;
+            mw.rs32[(size_t(m) * t.n + b) * SP + tid] = float(rs);
+        }
+    }
 }
 
 // Row sums of P_{m,b} (the message of a leaf with missing data).  grid (n, M), block 64.
@@ -278,14 +336,22 @@ __device__ __forceinline__ int renorm_cols(double (&v)[8], double* smax, int g, 
 // fall in 16 different banks.
 constexpr int kDL = kTileP + 4;
 
-// Stage a 64x64 matrix row-major with the padded stride LDM (k_build_P's operand layout).
-__device__ __forceinline__ void stage_matrix_pad(double* __restrict__ s, const double* __restrict__ g, int tid, int nthr) {
-    const double2* g2 = reinterpret_cast<const double2*>(g);
+__device__ __forceinline__ void cp_async16_f64(double* dst, const double* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                 ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(src) : "memory");
+}
+
+// Stage a 64x64 matrix row-major with the padded stride LDM (k_build_P's operand layout) by 16-byte
+// cp.async, one commit group: the copy runs while the CTA loads and multiplies its partials;
+// stage_wait() before the product reads it.
+__device__ __forceinline__ void stage_matrix_pad_async(double* __restrict__ s, const double* __restrict__ g, int tid, int nthr) {
     for (int e = tid; e < SP2 / 2; e += nthr) {
         const int r = e / (SP / 2), c2 = e % (SP / 2);
-        *reinterpret_cast<double2*>(s + r * LDM + 2 * c2) = __ldg(g2 + e);
+        cp_async16_f64(s + r * LDM + 2 * c2, g + 2 * e);
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // dst[i][p] = sum_k sM[i][k] sX[k][p] for the CTA's 64 x 32 tile on the FP64 tensor cores
 // (mma.sync m8n8k4): warp w owns output rows 8w .. 8w+7, all 32 columns as four 8x8 tiles,
@@ -323,7 +389,7 @@ __global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const 
     const int iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
     const bool root = (u == t.root);
-    if (!root) stage_matrix_pad(sP, w.P + mat_off(m, u, t.n), tid, 256);
+    if (!root) stage_matrix_pad_async(sP, w.P + mat_off(m, u, t.n), tid, 256);
     double v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = (8 * g + q) < t.S ? 1.0 : 0.0;
@@ -351,6 +417,7 @@ __global__ void __launch_bounds__(256) k_inside(Topo t, Model md, Work w, const 
     if (root) return;
 #pragma unroll
     for (int q = 0; q < 8; ++q) sD[(8 * g + q) * kDL + lane] = v[q];
+    stage_wait();
     __syncthreads();
     // message to the parent: (P_u D_u)_i = sum_j P[i][j] D_j
     tile_mm_store(sP, sD, w.Ms + part_off(iu, m, M, t.Pp) + size_t(blockIdx.x) * kTileP, Pp);
@@ -418,7 +485,7 @@ __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const
     const int u = t.parent[c], iu = t.iidx[u], M = md.M;
     const size_t Pp = size_t(t.Pp);
     const bool internal = !t.leaf[c];
-    if (internal) stage_matrix_pad(sPT, w.PT + mat_off(m, c, t.n), tid, 256);
+    if (internal) stage_matrix_pad_async(sPT, w.PT + mat_off(m, c, t.n), tid, 256);
     double v[8];
     if (u == t.root) {
 #pragma unroll
@@ -454,6 +521,7 @@ __global__ void __launch_bounds__(256) k_outside(Topo t, Model md, Work w, const
     if (!internal) return;
 #pragma unroll
     for (int q = 0; q < 8; ++q) sV[(8 * g + q) * kDL + lane] = v[q];
+    stage_wait();
     __syncthreads();
     // U_c = P_c^T V_c : (U_c)_i = sum_j PT[i][j] V_j
     tile_mm_store(sPT, sV, w.U + part_off(t.iidx[c], m, M, t.Pp) + size_t(blockIdx.x) * kTileP, Pp);
@@ -470,11 +538,6 @@ constexpr int kAccP = 32;                                      // patterns per s
 constexpr int kAL = kAccP + 4;                                 // row stride of a staged tile (doubles)
 constexpr size_t kAccStage = size_t(2) * SP * kAL;             // V and D tiles of one stage
 static const size_t kAccSmemF = 2 * kAccStage * sizeof(double);
-
-__device__ __forceinline__ void cp_async16_f64(double* dst, const double* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
-                 ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))), "l"(src) : "memory");
-}
 
 __global__ void __launch_bounds__(256) k_accumA(Topo t, Model md, Work w, const int* __restrict__ branches) {
     pdl_enter();
@@ -793,7 +856,8 @@ static const size_t kBuildSmem = size_t(2) * SP * LDM * sizeof(double);
 static const size_t kFrechetSmem = size_t(3) * SP * LDM * sizeof(double);
 
 void fp64_configure() {
-    cudaFuncSetAttribute(k_build_P, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
+    cudaFuncSetAttribute(k_build_P<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
+    cudaFuncSetAttribute(k_build_P<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBuildSmem));
     cudaFuncSetAttribute(k_inside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
     cudaFuncSetAttribute(k_outside, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPruneSmem));
     cudaFuncSetAttribute(k_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFrechetSmem));
@@ -802,9 +866,13 @@ void fp64_configure() {
 }
 
 int launch_build_P(const Topo& t, const Model& md, const Work& w, cudaStream_t s) {
-    launch_k(k_build_P, dim3(t.n, md.M), 256, kBuildSmem, s, t, md, w);
+    launch_k(k_build_P<false>, dim3(t.n, md.M), 256, kBuildSmem, s, t, md, w, MixedWork{});
     launch_k(k_rowsum, dim3(t.n, md.M), SP, 0, s, t, md, w);
     return 2;
+}
+int launch_build_P_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s) {
+    launch_k(k_build_P<true>, dim3(t.n, md.M), 256, kBuildSmem, s, t, md, w, mw);
+    return 1;
 }
 int launch_prep_given_P(const Topo& t, const Work& w, cudaStream_t s) {
     launch_k(k_prep_given_P, t.n, 256, 0, s, t, w);

@@ -50,7 +50,10 @@ struct MixedSizes {
     size_t part = 0, vf = 0, cols = 0, mats = 0, rs = 0, flags = 0;
 };
 h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z);
+// caller-supplied P: the split-precision operands from w.P / w.rs (new epoch included)
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
+// P, dP and the split-precision operands in one launch (h3g_fp64.cu); the FP64 P and P^T are not stored
+int launch_build_P_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 // count: chains of the pass (Topo::in_heads / out_heads)
 int launch_inside_mixed(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, int count, WaitCfg wc,
                         cudaStream_t s);
