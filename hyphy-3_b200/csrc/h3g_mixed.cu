@@ -213,8 +213,15 @@ __device__ __forceinline__ void tc_write_part(const TcTile& s, const float (&v)[
     }
 }
 
+// s = fl(a + b) and e = (a + b) - s exactly (Knuth's two-sum; no fast-math reassociation here)
+__device__ __forceinline__ float two_sum(float a, float b, float& e) {
+    const float s = a + b, bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+    return s;
+}
+
 // out = A * B^T for this thread's row and state group: issue (one thread),
-// wait (all), read the four per-K-step accumulators from TMEM and sum in FP64.
+// wait (all), read the four per-K-step accumulators from TMEM and add them with compensated FP32 sums.
 __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const Lane& l, int* err, uint32_t phase) {
     const int tid = threadIdx.x;
     tc::fence_async_smem();
@@ -256,10 +263,13 @@ __device__ __forceinline__ void tc_run(const TcTile& s, float (&o)[kSG], const L
         tc::tmem_wait_ld();
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            double acc = 0.0;
-#pragma unroll
-            for (int ks = 0; ks < kKSteps; ++ks) acc += double(t8[ks][i]);
-            o[8 * h + i] = float(acc);
+            // the four K-step sums added with their rounding errors carried (error-free two-sums in
+            // FP32): the FP64 sum's result without its conversions, which limited the pass's throughput
+            float e1, e2, e3;
+            const float s1 = two_sum(t8[0][i], t8[1][i], e1);
+            const float s2 = two_sum(t8[2][i], t8[3][i], e2);
+            const float sm = two_sum(s1, s2, e3);
+            o[8 * h + i] = sm + ((e1 + e2) + e3);
         }
     }
     tc::tc_fence_before();
@@ -554,7 +564,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
             const double scale = ldexp(w.f[size_t(m) * Pp + p], EL - EV - EDc);
             float* vf = mw.Vf + part_off(vslot(t, c), m, M, t.Pp) + so;
 #pragma unroll
-            for (int i = 0; i < kSG; ++i) vf[i * Pp] = float(double(v[i]) * scale);
+            for (int i = 0; i < kSG; ++i) vf[i * Pp] = v[i] * float(scale);
             if (!internal) break;                          // a leaf: no outside vector below it
             tc_write_part(s, v, l);
             tc_run(s, v, l, w.err, phase);                // v: U_c, the outside vector at c
