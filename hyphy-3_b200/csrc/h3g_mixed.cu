@@ -403,7 +403,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                     }
                 __syncthreads();
                 // the first two children's messages load together (padding states are zero in every
-                // message), then one product and one renormalisation; further children one at a time
+                // message), then one product and one renormalisation; further children one at a time.
+                // The product with the last child is not renormalised: the message product that follows
+                // is (power-of-two scaling is exact, so only values in the FP32 subnormal range, far
+                // below any realistic overlap of two normalised messages, could tell the difference)
                 const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k0], p, l.g, so);
                 E = s0.E;
                 if (k0 + 1 < k1) {
@@ -417,18 +420,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 } else {
                     msg_load(s0, v);
                 }
-                E += renorm_row(v, s.smax, l);
+                if (k0 + 2 < k1) E += renorm_row(v, s.smax, l);
                 for (int k = k0 + 2; k < k1; ++k) {
                     const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
                     float a[kSG];
                     msg_load(sr, a);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-                    E += sr.E + renorm_row(v, s.smax, l);
+                    E += sr.E;
+                    if (k + 1 < k1) E += renorm_row(v, s.smax, l);
                 }
             } else {
                 // a chain node: its only internal child is the previous node (message in v, exponent E);
-                // the other children are leaves
+                // the other children are leaves (the last product again left to the message's renormalisation)
+                const int k_last = t.kdesc[k1 - 1].x == carried ? k1 - 2 : k1 - 1;
                 for (int k = k0; k < k1; ++k) {
                     const int2 d = t.kdesc[k];
                     if (d.x == carried) continue;
@@ -437,7 +442,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                     msg_load(sr, a);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-                    E += sr.E + renorm_row(v, s.smax, l);
+                    E += sr.E;
+                    if (k != k_last) E += renorm_row(v, s.smax, l);
                 }
             }
             store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
@@ -547,7 +553,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                     EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
                 }
             }
-            // times every sibling's message, renormalised after each
+            // times every sibling's message, renormalised after each but the last (the gradient operand
+            // carries its scale in EV, and U_c is renormalised after its product)
+            const int k_last = t.kdesc[k1 - 1].x == c ? k1 - 2 : k1 - 1;
             for (int k = k0; k < k1; ++k) {
                 const int2 sb = t.kdesc[k];
                 if (sb.x == c) continue;
@@ -556,7 +564,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                 msg_load(sr, a);
 #pragma unroll
                 for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-                EV += sr.E + renorm_row(v, s.smax, l);
+                EV += sr.E;
+                if (k != k_last) EV += renorm_row(v, s.smax, l);
             }
             // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
             const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];
