@@ -614,11 +614,13 @@ static h3g_status ws_alloc(h3g_ctx* ctx, const WsLayout& L, int precision, DevAr
     } else {
         MixedSizes z;
         z.part = L.part; z.vf = L.vf; z.cols = L.ecols; z.mats = L.mats; z.rs = L.rsz; z.flags = L.ecols / TP;
-        h3g_status st = mixed_alloc(mw, A.ptrs, z);
+        h3g_status st = mixed_alloc(mw, A.ptrs, z, ctx->stream);
         if (st != H3G_OK) return fail(ctx, st, "mixed-precision workspace allocation failed");
     }
     cudaMemsetAsync(w.gc, 0, L.gsz * sizeof(double), ctx->stream);
     cudaMemsetAsync(w.stg, 0, L.gsz * sizeof(double), ctx->stream);
+    // batch slots run on streams of their own: the zeroing completes before any of them starts
+    H3G_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return H3G_OK;
 }
 

@@ -479,7 +479,10 @@ Scratch* scratch_for(h3g_ctx* ctx) {
         const std::vector<uint64_t> inc = host_codon_increments(), z = host_zobrist();
         if (cudaMemcpy(s->pos, pos.data(), pos.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(s->inc, inc.data(), inc.size() * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(s->z, z.data(), z.size() * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaMemcpy(s->z, z.data(), z.size() * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+            // a copy from pageable memory may return before its DMA lands, and the kernels run on a
+            // non-blocking stream that does not wait for the default stream
+            cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) {
             delete s;
             return nullptr;
         }

@@ -858,7 +858,7 @@ void mixed_configure() {
     cudaFuncSetAttribute(k_outside_mx, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMxSmem));
 }
 
-h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z) {
+h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z, cudaStream_t st) {
     auto take = [&](auto** ptr, size_t count) -> bool {
         void* p = nullptr;
         if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(**ptr)) != cudaSuccess) return false;
@@ -871,14 +871,18 @@ h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSize
               take(&mw.ED, cols) && take(&mw.EM, cols) && take(&mw.EU, cols) && take(&mw.PT32, mats) &&
               take(&mw.rs32, z.rs);
     // partials start at zero (their padding states 61 .. 63 are then zero before any evaluation)
-    ok = ok && cudaMemset(mw.D, 0, part * sizeof(float)) == cudaSuccess && cudaMemset(mw.Ms, 0, part * sizeof(float)) == cudaSuccess &&
-         cudaMemset(mw.U, 0, part * sizeof(float)) == cudaSuccess &&
-         cudaMemset(mw.Vf, 0, z.vf * sizeof(float)) == cudaSuccess;
+    // on the evaluations' stream: a default-stream memset is not ordered before the kernels of a
+    // non-blocking stream, and one landing after the first evaluation has begun clears published flags
+    ok = ok && cudaMemsetAsync(mw.D, 0, part * sizeof(float), st) == cudaSuccess &&
+         cudaMemsetAsync(mw.Ms, 0, part * sizeof(float), st) == cudaSuccess &&
+         cudaMemsetAsync(mw.U, 0, part * sizeof(float), st) == cudaSuccess &&
+         cudaMemsetAsync(mw.Vf, 0, z.vf * sizeof(float), st) == cudaSuccess;
     for (int q = 0; q < 3 && ok; ++q) ok = take(&mw.Bp[q], mats) && take(&mw.Bpt[q], mats);
     const size_t flags = z.flags;
     ok = ok && take(&mw.flag_in, flags) && take(&mw.flag_out, flags) && take(&mw.sync, 4);
-    ok = ok && cudaMemset(mw.flag_in, 0, flags * sizeof(int)) == cudaSuccess &&
-         cudaMemset(mw.flag_out, 0, flags * sizeof(int)) == cudaSuccess && cudaMemset(mw.sync, 0, 4 * sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(mw.flag_in, 0, flags * sizeof(int), st) == cudaSuccess &&
+         cudaMemsetAsync(mw.flag_out, 0, flags * sizeof(int), st) == cudaSuccess &&
+         cudaMemsetAsync(mw.sync, 0, 4 * sizeof(int), st) == cudaSuccess;
     return ok ? H3G_OK : H3G_ERR_OOM;
 }
 

@@ -49,7 +49,8 @@ void mixed_configure();
 struct MixedSizes {
     size_t part = 0, vf = 0, cols = 0, mats = 0, rs = 0, flags = 0;
 };
-h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z);
+// the buffers' zeroing is enqueued on st (the stream the evaluations run on)
+h3g_status mixed_alloc(MixedWork& mw, std::vector<void*>& owned, const MixedSizes& z, cudaStream_t st);
 // caller-supplied P: the split-precision operands from w.P / w.rs (new epoch included)
 int mixed_prepare(const Topo& t, const Model& md, const Work& w, const MixedWork& mw, cudaStream_t s);
 // P, dP and the split-precision operands in one launch (h3g_fp64.cu); the FP64 P and P^T are not stored

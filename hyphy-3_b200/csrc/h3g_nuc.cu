@@ -296,6 +296,9 @@ NucState* nuc_state(h3g_problem* pr, const FelProblemView& v, std::string* err) 
              cudaMemcpy(s->d_lv, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
     else if (ok)
         ok = take(&s->d_stk, size_t(deepest) * s->Pp) && take(&s->d_exp, size_t(deepest) * s->Pp);
+    // the copies above come from pageable memory on the default stream, which the evaluator's
+    // non-blocking stream does not wait for
+    ok = ok && cudaStreamSynchronize(cudaStreamLegacy) == cudaSuccess;
     if (!ok) {
         *err = "device allocation failed";
         delete s;

@@ -143,3 +143,24 @@ def test_api_memory_budget_is_bit_identical(ctx, oracle):
     assert got["log_likelihood"] == ref["log_likelihood"]
     for k in ("grad_branches", "grad_omegas", "grad_theta", "grad_weights", "site_log_likelihoods"):
         assert np.array_equal(np.asarray(got[k]), np.asarray(ref[k])), k
+
+
+def test_first_evaluation_after_each_reallocation(ctx, oracle):
+    """A new workspace is zeroed on the evaluations' stream before its first evaluation: ten
+    reallocations (alternating A-accumulation chunks and checkpoint block sizes), each followed at
+    once by a mixed evaluation, raise no expired wait, and that first evaluation equals the next one
+    on the same workspace bit for bit.  Zeroing on the default stream instead raced with the first
+    evaluation's published flags and, now and then, left a wait to expire."""
+    from hyphy3 import _capi
+    pr, args, bl = _problem(ctx, oracle, 1)
+    pr.set_model(precision=_capi.PREC_MIXED, **args)
+    ref = pr.eval(bl, WANT_ALL)
+    for i in range(10):
+        if i % 2:
+            pr.set_memory_budget(0, 9 if i % 4 == 1 else 0)
+        else:
+            pr.set_tuning(a_chunk=256 if i % 4 == 0 else 512)
+        first = pr.eval(bl, WANT_ALL)
+        _same(first, pr.eval(bl, WANT_ALL))
+        assert abs(first["lnl"] - ref["lnl"]) <= 1e-12 * abs(ref["lnl"])
+    pr.close()
