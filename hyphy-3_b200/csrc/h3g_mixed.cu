@@ -616,20 +616,22 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
 // stream into a kRing-deep shared-memory ring by 16-byte cp.async (one commit
 // group per tile); the threads split the oldest ring slot into one of two
 // BF16 MMA stages; one thread issues the MMAs of that stage asynchronously.
-// Copies for tile k+2, the split of tile k and the MMAs of tile k-1 overlap.
+// Copies for tiles k+1 .. k+3, the split of tile k and the MMAs of tile k-1 overlap.
 // grid (n, M, nchunk), block 512 (warp w: TMEM lane quadrant w % 4, column quarter w / 4).
 constexpr int kAccThreads = 512;
 constexpr int kAT = 64;                                   // patterns per tile (MMA K per tile)
 constexpr int kADrain = 16;                               // tiles per FP32 accumulation group
-constexpr int kRing = 3;                                  // FP32 tiles in flight
+constexpr int kRing = 4;                                  // FP32 tiles in flight
 constexpr uint32_t kVRows = 3 * SP;                       // stacked V terms
 constexpr uint32_t kVLbo = (kVRows / 8) * 128;            // K-chunk stride in the V stack
 constexpr uint32_t kDLbo = (SP / 8) * 128;                // K-chunk stride in a D term
 constexpr size_t kVStage = size_t(kVRows) * kAT * 2;      // 24 KB
 constexpr size_t kDTerm = size_t(SP) * kAT * 2;           // 8 KB
 constexpr size_t kStage = kVStage + 3 * kDTerm;           // 48 KB per BF16 MMA stage
-constexpr uint32_t kRawRow = kAT * 4 + 16;                // padded FP32 row: conflict-free 16-byte reads
-constexpr size_t kRawOp = size_t(SP) * kRawRow;           // 17 KB per operand
+// FP32 row of a tile, unpadded: its 16-byte chunk j sits at position j ^ (row & 7), so the 16-byte
+// reads of 8 consecutive rows hit 8 different bank groups (the padding this replaces cost the 4th ring slot)
+constexpr uint32_t kRawRow = kAT * 4;
+constexpr size_t kRawOp = size_t(SP) * kRawRow;           // 16 KB per operand
 constexpr size_t kRawSlot = 2 * kRawOp;                   // V and D
 constexpr size_t kAccSmem = 2 * kStage + kRing * kRawSlot + 8 * 2 + 16;
 // Two TMEM accumulator sets of 4 x 64 columns (all 512 columns: the shared memory above admits one
@@ -681,8 +683,9 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ void ld_row8(const unsigned char* raw, int row, int kc, float (&x)[8]) {
-    const float4* r = reinterpret_cast<const float4*>(raw + row * kRawRow + kc * 32);
-    const float4 a = r[0], b = r[1];
+    const unsigned char* rb = raw + row * kRawRow;
+    const float4 a = *reinterpret_cast<const float4*>(rb + (((2 * kc) ^ (row & 7)) << 4));
+    const float4 b = *reinterpret_cast<const float4*>(rb + (((2 * kc + 1) ^ (row & 7)) << 4));
     x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
 }
 
@@ -722,8 +725,9 @@ __global__ void __launch_bounds__(kAccThreads, 1) k_accumA_mx(Topo t, Model md, 
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int c = tid + kAccThreads * q, r = c >> 4, c16 = c & 15;
-                cp_async16(dst + r * kRawRow + c16 * 16, Vb + size_t(r) * Pp + p0 + 4 * c16);
-                if (!lf) cp_async16(dst + kRawOp + r * kRawRow + c16 * 16, Db + size_t(r) * Pp + p0 + 4 * c16);
+                const int pc = (c16 ^ (r & 7)) * 16;
+                cp_async16(dst + r * kRawRow + pc, Vb + size_t(r) * Pp + p0 + 4 * c16);
+                if (!lf) cp_async16(dst + kRawOp + r * kRawRow + pc, Db + size_t(r) * Pp + p0 + 4 * c16);
             }
             if (lf && tx >= 0 && tid < 36) {
                 // a leaf's states (64 B) and masks (512 B) of the tile, in the unused D area of the slot
