@@ -81,6 +81,18 @@ __device__ __forceinline__ int renorm_row(float (&v)[kSG], float* smax, const La
     return sh;
 }
 
+// After a node's last child product the product that follows renormalises anyway: skip the
+// exchange when every thread's 16 states reach 2^-64 (power-of-two scaling is exact, so the results
+// are the same), renormalise otherwise.  Without this guard, products at extreme branch lengths ran
+// into the FP32 subnormal range and the gradient operand's scale overflowed.
+__device__ __forceinline__ int renorm_if_small(float (&v)[kSG], float* smax, const Lane& l) {
+    float mx = 0.f;
+#pragma unroll
+    for (int i = 0; i < kSG; ++i) mx = fmaxf(mx, v[i]);
+    if (__syncthreads_and(mx >= 0x1p-64f)) return 0;
+    return renorm_row(v, smax, l);
+}
+
 // Where this thread's 16 states of a child's message live: a contiguous
 // row of PT32 / rs32 for a leaf (one-hot or fully ambiguous codon), a masked
 // sum of PT32 rows (partially ambiguous codon), or the child's stored message
@@ -404,9 +416,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 __syncthreads();
                 // the first two children's messages load together (padding states are zero in every
                 // message), then one product and one renormalisation; further children one at a time.
-                // The product with the last child is not renormalised: the message product that follows
-                // is (power-of-two scaling is exact, so only values in the FP32 subnormal range, far
-                // below any realistic overlap of two normalised messages, could tell the difference)
+                // The product with the last child is renormalised only when it is small (renorm_if_small)
                 const MsgSrc s0 = msg_src(t, mw, m, M, t.kdesc[k0], p, l.g, so);
                 E = s0.E;
                 if (k0 + 1 < k1) {
@@ -420,19 +430,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                 } else {
                     msg_load(s0, v);
                 }
-                if (k0 + 2 < k1) E += renorm_row(v, s.smax, l);
+                E += k0 + 2 < k1 ? renorm_row(v, s.smax, l) : renorm_if_small(v, s.smax, l);
                 for (int k = k0 + 2; k < k1; ++k) {
                     const MsgSrc sr = msg_src(t, mw, m, M, t.kdesc[k], p, l.g, so);
                     float a[kSG];
                     msg_load(sr, a);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-                    E += sr.E;
-                    if (k + 1 < k1) E += renorm_row(v, s.smax, l);
+                    E += sr.E + (k + 1 < k1 ? renorm_row(v, s.smax, l) : renorm_if_small(v, s.smax, l));
                 }
             } else {
                 // a chain node: its only internal child is the previous node (message in v, exponent E);
-                // the other children are leaves (the last product again left to the message's renormalisation)
+                // the other children are leaves (the last product again through renorm_if_small)
                 const int k_last = t.kdesc[k1 - 1].x == carried ? k1 - 2 : k1 - 1;
                 for (int k = k0; k < k1; ++k) {
                     const int2 d = t.kdesc[k];
@@ -442,8 +451,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_inside_mx(Topo t, Model md, Wor
                     msg_load(sr, a);
 #pragma unroll
                     for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-                    E += sr.E;
-                    if (k != k_last) E += renorm_row(v, s.smax, l);
+                    E += sr.E + (k != k_last ? renorm_row(v, s.smax, l) : renorm_if_small(v, s.smax, l));
                 }
             }
             store_part(v, mw.D + part_off(iu, m, M, t.Pp) + so, Pp);
@@ -553,8 +561,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                     EV = __ldcg(mw.EU + col_off(iu, m, M, t.Pp) + p);
                 }
             }
-            // times every sibling's message, renormalised after each but the last (the gradient operand
-            // carries its scale in EV, and U_c is renormalised after its product)
+            // times every sibling's message, renormalised after each (after the last only when it is
+            // small: the gradient operand carries its scale in EV, and U_c is renormalised after its product)
             const int k_last = t.kdesc[k1 - 1].x == c ? k1 - 2 : k1 - 1;
             for (int k = k0; k < k1; ++k) {
                 const int2 sb = t.kdesc[k];
@@ -564,8 +572,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_outside_mx(Topo t, Model md, Wo
                 msg_load(sr, a);
 #pragma unroll
                 for (int i = 0; i < kSG; ++i) v[i] *= a[i];
-                EV += sr.E;
-                if (k != k_last) EV += renorm_row(v, s.smax, l);
+                EV += sr.E + (k != k_last ? renorm_row(v, s.smax, l) : renorm_if_small(v, s.smax, l));
             }
             // gradient operand: f * V_true * D-scale, with V_true = v * 2^-EV and D_true = D * 2^-ED_c
             const int EL = mw.ED[col_off(ir, m, M, t.Pp) + p];

@@ -103,3 +103,25 @@ def test_mixed_deep_tree_no_underflow(ctx, oracle):
     ref_l, ref_g = oracle.branch_length_gradients(t, a, p, list(bl))
     assert abs(lnl - ref_l) / abs(ref_l) <= LNL_TOL
     assert _norm_rel(g, ref_g) <= GRAD_TOL
+
+
+def test_mixed_extreme_branch_lengths_stay_finite(ctx, oracle):
+    """Branch lengths pushed towards both ends (x e^{+-18}, clipped to [1e-8, 1e4], as an optimiser's
+    first trial step does): the mixed path's lnL and gradients stay finite and its lnL follows
+    FP64's (to 1e-6 here).  Products of nearly disjoint messages reach the FP32 subnormal range here; a node's last
+    product is then renormalised (renorm_if_small), else the gradient operand's scale overflows."""
+    from hyphy3 import _capi
+    t, a, wl = _workload(oracle, 1, n_sites=300)
+    p = {"alpha": 1.0, "beta": 0.5, "theta": list(wl.theta)}
+    Q, lam, U, V, _ = eigensystems(oracle, a, [p])
+    pr = problem_from_oracle(ctx, oracle, t, a)
+    rng = np.random.default_rng(5)
+    bl = np.array(t.branch_lengths) * np.exp(rng.choice([-18.0, 18.0], size=t.num_nodes()))
+    bl = np.clip(bl, 1e-8, 1e4)
+    bl[t.root] = 0.0
+    l64, g64 = pr.branch_length_gradients(pi=a.pi, Q=Q[0], lam=lam[0], U=U[0], V=V[0], bl=bl, precision=_capi.PREC_FP64)
+    lmx, gmx = pr.branch_length_gradients(pi=a.pi, Q=Q[0], lam=lam[0], U=U[0], V=V[0], bl=bl, precision=_capi.PREC_MIXED)
+    assert np.isfinite(l64) and np.isfinite(lmx)
+    assert np.all(np.isfinite(gmx)), np.flatnonzero(~np.isfinite(gmx))
+    assert abs(lmx - l64) / abs(l64) <= 10 * LNL_TOL       # far outside the fitted regime: a looser bar
+    pr.close()
