@@ -1,6 +1,6 @@
 """Split-precision tensor-core path vs the FP64 oracle.
 
-Accuracy bar (north star): |dlnL|/|lnL| <= 1e-7 and gradient relative error
+Accuracy bar of the mixed path: |dlnL|/|lnL| <= 1e-7 and gradient relative error
 (2-norm over all reported components) <= 1e-5 against FP64 on the same inputs.
 """
 import numpy as np
