@@ -352,13 +352,13 @@ __device__ __forceinline__ void wait_item(const int* flag, int epoch, int* err, 
         __nanosleep(64);
     }
 }
-// all threads: the partials are stored; make them visible and raise the flag
+// all threads: the partials are stored; make them visible and raise the flag.  Every thread's stores
+// precede the CTA barrier, the barrier synchronises them with thread 0, and thread 0's release store
+// (st.release.gpu, cumulative) orders all of them before the flag for a reader that acquires it
+// (wait_item's ld.acquire.gpu followed by its CTA barrier): no separate __threadfence is needed.
 __device__ __forceinline__ void publish(int* flag, int epoch) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        st_release(flag, epoch);
-    }
+    if (threadIdx.x == 0) st_release(flag, epoch);
 }
 // all threads: the item's partials are stored; make them visible, raise its flag, and
 // claim the CTA's next item in the same step (the item being published waits for nothing
@@ -367,8 +367,7 @@ __device__ __forceinline__ int publish_and_claim(int* flag, int epoch, int* ctr,
     __syncthreads();
     if (threadIdx.x == 0) {
         const int next = atomicAdd(ctr, 1);
-        __threadfence();
-        st_release(flag, epoch);
+        st_release(flag, epoch);                  // ordered as in publish()
         *s_item = next;
     }
     __syncthreads();
